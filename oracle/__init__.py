@@ -1,0 +1,377 @@
+"""CPU checkers for the SVBRDF fitting path.  TEST INFRASTRUCTURE ONLY.
+
+Two libraries sit behind this module, both built by ``oracle/Makefile``:
+
+* ``libsvf_oracle.so`` -- the C restatement of the reference path
+  (``svf_oracle.c``); always available.
+* ``_ref/libtempest_ref.so`` -- the reference's own CPU fitter compiled from its
+  sources with ``ref_harness.cc``; available where it was built.
+
+Only tests, ``bench.py``'s CPU-baseline leg and ``__graft_entry__.smoke()`` use
+them, as checkers or as the timed CPU baseline.  The product package
+(``tempestrenderer_b200``) never imports this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import struct
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libsvf_oracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libtempest_ref.so")
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+
+
+def build(reference_root: str | None = None) -> None:
+    """Builds the restatement and, when the reference sources exist, the reference."""
+    args = ["make", "-s", "-C", HERE, "-j8", "all"]
+    if reference_root:
+        args.append(f"REFERENCE_ROOT={reference_root}")
+    subprocess.run(args, check=True)
+
+
+# ----------------------------------------------------------------------------
+# the C restatement
+# ----------------------------------------------------------------------------
+
+
+class LsqStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("effective", C.c_uint32),
+                ("jacobians", C.c_uint32), ("residuals", C.c_uint32), ("mse", C.c_double)]
+
+
+class Mesh(C.Structure):
+    _fields_ = [("lights_parabolic", C.c_void_p), ("light_count", C.c_uint32),
+                ("triangles", C.c_void_p), ("triangle_count", C.c_uint32),
+                ("edges", C.c_void_p), ("edge_angles", C.c_void_p), ("edge_count", C.c_uint32)]
+
+
+class InitInfo(C.Structure):
+    _fields_ = [("ndf_denom", C.c_float), ("normal", C.c_float * 3), ("tangent", C.c_float * 3),
+                ("basis", C.c_float * 9), ("sggx_stddev", C.c_float * 3)]
+
+
+class Truth(C.Structure):
+    _fields_ = [("kd", C.c_float * 3), ("ks", C.c_float * 3), ("sigma", C.c_float * 2),
+                ("quat", C.c_float * 4), ("euler", C.c_float * 3), ("kind", C.c_uint32)]
+
+
+_oracle = None
+
+
+def lib():
+    global _oracle
+    if _oracle is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = C.CDLL(ORACLE_SO)
+        L.svfo_ring81_angles.argtypes = [_f32p]
+        L.svfo_ring81_angles.restype = C.c_uint32
+        L.svfo_angles_to_parabolic.argtypes = [_f32p, C.c_uint32, _f32p]
+        L.svfo_brdf_f32.argtypes = [_f64p, _f32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float]
+        L.svfo_brdf_f32.restype = C.c_float
+        L.svfo_brdf_f64.argtypes = [_f64p, _f32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double]
+        L.svfo_brdf_f64.restype = C.c_double
+        L.svfo_brdf_eval_all.argtypes = [_f64p, _f32p, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]
+        L.svfo_lsq_fit.argtypes = [_f32p, _f32p, C.c_uint32, C.c_float, C.c_uint32, _f32p, _f32p,
+                                   C.POINTER(LsqStats)]
+        L.svfo_lsq_fit.restype = C.c_float
+        L.svfo_lum_slice.argtypes = [_f32p, C.c_uint32, _f32p, _f32p]
+        L.svfo_sample_lum.argtypes = [C.POINTER(Mesh), _f32p, _f32p, _f32p]
+        L.svfo_sample_lum.restype = C.c_float
+        L.svfo_ndf_texture.argtypes = [C.POINTER(Mesh), _f32p, _f32p]
+        L.svfo_ndf_sample.argtypes = [_f32p, C.c_float, C.c_float]
+        L.svfo_ndf_sample.restype = C.c_float
+        L.svfo_default_init_from_ndf.argtypes = [_f32p, _f32p, C.POINTER(InitInfo)]
+        L.svfo_decompose.argtypes = [_f32p, _f32p, _f32p]
+        L.svfo_euler_to_matrix.argtypes = [_f32p, C.c_void_p, C.c_void_p]
+        L.svfo_philox4x32.argtypes = [_u32p, _u32p, _u32p]
+        L.svfo_synth_truth.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(Truth)]
+        L.svfo_synth_render.argtypes = [C.c_uint32, C.c_uint64, C.POINTER(Truth), _f32p, C.c_uint32,
+                                        C.c_float, _f32p]
+        _oracle = L
+    return _oracle
+
+
+def ring81_angles() -> np.ndarray:
+    out = np.zeros((81, 2), np.float32)
+    n = lib().svfo_ring81_angles(out)
+    assert n == 81
+    return out
+
+
+def angles_to_parabolic(theta_phi: np.ndarray) -> np.ndarray:
+    tp = np.ascontiguousarray(theta_phi, np.float32)
+    out = np.zeros_like(tp)
+    lib().svfo_angles_to_parabolic(tp, tp.shape[0], out)
+    return out
+
+
+def brdf_all(params7, lights_parabolic, fresnel=1.0):
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    L = lp.shape[0]
+    p = np.ascontiguousarray(params7, np.float64)
+    f32 = np.zeros(L * L, np.float32)
+    f64 = np.zeros(L * L, np.float64)
+    lib().svfo_brdf_eval_all(p, lp, L, fresnel, f32.ctypes.data, f64.ctypes.data)
+    return f32, f64
+
+
+def lsq_fit(lum, lights_parabolic, init7, fresnel=1.0, max_steps=1024):
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    out = np.zeros(7, np.float32)
+    st = LsqStats()
+    rmse = lib().svfo_lsq_fit(np.ascontiguousarray(lum, np.float32), lp, lp.shape[0], fresnel, max_steps,
+                              np.ascontiguousarray(init7, np.float32), out, C.byref(st))
+    return out, float(rmse), st
+
+
+def lum_slice(rgb):
+    rgb = np.ascontiguousarray(rgb, np.float32).reshape(-1, 3)
+    lum = np.zeros(rgb.shape[0], np.float32)
+    avg = np.zeros(3, np.float32)
+    lib().svfo_lum_slice(rgb, rgb.shape[0], lum, avg)
+    return lum, avg
+
+
+class MeshData:
+    """Direction table plus the interpolation mesh (triangles, boundary edges)."""
+
+    def __init__(self, lights_parabolic, triangles, edges, edge_angles):
+        self.lights_parabolic = np.ascontiguousarray(lights_parabolic, np.float32)
+        self.triangles = np.ascontiguousarray(triangles, np.uint32)
+        self.edges = np.ascontiguousarray(edges, np.uint32)
+        self.edge_angles = np.ascontiguousarray(edge_angles, np.float32)
+
+    def cstruct(self) -> Mesh:
+        return Mesh(self.lights_parabolic.ctypes.data, self.lights_parabolic.shape[0],
+                    self.triangles.ctypes.data, self.triangles.shape[0],
+                    self.edges.ctypes.data, self.edge_angles.ctypes.data, self.edges.shape[0])
+
+    def save(self, path):
+        np.savez(path, lights_parabolic=self.lights_parabolic, triangles=self.triangles,
+                 edges=self.edges, edge_angles=self.edge_angles)
+
+    @staticmethod
+    def load(path) -> "MeshData":
+        z = np.load(path)
+        return MeshData(z["lights_parabolic"], z["triangles"], z["edges"], z["edge_angles"])
+
+
+def ndf_texture(mesh: MeshData, lum) -> np.ndarray:
+    ndf = np.zeros(64 * 64, np.float32)
+    m = mesh.cstruct()
+    lib().svfo_ndf_texture(C.byref(m), np.ascontiguousarray(lum, np.float32), ndf)
+    return ndf
+
+
+def default_init_from_ndf(ndf):
+    init = np.zeros(7, np.float32)
+    info = InitInfo()
+    lib().svfo_default_init_from_ndf(np.ascontiguousarray(ndf, np.float32), init, C.byref(info))
+    return init, info
+
+
+def euler_to_matrix(euler3):
+    m = np.zeros(9, np.float32)
+    q = np.zeros(4, np.float32)
+    lib().svfo_euler_to_matrix(np.ascontiguousarray(euler3, np.float32), m.ctypes.data, q.ctypes.data)
+    return m.reshape(3, 3), q  # m[c] is column c
+
+
+def synth_truth(seed, mix, texel) -> Truth:
+    t = Truth()
+    lib().svfo_synth_truth(seed, mix, texel, C.byref(t))
+    return t
+
+
+def synth_render(seed, texel, truth: Truth, lights_parabolic, noise=0.01):
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    L = lp.shape[0]
+    rgb = np.zeros((L * L, 3), np.float32)
+    lib().svfo_synth_render(seed, texel, C.byref(truth), lp, L, noise, rgb)
+    return rgb
+
+
+def truth_lum_params(t: Truth) -> np.ndarray:
+    """The 7 luminance-model parameters of a synthetic texel."""
+    kd = np.array(t.kd[:], np.float32)
+    ks = np.array(t.ks[:], np.float32)
+    w = np.array([0.2126, 0.7152, 0.0722], np.float32)
+    return np.array([t.sigma[0], t.sigma[1], float(ks @ w), float(kd @ w), *t.euler[:]], np.float32)
+
+
+# ----------------------------------------------------------------------------
+# DFMF writer (the layout LoadBTF parses, src/image/btf.cc:389-1000)
+# ----------------------------------------------------------------------------
+
+
+def write_dfmf(path, theta_phi, rgb_texels, width=None, height=1, data_size=4):
+    """Writes texels [T][N][3] as a DFMF BTF whose SVD factors reproduce the
+    samples exactly: per channel, U = samples^T ([N][K], K = T) and SxV = I.
+
+    Texel t sits at file column t; LoadBTF flips rows (btf.cc:1000-1022), so with
+    height 1 texel t is at (x = t, y = 0) after loading.
+    """
+    rgb_texels = np.asarray(rgb_texels, np.float32)
+    T, N, _ = rgb_texels.shape
+    L = theta_phi.shape[0]
+    assert N == L * L
+    width = width or T
+    assert width * height == T
+    dt = {2: np.float16, 4: np.float32, 8: np.float64}[data_size]
+    with open(path, "wb") as f:
+        f.write(b"!")
+        f.write(b"DFMF")
+        f.write(b"08FC")
+        # BTFCommonHeader (btf.hh:48-57): Size, Version, 3x80 chars, PPMM, RGB
+        hdr = struct.pack("<II", 264, 1) + b"\0" * 240 + struct.pack("<f3f", 0.0, 1.0, 1.0, 1.0)
+        assert len(hdr) == 264
+        f.write(hdr)
+        f.write(struct.pack("<I", L))
+        tp = np.ascontiguousarray(theta_phi, np.float32)
+        for v in range(L):
+            f.write(tp[v].tobytes())
+            f.write(struct.pack("<I", L))
+            f.write(tp.tobytes())
+        f.write(struct.pack("<II", width, height))
+        f.write(struct.pack("<II", T, 0))                 # num_components, ColorModel
+        f.write(struct.pack("<3f", 0.0, 0.0, 0.0))        # ColorMean
+        f.write(np.eye(3, dtype=np.float32).tobytes())    # ColorTransform
+        eye = np.eye(T, dtype=dt)
+        for c in range(3):
+            f.write(struct.pack("<B", data_size))
+            f.write(struct.pack("<III", T, N, T))
+            f.write(np.ones(T, dt).tobytes())             # scalars
+            u = np.ascontiguousarray(rgb_texels[:, :, c].T.astype(dt))   # [N][K]
+            f.write(u.tobytes())
+            f.write(eye.tobytes())                         # SxV [cols][K]
+
+
+# ----------------------------------------------------------------------------
+# the reference build
+# ----------------------------------------------------------------------------
+
+_ref = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        L = C.CDLL(REF_SO)
+        L.ref_btf_load.argtypes = [C.c_char_p]
+        L.ref_btf_load.restype = C.c_void_p
+        L.ref_btf_free.argtypes = [C.c_void_p]
+        L.ref_btf_info.argtypes = [C.c_void_p, _u32p]
+        L.ref_btf_geometry.argtypes = [C.c_void_p, _f32p, _u32p, _u32p, _f32p]
+        L.ref_btf_fetch.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _f32p]
+        L.ref_btf_lum_slice.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _f32p, _f32p]
+        L.ref_brdf_eval.argtypes = [_f32p, C.c_uint32, C.c_float, _f64p, _f32p]
+        L.ref_lsq.argtypes = [_f32p, C.c_uint32, _f32p, C.c_float, C.c_uint32, _f32p, _f32p,
+                              C.POINTER(C.c_float), _u32p]
+        L.ref_fit_texel.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, _f32p, _f32p, _f32p,
+                                    C.POINTER(C.c_float), _u32p, C.c_void_p, C.c_void_p]
+        L.ref_fit_texel.restype = C.c_int
+        L.ref_time_fit_texels.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.c_float, C.c_void_p]
+        L.ref_time_fit_texels.restype = C.c_double
+        _ref = L
+    return _ref
+
+
+LSF_OPTON_DIFFUSE = 1 << 1
+
+
+class RefBTF:
+    """A BTF loaded by the reference's LoadBTF."""
+
+    def __init__(self, path):
+        self.handle = ref().ref_btf_load(path.encode())
+        if not self.handle:
+            raise RuntimeError(f"LoadBTF failed on {path}")
+        dims = np.zeros(5, np.uint32)
+        ref().ref_btf_info(self.handle, dims)
+        self.width, self.height, self.light_count, self.tri_count, self.edge_count = map(int, dims)
+
+    @staticmethod
+    def from_texels(theta_phi, rgb_texels, data_size=4) -> "RefBTF":
+        fd, path = tempfile.mkstemp(suffix=".btf")
+        os.close(fd)
+        try:
+            write_dfmf(path, theta_phi, rgb_texels, data_size=data_size)
+            return RefBTF(path)
+        finally:
+            os.unlink(path)
+
+    def mesh(self) -> MeshData:
+        L = self.light_count
+        lp = np.zeros((L, 2), np.float32)
+        tri = np.zeros((self.tri_count, 3), np.uint32)
+        e = np.zeros((self.edge_count, 3), np.uint32)
+        ea = np.zeros((self.edge_count, 2), np.float32)
+        ref().ref_btf_geometry(self.handle, lp, tri, e, ea)
+        return MeshData(lp, tri, e, ea)
+
+    def lum_slice(self, x, y=0):
+        N = self.light_count ** 2
+        lum = np.zeros(N, np.float32)
+        avg = np.zeros(3, np.float32)
+        ref().ref_btf_lum_slice(self.handle, x, y, lum, avg)
+        return lum, avg
+
+    def fit_texel(self, x, y=0, fresnel=1.0, want_ndf=False):
+        init7 = np.zeros(7, np.float32)
+        fit7 = np.zeros(7, np.float32)
+        maps = np.zeros(12, np.float32)
+        rmse = C.c_float()
+        st = np.zeros(2, np.uint32)
+        ndf = np.zeros(64 * 64, np.float32) if want_ndf else None
+        rc = ref().ref_fit_texel(self.handle, x, y, fresnel, init7, fit7, maps, C.byref(rmse), st,
+                                 ndf.ctypes.data if want_ndf else None, None)
+        if rc != 0:
+            raise RuntimeError("reference pipeline did not reach LeastSquaresFitSGGX")
+        return dict(init=init7, fit=fit7, maps=maps, rmse=rmse.value, iterations=int(st[0]),
+                    effective=int(st[1]), ndf=ndf)
+
+    def time_fit(self, first, count, workers, pool_threads, fresnel=1.0):
+        rm = np.zeros(count, np.float32)
+        secs = ref().ref_time_fit_texels(self.handle, first, count, workers, pool_threads, fresnel,
+                                         rm.ctypes.data)
+        return secs, rm
+
+    def __del__(self):
+        try:
+            if self.handle:
+                ref().ref_btf_free(self.handle)
+        except Exception:
+            pass
+
+
+def ref_lsq(lum, lights_parabolic, init7, fresnel=1.0, flags=LSF_OPTON_DIFFUSE):
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    out = np.zeros(7, np.float32)
+    rmse = C.c_float()
+    st = np.zeros(2, np.uint32)
+    ref().ref_lsq(lp, lp.shape[0], np.ascontiguousarray(lum, np.float32), fresnel, flags,
+                  np.ascontiguousarray(init7, np.float32), out, C.byref(rmse), st)
+    return out, rmse.value, int(st[0]), int(st[1])
+
+
+def ref_brdf_all(params7, lights_parabolic, fresnel=1.0):
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    L = lp.shape[0]
+    out = np.zeros(L * L, np.float32)
+    ref().ref_brdf_eval(lp, L, fresnel, np.ascontiguousarray(params7, np.float64), out)
+    return out
