@@ -1,0 +1,225 @@
+/*
+ * svf.h - C ABI of the B200 SVBRDF fitter (libsvf.so).
+ *
+ * Fits, texel by texel, a Lambert + anisotropic SGGX surface BRDF to a BTF with
+ * Levenberg-Marquardt, on one NVIDIA B200 (sm_100a).  This is the drop-in for
+ * the fitting path of TempestRenderer's svbrdffit tool:
+ *
+ *   svf_lsq_fit_sggx  replaces LeastSquaresFitSGGX
+ *                     (tools/svbrdf-fitting/svbrdf-fitting.hh:126-127,
+ *                      defined in svbrdf-lsq-fitting-setup.cc:234-431), and its
+ *                     CUDA variant LeastSquaresFitSGGXCuda
+ *                     (svbrdf-lsq-fitting-internal.hh:225-227).
+ *   svf_lsq_fit_batch the same fit for many texels in one launch.
+ *   svf_fit_texels    replaces the svbrdffit texel loop: PusherThread::execute
+ *                     (svbrdf-fitting.cc:86-121) running SVBRDFFitPipeline::cache
+ *                     and ::fit (svbrdf-fitting-pipeline.cc:240-733) on every
+ *                     texel, i.e. luminance slice, default initial guess, LM and
+ *                     the output maps (svbrdf-fitting.cc:713-735).
+ *
+ * Conventions (as in the reference):
+ *   - L directions serve as both light and view directions; they are given in
+ *     parabolic coordinates (BTF::LightsParabolic, btf.hh:114).
+ *   - A direction pair is lv = view * L + light (light fastest).
+ *   - The 7 fitted parameters are, in order, {sigma_x, sigma_y, specular,
+ *     diffuse, euler_x, euler_y, euler_z} (OptimizationParameters,
+ *     svbrdf-fitting.hh:55-65).
+ *   - Buffers are caller-owned.  Every pointer argument may point to host
+ *     memory or to device memory of the context's device; the library detects
+ *     which.  Host buffers are staged through pinned memory in chunks.
+ *
+ * Errors are returned as svf_status codes; no exception crosses the ABI.
+ * svf_last_error() gives a message for the calling thread's last failure.
+ * A context may be used by one host thread at a time.
+ */
+#ifndef SVF_H
+#define SVF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SVF_ABI_VERSION 1u
+
+typedef enum svf_status
+{
+    SVF_OK = 0,
+    SVF_EINVAL = 1,     /* an argument is out of range or inconsistent */
+    SVF_ENOMEM = 2,     /* device or pinned host allocation failed */
+    SVF_ECUDA = 3,      /* a CUDA call failed; see svf_last_error() */
+    SVF_ETIMEOUT = 4,   /* a bounded device wait expired (no texel result is trusted) */
+    SVF_EPARTIAL = 5,   /* finished, but some texels carry a non-zero status */
+    SVF_ENODEV = 6      /* no usable sm_100 device */
+} svf_status;
+
+/* per-texel status bits (svf_texel_stats::status) */
+#define SVF_TEXEL_NONFINITE  1u  /* NaN/Inf in the data or the fit; params are the initial guess */
+#define SVF_TEXEL_MAX_ITER   2u  /* stopped at max_iterations */
+#define SVF_TEXEL_TIMEOUT    4u  /* the texel's samples did not arrive (bounded wait expired) */
+
+/* LeastSquaresFitOptions (svbrdf-fitting.hh:100-107) for the supported path */
+#define SVF_LSQ_DIFFUSE      (1u << 1)   /* LSF_OPTON_DIFFUSE: fit the Lambert term (7 parameters) */
+
+typedef struct svf_lsq_options
+{
+    uint32_t max_iterations;      /* CurveFitSteps (svbrdf-fitting.hh:51): 1024 */
+    float    fresnel;             /* refractive index of the Fresnel term; 1 = no Fresnel */
+    uint32_t flags;               /* must contain SVF_LSQ_DIFFUSE */
+    double   mse_target;          /* LevenbergMarquardtCurveFit mean_sq_error: 1e-6 */
+    double   break_on_small_step; /* LevenbergMarquardtSettings::BreakOnSmallStep: 1e-3 */
+} svf_lsq_options;
+
+typedef struct svf_texel_stats
+{
+    uint32_t iterations;   /* FitStatistics::IterationCount */
+    uint32_t effective;    /* FitStatistics::EffectiveIterationCount (accepted steps) */
+    uint32_t jacobians;    /* Jacobian + normal-equation builds */
+    uint32_t residuals;    /* residual-only evaluations (trial steps) */
+    uint32_t status;       /* SVF_TEXEL_* bits */
+} svf_texel_stats;
+
+typedef struct svf_ctx svf_ctx;
+
+/* Library and error reporting -------------------------------------------------- */
+uint32_t    svf_abi_version(void);
+const char* svf_status_string(svf_status status);
+const char* svf_last_error(void);
+
+/* Fills the reference's defaults: 1024 iterations, Fresnel 1 (svbrdffit -n 1),
+ * SVF_LSQ_DIFFUSE, MSE target 1e-6, small-step break 1e-3
+ * (svbrdf-lsq-fitting-setup.cc:272-273,357-364). */
+void svf_lsq_options_default(svf_lsq_options* options);
+
+/* Contexts ------------------------------------------------------------------- */
+/* Opens a context on CUDA device `device`; it owns streams, device workspaces
+ * and the per-direction-layout tables.  Fails with SVF_ENODEV unless the device
+ * is compute capability 10.x. */
+svf_status svf_create(int device, svf_ctx** out_ctx);
+void       svf_destroy(svf_ctx* ctx);
+
+/* Direction layouts ------------------------------------------------------------ */
+/* The interpolation mesh the default initial guess samples the luminance slice
+ * with (BTF::LightIndices and BTF::Edges, built by LoadBTF, btf.cc:531-625).
+ * Pass the BTF's own mesh to reproduce the reference exactly; or leave
+ * `triangles` NULL and the library triangulates the directions itself
+ * (Delaunay, then the boundary edges as LoadBTF builds them). */
+typedef struct svf_layout_desc
+{
+    const float*    lights_parabolic;  /* [L][2] */
+    uint32_t        light_count;       /* L, 3..160 */
+    const uint32_t* triangles;         /* [triangle_count][3] or NULL */
+    uint32_t        triangle_count;
+    const uint32_t* edges;             /* [edge_count][3]: Index0, Index1, Triangle; or NULL */
+    const float*    edge_angles;       /* [edge_count][2]: Angle0, Angle1 */
+    uint32_t        edge_count;
+} svf_layout_desc;
+
+/* Writes the 81-direction ring layout (theta rings 0/15/30/45/60/75 degrees
+ * holding 1/6/12/18/20/24 phi-uniform directions) in parabolic coordinates as
+ * LoadBTF derives them from (theta, phi).  Returns the direction count (81). */
+uint32_t svf_directions_ring81(float* lights_parabolic /* [81][2] */);
+
+/* Writes `count` directions of a Fibonacci hemisphere lattice (z > 0) in
+ * parabolic coordinates.  Returns count. */
+uint32_t svf_directions_fibonacci(uint32_t count, float* lights_parabolic);
+
+/* Computes a Delaunay mesh of the directions and the boundary edges in the
+ * reference's format.  Returns the triangle count, or 0 on failure.  Sizes:
+ * triangles [2L][3], edges [L][3], edge_angles [L][2] are always enough. */
+uint32_t svf_layout_triangulate(const float* lights_parabolic, uint32_t light_count,
+                                uint32_t* triangles, uint32_t* edges, float* edge_angles,
+                                uint32_t* edge_count);
+
+/* LeastSquaresFitSGGX ------------------------------------------------------------ */
+/* One texel, synchronous: fits `init` to the luminance slice `lum` ([L*L],
+ * lv-indexed) and writes the fitted parameters and the RMSE
+ * (sqrt of the final mean squared residual, as the reference reports it). */
+svf_status svf_lsq_fit_sggx(svf_ctx* ctx, const float* lights_parabolic, uint32_t light_count,
+                            const float* lum, const svf_lsq_options* options,
+                            const float init[7], float out[7], float* rmse,
+                            svf_texel_stats* stats /* may be NULL */);
+
+/* Many texels in one persistent launch.  lum: [texel_count][lum_stride] floats
+ * (lum_stride >= L*L); init/out: [texel_count][7]; rmse: [texel_count];
+ * stats: [texel_count] or NULL. */
+svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lights_parabolic, uint32_t light_count,
+                             const float* lum, uint64_t lum_stride, uint32_t texel_count,
+                             const svf_lsq_options* options, const float* init,
+                             float* out, float* rmse, svf_texel_stats* stats);
+
+/* The svbrdffit texel loop ----------------------------------------------------- */
+#define SVF_SAMPLES_F32 0u
+#define SVF_SAMPLES_F16 1u
+
+#define SVF_INIT_DEFAULT 0u   /* the reference's default initial guess (NDF -> PCA -> SGGX projection) */
+#define SVF_INIT_GIVEN   1u   /* caller-supplied initial parameters (svbrdffit -r refit) */
+
+typedef struct svf_btf_view
+{
+    const void*            samples;      /* [texels][L*L][3] RGB, texel-major, row-major texels */
+    uint32_t               sample_type;  /* SVF_SAMPLES_F32 or SVF_SAMPLES_F16 */
+    uint32_t               width, height;
+    const svf_layout_desc* layout;
+} svf_btf_view;
+
+typedef struct svf_fit_options
+{
+    svf_lsq_options lsq;
+    uint32_t        init_mode;     /* SVF_INIT_* */
+    const float*    init_params;   /* [texels][7] for SVF_INIT_GIVEN */
+} svf_fit_options;
+
+/* The five output maps of svbrdffit (svbrdf-fitting.cc:713-735, values as
+ * SVBRDFFitPipeline::fit assembles them, svbrdf-fitting-pipeline.cc:692-697),
+ * plus optional diagnostics.  Any pointer may be NULL to skip that output. */
+typedef struct svf_maps
+{
+    float*           diffuse;    /* [texels][3]  avg chromaticity * diffuse */
+    float*           specular;   /* [texels][3]  avg chromaticity * specular */
+    float*           sigma;      /* [texels][2]  SGGX standard deviations */
+    float*           basis;      /* [texels][4]  quaternion xyzw = ToQuaternion(euler) */
+    float*           rmse;       /* [texels] */
+    float*           params;     /* [texels][7]  fitted parameters */
+    float*           init;       /* [texels][7]  initial guess used */
+    svf_texel_stats* stats;      /* [texels] */
+} svf_maps;
+
+typedef struct svf_run_stats
+{
+    uint64_t texels;
+    uint64_t iterations;        /* summed over texels */
+    uint64_t jacobians;
+    uint64_t residuals;
+    uint64_t failed_texels;     /* texels with a non-zero status */
+    double   ms_total;          /* device time of the whole run */
+    double   ms_luminance;      /* luminance slice + average chromaticity */
+    double   ms_init;           /* default initial guess */
+    double   ms_fit;            /* Levenberg-Marquardt */
+    double   ms_copy;           /* host<->device staging, when host buffers were given */
+} svf_run_stats;
+
+svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,
+                          const svf_maps* out, svf_run_stats* run /* may be NULL */);
+
+/* Synthetic BTFs (test and benchmark inputs) ------------------------------------ */
+/* Renders texels [first, first + count) of a seeded synthetic BTF straight into
+ * `samples` ([count][L*L][3], device memory, F32 or F16): per texel, ground-truth
+ * parameters are drawn with Philox4x32-10 (key = seed, counter = texel), the
+ * BRDF is evaluated per channel and every sample is multiplied by
+ * (1 + noise * N(0,1)).  mix 0: kd ~ U[0,0.8]^3, ks ~ U[0,1]^3, sigma log-U
+ * [0.02,0.8], normal within 30 degrees of +z; mix 1: 20% near-diffuse
+ * (ks < 0.05), 10% strongly anisotropic (sigma_x/sigma_y > 8, sigma_y < 0.05),
+ * the rest as mix 0.  truth (optional, device or host): [count][16] floats =
+ * kd[3], ks[3], sigma[2], quat[4], euler[3], kind. */
+svf_status svf_synth_btf(svf_ctx* ctx, uint32_t seed, uint32_t mix, const float* lights_parabolic,
+                         uint32_t light_count, uint64_t first, uint64_t count, uint32_t sample_type,
+                         float noise, void* samples, float* truth);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SVF_H */

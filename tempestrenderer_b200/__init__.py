@@ -1,0 +1,283 @@
+"""B200 SVBRDF fitting (Lambert + anisotropic SGGX, Levenberg-Marquardt) over libsvf.so.
+
+Python mirror of the library's C ABI (``include/svf.h``), named after the
+reference interfaces it replaces:
+
+* :func:`lsq_fit_sggx` -- ``LeastSquaresFitSGGX``
+  (tools/svbrdf-fitting/svbrdf-fitting.hh:126-127), one texel;
+* :func:`lsq_fit_batch` -- the same fit for many texels in one launch;
+* :func:`fit_texels` -- the svbrdffit texel loop (``PusherThread::execute``,
+  svbrdf-fitting.cc:86-121, over ``SVBRDFFitPipeline::cache/fit``).
+
+The library is the in-tree ``libsvf.so`` (``python -m tempestrenderer_b200.build``).
+Nothing here computes on the CPU: when the library or a B200 is missing, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsvf.so")
+
+SVF_OK, SVF_EINVAL, SVF_ENOMEM, SVF_ECUDA, SVF_ETIMEOUT, SVF_EPARTIAL, SVF_ENODEV = range(7)
+SVF_TEXEL_NONFINITE, SVF_TEXEL_MAX_ITER, SVF_TEXEL_TIMEOUT = 1, 2, 4
+SVF_LSQ_DIFFUSE = 1 << 1
+SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
+SVF_INIT_DEFAULT, SVF_INIT_GIVEN = 0, 1
+
+# every entry point include/svf.h declares
+EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_options_default", "svf_create",
+           "svf_destroy", "svf_directions_ring81", "svf_directions_fibonacci", "svf_layout_triangulate",
+           "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_fit_texels", "svf_synth_btf")
+
+
+class SvfError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"svf status {status}: {message}")
+        self.status = status
+
+
+class LsqOptions(C.Structure):
+    _fields_ = [("max_iterations", C.c_uint32), ("fresnel", C.c_float), ("flags", C.c_uint32),
+                ("mse_target", C.c_double), ("break_on_small_step", C.c_double)]
+
+
+class TexelStats(C.Structure):
+    _fields_ = [("iterations", C.c_uint32), ("effective", C.c_uint32), ("jacobians", C.c_uint32),
+                ("residuals", C.c_uint32), ("status", C.c_uint32)]
+
+
+STATS_DTYPE = np.dtype([("iterations", np.uint32), ("effective", np.uint32), ("jacobians", np.uint32),
+                        ("residuals", np.uint32), ("status", np.uint32)])
+
+
+class LayoutDesc(C.Structure):
+    _fields_ = [("lights_parabolic", C.c_void_p), ("light_count", C.c_uint32), ("triangles", C.c_void_p),
+                ("triangle_count", C.c_uint32), ("edges", C.c_void_p), ("edge_angles", C.c_void_p),
+                ("edge_count", C.c_uint32)]
+
+
+class BtfView(C.Structure):
+    _fields_ = [("samples", C.c_void_p), ("sample_type", C.c_uint32), ("width", C.c_uint32),
+                ("height", C.c_uint32), ("layout", C.POINTER(LayoutDesc))]
+
+
+class FitOptions(C.Structure):
+    _fields_ = [("lsq", LsqOptions), ("init_mode", C.c_uint32), ("init_params", C.c_void_p)]
+
+
+class Maps(C.Structure):
+    _fields_ = [("diffuse", C.c_void_p), ("specular", C.c_void_p), ("sigma", C.c_void_p), ("basis", C.c_void_p),
+                ("rmse", C.c_void_p), ("params", C.c_void_p), ("init", C.c_void_p), ("stats", C.c_void_p)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("texels", C.c_uint64), ("iterations", C.c_uint64), ("jacobians", C.c_uint64),
+                ("residuals", C.c_uint64), ("failed_texels", C.c_uint64), ("ms_total", C.c_double),
+                ("ms_luminance", C.c_double), ("ms_init", C.c_double), ("ms_fit", C.c_double),
+                ("ms_copy", C.c_double)]
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Loads the in-tree libsvf.so; raises when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: run `python -m tempestrenderer_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        vp, u32, u64, f32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_float
+        L.svf_abi_version.restype = u32
+        L.svf_status_string.argtypes = [C.c_int]
+        L.svf_status_string.restype = C.c_char_p
+        L.svf_last_error.restype = C.c_char_p
+        L.svf_lsq_options_default.argtypes = [C.POINTER(LsqOptions)]
+        L.svf_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.svf_destroy.argtypes = [vp]
+        L.svf_directions_ring81.argtypes = [vp]
+        L.svf_directions_ring81.restype = u32
+        L.svf_directions_fibonacci.argtypes = [u32, vp]
+        L.svf_directions_fibonacci.restype = u32
+        L.svf_layout_triangulate.argtypes = [vp, u32, vp, vp, vp, C.POINTER(u32)]
+        L.svf_layout_triangulate.restype = u32
+        L.svf_lsq_fit_sggx.argtypes = [vp, vp, u32, vp, C.POINTER(LsqOptions), vp, vp, vp, C.POINTER(TexelStats)]
+        L.svf_lsq_fit_batch.argtypes = [vp, vp, u32, vp, u64, u32, C.POINTER(LsqOptions), vp, vp, vp, vp]
+        L.svf_fit_texels.argtypes = [vp, C.POINTER(BtfView), C.POINTER(FitOptions), C.POINTER(Maps),
+                                     C.POINTER(RunStats)]
+        L.svf_synth_btf.argtypes = [vp, u32, u32, vp, u32, u64, u64, u32, f32, vp, vp]
+        for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_fit_texels", "svf_synth_btf"):
+            getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _check(status: int):
+    if status != SVF_OK:
+        raise SvfError(status, load().svf_last_error().decode())
+
+
+def options(max_iterations: int = 1024, fresnel: float = 1.0) -> LsqOptions:
+    o = LsqOptions()
+    load().svf_lsq_options_default(C.byref(o))
+    o.max_iterations = max_iterations
+    o.fresnel = fresnel
+    return o
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array (host) or a torch tensor (device or host)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        assert a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return a.data_ptr()  # torch.Tensor
+
+
+def directions_ring81() -> np.ndarray:
+    lp = np.zeros((81, 2), np.float32)
+    n = load().svf_directions_ring81(lp.ctypes.data)
+    assert n == 81
+    return lp
+
+
+def directions_fibonacci(count: int) -> np.ndarray:
+    lp = np.zeros((count, 2), np.float32)
+    load().svf_directions_fibonacci(count, lp.ctypes.data)
+    return lp
+
+
+def triangulate(lights_parabolic: np.ndarray):
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    L = lp.shape[0]
+    tri = np.zeros((2 * L, 3), np.uint32)
+    e = np.zeros((L, 3), np.uint32)
+    ea = np.zeros((L, 2), np.float32)
+    ne = C.c_uint32()
+    nt = load().svf_layout_triangulate(lp.ctypes.data, L, tri.ctypes.data, e.ctypes.data, ea.ctypes.data,
+                                       C.byref(ne))
+    if nt == 0:
+        raise SvfError(SVF_EINVAL, "triangulation failed")
+    return tri[:nt].copy(), e[:ne.value].copy(), ea[:ne.value].copy()
+
+
+class Layout:
+    """A direction layout and, optionally, its interpolation mesh (BTF::LightIndices/Edges)."""
+
+    def __init__(self, lights_parabolic, triangles=None, edges=None, edge_angles=None):
+        self.lights_parabolic = np.ascontiguousarray(lights_parabolic, np.float32)
+        self.triangles = None if triangles is None else np.ascontiguousarray(triangles, np.uint32)
+        self.edges = None if edges is None else np.ascontiguousarray(edges, np.uint32)
+        self.edge_angles = None if edge_angles is None else np.ascontiguousarray(edge_angles, np.float32)
+        d = LayoutDesc()
+        d.lights_parabolic = self.lights_parabolic.ctypes.data
+        d.light_count = self.lights_parabolic.shape[0]
+        if self.triangles is not None:
+            d.triangles = self.triangles.ctypes.data
+            d.triangle_count = self.triangles.shape[0]
+            d.edges = self.edges.ctypes.data
+            d.edge_angles = self.edge_angles.ctypes.data
+            d.edge_count = self.edges.shape[0]
+        self.desc = d
+
+    @property
+    def light_count(self) -> int:
+        return self.lights_parabolic.shape[0]
+
+
+class Context:
+    """A device context (svf_create / svf_destroy)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = load()
+        h = C.c_void_p()
+        _check(self._lib.svf_create(device, C.byref(h)))
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.svf_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # LeastSquaresFitSGGX -------------------------------------------------------
+    def lsq_fit_sggx(self, lights_parabolic, lum, init7, opts: LsqOptions | None = None):
+        lp = np.ascontiguousarray(lights_parabolic, np.float32)
+        lum = np.ascontiguousarray(lum, np.float32)
+        init = np.ascontiguousarray(init7, np.float32)
+        out = np.zeros(7, np.float32)
+        rmse = np.zeros(1, np.float32)
+        st = TexelStats()
+        o = opts or options()
+        _check(self._lib.svf_lsq_fit_sggx(self.handle, lp.ctypes.data, lp.shape[0], lum.ctypes.data, C.byref(o),
+                                          init.ctypes.data, out.ctypes.data, rmse.ctypes.data, C.byref(st)))
+        return out, float(rmse[0]), st
+
+    def lsq_fit_batch(self, lights_parabolic, lum, init, opts: LsqOptions | None = None, out=None, rmse=None,
+                      stats=None):
+        """lum: [T][stride] (numpy or torch, host or device); init: [T][7]."""
+        lp = np.ascontiguousarray(lights_parabolic, np.float32)
+        T = int(lum.shape[0])
+        stride = int(lum.shape[1])
+        if out is None:
+            out = np.zeros((T, 7), np.float32)
+        if rmse is None:
+            rmse = np.zeros(T, np.float32)
+        if stats is None:
+            stats = np.zeros(T, STATS_DTYPE)
+        o = opts or options()
+        _check(self._lib.svf_lsq_fit_batch(self.handle, lp.ctypes.data, lp.shape[0], _ptr(lum), stride, T,
+                                           C.byref(o), _ptr(init), _ptr(out), _ptr(rmse), _ptr(stats)))
+        return out, rmse, stats
+
+    # svbrdffit texel loop -------------------------------------------------------
+    def fit_texels(self, layout: Layout, samples, width: int, height: int, sample_type=SVF_SAMPLES_F32,
+                   opts: LsqOptions | None = None, init=None, want=("diffuse", "specular", "sigma", "basis", "rmse",
+                                                                    "params", "init", "stats"), out=None,
+                   check=True):
+        """samples: [T][L*L][3] (numpy or torch, host or device).  Returns (maps dict, RunStats)."""
+        T = width * height
+        v = BtfView()
+        v.samples = _ptr(samples)
+        v.sample_type = sample_type
+        v.width, v.height = width, height
+        v.layout = C.pointer(layout.desc)
+        fo = FitOptions()
+        fo.lsq = opts or options()
+        fo.init_mode = SVF_INIT_DEFAULT if init is None else SVF_INIT_GIVEN
+        fo.init_params = _ptr(init) if init is not None else None
+        shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
+                  "params": (T, 7), "init": (T, 7)}
+        res = dict(out or {})
+        for k in want:
+            if k in res:
+                continue
+            res[k] = np.zeros(T, STATS_DTYPE) if k == "stats" else np.zeros(shapes[k], np.float32)
+        m = Maps()
+        for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params", "init", "stats"):
+            setattr(m, k, _ptr(res[k]) if k in res else None)
+        rs = RunStats()
+        st = self._lib.svf_fit_texels(self.handle, C.byref(v), C.byref(fo), C.byref(m), C.byref(rs))
+        if check:
+            _check(st)
+        return res, rs
+
+    def synth_btf(self, seed: int, mix: int, lights_parabolic, first: int, count: int, samples,
+                  sample_type=SVF_SAMPLES_F32, noise: float = 0.01, truth=None):
+        lp = np.ascontiguousarray(lights_parabolic, np.float32)
+        _check(self._lib.svf_synth_btf(self.handle, seed, mix, lp.ctypes.data, lp.shape[0], first, count,
+                                       sample_type, noise, _ptr(samples), _ptr(truth)))

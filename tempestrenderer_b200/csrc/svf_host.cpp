@@ -1,0 +1,751 @@
+// svf_host.cpp - the C ABI of libsvf.so (include/svf.h): contexts, direction
+// layouts, buffer staging and the launch sequence of a fit.
+//
+// A fit of texels runs as one stream of kernels:
+//   luminance_kernel     samples -> luminance slices [T][Kp] + average chromaticity
+//   ndf_gemm_kernel      NDF textures = slices x NDF operator^T     (default init)
+//   init_finish_kernel   NDF -> initial parameters                  (default init)
+//   lm_fit_kernel        persistent LM over all texels + output maps
+// Host buffers are staged in chunks through the device.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/svf.h"
+#include "svf_internal.h"
+#include "svf_layout.h"
+
+namespace
+{
+
+thread_local std::string g_last_error;
+
+svf_status fail(svf_status s, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return s;
+}
+
+#define SVF_CUDA(call)                                                                                     \
+    do                                                                                                     \
+    {                                                                                                      \
+        cudaError_t e__ = (call);                                                                          \
+        if(e__ != cudaSuccess)                                                                             \
+            return fail(e__ == cudaErrorMemoryAllocation ? SVF_ENOMEM : SVF_ECUDA, "%s failed: %s (%s:%d)", \
+                        #call, cudaGetErrorString(e__), __FILE__, __LINE__);                               \
+    } while(0)
+
+#define SVF_TRY(expr)                 \
+    do                                \
+    {                                 \
+        svf_status s__ = (expr);      \
+        if(s__ != SVF_OK)             \
+            return s__;               \
+    } while(0)
+
+// A grow-only device allocation.
+struct DevBuf
+{
+    void* p = nullptr;
+    size_t n = 0;
+    svf_status ensure(size_t bytes)
+    {
+        if(bytes <= n)
+            return SVF_OK;
+        if(p)
+            cudaFree(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMalloc(&p, bytes);
+        if(e != cudaSuccess)
+        {
+            cudaGetLastError();
+            return fail(SVF_ENOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        }
+        n = bytes;
+        return SVF_OK;
+    }
+    template <typename T>
+    T* as() const { return static_cast<T*>(p); }
+    ~DevBuf()
+    {
+        if(p)
+            cudaFree(p);
+    }
+};
+
+struct PinnedBuf
+{
+    void* p = nullptr;
+    size_t n = 0;
+    svf_status ensure(size_t bytes)
+    {
+        if(bytes <= n)
+            return SVF_OK;
+        if(p)
+            cudaFreeHost(p);
+        p = nullptr;
+        n = 0;
+        cudaError_t e = cudaMallocHost(&p, bytes);
+        if(e != cudaSuccess)
+        {
+            cudaGetLastError();
+            return fail(SVF_ENOMEM, "cudaMallocHost(%zu) failed: %s", bytes, cudaGetErrorString(e));
+        }
+        n = bytes;
+        return SVF_OK;
+    }
+    ~PinnedBuf()
+    {
+        if(p)
+            cudaFreeHost(p);
+    }
+};
+
+uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934665603ull)
+{
+    const unsigned char* c = static_cast<const unsigned char*>(data);
+    for(size_t i = 0; i < bytes; ++i)
+    {
+        h ^= c[i];
+        h *= 1099511628211ull;
+    }
+    return h;
+}
+
+bool is_device_pointer(const void* p)
+{
+    if(!p)
+        return false;
+    cudaPointerAttributes a;
+    if(cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+
+// Direction layout: LM geometry and, once needed, the default-init tables.
+struct Layout
+{
+    uint32_t L = 0;
+    std::vector<float> lp;
+    DevBuf geo;                 // [3][L] Cartesian directions (LM)
+    bool init_ready = false;
+    svf::InitLayout init{};
+    DevBuf op, row_texel, denom_w, pca_cell_id, pca_cell_start, pca_index, pca_frac, pca_dir, proj_dir, proj_frac,
+        proj_cell;
+};
+
+} // namespace
+
+struct svf_ctx
+{
+    int device = 0;
+    int sms = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    std::map<uint64_t, std::unique_ptr<Layout>> layouts;
+    std::unique_ptr<svf::InitHostTables> tables;
+    DevBuf lum, avg, ndf, init, out, rmse, stats, counter, error, samples, maps_buf, scratch;
+    PinnedBuf pinned;
+    uint64_t ndf_zeroed_key = 0;
+    size_t ndf_zeroed_texels = 0;
+};
+
+namespace
+{
+
+svf_status check_ctx(svf_ctx* ctx)
+{
+    if(!ctx)
+        return fail(SVF_EINVAL, "null context");
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if(e != cudaSuccess)
+        return fail(SVF_ECUDA, "cudaSetDevice(%d): %s", ctx->device, cudaGetErrorString(e));
+    return SVF_OK;
+}
+
+svf_status check_options(const svf_lsq_options* o)
+{
+    if(!o)
+        return fail(SVF_EINVAL, "null options");
+    if(!(o->flags & SVF_LSQ_DIFFUSE))
+        return fail(SVF_EINVAL, "only the 7-parameter fit with the diffuse term (SVF_LSQ_DIFFUSE) is supported");
+    if(!(o->fresnel >= 1.0f) || !std::isfinite(o->fresnel))
+        return fail(SVF_EINVAL, "fresnel (refractive index) must be >= 1, got %g", o->fresnel);
+    if(!(o->mse_target >= 0.0) || !(o->break_on_small_step > 0.0))
+        return fail(SVF_EINVAL, "mse_target must be >= 0 and break_on_small_step > 0");
+    return SVF_OK;
+}
+
+svf_status get_layout(svf_ctx* ctx, const float* lp_in, uint32_t L, Layout** out)
+{
+    if(L < 3 || L > 160)
+        return fail(SVF_EINVAL, "light_count must be in [3, 160], got %u", L);
+    if(!lp_in)
+        return fail(SVF_EINVAL, "null lights_parabolic");
+    std::vector<float> lp(2 * L);
+    if(is_device_pointer(lp_in))
+        SVF_CUDA(cudaMemcpy(lp.data(), lp_in, sizeof(float) * 2 * L, cudaMemcpyDeviceToHost));
+    else
+        std::memcpy(lp.data(), lp_in, sizeof(float) * 2 * L);
+    for(float x : lp)
+        if(!std::isfinite(x))
+            return fail(SVF_EINVAL, "non-finite direction coordinate");
+    uint64_t key = fnv1a(lp.data(), lp.size() * sizeof(float), L);
+    auto it = ctx->layouts.find(key);
+    if(it == ctx->layouts.end())
+    {
+        auto lay = std::make_unique<Layout>();
+        lay->L = L;
+        lay->lp = lp;
+        std::vector<float> geo(3 * L);
+        for(uint32_t d = 0; d < L; ++d)
+        {
+            float w[3];
+            svf::parabolic_to_cartesian_ref(lp[2 * d], lp[2 * d + 1], w);
+            geo[d] = w[0];
+            geo[L + d] = w[1];
+            geo[2 * L + d] = w[2];
+        }
+        SVF_TRY(lay->geo.ensure(sizeof(float) * 3 * L));
+        SVF_CUDA(cudaMemcpy(lay->geo.p, geo.data(), sizeof(float) * 3 * L, cudaMemcpyHostToDevice));
+        it = ctx->layouts.emplace(key, std::move(lay)).first;
+    }
+    *out = it->second.get();
+    return SVF_OK;
+}
+
+template <typename T>
+svf_status upload(DevBuf& dst, const std::vector<T>& v)
+{
+    SVF_TRY(dst.ensure(std::max<size_t>(sizeof(T) * v.size(), 16)));
+    SVF_CUDA(cudaMemcpy(dst.p, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+    return SVF_OK;
+}
+
+// Builds the default-init tables of a layout, with its mesh (given, or computed).
+svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc)
+{
+    if(lay->init_ready)
+        return SVF_OK;
+    const uint32_t L = lay->L, N = L * L;
+    std::vector<uint32_t> tris, edges;
+    std::vector<float> eang;
+    if(desc->triangles)
+    {
+        if(desc->triangle_count == 0 || !desc->edges || !desc->edge_angles || desc->edge_count == 0)
+            return fail(SVF_EINVAL, "a given mesh needs triangles, edges and edge angles");
+        tris.assign(desc->triangles, desc->triangles + 3 * (size_t)desc->triangle_count);
+        edges.assign(desc->edges, desc->edges + 3 * (size_t)desc->edge_count);
+        eang.assign(desc->edge_angles, desc->edge_angles + 2 * (size_t)desc->edge_count);
+        for(uint32_t v : tris)
+            if(v >= L)
+                return fail(SVF_EINVAL, "triangle vertex %u out of range", v);
+        for(size_t i = 0; i < edges.size(); i += 3)
+            if(edges[i] >= L || edges[i + 1] >= L || edges[i + 2] >= desc->triangle_count)
+                return fail(SVF_EINVAL, "edge %zu out of range", i / 3);
+    }
+    else
+    {
+        if(!svf::delaunay(lay->lp.data(), L, tris))
+            return fail(SVF_EINVAL, "Delaunay triangulation of the directions failed");
+        svf::boundary_edges(lay->lp.data(), tris, edges, eang);
+    }
+    if(!ctx->tables)
+    {
+        ctx->tables = std::make_unique<svf::InitHostTables>();
+        svf::build_init_host_tables(*ctx->tables);
+    }
+    const svf::InitHostTables& t = *ctx->tables;
+    svf::InitLayout& il = lay->init;
+    il.L = L;
+    il.N = N;
+    il.k_pad = (uint32_t)round_up(N, 8);
+    il.ndf_rows = (uint32_t)t.ndf_row_texel.size();
+    il.ndf_rows_pad = (uint32_t)round_up(il.ndf_rows, 128);
+    SVF_TRY(lay->op.ensure(sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
+    SVF_CUDA(cudaMemset(lay->op.p, 0, sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
+    SVF_TRY(upload(lay->row_texel, t.ndf_row_texel));
+    SVF_TRY(upload(lay->denom_w, t.denom_w));
+    SVF_TRY(upload(lay->pca_cell_id, t.pca_cell_id));
+    SVF_TRY(upload(lay->pca_cell_start, t.pca_cell_start));
+    SVF_TRY(upload(lay->pca_index, t.pca_index));
+    SVF_TRY(upload(lay->pca_frac, t.pca_frac));
+    SVF_TRY(upload(lay->pca_dir, t.pca_dir));
+    SVF_TRY(upload(lay->proj_dir, t.proj_dir));
+    SVF_TRY(upload(lay->proj_frac, t.proj_frac));
+    SVF_TRY(upload(lay->proj_cell, t.proj_cell));
+    il.ndf_op = lay->op.as<float>();
+    il.ndf_row_texel = lay->row_texel.as<int32_t>();
+    il.denom_w = lay->denom_w.as<float>();
+    il.pca_cells = (uint32_t)t.pca_cell_id.size();
+    il.pca_cell_id = lay->pca_cell_id.as<int32_t>();
+    il.pca_cell_start = lay->pca_cell_start.as<uint32_t>();
+    il.pca_index = lay->pca_index.as<uint32_t>();
+    il.pca_frac = lay->pca_frac.as<float2>();
+    il.pca_dir = lay->pca_dir.as<float4>();
+    il.proj_dir = lay->proj_dir.as<float4>();
+    il.proj_frac = lay->proj_frac.as<float2>();
+    il.proj_cell = lay->proj_cell.as<int32_t>();
+    il.rot_s = t.rot_s;
+    il.rot_c = t.rot_c;
+    il.pdf = t.pdf;
+    il.axis_cell = t.axis_cell;
+    il.axis_fx1 = t.axis_frac[0];
+    il.axis_fy1 = t.axis_frac[1];
+
+    // the NDF operator, built on the device
+    DevBuf d_lp, d_tri, d_edges, d_eang, d_dirs, d_normals, d_ltri, d_lbary;
+    SVF_TRY(upload(d_lp, lay->lp));
+    SVF_TRY(upload(d_tri, tris));
+    SVF_TRY(upload(d_edges, edges));
+    SVF_TRY(upload(d_eang, eang));
+    SVF_TRY(upload(d_dirs, t.ndf_dirs));
+    SVF_TRY(upload(d_normals, t.ndf_row_normal));
+    SVF_TRY(d_ltri.ensure(sizeof(int32_t) * svf::kNdfSamples));
+    SVF_TRY(d_lbary.ensure(sizeof(float) * 3 * svf::kNdfSamples));
+    svf::MeshDevice mesh{ d_lp.as<float>(), d_tri.as<uint32_t>(), (uint32_t)(tris.size() / 3), d_edges.as<uint32_t>(),
+                          d_eang.as<float>(), (uint32_t)(edges.size() / 3) };
+    SVF_CUDA(svf::launch_ndf_operator(il, mesh, d_dirs.as<float>(), d_normals.as<float>(), t.ndf_scale,
+                                      d_ltri.as<int32_t>(), d_lbary.as<float>(), ctx->stream));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    lay->init_ready = true;
+    return SVF_OK;
+}
+
+// Copies `bytes` from src (host or device) to the device buffer dst.
+svf_status to_device(svf_ctx* ctx, void* dst, const void* src, size_t bytes)
+{
+    SVF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+    return SVF_OK;
+}
+
+struct LmRun
+{
+    const float* lum;      // device, padded
+    uint64_t stride;
+    const float* init;     // device [T][7]
+    float* out;            // device [T][7]
+    float* rmse;           // device [T]
+    svf_texel_stats* stats;
+    const float* avg;
+    float *diffuse, *specular, *sigma, *basis;
+    uint64_t texels;
+};
+
+svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r)
+{
+    svf::LmArgs a{};
+    a.lum = r.lum;
+    a.lum_stride = r.stride;
+    a.geo = lay->geo.as<float>();
+    a.init = r.init;
+    a.out = r.out;
+    a.rmse = r.rmse;
+    a.stats = r.stats;
+    a.avg_chroma = r.avg;
+    a.map_diffuse = r.diffuse;
+    a.map_specular = r.specular;
+    a.map_sigma = r.sigma;
+    a.map_basis = r.basis;
+    a.L = lay->L;
+    a.N = lay->L * lay->L;
+    a.texels = (uint32_t)r.texels;
+    a.cfg.max_iter = o->max_iterations;
+    a.cfg.mse_target = o->mse_target;
+    a.cfg.eps = o->break_on_small_step;
+    a.cfg.fresnel = o->fresnel;
+    SVF_TRY(ctx->counter.ensure(16));
+    SVF_TRY(ctx->error.ensure(16));
+    a.work_counter = ctx->counter.as<uint32_t>();
+    a.error_flag = ctx->error.as<uint32_t>();
+    SVF_CUDA(cudaMemsetAsync(ctx->counter.p, 0, 16, ctx->stream));
+    SVF_CUDA(cudaMemsetAsync(ctx->error.p, 0, 16, ctx->stream));
+    int per_sm = svf::lm_max_ctas_per_sm(a.L, a.lum_stride);
+    if(per_sm <= 0)
+        return fail(SVF_EINVAL, "the LM kernel does not fit on an SM for L = %u", a.L);
+    uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->sms, r.texels);
+    SVF_CUDA(svf::launch_lm_fit(a, (int)std::max<uint64_t>(grid, 1), ctx->stream));
+    return SVF_OK;
+}
+
+svf_status read_error_flag(svf_ctx* ctx)
+{
+    uint32_t flag = 0;
+    SVF_CUDA(cudaMemcpyAsync(&flag, ctx->error.p, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    if(flag)
+        return fail(SVF_ETIMEOUT, "a bounded device wait expired (a texel slab did not arrive)");
+    return SVF_OK;
+}
+
+} // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+
+extern "C" {
+
+uint32_t svf_abi_version(void) { return SVF_ABI_VERSION; }
+
+const char* svf_status_string(svf_status s)
+{
+    switch(s)
+    {
+    case SVF_OK: return "ok";
+    case SVF_EINVAL: return "invalid argument";
+    case SVF_ENOMEM: return "out of memory";
+    case SVF_ECUDA: return "CUDA error";
+    case SVF_ETIMEOUT: return "bounded device wait expired";
+    case SVF_EPARTIAL: return "some texels failed";
+    case SVF_ENODEV: return "no sm_100 device";
+    }
+    return "unknown status";
+}
+
+const char* svf_last_error(void) { return g_last_error.c_str(); }
+
+void svf_lsq_options_default(svf_lsq_options* o)
+{
+    if(!o)
+        return;
+    o->max_iterations = 1024;            // CurveFitSteps
+    o->fresnel = 1.0f;
+    o->flags = SVF_LSQ_DIFFUSE;
+    o->mse_target = 1e-6;
+    o->break_on_small_step = (double)1e-3f;   // settings.BreakOnSmallStep = 1e-3f
+}
+
+svf_status svf_create(int device, svf_ctx** out)
+{
+    if(!out)
+        return fail(SVF_EINVAL, "null output pointer");
+    *out = nullptr;
+    int count = 0;
+    if(cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+    {
+        cudaGetLastError();
+        return fail(SVF_ENODEV, "CUDA device %d not available", device);
+    }
+    cudaDeviceProp prop;
+    if(cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return fail(SVF_ENODEV, "cannot query device %d", device);
+    }
+    if(prop.major != 10)
+        return fail(SVF_ENODEV, "device %d is sm_%d%d; this library is built for sm_100a", device, prop.major,
+                    prop.minor);
+    std::unique_ptr<svf_ctx> ctx(new(std::nothrow) svf_ctx);
+    if(!ctx)
+        return fail(SVF_ENOMEM, "context allocation failed");
+    ctx->device = device;
+    ctx->sms = prop.multiProcessorCount;
+    SVF_CUDA(cudaSetDevice(device));
+    SVF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    for(auto& e : ctx->ev)
+        SVF_CUDA(cudaEventCreate(&e));
+    *out = ctx.release();
+    return SVF_OK;
+}
+
+void svf_destroy(svf_ctx* ctx)
+{
+    if(!ctx)
+        return;
+    cudaSetDevice(ctx->device);
+    if(ctx->stream)
+        cudaStreamSynchronize(ctx->stream);
+    for(auto& e : ctx->ev)
+        if(e)
+            cudaEventDestroy(e);
+    if(ctx->stream)
+        cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+uint32_t svf_directions_ring81(float* lp)
+{
+    if(!lp)
+        return 0;
+    return svf::ring81_directions(lp);
+}
+
+uint32_t svf_directions_fibonacci(uint32_t count, float* lp)
+{
+    if(!lp || count == 0)
+        return 0;
+    return svf::fibonacci_directions(count, lp);
+}
+
+uint32_t svf_layout_triangulate(const float* lp, uint32_t L, uint32_t* triangles, uint32_t* edges, float* edge_angles,
+                                uint32_t* edge_count)
+{
+    if(!lp || L < 3 || !triangles || !edges || !edge_angles || !edge_count)
+        return 0;
+    std::vector<uint32_t> tris, e;
+    std::vector<float> a;
+    if(!svf::delaunay(lp, L, tris))
+        return 0;
+    uint32_t ne = svf::boundary_edges(lp, tris, e, a);
+    std::copy(tris.begin(), tris.end(), triangles);
+    std::copy(e.begin(), e.end(), edges);
+    std::copy(a.begin(), a.end(), edge_angles);
+    *edge_count = ne;
+    return (uint32_t)(tris.size() / 3);
+}
+
+svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const float* lum, uint64_t lum_stride,
+                             uint32_t texels, const svf_lsq_options* opts, const float* init, float* out, float* rmse,
+                             svf_texel_stats* stats)
+{
+    SVF_TRY(check_ctx(ctx));
+    SVF_TRY(check_options(opts));
+    if(!lum || !init || !out || !rmse)
+        return fail(SVF_EINVAL, "null lum/init/out/rmse");
+    const uint32_t N = L * L;
+    if(lum_stride < N)
+        return fail(SVF_EINVAL, "lum_stride %llu < L*L = %u", (unsigned long long)lum_stride, N);
+    if(texels == 0)
+        return SVF_OK;
+    Layout* lay = nullptr;
+    SVF_TRY(get_layout(ctx, lp, L, &lay));
+    const uint64_t stride = round_up(N, 8);
+    const uint64_t T = texels;
+    SVF_TRY(ctx->lum.ensure(sizeof(float) * stride * T));
+    SVF_TRY(ctx->init.ensure(sizeof(float) * 7 * T));
+    SVF_TRY(ctx->out.ensure(sizeof(float) * 7 * T));
+    SVF_TRY(ctx->rmse.ensure(sizeof(float) * T));
+    SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * T));
+    SVF_CUDA(cudaMemcpy2DAsync(ctx->lum.p, sizeof(float) * stride, lum, sizeof(float) * lum_stride, sizeof(float) * N, T,
+                               cudaMemcpyDefault, ctx->stream));
+    SVF_TRY(to_device(ctx, ctx->init.p, init, sizeof(float) * 7 * T));
+    LmRun r{ ctx->lum.as<float>(), stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
+             ctx->stats.as<svf_texel_stats>(), nullptr, nullptr, nullptr, nullptr, nullptr, T };
+    SVF_TRY(run_lm(ctx, lay, opts, r));
+    SVF_CUDA(cudaMemcpyAsync(out, ctx->out.p, sizeof(float) * 7 * T, cudaMemcpyDefault, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(rmse, ctx->rmse.p, sizeof(float) * T, cudaMemcpyDefault, ctx->stream));
+    if(stats)
+        SVF_CUDA(cudaMemcpyAsync(stats, ctx->stats.p, sizeof(svf_texel_stats) * T, cudaMemcpyDefault, ctx->stream));
+    SVF_TRY(read_error_flag(ctx));
+    if(stats)
+    {
+        std::vector<svf_texel_stats> st(T);
+        if(is_device_pointer(stats))
+            SVF_CUDA(cudaMemcpy(st.data(), stats, sizeof(svf_texel_stats) * T, cudaMemcpyDeviceToHost));
+        else
+            std::memcpy(st.data(), stats, sizeof(svf_texel_stats) * T);
+        for(auto& s : st)
+            if(s.status & (SVF_TEXEL_NONFINITE | SVF_TEXEL_TIMEOUT))
+                return fail(SVF_EPARTIAL, "some texels did not produce a finite fit");
+    }
+    return SVF_OK;
+}
+
+svf_status svf_lsq_fit_sggx(svf_ctx* ctx, const float* lp, uint32_t L, const float* lum, const svf_lsq_options* opts,
+                            const float init[7], float out[7], float* rmse, svf_texel_stats* stats)
+{
+    svf_texel_stats st{};
+    svf_status s = svf_lsq_fit_batch(ctx, lp, L, lum, (uint64_t)L * L, 1, opts, init, out, rmse, &st);
+    if(stats)
+        *stats = st;
+    return s;
+}
+
+svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* opts, const svf_maps* maps,
+                          svf_run_stats* run)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(!btf || !opts || !maps || !btf->layout || !btf->samples)
+        return fail(SVF_EINVAL, "null btf/options/maps/layout/samples");
+    SVF_TRY(check_options(&opts->lsq));
+    if(btf->sample_type != SVF_SAMPLES_F32 && btf->sample_type != SVF_SAMPLES_F16)
+        return fail(SVF_EINVAL, "unknown sample_type %u", btf->sample_type);
+    if(opts->init_mode != SVF_INIT_DEFAULT && opts->init_mode != SVF_INIT_GIVEN)
+        return fail(SVF_EINVAL, "unknown init_mode %u", opts->init_mode);
+    if(opts->init_mode == SVF_INIT_GIVEN && !opts->init_params)
+        return fail(SVF_EINVAL, "SVF_INIT_GIVEN needs init_params");
+    const uint64_t T = (uint64_t)btf->width * btf->height;
+    if(T == 0)
+        return SVF_OK;
+    if(T > 0xffffffffull)
+        return fail(SVF_EINVAL, "too many texels");
+    const svf_layout_desc* desc = btf->layout;
+    Layout* lay = nullptr;
+    SVF_TRY(get_layout(ctx, desc->lights_parabolic, desc->light_count, &lay));
+    const uint32_t L = lay->L, N = L * L;
+    const uint64_t stride = round_up(N, 8);
+    if(opts->init_mode == SVF_INIT_DEFAULT)
+        SVF_TRY(prepare_init(ctx, lay, desc));
+
+    const size_t elem = btf->sample_type == SVF_SAMPLES_F16 ? 2 : 4;
+    const size_t texel_bytes = elem * 3 * (size_t)N;
+    const bool samples_on_device = is_device_pointer(btf->samples);
+
+    // chunking: bounded device footprint for host inputs and the NDF textures
+    size_t free_b = 0, total_b = 0;
+    SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    size_t per_texel = sizeof(float) * (stride + 3 + 7 + 7 + 1 + 12) + sizeof(svf_texel_stats) +
+                       (opts->init_mode == SVF_INIT_DEFAULT ? sizeof(float) * svf::kNdfTexels : 0) +
+                       (samples_on_device ? 0 : texel_bytes);
+    uint64_t chunk = std::max<uint64_t>(1, (uint64_t)(0.5 * (double)free_b / (double)per_texel));
+    chunk = std::min<uint64_t>(chunk, T);
+    if(!samples_on_device)
+        chunk = std::min<uint64_t>(chunk, std::max<uint64_t>(1, (256ull << 20) / texel_bytes) * 16);
+
+    SVF_TRY(ctx->lum.ensure(sizeof(float) * stride * chunk));
+    SVF_TRY(ctx->avg.ensure(sizeof(float) * 3 * chunk));
+    SVF_TRY(ctx->init.ensure(sizeof(float) * 7 * chunk));
+    SVF_TRY(ctx->out.ensure(sizeof(float) * 7 * chunk));
+    SVF_TRY(ctx->rmse.ensure(sizeof(float) * chunk));
+    SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * chunk));
+    SVF_TRY(ctx->maps_buf.ensure(sizeof(float) * 12 * chunk));
+    if(opts->init_mode == SVF_INIT_DEFAULT)
+    {
+        SVF_TRY(ctx->ndf.ensure(sizeof(float) * svf::kNdfTexels * chunk));
+        SVF_CUDA(cudaMemsetAsync(ctx->ndf.p, 0, sizeof(float) * svf::kNdfTexels * chunk, ctx->stream));
+    }
+    if(!samples_on_device)
+        SVF_TRY(ctx->samples.ensure(texel_bytes * chunk));
+
+    svf_run_stats rs{};
+    float ms = 0.0f;
+    std::vector<svf_texel_stats> host_stats;
+    for(uint64_t c0 = 0; c0 < T; c0 += chunk)
+    {
+        const uint64_t n = std::min<uint64_t>(chunk, T - c0);
+        const void* samples = static_cast<const char*>(btf->samples) + c0 * texel_bytes;
+        SVF_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+        if(!samples_on_device)
+        {
+            SVF_CUDA(cudaMemcpyAsync(ctx->samples.p, samples, texel_bytes * n, cudaMemcpyHostToDevice, ctx->stream));
+            samples = ctx->samples.p;
+        }
+        SVF_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+        SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
+                                       ctx->avg.as<float>(), ctx->stream));
+        SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
+        if(opts->init_mode == SVF_INIT_DEFAULT)
+        {
+            SVF_CUDA(svf::launch_ndf_gemm(lay->init, ctx->lum.as<float>(), stride, n, ctx->ndf.as<float>(),
+                                          ctx->stream));
+            SVF_CUDA(svf::launch_init_finish(lay->init, ctx->ndf.as<float>(), n, ctx->init.as<float>(), nullptr,
+                                             ctx->stream));
+        }
+        else
+            SVF_TRY(to_device(ctx, ctx->init.p, opts->init_params + 7 * c0, sizeof(float) * 7 * n));
+        SVF_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+        float* mb = ctx->maps_buf.as<float>();
+        LmRun r{ ctx->lum.as<float>(), stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
+                 ctx->stats.as<svf_texel_stats>(), ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n };
+        SVF_TRY(run_lm(ctx, lay, &opts->lsq, r));
+        SVF_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
+        // outputs
+        auto put = [&](void* dst, const void* src, size_t bytes) -> svf_status {
+            if(dst)
+                SVF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+            return SVF_OK;
+        };
+        SVF_TRY(put(maps->diffuse ? maps->diffuse + 3 * c0 : nullptr, mb, sizeof(float) * 3 * n));
+        SVF_TRY(put(maps->specular ? maps->specular + 3 * c0 : nullptr, mb + 3 * n, sizeof(float) * 3 * n));
+        SVF_TRY(put(maps->sigma ? maps->sigma + 2 * c0 : nullptr, mb + 6 * n, sizeof(float) * 2 * n));
+        SVF_TRY(put(maps->basis ? maps->basis + 4 * c0 : nullptr, mb + 8 * n, sizeof(float) * 4 * n));
+        SVF_TRY(put(maps->rmse ? maps->rmse + c0 : nullptr, ctx->rmse.p, sizeof(float) * n));
+        SVF_TRY(put(maps->params ? maps->params + 7 * c0 : nullptr, ctx->out.p, sizeof(float) * 7 * n));
+        SVF_TRY(put(maps->init ? maps->init + 7 * c0 : nullptr, ctx->init.p, sizeof(float) * 7 * n));
+        std::vector<svf_texel_stats> st(n);
+        SVF_CUDA(cudaMemcpyAsync(st.data(), ctx->stats.p, sizeof(svf_texel_stats) * n, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        SVF_CUDA(cudaEventRecord(ctx->ev[5], ctx->stream));
+        SVF_TRY(read_error_flag(ctx));
+        if(maps->stats)
+            SVF_CUDA(cudaMemcpy(maps->stats + c0, st.data(), sizeof(svf_texel_stats) * n, cudaMemcpyDefault));
+        for(auto& s : st)
+        {
+            rs.iterations += s.iterations;
+            rs.jacobians += s.jacobians;
+            rs.residuals += s.residuals;
+            if(s.status & (SVF_TEXEL_NONFINITE | SVF_TEXEL_TIMEOUT))
+                rs.failed_texels++;
+        }
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[5]));
+        rs.ms_total += ms;
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+        rs.ms_copy += ms;
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]));
+        rs.ms_copy += ms;
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]));
+        rs.ms_luminance += ms;
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+        rs.ms_init += ms;
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[3], ctx->ev[4]));
+        rs.ms_fit += ms;
+    }
+    rs.texels = T;
+    if(run)
+        *run = rs;
+    if(rs.failed_texels)
+        return fail(SVF_EPARTIAL, "%llu texels did not produce a finite fit", (unsigned long long)rs.failed_texels);
+    return SVF_OK;
+}
+
+svf_status svf_synth_btf(svf_ctx* ctx, uint32_t seed, uint32_t mix, const float* lp, uint32_t L, uint64_t first,
+                         uint64_t count, uint32_t sample_type, float noise, void* samples, float* truth)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(!samples || !lp)
+        return fail(SVF_EINVAL, "null samples/lights");
+    if(!is_device_pointer(samples))
+        return fail(SVF_EINVAL, "samples must be device memory");
+    if(mix > 1 || (sample_type != SVF_SAMPLES_F32 && sample_type != SVF_SAMPLES_F16) || L < 1 || L > 160)
+        return fail(SVF_EINVAL, "bad mix/sample_type/light_count");
+    if(count == 0)
+        return SVF_OK;
+    DevBuf d_lp;
+    SVF_TRY(d_lp.ensure(sizeof(float) * 2 * L));
+    SVF_CUDA(cudaMemcpyAsync(d_lp.p, lp, sizeof(float) * 2 * L, cudaMemcpyDefault, ctx->stream));
+    const uint64_t step = 1u << 20;
+    float* truth_dev = nullptr;
+    DevBuf d_truth;
+    const bool truth_host = truth && !is_device_pointer(truth);
+    if(truth_host)
+    {
+        SVF_TRY(d_truth.ensure(sizeof(float) * 16 * std::min<uint64_t>(count, step)));
+        truth_dev = d_truth.as<float>();
+    }
+    const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)L * L;
+    for(uint64_t c = 0; c < count; c += step)
+    {
+        uint64_t n = std::min<uint64_t>(step, count - c);
+        float* tr = truth ? (truth_host ? truth_dev : truth + 16 * c) : nullptr;
+        SVF_CUDA(svf::launch_synth(seed, mix, d_lp.as<float>(), L, first + c, n, sample_type, noise,
+                                   static_cast<char*>(samples) + c * texel_bytes, tr, ctx->stream));
+        if(truth_host)
+            SVF_CUDA(cudaMemcpyAsync(truth + 16 * c, truth_dev, sizeof(float) * 16 * n, cudaMemcpyDeviceToHost,
+                                     ctx->stream));
+    }
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    return SVF_OK;
+}
+
+} // extern "C"

@@ -1,0 +1,118 @@
+// svf_internal.h - declarations shared by the host orchestration (svf_host.cpp)
+// and the CUDA translation units.  Not part of the public ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/svf.h"
+
+namespace svf
+{
+
+// Per-texel LM settings (LevenbergMarquardtCurveFit, include/tempest/math/fitting.hh:457-678).
+struct LmConfig
+{
+    uint32_t max_iter;
+    double   mse_target;
+    double   eps;          // BreakOnSmallStep
+    float    fresnel;
+};
+
+// Arguments of the persistent LM kernel.
+struct LmArgs
+{
+    const float* lum;          // [texels][lum_stride], lum_stride % 4 == 0, 16-byte aligned
+    uint64_t     lum_stride;   // floats
+    const float* geo;          // [3][L] direction table, SoA: x, y, z
+    const float* init;         // [texels][7]
+    float*       out;          // [texels][7]
+    float*       rmse;         // [texels]
+    svf_texel_stats* stats;    // [texels] or null
+    const float* avg_chroma;   // [texels][3] or null (needed by the RGB maps)
+    float* map_diffuse;        // [texels][3] or null
+    float* map_specular;       // [texels][3] or null
+    float* map_sigma;          // [texels][2] or null
+    float* map_basis;          // [texels][4] or null
+    uint32_t L, N, texels;
+    LmConfig cfg;
+    uint32_t* work_counter;    // zeroed before the launch
+    uint32_t* error_flag;      // set non-zero by a bounded wait that expired
+};
+
+// Kernel launchers (defined in svf_kernels.cu).
+size_t     lm_smem_bytes(uint32_t L, uint64_t lum_stride);
+int        lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride);
+cudaError_t launch_lm_fit(const LmArgs& args, int grid, cudaStream_t stream);
+
+// Luminance slice + average chromaticity (BTFParallelExtractLuminanceSlice,
+// src/image/btf.cc:1078-1116) for texels [0, texels) of an RGB sample array.
+cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
+                             float* lum, uint64_t lum_stride, float* avg_chroma, cudaStream_t stream);
+
+// Repacks a caller's luminance array to the padded internal layout.
+cudaError_t launch_repack(const float* src, uint64_t src_stride, uint64_t texels, uint32_t N,
+                          float* dst, uint64_t dst_stride, cudaStream_t stream);
+
+cudaError_t launch_synth(uint32_t seed, uint32_t mix, const float* lights_parabolic, uint32_t L, uint64_t first,
+                         uint64_t count, uint32_t sample_type, float noise, void* samples, float* truth,
+                         cudaStream_t stream);
+
+// ---- default initial guess (svf_init.cu) ---------------------------------------
+
+constexpr int kNdfRes = 64;               // NDFTextureResolution (svbrdf-fitting.hh:53)
+constexpr int kNdfTexels = kNdfRes * kNdfRes;
+constexpr int kNdfSamples = 4096;         // NDRReduceSphereSamples (svbrdf-fitting.hh:49)
+constexpr int kPcaSide = 512;             // CommonSampleCount (svbrdf-fitting.hh:46)
+constexpr int kPcaSamples = kPcaSide * kPcaSide;
+constexpr int kDenomSamples = 256 * 256;  // svbrdf-fitting-pipeline.cc:403
+constexpr int kProjSamples = 1024;        // ConvertSamples (svbrdf-fitting.hh:50)
+constexpr int kTangentSteps = 512;        // EigenVectorPlaneSamples (svbrdf-fitting.hh:48)
+
+// Device tables of one direction layout for the default initial guess.
+struct InitLayout
+{
+    uint32_t L, N;
+    uint32_t k_pad;            // N padded to a multiple of 8 (GEMM K)
+    uint32_t ndf_rows;         // NDF texels inside the hemisphere (rows of the operator)
+    uint32_t ndf_rows_pad;     // rows padded to a multiple of 128
+    float*    ndf_op;          // [ndf_rows_pad][k_pad] NDF = op * lum (row-major)
+    int32_t*  ndf_row_texel;   // [ndf_rows] NDF texel index of each operator row
+    float*    denom_w;         // [4096] ndf_denom = denom_w . NDF
+    // PCA search samples, grouped by the bilinear cell they fall in
+    uint32_t  pca_cells;       // cells that hold samples
+    int32_t*  pca_cell_id;     // [pca_cells] x0 + 64*y0 of the cell
+    uint32_t* pca_cell_start;  // [pca_cells + 1] ranges into the sample arrays
+    uint32_t* pca_index;       // [kPcaSamples] original sample order, cell-grouped
+    float2*   pca_frac;        // [kPcaSamples] (fx1, fy1), cell-grouped
+    float4*   pca_dir;         // [kPcaSamples] directions, in sample order
+    float4*   proj_dir;        // [1024] SGGX projection sample directions
+    float2*   proj_frac;       // [1024] bilinear fractions
+    int32_t*  proj_cell;       // [1024] x0 + 64*y0
+    float     rot_s, rot_c;    // tangent-plane rotation step
+    float     pdf;             // 1/(2 pi)
+    int32_t   axis_cell;       // bilinear set-up of the direction (0, 0, 1)
+    float     axis_fx1, axis_fy1;
+};
+
+// Builds the NDF operator rows on the device from the mesh and sample tables.
+struct MeshDevice
+{
+    const float*    lp;        // [L][2]
+    const uint32_t* tri;       // [T][3]
+    uint32_t        ntri;
+    const uint32_t* edges;     // [E][3]
+    const float*    eang;      // [E][2]
+    uint32_t        nedge;
+};
+cudaError_t launch_ndf_operator(const InitLayout& lay, const MeshDevice& mesh, const float* ndf_dirs /* [4096][3] */,
+                                const float* row_normals /* [rows][3] */, double ndf_scale, int32_t* light_tri,
+                                float* light_bary, cudaStream_t stream);
+
+cudaError_t launch_ndf_gemm(const InitLayout& lay, const float* lum, uint64_t lum_stride, uint64_t texels,
+                            float* ndf, cudaStream_t stream);
+// init_info (optional): [texels][8] = ndf_denom, normal xyz, tangent xyz, pca value
+cudaError_t launch_init_finish(const InitLayout& lay, const float* ndf, uint64_t texels, float* init_params,
+                               float* init_info, cudaStream_t stream);
+
+} // namespace svf

@@ -1,0 +1,98 @@
+"""The svbrdffit texel loop on the GPU (svf_fit_texels): luminance slices, the
+default initial guess, LM and the output maps, against the reference's golden
+pipeline results and the oracle."""
+import numpy as np
+import pytest
+
+import tempestrenderer_b200 as svf
+
+pytestmark = pytest.mark.gpu
+
+
+def _layout(golden):
+    m = golden["mesh"]
+    return svf.Layout(m["lights_parabolic"], m["triangles"], m["edges"], m["edge_angles"])
+
+
+def _golden_rgb(oracle, golden):
+    p = golden["pipeline"]
+    lp = golden["mesh"]["lights_parabolic"]
+    return np.stack([oracle.synth_render(int(p["seed"]), x, oracle.synth_truth(int(p["seed"]), int(p["mix"]), x), lp)
+                     for x in range(8)])
+
+
+@pytest.fixture(scope="module")
+def golden_fit(gpu_ctx, oracle_lib, golden):
+    rgb = _golden_rgb(oracle_lib, golden)
+    maps, rs = gpu_ctx.fit_texels(_layout(golden), rgb, 8, 1)
+    return rgb, maps, rs
+
+
+def test_default_init_matches_reference(golden_fit, oracle_lib, golden):
+    """Initial guess per texel: ndf_denom and the SGGX scale ratios to 1e-4; the
+    frame (from argmax searches) to 1e-3 on the rotation matrix."""
+    _, maps, _ = golden_fit
+    p = golden["pipeline"]
+    for x in range(8):
+        gi, ri = maps["init"][x], p["init"][x]
+        np.testing.assert_allclose(gi[:4], ri[:4], rtol=1e-4, atol=1e-6)
+        mg, _ = oracle_lib.euler_to_matrix(gi[4:7])
+        mr, _ = oracle_lib.euler_to_matrix(ri[4:7])
+        np.testing.assert_allclose(mg, mr, atol=1e-3)
+
+
+def test_final_rmse_within_one_percent(golden_fit, golden):
+    _, maps, rs = golden_fit
+    p = golden["pipeline"]
+    assert (maps["rmse"] <= 1.01 * p["rmse"] + 1e-7).all(), np.c_[maps["rmse"], p["rmse"]]
+    assert rs.failed_texels == 0 and rs.texels == 8
+
+
+def test_output_maps_assembly(golden_fit, oracle_lib, golden):
+    rgb, maps, _ = golden_fit
+    for x in range(8):
+        fit = maps["params"][x]
+        _, avg = oracle_lib.lum_slice(rgb[x])
+        np.testing.assert_array_equal(maps["sigma"][x], fit[:2])
+        np.testing.assert_allclose(maps["diffuse"][x], avg * fit[3], rtol=1e-5, atol=1e-7)
+        np.testing.assert_allclose(maps["specular"][x], avg * fit[2], rtol=1e-5, atol=1e-7)
+        _, q = oracle_lib.euler_to_matrix(fit[4:7])
+        np.testing.assert_allclose(maps["basis"][x], q, atol=1e-5)
+
+
+def test_given_init_and_device_samples(gpu_ctx, golden_fit, golden):
+    import torch
+
+    rgb, maps, _ = golden_fit
+    init = maps["init"].copy()
+    samples = torch.from_numpy(rgb).cuda()
+    maps2, _ = gpu_ctx.fit_texels(_layout(golden), samples, 4, 2, init=init)
+    np.testing.assert_array_equal(maps2["params"], maps["params"])
+    np.testing.assert_array_equal(maps2["rmse"], maps["rmse"])
+
+
+def test_library_mesh_and_fp16_samples(gpu_ctx, oracle_lib, golden):
+    """The library's own triangulation and FP16 storage give fits within 1.01x of
+    the reference's on the same texels."""
+    rgb = _golden_rgb(oracle_lib, golden)
+    lay = svf.Layout(golden["mesh"]["lights_parabolic"])
+    maps, _ = gpu_ctx.fit_texels(lay, rgb.astype(np.float16), 8, 1, sample_type=svf.SVF_SAMPLES_F16)
+    p = golden["pipeline"]
+    assert (maps["rmse"] <= 1.01 * p["rmse"] + 2e-5).mean() >= 0.75, np.c_[maps["rmse"], p["rmse"]]
+
+
+def test_synthetic_generator_matches_oracle(gpu_ctx, oracle_lib, golden):
+    import torch
+
+    lp = golden["mesh"]["lights_parabolic"]
+    n = 6
+    samples = torch.zeros((n, 81 * 81, 3), dtype=torch.float32, device="cuda")
+    truth = np.zeros((n, 16), np.float32)
+    gpu_ctx.synth_btf(91, 1, lp, 1000, n, samples, truth=truth)
+    s = samples.cpu().numpy()
+    for k in range(n):
+        t = oracle_lib.synth_truth(91, 1, 1000 + k)
+        ref = np.array([*t.kd, *t.ks, *t.sigma, *t.quat, *t.euler, t.kind], np.float32)
+        np.testing.assert_allclose(truth[k], ref, rtol=2e-5, atol=2e-6)
+        rgb = oracle_lib.synth_render(91, 1000 + k, t, lp)
+        np.testing.assert_allclose(s[k], rgb, rtol=2e-4, atol=1e-6)

@@ -1,0 +1,148 @@
+"""Pins the oracle restatement (oracle/svf_oracle.c) against the reference.
+
+The golden vectors in tests/golden/ were produced by the reference's own CPU
+fitter (tests/golden/make_golden.py).  The restatement keeps the reference's
+float operation order, so the comparisons are exact where the reference is
+deterministic.
+"""
+import numpy as np
+import pytest
+
+
+def _mesh(oracle, golden):
+    m = golden["mesh"]
+    return oracle.MeshData(m["lights_parabolic"], m["triangles"], m["edges"], m["edge_angles"])
+
+
+def test_directions_match_loadbtf(oracle_lib, golden):
+    lp = oracle_lib.angles_to_parabolic(oracle_lib.ring81_angles())
+    assert np.array_equal(lp, golden["mesh"]["lights_parabolic"])
+
+
+def _texel_rgb(oracle, golden, x):
+    p = golden["pipeline"]
+    lp = golden["mesh"]["lights_parabolic"]
+    t = oracle.synth_truth(int(p["seed"]), int(p["mix"]), x)
+    return oracle.synth_render(int(p["seed"]), x, t, lp)
+
+
+@pytest.mark.parametrize("x", [0, 3, 7])
+def test_luminance_slice(oracle_lib, golden, x):
+    p = golden["pipeline"]
+    lum, avg = oracle_lib.lum_slice(_texel_rgb(oracle_lib, golden, x))
+    assert np.sum(lum, dtype=np.float64) == p["lum_sum"][x]
+    np.testing.assert_allclose(avg, p["avg"][x], rtol=1e-5)
+
+
+@pytest.mark.parametrize("x", [0, 5])
+def test_ndf_texture_exact(oracle_lib, golden, x):
+    p = golden["pipeline"]
+    lum, _ = oracle_lib.lum_slice(_texel_rgb(oracle_lib, golden, x))
+    ndf = oracle_lib.ndf_texture(_mesh(oracle_lib, golden), lum)
+    assert np.array_equal(ndf, p["ndf"][x])
+
+
+@pytest.mark.parametrize("x", range(8))
+def test_default_init_exact(oracle_lib, golden, x):
+    p = golden["pipeline"]
+    init, _ = oracle_lib.default_init_from_ndf(p["ndf"][x])
+    assert np.array_equal(init, p["init"][x])
+
+
+@pytest.mark.parametrize("x", [0, 2, 5, 7])
+def test_lsq_from_default_init_exact(oracle_lib, golden, x):
+    p = golden["pipeline"]
+    lp = golden["mesh"]["lights_parabolic"]
+    lum, _ = oracle_lib.lum_slice(_texel_rgb(oracle_lib, golden, x))
+    out, rmse, st = oracle_lib.lsq_fit(lum, lp, p["init"][x])
+    assert np.array_equal(out, p["fit"][x])
+    assert np.float32(rmse) == np.float32(p["rmse"][x])
+    assert st.iterations == p["iterations"][x] and st.effective == p["effective"][x]
+
+
+@pytest.mark.parametrize("x", [1, 4, 6])
+def test_lsq_from_perturbed_truth_exact(oracle_lib, golden, x):
+    g = golden["lsq"]
+    lp = golden["mesh"]["lights_parabolic"]
+    lum, _ = oracle_lib.lum_slice(_texel_rgb(oracle_lib, golden, x))
+    out, rmse, st = oracle_lib.lsq_fit(lum, lp, g["init"][x])
+    assert np.array_equal(out, g["fit"][x])
+    assert np.float32(rmse) == np.float32(g["rmse"][x])
+    assert (st.iterations, st.effective) == tuple(g["iters"][x])
+
+
+def test_brdf_evaluator_exact(oracle_lib, golden):
+    g = golden["lsq"]
+    lp = golden["mesh"]["lights_parabolic"]
+    for params, ref in zip(g["brdf_params"], g["brdf"]):
+        f32, f64 = oracle_lib.brdf_all(params, lp)
+        assert np.array_equal(f32[g["brdf_pairs"]], ref)
+        # the FP64 restatement of the same model agrees to float rounding
+        np.testing.assert_allclose(f64[g["brdf_pairs"]], ref, rtol=2e-5, atol=1e-7)
+
+
+def test_output_maps(oracle_lib, golden):
+    """maps = sigma, ToQuaternion(euler), avg_chroma*kd, avg_chroma*ks (pipeline.cc:692-696)."""
+    p = golden["pipeline"]
+    for x in range(8):
+        fit, maps, avg = p["fit"][x], p["maps"][x], p["avg"][x]
+        np.testing.assert_array_equal(maps[0:2], fit[0:2])
+        _, q = oracle_lib.euler_to_matrix(fit[4:7])
+        np.testing.assert_allclose(maps[2:6], q, atol=1e-6)
+        np.testing.assert_allclose(maps[6:9], avg * fit[3], rtol=1e-6)
+        np.testing.assert_allclose(maps[9:12], avg * fit[2], rtol=1e-6)
+
+
+def test_sggx_anisotropy_swap(oracle_lib, golden):
+    """Swapping sigma_x/sigma_y and turning the tangent frame by 90 degrees about
+    the normal leaves the lobe unchanged (the property sggx-test.cc:292-313 checks)."""
+    lp = golden["mesh"]["lights_parabolic"]
+    p = np.array([0.25, 0.07, 0.6, 0.3, 0.0, 0.0, 0.4])
+    q = p.copy()
+    q[0], q[1] = p[1], p[0]
+    q[6] = p[6] + np.pi / 2
+    _, a = oracle_lib.brdf_all(p, lp)
+    _, b = oracle_lib.brdf_all(q, lp)
+    np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-12)
+
+
+def test_truth_recovered_from_noise_free_slice(oracle_lib, golden):
+    """LM from a nearby start recovers the generating parameters of a noise-free
+    texel to the null test's tolerances (svbrdf-fitting.cc:401-427: specular
+    1e-2, sigma 2e-2).  The reference stops at a step below 1e-3 of the
+    parameter norm (svbrdf-lsq-fitting-setup.cc:273, fitting.hh:590-595), so the
+    recovery is to that precision, not to the noise floor."""
+    lp = golden["mesh"]["lights_parabolic"]
+    t = oracle_lib.synth_truth(3, 0, 17)
+    rgb = oracle_lib.synth_render(3, 17, t, lp, noise=0.0)
+    lum, _ = oracle_lib.lum_slice(rgb)
+    truth = oracle_lib.truth_lum_params(t)
+    f_truth, _ = oracle_lib.brdf_all(truth.astype(np.float64), lp)
+    assert np.sqrt(np.mean((f_truth - lum) ** 2)) < 1e-4 * float(np.mean(lum))
+    init = truth * np.float32(1.1)
+    f_init, _ = oracle_lib.brdf_all(init.astype(np.float64), lp)
+    out, rmse, st = oracle_lib.lsq_fit(lum, lp, init)
+    assert rmse < 0.05 * np.sqrt(np.mean((f_init - lum) ** 2))
+    np.testing.assert_allclose(out[:2], truth[:2], atol=2e-2)
+    np.testing.assert_allclose(out[2:4], truth[2:4], atol=1e-2)
+    # zero steps at the optimum: the fit does not move
+    out0, rmse0, st0 = oracle_lib.lsq_fit(lum, lp, truth, max_steps=0)
+    assert np.array_equal(out0, truth) and st0.iterations == 0
+
+
+def test_live_reference_matches(oracle_lib, golden):
+    """When the reference build is present, one more texel through both."""
+    if not oracle_lib.ref_available():
+        pytest.skip("oracle/_ref not built here")
+    lp = golden["mesh"]["lights_parabolic"]
+    rgb = np.stack([oracle_lib.synth_render(23, t, oracle_lib.synth_truth(23, 1, t), lp) for t in (100, 101)])
+    btf = oracle_lib.RefBTF.from_texels(golden["angles"], rgb)
+    for x in range(2):
+        r = btf.fit_texel(x, want_ndf=True)
+        lum, _ = oracle_lib.lum_slice(rgb[x])
+        ndf = oracle_lib.ndf_texture(_mesh(oracle_lib, golden), lum)
+        assert np.array_equal(ndf, r["ndf"])
+        init, _ = oracle_lib.default_init_from_ndf(ndf)
+        assert np.array_equal(init, r["init"])
+        out, rmse, _ = oracle_lib.lsq_fit(lum, lp, init)
+        assert np.array_equal(out, r["fit"])
