@@ -70,6 +70,9 @@ typedef struct svf_lsq_options
     uint32_t flags;               /* must contain SVF_LSQ_DIFFUSE */
     double   mse_target;          /* LevenbergMarquardtCurveFit mean_sq_error: 1e-6 */
     double   break_on_small_step; /* LevenbergMarquardtSettings::BreakOnSmallStep: 1e-3 */
+    uint32_t restarts;            /* times LM continues, with fresh damping, from the point where
+                                     the reference's stopping rules end it; 0 = the reference's
+                                     single run.  Default 1. */
 } svf_lsq_options;
 
 typedef struct svf_texel_stats

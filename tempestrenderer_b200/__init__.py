@@ -43,7 +43,7 @@ class SvfError(RuntimeError):
 
 class LsqOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_uint32), ("fresnel", C.c_float), ("flags", C.c_uint32),
-                ("mse_target", C.c_double), ("break_on_small_step", C.c_double)]
+                ("mse_target", C.c_double), ("break_on_small_step", C.c_double), ("restarts", C.c_uint32)]
 
 
 class TexelStats(C.Structure):
@@ -122,11 +122,13 @@ def _check(status: int):
         raise SvfError(status, load().svf_last_error().decode())
 
 
-def options(max_iterations: int = 1024, fresnel: float = 1.0) -> LsqOptions:
+def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | None = None) -> LsqOptions:
     o = LsqOptions()
     load().svf_lsq_options_default(C.byref(o))
     o.max_iterations = max_iterations
     o.fresnel = fresnel
+    if restarts is not None:
+        o.restarts = restarts
     return o
 
 

@@ -142,16 +142,22 @@ bool is_device_pointer(const void* p)
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
-// Direction layout: LM geometry and, once needed, the default-init tables.
+// Default-init tables of one (direction table, mesh) pair.
+struct InitData
+{
+    svf::InitLayout init{};
+    DevBuf op, row_texel, denom_w, pca_cell_id, pca_cell_start, pca_index, pca_frac, pca_dir, proj_dir, proj_frac,
+        proj_cell;
+};
+
+// Direction layout: LM geometry and, once needed, the default-init tables per
+// interpolation mesh (the caller's mesh, or the library's own triangulation).
 struct Layout
 {
     uint32_t L = 0;
     std::vector<float> lp;
     DevBuf geo;                 // [3][L] Cartesian directions (LM)
-    bool init_ready = false;
-    svf::InitLayout init{};
-    DevBuf op, row_texel, denom_w, pca_cell_id, pca_cell_start, pca_index, pca_frac, pca_dir, proj_dir, proj_frac,
-        proj_cell;
+    std::map<uint64_t, std::unique_ptr<InitData>> inits;
 };
 
 } // namespace
@@ -193,6 +199,8 @@ svf_status check_options(const svf_lsq_options* o)
         return fail(SVF_EINVAL, "fresnel (refractive index) must be >= 1, got %g", o->fresnel);
     if(!(o->mse_target >= 0.0) || !(o->break_on_small_step > 0.0))
         return fail(SVF_EINVAL, "mse_target must be >= 0 and break_on_small_step > 0");
+    if(o->restarts > 16)
+        return fail(SVF_EINVAL, "restarts must be <= 16, got %u", o->restarts);
     return SVF_OK;
 }
 
@@ -242,18 +250,30 @@ svf_status upload(DevBuf& dst, const std::vector<T>& v)
     return SVF_OK;
 }
 
-// Builds the default-init tables of a layout, with its mesh (given, or computed).
-svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc)
+// Builds (once per mesh) the default-init tables of a layout, with the given
+// mesh or the library's own triangulation.
+svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc, const svf::InitLayout** out)
 {
-    if(lay->init_ready)
-        return SVF_OK;
     const uint32_t L = lay->L, N = L * L;
-    std::vector<uint32_t> tris, edges;
-    std::vector<float> eang;
+    uint64_t key = 0;   // 0: the library's triangulation
     if(desc->triangles)
     {
         if(desc->triangle_count == 0 || !desc->edges || !desc->edge_angles || desc->edge_count == 0)
             return fail(SVF_EINVAL, "a given mesh needs triangles, edges and edge angles");
+        key = fnv1a(desc->triangles, sizeof(uint32_t) * 3 * (size_t)desc->triangle_count);
+        key = fnv1a(desc->edges, sizeof(uint32_t) * 3 * (size_t)desc->edge_count, key);
+        key = fnv1a(desc->edge_angles, sizeof(float) * 2 * (size_t)desc->edge_count, key) | 1u;
+    }
+    auto found = lay->inits.find(key);
+    if(found != lay->inits.end())
+    {
+        *out = &found->second->init;
+        return SVF_OK;
+    }
+    std::vector<uint32_t> tris, edges;
+    std::vector<float> eang;
+    if(desc->triangles)
+    {
         tris.assign(desc->triangles, desc->triangles + 3 * (size_t)desc->triangle_count);
         edges.assign(desc->edges, desc->edges + 3 * (size_t)desc->edge_count);
         eang.assign(desc->edge_angles, desc->edge_angles + 2 * (size_t)desc->edge_count);
@@ -276,36 +296,38 @@ svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc)
         svf::build_init_host_tables(*ctx->tables);
     }
     const svf::InitHostTables& t = *ctx->tables;
-    svf::InitLayout& il = lay->init;
+    auto data = std::make_unique<InitData>();
+    InitData* dd = data.get();
+    svf::InitLayout& il = dd->init;
     il.L = L;
     il.N = N;
     il.k_pad = (uint32_t)round_up(N, 8);
     il.ndf_rows = (uint32_t)t.ndf_row_texel.size();
     il.ndf_rows_pad = (uint32_t)round_up(il.ndf_rows, 128);
-    SVF_TRY(lay->op.ensure(sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
-    SVF_CUDA(cudaMemset(lay->op.p, 0, sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
-    SVF_TRY(upload(lay->row_texel, t.ndf_row_texel));
-    SVF_TRY(upload(lay->denom_w, t.denom_w));
-    SVF_TRY(upload(lay->pca_cell_id, t.pca_cell_id));
-    SVF_TRY(upload(lay->pca_cell_start, t.pca_cell_start));
-    SVF_TRY(upload(lay->pca_index, t.pca_index));
-    SVF_TRY(upload(lay->pca_frac, t.pca_frac));
-    SVF_TRY(upload(lay->pca_dir, t.pca_dir));
-    SVF_TRY(upload(lay->proj_dir, t.proj_dir));
-    SVF_TRY(upload(lay->proj_frac, t.proj_frac));
-    SVF_TRY(upload(lay->proj_cell, t.proj_cell));
-    il.ndf_op = lay->op.as<float>();
-    il.ndf_row_texel = lay->row_texel.as<int32_t>();
-    il.denom_w = lay->denom_w.as<float>();
+    SVF_TRY(dd->op.ensure(sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
+    SVF_CUDA(cudaMemset(dd->op.p, 0, sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
+    SVF_TRY(upload(dd->row_texel, t.ndf_row_texel));
+    SVF_TRY(upload(dd->denom_w, t.denom_w));
+    SVF_TRY(upload(dd->pca_cell_id, t.pca_cell_id));
+    SVF_TRY(upload(dd->pca_cell_start, t.pca_cell_start));
+    SVF_TRY(upload(dd->pca_index, t.pca_index));
+    SVF_TRY(upload(dd->pca_frac, t.pca_frac));
+    SVF_TRY(upload(dd->pca_dir, t.pca_dir));
+    SVF_TRY(upload(dd->proj_dir, t.proj_dir));
+    SVF_TRY(upload(dd->proj_frac, t.proj_frac));
+    SVF_TRY(upload(dd->proj_cell, t.proj_cell));
+    il.ndf_op = dd->op.as<float>();
+    il.ndf_row_texel = dd->row_texel.as<int32_t>();
+    il.denom_w = dd->denom_w.as<float>();
     il.pca_cells = (uint32_t)t.pca_cell_id.size();
-    il.pca_cell_id = lay->pca_cell_id.as<int32_t>();
-    il.pca_cell_start = lay->pca_cell_start.as<uint32_t>();
-    il.pca_index = lay->pca_index.as<uint32_t>();
-    il.pca_frac = lay->pca_frac.as<float2>();
-    il.pca_dir = lay->pca_dir.as<float4>();
-    il.proj_dir = lay->proj_dir.as<float4>();
-    il.proj_frac = lay->proj_frac.as<float2>();
-    il.proj_cell = lay->proj_cell.as<int32_t>();
+    il.pca_cell_id = dd->pca_cell_id.as<int32_t>();
+    il.pca_cell_start = dd->pca_cell_start.as<uint32_t>();
+    il.pca_index = dd->pca_index.as<uint32_t>();
+    il.pca_frac = dd->pca_frac.as<float2>();
+    il.pca_dir = dd->pca_dir.as<float4>();
+    il.proj_dir = dd->proj_dir.as<float4>();
+    il.proj_frac = dd->proj_frac.as<float2>();
+    il.proj_cell = dd->proj_cell.as<int32_t>();
     il.rot_s = t.rot_s;
     il.rot_c = t.rot_c;
     il.pdf = t.pdf;
@@ -328,7 +350,8 @@ svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc)
     SVF_CUDA(svf::launch_ndf_operator(il, mesh, d_dirs.as<float>(), d_normals.as<float>(), t.ndf_scale,
                                       d_ltri.as<int32_t>(), d_lbary.as<float>(), ctx->stream));
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));
-    lay->init_ready = true;
+    *out = &dd->init;
+    lay->inits.emplace(key, std::move(data));
     return SVF_OK;
 }
 
@@ -374,6 +397,7 @@ svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmR
     a.cfg.mse_target = o->mse_target;
     a.cfg.eps = o->break_on_small_step;
     a.cfg.fresnel = o->fresnel;
+    a.cfg.restarts = o->restarts;
     SVF_TRY(ctx->counter.ensure(16));
     SVF_TRY(ctx->error.ensure(16));
     a.work_counter = ctx->counter.as<uint32_t>();
@@ -434,6 +458,7 @@ void svf_lsq_options_default(svf_lsq_options* o)
     o->flags = SVF_LSQ_DIFFUSE;
     o->mse_target = 1e-6;
     o->break_on_small_step = (double)1e-3f;   // settings.BreakOnSmallStep = 1e-3f
+    o->restarts = 1;
 }
 
 svf_status svf_create(int device, svf_ctx** out)
@@ -595,8 +620,9 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     SVF_TRY(get_layout(ctx, desc->lights_parabolic, desc->light_count, &lay));
     const uint32_t L = lay->L, N = L * L;
     const uint64_t stride = round_up(N, 8);
+    const svf::InitLayout* init_lay = nullptr;
     if(opts->init_mode == SVF_INIT_DEFAULT)
-        SVF_TRY(prepare_init(ctx, lay, desc));
+        SVF_TRY(prepare_init(ctx, lay, desc, &init_lay));
 
     const size_t elem = btf->sample_type == SVF_SAMPLES_F16 ? 2 : 4;
     const size_t texel_bytes = elem * 3 * (size_t)N;
@@ -647,9 +673,9 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
         if(opts->init_mode == SVF_INIT_DEFAULT)
         {
-            SVF_CUDA(svf::launch_ndf_gemm(lay->init, ctx->lum.as<float>(), stride, n, ctx->ndf.as<float>(),
+            SVF_CUDA(svf::launch_ndf_gemm(*init_lay, ctx->lum.as<float>(), stride, n, ctx->ndf.as<float>(),
                                           ctx->stream));
-            SVF_CUDA(svf::launch_init_finish(lay->init, ctx->ndf.as<float>(), n, ctx->init.as<float>(), nullptr,
+            SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->ndf.as<float>(), n, ctx->init.as<float>(), nullptr,
                                              ctx->stream));
         }
         else

@@ -17,6 +17,7 @@ struct LmConfig
     double   mse_target;
     double   eps;          // BreakOnSmallStep
     float    fresnel;
+    uint32_t restarts;     // continuations from a stop point with fresh damping
 };
 
 // Arguments of the persistent LM kernel.

@@ -107,8 +107,29 @@ struct LmState
     double H[kHessian];     // J^T J, packed upper
     double S;               // sum of squared residuals at p
     double lam, nu, rho;
-    uint32_t iter, eff, njac, nres, status;
+    uint32_t iter, eff, njac, nres, status, restarts_left;
 };
+
+// Fresh damping from the current normal equations (fitting.hh:531-538).
+__device__ __forceinline__ void lm_reset_damping(LmState& st)
+{
+    double damping = 1.0;   // InitialMinDamping
+    for(int i = 0; i < kParams; ++i)
+        damping = fmax(damping, st.H[hidx(i, i)]);
+    st.lam = damping * 0.75;   // InitialDampingMultiplier
+    st.nu = 2.0;               // DampingFailureMultiplier
+}
+
+// Where the reference's loop ends, optionally continue once more with fresh
+// damping from the same point; false when the fit is finished.
+__device__ __forceinline__ bool lm_restart(LmState& st, const LmConfig& cfg, double n_pairs)
+{
+    if(st.restarts_left == 0 || !(st.iter < cfg.max_iter && cfg.mse_target < st.S / n_pairs))
+        return false;
+    --st.restarts_left;
+    lm_reset_damping(st);
+    return true;
+}
 
 // In-place Cholesky of a packed 7x7 SPD matrix; false unless every pivot is
 // positive and finite.
@@ -157,6 +178,49 @@ __device__ void cholesky7_solve(const double* Lm, const double* b, double* x)
     }
 }
 
+// Damped step (H + lam I) d = g by Cholesky.  Active set at the bound: a
+// parameter with a lower bound (sigma, specular, diffuse) that sits exactly at 0
+// and whose step points below it is held at 0 for this solve (its row and
+// column are dropped) and the system is solved again.  The reference instead
+// rejects every such step (AcceptStepConstraints), which with an exact
+// derivative would hold the parameter at 0 for good; its finite-difference
+// derivative at exactly 0 (fitting.hh:896-905, step 1e-8) is below float
+// resolution there.  Returns false when the factorisation fails.
+__device__ bool lm_solve(LmState& st)
+{
+    uint32_t frozen = 0;
+    for(int round = 0; round < 5; ++round)
+    {
+        double A[kHessian], b[kParams];
+        for(int i = 0; i < kHessian; ++i)
+            A[i] = st.H[i];
+        for(int i = 0; i < kParams; ++i)
+        {
+            A[hidx(i, i)] += st.lam;
+            b[i] = st.g[i];
+        }
+        for(int i = 0; i < 4; ++i)
+            if(frozen & (1u << i))
+            {
+                for(int j = 0; j < kParams; ++j)
+                    if(j != i)
+                        A[hidx(i, j)] = 0.0;
+                b[i] = 0.0;
+            }
+        if(!cholesky7(A))
+            return false;
+        cholesky7_solve(A, b, st.d);
+        uint32_t more = frozen;
+        for(int i = 0; i < 4; ++i)
+            if(st.p[i] == 0.0 && st.d[i] > 0.0)
+                more |= 1u << i;
+        if(more == frozen)
+            return true;
+        frozen = more;
+    }
+    return true;
+}
+
 // The top of one LM iteration (fitting.hh:541-590): solve for a step that passes
 // the constraints, or finish.  Returns kCmdTrial (st.pt holds the trial point)
 // or kCmdDone.
@@ -170,12 +234,7 @@ __device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
                 st.status |= SVF_TEXEL_MAX_ITER;
             return kCmdDone;
         }
-        double A[kHessian];
-        for(int i = 0; i < kHessian; ++i)
-            A[i] = st.H[i];
-        for(int i = 0; i < kParams; ++i)
-            A[hidx(i, i)] += st.lam;
-        if(!cholesky7(A))
+        if(!lm_solve(st))
         {
             // the reference's inverse came out non-finite: damp harder
             st.lam *= st.nu;
@@ -183,7 +242,6 @@ __device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
             ++st.iter;
             continue;
         }
-        cholesky7_solve(A, st.g, st.d);
         double step2 = 0.0, mag2 = 0.0;
         for(int i = 0; i < kParams; ++i)
         {
@@ -198,7 +256,11 @@ __device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
             return kCmdDone;
         }
         if(step_len <= cfg.eps * (sqrt(mag2) + cfg.eps))
+        {
+            if(lm_restart(st, cfg, n_pairs))
+                continue;
             return kCmdDone;
+        }
         // AcceptStepConstraints (svbrdf-lsq-fitting-internal.hh:67-77)
         bool accept = true;
         for(int i = 0; i < 4; ++i)
@@ -244,7 +306,7 @@ __device__ int lm_after_trial(LmState& st, const LmConfig& cfg, double S1, doubl
 }
 
 // After the Jacobian at an accepted point (fitting.hh:612-660).
-__device__ int lm_after_jacobian(LmState& st, const LmConfig& cfg, const double* red)
+__device__ int lm_after_jacobian(LmState& st, const LmConfig& cfg, const double* red, double n_pairs)
 {
     ++st.njac;
     double glen = 0.0;
@@ -253,10 +315,10 @@ __device__ int lm_after_jacobian(LmState& st, const LmConfig& cfg, const double*
         st.g[i] = -red[kHessian + i];
         glen += st.g[i] * st.g[i];
     }
-    if(glen <= cfg.eps * cfg.eps)
-        return kCmdDone;
     for(int i = 0; i < kHessian; ++i)
         st.H[i] = red[i];
+    if(glen <= cfg.eps * cfg.eps)
+        return lm_restart(st, cfg, n_pairs) ? kCmdContinue : kCmdDone;
     const double min_mul = (double)(1.0f / 3.0f);
     double t = 2.0 * st.rho - 1.0;
     double mul = fmax(min_mul, 1.0 - t * t * t);
@@ -546,19 +608,13 @@ __global__ void __launch_bounds__(kThreads) lm_fit_kernel(LmArgs args)
         if(threadIdx.x == 0)
         {
             st.njac = 1;
+            st.restarts_left = args.cfg.restarts;
             st.S = sh_red_out[kHessian + kParams];
-            double damping = 1.0;   // InitialMinDamping
             for(int i = 0; i < kParams; ++i)
-            {
                 st.g[i] = -sh_red_out[kHessian + i];
-                st.H[i] = 0.0;
-            }
             for(int i = 0; i < kHessian; ++i)
                 st.H[i] = sh_red_out[i];
-            for(int i = 0; i < kParams; ++i)
-                damping = fmax(damping, st.H[hidx(i, i)]);
-            st.lam = damping * 0.75;   // InitialDampingMultiplier
-            st.nu = 2.0;               // DampingFailureMultiplier
+            lm_reset_damping(st);
             if(!isfinite(st.S))
                 st.status |= SVF_TEXEL_NONFINITE;
         }
@@ -589,7 +645,7 @@ __global__ void __launch_bounds__(kThreads) lm_fit_kernel(LmArgs args)
                 // the table built for the trial point is the accepted point's
                 pair_pass<true>(sh, lum, sh_pf, L, args.cfg.fresnel, sh_red_out);
                 if(threadIdx.x == 0)
-                    sh_cmd = lm_after_jacobian(st, args.cfg, sh_red_out);
+                    sh_cmd = lm_after_jacobian(st, args.cfg, sh_red_out, n_pairs);
                 __syncthreads();
                 if(sh_cmd == kCmdDone)
                     break;

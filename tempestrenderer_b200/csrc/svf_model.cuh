@@ -48,7 +48,7 @@ constexpr int kHessian = 28;          // packed upper triangle of the 7x7 J^T J
 struct ParamSet
 {
     float sx, sy, ks, kd;   // clamped parameters
-    float ks_on, kd_on;     // 1 where the unclamped albedo is > 0 (derivative mask)
+    float ks_on, kd_on;     // 1 where the unclamped albedo is >= 0 (derivative mask)
     float R[9];             // ToMatrix3: column c is R[3c..3c+2]
     float om[3][3];         // body-frame angular velocity of R per Euler angle
     float u, v;             // 1/sx^2, 1/sy^2
@@ -74,8 +74,12 @@ SVF_HD void make_param_set(const float* p, ParamSet& ps)
     ps.sy = p[1] > 0.0f ? p[1] : 0.0f;
     ps.ks = p[2] > 0.0f ? p[2] : 0.0f;
     ps.kd = p[3] > 0.0f ? p[3] : 0.0f;
-    ps.ks_on = p[2] > 0.0f ? 1.0f : 0.0f;
-    ps.kd_on = p[3] > 0.0f ? 1.0f : 0.0f;
+    // Derivative masks of the clamped albedos: the step constraint keeps them
+    // >= 0 (AcceptStepConstraints), so at exactly 0 the right derivative applies
+    // (the default initial guess starts with diffuse = 0, pipeline.cc:659); the
+    // LM's active-set rule holds a parameter at 0 when its step points below it.
+    ps.ks_on = p[2] >= 0.0f ? 1.0f : 0.0f;
+    ps.kd_on = p[3] >= 0.0f ? 1.0f : 0.0f;
 
     float s1, c1, s2, c2, s3, c3;
     sincos_f(0.5f * p[4], &s1, &c1);
