@@ -1,0 +1,324 @@
+"""Benchmark: fitted texels/s of the SVBRDF fit (81x81 directions) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one step): the svbrdffit texel loop over a 400x400-texel synthetic
+BTF with the 81-direction ring layout (6561 direction pairs), RGB FP32 samples,
+the uneven parameter mix (20% near-diffuse, 10% strongly anisotropic) -- the
+batched persistent fit of 400x400 texels.  Per texel: luminance slice, the
+reference's default initial guess (NDF -> PCA -> SGGX projection), LM
+(max 1024 iterations, Fresnel 1) and the five output maps.
+
+* value: texels/s with the samples resident in HBM (12.6 GB, larger than L2),
+  timed with CUDA events on the library's stream, max over ranks.
+* e2e: the same through the public C ABI with pinned HOST buffers: the step's
+  samples are copied host->device and all maps device->host inside the timed
+  region.
+* roofline: the LM kernel (the dominant kernel) against the FP32 CUDA-core peak
+  (SMs x 128 lanes x 2 flops x SM clock sampled under load), with its
+  algorithmic flops counted per pair evaluation.
+* cpu_baseline: the reference's own CPU fitter (oracle/_ref, compiled from the
+  reference's sources) on a bounded sample of the same texels, all host cores.
+
+Multi-GPU: texels are independent; each rank fits its own 400x400 shard (weak
+scaling), no data-path collective.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "fitted texels/s (81x81 dirs) at residual <=1.01x plain LM; % of FP32/HBM peak"
+SEED, MIX = 2024, 1
+WIDTH = HEIGHT = 400
+# flops per direction-pair evaluation of the LM kernel (FMA = 2), counted from
+# svf_model.cuh::eval_pair and the accumulation in svf_kernels.cu::pair_pass
+FLOPS_JACOBIAN_PASS = 169
+FLOPS_RESIDUAL_PASS = 33
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"svf_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) >= 9 and f[1].replace(".", "").isdigit():
+                    rows.append(f)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = np.array([float(r[1]) for r in rows])
+        reasons = set()
+        for r in rows:
+            for name, val in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"),
+                                 r[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def ring81_mesh():
+    import tempestrenderer_b200 as svf
+
+    lp = svf.directions_ring81()
+    tri, edges, angles = svf.triangulate(lp)
+    return svf.Layout(lp, tri, edges, angles)
+
+
+# ----------------------------------------------------------------------------
+# the reference's CPU fitter
+# ----------------------------------------------------------------------------
+
+def reference_fit_rate(texels: int, first: int = 0, threads: int | None = None):
+    """Times the reference's texel loop (oracle/_ref) on `texels` texels of the
+    benchmark BTF, all host threads; returns (texels/s, seconds, threads)."""
+    import oracle
+
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref/libtempest_ref.so is not built")
+    threads = threads or os.cpu_count() or 1
+    tp = oracle.ring81_angles()
+    lp = oracle.angles_to_parabolic(tp)
+    rgb = np.stack([oracle.synth_render(SEED, first + t, oracle.synth_truth(SEED, MIX, first + t), lp)
+                    for t in range(texels)])
+    btf = oracle.RefBTF.from_texels(tp, rgb)
+    secs, rmse = btf.time_fit(0, texels, threads, 0)
+    return texels / secs, secs, threads, rmse
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    sample = max(16, 2 * threads)
+    for _ in range(args.warmup):
+        reference_fit_rate(min(sample, 16), threads=threads)
+    rates, secs_total, done = [], 0.0, 0
+    for k in range(args.steps):
+        rate, secs, thr, _ = reference_fit_rate(sample, first=k * sample, threads=threads)
+        rates.append(rate)
+        secs_total += secs
+        done += sample
+    value = done / secs_total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "texels/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs_total / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32/f64",
+            "data": "synthetic",
+            "config": {"workload": f"svbrdffit texel loop, {WIDTH}x{HEIGHT} texels, ring-81 layout, RGB FP32, "
+                                   f"mix 20% near-diffuse/10% anisotropic, default init, LM 1024 max",
+                       "texels_per_step": sample, "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": "texels/s", "cores": threads, "kind": "reference",
+                             "sample": f"{sample} texels of the benchmark BTF per step, {threads} worker threads"},
+            "e2e": {"value": value, "unit": "texels/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------
+# the GPU fitter
+# ----------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+
+    import tempestrenderer_b200 as svf
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    W, H = args.width, args.height
+    T = W * H
+    layout = ring81_mesh()
+    L = layout.light_count
+    N = L * L
+    ctx = svf.Context(local)
+    # this rank's shard of a larger synthetic BTF: texels [rank*T, (rank+1)*T)
+    samples = torch.empty((T, N, 3), dtype=torch.float32, device=dev)
+    ctx.synth_btf(SEED, MIX, layout.lights_parabolic, rank * T, T, samples)
+    torch.cuda.synchronize()
+    maps = {k: torch.zeros(s, dtype=torch.float32, device=dev) for k, s in
+            {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
+             "params": (T, 7)}.items()}
+    want = tuple(maps.keys())
+    opts = svf.options(max_iterations=1024)
+
+    def step():
+        res, rs = ctx.fit_texels(layout, samples, W, H, opts=opts, want=want, out=maps, check=False)
+        return rs
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    stats = []
+    with ClockSampler(local) as clocks:
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            stats.append(step())
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    if dist:
+        dist.barrier()
+    ms = float(sum(s.ms_total for s in stats))
+    ms_fit = float(sum(s.ms_fit for s in stats))
+    ms_init = float(sum(s.ms_init for s in stats))
+    ms_lum = float(sum(s.ms_luminance for s in stats))
+    jac = sum(s.jacobians for s in stats)
+    res = sum(s.residuals for s in stats)
+    failed = sum(s.failed_texels for s in stats)
+    t_max = ms
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max = float(t.item())
+    value = world * T * args.steps / (t_max / 1e3)
+
+    # e2e through the C ABI with pinned host buffers
+    e2e = None
+    if args.e2e_steps > 0:
+        host_samples = torch.empty((T, N, 3), dtype=torch.float32, pin_memory=True)
+        host_samples.copy_(samples)
+        host_maps = {k: torch.zeros(v.shape, dtype=torch.float32, pin_memory=True) for k, v in maps.items()}
+        ctx.fit_texels(layout, host_samples, W, H, opts=opts, want=want, out=host_maps, check=False)
+        if dist:
+            dist.barrier()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        ev0.record()
+        for _ in range(args.e2e_steps):
+            ctx.fit_texels(layout, host_samples, W, H, opts=opts, want=want, out=host_maps, check=False)
+        ev1.record()
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        h2d = host_samples.numel() * 4
+        d2h = sum(v.numel() * 4 for v in host_maps.values())
+        e2e = {"value": world * T * args.e2e_steps / e2e_s, "unit": "texels/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": args.e2e_steps}
+        del host_samples
+
+    if rank == 0:
+        props = torch.cuda.get_device_properties(dev)
+        clk = clocks.summary()
+        peaks_path = os.path.join(HERE, "MEASURED_PEAKS.json")
+        peaks = json.load(open(peaks_path)) if os.path.exists(peaks_path) else {}
+        sm_mhz = clk["sm_mhz"] or peaks.get("clocks_under_load", {}).get("sm_mhz_median") or 1335.0
+        fp32_peak = props.multi_processor_count * 128 * 2 * sm_mhz * 1e6 / 1e12   # TFLOP/s at the sampled clock
+        lm_flops = N * (FLOPS_JACOBIAN_PASS * jac + FLOPS_RESIDUAL_PASS * res)
+        achieved = lm_flops / (ms_fit / 1e3) / 1e12
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                rate, secs, thr, _ = reference_fit_rate(max(16, 2 * (os.cpu_count() or 1)))
+                cpu = {"value": rate, "unit": "texels/s", "cores": thr, "kind": "reference",
+                       "sample": f"first {max(16, 2 * thr)} texels of the benchmark BTF, {thr} threads, "
+                                 f"{secs:.1f} s"}
+            except Exception as e:  # the checker may be absent on a box without it built
+                cpu = {"value": None, "unit": "texels/s", "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"unavailable: {e}"}
+        line = {
+            "metric": METRIC, "value": value, "unit": "texels/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"svbrdffit texel loop, {W}x{H} texels per GPU, ring-81 layout (6561 pairs), "
+                                   f"RGB FP32 in HBM, mix 20% near-diffuse/10% anisotropic, default init, LM 1024 max",
+                       "texels_per_gpu": T, "l2": "inputs 12.6 GB per GPU, larger than L2",
+                       "parallelism": f"texel shards x{world}"},
+            "roofline": {"bound": "fp32", "kernel": "lm_fit_kernel", "achieved": achieved, "peak": fp32_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                         "peak_source": f"derived: {props.multi_processor_count} SMs x 128 FP32 lanes x 2 x "
+                                        f"{sm_mhz:.0f} MHz (sampled SM clock under load)"},
+            "phases_ms": {"luminance": ms_lum / args.steps, "init": ms_init / args.steps,
+                          "lm": ms_fit / args.steps},
+            "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
+                        "failed_texels": failed},
+            "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
+            "wall_s": wall,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--width", type=int, default=WIDTH)
+    ap.add_argument("--height", type=int, default=HEIGHT)
+    ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())
