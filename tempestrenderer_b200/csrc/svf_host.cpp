@@ -27,16 +27,16 @@
 namespace
 {
 
-thread_local std::string g_last_error;
+// The calling thread's last error message, in a fixed buffer so that reporting
+// an error (out-of-memory included) allocates nothing.
+thread_local char g_last_error[512];
 
 svf_status fail(svf_status s, const char* fmt, ...)
 {
-    char buf[512];
     va_list ap;
     va_start(ap, fmt);
-    vsnprintf(buf, sizeof(buf), fmt, ap);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
     va_end(ap);
-    g_last_error = buf;
     return s;
 }
 
@@ -447,7 +447,7 @@ const char* svf_status_string(svf_status s)
     return "unknown status";
 }
 
-const char* svf_last_error(void) { return g_last_error.c_str(); }
+const char* svf_last_error(void) { return g_last_error; }
 
 void svf_lsq_options_default(svf_lsq_options* o)
 {
