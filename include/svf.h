@@ -153,6 +153,38 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lights_parabolic, uint32
                              const svf_lsq_options* options, const float* init,
                              float* out, float* rmse, svf_texel_stats* stats);
 
+/* svf_lsq_fit_batch without any allocation.  This entry point has no
+ * counterpart in the reference.
+ *
+ * It is for callers that must not allocate GPU memory while they fit: an
+ * engine or framework that owns every device allocation through its own pool
+ * and forbids cudaMalloc/cudaFree behind its back, or a frame loop that must
+ * not stall or fragment memory on allocation.  It calls no cudaMalloc,
+ * cudaFree or other allocating routine and needs no context.  Its working
+ * memory (luminance slabs, direction table, work counter, error flag) is one
+ * static device array of SVF_NOALLOC_SCRATCH_BYTES that every GPU which loads
+ * the library holds until the process exits.
+ *
+ * - Every buffer (lights_parabolic, lum, init, out, rmse, stats) must be device
+ *   memory of the current device; stats may be NULL.
+ * - Limits: light_count <= 160 and texel_count * (L*L rounded up to 8) <=
+ *   SVF_NOALLOC_MAX_SLAB_FLOATS (79 texels at 81 directions); larger sizes are
+ *   rejected with SVF_EINVAL.
+ * - stream is a cudaStream_t (NULL for the legacy default stream); the call
+ *   enqueues its work there and waits for it before returning.
+ * - The first call on each device looks up the address of the static array
+ *   (cudaGetSymbolAddress) with that device current; make that first call
+ *   before any stream capture.
+ * - All calls share the array and it keeps the last call's contents; calls
+ *   whose work overlaps on the GPU (other threads or streams) race on it and
+ *   must be serialised by the caller. */
+#define SVF_NOALLOC_MAX_SLAB_FLOATS (1u << 19)
+#define SVF_NOALLOC_SCRATCH_BYTES   ((size_t)(SVF_NOALLOC_MAX_SLAB_FLOATS) * 4u + 4096u)
+svf_status svf_lsq_fit_batch_noalloc(const float* lights_parabolic, uint32_t light_count, const float* lum,
+                                     uint64_t lum_stride, uint32_t texel_count, const svf_lsq_options* options,
+                                     const float* init, float* out, float* rmse, svf_texel_stats* stats,
+                                     void* stream);
+
 /* The svbrdffit texel loop ----------------------------------------------------- */
 #define SVF_SAMPLES_F32 0u
 #define SVF_SAMPLES_F16 1u

@@ -32,7 +32,7 @@ SVF_INIT_DEFAULT, SVF_INIT_GIVEN = 0, 1
 # every entry point include/svf.h declares
 EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_options_default", "svf_create",
            "svf_destroy", "svf_directions_ring81", "svf_directions_fibonacci", "svf_layout_triangulate",
-           "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_fit_texels", "svf_synth_btf")
+           "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc", "svf_fit_texels", "svf_synth_btf")
 
 
 class SvfError(RuntimeError):
@@ -108,10 +108,12 @@ def load() -> C.CDLL:
         L.svf_layout_triangulate.restype = u32
         L.svf_lsq_fit_sggx.argtypes = [vp, vp, u32, vp, C.POINTER(LsqOptions), vp, vp, vp, C.POINTER(TexelStats)]
         L.svf_lsq_fit_batch.argtypes = [vp, vp, u32, vp, u64, u32, C.POINTER(LsqOptions), vp, vp, vp, vp]
+        L.svf_lsq_fit_batch_noalloc.argtypes = [vp, u32, vp, u64, u32, C.POINTER(LsqOptions), vp, vp, vp, vp, vp]
         L.svf_fit_texels.argtypes = [vp, C.POINTER(BtfView), C.POINTER(FitOptions), C.POINTER(Maps),
                                      C.POINTER(RunStats)]
         L.svf_synth_btf.argtypes = [vp, u32, u32, vp, u32, u64, u64, u32, f32, vp, vp]
-        for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_fit_texels", "svf_synth_btf"):
+        for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
+                     "svf_fit_texels", "svf_synth_btf"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib

@@ -587,6 +587,48 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
     return SVF_OK;
 }
 
+svf_status svf_lsq_fit_batch_noalloc(const float* lp, uint32_t L, const float* lum, uint64_t lum_stride,
+                                     uint32_t texels, const svf_lsq_options* opts, const float* init, float* out,
+                                     float* rmse, svf_texel_stats* stats, void* stream)
+{
+    // Nothing here allocates: the checks read pointer attributes, errors go to the
+    // fixed per-thread message buffer, the work runs in the static scratch array.
+    SVF_TRY(check_options(opts));
+    if(L < 3 || L > 160)
+        return fail(SVF_EINVAL, "light_count must be in [3, 160], got %u", L);
+    const uint64_t N = (uint64_t)L * L;
+    if(lum_stride < N)
+        return fail(SVF_EINVAL, "lum_stride %llu < L*L = %llu", (unsigned long long)lum_stride, (unsigned long long)N);
+    if(texels == 0)
+        return SVF_OK;
+    const uint64_t slab = round_up(N, 8);
+    if((uint64_t)texels * slab > SVF_NOALLOC_MAX_SLAB_FLOATS)
+        return fail(SVF_EINVAL,
+                    "svf_lsq_fit_batch_noalloc: %u texels of %u directions need %llu slab floats, more than the "
+                    "static scratch holds (SVF_NOALLOC_MAX_SLAB_FLOATS = %u, i.e. at most %llu texels here); "
+                    "split the batch",
+                    texels, L, (unsigned long long)((uint64_t)texels * slab), SVF_NOALLOC_MAX_SLAB_FLOATS,
+                    (unsigned long long)(SVF_NOALLOC_MAX_SLAB_FLOATS / slab));
+    const void* must_be_device[] = { lp, lum, init, out, rmse };
+    for(const void* p : must_be_device)
+        if(!is_device_pointer(p))
+            return fail(SVF_EINVAL, "svf_lsq_fit_batch_noalloc: every buffer must be device memory (and not NULL)");
+    if(stats && !is_device_pointer(stats))
+        return fail(SVF_EINVAL, "svf_lsq_fit_batch_noalloc: stats must be device memory or NULL");
+    svf::LmConfig cfg;
+    cfg.max_iter = opts->max_iterations;
+    cfg.mse_target = opts->mse_target;
+    cfg.eps = opts->break_on_small_step;
+    cfg.fresnel = opts->fresnel;
+    cfg.restarts = opts->restarts;
+    uint32_t error_flag = 0;
+    SVF_CUDA(svf::launch_lm_fit_noalloc(lp, L, lum, lum_stride, texels, cfg, init, out, rmse, stats,
+                                        static_cast<cudaStream_t>(stream), &error_flag));
+    if(error_flag)
+        return fail(SVF_ETIMEOUT, "a bounded device wait expired (a texel slab did not arrive)");
+    return SVF_OK;
+}
+
 svf_status svf_lsq_fit_sggx(svf_ctx* ctx, const float* lp, uint32_t L, const float* lum, const svf_lsq_options* opts,
                             const float init[7], float out[7], float* rmse, svf_texel_stats* stats)
 {

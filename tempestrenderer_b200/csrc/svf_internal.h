@@ -46,6 +46,13 @@ size_t     lm_smem_bytes(uint32_t L, uint64_t lum_stride);
 int        lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride);
 cudaError_t launch_lm_fit(const LmArgs& args, int grid, cudaStream_t stream);
 
+// svf_lsq_fit_batch_noalloc: repack, geometry and LM on `stream` with the
+// library's static device scratch array; waits for the stream and returns the
+// kernel's error flag in *error_flag.
+cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, const float* lum, uint64_t lum_stride,
+                                  uint32_t texels, const LmConfig& cfg, const float* init, float* out, float* rmse,
+                                  svf_texel_stats* stats, cudaStream_t stream, uint32_t* error_flag);
+
 // Luminance slice + average chromaticity (BTFParallelExtractLuminanceSlice,
 // src/image/btf.cc:1078-1116) for texels [0, texels) of an RGB sample array.
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,

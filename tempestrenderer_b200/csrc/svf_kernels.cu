@@ -17,6 +17,9 @@
 #include <cuda_fp16.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <mutex>
+
 #include "svf_internal.h"
 #include "svf_model.cuh"
 
@@ -1015,7 +1018,118 @@ __global__ void __launch_bounds__(256) synth_kernel(uint32_t seed, uint32_t mix,
     }
 }
 
+// ------------------------------------------------------------------------------
+// allocation-free LM batch: working memory in one static device array
+// ------------------------------------------------------------------------------
+
+// Layout of the static array: luminance slabs, then the direction table, then
+// the work counter and the error flag.
+constexpr size_t kNoAllocGeoOffset = size_t(SVF_NOALLOC_MAX_SLAB_FLOATS) * sizeof(float);
+constexpr size_t kNoAllocFlagOffset = kNoAllocGeoOffset + 3 * 160 * sizeof(float);
+static_assert(kNoAllocFlagOffset + 16 <= SVF_NOALLOC_SCRATCH_BYTES, "no-alloc scratch layout overflows");
+
+// Direction table [3][L] from parabolic coordinates, with the operation order
+// and rounding of ParabolicToCartesianCoordinates (vector3.hh:389-393) that the
+// host computes for the other entry points, so both fit identical geometry.
+__global__ void geo_from_parabolic_kernel(const float* __restrict__ lp, uint32_t L, float* __restrict__ geo)
+{
+    const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+    if(d >= L)
+        return;
+    const float px = lp[2 * d], py = lp[2 * d + 1];
+    const float len_sq = __fadd_rn(__fmul_rn(px, px), __fmul_rn(py, py));
+    const float den = __fadd_rn(len_sq, 1.0f);
+    geo[d] = __fdiv_rn(__fmul_rn(2.0f, px), den);
+    geo[L + d] = __fdiv_rn(__fmul_rn(2.0f, py), den);
+    geo[2 * L + d] = __fdiv_rn(__fsub_rn(1.0f, len_sq), __fadd_rn(1.0f, len_sq));
+}
+
 } // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SVF_NOALLOC_SCRATCH_BYTES];
+
+namespace
+{
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_address[kNoAllocMaxDevices];
+
+// Device address of g_noalloc_scratch on the current device, looked up once per
+// device.  In host code the array's name is only a host-side stand-in.
+cudaError_t noalloc_scratch_address(void** out)
+{
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if(e != cudaSuccess)
+        return e;
+    if(dev < 0 || dev >= kNoAllocMaxDevices)
+        return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if(!g_noalloc_address[dev])
+    {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if(e != cudaSuccess)
+            return e;
+        g_noalloc_address[dev] = p;
+    }
+    *out = g_noalloc_address[dev];
+    return cudaSuccess;
+}
+} // namespace
+
+cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, const float* lum, uint64_t lum_stride,
+                                  uint32_t texels, const LmConfig& cfg, const float* init, float* out, float* rmse,
+                                  svf_texel_stats* stats, cudaStream_t stream, uint32_t* error_flag)
+{
+    void* base = nullptr;
+    cudaError_t e = noalloc_scratch_address(&base);
+    if(e != cudaSuccess)
+        return e;
+    unsigned char* scratch = static_cast<unsigned char*>(base);
+    float* slabs = reinterpret_cast<float*>(scratch);
+    float* geo = reinterpret_cast<float*>(scratch + kNoAllocGeoOffset);
+    uint32_t* flags = reinterpret_cast<uint32_t*>(scratch + kNoAllocFlagOffset);
+    const uint32_t N = L * L;
+    const uint64_t stride = (N + 7u) & ~uint64_t(7);
+
+    // the array keeps the previous call's contents: counter and flag start at 0
+    if((e = cudaMemsetAsync(flags, 0, 16, stream)) != cudaSuccess)
+        return e;
+    geo_from_parabolic_kernel<<<(L + 127) / 128, 128, 0, stream>>>(lights_parabolic, L, geo);
+    if((e = cudaGetLastError()) != cudaSuccess)
+        return e;
+    repack_kernel<<<texels, 256, 0, stream>>>(lum, lum_stride, N, slabs, stride);
+    if((e = cudaGetLastError()) != cudaSuccess)
+        return e;
+    int dev = 0, sms = 0;
+    if((e = cudaGetDevice(&dev)) != cudaSuccess ||
+       (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return e;
+    LmArgs a{};
+    a.lum = slabs;
+    a.lum_stride = stride;
+    a.geo = geo;
+    a.init = init;
+    a.out = out;
+    a.rmse = rmse;
+    a.stats = stats;
+    a.L = L;
+    a.N = N;
+    a.texels = texels;
+    a.cfg = cfg;
+    a.work_counter = flags;
+    a.error_flag = flags + 1;
+    const int per_sm = lm_max_ctas_per_sm(L, stride);
+    if(per_sm <= 0)
+        return cudaErrorInvalidConfiguration;
+    const uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * sms, texels);
+    if((e = launch_lm_fit(a, (int)std::max<uint64_t>(grid, 1), stream)) != cudaSuccess)
+        return e;
+    if((e = cudaMemcpyAsync(error_flag, flags + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+        return e;
+    return cudaStreamSynchronize(stream);
+}
 
 size_t lm_smem_bytes(uint32_t L, uint64_t lum_stride)
 {
