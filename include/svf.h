@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define SVF_ABI_VERSION 1u
+#define SVF_ABI_VERSION 2u
 
 typedef enum svf_status
 {
@@ -220,6 +220,10 @@ typedef struct svf_maps
     float*           params;     /* [texels][7]  fitted parameters */
     float*           init;       /* [texels][7]  initial guess used */
     svf_texel_stats* stats;      /* [texels] */
+    float*           ndf;        /* [texels][64*64]  NDF texture of the default initial
+                                  * guess (getLastNDFTexture, svbrdf-fitting.hh:180),
+                                  * row-major, 0 outside the hemisphere; SVF_INIT_DEFAULT
+                                  * only */
 } svf_maps;
 
 typedef struct svf_run_stats
@@ -234,6 +238,8 @@ typedef struct svf_run_stats
     double   ms_init;           /* default initial guess */
     double   ms_fit;            /* Levenberg-Marquardt */
     double   ms_copy;           /* host<->device staging, when host buffers were given */
+    uint32_t lm_threads;        /* LM kernel configuration the autotuner chose: CTA size */
+    uint32_t lm_chunks;         /* and 32-light chunks held in registers per lane */
 } svf_run_stats;
 
 svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,

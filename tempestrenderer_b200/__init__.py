@@ -72,14 +72,15 @@ class FitOptions(C.Structure):
 
 class Maps(C.Structure):
     _fields_ = [("diffuse", C.c_void_p), ("specular", C.c_void_p), ("sigma", C.c_void_p), ("basis", C.c_void_p),
-                ("rmse", C.c_void_p), ("params", C.c_void_p), ("init", C.c_void_p), ("stats", C.c_void_p)]
+                ("rmse", C.c_void_p), ("params", C.c_void_p), ("init", C.c_void_p), ("stats", C.c_void_p),
+                ("ndf", C.c_void_p)]
 
 
 class RunStats(C.Structure):
     _fields_ = [("texels", C.c_uint64), ("iterations", C.c_uint64), ("jacobians", C.c_uint64),
                 ("residuals", C.c_uint64), ("failed_texels", C.c_uint64), ("ms_total", C.c_double),
                 ("ms_luminance", C.c_double), ("ms_init", C.c_double), ("ms_fit", C.c_double),
-                ("ms_copy", C.c_double)]
+                ("ms_copy", C.c_double), ("lm_threads", C.c_uint32), ("lm_chunks", C.c_uint32)]
 
 
 _lib = None
@@ -265,14 +266,14 @@ class Context:
         fo.init_mode = SVF_INIT_DEFAULT if init is None else SVF_INIT_GIVEN
         fo.init_params = _ptr(init) if init is not None else None
         shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
-                  "params": (T, 7), "init": (T, 7)}
+                  "params": (T, 7), "init": (T, 7), "ndf": (T, 64 * 64)}
         res = dict(out or {})
         for k in want:
             if k in res:
                 continue
             res[k] = np.zeros(T, STATS_DTYPE) if k == "stats" else np.zeros(shapes[k], np.float32)
         m = Maps()
-        for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params", "init", "stats"):
+        for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params", "init", "stats", "ndf"):
             setattr(m, k, _ptr(res[k]) if k in res else None)
         rs = RunStats()
         st = self._lib.svf_fit_texels(self.handle, C.byref(v), C.byref(fo), C.byref(m), C.byref(rs))

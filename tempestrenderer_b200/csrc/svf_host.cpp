@@ -3,7 +3,7 @@
 //
 // A fit of texels runs as one stream of kernels:
 //   luminance_kernel     samples -> luminance slices [T][Kp] + average chromaticity
-//   ndf_gemm_kernel      NDF textures = slices x NDF operator^T     (default init)
+//   ndf_tc_kernel        NDF rows = slices x NDF operator^T, tcgen05 (default init)
 //   init_finish_kernel   NDF -> initial parameters                  (default init)
 //   lm_fit_kernel        persistent LM over all texels + output maps
 // Host buffers are staged in chunks through the device.
@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -146,7 +147,7 @@ inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 struct InitData
 {
     svf::InitLayout init{};
-    DevBuf op, row_texel, denom_w, pca_cell_id, pca_cell_start, pca_index, pca_frac, pca_dir, proj_dir, proj_frac,
+    DevBuf op, op_hi, op_lo, row_texel, denom_w, pca_cell_id, pca_cell_start, pca_index, pca_frac, pca_dir, proj_dir, proj_frac,
         proj_cell;
 };
 
@@ -158,6 +159,8 @@ struct Layout
     std::vector<float> lp;
     DevBuf geo;                 // [3][L] Cartesian directions (LM)
     std::map<uint64_t, std::unique_ptr<InitData>> inits;
+    bool tuned = false;         // LM kernel configuration chosen by the autotuner
+    svf::LmKernelChoice choice{ 0, 0 };
 };
 
 } // namespace
@@ -170,10 +173,9 @@ struct svf_ctx
     cudaEvent_t ev[8] = {};
     std::map<uint64_t, std::unique_ptr<Layout>> layouts;
     std::unique_ptr<svf::InitHostTables> tables;
-    DevBuf lum, avg, ndf, init, out, rmse, stats, counter, error, samples, maps_buf, scratch;
+    DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, maps_buf,
+        scratch;
     PinnedBuf pinned;
-    uint64_t ndf_zeroed_key = 0;
-    size_t ndf_zeroed_texels = 0;
 };
 
 namespace
@@ -303,7 +305,7 @@ svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc, 
     il.N = N;
     il.k_pad = (uint32_t)round_up(N, 8);
     il.ndf_rows = (uint32_t)t.ndf_row_texel.size();
-    il.ndf_rows_pad = (uint32_t)round_up(il.ndf_rows, 128);
+    il.ndf_rows_pad = (uint32_t)round_up(il.ndf_rows, 256);
     SVF_TRY(dd->op.ensure(sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
     SVF_CUDA(cudaMemset(dd->op.p, 0, sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
     SVF_TRY(upload(dd->row_texel, t.ndf_row_texel));
@@ -349,6 +351,13 @@ svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc, 
                           d_eang.as<float>(), (uint32_t)(edges.size() / 3) };
     SVF_CUDA(svf::launch_ndf_operator(il, mesh, d_dirs.as<float>(), d_normals.as<float>(), t.ndf_scale,
                                       d_ltri.as<int32_t>(), d_lbary.as<float>(), ctx->stream));
+    // its BF16 hi/lo split for the tensor-core GEMM
+    const uint64_t op_elems = (uint64_t)il.ndf_rows_pad * il.k_pad;
+    SVF_TRY(dd->op_hi.ensure(2 * op_elems));
+    SVF_TRY(dd->op_lo.ensure(2 * op_elems));
+    SVF_CUDA(svf::launch_split_bf16(il.ndf_op, op_elems, dd->op_hi.p, dd->op_lo.p, ctx->stream));
+    il.ndf_op_hi = dd->op_hi.p;
+    il.ndf_op_lo = dd->op_lo.p;
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));
     *out = &dd->init;
     lay->inits.emplace(key, std::move(data));
@@ -375,7 +384,110 @@ struct LmRun
     uint64_t texels;
 };
 
+svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c);
+
+// Autotuner of the LM kernel configuration (CTA size), once per layout: each
+// candidate fits the same seeded synthetic probe (2048 texels of the uneven
+// parameter mix, from a perturbed ground truth) and is scored by model flops per
+// second (the flops per Jacobian and residual pass times the passes it ran,
+// over its CUDA-event time).  The first candidate, the 64-thread kernel, is kept
+// unless another is more than 3% faster.  Tuning on a fixed probe, not on the
+// caller's texels, keeps every texel of a call on one configuration.
+svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
+{
+    if(lay->tuned)
+        return SVF_OK;
+    svf::LmKernelChoice cand[4];
+    const int n_cand = svf::lm_candidates(lay->L, cand, 4);
+    lay->choice = cand[0];
+    if(n_cand <= 1)
+    {
+        lay->tuned = true;
+        return SVF_OK;
+    }
+    const uint32_t L = lay->L, N = L * L;
+    const uint64_t stride = round_up(N, 8), T = 2048;
+    DevBuf samples, truth, lum, avg, init, out, rmse, stats;
+    SVF_TRY(samples.ensure(sizeof(float) * 3 * N * T));
+    SVF_TRY(truth.ensure(sizeof(float) * 16 * T));
+    SVF_TRY(lum.ensure(sizeof(float) * stride * T));
+    SVF_TRY(avg.ensure(sizeof(float) * 3 * T));
+    SVF_TRY(init.ensure(sizeof(float) * 7 * T));
+    SVF_TRY(out.ensure(sizeof(float) * 7 * T));
+    SVF_TRY(rmse.ensure(sizeof(float) * T));
+    SVF_TRY(stats.ensure(sizeof(svf_texel_stats) * T));
+    DevBuf d_lp;
+    SVF_TRY(upload(d_lp, lay->lp));
+    SVF_CUDA(svf::launch_synth(0x5EEDu, 1, d_lp.as<float>(), L, 0, T, SVF_SAMPLES_F32, 0.01f, samples.p,
+                               truth.as<float>(), ctx->stream));
+    SVF_CUDA(svf::launch_luminance(samples.p, SVF_SAMPLES_F32, T, N, lum.as<float>(), stride, avg.as<float>(),
+                                   nullptr, nullptr, ctx->stream));
+    std::vector<float> tr(16 * T), in(7 * T);
+    SVF_CUDA(cudaMemcpyAsync(tr.data(), truth.p, sizeof(float) * 16 * T, cudaMemcpyDeviceToHost, ctx->stream));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    for(uint64_t t = 0; t < T; ++t)
+    {
+        const float* q = &tr[16 * t];   // kd[3], ks[3], sigma[2], quat[4], euler[3], kind
+        const float lw[3] = { 0.2126f, 0.7152f, 0.0722f };
+        const float wob = 1.0f + 0.15f * (float)((int)(t % 7) - 3) / 3.0f;
+        float* p = &in[7 * t];
+        p[0] = q[6] * wob;
+        p[1] = q[7] / wob;
+        p[2] = (lw[0] * q[3] + lw[1] * q[4] + lw[2] * q[5]) * wob;
+        p[3] = (lw[0] * q[0] + lw[1] * q[1] + lw[2] * q[2]) / wob;
+        p[4] = q[12] + 0.1f;
+        p[5] = q[13] - 0.1f;
+        p[6] = q[14] + 0.1f;
+    }
+    SVF_CUDA(cudaMemcpyAsync(init.p, in.data(), sizeof(float) * 7 * T, cudaMemcpyHostToDevice, ctx->stream));
+    LmRun r{ lum.as<float>(), stride, init.as<float>(), out.as<float>(), rmse.as<float>(),
+             stats.as<svf_texel_stats>(), nullptr, nullptr, nullptr, nullptr, nullptr, T };
+    // warm-up (module load, attribute set-up) on a small slice
+    LmRun warm = r;
+    warm.texels = 256;
+    for(int c = 0; c < n_cand; ++c)
+        SVF_TRY(launch_lm(ctx, lay, o, warm, cand[c]));
+    double best_rate = 0.0, first_rate = 0.0;
+    int best = 0;
+    std::vector<svf_texel_stats> st(T);
+    for(int c = 0; c < n_cand; ++c)
+    {
+        SVF_CUDA(cudaEventRecord(ctx->ev[6], ctx->stream));
+        SVF_TRY(launch_lm(ctx, lay, o, r, cand[c]));
+        SVF_CUDA(cudaEventRecord(ctx->ev[7], ctx->stream));
+        SVF_CUDA(cudaMemcpyAsync(st.data(), stats.p, sizeof(svf_texel_stats) * T, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+        float ms = 0.0f;
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[6], ctx->ev[7]));
+        double flops = 0.0;
+        for(auto& s : st)
+            flops += (double)N * (169.0 * s.jacobians + 33.0 * s.residuals);
+        const double rate = flops / std::max(1e-3, (double)ms);
+        if(getenv("SVF_DEBUG"))
+            fprintf(stderr, "svf: LM tune L=%u threads=%d chunks=%d: %.3f ms, %.2f TFLOP/s (model)\n", L,
+                    cand[c].threads, cand[c].nc, ms, rate * 1e-9);
+        if(c == 0)
+            first_rate = rate;
+        if(rate > best_rate)
+        {
+            best_rate = rate;
+            best = c;
+        }
+    }
+    lay->choice = best_rate > 1.03 * first_rate ? cand[best] : cand[0];
+    lay->tuned = true;
+    return SVF_OK;
+}
+
 svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r)
+{
+    if(!lay->tuned && r.texels >= 4096)
+        SVF_TRY(tune_lm(ctx, lay, o));
+    return launch_lm(ctx, lay, o, r, lay->tuned ? lay->choice : svf::lm_default_choice(lay->L));
+}
+
+svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c)
 {
     svf::LmArgs a{};
     a.lum = r.lum;
@@ -403,22 +515,25 @@ svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmR
     a.work_counter = ctx->counter.as<uint32_t>();
     a.error_flag = ctx->error.as<uint32_t>();
     SVF_CUDA(cudaMemsetAsync(ctx->counter.p, 0, 16, ctx->stream));
-    SVF_CUDA(cudaMemsetAsync(ctx->error.p, 0, 16, ctx->stream));
-    int per_sm = svf::lm_max_ctas_per_sm(a.L, a.lum_stride);
+    SVF_CUDA(cudaMemsetAsync(ctx->error.p, 0, 8, ctx->stream));   // word 2 belongs to the NDF GEMM
+    int per_sm = svf::lm_max_ctas_per_sm(a.L, a.lum_stride, c);
     if(per_sm <= 0)
-        return fail(SVF_EINVAL, "the LM kernel does not fit on an SM for L = %u", a.L);
+        return fail(SVF_EINVAL, "the LM kernel (%d threads) does not fit on an SM for L = %u", c.threads, a.L);
     uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->sms, r.texels);
-    SVF_CUDA(svf::launch_lm_fit(a, (int)std::max<uint64_t>(grid, 1), ctx->stream));
+    SVF_CUDA(svf::launch_lm_fit(a, c, (int)std::max<uint64_t>(grid, 1), ctx->stream));
     return SVF_OK;
 }
 
-svf_status read_error_flag(svf_ctx* ctx)
+// Error words: [0] LM kernel, [2] NDF GEMM (with_ndf).
+svf_status read_error_flag(svf_ctx* ctx, bool with_ndf = false)
 {
-    uint32_t flag = 0;
-    SVF_CUDA(cudaMemcpyAsync(&flag, ctx->error.p, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
+    uint32_t flag[3] = {};
+    SVF_CUDA(cudaMemcpyAsync(flag, ctx->error.p, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));
-    if(flag)
+    if(flag[0])
         return fail(SVF_ETIMEOUT, "a bounded device wait expired (a texel slab did not arrive)");
+    if(with_ndf && flag[2])
+        return fail(SVF_ETIMEOUT, "a bounded device wait expired in the NDF GEMM");
     return SVF_OK;
 }
 
@@ -673,11 +788,16 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     // chunking: bounded device footprint for host inputs and the NDF textures
     size_t free_b = 0, total_b = 0;
     SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const bool default_init = opts->init_mode == SVF_INIT_DEFAULT;
+    if(maps->ndf && !default_init)
+        return fail(SVF_EINVAL, "the NDF map exists only with the default initial guess");
+    const uint32_t ndf_ld = default_init ? init_lay->ndf_rows_pad : 0;
     size_t per_texel = sizeof(float) * (stride + 3 + 7 + 7 + 1 + 12) + sizeof(svf_texel_stats) +
-                       (opts->init_mode == SVF_INIT_DEFAULT ? sizeof(float) * svf::kNdfTexels : 0) +
-                       (samples_on_device ? 0 : texel_bytes);
+                       (default_init ? 2 * 2 * stride + sizeof(float) * ndf_ld : 0) +
+                       (maps->ndf ? sizeof(float) * svf::kNdfTexels : 0) + (samples_on_device ? 0 : texel_bytes);
     uint64_t chunk = std::max<uint64_t>(1, (uint64_t)(0.5 * (double)free_b / (double)per_texel));
     chunk = std::min<uint64_t>(chunk, T);
+    chunk = std::min<uint64_t>(chunk, 65535ull * 128);   // the NDF GEMM's grid rows of 128 texels
     if(!samples_on_device)
         chunk = std::min<uint64_t>(chunk, std::max<uint64_t>(1, (256ull << 20) / texel_bytes) * 16);
 
@@ -688,11 +808,15 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     SVF_TRY(ctx->rmse.ensure(sizeof(float) * chunk));
     SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * chunk));
     SVF_TRY(ctx->maps_buf.ensure(sizeof(float) * 12 * chunk));
-    if(opts->init_mode == SVF_INIT_DEFAULT)
+    SVF_TRY(ctx->error.ensure(16));
+    if(default_init)
     {
-        SVF_TRY(ctx->ndf.ensure(sizeof(float) * svf::kNdfTexels * chunk));
-        SVF_CUDA(cudaMemsetAsync(ctx->ndf.p, 0, sizeof(float) * svf::kNdfTexels * chunk, ctx->stream));
+        SVF_TRY(ctx->lum_hi.ensure(2 * stride * chunk));
+        SVF_TRY(ctx->lum_lo.ensure(2 * stride * chunk));
+        SVF_TRY(ctx->ndf.ensure(sizeof(float) * ndf_ld * chunk));
     }
+    if(maps->ndf)
+        SVF_TRY(ctx->ndf_tex.ensure(sizeof(float) * svf::kNdfTexels * chunk));
     if(!samples_on_device)
         SVF_TRY(ctx->samples.ensure(texel_bytes * chunk));
 
@@ -711,14 +835,20 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         }
         SVF_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
-                                       ctx->avg.as<float>(), ctx->stream));
+                                       ctx->avg.as<float>(), default_init ? ctx->lum_hi.p : nullptr,
+                                       default_init ? ctx->lum_lo.p : nullptr, ctx->stream));
         SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
-        if(opts->init_mode == SVF_INIT_DEFAULT)
+        if(default_init)
         {
-            SVF_CUDA(svf::launch_ndf_gemm(*init_lay, ctx->lum.as<float>(), stride, n, ctx->ndf.as<float>(),
-                                          ctx->stream));
-            SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->ndf.as<float>(), n, ctx->init.as<float>(), nullptr,
-                                             ctx->stream));
+            uint32_t* ndf_error = ctx->error.as<uint32_t>() + 2;
+            SVF_CUDA(cudaMemsetAsync(ndf_error, 0, sizeof(uint32_t), ctx->stream));
+            cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.p, ctx->lum_lo.p, n, stride, init_lay->ndf_op_hi,
+                                               init_lay->ndf_op_lo, init_lay->ndf_rows_pad, init_lay->k_pad, N,
+                                               ctx->ndf.as<float>(), ndf_ld, ndf_error, ctx->stream);
+            if(e != cudaSuccess)
+                return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
+            SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->ndf.as<float>(), ndf_ld, n, ctx->init.as<float>(),
+                                             nullptr, maps->ndf ? ctx->ndf_tex.as<float>() : nullptr, ctx->stream));
         }
         else
             SVF_TRY(to_device(ctx, ctx->init.p, opts->init_params + 7 * c0, sizeof(float) * 7 * n));
@@ -741,11 +871,13 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_TRY(put(maps->rmse ? maps->rmse + c0 : nullptr, ctx->rmse.p, sizeof(float) * n));
         SVF_TRY(put(maps->params ? maps->params + 7 * c0 : nullptr, ctx->out.p, sizeof(float) * 7 * n));
         SVF_TRY(put(maps->init ? maps->init + 7 * c0 : nullptr, ctx->init.p, sizeof(float) * 7 * n));
+        SVF_TRY(put(maps->ndf ? maps->ndf + (uint64_t)svf::kNdfTexels * c0 : nullptr, ctx->ndf_tex.p,
+                    sizeof(float) * svf::kNdfTexels * n));
         std::vector<svf_texel_stats> st(n);
         SVF_CUDA(cudaMemcpyAsync(st.data(), ctx->stats.p, sizeof(svf_texel_stats) * n, cudaMemcpyDeviceToHost,
                                  ctx->stream));
         SVF_CUDA(cudaEventRecord(ctx->ev[5], ctx->stream));
-        SVF_TRY(read_error_flag(ctx));
+        SVF_TRY(read_error_flag(ctx, default_init));
         if(maps->stats)
             SVF_CUDA(cudaMemcpy(maps->stats + c0, st.data(), sizeof(svf_texel_stats) * n, cudaMemcpyDefault));
         for(auto& s : st)
@@ -770,6 +902,9 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         rs.ms_fit += ms;
     }
     rs.texels = T;
+    const svf::LmKernelChoice used = lay->tuned ? lay->choice : svf::lm_default_choice(L);
+    rs.lm_threads = (uint32_t)used.threads;
+    rs.lm_chunks = (uint32_t)used.nc;
     if(run)
         *run = rs;
     if(rs.failed_texels)

@@ -7,7 +7,7 @@
 //      directions are the same for every texel, so the NDF is a fixed linear map
 //      of the slice: NDF = Op * lum.  Op ([rows][N], rows = NDF texels inside the
 //      hemisphere) is built once per direction layout (ndf_operator_kernel) and
-//      applied to all texels as one GEMM (ndf_gemm_kernel).
+//      applied to all texels as one tensor-core GEMM (svf_ndf_tc.cu).
 //   2. Per texel (init_finish_kernel): ndf_denom (a fixed linear functional of the
 //      NDF), the PCA normal search (argmax of the bilinear NDF over 512^2
 //      directions, pruned per bilinear cell), the tangent search (512 in-plane
@@ -226,88 +226,6 @@ __global__ void __launch_bounds__(256) ndf_operator_kernel(MeshDevice mesh, uint
 }
 
 // ---------------------------------------------------------------------------
-// NDF = lum * Op^T: FP32 SIMT GEMM, 128x128 tiles, 8x8 outputs per thread
-// ---------------------------------------------------------------------------
-
-constexpr int kBM = 128, kBN = 128, kBK = 8;
-
-__global__ void __launch_bounds__(256) ndf_gemm_kernel(const float* __restrict__ A, uint64_t lda, uint64_t M,
-                                                       const float* __restrict__ B, uint32_t K,
-                                                       const int32_t* __restrict__ row_texel, uint32_t rows,
-                                                       float* __restrict__ ndf)
-{
-    __shared__ __align__(16) float As[2][kBK][kBM];
-    __shared__ __align__(16) float Bs[2][kBK][kBN];
-    const uint32_t tid = threadIdx.x;
-    const uint64_t m0 = (uint64_t)blockIdx.y * kBM;
-    const uint32_t n0 = blockIdx.x * kBN;
-    const uint32_t lr = tid >> 1, lk = (tid & 1) * 4;
-    const bool a_ok = m0 + lr < M;
-    const float* a_src = A + (a_ok ? (m0 + lr) * lda : 0) + lk;
-    const float* b_src = B + (uint64_t)(n0 + lr) * K + lk;
-    const uint32_t tx = tid & 15, ty = tid >> 4;
-
-    float acc[8][8];
-#pragma unroll
-    for(int i = 0; i < 8; ++i)
-#pragma unroll
-        for(int j = 0; j < 8; ++j)
-            acc[i][j] = 0.0f;
-
-    float4 ra = a_ok ? *reinterpret_cast<const float4*>(a_src) : make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 rb = *reinterpret_cast<const float4*>(b_src);
-    As[0][lk + 0][lr] = ra.x; As[0][lk + 1][lr] = ra.y; As[0][lk + 2][lr] = ra.z; As[0][lk + 3][lr] = ra.w;
-    Bs[0][lk + 0][lr] = rb.x; Bs[0][lk + 1][lr] = rb.y; Bs[0][lk + 2][lr] = rb.z; Bs[0][lk + 3][lr] = rb.w;
-    __syncthreads();
-    const uint32_t tiles = K / kBK;
-    for(uint32_t kt = 0; kt < tiles; ++kt)
-    {
-        const int cur = kt & 1;
-        if(kt + 1 < tiles)
-        {
-            ra = a_ok ? *reinterpret_cast<const float4*>(a_src + (kt + 1) * kBK) : make_float4(0.f, 0.f, 0.f, 0.f);
-            rb = *reinterpret_cast<const float4*>(b_src + (kt + 1) * kBK);
-        }
-#pragma unroll
-        for(int k = 0; k < kBK; ++k)
-        {
-            float4 a0 = *reinterpret_cast<const float4*>(&As[cur][k][ty * 8]);
-            float4 a1 = *reinterpret_cast<const float4*>(&As[cur][k][ty * 8 + 4]);
-            float4 b0 = *reinterpret_cast<const float4*>(&Bs[cur][k][tx * 8]);
-            float4 b1 = *reinterpret_cast<const float4*>(&Bs[cur][k][tx * 8 + 4]);
-            const float av[8] = { a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w };
-            const float bv[8] = { b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w };
-#pragma unroll
-            for(int i = 0; i < 8; ++i)
-#pragma unroll
-                for(int j = 0; j < 8; ++j)
-                    acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
-        }
-        if(kt + 1 < tiles)
-        {
-            const int nxt = cur ^ 1;
-            As[nxt][lk + 0][lr] = ra.x; As[nxt][lk + 1][lr] = ra.y; As[nxt][lk + 2][lr] = ra.z; As[nxt][lk + 3][lr] = ra.w;
-            Bs[nxt][lk + 0][lr] = rb.x; Bs[nxt][lk + 1][lr] = rb.y; Bs[nxt][lk + 2][lr] = rb.z; Bs[nxt][lk + 3][lr] = rb.w;
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for(int i = 0; i < 8; ++i)
-    {
-        const uint64_t m = m0 + ty * 8 + i;
-        if(m >= M)
-            continue;
-#pragma unroll
-        for(int j = 0; j < 8; ++j)
-        {
-            const uint32_t r = n0 + tx * 8 + j;
-            if(r < rows)
-                ndf[m * kNdfTexels + row_texel[r]] = acc[i][j];
-        }
-    }
-}
-
-// ---------------------------------------------------------------------------
 // per-texel finish of the initial guess
 // ---------------------------------------------------------------------------
 
@@ -414,8 +332,10 @@ __device__ double block_sum(double x, double* sd)
     return s;
 }
 
-__global__ void __launch_bounds__(kFinishThreads) init_finish_kernel(InitLayout lay, const float* __restrict__ ndf_all,
-                                                                     float* __restrict__ init, float* __restrict__ info)
+__global__ void __launch_bounds__(kFinishThreads) init_finish_kernel(InitLayout lay, const float* __restrict__ ndf_rows,
+                                                                     uint32_t ldr, float* __restrict__ init,
+                                                                     float* __restrict__ info,
+                                                                     float* __restrict__ ndf_out)
 {
     __shared__ __align__(16) float ndf[kNdfTexels];
     __shared__ float tan_seq[3][kTangentSteps];
@@ -424,10 +344,18 @@ __global__ void __launch_bounds__(kFinishThreads) init_finish_kernel(InitLayout 
     __shared__ double sd[32];
     __shared__ float sh_n[3], sh_B[9];
     const uint64_t t = blockIdx.x;
-    const float4* src = reinterpret_cast<const float4*>(ndf_all + t * kNdfTexels);
-    for(uint32_t i = threadIdx.x; i < kNdfTexels / 4; i += kFinishThreads)
-        reinterpret_cast<float4*>(ndf)[i] = src[i];
+    // the operator rows are the NDF texels inside the hemisphere; the rest are 0
+    // (NDFRecord, pipeline.cc:118-123)
+    for(uint32_t i = threadIdx.x; i < kNdfTexels; i += kFinishThreads)
+        ndf[i] = 0.0f;
     __syncthreads();
+    const float* src = ndf_rows + t * ldr;
+    for(uint32_t r = threadIdx.x; r < lay.ndf_rows; r += kFinishThreads)
+        ndf[lay.ndf_row_texel[r]] = src[r];
+    __syncthreads();
+    if(ndf_out)
+        for(uint32_t i = threadIdx.x; i < kNdfTexels; i += kFinishThreads)
+            ndf_out[t * kNdfTexels + i] = ndf[i];
 
     // ndf_denom (pipeline.cc:403-406)
     double part = 0.0;
@@ -679,23 +607,13 @@ cudaError_t launch_ndf_operator(const InitLayout& lay, const MeshDevice& mesh, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_ndf_gemm(const InitLayout& lay, const float* lum, uint64_t lum_stride, uint64_t texels, float* ndf,
-                            cudaStream_t stream)
+cudaError_t launch_init_finish(const InitLayout& lay, const float* ndf_rows, uint32_t ldr, uint64_t texels,
+                               float* init_params, float* init_info, float* ndf_out, cudaStream_t stream)
 {
     if(texels == 0)
         return cudaSuccess;
-    dim3 grid(lay.ndf_rows_pad / kBN, (unsigned)((texels + kBM - 1) / kBM));
-    ndf_gemm_kernel<<<grid, 256, 0, stream>>>(lum, lum_stride, texels, lay.ndf_op, lay.k_pad, lay.ndf_row_texel,
-                                              lay.ndf_rows, ndf);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_init_finish(const InitLayout& lay, const float* ndf, uint64_t texels, float* init_params,
-                               float* init_info, cudaStream_t stream)
-{
-    if(texels == 0)
-        return cudaSuccess;
-    init_finish_kernel<<<(unsigned)texels, kFinishThreads, 0, stream>>>(lay, ndf, init_params, init_info);
+    init_finish_kernel<<<(unsigned)texels, kFinishThreads, 0, stream>>>(lay, ndf_rows, ldr, init_params, init_info,
+                                                                        ndf_out);
     return cudaGetLastError();
 }
 

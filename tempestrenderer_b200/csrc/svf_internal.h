@@ -41,10 +41,18 @@ struct LmArgs
     uint32_t* error_flag;      // set non-zero by a bounded wait that expired
 };
 
-// Kernel launchers (defined in svf_kernels.cu).
-size_t     lm_smem_bytes(uint32_t L, uint64_t lum_stride);
-int        lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride);
-cudaError_t launch_lm_fit(const LmArgs& args, int grid, cudaStream_t stream);
+// LM kernel configuration (svf_lm.cu): CTA size and the number of 32-light
+// chunks each lane keeps in registers (>= ceil(L/32)).
+struct LmKernelChoice
+{
+    int threads;
+    int nc;
+};
+LmKernelChoice lm_default_choice(uint32_t L);
+int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);
+size_t         lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c);
+int            lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c);
+cudaError_t    launch_lm_fit(const LmArgs& args, LmKernelChoice c, int grid, cudaStream_t stream);
 
 // svf_lsq_fit_batch_noalloc: repack, geometry and LM on `stream` with the
 // library's static device scratch array; waits for the stream and returns the
@@ -55,8 +63,11 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
 
 // Luminance slice + average chromaticity (BTFParallelExtractLuminanceSlice,
 // src/image/btf.cc:1078-1116) for texels [0, texels) of an RGB sample array.
+// lum_hi/lum_lo (optional, both or neither): the BF16 split of the slice for the
+// NDF GEMM, same row pitch, columns [0, N) written.
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
-                             float* lum, uint64_t lum_stride, float* avg_chroma, cudaStream_t stream);
+                             float* lum, uint64_t lum_stride, float* avg_chroma, void* lum_hi, void* lum_lo,
+                             cudaStream_t stream);
 
 // Repacks a caller's luminance array to the padded internal layout.
 cudaError_t launch_repack(const float* src, uint64_t src_stride, uint64_t texels, uint32_t N,
@@ -83,8 +94,10 @@ struct InitLayout
     uint32_t L, N;
     uint32_t k_pad;            // N padded to a multiple of 8 (GEMM K)
     uint32_t ndf_rows;         // NDF texels inside the hemisphere (rows of the operator)
-    uint32_t ndf_rows_pad;     // rows padded to a multiple of 128
-    float*    ndf_op;          // [ndf_rows_pad][k_pad] NDF = op * lum (row-major)
+    uint32_t ndf_rows_pad;     // rows padded to a multiple of 256 (the GEMM's N tile)
+    float*    ndf_op;          // [ndf_rows_pad][k_pad] NDF = op * lum (row-major, FP32)
+    void*     ndf_op_hi;       // [ndf_rows_pad][k_pad] BF16 hi/lo split of ndf_op
+    void*     ndf_op_lo;
     int32_t*  ndf_row_texel;   // [ndf_rows] NDF texel index of each operator row
     float*    denom_w;         // [4096] ndf_denom = denom_w . NDF
     // PCA search samples, grouped by the bilinear cell they fall in
@@ -117,10 +130,18 @@ cudaError_t launch_ndf_operator(const InitLayout& lay, const MeshDevice& mesh, c
                                 const float* row_normals /* [rows][3] */, double ndf_scale, int32_t* light_tri,
                                 float* light_bary, cudaStream_t stream);
 
-cudaError_t launch_ndf_gemm(const InitLayout& lay, const float* lum, uint64_t lum_stride, uint64_t texels,
-                            float* ndf, cudaStream_t stream);
-// init_info (optional): [texels][8] = ndf_denom, normal xyz, tangent xyz, pca value
-cudaError_t launch_init_finish(const InitLayout& lay, const float* ndf, uint64_t texels, float* init_params,
-                               float* init_info, cudaStream_t stream);
+// NDF rows C[T][ldc] = A x B^T on the tensor cores (svf_ndf_tc.cu) from BF16
+// hi/lo splits of A (slabs, [T][lda]) and B (operator, [rows_pad][ldb]); k
+// columns of each are used.
+size_t      ndf_tc_smem_bytes();
+cudaError_t launch_split_bf16(const float* x, uint64_t n, void* hi, void* lo, cudaStream_t stream);
+cudaError_t launch_ndf_tc(const void* a_hi, const void* a_lo, uint64_t texels, uint64_t lda, const void* b_hi,
+                          const void* b_lo, uint32_t rows_pad, uint64_t ldb, uint32_t k, float* C, uint32_t ldc,
+                          uint32_t* error_flag, cudaStream_t stream);
+// ndf_rows: [texels][ldr] operator-row NDF values.  init_info (optional):
+// [texels][8] = ndf_denom, normal xyz, tangent xyz, pca value; ndf_out
+// (optional): [texels][4096] NDF textures.
+cudaError_t launch_init_finish(const InitLayout& lay, const float* ndf_rows, uint32_t ldr, uint64_t texels,
+                               float* init_params, float* init_info, float* ndf_out, cudaStream_t stream);
 
 } // namespace svf

@@ -1,18 +1,7 @@
-// svf_kernels.cu - luminance slice, the persistent Levenberg-Marquardt fit and
-// the synthetic BTF renderer, for sm_100a.
-//
-// The LM kernel is persistent: a grid of (resident CTAs per SM) x (SMs) CTAs
-// pulls texels from a global atomic counter (work stealing; a texel that
-// converges early frees its CTA at once).  Each CTA fits one texel at a time
-// with 256 threads.  The texel's luminance slab is staged into shared memory by
-// one bulk TMA copy (cp.async.bulk, completion on an mbarrier), double-buffered:
-// the next texel's slab streams in while the current one is fitted.  Per LM
-// evaluation the CTA tabulates the direction-only terms of the model
-// (svf_model.cuh) for the L directions, then every warp walks the pairs of its
-// views with lanes spread over lights, accumulating r^2 (FP64) and the packed
-// J^T J and J^T r (FP32 per thread, FP64 across warps).  One thread runs the LM
-// control in FP64: damped normal equations by Cholesky, the small-step and
-// gradient tests and the gain-ratio accept/reject of fitting.hh:457-678.
+// svf_kernels.cu - luminance slice, repacking, the synthetic BTF renderer and
+// the allocation-free LM entry, for sm_100a.  The LM kernel itself is in
+// svf_lm.cu.
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
 #include <stdint.h>
@@ -28,691 +17,6 @@ namespace svf
 
 namespace
 {
-
-constexpr int kThreads = 256;
-constexpr int kWarps = kThreads / 32;
-constexpr int kRed = 36;                     // 28 (J^T J) + 7 (J^T r) + r^2
-constexpr int kTabFields = 13;               // DirEntry fields kept in shared memory
-constexpr uint32_t kWaitSpins = 1u << 22;    // bound of every mbarrier wait
-
-enum : int
-{
-    kCmdTrial = 0,
-    kCmdJacobian = 1,
-    kCmdDone = 2,
-    kCmdContinue = 3
-};
-
-// ------------------------------------------------------------------------------
-// mbarrier + bulk copy (TMA) helpers
-// ------------------------------------------------------------------------------
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void fence_barrier_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async()
-{
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-
-// Arms `bar` for `bytes` and starts one bulk copy global -> shared.
-// dst, src 16-byte aligned; bytes a multiple of 16.
-__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
-{
-    uint32_t b = smem_addr(bar);
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(b), "r"(bytes) : "memory");
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-                 ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(b)
-                 : "memory");
-}
-
-// Bounded wait for phase `parity` of `bar`; false when the bound expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
-{
-    uint32_t b = smem_addr(bar);
-    for(uint32_t i = 0; i < kWaitSpins; ++i)
-    {
-        uint32_t done;
-        asm volatile("{\n\t.reg .pred p;\n\t"
-                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(done)
-                     : "r"(b), "r"(parity)
-                     : "memory");
-        if(done)
-            return true;
-    }
-    return false;
-}
-
-// ------------------------------------------------------------------------------
-// FP64 LM control (thread 0 only)
-// ------------------------------------------------------------------------------
-
-struct LmState
-{
-    double p[kParams];      // current parameters
-    double pt[kParams];     // trial parameters
-    double d[kParams];      // step
-    double g[kParams];      // gradient J_r^T r of the residual r = y - f
-    double H[kHessian];     // J^T J, packed upper
-    double S;               // sum of squared residuals at p
-    double lam, nu, rho;
-    uint32_t iter, eff, njac, nres, status, restarts_left;
-};
-
-// Fresh damping from the current normal equations (fitting.hh:531-538).
-__device__ __forceinline__ void lm_reset_damping(LmState& st)
-{
-    double damping = 1.0;   // InitialMinDamping
-    for(int i = 0; i < kParams; ++i)
-        damping = fmax(damping, st.H[hidx(i, i)]);
-    st.lam = damping * 0.75;   // InitialDampingMultiplier
-    st.nu = 2.0;               // DampingFailureMultiplier
-}
-
-// Where the reference's loop ends, optionally continue once more with fresh
-// damping from the same point; false when the fit is finished.
-__device__ __forceinline__ bool lm_restart(LmState& st, const LmConfig& cfg, double n_pairs)
-{
-    if(st.restarts_left == 0 || !(st.iter < cfg.max_iter && cfg.mse_target < st.S / n_pairs))
-        return false;
-    --st.restarts_left;
-    lm_reset_damping(st);
-    return true;
-}
-
-// In-place Cholesky of a packed 7x7 SPD matrix; false unless every pivot is
-// positive and finite.
-__device__ bool cholesky7(double* A)
-{
-    for(int j = 0; j < kParams; ++j)
-    {
-        double s = A[hidx(j, j)];
-        for(int k = 0; k < j; ++k)
-        {
-            double l = A[hidx(j, k)];
-            s -= l * l;
-        }
-        if(!(s > 0.0) || !isfinite(s))
-            return false;
-        double ljj = sqrt(s);
-        A[hidx(j, j)] = ljj;
-        double r = 1.0 / ljj;
-        for(int i = j + 1; i < kParams; ++i)
-        {
-            double t = A[hidx(i, j)];
-            for(int k = 0; k < j; ++k)
-                t -= A[hidx(i, k)] * A[hidx(j, k)];
-            A[hidx(i, j)] = t * r;
-        }
-    }
-    return true;
-}
-
-__device__ void cholesky7_solve(const double* Lm, const double* b, double* x)
-{
-    double y[kParams];
-    for(int i = 0; i < kParams; ++i)
-    {
-        double t = b[i];
-        for(int k = 0; k < i; ++k)
-            t -= Lm[hidx(i, k)] * y[k];
-        y[i] = t / Lm[hidx(i, i)];
-    }
-    for(int i = kParams - 1; i >= 0; --i)
-    {
-        double t = y[i];
-        for(int k = i + 1; k < kParams; ++k)
-            t -= Lm[hidx(k, i)] * x[k];
-        x[i] = t / Lm[hidx(i, i)];
-    }
-}
-
-// Damped step (H + lam I) d = g by Cholesky.  Active set at the bound: a
-// parameter with a lower bound (sigma, specular, diffuse) that sits exactly at 0
-// and whose step points below it is held at 0 for this solve (its row and
-// column are dropped) and the system is solved again.  The reference instead
-// rejects every such step (AcceptStepConstraints), which with an exact
-// derivative would hold the parameter at 0 for good; its finite-difference
-// derivative at exactly 0 (fitting.hh:896-905, step 1e-8) is below float
-// resolution there.  Returns false when the factorisation fails.
-__device__ bool lm_solve(LmState& st)
-{
-    uint32_t frozen = 0;
-    for(int round = 0; round < 5; ++round)
-    {
-        double A[kHessian], b[kParams];
-        for(int i = 0; i < kHessian; ++i)
-            A[i] = st.H[i];
-        for(int i = 0; i < kParams; ++i)
-        {
-            A[hidx(i, i)] += st.lam;
-            b[i] = st.g[i];
-        }
-        for(int i = 0; i < 4; ++i)
-            if(frozen & (1u << i))
-            {
-                for(int j = 0; j < kParams; ++j)
-                    if(j != i)
-                        A[hidx(i, j)] = 0.0;
-                b[i] = 0.0;
-            }
-        if(!cholesky7(A))
-            return false;
-        cholesky7_solve(A, b, st.d);
-        uint32_t more = frozen;
-        for(int i = 0; i < 4; ++i)
-            if(st.p[i] == 0.0 && st.d[i] > 0.0)
-                more |= 1u << i;
-        if(more == frozen)
-            return true;
-        frozen = more;
-    }
-    return true;
-}
-
-// The top of one LM iteration (fitting.hh:541-590): solve for a step that passes
-// the constraints, or finish.  Returns kCmdTrial (st.pt holds the trial point)
-// or kCmdDone.
-__device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
-{
-    for(;;)
-    {
-        if(!(st.iter < cfg.max_iter && cfg.mse_target < st.S / n_pairs))
-        {
-            if(st.iter >= cfg.max_iter)
-                st.status |= SVF_TEXEL_MAX_ITER;
-            return kCmdDone;
-        }
-        if(!lm_solve(st))
-        {
-            // the reference's inverse came out non-finite: damp harder
-            st.lam *= st.nu;
-            st.nu *= st.nu;
-            ++st.iter;
-            continue;
-        }
-        double step2 = 0.0, mag2 = 0.0;
-        for(int i = 0; i < kParams; ++i)
-        {
-            step2 += st.d[i] * st.d[i];
-            double t = st.p[i] + cfg.eps;
-            mag2 += t * t;
-        }
-        double step_len = sqrt(step2);
-        if(!isfinite(step_len))
-        {
-            st.status |= SVF_TEXEL_NONFINITE;
-            return kCmdDone;
-        }
-        if(step_len <= cfg.eps * (sqrt(mag2) + cfg.eps))
-        {
-            if(lm_restart(st, cfg, n_pairs))
-                continue;
-            return kCmdDone;
-        }
-        // AcceptStepConstraints (svbrdf-lsq-fitting-internal.hh:67-77)
-        bool accept = true;
-        for(int i = 0; i < 4; ++i)
-            if(st.p[i] - st.d[i] < 0.0f)
-                accept = false;
-        if(!accept)
-        {
-            st.lam *= st.nu;
-            st.nu *= st.nu;
-            ++st.iter;
-            continue;
-        }
-        for(int i = 0; i < kParams; ++i)
-            st.pt[i] = st.p[i] - st.d[i];
-        return kCmdTrial;
-    }
-}
-
-// After the trial residual (fitting.hh:597-612,661-674): accept or damp.
-__device__ int lm_after_trial(LmState& st, const LmConfig& cfg, double S1, double n_pairs)
-{
-    ++st.nres;
-    double pred = 0.0;
-    for(int i = 0; i < kParams; ++i)
-        pred += st.d[i] * (st.d[i] * st.lam + st.g[i]);
-    pred *= 0.5;
-    double rho = 0.5 * (st.S - S1) / pred;
-    if(rho > 0.0)
-    {
-        ++st.eff;
-        for(int i = 0; i < kParams; ++i)
-            st.p[i] = st.pt[i];
-        st.S = S1;
-        st.rho = rho;
-        if(S1 / n_pairs <= cfg.mse_target)
-            return kCmdDone;
-        return kCmdJacobian;
-    }
-    st.lam *= st.nu;
-    st.nu *= st.nu;
-    ++st.iter;
-    return kCmdContinue;
-}
-
-// After the Jacobian at an accepted point (fitting.hh:612-660).
-__device__ int lm_after_jacobian(LmState& st, const LmConfig& cfg, const double* red, double n_pairs)
-{
-    ++st.njac;
-    double glen = 0.0;
-    for(int i = 0; i < kParams; ++i)
-    {
-        st.g[i] = -red[kHessian + i];
-        glen += st.g[i] * st.g[i];
-    }
-    for(int i = 0; i < kHessian; ++i)
-        st.H[i] = red[i];
-    if(glen <= cfg.eps * cfg.eps)
-        return lm_restart(st, cfg, n_pairs) ? kCmdContinue : kCmdDone;
-    const double min_mul = (double)(1.0f / 3.0f);
-    double t = 2.0 * st.rho - 1.0;
-    double mul = fmax(min_mul, 1.0 - t * t * t);
-    st.lam *= mul;
-    st.nu = 2.0;
-    ++st.iter;
-    return kCmdContinue;
-}
-
-// ------------------------------------------------------------------------------
-// shared-memory layout of the LM kernel
-// ------------------------------------------------------------------------------
-
-struct LmShared
-{
-    float*  geo;     // [3][Lp]
-    float*  tab;     // [kTabFields][Lp]
-    float*  lum[2];  // [lum_stride] each
-    float*  red;     // [kWarps][kRed]
-    double* redd;    // [kWarps]
-    uint64_t* bar;   // [2]
-    uint32_t Lp;
-};
-
-__host__ __device__ inline uint32_t pad4(uint32_t x) { return (x + 3u) & ~3u; }
-
-__host__ __device__ inline size_t lm_smem_layout(uint32_t L, uint64_t lum_stride, size_t* off_tab, size_t* off_lum,
-                                                 size_t* off_red, size_t* off_redd, size_t* off_bar)
-{
-    uint32_t Lp = pad4(L);
-    size_t o = 0;
-    o += sizeof(float) * 3 * Lp;
-    *off_tab = o;
-    o += sizeof(float) * kTabFields * Lp;
-    o = (o + 127) & ~size_t(127);
-    *off_lum = o;
-    o += sizeof(float) * 2 * lum_stride;
-    o = (o + 15) & ~size_t(15);
-    *off_red = o;
-    o += sizeof(float) * kWarps * kRed;
-    o = (o + 7) & ~size_t(7);
-    *off_redd = o;
-    o += sizeof(double) * kWarps;
-    *off_bar = o;
-    o += sizeof(uint64_t) * 2;
-    return o;
-}
-
-// Tabulates DirEntry for every direction for the parameters in `pf`.
-__device__ __forceinline__ void build_table(const LmShared& sh, const float* pf, uint32_t L)
-{
-    ParamSet ps;
-    make_param_set(pf, ps);
-    for(uint32_t d = threadIdx.x; d < L; d += kThreads)
-    {
-        DirEntry e;
-        make_dir_entry(ps, sh.geo[d], sh.geo[sh.Lp + d], sh.geo[2 * sh.Lp + d], e);
-        float* t = sh.tab + d;
-        const uint32_t s = sh.Lp;
-        t[0 * s] = e.a[0];
-        t[1 * s] = e.a[1];
-        t[2 * s] = e.a[2];
-        t[3 * s] = e.sp;
-        t[4 * s] = e.dsp[0];
-        t[5 * s] = e.dsp[1];
-        t[6 * s] = e.dsp[2];
-        t[7 * s] = e.dsp[3];
-        t[8 * s] = e.dsp[4];
-        t[9 * s] = e.kdc;
-        t[10 * s] = e.kv;
-        t[11 * s] = e.up;
-    }
-}
-
-__device__ __forceinline__ void load_entry(const LmShared& sh, uint32_t d, DirEntry& e, float* w)
-{
-    const float* t = sh.tab + d;
-    const uint32_t s = sh.Lp;
-    e.a[0] = t[0 * s];
-    e.a[1] = t[1 * s];
-    e.a[2] = t[2 * s];
-    e.sp = t[3 * s];
-    e.dsp[0] = t[4 * s];
-    e.dsp[1] = t[5 * s];
-    e.dsp[2] = t[6 * s];
-    e.dsp[3] = t[7 * s];
-    e.dsp[4] = t[8 * s];
-    e.kdc = t[9 * s];
-    e.kv = t[10 * s];
-    e.up = t[11 * s];
-    w[0] = sh.geo[d];
-    w[1] = sh.geo[s + d];
-    w[2] = sh.geo[2 * s + d];
-}
-
-// One pass over the N pairs of the current texel.  Warps own views
-// (v = warp, warp + kWarps, ...), lanes own lights (chunks of 32), so a view's
-// table entry is a broadcast read and a light's entry stays in registers for
-// the whole chunk.  Jacobian passes reduce r^2, J^T J and J^T r into `out`
-// (thread 0 only); residual passes reduce r^2.
-template <bool kJacobian>
-__device__ void pair_pass(const LmShared& sh, const float* lum, const float* pf, uint32_t L, float refr,
-                          double* out)
-{
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    ParamSet ps;
-    make_param_set(pf, ps);
-    const bool fresnel_on = refr != 1.0f;
-
-    double r2 = 0.0;
-    float acc[kJacobian ? kHessian + kParams : 1];
-#pragma unroll
-    for(int i = 0; i < (kJacobian ? kHessian + kParams : 1); ++i)
-        acc[i] = 0.0f;
-
-    for(uint32_t base = 0; base < L; base += 32)
-    {
-        const uint32_t li = base + lane;
-        const bool valid = li < L;
-        DirEntry le;
-        float wi[3];
-        load_entry(sh, valid ? li : 0, le, wi);
-        for(uint32_t v = warp; v < L; v += kWarps)
-        {
-            DirEntry ve;
-            float wo[3];
-            load_entry(sh, v, ve, wo);
-            if(!valid)
-                continue;
-            const float y = lum[v * L + li];
-            const float F = fresnel_on ? fresnel_factor(refr, wi, wo) : 1.0f;
-            float J[kParams];
-            const float f = eval_pair<kJacobian>(ps, wi, le, wo, ve, F, J);
-            const float r = y - f;
-            r2 = fma((double)r, (double)r, r2);
-            if(kJacobian)
-            {
-                int k = 0;
-#pragma unroll
-                for(int a = 0; a < kParams; ++a)
-                {
-#pragma unroll
-                    for(int b = a; b < kParams; ++b)
-                    {
-                        acc[k] = fmaf(J[a], J[b], acc[k]);
-                        ++k;
-                    }
-                }
-#pragma unroll
-                for(int a = 0; a < kParams; ++a)
-                    acc[kHessian + a] = fmaf(J[a], r, acc[kHessian + a]);
-            }
-        }
-    }
-
-    // warp reduction, then across warps in FP64
-#pragma unroll
-    for(int o = 16; o > 0; o >>= 1)
-        r2 += __shfl_xor_sync(0xffffffffu, r2, o);
-    if(kJacobian)
-    {
-#pragma unroll
-        for(int i = 0; i < kHessian + kParams; ++i)
-        {
-            float x = acc[i];
-#pragma unroll
-            for(int o = 16; o > 0; o >>= 1)
-                x += __shfl_xor_sync(0xffffffffu, x, o);
-            acc[i] = x;
-        }
-    }
-    if(lane == 0)
-    {
-        sh.redd[warp] = r2;
-        if(kJacobian)
-            for(int i = 0; i < kHessian + kParams; ++i)
-                sh.red[warp * kRed + i] = acc[i];
-    }
-    __syncthreads();
-    if(threadIdx.x == 0)
-    {
-        double s = 0.0;
-        for(int w = 0; w < kWarps; ++w)
-            s += sh.redd[w];
-        out[kHessian + kParams] = s;
-        if(kJacobian)
-            for(int i = 0; i < kHessian + kParams; ++i)
-            {
-                double t = 0.0;
-                for(int w = 0; w < kWarps; ++w)
-                    t += (double)sh.red[w * kRed + i];
-                out[i] = t;
-            }
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) lm_fit_kernel(LmArgs args)
-{
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    size_t off_tab, off_lum, off_red, off_redd, off_bar;
-    lm_smem_layout(args.L, args.lum_stride, &off_tab, &off_lum, &off_red, &off_redd, &off_bar);
-    LmShared sh;
-    sh.Lp = pad4(args.L);
-    sh.geo = reinterpret_cast<float*>(smem_raw);
-    sh.tab = reinterpret_cast<float*>(smem_raw + off_tab);
-    sh.lum[0] = reinterpret_cast<float*>(smem_raw + off_lum);
-    sh.lum[1] = sh.lum[0] + args.lum_stride;
-    sh.red = reinterpret_cast<float*>(smem_raw + off_red);
-    sh.redd = reinterpret_cast<double*>(smem_raw + off_redd);
-    sh.bar = reinterpret_cast<uint64_t*>(smem_raw + off_bar);
-
-    __shared__ float sh_pf[kParams];
-    __shared__ int sh_cmd;
-    __shared__ uint32_t sh_next;
-    __shared__ double sh_red_out[kHessian + kParams + 1];
-
-    const uint32_t L = args.L, N = args.N;
-    const uint32_t slab_bytes = (uint32_t)(args.lum_stride * sizeof(float));
-    for(uint32_t i = threadIdx.x; i < 3 * sh.Lp; i += kThreads)
-    {
-        uint32_t c = i / sh.Lp, d = i % sh.Lp;
-        sh.geo[i] = d < L ? args.geo[c * L + d] : 0.0f;
-    }
-    if(threadIdx.x == 0)
-    {
-        mbar_init(&sh.bar[0], 1);
-        mbar_init(&sh.bar[1], 1);
-        fence_barrier_init();
-        uint32_t t0 = atomicAdd(args.work_counter, 1u);
-        if(t0 < args.texels)
-            bulk_load(sh.lum[0], args.lum + (uint64_t)t0 * args.lum_stride, slab_bytes, &sh.bar[0]);
-        sh_next = t0;
-    }
-    __syncthreads();
-
-    uint32_t t = sh_next;
-    uint32_t buf = 0;
-    uint32_t phase[2] = { 0u, 0u };
-    const double n_pairs = (double)N;
-    LmState st;   // meaningful in thread 0 only
-
-    while(t < args.texels)
-    {
-        __syncthreads();   // everyone has read sh_next
-        if(threadIdx.x == 0)
-        {
-            uint32_t tn = atomicAdd(args.work_counter, 1u);
-            if(tn < args.texels)
-            {
-                fence_proxy_async();
-                bulk_load(sh.lum[buf ^ 1u], args.lum + (uint64_t)tn * args.lum_stride, slab_bytes, &sh.bar[buf ^ 1u]);
-            }
-            sh_next = tn;
-        }
-        const bool arrived = mbar_wait(&sh.bar[buf], phase[buf]);
-        phase[buf] ^= 1u;
-        if(!arrived)
-        {
-            // The copy did not land within the bound: flag it, give the copies in
-            // flight one more bounded wait, and leave.
-            if(threadIdx.x == 0)
-            {
-                atomicOr(args.error_flag, 1u);
-                if(args.stats)
-                    args.stats[t].status = SVF_TEXEL_TIMEOUT;
-            }
-            mbar_wait(&sh.bar[buf], phase[buf] ^ 1u);
-            mbar_wait(&sh.bar[buf ^ 1u], phase[buf ^ 1u]);
-            return;
-        }
-        const float* lum = sh.lum[buf];
-
-        // ---- fit texel t ----
-        if(threadIdx.x == 0)
-        {
-            for(int i = 0; i < kParams; ++i)
-            {
-                st.p[i] = (double)args.init[(uint64_t)t * kParams + i];
-                sh_pf[i] = (float)st.p[i];
-            }
-            st.iter = st.eff = st.njac = st.nres = st.status = 0;
-        }
-        __syncthreads();
-        build_table(sh, sh_pf, L);
-        __syncthreads();
-        pair_pass<true>(sh, lum, sh_pf, L, args.cfg.fresnel, sh_red_out);
-        if(threadIdx.x == 0)
-        {
-            st.njac = 1;
-            st.restarts_left = args.cfg.restarts;
-            st.S = sh_red_out[kHessian + kParams];
-            for(int i = 0; i < kParams; ++i)
-                st.g[i] = -sh_red_out[kHessian + i];
-            for(int i = 0; i < kHessian; ++i)
-                st.H[i] = sh_red_out[i];
-            lm_reset_damping(st);
-            if(!isfinite(st.S))
-                st.status |= SVF_TEXEL_NONFINITE;
-        }
-        for(;;)
-        {
-            if(threadIdx.x == 0)
-            {
-                int cmd = lm_next(st, args.cfg, n_pairs);
-                if(cmd == kCmdTrial)
-                    for(int i = 0; i < kParams; ++i)
-                        sh_pf[i] = (float)st.pt[i];
-                sh_cmd = cmd;
-            }
-            __syncthreads();
-            if(sh_cmd == kCmdDone)
-                break;
-            build_table(sh, sh_pf, L);
-            __syncthreads();
-            pair_pass<false>(sh, lum, sh_pf, L, args.cfg.fresnel, sh_red_out);
-            if(threadIdx.x == 0)
-                sh_cmd = lm_after_trial(st, args.cfg, sh_red_out[kHessian + kParams], n_pairs);
-            __syncthreads();
-            const int cmd = sh_cmd;
-            if(cmd == kCmdDone)
-                break;
-            if(cmd == kCmdJacobian)
-            {
-                // the table built for the trial point is the accepted point's
-                pair_pass<true>(sh, lum, sh_pf, L, args.cfg.fresnel, sh_red_out);
-                if(threadIdx.x == 0)
-                    sh_cmd = lm_after_jacobian(st, args.cfg, sh_red_out, n_pairs);
-                __syncthreads();
-                if(sh_cmd == kCmdDone)
-                    break;
-            }
-        }
-
-        // ---- outputs (LeastSquaresFitSGGX :381-429, SVBRDFFitPipeline::fit :692-697) ----
-        if(threadIdx.x == 0)
-        {
-            float pout[kParams];
-            for(int i = 0; i < kParams; ++i)
-            {
-                pout[i] = (float)st.p[i];
-                args.out[(uint64_t)t * kParams + i] = pout[i];
-            }
-            double mse = st.S / n_pairs;
-            if(!isfinite(mse))
-                st.status |= SVF_TEXEL_NONFINITE;
-            args.rmse[t] = (float)sqrt(mse);
-            if(args.stats)
-            {
-                svf_texel_stats s;
-                s.iterations = st.iter;
-                s.effective = st.eff;
-                s.jacobians = st.njac;
-                s.residuals = st.nres;
-                s.status = st.status;
-                args.stats[t] = s;
-            }
-            if(args.map_sigma)
-            {
-                args.map_sigma[2 * (uint64_t)t] = pout[0];
-                args.map_sigma[2 * (uint64_t)t + 1] = pout[1];
-            }
-            if(args.map_basis)
-            {
-                // ToQuaternion(euler), quaternion.hh:82-94
-                float s1, c1, s2, c2, s3, c3;
-                sincosf(0.5f * pout[4], &s1, &c1);
-                sincosf(0.5f * pout[5], &s2, &c2);
-                sincosf(0.5f * pout[6], &s3, &c3);
-                float* q = args.map_basis + 4 * (uint64_t)t;
-                q[0] = s1 * c2 * c3 + c1 * s2 * s3;
-                q[1] = -s1 * c2 * s3 + c1 * s2 * c3;
-                q[2] = c1 * c2 * s3 + s1 * s2 * c3;
-                q[3] = c1 * c2 * c3 - s1 * s2 * s3;
-            }
-            if(args.avg_chroma && (args.map_diffuse || args.map_specular))
-            {
-                const float* a = args.avg_chroma + 3 * (uint64_t)t;
-                for(int c = 0; c < 3; ++c)
-                {
-                    if(args.map_diffuse)
-                        args.map_diffuse[3 * (uint64_t)t + c] = a[c] * pout[3];
-                    if(args.map_specular)
-                        args.map_specular[3 * (uint64_t)t + c] = a[c] * pout[2];
-                }
-            }
-        }
-        __syncthreads();
-        t = sh_next;
-        buf ^= 1u;
-    }
-}
 
 // ------------------------------------------------------------------------------
 // luminance slice
@@ -730,7 +34,9 @@ __device__ __forceinline__ float to_f<__half>(__half x) { return __half2float(x)
 // chromaticity rgb/lum, or (1,1,1) when lum <= 1e-6, averaged over the pairs.
 template <typename T>
 __global__ void __launch_bounds__(256) luminance_kernel(const T* __restrict__ samples, uint32_t N, float* __restrict__ lum,
-                                                         uint64_t lum_stride, float* __restrict__ avg)
+                                                         uint64_t lum_stride, float* __restrict__ avg,
+                                                         __nv_bfloat16* __restrict__ lum_hi,
+                                                         __nv_bfloat16* __restrict__ lum_lo)
 {
     const uint64_t t = blockIdx.x;
     const T* src = samples + t * (uint64_t)N * 3;
@@ -741,6 +47,13 @@ __global__ void __launch_bounds__(256) luminance_kernel(const T* __restrict__ sa
         float r = to_f(src[3 * i]), g = to_f(src[3 * i + 1]), b = to_f(src[3 * i + 2]);
         float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
         dst[i] = l;
+        if(lum_hi)
+        {
+            // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
+            const __nv_bfloat16 h = __float2bfloat16_rn(l);
+            lum_hi[t * lum_stride + i] = h;
+            lum_lo[t * lum_stride + i] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
+        }
         if(l > 1e-6f)
         {
             float rl = 1.0f / l;
@@ -1120,54 +433,33 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
     a.cfg = cfg;
     a.work_counter = flags;
     a.error_flag = flags + 1;
-    const int per_sm = lm_max_ctas_per_sm(L, stride);
+    const LmKernelChoice choice = lm_default_choice(L);
+    const int per_sm = lm_max_ctas_per_sm(L, stride, choice);
     if(per_sm <= 0)
         return cudaErrorInvalidConfiguration;
     const uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * sms, texels);
-    if((e = launch_lm_fit(a, (int)std::max<uint64_t>(grid, 1), stream)) != cudaSuccess)
+    if((e = launch_lm_fit(a, choice, (int)std::max<uint64_t>(grid, 1), stream)) != cudaSuccess)
         return e;
     if((e = cudaMemcpyAsync(error_flag, flags + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
         return e;
     return cudaStreamSynchronize(stream);
 }
 
-size_t lm_smem_bytes(uint32_t L, uint64_t lum_stride)
-{
-    size_t a, b, c, d, e;
-    return lm_smem_layout(L, lum_stride, &a, &b, &c, &d, &e);
-}
-
-int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride)
-{
-    int n = 0;
-    size_t smem = lm_smem_bytes(L, lum_stride);
-    cudaFuncSetAttribute(lm_fit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, lm_fit_kernel, kThreads, smem) != cudaSuccess)
-        return 0;
-    return n;
-}
-
-cudaError_t launch_lm_fit(const LmArgs& args, int grid, cudaStream_t stream)
-{
-    size_t smem = lm_smem_bytes(args.L, args.lum_stride);
-    cudaError_t e = cudaFuncSetAttribute(lm_fit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if(e != cudaSuccess)
-        return e;
-    lm_fit_kernel<<<grid, kThreads, smem, stream>>>(args);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N, float* lum,
-                             uint64_t lum_stride, float* avg, cudaStream_t stream)
+                             uint64_t lum_stride, float* avg, void* lum_hi, void* lum_lo, cudaStream_t stream)
 {
     if(texels == 0)
         return cudaSuccess;
+    if((lum_hi == nullptr) != (lum_lo == nullptr))
+        return cudaErrorInvalidValue;
+    __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(lum_hi);
+    __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(lum_lo);
     if(sample_type == SVF_SAMPLES_F16)
         luminance_kernel<__half><<<(unsigned)texels, 256, 0, stream>>>(static_cast<const __half*>(samples), N, lum,
-                                                                     lum_stride, avg);
+                                                                     lum_stride, avg, hi, lo);
     else
         luminance_kernel<float><<<(unsigned)texels, 256, 0, stream>>>(static_cast<const float*>(samples), N, lum,
-                                                                    lum_stride, avg);
+                                                                    lum_stride, avg, hi, lo);
     return cudaGetLastError();
 }
 
