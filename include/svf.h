@@ -239,7 +239,7 @@ typedef struct svf_run_stats
     double   ms_fit;            /* Levenberg-Marquardt */
     double   ms_copy;           /* host<->device staging, when host buffers were given */
     uint32_t lm_threads;        /* LM kernel configuration the autotuner chose: CTA size */
-    uint32_t lm_chunks;         /* and 32-light chunks held in registers per lane */
+    uint32_t lm_slots;          /* and texels in flight per CTA */
 } svf_run_stats;
 
 svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,

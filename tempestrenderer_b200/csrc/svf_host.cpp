@@ -406,7 +406,8 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
         return SVF_OK;
     }
     const uint32_t L = lay->L, N = L * L;
-    const uint64_t stride = round_up(N, 8), T = 2048;
+    // enough texels to keep every slot of every resident CTA busy for a while
+    const uint64_t stride = round_up(N, 8), T = 8192;
     DevBuf samples, truth, lum, avg, init, out, rmse, stats;
     SVF_TRY(samples.ensure(sizeof(float) * 3 * N * T));
     SVF_TRY(truth.ensure(sizeof(float) * 16 * T));
@@ -445,12 +446,25 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
     // warm-up (module load, attribute set-up) on a small slice
     LmRun warm = r;
     warm.texels = 256;
+    // candidates that do not fit on an SM (shared memory at large L) drop out
+    int n_fit = 0;
     for(int c = 0; c < n_cand; ++c)
+        if(svf::lm_max_ctas_per_sm(L, stride, cand[c]) > 0)
+            cand[n_fit++] = cand[c];
+    if(n_fit == 0)
+        return fail(SVF_EINVAL, "no LM kernel configuration fits on an SM for L = %u", L);
+    lay->choice = cand[0];
+    if(n_fit == 1)
+    {
+        lay->tuned = true;
+        return SVF_OK;
+    }
+    for(int c = 0; c < n_fit; ++c)
         SVF_TRY(launch_lm(ctx, lay, o, warm, cand[c]));
     double best_rate = 0.0, first_rate = 0.0;
     int best = 0;
     std::vector<svf_texel_stats> st(T);
-    for(int c = 0; c < n_cand; ++c)
+    for(int c = 0; c < n_fit; ++c)
     {
         SVF_CUDA(cudaEventRecord(ctx->ev[6], ctx->stream));
         SVF_TRY(launch_lm(ctx, lay, o, r, cand[c]));
@@ -465,8 +479,8 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
             flops += (double)N * (169.0 * s.jacobians + 33.0 * s.residuals);
         const double rate = flops / std::max(1e-3, (double)ms);
         if(getenv("SVF_DEBUG"))
-            fprintf(stderr, "svf: LM tune L=%u threads=%d chunks=%d: %.3f ms, %.2f TFLOP/s (model)\n", L,
-                    cand[c].threads, cand[c].nc, ms, rate * 1e-9);
+            fprintf(stderr, "svf: LM tune L=%u threads=%d slots=%d: %.3f ms, %.2f TFLOP/s (model)\n", L,
+                    cand[c].threads, cand[c].slots, ms, rate * 1e-9);
         if(c == 0)
             first_rate = rate;
         if(rate > best_rate)
@@ -904,7 +918,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     rs.texels = T;
     const svf::LmKernelChoice used = lay->tuned ? lay->choice : svf::lm_default_choice(L);
     rs.lm_threads = (uint32_t)used.threads;
-    rs.lm_chunks = (uint32_t)used.nc;
+    rs.lm_slots = (uint32_t)used.slots;
     if(run)
         *run = rs;
     if(rs.failed_texels)

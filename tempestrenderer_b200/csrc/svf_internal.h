@@ -41,12 +41,12 @@ struct LmArgs
     uint32_t* error_flag;      // set non-zero by a bounded wait that expired
 };
 
-// LM kernel configuration (svf_lm.cu): CTA size and the number of 32-light
-// chunks each lane keeps in registers (>= ceil(L/32)).
+// LM kernel configuration (svf_lm.cu): CTA size (one control warp + pair
+// workers) and the texel slots each CTA keeps in flight.
 struct LmKernelChoice
 {
     int threads;
-    int nc;
+    int slots;
 };
 LmKernelChoice lm_default_choice(uint32_t L);
 int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);

@@ -4,22 +4,33 @@
 //
 // Work distribution: a persistent grid of (resident CTAs per SM) x (SMs) CTAs
 // pulls texels from a global atomic counter (work stealing: a texel that
-// converges early frees its CTA at once).  A CTA fits one texel at a time.
-// Small CTAs (64-256 threads) keep several texels in flight per SM, so that the
-// serial FP64 step of one texel overlaps the pair passes of the others.
+// converges early frees its slot at once).  Each CTA is warp-specialised and
+// keeps S texels ("slots") in flight:
 //
-// Per texel: its luminance slab is staged into shared memory by one bulk TMA
-// copy (cp.async.bulk, completion on an mbarrier, bounded wait); the next
-// texel's copy is issued as soon as the current fit stops reading its slab.
-// Per LM evaluation the CTA tabulates the direction-only terms of the model
-// (svf_model.cuh) for the L directions, 16 floats per direction; then each warp
-// walks its views and each lane keeps the table entries of its NC lights in
-// registers, so a view's entry is four broadcast 16-byte loads used for NC
-// pairs.  Jacobian passes accumulate the packed J^T J and J^T r in FP32 per
-// thread and r^2 in FP64, reduced with warp shuffles and summed across warps
-// in FP64.  One thread runs the LM control in FP64 (state in shared memory):
-// the damped normal equations by Cholesky, the small-step and gradient tests
-// and the gain-ratio accept/reject.
+//   warp 0, the control warp: per slot, the FP64 LM control (thread 0; state in
+//     shared memory), the cross-warp FP64 sums of the pass results, the
+//     direction table for the next evaluation (all 32 lanes), the texel's
+//     outputs and the bulk TMA copy (cp.async.bulk, mbarrier, bounded wait) of
+//     the next texel's luminance slab into the slot;
+//   warps 1..NW, the pair workers: the pair passes of slot 0, 1, .., S-1, 0, ..
+//     in turn.
+//
+// Named barriers hand each slot back and forth: READY[s] (control -> workers:
+// the command, table and constants of slot s are in place) and DONE[s]
+// (workers -> control: the per-warp partial sums are written).  While the
+// control warp solves the damped normal equations of one slot, the workers
+// evaluate another slot's pairs, so the serial FP64 work is off the pair
+// throughput's critical path.
+//
+// A pass evaluates nothing per pair that depends on one direction only: the
+// table (svf_model.cuh) holds 12 floats per direction.  The workers walk the
+// L (L + 1) / 2 unordered direction pairs, one per lane, and evaluate the
+// specular core once for both ordered pairs (sym_pair).  Jacobian passes
+// accumulate the packed J^T J and J^T r in FP32 per lane and r^2 in FP64,
+// reduce them within the warp (reduce-scatter), and the control warp sums the
+// warps in FP64.  The LM control follows fitting.hh: the damped normal
+// equations by Cholesky, the small-step and gradient tests and the gain-ratio
+// accept/reject.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -34,7 +45,7 @@ namespace svf
 namespace
 {
 
-constexpr int kEntry = 16;                   // floats per direction-table entry
+constexpr int kEntry = 12;                   // floats per direction-table entry
 constexpr int kRed = kHessian + kParams;     // FP32 partial sums per thread (J^T J, J^T r)
 constexpr uint32_t kWaitSpins = 1u << 22;    // bound of every mbarrier wait
 
@@ -335,10 +346,10 @@ __device__ int lm_after_jacobian(LmState& st, const LmConfig& cfg, const double*
 }
 
 // ------------------------------------------------------------------------------
-// shared memory and the direction table
+// direction table and pair evaluation
 // ------------------------------------------------------------------------------
 
-// Per-texel-evaluation constants shared by every pair.
+// Per-evaluation constants shared by every pair.
 struct PassConst
 {
     float u, v, rsx, rsy, ks, kd, ks_on, kd_on;
@@ -347,30 +358,16 @@ struct PassConst
 
 __host__ __device__ inline uint32_t pad4(uint32_t x) { return (x + 3u) & ~3u; }
 
-template <int THREADS>
-struct Smem
-{
-    static constexpr int kWarps = THREADS / 32;
-    // [Lp][kEntry] direction table | [stride] slab | partials | state
-    __host__ __device__ static size_t tab_bytes(uint32_t L) { return sizeof(float) * kEntry * pad4(L); }
-    __host__ __device__ static size_t slab_offset(uint32_t L) { return (tab_bytes(L) + 127) & ~size_t(127); }
-    __host__ __device__ static size_t red_offset(uint32_t L, uint64_t stride)
-    {
-        return (slab_offset(L) + sizeof(float) * stride + 15) & ~size_t(15);
-    }
-    __host__ __device__ static size_t bytes(uint32_t L, uint64_t stride)
-    {
-        return red_offset(L, stride) + sizeof(float) * kWarps * kRed + sizeof(double) * kWarps;
-    }
-};
-
-// Entry layout (16 floats): a0 a1 a2 sp | dsp0..3 | dsp4 kv up kdc | w0 w1 w2 0
+// Entry layout (12 floats): a0 a1 a2 sp | dsp0..3 | dsp4 kv up kdc.  The
+// directions themselves are not kept: R is orthonormal, so |w_i + w_o| = |s|
+// and cos(h, w_i) = s.a_i / |s| with s = a_i + a_o.  Built by the 32 lanes of
+// the control warp.
 __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32_t L, const float* pf, PassConst* pc,
-                                            int threads)
+                                            uint32_t lane)
 {
     ParamSet ps;
     make_param_set(pf, ps);
-    for(uint32_t d = threadIdx.x; d < L; d += threads)
+    for(uint32_t d = lane; d < L; d += 32)
     {
         const float wx = geo[d], wy = geo[L + d], wz = geo[2 * L + d];
         DirEntry e;
@@ -379,9 +376,8 @@ __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32
         t[0] = make_float4(e.a[0], e.a[1], e.a[2], e.sp);
         t[1] = make_float4(e.dsp[0], e.dsp[1], e.dsp[2], e.dsp[3]);
         t[2] = make_float4(e.dsp[4], ps.kspec * e.kv, e.up, e.kdc);
-        t[3] = make_float4(wx, wy, wz, 0.0f);
     }
-    if(threadIdx.x == 0)
+    if(lane == 0)
     {
         pc->u = ps.u;
         pc->v = ps.v;
@@ -401,406 +397,632 @@ __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32
 
 struct Entry
 {
-    float a0, a1, a2, sp, d0, d1, d2, d3, d4, kv, up, kdc, w0, w1, w2;
+    float a0, a1, a2, sp, d0, d1, d2, d3, d4, kv, up, kdc;
 };
+
+// MUFU reciprocal (about 1 ulp); the pair terms need no correctly rounded divide.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 __device__ __forceinline__ Entry load_entry(const float* tab, uint32_t d)
 {
     const float4* t = reinterpret_cast<const float4*>(tab + kEntry * d);
-    const float4 x = t[0], y = t[1], z = t[2], w = t[3];
-    return Entry{ x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w, z.x, z.y, z.z, z.w, w.x, w.y, w.z };
+    const float4 x = t[0], y = t[1], z = t[2];
+    return Entry{ x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w, z.x, z.y, z.z, z.w };
 }
 
-// One pair: residual r = y - f and, for Jacobian passes, the gradient J of f
-// (the factored model of svf_model.cuh with the per-view lobe constant folded
-// into vo.kv).
-template <bool kJac>
-__device__ __forceinline__ float pair_eval(const PassConst& c, const Entry& li, const Entry& vo, float F, float y,
-                                           float* J)
+// Warp reduce-scatter of 32 values: on return v[0] of lane j holds the warp's
+// sum of v[j] (recursive halving: 31 shuffles instead of 32 x 5).
+__device__ __forceinline__ void reduce_scatter32(float* v, uint32_t lane)
 {
-    const float W0 = li.w0 + vo.w0, W1 = li.w1 + vo.w1, W2 = li.w2 + vo.w2;
-    const float g = W0 * W0 + W1 * W1 + W2 * W2;
-    const float s0 = li.a0 + vo.a0, s1 = li.a1 + vo.a1, s2 = li.a2 + vo.a2;
-    const float q0 = s0 * s0, q1 = s1 * s1;
-    const float Q = c.u * q0 + c.v * q1 + s2 * s2;
-    const float S = li.sp + vo.sp;
-    const float QQS = Q * Q * S;
-    const float rden = QQS > 0.0f ? __frcp_rn(QQS) : 0.0f;
-    const float spec = vo.kv * li.up * F * g * g * rden;
-    const float f = vo.up * (c.kd * li.kdc) + c.ks * spec;
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+    {
+        const bool upper = (lane & (uint32_t)o) != 0;
+#pragma unroll
+        for(int i = 0; i < o; ++i)
+        {
+            const float send = upper ? v[i] : v[i + o];
+            const float keep = upper ? v[i + o] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+}
+
+__device__ __forceinline__ float warp_sum(float x)
+{
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+__device__ __forceinline__ double warp_sum(double x)
+{
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+        x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
+}
+
+// Symmetric pair evaluation.  For the two ordered pairs of one unordered pair
+// {a, b} (light b seen from view a, and light a seen from view b) the
+// specular core is the same: s = a_a + a_b, Q, S = sp_a + sp_b, g = |s|^2 and
+// the Fresnel factor (cos(h, w_i) = cos(h, w_o)) do not depend on which
+// direction is the light, nor do their parameter derivatives.  With
+// C = F g^2 / (Q^2 S) and G the derivative factors,
+//
+//   spec_io = w_io C,                      w_io = kspec kv_o up_i
+//   f_io    = kd h_io + ks spec_io,        h_io = up_o kdc_i
+//   J_io    = spec_io V + kd_on h_io e_kd, V = (ks G_sx, ks G_sy, ks_on, 0, ks G_e0, ks G_e1, ks G_e2)
+//
+// so J^T J and J^T r of both ordered pairs take P = spec_1^2 + spec_2^2 times
+// V V^T plus rank-one terms in e_kd, and the core is evaluated once per
+// unordered pair.  On the diagonal (a = b) the second ordered pair has zero
+// weights.
+//
+// Enumeration: unordered pair f -> offset d = f / L, view a = f mod L,
+// light b = (a + d) mod L, for d = 0 .. L/2; for even L the offset L/2 is
+// taken only for a < L/2.  Consecutive lanes take consecutive f, so their
+// table entries fall in distinct shared-memory banks.
+template <bool kJac, bool kFresnel>
+__device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, const Entry& eb, float refr, float y1,
+                                         float y2, float wt1, float wt2, float* acc, double& r2)
+{
+    const float s0 = ea.a0 + eb.a0, s1 = ea.a1 + eb.a1, s2 = ea.a2 + eb.a2;
+    const float q0 = s0 * s0, q1 = s1 * s1, q2 = s2 * s2;
+    const float g = q0 + q1 + q2;   // |w_a + w_b|^2
+    const float Q = c.u * q0 + c.v * q1 + q2;
+    const float S = ea.sp + eb.sp;
+    const float QQ = Q * Q;
+    const float QQS = QQ * S;
+    // (below the normal range the lobe is treated as vanishing, as at 0)
+    const float rden = QQS > 1e-37f ? rcp_approx(QQS) : 0.0f;
+    float F = 1.0f;
+    if(kFresnel)
+    {
+        const float wa[3] = { ea.a0, ea.a1, ea.a2 }, wb[3] = { eb.a0, eb.a1, eb.a2 };
+        F = fresnel_factor(refr, wb, wa);
+    }
+    const float C = F * g * g * rden;
+    // ordered pair 1: view a, light b; ordered pair 2: view b, light a
+    const float w1 = wt1 * ea.kv * eb.up, w2 = wt2 * eb.kv * ea.up;
+    const float h1 = wt1 * ea.up * eb.kdc, h2 = wt2 * eb.up * ea.kdc;
+    const float sp1 = w1 * C, sp2 = w2 * C;
+    const float r1 = y1 - (c.kd * h1 + c.ks * sp1);
+    const float r2b = y2 - (c.kd * h2 + c.ks * sp2);
+    r2 = fma((double)r1, (double)r1, r2);
+    r2 = fma((double)r2b, (double)r2b, r2);
     if(kJac)
     {
-        const float A = c.ks * spec;
-        const float rQ = Q * S * rden;
-        const float rS = Q * Q * rden;
+        const float rQ = Q * S * rden;   // 1/Q
+        const float rS = QQ * rden;      // 1/S
         const float t0 = s1 * s2 * (c.v - 1.0f);
         const float t1 = s0 * s2 * (1.0f - c.u);
         const float t2 = s0 * s1 * (c.u - c.v);
-        J[0] = A * (c.rsx * (4.0f * c.u * q0 * rQ - 1.0f) - (li.d0 + vo.d0) * rS);
-        J[1] = A * (c.rsy * (4.0f * c.v * q1 * rQ - 1.0f) - (li.d1 + vo.d1) * rS);
-        J[2] = c.ks_on * spec;
-        J[3] = c.kd_on * vo.up * li.kdc;
+        float V[kParams];
+        V[0] = c.ks * (c.rsx * (4.0f * c.u * q0 * rQ - 1.0f) - (ea.d0 + eb.d0) * rS);
+        V[1] = c.ks * (c.rsy * (4.0f * c.v * q1 * rQ - 1.0f) - (ea.d1 + eb.d1) * rS);
+        V[2] = c.ks_on;
+        V[3] = 0.0f;
         const float m4 = -4.0f * rQ;
-        const float dd[3] = { li.d2 + vo.d2, li.d3 + vo.d3, li.d4 + vo.d4 };
+        const float dd[3] = { ea.d2 + eb.d2, ea.d3 + eb.d3, ea.d4 + eb.d4 };
 #pragma unroll
         for(int k = 0; k < 3; ++k)
         {
             const float dq = c.om[3 * k] * t0 + c.om[3 * k + 1] * t1 + c.om[3 * k + 2] * t2;
-            J[4 + k] = A * (m4 * dq - dd[k] * rS);
+            V[4 + k] = c.ks * (m4 * dq - dd[k] * rS);
+        }
+        const float P = sp1 * sp1 + sp2 * sp2;
+        const float X = c.kd_on * (sp1 * h1 + sp2 * h2);
+        const float Z = c.kd_on * (h1 * h1 + h2 * h2);
+        const float R = sp1 * r1 + sp2 * r2b;
+        const float U = c.kd_on * (h1 * r1 + h2 * r2b);
+        float PV[kParams];
+#pragma unroll
+        for(int i = 0; i < kParams; ++i)
+            PV[i] = P * V[i];
+        int n = 0;
+#pragma unroll
+        for(int i = 0; i < kParams; ++i)
+#pragma unroll
+            for(int j = i; j < kParams; ++j)
+            {
+                if(i == 3 && j == 3)
+                    acc[n] += Z;
+                else if(i == 3)
+                    acc[n] = fmaf(X, V[j], acc[n]);
+                else if(j == 3)
+                    acc[n] = fmaf(X, V[i], acc[n]);
+                else
+                    acc[n] = fmaf(PV[i], V[j], acc[n]);
+                ++n;
+            }
+#pragma unroll
+        for(int i = 0; i < kParams; ++i)
+        {
+            if(i == 3)
+                acc[kHessian + i] += U;
+            else
+                acc[kHessian + i] = fmaf(R, V[i], acc[kHessian + i]);
         }
     }
-    return y - f;
 }
 
-// One pass over the N pairs of the current texel; thread 0 receives the sums
-// (J^T J, J^T r in out[0..34] for Jacobian passes; r^2 in out[35]).
-template <int THREADS, int NC, bool kJac>
-__device__ void pair_pass(const float* tab, const PassConst& c, const float* slab, uint32_t L, float refr, float* red,
-                          double* redd, double* out)
+// One worker warp's share of a pass over the pairs of a slot (unordered pairs
+// wtid, wtid + 32 NW, ...).  Writes the warp's partial sums: J^T J and J^T r
+// (Jacobian passes) to red[wwarp][0..34] and r^2 to redd[wwarp].  Every lane
+// runs the same number of iterations; slots past the enumeration and the
+// repeated offset of an even L carry zero weights and y = 0, so they add
+// exactly 0.
+template <int NW, bool kJac, bool kFresnel>
+__device__ void worker_pass(const float* tab, const PassConst& c, const float* slab, uint32_t L, float refr,
+                            float* red, double* redd, uint32_t wwarp, uint32_t lane)
 {
-    constexpr int kWarps = THREADS / 32;
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const bool fresnel_on = refr != 1.0f;
+    static_assert(kRed == 35, "reduction layout: 32 reduce-scattered sums + 3");
+    constexpr uint32_t kStride = 32u * NW;
+    const uint32_t half = L >> 1;
+    const uint32_t total = L * (half + 1);
+    const uint32_t iters = (total + kStride - 1) / kStride;
+    const uint32_t sd = kStride / L, sv = kStride - sd * L;
+    uint32_t f = wwarp * 32u + lane;
+    uint32_t d = f / L, a = f - d * L;
 
-    Entry le[NC];
-    bool lv[NC];
-#pragma unroll
-    for(int k = 0; k < NC; ++k)
-    {
-        const uint32_t li = 32u * k + lane;
-        lv[k] = li < L;
-        le[k] = load_entry(tab, lv[k] ? li : 0u);
-    }
     double r2 = 0.0;
     float acc[kJac ? kRed : 1];
 #pragma unroll
     for(int i = 0; i < (kJac ? kRed : 1); ++i)
         acc[i] = 0.0f;
 
-    for(uint32_t v = warp; v < L; v += kWarps)
+    for(uint32_t it = 0; it < iters; ++it)
     {
-        const Entry vo = load_entry(tab, v);
-        const float* row = slab + v * L + lane;
-#pragma unroll
-        for(int k = 0; k < NC; ++k)
+        const bool valid = f < total && !(2u * d == L && a >= half);
+        uint32_t b = a + d;
+        b = b >= L ? b - L : b;
+        const uint32_t ia = valid ? a : 0u, ib = valid ? b : 0u;
+        const Entry ea = load_entry(tab, ia);
+        const Entry eb = load_entry(tab, ib);
+        // pair 1: view a, light b (slab row a); pair 2: view b, light a
+        const float y1 = valid ? slab[ia * L + ib] : 0.0f;
+        const bool two = valid && d != 0u;
+        const float y2 = two ? slab[ib * L + ia] : 0.0f;
+        sym_pair<kJac, kFresnel>(c, ea, eb, refr, y1, y2, valid ? 1.0f : 0.0f, two ? 1.0f : 0.0f, acc, r2);
+        f += kStride;
+        a += sv;
+        d += sd;
+        if(a >= L)
         {
-            if(!lv[k])
-                continue;
-            const float y = row[32 * k];
-            float F = 1.0f;
-            if(fresnel_on)
-            {
-                const float wi[3] = { le[k].w0, le[k].w1, le[k].w2 }, wo[3] = { vo.w0, vo.w1, vo.w2 };
-                F = fresnel_factor(refr, wi, wo);
-            }
-            float J[kParams];
-            const float r = pair_eval<kJac>(c, le[k], vo, F, y, J);
-            r2 = fma((double)r, (double)r, r2);
-            if(kJac)
-            {
-                int n = 0;
-#pragma unroll
-                for(int a = 0; a < kParams; ++a)
-#pragma unroll
-                    for(int b = a; b < kParams; ++b)
-                    {
-                        acc[n] = fmaf(J[a], J[b], acc[n]);
-                        ++n;
-                    }
-#pragma unroll
-                for(int a = 0; a < kParams; ++a)
-                    acc[kHessian + a] = fmaf(J[a], r, acc[kHessian + a]);
-            }
+            a -= L;
+            ++d;
         }
     }
 
-#pragma unroll
-    for(int o = 16; o > 0; o >>= 1)
-        r2 += __shfl_xor_sync(0xffffffffu, r2, o);
+    r2 = warp_sum(r2);
     if(kJac)
     {
-#pragma unroll
-        for(int i = 0; i < kRed; ++i)
+        const float t32 = warp_sum(acc[32]), t33 = warp_sum(acc[33]), t34 = warp_sum(acc[34]);
+        reduce_scatter32(acc, lane);
+        red[wwarp * kRed + lane] = acc[0];
+        if(lane == 0)
         {
-            float x = acc[i];
-#pragma unroll
-            for(int o = 16; o > 0; o >>= 1)
-                x += __shfl_xor_sync(0xffffffffu, x, o);
-            acc[i] = x;
+            red[wwarp * kRed + 32] = t32;
+            red[wwarp * kRed + 33] = t33;
+            red[wwarp * kRed + 34] = t34;
         }
     }
     if(lane == 0)
+        redd[wwarp] = r2;
+}
+
+// ------------------------------------------------------------------------------
+// the warp-specialised persistent kernel
+// ------------------------------------------------------------------------------
+
+enum : int
+{
+    kSlotIdle = 0,       // no pass (no texel, or its slab is still arriving)
+    kSlotJacobian = 1,   // J^T J, J^T r and r^2 at the tabulated point
+    kSlotTrial = 2,      // r^2 at the tabulated point
+    kSlotExit = 3
+};
+
+constexpr uint32_t kNoTexel = 0xffffffffu;
+
+// Per-slot control state (static shared memory).
+struct Slot
+{
+    LmState st;
+    PassConst pc;
+    double sums[kRed + 1];
+    float pf[kParams];
+    uint64_t bar;         // the slab copy's mbarrier
+    uint32_t texel;       // texel in the slot, or kNoTexel
+    uint32_t parity;      // next phase of `bar`
+    int cmd;              // command of the pass the workers run next
+    int first;            // the pending Jacobian is the texel's first
+    int loading;          // the slab copy of `texel` is in flight
+    int dead;             // a copy did not arrive: the slot takes no more texels
+};
+
+// Dynamic shared memory per slot: [stride] slab | [Lp][kEntry] table |
+// [NW] double partials | [NW][kRed] float partials (doubles first: NW * kRed
+// floats need not be a multiple of 8 bytes).  Every part starts 128-byte aligned.
+template <int NW>
+struct SlotSmem
+{
+    __host__ __device__ static size_t slab_bytes(uint64_t stride) { return (sizeof(float) * stride + 127) & ~size_t(127); }
+    __host__ __device__ static size_t tab_bytes(uint32_t L) { return (sizeof(float) * kEntry * pad4(L) + 127) & ~size_t(127); }
+    __host__ __device__ static size_t red_bytes() { return (sizeof(float) * NW * kRed + sizeof(double) * NW + 127) & ~size_t(127); }
+    __host__ __device__ static size_t bytes(uint32_t L, uint64_t stride)
     {
-        redd[warp] = r2;
-        if(kJac)
-#pragma unroll
-            for(int i = 0; i < kRed; ++i)
-                red[warp * kRed + i] = acc[i];
+        return slab_bytes(stride) + tab_bytes(L) + red_bytes();
     }
-    __syncthreads();
-    if(threadIdx.x == 0)
+};
+
+__device__ __forceinline__ void nbar_sync(uint32_t id, uint32_t n)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+__device__ __forceinline__ void nbar_arrive(uint32_t id, uint32_t n)
+{
+    asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(n) : "memory");
+}
+
+// Named barrier ids: 0 is __syncthreads; READY[s] = 1 + s, DONE[s] = 1 + S + s.
+__device__ __forceinline__ uint32_t bar_ready(int s) { return 1u + (uint32_t)s; }
+template <int S>
+__device__ __forceinline__ uint32_t bar_done(int s) { return 1u + (uint32_t)S + (uint32_t)s; }
+
+// Writes a finished texel's outputs (LeastSquaresFitSGGX :381-429,
+// SVBRDFFitPipeline::fit :692-697).  Control thread.
+__device__ void write_texel(const LmArgs& args, LmState& st, uint32_t t, double n_pairs)
+{
+    float pout[kParams];
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
     {
-        double s = 0.0;
+        pout[i] = (float)st.p[i];
+        args.out[(uint64_t)t * kParams + i] = pout[i];
+    }
+    const double mse = st.S / n_pairs;
+    if(!isfinite(mse))
+        st.status |= SVF_TEXEL_NONFINITE;
+    args.rmse[t] = (float)sqrt(mse);
+    if(args.stats)
+    {
+        svf_texel_stats s;
+        s.iterations = st.iter;
+        s.effective = st.eff;
+        s.jacobians = st.njac;
+        s.residuals = st.nres;
+        s.status = st.status;
+        args.stats[t] = s;
+    }
+    if(args.map_sigma)
+    {
+        args.map_sigma[2 * (uint64_t)t] = pout[0];
+        args.map_sigma[2 * (uint64_t)t + 1] = pout[1];
+    }
+    if(args.map_basis)
+    {
+        // ToQuaternion(euler), quaternion.hh:82-94
+        float s1, c1, s2, c2, s3, c3;
+        sincosf(0.5f * pout[4], &s1, &c1);
+        sincosf(0.5f * pout[5], &s2, &c2);
+        sincosf(0.5f * pout[6], &s3, &c3);
+        float* q = args.map_basis + 4 * (uint64_t)t;
+        q[0] = s1 * c2 * c3 + c1 * s2 * s3;
+        q[1] = -s1 * c2 * s3 + c1 * s2 * c3;
+        q[2] = c1 * c2 * s3 + s1 * s2 * c3;
+        q[3] = c1 * c2 * c3 - s1 * s2 * s3;
+    }
+    if(args.avg_chroma && (args.map_diffuse || args.map_specular))
+    {
+        const float* a = args.avg_chroma + 3 * (uint64_t)t;
 #pragma unroll
-        for(int w = 0; w < kWarps; ++w)
-            s += redd[w];
-        out[kRed] = s;
-        if(kJac)
-            for(int i = 0; i < kRed; ++i)
-            {
-                double t = 0.0;
-#pragma unroll
-                for(int w = 0; w < kWarps; ++w)
-                    t += (double)red[w * kRed + i];
-                out[i] = t;
-            }
+        for(int k = 0; k < 3; ++k)
+        {
+            if(args.map_diffuse)
+                args.map_diffuse[3 * (uint64_t)t + k] = a[k] * pout[3];
+            if(args.map_specular)
+                args.map_specular[3 * (uint64_t)t + k] = a[k] * pout[2];
+        }
     }
 }
 
-// Resident CTAs per SM the register budget is sized for: with ~33 KB of shared
-// memory per CTA at 81 directions, six 64-thread CTAs fit an SM.
-constexpr int min_blocks(int threads) { return threads == 64 ? 6 : (threads == 128 ? 4 : 2); }
-
-template <int THREADS, int NC>
-__global__ void __launch_bounds__(THREADS, min_blocks(THREADS)) lm_fit_kernel(LmArgs args)
+// Control thread: takes the next texel for slot `sl` and starts its slab copy
+// (the slab is no longer read: the workers finished the slot's last pass).
+__device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot& sl, float* slab, uint32_t slab_bytes)
 {
-    using SM = Smem<THREADS>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float* tab = reinterpret_cast<float*>(smem_raw);
-    float* slab = reinterpret_cast<float*>(smem_raw + SM::slab_offset(args.L));
-    float* red = reinterpret_cast<float*>(smem_raw + SM::red_offset(args.L, args.lum_stride));
-    double* redd = reinterpret_cast<double*>(red + SM::kWarps * kRed);
+    const uint32_t t = sl.dead ? kNoTexel : atomicAdd(args.work_counter, 1u);
+    if(t < args.texels)
+    {
+        bulk_load(slab, args.lum + (uint64_t)t * args.lum_stride, slab_bytes, &sl.bar);
+        sl.texel = t;
+        sl.loading = 1;
+    }
+    else
+    {
+        sl.texel = kNoTexel;
+        sl.loading = 0;
+    }
+    sl.cmd = kSlotIdle;
+}
 
-    __shared__ LmState st;
-    __shared__ PassConst pc;
-    __shared__ __align__(8) uint64_t bar;
-    __shared__ float sh_pf[kParams];
-    __shared__ int sh_cmd;
-    __shared__ uint32_t sh_next;
-    __shared__ double sh_out[kRed + 1];
+// Control thread: the slot's slab has arrived; set up the fit of its texel.
+// False when the copy did not arrive within the bound.
+__device__ __forceinline__ bool slot_start(const LmArgs& args, Slot& sl)
+{
+    if(!mbar_wait(&sl.bar, sl.parity))
+    {
+        atomicOr(args.error_flag, 1u);
+        if(args.stats)
+            args.stats[sl.texel].status = SVF_TEXEL_TIMEOUT;
+        sl.dead = 1;
+        sl.loading = 0;
+        sl.texel = kNoTexel;
+        sl.cmd = kSlotIdle;
+        return false;
+    }
+    sl.parity ^= 1u;
+    sl.loading = 0;
+    LmState& st = sl.st;
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+    {
+        st.p[i] = (double)args.init[(uint64_t)sl.texel * kParams + i];
+        sl.pf[i] = (float)st.p[i];
+    }
+    st.iter = st.eff = st.njac = st.nres = st.status = 0;
+    st.restarts_left = args.cfg.restarts;
+    sl.first = 1;
+    sl.cmd = kSlotJacobian;
+    return true;
+}
+
+// Resident CTAs per SM the register budget is sized for.
+constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : 2; }
+
+template <int NW, int S, bool kFresnel>
+__global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_fit_kernel(LmArgs args)
+{
+    constexpr uint32_t kThreads = 32 * (NW + 1);
+    using SM = SlotSmem<NW>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ Slot slots[S];
 
     const uint32_t L = args.L;
     const double n_pairs = (double)args.N;
     const uint32_t slab_bytes = (uint32_t)(args.lum_stride * sizeof(float));
-    const float* geo = args.geo;
+    const size_t per_slot = SM::bytes(L, args.lum_stride);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 
-    if(threadIdx.x == 0)
+    auto slab_of = [&](int s) { return reinterpret_cast<float*>(smem_raw + s * per_slot); };
+    auto tab_of = [&](int s) { return reinterpret_cast<float*>(smem_raw + s * per_slot + SM::slab_bytes(args.lum_stride)); };
+    auto redd_of = [&](int s) {
+        return reinterpret_cast<double*>(smem_raw + s * per_slot + SM::slab_bytes(args.lum_stride) + SM::tab_bytes(L));
+    };
+    auto red_of = [&](int s) { return reinterpret_cast<float*>(redd_of(s) + NW); };
+
+    if(warp != 0)
     {
-        mbar_init(&bar, 1);
-        const uint32_t t0 = atomicAdd(args.work_counter, 1u);
-        if(t0 < args.texels)
-            bulk_load(slab, args.lum + (uint64_t)t0 * args.lum_stride, slab_bytes, &bar);
-        sh_next = t0;
+        // ---- pair workers
+        const uint32_t wwarp = warp - 1;
+        for(int s = 0;; s = (s + 1 == S) ? 0 : s + 1)
+        {
+            nbar_sync(bar_ready(s), kThreads);
+            const int cmd = slots[s].cmd;
+            if(cmd == kSlotExit)
+                break;
+            if(cmd == kSlotJacobian)
+                worker_pass<NW, true, kFresnel>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
+                                          redd_of(s), wwarp, lane);
+            else if(cmd == kSlotTrial)
+                worker_pass<NW, false, kFresnel>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
+                                           redd_of(s), wwarp, lane);
+            nbar_arrive(bar_done<S>(s), kThreads);
+        }
+        return;
     }
-    __syncthreads();
-    uint32_t phase = 0;
-    uint32_t t = sh_next;
 
-    while(t < args.texels)
+    // ---- control warp
+    if(lane == 0)
     {
-        if(!mbar_wait(&bar, phase))
+        for(int s = 0; s < S; ++s)
         {
-            // the copy did not land within the bound: flag it, give it one more
-            // bounded wait, and leave
-            if(threadIdx.x == 0)
-            {
-                atomicOr(args.error_flag, 1u);
-                if(args.stats)
-                    args.stats[t].status = SVF_TEXEL_TIMEOUT;
-            }
-            mbar_wait(&bar, phase);
-            return;
+            Slot& sl = slots[s];
+            mbar_init(&sl.bar, 1);
+            sl.parity = 0;
+            sl.dead = 0;
+            slot_fetch(args, sl, slab_of(s), slab_bytes);
         }
-        phase ^= 1u;
+        for(int s = 0; s < S; ++s)
+            if(slots[s].loading)
+                slot_start(args, slots[s]);
+    }
+    __syncwarp();
+    for(int s = 0; s < S; ++s)
+    {
+        if(slots[s].cmd == kSlotJacobian)
+            build_table(tab_of(s), args.geo, L, slots[s].pf, &slots[s].pc, lane);
+        __syncwarp();
+        nbar_arrive(bar_ready(s), kThreads);
+    }
 
-        if(threadIdx.x == 0)
+    for(int s = 0;; s = (s + 1 == S) ? 0 : s + 1)
+    {
+        Slot& sl = slots[s];
+        nbar_sync(bar_done<S>(s), kThreads);
+        const int done_cmd = sl.cmd;
+        // FP64 sums of the workers' partials, one lane per sum
+        if(done_cmd == kSlotJacobian)
         {
-#pragma unroll
-            for(int i = 0; i < kParams; ++i)
+            const float* red = red_of(s);
+            const double* redd = redd_of(s);
+            for(uint32_t i = lane; i <= (uint32_t)kRed; i += 32)
             {
-                st.p[i] = (double)args.init[(uint64_t)t * kParams + i];
-                sh_pf[i] = (float)st.p[i];
+                double t = 0.0;
+                if(i < (uint32_t)kRed)
+                {
+#pragma unroll
+                    for(int w = 0; w < NW; ++w)
+                        t += (double)red[w * kRed + i];
+                }
+                else
+                {
+#pragma unroll
+                    for(int w = 0; w < NW; ++w)
+                        t += redd[w];
+                }
+                sl.sums[i] = t;
             }
-            st.iter = st.eff = st.njac = st.nres = st.status = 0;
-            st.restarts_left = args.cfg.restarts;
         }
-        __syncthreads();
-        build_table(tab, geo, L, sh_pf, &pc, THREADS);
-        __syncthreads();
-        pair_pass<THREADS, NC, true>(tab, pc, slab, L, args.cfg.fresnel, red, redd, sh_out);
-        if(threadIdx.x == 0)
+        else if(done_cmd == kSlotTrial && lane == 0)
         {
-            st.njac = 1;
-            st.S = sh_out[kRed];
+            const double* redd = redd_of(s);
+            double t = 0.0;
 #pragma unroll
-            for(int i = 0; i < kParams; ++i)
-                st.g[i] = -sh_out[kHessian + i];
-#pragma unroll
-            for(int i = 0; i < kHessian; ++i)
-                st.H[i] = sh_out[i];
-            lm_reset_damping(st);
-            if(!isfinite(st.S))
-                st.status |= SVF_TEXEL_NONFINITE;
+            for(int w = 0; w < NW; ++w)
+                t += redd[w];
+            sl.sums[kRed] = t;
         }
-        for(;;)
+        __syncwarp();
+
+        bool build = false, exit_now = false;
+        if(lane == 0)
         {
-            if(threadIdx.x == 0)
+            LmState& st = sl.st;
+            int next = kCmdDone;
+            if(done_cmd == kSlotJacobian)
             {
-                const int cmd = lm_next(st, args.cfg, n_pairs);
-                if(cmd == kCmdTrial)
+                if(sl.first)
+                {
+                    sl.first = 0;
+                    st.njac = 1;
+                    st.S = sl.sums[kRed];
 #pragma unroll
                     for(int i = 0; i < kParams; ++i)
-                        sh_pf[i] = (float)st.pt[i];
-                sh_cmd = cmd;
-            }
-            __syncthreads();
-            if(sh_cmd == kCmdDone)
-                break;
-            build_table(tab, geo, L, sh_pf, &pc, THREADS);
-            __syncthreads();
-            pair_pass<THREADS, NC, false>(tab, pc, slab, L, args.cfg.fresnel, red, redd, sh_out);
-            if(threadIdx.x == 0)
-                sh_cmd = lm_after_trial(st, args.cfg, sh_out[kRed], n_pairs);
-            __syncthreads();
-            const int cmd = sh_cmd;
-            if(cmd == kCmdDone)
-                break;
-            if(cmd == kCmdJacobian)
-            {
-                // the table built for the trial point is the accepted point's
-                pair_pass<THREADS, NC, true>(tab, pc, slab, L, args.cfg.fresnel, red, redd, sh_out);
-                if(threadIdx.x == 0)
-                    sh_cmd = lm_after_jacobian(st, args.cfg, sh_out, n_pairs);
-                __syncthreads();
-                if(sh_cmd == kCmdDone)
-                    break;
-            }
-        }
-
-        // The slab is no longer read: start the next texel's copy, then write the
-        // outputs (LeastSquaresFitSGGX :381-429, SVBRDFFitPipeline::fit :692-697).
-        if(threadIdx.x == 0)
-        {
-            const uint32_t tn = atomicAdd(args.work_counter, 1u);
-            if(tn < args.texels)
-                bulk_load(slab, args.lum + (uint64_t)tn * args.lum_stride, slab_bytes, &bar);
-            sh_next = tn;
-
-            float pout[kParams];
+                        st.g[i] = -sl.sums[kHessian + i];
 #pragma unroll
-            for(int i = 0; i < kParams; ++i)
-            {
-                pout[i] = (float)st.p[i];
-                args.out[(uint64_t)t * kParams + i] = pout[i];
+                    for(int i = 0; i < kHessian; ++i)
+                        st.H[i] = sl.sums[i];
+                    lm_reset_damping(st);
+                    if(!isfinite(st.S))
+                        st.status |= SVF_TEXEL_NONFINITE;
+                    next = kCmdContinue;
+                }
+                else
+                    next = lm_after_jacobian(st, args.cfg, sl.sums, n_pairs);
             }
-            const double mse = st.S / n_pairs;
-            if(!isfinite(mse))
-                st.status |= SVF_TEXEL_NONFINITE;
-            args.rmse[t] = (float)sqrt(mse);
-            if(args.stats)
+            else if(done_cmd == kSlotTrial)
             {
-                svf_texel_stats s;
-                s.iterations = st.iter;
-                s.effective = st.eff;
-                s.jacobians = st.njac;
-                s.residuals = st.nres;
-                s.status = st.status;
-                args.stats[t] = s;
+                next = lm_after_trial(st, args.cfg, sl.sums[kRed], n_pairs);
             }
-            if(args.map_sigma)
+            if(done_cmd == kSlotJacobian || done_cmd == kSlotTrial)
             {
-                args.map_sigma[2 * (uint64_t)t] = pout[0];
-                args.map_sigma[2 * (uint64_t)t + 1] = pout[1];
-            }
-            if(args.map_basis)
-            {
-                // ToQuaternion(euler), quaternion.hh:82-94
-                float s1, c1, s2, c2, s3, c3;
-                sincosf(0.5f * pout[4], &s1, &c1);
-                sincosf(0.5f * pout[5], &s2, &c2);
-                sincosf(0.5f * pout[6], &s3, &c3);
-                float* q = args.map_basis + 4 * (uint64_t)t;
-                q[0] = s1 * c2 * c3 + c1 * s2 * s3;
-                q[1] = -s1 * c2 * s3 + c1 * s2 * c3;
-                q[2] = c1 * c2 * s3 + s1 * s2 * c3;
-                q[3] = c1 * c2 * c3 - s1 * s2 * s3;
-            }
-            if(args.avg_chroma && (args.map_diffuse || args.map_specular))
-            {
-                const float* a = args.avg_chroma + 3 * (uint64_t)t;
-#pragma unroll
-                for(int k = 0; k < 3; ++k)
+                if(next == kCmdContinue)
+                    next = lm_next(st, args.cfg, n_pairs);
+                if(next == kCmdTrial)
                 {
-                    if(args.map_diffuse)
-                        args.map_diffuse[3 * (uint64_t)t + k] = a[k] * pout[3];
-                    if(args.map_specular)
-                        args.map_specular[3 * (uint64_t)t + k] = a[k] * pout[2];
+#pragma unroll
+                    for(int i = 0; i < kParams; ++i)
+                        sl.pf[i] = (float)st.pt[i];
+                    sl.cmd = kSlotTrial;
+                    build = true;
+                }
+                else if(next == kCmdJacobian)
+                {
+                    // the table built for the trial point is the accepted point's
+                    sl.cmd = kSlotJacobian;
+                }
+                else
+                {
+                    write_texel(args, st, sl.texel, n_pairs);
+                    slot_fetch(args, sl, slab_of(s), slab_bytes);
+                }
+            }
+            else if(sl.loading)
+            {
+                // the slab was requested during an earlier visit
+                build = slot_start(args, sl);
+            }
+            if(sl.cmd == kSlotIdle && !sl.loading)
+            {
+                bool all_idle = true;
+                for(int j = 0; j < S; ++j)
+                    all_idle = all_idle && slots[j].cmd == kSlotIdle && !slots[j].loading;
+                if(all_idle)
+                {
+                    sl.cmd = kSlotExit;
+                    exit_now = true;
                 }
             }
         }
-        __syncthreads();
-        t = sh_next;
+        __syncwarp();   // orders lane 0's slot updates before the other lanes read them
+        build = __shfl_sync(0xffffffffu, build, 0);
+        exit_now = __shfl_sync(0xffffffffu, exit_now, 0);
+        if(build)
+            build_table(tab_of(s), args.geo, L, sl.pf, &sl.pc, lane);
+        __syncwarp();
+        nbar_arrive(bar_ready(s), kThreads);
+        if(exit_now)
+        {
+            // the workers finish the passes already handed out (all idle) and
+            // then meet the exit command of slot s
+            for(int j = 1; j < S; ++j)
+                nbar_sync(bar_done<S>((s + j) % S), kThreads);
+            break;
+        }
     }
 }
 
 using KernelFn = void (*)(LmArgs);
 
-template <int THREADS>
-KernelFn pick_nc(int nc)
+KernelFn kernel_for(LmKernelChoice c, bool fresnel)
 {
-    switch(nc)
-    {
-    case 1: return lm_fit_kernel<THREADS, 1>;
-    case 2: return lm_fit_kernel<THREADS, 2>;
-    case 3: return lm_fit_kernel<THREADS, 3>;
-    case 4: return lm_fit_kernel<THREADS, 4>;
-    case 5: return lm_fit_kernel<THREADS, 5>;
-    default: return nullptr;
-    }
-}
-
-KernelFn kernel_for(LmKernelChoice c)
-{
-    switch(c.threads)
-    {
-    case 64: return pick_nc<64>(c.nc);
-    case 128: return pick_nc<128>(c.nc);
-    case 256: return pick_nc<256>(c.nc);
-    default: return nullptr;
-    }
+    if(c.threads == 256 && c.slots == 2)
+        return fresnel ? lm_fit_kernel<7, 2, true> : lm_fit_kernel<7, 2, false>;
+    if(c.threads == 256 && c.slots == 3)
+        return fresnel ? lm_fit_kernel<7, 3, true> : lm_fit_kernel<7, 3, false>;
+    if(c.threads == 128 && c.slots == 2)
+        return fresnel ? lm_fit_kernel<3, 2, true> : lm_fit_kernel<3, 2, false>;
+    if(c.threads == 128 && c.slots == 3)
+        return fresnel ? lm_fit_kernel<3, 3, true> : lm_fit_kernel<3, 3, false>;
+    return nullptr;
 }
 
 } // namespace
 
-LmKernelChoice lm_default_choice(uint32_t L)
+LmKernelChoice lm_default_choice(uint32_t)
 {
-    return LmKernelChoice{ 64, (int)((L + 31) / 32) };
+    return LmKernelChoice{ 256, 3 };
 }
 
-int lm_candidates(uint32_t L, LmKernelChoice* out, int max)
+int lm_candidates(uint32_t, LmKernelChoice* out, int max)
 {
-    const int nc = (int)((L + 31) / 32);
-    const int threads[3] = { 64, 128, 256 };
+    const LmKernelChoice all[4] = { { 256, 3 }, { 256, 2 }, { 128, 3 }, { 128, 2 } };
     int n = 0;
-    for(int i = 0; i < 3 && n < max; ++i)
-        out[n++] = LmKernelChoice{ threads[i], nc };
+    for(int i = 0; i < 4 && n < max; ++i)
+        out[n++] = all[i];
     return n;
 }
 
 size_t lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
 {
-    switch(c.threads)
-    {
-    case 64: return Smem<64>::bytes(L, lum_stride);
-    case 128: return Smem<128>::bytes(L, lum_stride);
-    default: return Smem<256>::bytes(L, lum_stride);
-    }
+    const size_t per = c.threads == 128 ? SlotSmem<3>::bytes(L, lum_stride) : SlotSmem<7>::bytes(L, lum_stride);
+    return per * (size_t)c.slots;
 }
 
 int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
 {
-    KernelFn k = kernel_for(c);
-    if(!k || (uint32_t)c.nc * 32u < L)
+    // the Fresnel and Fresnel-free variants share registers and shared memory
+    KernelFn k = kernel_for(c, false);
+    if(!k || L == 0)
         return 0;
     const size_t smem = lm_smem_bytes(L, lum_stride, c);
     if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
@@ -820,8 +1042,8 @@ int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
 
 cudaError_t launch_lm_fit(const LmArgs& args, LmKernelChoice c, int grid, cudaStream_t stream)
 {
-    KernelFn k = kernel_for(c);
-    if(!k || (uint32_t)c.nc * 32u < args.L)
+    KernelFn k = kernel_for(c, args.cfg.fresnel != 1.0f);
+    if(!k || args.L == 0)
         return cudaErrorInvalidConfiguration;
     const size_t smem = lm_smem_bytes(args.L, args.lum_stride, c);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
