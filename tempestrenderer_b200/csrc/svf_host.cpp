@@ -169,12 +169,15 @@ struct svf_ctx
 {
     int device = 0;
     int sms = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;        // compute
+    cudaStream_t copy_stream = nullptr;   // host -> device staging of svf_fit_texels
     cudaEvent_t ev[8] = {};
+    cudaEvent_t copied[2] = {}, freed[2] = {};   // staging handoff (no timing)
+    std::vector<cudaEvent_t> chunk_ev;           // per-chunk phase timing
     std::map<uint64_t, std::unique_ptr<Layout>> layouts;
     std::unique_ptr<svf::InitHostTables> tables;
-    DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, maps_buf,
-        scratch;
+    DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, samples2,
+        maps_buf, scratch;
     PinnedBuf pinned;
 };
 
@@ -385,14 +388,15 @@ struct LmRun
 };
 
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c);
+svf_status read_error_flag(svf_ctx* ctx, bool with_ndf = false);
 
-// Autotuner of the LM kernel configuration (CTA size), once per layout: each
-// candidate fits the same seeded synthetic probe (2048 texels of the uneven
-// parameter mix, from a perturbed ground truth) and is scored by model flops per
-// second (the flops per Jacobian and residual pass times the passes it ran,
-// over its CUDA-event time).  The first candidate, the 64-thread kernel, is kept
-// unless another is more than 3% faster.  Tuning on a fixed probe, not on the
-// caller's texels, keeps every texel of a call on one configuration.
+// Autotuner of the LM kernel configuration (CTA size and texel slots), once per
+// layout: each candidate fits the same seeded synthetic probe (8192 texels of
+// the uneven parameter mix, from a perturbed ground truth) and is scored by
+// model flops per second (the flops per Jacobian and residual pass times the
+// passes it ran, over its CUDA-event time).  The first candidate is kept unless
+// another is more than 3% faster.  Tuning on a fixed probe, not on the caller's
+// texels, keeps every texel of a call on one configuration.
 svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
 {
     if(lay->tuned)
@@ -491,6 +495,9 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
     }
     lay->choice = best_rate > 1.03 * first_rate ? cand[best] : cand[0];
     lay->tuned = true;
+    // the probe's launches write only the LM word
+    SVF_TRY(read_error_flag(ctx));
+    SVF_CUDA(cudaMemsetAsync(ctx->error.p, 0, sizeof(uint32_t), ctx->stream));
     return SVF_OK;
 }
 
@@ -528,8 +535,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     SVF_TRY(ctx->error.ensure(16));
     a.work_counter = ctx->counter.as<uint32_t>();
     a.error_flag = ctx->error.as<uint32_t>();
-    SVF_CUDA(cudaMemsetAsync(ctx->counter.p, 0, 16, ctx->stream));
-    SVF_CUDA(cudaMemsetAsync(ctx->error.p, 0, 8, ctx->stream));   // word 2 belongs to the NDF GEMM
+    SVF_CUDA(cudaMemsetAsync(ctx->counter.p, 0, 16, ctx->stream));   // the error words are zeroed per call
     int per_sm = svf::lm_max_ctas_per_sm(a.L, a.lum_stride, c);
     if(per_sm <= 0)
         return fail(SVF_EINVAL, "the LM kernel (%d threads) does not fit on an SM for L = %u", c.threads, a.L);
@@ -538,8 +544,16 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     return SVF_OK;
 }
 
-// Error words: [0] LM kernel, [2] NDF GEMM (with_ndf).
-svf_status read_error_flag(svf_ctx* ctx, bool with_ndf = false)
+// Error words: [0] LM kernel, [2] NDF GEMM.  Zeroed once per call, so that a
+// flag raised by any launch of the call is seen.
+svf_status zero_error_flags(svf_ctx* ctx)
+{
+    SVF_TRY(ctx->error.ensure(16));
+    SVF_CUDA(cudaMemsetAsync(ctx->error.p, 0, 16, ctx->stream));
+    return SVF_OK;
+}
+
+svf_status read_error_flag(svf_ctx* ctx, bool with_ndf)
 {
     uint32_t flag[3] = {};
     SVF_CUDA(cudaMemcpyAsync(flag, ctx->error.p, sizeof(flag), cudaMemcpyDeviceToHost, ctx->stream));
@@ -617,8 +631,14 @@ svf_status svf_create(int device, svf_ctx** out)
     ctx->sms = prop.multiProcessorCount;
     SVF_CUDA(cudaSetDevice(device));
     SVF_CUDA(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+    SVF_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     for(auto& e : ctx->ev)
         SVF_CUDA(cudaEventCreate(&e));
+    for(int i = 0; i < 2; ++i)
+    {
+        SVF_CUDA(cudaEventCreateWithFlags(&ctx->copied[i], cudaEventDisableTiming));
+        SVF_CUDA(cudaEventCreateWithFlags(&ctx->freed[i], cudaEventDisableTiming));
+    }
     *out = ctx.release();
     return SVF_OK;
 }
@@ -630,9 +650,22 @@ void svf_destroy(svf_ctx* ctx)
     cudaSetDevice(ctx->device);
     if(ctx->stream)
         cudaStreamSynchronize(ctx->stream);
+    if(ctx->copy_stream)
+        cudaStreamSynchronize(ctx->copy_stream);
     for(auto& e : ctx->ev)
         if(e)
             cudaEventDestroy(e);
+    for(int i = 0; i < 2; ++i)
+    {
+        if(ctx->copied[i])
+            cudaEventDestroy(ctx->copied[i]);
+        if(ctx->freed[i])
+            cudaEventDestroy(ctx->freed[i]);
+    }
+    for(auto e : ctx->chunk_ev)
+        cudaEventDestroy(e);
+    if(ctx->copy_stream)
+        cudaStreamDestroy(ctx->copy_stream);
     if(ctx->stream)
         cudaStreamDestroy(ctx->stream);
     delete ctx;
@@ -696,6 +729,7 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
     SVF_TRY(to_device(ctx, ctx->init.p, init, sizeof(float) * 7 * T));
     LmRun r{ ctx->lum.as<float>(), stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
              ctx->stats.as<svf_texel_stats>(), nullptr, nullptr, nullptr, nullptr, nullptr, T };
+    SVF_TRY(zero_error_flags(ctx));
     SVF_TRY(run_lm(ctx, lay, opts, r));
     SVF_CUDA(cudaMemcpyAsync(out, ctx->out.p, sizeof(float) * 7 * T, cudaMemcpyDefault, ctx->stream));
     SVF_CUDA(cudaMemcpyAsync(rmse, ctx->rmse.p, sizeof(float) * T, cudaMemcpyDefault, ctx->stream));
@@ -798,31 +832,36 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     const size_t elem = btf->sample_type == SVF_SAMPLES_F16 ? 2 : 4;
     const size_t texel_bytes = elem * 3 * (size_t)N;
     const bool samples_on_device = is_device_pointer(btf->samples);
-
-    // chunking: bounded device footprint for host inputs and the NDF textures
-    size_t free_b = 0, total_b = 0;
-    SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const bool default_init = opts->init_mode == SVF_INIT_DEFAULT;
     if(maps->ndf && !default_init)
         return fail(SVF_EINVAL, "the NDF map exists only with the default initial guess");
     const uint32_t ndf_ld = default_init ? init_lay->ndf_rows_pad : 0;
-    size_t per_texel = sizeof(float) * (stride + 3 + 7 + 7 + 1 + 12) + sizeof(svf_texel_stats) +
-                       (default_init ? 2 * 2 * stride + sizeof(float) * ndf_ld : 0) +
-                       (maps->ndf ? sizeof(float) * svf::kNdfTexels : 0) + (samples_on_device ? 0 : texel_bytes);
+
+    // Chunking.  Device-resident samples: as few chunks as the device memory
+    // allows.  Host samples: a pipeline of chunks, each copied host -> device on
+    // the copy stream into one of two staging buffers while the compute stream
+    // fits the previous chunk; a staging buffer is free again once the
+    // luminance kernel has read it.
+    size_t free_b = 0, total_b = 0;
+    SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_texel = sizeof(float) * (stride + 3 + 7 + 7 + 1 + 12) +
+                             (default_init ? 2 * 2 * stride + sizeof(float) * ndf_ld : 0) +
+                             (maps->ndf ? sizeof(float) * svf::kNdfTexels : 0) +
+                             (samples_on_device ? 0 : 2 * texel_bytes);
     uint64_t chunk = std::max<uint64_t>(1, (uint64_t)(0.5 * (double)free_b / (double)per_texel));
+    if(!samples_on_device)
+        chunk = std::min<uint64_t>(chunk, std::max<uint64_t>(8192, (T + 7) / 8));
     chunk = std::min<uint64_t>(chunk, T);
     chunk = std::min<uint64_t>(chunk, 65535ull * 128);   // the NDF GEMM's grid rows of 128 texels
-    if(!samples_on_device)
-        chunk = std::min<uint64_t>(chunk, std::max<uint64_t>(1, (256ull << 20) / texel_bytes) * 16);
+    const uint64_t n_chunks = (T + chunk - 1) / chunk;
 
     SVF_TRY(ctx->lum.ensure(sizeof(float) * stride * chunk));
     SVF_TRY(ctx->avg.ensure(sizeof(float) * 3 * chunk));
     SVF_TRY(ctx->init.ensure(sizeof(float) * 7 * chunk));
     SVF_TRY(ctx->out.ensure(sizeof(float) * 7 * chunk));
     SVF_TRY(ctx->rmse.ensure(sizeof(float) * chunk));
-    SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * chunk));
+    SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * T));
     SVF_TRY(ctx->maps_buf.ensure(sizeof(float) * 12 * chunk));
-    SVF_TRY(ctx->error.ensure(16));
     if(default_init)
     {
         SVF_TRY(ctx->lum_hi.ensure(2 * stride * chunk));
@@ -831,34 +870,75 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     }
     if(maps->ndf)
         SVF_TRY(ctx->ndf_tex.ensure(sizeof(float) * svf::kNdfTexels * chunk));
+    DevBuf* staging[2] = { &ctx->samples, &ctx->samples2 };
     if(!samples_on_device)
-        SVF_TRY(ctx->samples.ensure(texel_bytes * chunk));
-
-    svf_run_stats rs{};
-    float ms = 0.0f;
-    std::vector<svf_texel_stats> host_stats;
-    for(uint64_t c0 = 0; c0 < T; c0 += chunk)
     {
-        const uint64_t n = std::min<uint64_t>(chunk, T - c0);
-        const void* samples = static_cast<const char*>(btf->samples) + c0 * texel_bytes;
+        SVF_TRY(ctx->samples.ensure(texel_bytes * chunk));
+        if(n_chunks > 1)
+            SVF_TRY(ctx->samples2.ensure(texel_bytes * chunk));
+    }
+    // per chunk: copy start/end (copy stream), then lum, init, LM, outputs (compute stream)
+    constexpr int kEv = 7;
+    while(ctx->chunk_ev.size() < kEv * n_chunks)
+    {
+        cudaEvent_t e;
+        SVF_CUDA(cudaEventCreate(&e));
+        ctx->chunk_ev.push_back(e);
+    }
+    auto ev = [&](uint64_t c, int k) { return ctx->chunk_ev[kEv * c + (uint64_t)k]; };
+
+    // host -> device copy of chunk c into staging buffer c % 2
+    auto issue_copy = [&](uint64_t c) -> svf_status {
+        const uint64_t c0 = c * chunk, n = std::min<uint64_t>(chunk, T - c0);
+        const int buf = (int)(c & 1);
+        if(c >= 2)
+            SVF_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->freed[buf], 0));
+        SVF_CUDA(cudaEventRecord(ev(c, 0), ctx->copy_stream));
+        SVF_CUDA(cudaMemcpyAsync(staging[buf]->p, static_cast<const char*>(btf->samples) + c0 * texel_bytes,
+                                 texel_bytes * n, cudaMemcpyHostToDevice, ctx->copy_stream));
+        SVF_CUDA(cudaEventRecord(ev(c, 1), ctx->copy_stream));
+        SVF_CUDA(cudaEventRecord(ctx->copied[buf], ctx->copy_stream));
+        return SVF_OK;
+    };
+
+    SVF_TRY(zero_error_flags(ctx));
+    if(!samples_on_device)
+    {
+        // the compute stream's earlier work (a previous call) is done with the
+        // staging buffers before the first copies overwrite them
         SVF_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+        SVF_CUDA(cudaStreamWaitEvent(ctx->copy_stream, ctx->ev[0], 0));
+        SVF_TRY(issue_copy(0));
+        if(n_chunks > 1)
+            SVF_TRY(issue_copy(1));
+    }
+    for(uint64_t c = 0; c < n_chunks; ++c)
+    {
+        const uint64_t c0 = c * chunk, n = std::min<uint64_t>(chunk, T - c0);
+        const void* samples = static_cast<const char*>(btf->samples) + c0 * texel_bytes;
+        const int buf = (int)(c & 1);
         if(!samples_on_device)
         {
-            SVF_CUDA(cudaMemcpyAsync(ctx->samples.p, samples, texel_bytes * n, cudaMemcpyHostToDevice, ctx->stream));
-            samples = ctx->samples.p;
+            SVF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->copied[buf], 0));
+            samples = staging[buf]->p;
         }
-        SVF_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+        SVF_CUDA(cudaEventRecord(ev(c, 2), ctx->stream));
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
                                        ctx->avg.as<float>(), default_init ? ctx->lum_hi.p : nullptr,
                                        default_init ? ctx->lum_lo.p : nullptr, ctx->stream));
-        SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
+        if(!samples_on_device)
+        {
+            SVF_CUDA(cudaEventRecord(ctx->freed[buf], ctx->stream));
+            if(c + 2 < n_chunks)
+                SVF_TRY(issue_copy(c + 2));
+        }
+        SVF_CUDA(cudaEventRecord(ev(c, 3), ctx->stream));
         if(default_init)
         {
-            uint32_t* ndf_error = ctx->error.as<uint32_t>() + 2;
-            SVF_CUDA(cudaMemsetAsync(ndf_error, 0, sizeof(uint32_t), ctx->stream));
             cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.p, ctx->lum_lo.p, n, stride, init_lay->ndf_op_hi,
                                                init_lay->ndf_op_lo, init_lay->ndf_rows_pad, init_lay->k_pad, N,
-                                               ctx->ndf.as<float>(), ndf_ld, ndf_error, ctx->stream);
+                                               ctx->ndf.as<float>(), ndf_ld, ctx->error.as<uint32_t>() + 2,
+                                               ctx->stream);
             if(e != cudaSuccess)
                 return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
             SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->ndf.as<float>(), ndf_ld, n, ctx->init.as<float>(),
@@ -866,13 +946,14 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         }
         else
             SVF_TRY(to_device(ctx, ctx->init.p, opts->init_params + 7 * c0, sizeof(float) * 7 * n));
-        SVF_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+        SVF_CUDA(cudaEventRecord(ev(c, 4), ctx->stream));
         float* mb = ctx->maps_buf.as<float>();
         LmRun r{ ctx->lum.as<float>(), stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
-                 ctx->stats.as<svf_texel_stats>(), ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n };
+                 ctx->stats.as<svf_texel_stats>() + c0, ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n,
+                 n };
         SVF_TRY(run_lm(ctx, lay, &opts->lsq, r));
-        SVF_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
-        // outputs
+        SVF_CUDA(cudaEventRecord(ev(c, 5), ctx->stream));
+        // outputs (into host or device buffers of the caller)
         auto put = [&](void* dst, const void* src, size_t bytes) -> svf_status {
             if(dst)
                 SVF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
@@ -887,34 +968,41 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_TRY(put(maps->init ? maps->init + 7 * c0 : nullptr, ctx->init.p, sizeof(float) * 7 * n));
         SVF_TRY(put(maps->ndf ? maps->ndf + (uint64_t)svf::kNdfTexels * c0 : nullptr, ctx->ndf_tex.p,
                     sizeof(float) * svf::kNdfTexels * n));
-        std::vector<svf_texel_stats> st(n);
-        SVF_CUDA(cudaMemcpyAsync(st.data(), ctx->stats.p, sizeof(svf_texel_stats) * n, cudaMemcpyDeviceToHost,
-                                 ctx->stream));
-        SVF_CUDA(cudaEventRecord(ctx->ev[5], ctx->stream));
-        SVF_TRY(read_error_flag(ctx, default_init));
-        if(maps->stats)
-            SVF_CUDA(cudaMemcpy(maps->stats + c0, st.data(), sizeof(svf_texel_stats) * n, cudaMemcpyDefault));
-        for(auto& s : st)
-        {
-            rs.iterations += s.iterations;
-            rs.jacobians += s.jacobians;
-            rs.residuals += s.residuals;
-            if(s.status & (SVF_TEXEL_NONFINITE | SVF_TEXEL_TIMEOUT))
-                rs.failed_texels++;
-        }
-        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[5]));
-        rs.ms_total += ms;
-        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
-        rs.ms_copy += ms;
-        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]));
-        rs.ms_copy += ms;
-        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]));
-        rs.ms_luminance += ms;
-        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
-        rs.ms_init += ms;
-        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[3], ctx->ev[4]));
-        rs.ms_fit += ms;
+        SVF_CUDA(cudaEventRecord(ev(c, 6), ctx->stream));
     }
+    std::vector<svf_texel_stats> st(T);
+    SVF_CUDA(cudaMemcpyAsync(st.data(), ctx->stats.p, sizeof(svf_texel_stats) * T, cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    SVF_TRY(read_error_flag(ctx, default_init));   // waits for the compute stream
+    SVF_CUDA(cudaStreamSynchronize(ctx->copy_stream));
+    if(maps->stats)
+        SVF_CUDA(cudaMemcpy(maps->stats, st.data(), sizeof(svf_texel_stats) * T, cudaMemcpyDefault));
+
+    svf_run_stats rs{};
+    for(auto& x : st)
+    {
+        rs.iterations += x.iterations;
+        rs.jacobians += x.jacobians;
+        rs.residuals += x.residuals;
+        if(x.status & (SVF_TEXEL_NONFINITE | SVF_TEXEL_TIMEOUT))
+            rs.failed_texels++;
+    }
+    auto span = [&](cudaEvent_t a0, cudaEvent_t a1) -> double {
+        float ms = 0.0f;
+        return cudaEventElapsedTime(&ms, a0, a1) == cudaSuccess ? (double)ms : 0.0;
+    };
+    for(uint64_t c = 0; c < n_chunks; ++c)
+    {
+        if(!samples_on_device)
+            rs.ms_copy += span(ev(c, 0), ev(c, 1));
+        rs.ms_luminance += span(ev(c, 2), ev(c, 3));
+        rs.ms_init += span(ev(c, 3), ev(c, 4));
+        rs.ms_fit += span(ev(c, 4), ev(c, 5));
+        rs.ms_copy += span(ev(c, 5), ev(c, 6));
+    }
+    // the whole call: from the first copy (or the first kernel) to the last output
+    rs.ms_total = span(samples_on_device ? ev(0, 2) : ev(0, 0), ev(n_chunks - 1, 6));
+    cudaGetLastError();
     rs.texels = T;
     const svf::LmKernelChoice used = lay->tuned ? lay->choice : svf::lm_default_choice(L);
     rs.lm_threads = (uint32_t)used.threads;

@@ -8,12 +8,13 @@
 // keeps S texels ("slots") in flight:
 //
 //   warp 0, the control warp: per slot, the FP64 LM control (thread 0; state in
-//     shared memory), the cross-warp FP64 sums of the pass results, the
-//     direction table for the next evaluation (all 32 lanes), the texel's
+//     shared memory), the direction table for the next evaluation (all 32
+//     lanes), the texel's
 //     outputs and the bulk TMA copy (cp.async.bulk, mbarrier, bounded wait) of
 //     the next texel's luminance slab into the slot;
 //   warps 1..NW, the pair workers: the pair passes of slot 0, 1, .., S-1, 0, ..
-//     in turn.
+//     in turn; the last worker warp to finish a pass sums the warps' partials
+//     in FP64, in warp order.
 //
 // Named barriers hand each slot back and forth: READY[s] (control -> workers:
 // the command, table and constants of slot s are in place) and DONE[s]
@@ -25,8 +26,9 @@
 // A pass evaluates nothing per pair that depends on one direction only: the
 // table (svf_model.cuh) holds 12 floats per direction.  The workers walk the
 // L (L + 1) / 2 unordered direction pairs, one per lane, and evaluate the
-// specular core once for both ordered pairs (sym_pair).  Jacobian passes
-// accumulate the packed J^T J and J^T r in FP32 per lane and r^2 in FP64,
+// specular core once for both ordered pairs (sym_pair).  Every pass evaluates
+// the residual and the Jacobian (a trial point's Jacobian is the next one when
+// the step is accepted, and most are) and accumulates the packed J^T J and J^T r in FP32 per lane and r^2 in FP64,
 // reduce them within the warp (reduce-scatter), and the control warp sums the
 // warps in FP64.  The LM control follows fitting.hh: the damped normal
 // equations by Cholesky, the small-step and gradient tests and the gain-ratio
@@ -151,7 +153,7 @@ __device__ __forceinline__ bool lm_restart(LmState& st, const LmConfig& cfg, dou
 // parameter at 0 for good; its central difference at exactly 0 (fitting.hh:
 // 896-905, step 1e-8) is below float resolution there.  False when the
 // factorisation fails.
-__device__ bool lm_solve(LmState& st)
+__device__ __noinline__ bool lm_solve(LmState& st)
 {
     uint32_t frozen = 0;
     for(int round = 0; round < 5; ++round)
@@ -358,24 +360,29 @@ struct PassConst
 
 __host__ __device__ inline uint32_t pad4(uint32_t x) { return (x + 3u) & ~3u; }
 
-// Entry layout (12 floats): a0 a1 a2 sp | dsp0..3 | dsp4 kv up kdc.  The
-// directions themselves are not kept: R is orthonormal, so |w_i + w_o| = |s|
-// and cos(h, w_i) = s.a_i / |s| with s = a_i + a_o.  Built by the 32 lanes of
-// the control warp.
+// Table layout: three float4 arrays of pad4(L) entries (16-byte stride, so 8
+// lanes reading 8 consecutive directions hit 32 distinct banks):
+//   core0[d] = (a0, a1, a2, sp), core1[d] = (kspec kv, up, kdc, dsp4),
+//   deriv[d] = (dsp0, dsp1, dsp2, dsp3)
+// The directions themselves are not
+// kept: R is orthonormal, so |w_i + w_o| = |s| and cos(h, w_i) = s.a_i / |s|
+// with s = a_i + a_o.  Built by the 32 lanes of the control warp.
 __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32_t L, const float* pf, PassConst* pc,
                                             uint32_t lane)
 {
     ParamSet ps;
     make_param_set(pf, ps);
+    float4* core0 = reinterpret_cast<float4*>(tab);
+    float4* core1 = core0 + pad4(L);
+    float4* deriv = core1 + pad4(L);
     for(uint32_t d = lane; d < L; d += 32)
     {
         const float wx = geo[d], wy = geo[L + d], wz = geo[2 * L + d];
         DirEntry e;
         make_dir_entry(ps, wx, wy, wz, e);
-        float4* t = reinterpret_cast<float4*>(tab + kEntry * d);
-        t[0] = make_float4(e.a[0], e.a[1], e.a[2], e.sp);
-        t[1] = make_float4(e.dsp[0], e.dsp[1], e.dsp[2], e.dsp[3]);
-        t[2] = make_float4(e.dsp[4], ps.kspec * e.kv, e.up, e.kdc);
+        core0[d] = make_float4(e.a[0], e.a[1], e.a[2], e.sp);
+        core1[d] = make_float4(ps.kspec * e.kv, e.up, e.kdc, e.dsp[4]);
+        deriv[d] = make_float4(e.dsp[0], e.dsp[1], e.dsp[2], e.dsp[3]);
     }
     if(lane == 0)
     {
@@ -408,11 +415,12 @@ __device__ __forceinline__ float rcp_approx(float x)
     return r;
 }
 
-__device__ __forceinline__ Entry load_entry(const float* tab, uint32_t d)
+// Loads a direction's entry.
+__device__ __forceinline__ Entry load_entry(const float* tab, uint32_t Lp, uint32_t d)
 {
-    const float4* t = reinterpret_cast<const float4*>(tab + kEntry * d);
-    const float4 x = t[0], y = t[1], z = t[2];
-    return Entry{ x.x, x.y, x.z, x.w, y.x, y.y, y.z, y.w, z.x, z.y, z.z, z.w };
+    const float4* core0 = reinterpret_cast<const float4*>(tab);
+    const float4 x = core0[d], y = core0[Lp + d], z = core0[2 * Lp + d];
+    return Entry{ x.x, x.y, x.z, x.w, z.x, z.y, z.z, z.w, y.w, y.x, y.y, y.z };
 }
 
 // Warp reduce-scatter of 32 values: on return v[0] of lane j holds the warp's
@@ -465,11 +473,13 @@ __device__ __forceinline__ double warp_sum(double x)
 // unordered pair.  On the diagonal (a = b) the second ordered pair has zero
 // weights.
 //
-// Enumeration: unordered pair f -> offset d = f / L, view a = f mod L,
-// light b = (a + d) mod L, for d = 0 .. L/2; for even L the offset L/2 is
-// taken only for a < L/2.  Consecutive lanes take consecutive f, so their
-// table entries fall in distinct shared-memory banks.
-template <bool kJac, bool kFresnel>
+// Enumeration: unordered pair f -> view a = f / nd, offset d = f mod nd
+// (nd = L/2 + 1), light b = (a + d) mod L; for even L the offset L/2 is taken
+// only for a < L/2.  A warp's 32 consecutive f span at most two views a (the
+// entry of a is a broadcast), consecutive lights b (distinct banks), slab
+// elements a L + b (consecutive) and b L + a (stride L: distinct banks for
+// odd L).
+template <bool kFresnel>
 __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, const Entry& eb, float refr, float y1,
                                          float y2, float wt1, float wt2, float* acc, double& r2)
 {
@@ -497,7 +507,6 @@ __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, co
     const float r2b = y2 - (c.kd * h2 + c.ks * sp2);
     r2 = fma((double)r1, (double)r1, r2);
     r2 = fma((double)r2b, (double)r2b, r2);
-    if(kJac)
     {
         const float rQ = Q * S * rden;   // 1/Q
         const float rS = QQ * rden;      // 1/S
@@ -555,27 +564,27 @@ __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, co
 
 // One worker warp's share of a pass over the pairs of a slot (unordered pairs
 // wtid, wtid + 32 NW, ...).  Writes the warp's partial sums: J^T J and J^T r
-// (Jacobian passes) to red[wwarp][0..34] and r^2 to redd[wwarp].  Every lane
+// to red[wwarp][0..34] and r^2 to redd[wwarp].  Every lane
 // runs the same number of iterations; slots past the enumeration and the
 // repeated offset of an even L carry zero weights and y = 0, so they add
 // exactly 0.
-template <int NW, bool kJac, bool kFresnel>
+template <int NW, bool kFresnel>
 __device__ void worker_pass(const float* tab, const PassConst& c, const float* slab, uint32_t L, float refr,
                             float* red, double* redd, uint32_t wwarp, uint32_t lane)
 {
     static_assert(kRed == 35, "reduction layout: 32 reduce-scattered sums + 3");
     constexpr uint32_t kStride = 32u * NW;
-    const uint32_t half = L >> 1;
-    const uint32_t total = L * (half + 1);
+    const uint32_t half = L >> 1, nd = half + 1, Lp = pad4(L);
+    const uint32_t total = L * nd;
     const uint32_t iters = (total + kStride - 1) / kStride;
-    const uint32_t sd = kStride / L, sv = kStride - sd * L;
+    const uint32_t sa = kStride / nd, sd = kStride - sa * nd;
     uint32_t f = wwarp * 32u + lane;
-    uint32_t d = f / L, a = f - d * L;
+    uint32_t a = f / nd, d = f - a * nd;
 
     double r2 = 0.0;
-    float acc[kJac ? kRed : 1];
+    float acc[kRed];
 #pragma unroll
-    for(int i = 0; i < (kJac ? kRed : 1); ++i)
+    for(int i = 0; i < kRed; ++i)
         acc[i] = 0.0f;
 
     for(uint32_t it = 0; it < iters; ++it)
@@ -584,25 +593,24 @@ __device__ void worker_pass(const float* tab, const PassConst& c, const float* s
         uint32_t b = a + d;
         b = b >= L ? b - L : b;
         const uint32_t ia = valid ? a : 0u, ib = valid ? b : 0u;
-        const Entry ea = load_entry(tab, ia);
-        const Entry eb = load_entry(tab, ib);
+        const Entry ea = load_entry(tab, Lp, ia);
+        const Entry eb = load_entry(tab, Lp, ib);
         // pair 1: view a, light b (slab row a); pair 2: view b, light a
         const float y1 = valid ? slab[ia * L + ib] : 0.0f;
         const bool two = valid && d != 0u;
         const float y2 = two ? slab[ib * L + ia] : 0.0f;
-        sym_pair<kJac, kFresnel>(c, ea, eb, refr, y1, y2, valid ? 1.0f : 0.0f, two ? 1.0f : 0.0f, acc, r2);
+        sym_pair<kFresnel>(c, ea, eb, refr, y1, y2, valid ? 1.0f : 0.0f, two ? 1.0f : 0.0f, acc, r2);
         f += kStride;
-        a += sv;
+        a += sa;
         d += sd;
-        if(a >= L)
+        if(d >= nd)
         {
-            a -= L;
-            ++d;
+            d -= nd;
+            ++a;
         }
     }
 
     r2 = warp_sum(r2);
-    if(kJac)
     {
         const float t32 = warp_sum(acc[32]), t33 = warp_sum(acc[33]), t34 = warp_sum(acc[34]);
         reduce_scatter32(acc, lane);
@@ -625,8 +633,7 @@ __device__ void worker_pass(const float* tab, const PassConst& c, const float* s
 enum : int
 {
     kSlotIdle = 0,       // no pass (no texel, or its slab is still arriving)
-    kSlotJacobian = 1,   // J^T J, J^T r and r^2 at the tabulated point
-    kSlotTrial = 2,      // r^2 at the tabulated point
+    kSlotPass = 1,       // J^T J, J^T r and r^2 at the tabulated point
     kSlotExit = 3
 };
 
@@ -643,9 +650,10 @@ struct Slot
     uint32_t texel;       // texel in the slot, or kNoTexel
     uint32_t parity;      // next phase of `bar`
     int cmd;              // command of the pass the workers run next
-    int first;            // the pending Jacobian is the texel's first
+    int first;            // the pending pass is at the texel's initial point (else at a trial point)
     int loading;          // the slab copy of `texel` is in flight
     int dead;             // a copy did not arrive: the slot takes no more texels
+    uint32_t arrived;     // worker warps done with the current pass (the last one sums)
 };
 
 // Dynamic shared memory per slot: [stride] slab | [Lp][kEntry] table |
@@ -781,8 +789,30 @@ __device__ __forceinline__ bool slot_start(const LmArgs& args, Slot& sl)
     st.iter = st.eff = st.njac = st.nres = st.status = 0;
     st.restarts_left = args.cfg.restarts;
     sl.first = 1;
-    sl.cmd = kSlotJacobian;
+    sl.cmd = kSlotPass;
     return true;
+}
+
+// FP64 sums of the worker warps' partials, one lane per sum, warps in order.
+template <int NW>
+__device__ __forceinline__ void sum_partials(const float* red, const double* redd, double* sums, uint32_t lane)
+{
+    for(uint32_t i = lane; i < (uint32_t)kRed; i += 32)
+    {
+        double t = 0.0;
+#pragma unroll
+        for(int w = 0; w < NW; ++w)
+            t += (double)red[w * kRed + i];
+        sums[i] = t;
+    }
+    if(lane == 0)
+    {
+        double t = 0.0;
+#pragma unroll
+        for(int w = 0; w < NW; ++w)
+            t += redd[w];
+        sums[kRed] = t;
+    }
 }
 
 // Resident CTAs per SM the register budget is sized for.
@@ -819,12 +849,30 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
             const int cmd = slots[s].cmd;
             if(cmd == kSlotExit)
                 break;
-            if(cmd == kSlotJacobian)
-                worker_pass<NW, true, kFresnel>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
-                                          redd_of(s), wwarp, lane);
-            else if(cmd == kSlotTrial)
-                worker_pass<NW, false, kFresnel>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
-                                           redd_of(s), wwarp, lane);
+            if(cmd == kSlotPass)
+            {
+                worker_pass<NW, kFresnel>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
+                                                redd_of(s), wwarp, lane);
+                // the last worker warp to finish sums the partials in FP64, in warp
+                // order (deterministic), while the others move on
+                __syncwarp();
+                uint32_t prior = 0;
+                if(lane == 0)
+                {
+                    __threadfence_block();   // release this warp's partials
+                    prior = atomicAdd(&slots[s].arrived, 1u);
+                    __threadfence_block();   // acquire the other warps' partials
+                }
+                prior = __shfl_sync(0xffffffffu, prior, 0);
+                if(prior == NW - 1)
+                {
+                    __syncwarp();
+                    sum_partials<NW>(red_of(s), redd_of(s), slots[s].sums, lane);
+                    if(lane == 0)
+                        slots[s].arrived = 0;
+                    __syncwarp();
+                }
+            }
             nbar_arrive(bar_done<S>(s), kThreads);
         }
         return;
@@ -839,6 +887,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
             mbar_init(&sl.bar, 1);
             sl.parity = 0;
             sl.dead = 0;
+            sl.arrived = 0;
             slot_fetch(args, sl, slab_of(s), slab_bytes);
         }
         for(int s = 0; s < S; ++s)
@@ -848,7 +897,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
     __syncwarp();
     for(int s = 0; s < S; ++s)
     {
-        if(slots[s].cmd == kSlotJacobian)
+        if(slots[s].cmd == kSlotPass)
             build_table(tab_of(s), args.geo, L, slots[s].pf, &slots[s].pc, lane);
         __syncwarp();
         nbar_arrive(bar_ready(s), kThreads);
@@ -858,48 +907,19 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
     {
         Slot& sl = slots[s];
         nbar_sync(bar_done<S>(s), kThreads);
-        const int done_cmd = sl.cmd;
-        // FP64 sums of the workers' partials, one lane per sum
-        if(done_cmd == kSlotJacobian)
-        {
-            const float* red = red_of(s);
-            const double* redd = redd_of(s);
-            for(uint32_t i = lane; i <= (uint32_t)kRed; i += 32)
-            {
-                double t = 0.0;
-                if(i < (uint32_t)kRed)
-                {
-#pragma unroll
-                    for(int w = 0; w < NW; ++w)
-                        t += (double)red[w * kRed + i];
-                }
-                else
-                {
-#pragma unroll
-                    for(int w = 0; w < NW; ++w)
-                        t += redd[w];
-                }
-                sl.sums[i] = t;
-            }
-        }
-        else if(done_cmd == kSlotTrial && lane == 0)
-        {
-            const double* redd = redd_of(s);
-            double t = 0.0;
-#pragma unroll
-            for(int w = 0; w < NW; ++w)
-                t += redd[w];
-            sl.sums[kRed] = t;
-        }
-        __syncwarp();
+        const int done_cmd = sl.cmd;   // the last worker warp has left the sums in sl.sums
 
         bool build = false, exit_now = false;
         if(lane == 0)
         {
             LmState& st = sl.st;
             int next = kCmdDone;
-            if(done_cmd == kSlotJacobian)
+            if(done_cmd == kSlotPass)
             {
+                // Every pass evaluates J^T J and J^T r with r^2: at a trial point
+                // the Jacobian of an accepted step is then already at hand, so
+                // the separate Jacobian evaluation of fitting.hh:612-616 at the
+                // same point is not repeated (same arithmetic, same result).
                 if(sl.first)
                 {
                     sl.first = 0;
@@ -917,14 +937,11 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                     next = kCmdContinue;
                 }
                 else
-                    next = lm_after_jacobian(st, args.cfg, sl.sums, n_pairs);
-            }
-            else if(done_cmd == kSlotTrial)
-            {
-                next = lm_after_trial(st, args.cfg, sl.sums[kRed], n_pairs);
-            }
-            if(done_cmd == kSlotJacobian || done_cmd == kSlotTrial)
-            {
+                {
+                    next = lm_after_trial(st, args.cfg, sl.sums[kRed], n_pairs);
+                    if(next == kCmdJacobian)
+                        next = lm_after_jacobian(st, args.cfg, sl.sums, n_pairs);
+                }
                 if(next == kCmdContinue)
                     next = lm_next(st, args.cfg, n_pairs);
                 if(next == kCmdTrial)
@@ -932,13 +949,8 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
 #pragma unroll
                     for(int i = 0; i < kParams; ++i)
                         sl.pf[i] = (float)st.pt[i];
-                    sl.cmd = kSlotTrial;
+                    sl.cmd = kSlotPass;
                     build = true;
-                }
-                else if(next == kCmdJacobian)
-                {
-                    // the table built for the trial point is the accepted point's
-                    sl.cmd = kSlotJacobian;
                 }
                 else
                 {

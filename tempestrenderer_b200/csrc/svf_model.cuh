@@ -56,6 +56,17 @@ struct ParamSet
     float kspec;            // F-free lobe constant 1/(4 pi sx sy), 0 when the lobe is off
 };
 
+// Reciprocal for the table set-up: the device's fast division (about 2 ulp;
+// the table terms need no correctly rounded divide), IEEE on the host.
+SVF_HD float rcp_model(float x)
+{
+#if defined(__CUDA_ARCH__)
+    return __fdividef(1.0f, x);
+#else
+    return 1.0f / x;
+#endif
+}
+
 SVF_HD void sincos_f(float x, float* s, float* c)
 {
 #if defined(__CUDA_ARCH__)
@@ -96,7 +107,7 @@ SVF_HD void make_param_set(const float* p, ParamSet& ps)
           0.5f * (c1 * c2 * c3 - s1 * s2 * s3), 0.5f * (-c1 * c2 * s3 - s1 * s2 * c3) } };
     // the lobe uses ToMatrix3(Normalize(q)) (ggx-models-impl.hh:520)
     float ql = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-    float rq = 1.0f / ql;
+    float rq = rcp_model(ql);
     float x = q[0] * rq, y = q[1] * rq, z = q[2] * rq, w = q[3] * rq;
     float* R = ps.R;
     R[0] = 1.0f - 2.0f * (y * y + z * z); R[1] = 2.0f * (x * y + z * w);        R[2] = 2.0f * (x * z - y * w);
@@ -125,15 +136,17 @@ SVF_HD void make_param_set(const float* p, ParamSet& ps)
     }
 
     bool lobe = ps.sx >= 1e-6f && ps.sy >= 1e-6f;
-    float u = lobe ? 1.0f / (ps.sx * ps.sx) : 0.0f;
-    float v = lobe ? 1.0f / (ps.sy * ps.sy) : 0.0f;
+    float rsx = lobe ? rcp_model(ps.sx) : 0.0f;
+    float rsy = lobe ? rcp_model(ps.sy) : 0.0f;
+    float u = rsx * rsx;
+    float v = rsy * rsy;
     // det S^-1 = u v (ggx-models-impl.hh:53-54 drops the lobe below 1e-6)
     lobe = lobe && (u * v >= 1e-6f);
     ps.u = u;
     ps.v = v;
-    ps.rsx = lobe ? 1.0f / ps.sx : 0.0f;
-    ps.rsy = lobe ? 1.0f / ps.sy : 0.0f;
-    ps.kspec = lobe ? 0.25f / (kRefPi * ps.sx * ps.sy) : 0.0f;
+    ps.rsx = lobe ? rsx : 0.0f;
+    ps.rsy = lobe ? rsy : 0.0f;
+    ps.kspec = lobe ? (0.25f / kRefPi) * rsx * rsy : 0.0f;
 }
 
 // Per-direction table entry for one parameter set.
@@ -157,15 +170,21 @@ SVF_HD void make_dir_entry(const ParamSet& ps, float wx, float wy, float wz, Dir
     e.a[1] = a1;
     e.a[2] = a2;
     float sx2 = ps.sx * ps.sx, sy2 = ps.sy * ps.sy;
-    float sig = sqrtf(sx2 * a0 * a0 + sy2 * a1 * a1 + a2 * a2);
+    float sig2 = sx2 * a0 * a0 + sy2 * a1 * a1 + a2 * a2;
+#if defined(__CUDA_ARCH__)
+    float rsig = sig2 > 0.0f ? rsqrtf(sig2) : 0.0f;
+    float sig = sig2 * rsig;
+#else
+    float sig = sqrtf(sig2);
+    float rsig = sig > 0.0f ? 1.0f / sig : 0.0f;
+#endif
     bool up = wz > 0.0f;
     float c = up ? wz : 1.0f;
-    float rc = 1.0f / c;
+    float rc = rcp_model(c);
     e.kdc = up ? wz * (1.0f / kRefPi) : 0.0f;
     e.kv = (up && sig >= 1e-6f) ? rc : 0.0f;
     e.up = up ? 1.0f : 0.0f;
     e.sp = sig * rc;
-    float rsig = sig > 0.0f ? 1.0f / sig : 0.0f;
     float k = rsig * rc;
     e.dsp[0] = ps.sx * a0 * a0 * k;
     e.dsp[1] = ps.sy * a1 * a1 * k;
