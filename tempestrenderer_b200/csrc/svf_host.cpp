@@ -158,6 +158,7 @@ struct Layout
     uint32_t L = 0;
     std::vector<float> lp;
     DevBuf geo;                 // [3][L] Cartesian directions (LM)
+    bool all_up = false;        // every direction has z > 0 (LM kernel specialisation)
     std::map<uint64_t, std::unique_ptr<InitData>> inits;
     bool tuned = false;         // LM kernel configuration chosen by the autotuner
     svf::LmKernelChoice choice{ 0, 0 };
@@ -239,6 +240,9 @@ svf_status get_layout(svf_ctx* ctx, const float* lp_in, uint32_t L, Layout** out
             geo[L + d] = w[1];
             geo[2 * L + d] = w[2];
         }
+        lay->all_up = true;
+        for(uint32_t d = 0; d < L; ++d)
+            lay->all_up = lay->all_up && geo[2 * L + d] > 0.0f;
         SVF_TRY(lay->geo.ensure(sizeof(float) * 3 * L));
         SVF_CUDA(cudaMemcpy(lay->geo.p, geo.data(), sizeof(float) * 3 * L, cudaMemcpyHostToDevice));
         it = ctx->layouts.emplace(key, std::move(lay)).first;
@@ -524,6 +528,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     a.map_sigma = r.sigma;
     a.map_basis = r.basis;
     a.L = lay->L;
+    a.all_up = lay->all_up ? 1u : 0u;
     a.N = lay->L * lay->L;
     a.texels = (uint32_t)r.texels;
     a.cfg.max_iter = o->max_iterations;

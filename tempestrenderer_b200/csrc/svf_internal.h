@@ -36,6 +36,7 @@ struct LmArgs
     float* map_sigma;          // [texels][2] or null
     float* map_basis;          // [texels][4] or null
     uint32_t L, N, texels;
+    uint32_t all_up;           // every direction has z > 0
     LmConfig cfg;
     uint32_t* work_counter;    // zeroed before the launch
     uint32_t* error_flag;      // set non-zero by a bounded wait that expired

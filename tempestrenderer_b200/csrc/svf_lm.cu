@@ -479,7 +479,7 @@ __device__ __forceinline__ double warp_sum(double x)
 // entry of a is a broadcast), consecutive lights b (distinct banks), slab
 // elements a L + b (consecutive) and b L + a (stride L: distinct banks for
 // odd L).
-template <bool kFresnel>
+template <bool kFresnel, bool kAllUp>
 __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, const Entry& eb, float refr, float y1,
                                          float y2, float wt1, float wt2, float* acc, double& r2)
 {
@@ -500,8 +500,11 @@ __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, co
     }
     const float C = F * g * g * rden;
     // ordered pair 1: view a, light b; ordered pair 2: view b, light a
-    const float w1 = wt1 * ea.kv * eb.up, w2 = wt2 * eb.kv * ea.up;
-    const float h1 = wt1 * ea.up * eb.kdc, h2 = wt2 * eb.up * ea.kdc;
+    // (with every direction above the horizon the up factors are 1)
+    const float w1 = kAllUp ? wt1 * ea.kv : wt1 * ea.kv * eb.up;
+    const float w2 = kAllUp ? wt2 * eb.kv : wt2 * eb.kv * ea.up;
+    const float h1 = kAllUp ? wt1 * eb.kdc : wt1 * ea.up * eb.kdc;
+    const float h2 = kAllUp ? wt2 * ea.kdc : wt2 * eb.up * ea.kdc;
     const float sp1 = w1 * C, sp2 = w2 * C;
     const float r1 = y1 - (c.kd * h1 + c.ks * sp1);
     const float r2b = y2 - (c.kd * h2 + c.ks * sp2);
@@ -562,13 +565,42 @@ __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, co
     }
 }
 
+// One step of a worker lane over its unordered pairs: pair f = (a, d), then
+// f += 32 NW.  kGuard: f may be past the enumeration or, for even L, on the
+// repeated offset L/2 (such slots get zero weights, y = 0 and in-range
+// indices); without it every pair is valid (odd L, f < total).
+template <int NW, bool kFresnel, bool kAllUp, bool kGuard>
+__device__ __forceinline__ void pair_step(const float* tab, const PassConst& c, const float* slab, uint32_t L,
+                                          uint32_t Lp, uint32_t nd, uint32_t total, uint32_t sa, uint32_t sd, float refr,
+                                          uint32_t& f, uint32_t& a, uint32_t& d, float* acc, double& r2)
+{
+    const bool valid = !kGuard || (f < total && !(2u * d == L && a >= (L >> 1)));
+    uint32_t b = a + d;
+    b = b >= L ? b - L : b;
+    const uint32_t ia = valid ? a : 0u, ib = valid ? b : 0u;
+    const Entry ea = load_entry(tab, Lp, ia);
+    const Entry eb = load_entry(tab, Lp, ib);
+    // pair 1: view a, light b (slab row a); pair 2: view b, light a
+    const float y1 = valid ? slab[ia * L + ib] : 0.0f;
+    const bool two = valid && d != 0u;
+    const float y2 = two ? slab[ib * L + ia] : 0.0f;
+    sym_pair<kFresnel, kAllUp>(c, ea, eb, refr, y1, y2, kGuard ? (valid ? 1.0f : 0.0f) : 1.0f, two ? 1.0f : 0.0f,
+                               acc, r2);
+    f += 32u * NW;
+    a += sa;
+    d += sd;
+    if(d >= nd)
+    {
+        d -= nd;
+        ++a;
+    }
+}
+
 // One worker warp's share of a pass over the pairs of a slot (unordered pairs
 // wtid, wtid + 32 NW, ...).  Writes the warp's partial sums: J^T J and J^T r
-// to red[wwarp][0..34] and r^2 to redd[wwarp].  Every lane
-// runs the same number of iterations; slots past the enumeration and the
-// repeated offset of an even L carry zero weights and y = 0, so they add
-// exactly 0.
-template <int NW, bool kFresnel>
+// to red[wwarp][0..34] and r^2 to redd[wwarp].  Every lane runs the same
+// number of steps; for odd L only the last one needs the guard.
+template <int NW, bool kFresnel, bool kAllUp>
 __device__ void worker_pass(const float* tab, const PassConst& c, const float* slab, uint32_t L, float refr,
                             float* red, double* redd, uint32_t wwarp, uint32_t lane)
 {
@@ -577,6 +609,7 @@ __device__ void worker_pass(const float* tab, const PassConst& c, const float* s
     const uint32_t half = L >> 1, nd = half + 1, Lp = pad4(L);
     const uint32_t total = L * nd;
     const uint32_t iters = (total + kStride - 1) / kStride;
+    const uint32_t full = (L & 1u) ? total / kStride : 0u;   // steps with every pair valid
     const uint32_t sa = kStride / nd, sd = kStride - sa * nd;
     uint32_t f = wwarp * 32u + lane;
     uint32_t a = f / nd, d = f - a * nd;
@@ -587,28 +620,10 @@ __device__ void worker_pass(const float* tab, const PassConst& c, const float* s
     for(int i = 0; i < kRed; ++i)
         acc[i] = 0.0f;
 
-    for(uint32_t it = 0; it < iters; ++it)
-    {
-        const bool valid = f < total && !(2u * d == L && a >= half);
-        uint32_t b = a + d;
-        b = b >= L ? b - L : b;
-        const uint32_t ia = valid ? a : 0u, ib = valid ? b : 0u;
-        const Entry ea = load_entry(tab, Lp, ia);
-        const Entry eb = load_entry(tab, Lp, ib);
-        // pair 1: view a, light b (slab row a); pair 2: view b, light a
-        const float y1 = valid ? slab[ia * L + ib] : 0.0f;
-        const bool two = valid && d != 0u;
-        const float y2 = two ? slab[ib * L + ia] : 0.0f;
-        sym_pair<kFresnel>(c, ea, eb, refr, y1, y2, valid ? 1.0f : 0.0f, two ? 1.0f : 0.0f, acc, r2);
-        f += kStride;
-        a += sa;
-        d += sd;
-        if(d >= nd)
-        {
-            d -= nd;
-            ++a;
-        }
-    }
+    for(uint32_t it = 0; it < full; ++it)
+        pair_step<NW, kFresnel, kAllUp, false>(tab, c, slab, L, Lp, nd, total, sa, sd, refr, f, a, d, acc, r2);
+    for(uint32_t it = full; it < iters; ++it)
+        pair_step<NW, kFresnel, kAllUp, true>(tab, c, slab, L, Lp, nd, total, sa, sd, refr, f, a, d, acc, r2);
 
     r2 = warp_sum(r2);
     {
@@ -818,7 +833,7 @@ __device__ __forceinline__ void sum_partials(const float* red, const double* red
 // Resident CTAs per SM the register budget is sized for.
 constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : 2; }
 
-template <int NW, int S, bool kFresnel>
+template <int NW, int S, bool kFresnel, bool kAllUp>
 __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_fit_kernel(LmArgs args)
 {
     constexpr uint32_t kThreads = 32 * (NW + 1);
@@ -851,7 +866,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 break;
             if(cmd == kSlotPass)
             {
-                worker_pass<NW, kFresnel>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
+                worker_pass<NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
                                                 redd_of(s), wwarp, lane);
                 // the last worker warp to finish sums the partials in FP64, in warp
                 // order (deterministic), while the others move on
@@ -995,16 +1010,24 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
 
 using KernelFn = void (*)(LmArgs);
 
-KernelFn kernel_for(LmKernelChoice c, bool fresnel)
+template <int NW, int S>
+KernelFn pick(bool fresnel, bool all_up)
+{
+    if(fresnel)
+        return all_up ? lm_fit_kernel<NW, S, true, true> : lm_fit_kernel<NW, S, true, false>;
+    return all_up ? lm_fit_kernel<NW, S, false, true> : lm_fit_kernel<NW, S, false, false>;
+}
+
+KernelFn kernel_for(LmKernelChoice c, bool fresnel, bool all_up)
 {
     if(c.threads == 256 && c.slots == 2)
-        return fresnel ? lm_fit_kernel<7, 2, true> : lm_fit_kernel<7, 2, false>;
+        return pick<7, 2>(fresnel, all_up);
     if(c.threads == 256 && c.slots == 3)
-        return fresnel ? lm_fit_kernel<7, 3, true> : lm_fit_kernel<7, 3, false>;
+        return pick<7, 3>(fresnel, all_up);
     if(c.threads == 128 && c.slots == 2)
-        return fresnel ? lm_fit_kernel<3, 2, true> : lm_fit_kernel<3, 2, false>;
+        return pick<3, 2>(fresnel, all_up);
     if(c.threads == 128 && c.slots == 3)
-        return fresnel ? lm_fit_kernel<3, 3, true> : lm_fit_kernel<3, 3, false>;
+        return pick<3, 3>(fresnel, all_up);
     return nullptr;
 }
 
@@ -1032,8 +1055,8 @@ size_t lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
 
 int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
 {
-    // the Fresnel and Fresnel-free variants share registers and shared memory
-    KernelFn k = kernel_for(c, false);
+    // the variants share the launch configuration
+    KernelFn k = kernel_for(c, false, false);
     if(!k || L == 0)
         return 0;
     const size_t smem = lm_smem_bytes(L, lum_stride, c);
@@ -1054,7 +1077,7 @@ int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
 
 cudaError_t launch_lm_fit(const LmArgs& args, LmKernelChoice c, int grid, cudaStream_t stream)
 {
-    KernelFn k = kernel_for(c, args.cfg.fresnel != 1.0f);
+    KernelFn k = kernel_for(c, args.cfg.fresnel != 1.0f, args.all_up != 0);
     if(!k || args.L == 0)
         return cudaErrorInvalidConfiguration;
     const size_t smem = lm_smem_bytes(args.L, args.lum_stride, c);
