@@ -16,7 +16,10 @@ reference's default initial guess (NDF -> PCA -> SGGX projection), LM
   region.
 * roofline: the LM kernel (the dominant kernel) against the FP32 CUDA-core peak
   (SMs x 128 lanes x 2 flops x SM clock sampled under load), with its
-  algorithmic flops counted per pair evaluation.
+  algorithmic flops counted per ordered direction pair (see DESIGN.md);
+  traffic from the ncu capture summarised in profiles/.
+* roofline_ndf: the NDF GEMM of the default initial guess (tcgen05 tensor
+  cores) against the measured BF16 peak in MEASURED_PEAKS.json.
 * cpu_baseline: the reference's own CPU fitter (oracle/_ref, compiled from the
   reference's sources) on a bounded sample of the same texels, all host cores.
 
@@ -40,10 +43,21 @@ sys.path.insert(0, HERE)
 METRIC = "fitted texels/s (81x81 dirs) at residual <=1.01x plain LM; % of FP32/HBM peak"
 SEED, MIX = 2024, 1
 WIDTH = HEIGHT = 400
-# flops per direction-pair evaluation of the LM kernel (FMA = 2), counted from
-# svf_model.cuh::eval_pair and the accumulation in svf_kernels.cu::pair_pass
+# Algorithmic flops of an analytic-Jacobian LM per ordered direction pair (FMA = 2),
+# counted from svf_model.cuh::eval_pair plus the packed J^T J / J^T r accumulation:
+# a Jacobian evaluation (accepted steps and the start point) and a residual
+# evaluation (every trial).  The kernel evaluates the specular core once per
+# unordered pair (svf_lm.cu::sym_pair), so it executes fewer.
 FLOPS_JACOBIAN_PASS = 169
 FLOPS_RESIDUAL_PASS = 33
+# DRAM bytes per texel of lm_fit_kernel, measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum = 675.3 MB + 6.6 MB for 25600 texels; the luminance slab
+# is read once): profiles/lm_fit_kernel_160x160_ring81.md.
+LM_DRAM_BYTES_PER_TEXEL = (675.3e6 + 6.6e6) / 25600
+# DRAM bytes per texel of ndf_tc_kernel, measured by ncu (2.30 GB + 335 MB for
+# 25600 texels): profiles/ndf_tc_kernel_160x160_ring81.md.
+NDF_DRAM_BYTES_PER_TEXEL = (2.30e9 + 335e6) / 25600
+NDF_ROWS, NDF_ROWS_PAD = 3217, 3328   # 64x64 NDF texels inside the hemisphere, padded to the tile
 
 
 def log(*a):
@@ -220,6 +234,7 @@ def run_ours(args):
     ms = float(sum(s.ms_total for s in stats))
     ms_fit = float(sum(s.ms_fit for s in stats))
     ms_init = float(sum(s.ms_init for s in stats))
+    ms_ndf = float(sum(s.ms_ndf for s in stats))
     ms_lum = float(sum(s.ms_luminance for s in stats))
     jac = sum(s.jacobians for s in stats)
     res = sum(s.residuals for s in stats)
@@ -267,6 +282,11 @@ def run_ours(args):
         fp32_peak = props.multi_processor_count * 128 * 2 * sm_mhz * 1e6 / 1e12   # TFLOP/s at the sampled clock
         lm_flops = N * (FLOPS_JACOBIAN_PASS * jac + FLOPS_RESIDUAL_PASS * res)
         achieved = lm_flops / (ms_fit / 1e3) / 1e12
+        bf16_peak = peaks.get("bf16_tflops")
+        kp = (N + 7) // 8 * 8
+        ndf_alg = 2.0 * T * NDF_ROWS * N * args.steps               # one FP32 GEMM
+        ndf_hw = 2.0 * T * NDF_ROWS_PAD * ((kp + 63) // 64 * 64) * 3 * args.steps   # BF16x3, padded tiles
+        ndf_ach = ndf_alg / (ms_ndf / 1e3) / 1e12 if ms_ndf > 0 else None
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
             try:
@@ -286,11 +306,22 @@ def run_ours(args):
                        "texels_per_gpu": T, "l2": "inputs 12.6 GB per GPU, larger than L2",
                        "parallelism": f"texel shards x{world}"},
             "roofline": {"bound": "fp32", "kernel": "lm_fit_kernel", "achieved": achieved, "peak": fp32_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+                         "traffic": LM_DRAM_BYTES_PER_TEXEL * T,
+                         "traffic_source": "ncu dram bytes per texel (profiles/lm_fit_kernel_160x160_ring81.md) x texels",
                          "peak_source": f"derived: {props.multi_processor_count} SMs x 128 FP32 lanes x 2 x "
-                                        f"{sm_mhz:.0f} MHz (sampled SM clock under load)"},
+                                        f"{sm_mhz:.0f} MHz (sampled SM clock under load); MEASURED_PEAKS.json "
+                                        f"has no FP32 figure"},
+            "roofline_ndf": None if ndf_ach is None or not bf16_peak else {
+                "bound": "tensor", "kernel": "ndf_tc_kernel", "achieved": ndf_ach, "peak": bf16_peak,
+                "unit": "TFLOP/s", "frac": ndf_ach / bf16_peak, "peak_source": "measured (bf16_tflops, burst)",
+                "hw_bf16_tflops": ndf_hw / (ms_ndf / 1e3) / 1e12,
+                "hw_frac": ndf_hw / (ms_ndf / 1e3) / 1e12 / bf16_peak,
+                "traffic": NDF_DRAM_BYTES_PER_TEXEL * T,
+                "note": "achieved counts one FP32 GEMM (2 x texels x 3217 x 6561); hw counts the 3 BF16 "
+                        "products over padded tiles the tensor cores execute"},
             "phases_ms": {"luminance": ms_lum / args.steps, "init": ms_init / args.steps,
-                          "lm": ms_fit / args.steps},
+                          "ndf_gemm": ms_ndf / args.steps, "lm": ms_fit / args.steps},
             "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
                         "failed_texels": failed},
             "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,

@@ -240,6 +240,7 @@ typedef struct svf_run_stats
     double   ms_copy;           /* host<->device staging, when host buffers were given */
     uint32_t lm_threads;        /* LM kernel configuration the autotuner chose: CTA size */
     uint32_t lm_slots;          /* and texels in flight per CTA */
+    double   ms_ndf;            /* the NDF GEMM of the default initial guess (part of ms_init) */
 } svf_run_stats;
 
 svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,

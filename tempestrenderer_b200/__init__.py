@@ -80,7 +80,8 @@ class RunStats(C.Structure):
     _fields_ = [("texels", C.c_uint64), ("iterations", C.c_uint64), ("jacobians", C.c_uint64),
                 ("residuals", C.c_uint64), ("failed_texels", C.c_uint64), ("ms_total", C.c_double),
                 ("ms_luminance", C.c_double), ("ms_init", C.c_double), ("ms_fit", C.c_double),
-                ("ms_copy", C.c_double), ("lm_threads", C.c_uint32), ("lm_slots", C.c_uint32)]
+                ("ms_copy", C.c_double), ("lm_threads", C.c_uint32), ("lm_slots", C.c_uint32),
+                ("ms_ndf", C.c_double)]
 
 
 _lib = None

@@ -882,8 +882,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         if(n_chunks > 1)
             SVF_TRY(ctx->samples2.ensure(texel_bytes * chunk));
     }
-    // per chunk: copy start/end (copy stream), then lum, init, LM, outputs (compute stream)
-    constexpr int kEv = 7;
+    // per chunk: copy start/end (copy stream), then lum, init, LM, outputs, NDF GEMM end (compute stream)
+    constexpr int kEv = 8;
     while(ctx->chunk_ev.size() < kEv * n_chunks)
     {
         cudaEvent_t e;
@@ -946,6 +946,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                                                ctx->stream);
             if(e != cudaSuccess)
                 return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
+            SVF_CUDA(cudaEventRecord(ev(c, 7), ctx->stream));
             SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->ndf.as<float>(), ndf_ld, n, ctx->init.as<float>(),
                                              nullptr, maps->ndf ? ctx->ndf_tex.as<float>() : nullptr, ctx->stream));
         }
@@ -1002,6 +1003,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             rs.ms_copy += span(ev(c, 0), ev(c, 1));
         rs.ms_luminance += span(ev(c, 2), ev(c, 3));
         rs.ms_init += span(ev(c, 3), ev(c, 4));
+        if(default_init)
+            rs.ms_ndf += span(ev(c, 3), ev(c, 7));
         rs.ms_fit += span(ev(c, 4), ev(c, 5));
         rs.ms_copy += span(ev(c, 5), ev(c, 6));
     }
