@@ -509,7 +509,7 @@ svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmR
 {
     if(!lay->tuned && r.texels >= 4096)
         SVF_TRY(tune_lm(ctx, lay, o));
-    return launch_lm(ctx, lay, o, r, lay->tuned ? lay->choice : svf::lm_default_choice(lay->L));
+    return launch_lm(ctx, lay, o, r, lay->tuned ? lay->choice : svf::lm_default_choice(lay->L, r.stride));
 }
 
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c)
@@ -1012,7 +1012,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     rs.ms_total = span(samples_on_device ? ev(0, 2) : ev(0, 0), ev(n_chunks - 1, 6));
     cudaGetLastError();
     rs.texels = T;
-    const svf::LmKernelChoice used = lay->tuned ? lay->choice : svf::lm_default_choice(L);
+    const svf::LmKernelChoice used = lay->tuned ? lay->choice : svf::lm_default_choice(L, stride);
     rs.lm_threads = (uint32_t)used.threads;
     rs.lm_slots = (uint32_t)used.slots;
     if(run)

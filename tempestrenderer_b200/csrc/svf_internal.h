@@ -49,7 +49,7 @@ struct LmKernelChoice
     int threads;
     int slots;
 };
-LmKernelChoice lm_default_choice(uint32_t L);
+LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride);
 int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);
 size_t         lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c);
 int            lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c);

@@ -433,7 +433,7 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
     a.cfg = cfg;
     a.work_counter = flags;
     a.error_flag = flags + 1;
-    const LmKernelChoice choice = lm_default_choice(L);
+    const LmKernelChoice choice = lm_default_choice(L, stride);
     const int per_sm = lm_max_ctas_per_sm(L, stride, choice);
     if(per_sm <= 0)
         return cudaErrorInvalidConfiguration;

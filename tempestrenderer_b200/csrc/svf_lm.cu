@@ -1033,9 +1033,15 @@ KernelFn kernel_for(LmKernelChoice c, bool fresnel, bool all_up)
 
 } // namespace
 
-LmKernelChoice lm_default_choice(uint32_t)
+LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride)
 {
-    return LmKernelChoice{ 256, 3 };
+    // the first candidate whose shared memory fits on an SM (fewer slots at large L)
+    LmKernelChoice cand[4];
+    const int n = lm_candidates(L, cand, 4);
+    for(int i = 0; i < n; ++i)
+        if(lm_max_ctas_per_sm(L, lum_stride, cand[i]) > 0)
+            return cand[i];
+    return cand[0];
 }
 
 int lm_candidates(uint32_t, LmKernelChoice* out, int max)
