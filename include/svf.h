@@ -16,6 +16,8 @@
  *                     and ::fit (svbrdf-fitting-pipeline.cc:240-733) on every
  *                     texel, i.e. luminance slice, default initial guess, LM and
  *                     the output maps (svbrdf-fitting.cc:713-735).
+ *   svf_fit_btfs      the same loop over a batch of BTFs of uneven sizes and
+ *                     layouts, sharing the persistent LM launches.
  *
  * Conventions (as in the reference):
  *   - L directions serve as both light and view directions; they are given in
@@ -245,6 +247,19 @@ typedef struct svf_run_stats
 
 svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,
                           const svf_maps* out, svf_run_stats* run /* may be NULL */);
+
+/* The texel loop over a batch of BTFs of uneven sizes and any mix of direction
+ * layouts (several svbrdffit runs, svbrdf-fitting.cc:86-121, in one call).
+ * BTF i has its own view, options (init mode and initial parameters; the lsq
+ * options must be the same for all) and maps.  Texels of up to 16 BTFs share
+ * one persistent LM launch, whatever their layouts; a slot that finishes a
+ * texel takes the next one of any BTF.  runs (optional): one svf_run_stats per
+ * BTF (texels, iterations, Jacobians, trials, failed texels; the times are the
+ * whole call's); total (optional): the whole call.  SVF_EPARTIAL when a texel
+ * of any BTF produced no finite fit. */
+svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, const svf_fit_options* options,
+                        const svf_maps* maps, svf_run_stats* runs /* [n_btf] or NULL */,
+                        svf_run_stats* total /* may be NULL */);
 
 /* Synthetic BTFs (test and benchmark inputs) ------------------------------------ */
 /* Renders texels [first, first + count) of a seeded synthetic BTF straight into

@@ -32,7 +32,8 @@ SVF_INIT_DEFAULT, SVF_INIT_GIVEN = 0, 1
 # every entry point include/svf.h declares
 EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_options_default", "svf_create",
            "svf_destroy", "svf_directions_ring81", "svf_directions_fibonacci", "svf_layout_triangulate",
-           "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc", "svf_fit_texels", "svf_synth_btf")
+           "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc", "svf_fit_texels", "svf_fit_btfs",
+           "svf_synth_btf")
 
 
 class SvfError(RuntimeError):
@@ -114,8 +115,10 @@ def load() -> C.CDLL:
         L.svf_fit_texels.argtypes = [vp, C.POINTER(BtfView), C.POINTER(FitOptions), C.POINTER(Maps),
                                      C.POINTER(RunStats)]
         L.svf_synth_btf.argtypes = [vp, u32, u32, vp, u32, u64, u64, u32, f32, vp, vp]
+        L.svf_fit_btfs.argtypes = [vp, C.POINTER(BtfView), u32, C.POINTER(FitOptions), C.POINTER(Maps),
+                                   C.POINTER(RunStats), C.POINTER(RunStats)]
         for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
-                     "svf_fit_texels", "svf_synth_btf"):
+                     "svf_fit_texels", "svf_fit_btfs", "svf_synth_btf"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -281,6 +284,41 @@ class Context:
         if check:
             _check(st)
         return res, rs
+
+    def fit_btfs(self, btfs, opts: LsqOptions | None = None, want=("diffuse", "specular", "sigma", "basis", "rmse",
+                                                                  "params", "init", "stats"), check=True):
+        """btfs: list of dicts {layout, samples, width, height[, sample_type][, init]}.  All texels go through
+        shared LM launches (svf_fit_btfs).  Returns ([maps dict per BTF], [RunStats per BTF], RunStats total)."""
+        n = len(btfs)
+        views = (BtfView * n)()
+        fos = (FitOptions * n)()
+        ms = (Maps * n)()
+        keep, results = [], []
+        for i, b in enumerate(btfs):
+            T = b["width"] * b["height"]
+            views[i].samples = _ptr(b["samples"])
+            views[i].sample_type = b.get("sample_type", SVF_SAMPLES_F32)
+            views[i].width, views[i].height = b["width"], b["height"]
+            views[i].layout = C.pointer(b["layout"].desc)
+            fos[i].lsq = opts or options()
+            init = b.get("init")
+            fos[i].init_mode = SVF_INIT_DEFAULT if init is None else SVF_INIT_GIVEN
+            if init is not None:
+                init = np.ascontiguousarray(init, np.float32)
+                keep.append(init)
+                fos[i].init_params = init.ctypes.data
+            shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
+                      "params": (T, 7), "init": (T, 7), "ndf": (T, 64 * 64)}
+            res = {k: (np.zeros(T, STATS_DTYPE) if k == "stats" else np.zeros(shapes[k], np.float32)) for k in want}
+            for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params", "init", "stats", "ndf"):
+                setattr(ms[i], k, _ptr(res[k]) if k in res else None)
+            results.append(res)
+        runs = (RunStats * n)()
+        total = RunStats()
+        st = self._lib.svf_fit_btfs(self.handle, views, n, fos, ms, runs, C.byref(total))
+        if check:
+            _check(st)
+        return results, list(runs), total
 
     def synth_btf(self, seed: int, mix: int, lights_parabolic, first: int, count: int, samples,
                   sample_type=SVF_SAMPLES_F32, noise: float = 0.01, truth=None):

@@ -389,6 +389,11 @@ struct LmRun
     const float* avg;
     float *diffuse, *specular, *sigma, *basis;
     uint64_t texels;
+    // several layouts in one launch (svf_fit_btfs): segments replace lum/stride
+    // and the layout's table; all_up over all of them
+    const svf::LmSegment* seg = nullptr;
+    uint32_t n_seg = 0;
+    bool all_up = false;
 };
 
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c);
@@ -515,9 +520,27 @@ svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmR
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c)
 {
     svf::LmArgs a{};
-    a.lum = r.lum;
-    a.lum_stride = r.stride;
-    a.geo = lay->geo.as<float>();
+    if(r.n_seg == 0)
+    {
+        a.seg[0] = svf::LmSegment{ 0, lay->L, r.stride, r.lum, lay->geo.as<float>() };
+        a.n_seg = 1;
+        a.L = lay->L;
+        a.lum_stride = r.stride;
+        a.all_up = lay->all_up ? 1u : 0u;
+    }
+    else
+    {
+        if(r.n_seg > (uint32_t)svf::kLmMaxSegments)
+            return fail(SVF_EINVAL, "internal: %u LM segments", r.n_seg);
+        a.n_seg = r.n_seg;
+        for(uint32_t i = 0; i < r.n_seg; ++i)
+        {
+            a.seg[i] = r.seg[i];
+            a.L = std::max(a.L, r.seg[i].L);
+            a.lum_stride = std::max<uint64_t>(a.lum_stride, r.seg[i].stride);
+        }
+        a.all_up = r.all_up ? 1u : 0u;
+    }
     a.init = r.init;
     a.out = r.out;
     a.rmse = r.rmse;
@@ -527,9 +550,6 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     a.map_specular = r.specular;
     a.map_sigma = r.sigma;
     a.map_basis = r.basis;
-    a.L = lay->L;
-    a.all_up = lay->all_up ? 1u : 0u;
-    a.N = lay->L * lay->L;
     a.texels = (uint32_t)r.texels;
     a.cfg.max_iter = o->max_iterations;
     a.cfg.mse_target = o->mse_target;
@@ -1019,6 +1039,305 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         *run = rs;
     if(rs.failed_texels)
         return fail(SVF_EPARTIAL, "%llu texels did not produce a finite fit", (unsigned long long)rs.failed_texels);
+    return SVF_OK;
+}
+
+svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, const svf_fit_options* opts,
+                        const svf_maps* maps, svf_run_stats* runs, svf_run_stats* total)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(n_btf == 0)
+        return SVF_OK;
+    if(!btfs || !opts || !maps)
+        return fail(SVF_EINVAL, "null btfs/options/maps");
+    SVF_TRY(check_options(&opts[0].lsq));
+
+    // per BTF: layout, default-init tables, sizes
+    struct Item
+    {
+        Layout* lay = nullptr;
+        const svf::InitLayout* init = nullptr;
+        uint64_t T = 0, stride = 0;
+        size_t texel_bytes = 0;
+        bool on_device = false, default_init = false;
+    };
+    std::vector<Item> it(n_btf);
+    for(uint32_t b = 0; b < n_btf; ++b)
+    {
+        const svf_btf_view& v = btfs[b];
+        const svf_fit_options& o = opts[b];
+        if(!v.layout || !v.samples)
+            return fail(SVF_EINVAL, "btf %u: null layout/samples", b);
+        if(v.sample_type != SVF_SAMPLES_F32 && v.sample_type != SVF_SAMPLES_F16)
+            return fail(SVF_EINVAL, "btf %u: unknown sample_type %u", b, v.sample_type);
+        if(o.init_mode != SVF_INIT_DEFAULT && o.init_mode != SVF_INIT_GIVEN)
+            return fail(SVF_EINVAL, "btf %u: unknown init_mode %u", b, o.init_mode);
+        if(o.init_mode == SVF_INIT_GIVEN && !o.init_params)
+            return fail(SVF_EINVAL, "btf %u: SVF_INIT_GIVEN needs init_params", b);
+        const svf_lsq_options &a = o.lsq, &z = opts[0].lsq;
+        if(a.max_iterations != z.max_iterations || a.fresnel != z.fresnel || a.flags != z.flags ||
+           a.mse_target != z.mse_target || a.break_on_small_step != z.break_on_small_step || a.restarts != z.restarts)
+            return fail(SVF_EINVAL, "btf %u: the lsq options must be the same for every BTF of a call", b);
+        if(maps[b].ndf && o.init_mode != SVF_INIT_DEFAULT)
+            return fail(SVF_EINVAL, "btf %u: the NDF map exists only with the default initial guess", b);
+        Item& x = it[b];
+        x.T = (uint64_t)v.width * v.height;
+        if(x.T > 0xffffffffull)
+            return fail(SVF_EINVAL, "btf %u: too many texels", b);
+        SVF_TRY(get_layout(ctx, v.layout->lights_parabolic, v.layout->light_count, &x.lay));
+        x.stride = round_up((uint64_t)x.lay->L * x.lay->L, 8);
+        x.texel_bytes = (v.sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)x.lay->L * x.lay->L;
+        x.on_device = is_device_pointer(v.samples);
+        x.default_init = o.init_mode == SVF_INIT_DEFAULT;
+        if(x.default_init)
+            SVF_TRY(prepare_init(ctx, x.lay, v.layout, &x.init));
+    }
+    uint32_t ndf_ld = 0;   // NDF rows per texel (the same for every layout: the 64x64 texture's hemisphere)
+    for(auto& x : it)
+        if(x.default_init)
+            ndf_ld = std::max(ndf_ld, x.init->ndf_rows_pad);
+
+    // Chunks of up to kLmMaxSegments pieces (runs of one BTF's texels) within a
+    // device-memory budget; each chunk is one LM launch.
+    size_t free_b = 0, total_b = 0;
+    SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = free_b / 2;
+    auto texel_cost = [&](uint32_t b) -> size_t {
+        const Item& x = it[b];
+        return sizeof(float) * (x.stride + 3 + 7 + 7 + 1 + 12) + sizeof(svf_texel_stats) +
+               (x.default_init ? 2 * 2 * x.stride + sizeof(float) * ndf_ld : 0) +
+               (maps[b].ndf ? sizeof(float) * svf::kNdfTexels : 0) + (x.on_device ? 0 : x.texel_bytes);
+    };
+    struct Piece
+    {
+        uint32_t b;
+        uint64_t first, count, k0;   // texels of BTF b; k0: position in the chunk
+        uint64_t off;                // slab offset (floats) in the chunk
+    };
+    std::vector<std::vector<Piece>> chunks(1);
+    uint64_t chunk_texels = 0, chunk_floats = 0;
+    size_t chunk_bytes = 0;
+    const uint64_t max_texels = 65535ull * 128;   // the NDF GEMM's grid rows of 128 texels
+    for(uint32_t b = 0; b < n_btf; ++b)
+    {
+        uint64_t first = 0;
+        while(first < it[b].T)
+        {
+            const size_t cost = texel_cost(b);
+            uint64_t room = std::min<uint64_t>((budget - std::min(budget, chunk_bytes)) / cost, max_texels - chunk_texels);
+            if(chunks.back().size() >= (size_t)svf::kLmMaxSegments || room == 0)
+            {
+                if(chunks.back().empty())
+                    return fail(SVF_ENOMEM, "btf %u: one texel does not fit in device memory", b);
+                chunks.emplace_back();
+                chunk_texels = chunk_floats = 0;
+                chunk_bytes = 0;
+                continue;
+            }
+            const uint64_t n = std::min<uint64_t>(room, it[b].T - first);
+            chunks.back().push_back(Piece{ b, first, n, chunk_texels, chunk_floats });
+            chunk_texels += n;
+            chunk_floats += n * it[b].stride;
+            chunk_bytes += n * cost;
+            first += n;
+        }
+    }
+    if(chunks.back().empty())
+        chunks.pop_back();
+
+    // buffers for the largest chunk
+    uint64_t max_n = 0, max_floats = 0;
+    size_t max_stage = 0;
+    bool any_ndf = false, any_default = false;
+    for(auto& ch : chunks)
+    {
+        uint64_t n = 0, f = 0;
+        for(auto& p : ch)
+        {
+            n += p.count;
+            f += p.count * it[p.b].stride;
+            if(!it[p.b].on_device)
+                max_stage = std::max(max_stage, it[p.b].texel_bytes * (size_t)p.count);
+            any_ndf = any_ndf || maps[p.b].ndf;
+            any_default = any_default || it[p.b].default_init;
+        }
+        max_n = std::max(max_n, n);
+        max_floats = std::max(max_floats, f);
+    }
+    SVF_TRY(ctx->lum.ensure(sizeof(float) * max_floats));
+    SVF_TRY(ctx->avg.ensure(sizeof(float) * 3 * max_n));
+    SVF_TRY(ctx->init.ensure(sizeof(float) * 7 * max_n));
+    SVF_TRY(ctx->out.ensure(sizeof(float) * 7 * max_n));
+    SVF_TRY(ctx->rmse.ensure(sizeof(float) * max_n));
+    SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * max_n));
+    SVF_TRY(ctx->maps_buf.ensure(sizeof(float) * 12 * max_n));
+    if(any_default)
+    {
+        SVF_TRY(ctx->lum_hi.ensure(2 * max_floats));
+        SVF_TRY(ctx->lum_lo.ensure(2 * max_floats));
+        SVF_TRY(ctx->ndf.ensure(sizeof(float) * ndf_ld * max_n));
+    }
+    if(any_ndf)
+        SVF_TRY(ctx->ndf_tex.ensure(sizeof(float) * svf::kNdfTexels * max_n));
+    if(max_stage)
+        SVF_TRY(ctx->samples.ensure(max_stage));
+
+    std::vector<svf_run_stats> rs(n_btf);
+    svf_run_stats all{};
+    SVF_TRY(zero_error_flags(ctx));
+    SVF_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    float ms = 0.0f;
+    for(auto& ch : chunks)
+    {
+        uint64_t n = 0;
+        for(auto& p : ch)
+            n += p.count;
+        SVF_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+        // luminance and initial guess, piece by piece
+        for(auto& p : ch)
+        {
+            const Item& x = it[p.b];
+            const svf_btf_view& v = btfs[p.b];
+            const void* samples = static_cast<const char*>(v.samples) + p.first * x.texel_bytes;
+            if(!x.on_device)
+            {
+                SVF_CUDA(cudaMemcpyAsync(ctx->samples.p, samples, x.texel_bytes * p.count, cudaMemcpyHostToDevice,
+                                         ctx->stream));
+                samples = ctx->samples.p;
+            }
+            const uint32_t L = x.lay->L, N = L * L;
+            float* lum = ctx->lum.as<float>() + p.off;
+            SVF_CUDA(svf::launch_luminance(samples, v.sample_type, p.count, N, lum, x.stride,
+                                           ctx->avg.as<float>() + 3 * p.k0,
+                                           x.default_init ? ctx->lum_hi.as<uint16_t>() + p.off : nullptr,
+                                           x.default_init ? ctx->lum_lo.as<uint16_t>() + p.off : nullptr,
+                                           ctx->stream));
+            if(x.default_init)
+            {
+                cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.as<uint16_t>() + p.off, ctx->lum_lo.as<uint16_t>() + p.off,
+                                                   p.count, x.stride, x.init->ndf_op_hi, x.init->ndf_op_lo,
+                                                   x.init->ndf_rows_pad, x.init->k_pad, N,
+                                                   ctx->ndf.as<float>() + p.k0 * ndf_ld, ndf_ld,
+                                                   ctx->error.as<uint32_t>() + 2, ctx->stream);
+                if(e != cudaSuccess)
+                    return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
+                SVF_CUDA(svf::launch_init_finish(*x.init, ctx->ndf.as<float>() + p.k0 * ndf_ld, ndf_ld, p.count,
+                                                 ctx->init.as<float>() + 7 * p.k0, nullptr,
+                                                 maps[p.b].ndf ? ctx->ndf_tex.as<float>() + p.k0 * svf::kNdfTexels
+                                                               : nullptr,
+                                                 ctx->stream));
+            }
+            else
+                SVF_TRY(to_device(ctx, ctx->init.as<float>() + 7 * p.k0, opts[p.b].init_params + 7 * p.first,
+                                  sizeof(float) * 7 * p.count));
+        }
+        SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
+        // one LM launch over the pieces, whatever their layouts
+        svf::LmSegment seg[svf::kLmMaxSegments];
+        Layout* big = it[ch[0].b].lay;
+        bool all_up = true;
+        uint64_t max_stride = 0;
+        for(size_t i = 0; i < ch.size(); ++i)
+        {
+            const Item& x = it[ch[i].b];
+            seg[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride, ctx->lum.as<float>() + ch[i].off,
+                                     x.lay->geo.as<float>() };
+            all_up = all_up && x.lay->all_up;
+            max_stride = std::max(max_stride, x.stride);
+            if(x.lay->L > big->L)
+                big = x.lay;
+        }
+        float* mb = ctx->maps_buf.as<float>();
+        LmRun r{ nullptr, max_stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
+                 ctx->stats.as<svf_texel_stats>(), ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n,
+                 seg, (uint32_t)ch.size(), all_up };
+        SVF_TRY(run_lm(ctx, big, &opts[0].lsq, r));
+        SVF_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
+        // outputs, piece by piece
+        std::vector<svf_texel_stats> st(n);
+        SVF_CUDA(cudaMemcpyAsync(st.data(), ctx->stats.p, sizeof(svf_texel_stats) * n, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        for(auto& p : ch)
+        {
+            const svf_maps& m = maps[p.b];
+            auto put = [&](void* dst, const void* src, size_t bytes) -> svf_status {
+                if(dst)
+                    SVF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+                return SVF_OK;
+            };
+            const uint64_t k = p.k0, c = p.count, f = p.first;
+            SVF_TRY(put(m.diffuse ? m.diffuse + 3 * f : nullptr, mb + 3 * k, sizeof(float) * 3 * c));
+            SVF_TRY(put(m.specular ? m.specular + 3 * f : nullptr, mb + 3 * n + 3 * k, sizeof(float) * 3 * c));
+            SVF_TRY(put(m.sigma ? m.sigma + 2 * f : nullptr, mb + 6 * n + 2 * k, sizeof(float) * 2 * c));
+            SVF_TRY(put(m.basis ? m.basis + 4 * f : nullptr, mb + 8 * n + 4 * k, sizeof(float) * 4 * c));
+            SVF_TRY(put(m.rmse ? m.rmse + f : nullptr, ctx->rmse.as<float>() + k, sizeof(float) * c));
+            SVF_TRY(put(m.params ? m.params + 7 * f : nullptr, ctx->out.as<float>() + 7 * k, sizeof(float) * 7 * c));
+            SVF_TRY(put(m.init ? m.init + 7 * f : nullptr, ctx->init.as<float>() + 7 * k, sizeof(float) * 7 * c));
+            SVF_TRY(put(m.ndf ? m.ndf + (uint64_t)svf::kNdfTexels * f : nullptr,
+                        ctx->ndf_tex.as<float>() + (uint64_t)svf::kNdfTexels * k, sizeof(float) * svf::kNdfTexels * c));
+        }
+        SVF_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
+        SVF_TRY(read_error_flag(ctx, any_default));   // waits for the chunk
+        for(auto& p : ch)
+        {
+            svf_run_stats& q = rs[p.b];
+            q.texels += p.count;
+            for(uint64_t i = 0; i < p.count; ++i)
+            {
+                const svf_texel_stats& x = st[p.k0 + i];
+                q.iterations += x.iterations;
+                q.jacobians += x.jacobians;
+                q.residuals += x.residuals;
+                if(x.status & (SVF_TEXEL_NONFINITE | SVF_TEXEL_TIMEOUT))
+                    q.failed_texels++;
+            }
+            if(maps[p.b].stats)
+                SVF_CUDA(cudaMemcpy(maps[p.b].stats + p.first, st.data() + p.k0, sizeof(svf_texel_stats) * p.count,
+                                    cudaMemcpyDefault));
+        }
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]));
+        all.ms_init += ms;   // luminance, NDF GEMM and init finish (and any host copies) of the pieces
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+        all.ms_fit += ms;
+        SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[3], ctx->ev[4]));
+        all.ms_copy += ms;
+    }
+    SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[4]));
+    all.ms_total = ms;
+    Layout* big = it[0].lay;
+    uint64_t big_stride = it[0].stride;
+    for(auto& x : it)
+        if(x.lay->L > big->L)
+        {
+            big = x.lay;
+            big_stride = x.stride;
+        }
+    const svf::LmKernelChoice used = big->tuned ? big->choice : svf::lm_default_choice(big->L, big_stride);
+    for(auto& q : rs)
+    {
+        all.texels += q.texels;
+        all.iterations += q.iterations;
+        all.jacobians += q.jacobians;
+        all.residuals += q.residuals;
+        all.failed_texels += q.failed_texels;
+    }
+    all.lm_threads = (uint32_t)used.threads;
+    all.lm_slots = (uint32_t)used.slots;
+    for(uint32_t b = 0; b < n_btf; ++b)
+    {
+        rs[b].ms_total = all.ms_total;
+        rs[b].ms_init = all.ms_init;
+        rs[b].ms_fit = all.ms_fit;
+        rs[b].ms_copy = all.ms_copy;
+        rs[b].lm_threads = all.lm_threads;
+        rs[b].lm_slots = all.lm_slots;
+        if(runs)
+            runs[b] = rs[b];
+    }
+    if(total)
+        *total = all;
+    if(all.failed_texels)
+        return fail(SVF_EPARTIAL, "%llu texels did not produce a finite fit", (unsigned long long)all.failed_texels);
     return SVF_OK;
 }
 

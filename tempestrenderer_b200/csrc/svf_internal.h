@@ -20,12 +20,25 @@ struct LmConfig
     uint32_t restarts;     // continuations from a stop point with fresh damping
 };
 
+// A run of texels of one direction layout in an LM launch: texels
+// [first, next segment's first) take their slabs from lum + (t - first) * stride.
+constexpr int kLmMaxSegments = 16;
+struct LmSegment
+{
+    uint32_t     first;        // first texel of the segment (segments in increasing order, seg[0].first = 0)
+    uint32_t     L;            // directions of the layout (L^2 pairs)
+    uint64_t     stride;       // floats per slab, % 4 == 0
+    const float* lum;          // [count][stride], 16-byte aligned
+    const float* geo;          // [3][L] direction table, SoA: x, y, z
+};
+
 // Arguments of the persistent LM kernel.
 struct LmArgs
 {
-    const float* lum;          // [texels][lum_stride], lum_stride % 4 == 0, 16-byte aligned
-    uint64_t     lum_stride;   // floats
-    const float* geo;          // [3][L] direction table, SoA: x, y, z
+    LmSegment    seg[kLmMaxSegments];
+    uint32_t     n_seg;        // >= 1
+    uint32_t     L;            // the largest layout of the segments
+    uint64_t     lum_stride;   // the largest slab stride (floats): sizes the shared memory
     const float* init;         // [texels][7]
     float*       out;          // [texels][7]
     float*       rmse;         // [texels]
@@ -35,8 +48,8 @@ struct LmArgs
     float* map_specular;       // [texels][3] or null
     float* map_sigma;          // [texels][2] or null
     float* map_basis;          // [texels][4] or null
-    uint32_t L, N, texels;
-    uint32_t all_up;           // every direction has z > 0
+    uint32_t texels;
+    uint32_t all_up;           // every direction of every segment has z > 0
     LmConfig cfg;
     uint32_t* work_counter;    // zeroed before the launch
     uint32_t* error_flag;      // set non-zero by a bounded wait that expired

@@ -420,15 +420,14 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
         return e;
     LmArgs a{};
-    a.lum = slabs;
+    a.seg[0] = LmSegment{ 0, L, stride, slabs, geo };
+    a.n_seg = 1;
+    a.L = L;
     a.lum_stride = stride;
-    a.geo = geo;
     a.init = init;
     a.out = out;
     a.rmse = rmse;
     a.stats = stats;
-    a.L = L;
-    a.N = N;
     a.texels = texels;
     a.cfg = cfg;
     a.work_counter = flags;

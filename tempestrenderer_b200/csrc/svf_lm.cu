@@ -669,6 +669,10 @@ struct Slot
     int loading;          // the slab copy of `texel` is in flight
     int dead;             // a copy did not arrive: the slot takes no more texels
     uint32_t arrived;     // worker warps done with the current pass (the last one sums)
+    uint32_t L;           // layout of the texel in the slot
+    uint32_t slab_bytes;
+    double npairs;        // L^2
+    const float* geo;
 };
 
 // Dynamic shared memory per slot: [stride] slab | [Lp][kEntry] table |
@@ -760,12 +764,21 @@ __device__ void write_texel(const LmArgs& args, LmState& st, uint32_t t, double 
 
 // Control thread: takes the next texel for slot `sl` and starts its slab copy
 // (the slab is no longer read: the workers finished the slot's last pass).
-__device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot& sl, float* slab, uint32_t slab_bytes)
+__device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot& sl, float* slab)
 {
     const uint32_t t = sl.dead ? kNoTexel : atomicAdd(args.work_counter, 1u);
     if(t < args.texels)
     {
-        bulk_load(slab, args.lum + (uint64_t)t * args.lum_stride, slab_bytes, &sl.bar);
+        uint32_t k = 0;
+        for(uint32_t i = 1; i < args.n_seg; ++i)
+            if(t >= args.seg[i].first)
+                k = i;
+        const LmSegment& g = args.seg[k];
+        sl.L = g.L;
+        sl.npairs = (double)g.L * (double)g.L;
+        sl.geo = g.geo;
+        sl.slab_bytes = (uint32_t)(g.stride * sizeof(float));
+        bulk_load(slab, g.lum + (uint64_t)(t - g.first) * g.stride, sl.slab_bytes, &sl.bar);
         sl.texel = t;
         sl.loading = 1;
     }
@@ -841,9 +854,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ Slot slots[S];
 
-    const uint32_t L = args.L;
-    const double n_pairs = (double)args.N;
-    const uint32_t slab_bytes = (uint32_t)(args.lum_stride * sizeof(float));
+    const uint32_t L = args.L;   // the largest layout: sizes each slot's shared memory
     const size_t per_slot = SM::bytes(L, args.lum_stride);
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 
@@ -866,8 +877,8 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 break;
             if(cmd == kSlotPass)
             {
-                worker_pass<NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), L, args.cfg.fresnel, red_of(s),
-                                                redd_of(s), wwarp, lane);
+                worker_pass<NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), slots[s].L, args.cfg.fresnel,
+                                                  red_of(s), redd_of(s), wwarp, lane);
                 // the last worker warp to finish sums the partials in FP64, in warp
                 // order (deterministic), while the others move on
                 __syncwarp();
@@ -903,7 +914,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
             sl.parity = 0;
             sl.dead = 0;
             sl.arrived = 0;
-            slot_fetch(args, sl, slab_of(s), slab_bytes);
+            slot_fetch(args, sl, slab_of(s));
         }
         for(int s = 0; s < S; ++s)
             if(slots[s].loading)
@@ -913,7 +924,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
     for(int s = 0; s < S; ++s)
     {
         if(slots[s].cmd == kSlotPass)
-            build_table(tab_of(s), args.geo, L, slots[s].pf, &slots[s].pc, lane);
+            build_table(tab_of(s), slots[s].geo, slots[s].L, slots[s].pf, &slots[s].pc, lane);
         __syncwarp();
         nbar_arrive(bar_ready(s), kThreads);
     }
@@ -953,12 +964,12 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 }
                 else
                 {
-                    next = lm_after_trial(st, args.cfg, sl.sums[kRed], n_pairs);
+                    next = lm_after_trial(st, args.cfg, sl.sums[kRed], sl.npairs);
                     if(next == kCmdJacobian)
-                        next = lm_after_jacobian(st, args.cfg, sl.sums, n_pairs);
+                        next = lm_after_jacobian(st, args.cfg, sl.sums, sl.npairs);
                 }
                 if(next == kCmdContinue)
-                    next = lm_next(st, args.cfg, n_pairs);
+                    next = lm_next(st, args.cfg, sl.npairs);
                 if(next == kCmdTrial)
                 {
 #pragma unroll
@@ -969,8 +980,8 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 }
                 else
                 {
-                    write_texel(args, st, sl.texel, n_pairs);
-                    slot_fetch(args, sl, slab_of(s), slab_bytes);
+                    write_texel(args, st, sl.texel, sl.npairs);
+                    slot_fetch(args, sl, slab_of(s));
                 }
             }
             else if(sl.loading)
@@ -994,7 +1005,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
         build = __shfl_sync(0xffffffffu, build, 0);
         exit_now = __shfl_sync(0xffffffffu, exit_now, 0);
         if(build)
-            build_table(tab_of(s), args.geo, L, sl.pf, &sl.pc, lane);
+            build_table(tab_of(s), sl.geo, sl.L, sl.pf, &sl.pc, lane);
         __syncwarp();
         nbar_arrive(bar_ready(s), kThreads);
         if(exit_now)
