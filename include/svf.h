@@ -64,6 +64,15 @@ typedef enum svf_status
 
 /* LeastSquaresFitOptions (svbrdf-fitting.hh:100-107) for the supported path */
 #define SVF_LSQ_DIFFUSE      (1u << 1)   /* LSF_OPTON_DIFFUSE: fit the Lambert term (7 parameters) */
+/* The RGB fit (no counterpart in the reference, which fits the luminance and
+ * colours the maps with the average chromaticity): 11 parameters per texel,
+ * {kd rgb, ks rgb, sx, sy} plus the orientation, fitted to the three channels
+ * with the same LM; the orientation is a quaternion moved by local rotations.
+ * Samples are staged as FP16 for it.  svf_fit_texels / svf_fit_btfs only; its
+ * parameters (params, init maps, SVF_INIT_GIVEN) are 12 floats per texel,
+ * {kd rgb, ks rgb, sx, sy, quaternion xyzw}; the diffuse / specular maps are
+ * the fitted albedos and rmse is over the three channels. */
+#define SVF_LSQ_RGB          (1u << 8)
 
 typedef struct svf_lsq_options
 {
@@ -219,8 +228,8 @@ typedef struct svf_maps
     float*           sigma;      /* [texels][2]  SGGX standard deviations */
     float*           basis;      /* [texels][4]  quaternion xyzw = ToQuaternion(euler) */
     float*           rmse;       /* [texels] */
-    float*           params;     /* [texels][7]  fitted parameters */
-    float*           init;       /* [texels][7]  initial guess used */
+    float*           params;     /* [texels][7]  fitted parameters ([texels][12] with SVF_LSQ_RGB) */
+    float*           init;       /* [texels][7]  initial guess used ([texels][12] with SVF_LSQ_RGB) */
     svf_texel_stats* stats;      /* [texels] */
     float*           ndf;        /* [texels][64*64]  NDF texture of the default initial
                                   * guess (getLastNDFTexture, svbrdf-fitting.hh:180),

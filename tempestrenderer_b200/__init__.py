@@ -26,6 +26,7 @@ LIB_PATH = os.path.join(HERE, "libsvf.so")
 SVF_OK, SVF_EINVAL, SVF_ENOMEM, SVF_ECUDA, SVF_ETIMEOUT, SVF_EPARTIAL, SVF_ENODEV = range(7)
 SVF_TEXEL_NONFINITE, SVF_TEXEL_MAX_ITER, SVF_TEXEL_TIMEOUT = 1, 2, 4
 SVF_LSQ_DIFFUSE = 1 << 1
+SVF_LSQ_RGB = 1 << 8
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN = 0, 1
 
@@ -129,11 +130,15 @@ def _check(status: int):
         raise SvfError(status, load().svf_last_error().decode())
 
 
-def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | None = None) -> LsqOptions:
+def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | None = None,
+            rgb: bool = False) -> LsqOptions:
+    """LM options; rgb selects the 11-parameter RGB fit (svf_fit_texels / svf_fit_btfs)."""
     o = LsqOptions()
     load().svf_lsq_options_default(C.byref(o))
     o.max_iterations = max_iterations
     o.fresnel = fresnel
+    if rgb:
+        o.flags |= SVF_LSQ_RGB
     if restarts is not None:
         o.restarts = restarts
     return o
@@ -269,8 +274,9 @@ class Context:
         fo.lsq = opts or options()
         fo.init_mode = SVF_INIT_DEFAULT if init is None else SVF_INIT_GIVEN
         fo.init_params = _ptr(init) if init is not None else None
+        kout = 12 if fo.lsq.flags & SVF_LSQ_RGB else 7
         shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
-                  "params": (T, 7), "init": (T, 7), "ndf": (T, 64 * 64)}
+                  "params": (T, kout), "init": (T, kout), "ndf": (T, 64 * 64)}
         res = dict(out or {})
         for k in want:
             if k in res:
@@ -307,8 +313,9 @@ class Context:
                 init = np.ascontiguousarray(init, np.float32)
                 keep.append(init)
                 fos[i].init_params = init.ctypes.data
+            kout = 12 if fos[i].lsq.flags & SVF_LSQ_RGB else 7
             shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
-                      "params": (T, 7), "init": (T, 7), "ndf": (T, 64 * 64)}
+                      "params": (T, kout), "init": (T, kout), "ndf": (T, 64 * 64)}
             res = {k: (np.zeros(T, STATS_DTYPE) if k == "stats" else np.zeros(shapes[k], np.float32)) for k in want}
             for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params", "init", "stats", "ndf"):
                 setattr(ms[i], k, _ptr(res[k]) if k in res else None)

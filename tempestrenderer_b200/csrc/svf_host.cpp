@@ -178,7 +178,7 @@ struct svf_ctx
     std::map<uint64_t, std::unique_ptr<Layout>> layouts;
     std::unique_ptr<svf::InitHostTables> tables;
     DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, samples2,
-        maps_buf, scratch;
+        maps_buf, scratch, rgb16, init_rgb;
     PinnedBuf pinned;
 };
 
@@ -200,7 +200,9 @@ svf_status check_options(const svf_lsq_options* o)
     if(!o)
         return fail(SVF_EINVAL, "null options");
     if(!(o->flags & SVF_LSQ_DIFFUSE))
-        return fail(SVF_EINVAL, "only the 7-parameter fit with the diffuse term (SVF_LSQ_DIFFUSE) is supported");
+        return fail(SVF_EINVAL, "only the fits with the diffuse term (SVF_LSQ_DIFFUSE) are supported");
+    if(o->flags & ~(SVF_LSQ_DIFFUSE | SVF_LSQ_RGB))
+        return fail(SVF_EINVAL, "unknown lsq flags 0x%x", o->flags & ~(SVF_LSQ_DIFFUSE | SVF_LSQ_RGB));
     if(!(o->fresnel >= 1.0f) || !std::isfinite(o->fresnel))
         return fail(SVF_EINVAL, "fresnel (refractive index) must be >= 1, got %g", o->fresnel);
     if(!(o->mse_target >= 0.0) || !(o->break_on_small_step > 0.0))
@@ -380,10 +382,10 @@ svf_status to_device(svf_ctx* ctx, void* dst, const void* src, size_t bytes)
 
 struct LmRun
 {
-    const float* lum;      // device, padded
-    uint64_t stride;
-    const float* init;     // device [T][7]
-    float* out;            // device [T][7]
+    const void* lum;       // device, padded slabs (FP32 luminance; FP16 RGB for the RGB fit)
+    uint64_t stride;       // slab elements
+    const float* init;     // device [T][7] ([T][12] RGB)
+    float* out;            // device [T][7] ([T][12] RGB)
     float* rmse;           // device [T]
     svf_texel_stats* stats;
     const float* avg;
@@ -394,6 +396,7 @@ struct LmRun
     const svf::LmSegment* seg = nullptr;
     uint32_t n_seg = 0;
     bool all_up = false;
+    bool rgb = false;      // the 11-parameter RGB fit
 };
 
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c);
@@ -510,11 +513,20 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
     return SVF_OK;
 }
 
+// The LM configuration of a run: the autotuned one for the luminance fit, the
+// first that fits for the RGB fit (its slabs differ from the probe's).
+svf::LmKernelChoice lm_choice(Layout* lay, uint64_t stride, bool rgb)
+{
+    if(rgb)
+        return svf::lm_default_choice(lay->L, stride, true);
+    return lay->tuned ? lay->choice : svf::lm_default_choice(lay->L, stride);
+}
+
 svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r)
 {
-    if(!lay->tuned && r.texels >= 4096)
+    if(!r.rgb && !lay->tuned && r.texels >= 4096)
         SVF_TRY(tune_lm(ctx, lay, o));
-    return launch_lm(ctx, lay, o, r, lay->tuned ? lay->choice : svf::lm_default_choice(lay->L, r.stride));
+    return launch_lm(ctx, lay, o, r, lm_choice(lay, r.stride, r.rgb));
 }
 
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c)
@@ -561,7 +573,8 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     a.work_counter = ctx->counter.as<uint32_t>();
     a.error_flag = ctx->error.as<uint32_t>();
     SVF_CUDA(cudaMemsetAsync(ctx->counter.p, 0, 16, ctx->stream));   // the error words are zeroed per call
-    int per_sm = svf::lm_max_ctas_per_sm(a.L, a.lum_stride, c);
+    a.rgb = r.rgb ? 1u : 0u;
+    int per_sm = svf::lm_max_ctas_per_sm(a.L, a.lum_stride, c, r.rgb);
     if(per_sm <= 0)
         return fail(SVF_EINVAL, "the LM kernel (%d threads) does not fit on an SM for L = %u", c.threads, a.L);
     uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * ctx->sms, r.texels);
@@ -733,6 +746,8 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
 {
     SVF_TRY(check_ctx(ctx));
     SVF_TRY(check_options(opts));
+    if(opts->flags & SVF_LSQ_RGB)
+        return fail(SVF_EINVAL, "the RGB fit (SVF_LSQ_RGB) takes RGB samples: use svf_fit_texels");
     if(!lum || !init || !out || !rmse)
         return fail(SVF_EINVAL, "null lum/init/out/rmse");
     const uint32_t N = L * L;
@@ -782,6 +797,8 @@ svf_status svf_lsq_fit_batch_noalloc(const float* lp, uint32_t L, const float* l
     // Nothing here allocates: the checks read pointer attributes, errors go to the
     // fixed per-thread message buffer, the work runs in the static scratch array.
     SVF_TRY(check_options(opts));
+    if(opts->flags & SVF_LSQ_RGB)
+        return fail(SVF_EINVAL, "the RGB fit (SVF_LSQ_RGB) takes RGB samples: use svf_fit_texels");
     if(L < 3 || L > 160)
         return fail(SVF_EINVAL, "light_count must be in [3, 160], got %u", L);
     const uint64_t N = (uint64_t)L * L;
@@ -861,6 +878,10 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     if(maps->ndf && !default_init)
         return fail(SVF_EINVAL, "the NDF map exists only with the default initial guess");
     const uint32_t ndf_ld = default_init ? init_lay->ndf_rows_pad : 0;
+    // the RGB fit: FP16 RGB slabs, 12 floats of parameters per texel
+    const bool rgb = (opts->lsq.flags & SVF_LSQ_RGB) != 0;
+    const uint64_t stride3 = round_up(3ull * N, 8);
+    const uint64_t kout = rgb ? 12 : 7;
 
     // Chunking.  Device-resident samples: as few chunks as the device memory
     // allows.  Host samples: a pipeline of chunks, each copied host -> device on
@@ -869,7 +890,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     // luminance kernel has read it.
     size_t free_b = 0, total_b = 0;
     SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
-    const size_t per_texel = sizeof(float) * (stride + 3 + 7 + 7 + 1 + 12) +
+    const size_t per_texel = sizeof(float) * (stride + 3 + 2 * kout + 7 + 1 + 12) + (rgb ? 2 * stride3 : 0) +
                              (default_init ? 2 * 2 * stride + sizeof(float) * ndf_ld : 0) +
                              (maps->ndf ? sizeof(float) * svf::kNdfTexels : 0) +
                              (samples_on_device ? 0 : 2 * texel_bytes);
@@ -883,7 +904,12 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     SVF_TRY(ctx->lum.ensure(sizeof(float) * stride * chunk));
     SVF_TRY(ctx->avg.ensure(sizeof(float) * 3 * chunk));
     SVF_TRY(ctx->init.ensure(sizeof(float) * 7 * chunk));
-    SVF_TRY(ctx->out.ensure(sizeof(float) * 7 * chunk));
+    SVF_TRY(ctx->out.ensure(sizeof(float) * kout * chunk));
+    if(rgb)
+    {
+        SVF_TRY(ctx->rgb16.ensure(2 * stride3 * chunk));
+        SVF_TRY(ctx->init_rgb.ensure(sizeof(float) * 12 * chunk));
+    }
     SVF_TRY(ctx->rmse.ensure(sizeof(float) * chunk));
     SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * T));
     SVF_TRY(ctx->maps_buf.ensure(sizeof(float) * 12 * chunk));
@@ -950,7 +976,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_CUDA(cudaEventRecord(ev(c, 2), ctx->stream));
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
                                        ctx->avg.as<float>(), default_init ? ctx->lum_hi.p : nullptr,
-                                       default_init ? ctx->lum_lo.p : nullptr, ctx->stream));
+                                       default_init ? ctx->lum_lo.p : nullptr, ctx->stream,
+                                       rgb ? ctx->rgb16.p : nullptr, stride3));
         if(!samples_on_device)
         {
             SVF_CUDA(cudaEventRecord(ctx->freed[buf], ctx->stream));
@@ -971,12 +998,18 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                                              nullptr, maps->ndf ? ctx->ndf_tex.as<float>() : nullptr, ctx->stream));
         }
         else
-            SVF_TRY(to_device(ctx, ctx->init.p, opts->init_params + 7 * c0, sizeof(float) * 7 * n));
+            SVF_TRY(to_device(ctx, rgb ? ctx->init_rgb.p : ctx->init.p, opts->init_params + kout * c0,
+                              sizeof(float) * kout * n));
+        if(rgb && default_init)
+            SVF_CUDA(svf::launch_rgb_init(ctx->init.as<float>(), ctx->avg.as<float>(), n, ctx->init_rgb.as<float>(),
+                                          ctx->stream));
+        const float* init_used = rgb ? ctx->init_rgb.as<float>() : ctx->init.as<float>();
         SVF_CUDA(cudaEventRecord(ev(c, 4), ctx->stream));
         float* mb = ctx->maps_buf.as<float>();
-        LmRun r{ ctx->lum.as<float>(), stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
-                 ctx->stats.as<svf_texel_stats>() + c0, ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n,
-                 n };
+        LmRun r{ rgb ? (const void*)ctx->rgb16.p : (const void*)ctx->lum.p, rgb ? stride3 : stride, init_used,
+                 ctx->out.as<float>(), ctx->rmse.as<float>(), ctx->stats.as<svf_texel_stats>() + c0,
+                 ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n };
+        r.rgb = rgb;
         SVF_TRY(run_lm(ctx, lay, &opts->lsq, r));
         SVF_CUDA(cudaEventRecord(ev(c, 5), ctx->stream));
         // outputs (into host or device buffers of the caller)
@@ -990,8 +1023,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_TRY(put(maps->sigma ? maps->sigma + 2 * c0 : nullptr, mb + 6 * n, sizeof(float) * 2 * n));
         SVF_TRY(put(maps->basis ? maps->basis + 4 * c0 : nullptr, mb + 8 * n, sizeof(float) * 4 * n));
         SVF_TRY(put(maps->rmse ? maps->rmse + c0 : nullptr, ctx->rmse.p, sizeof(float) * n));
-        SVF_TRY(put(maps->params ? maps->params + 7 * c0 : nullptr, ctx->out.p, sizeof(float) * 7 * n));
-        SVF_TRY(put(maps->init ? maps->init + 7 * c0 : nullptr, ctx->init.p, sizeof(float) * 7 * n));
+        SVF_TRY(put(maps->params ? maps->params + kout * c0 : nullptr, ctx->out.p, sizeof(float) * kout * n));
+        SVF_TRY(put(maps->init ? maps->init + kout * c0 : nullptr, init_used, sizeof(float) * kout * n));
         SVF_TRY(put(maps->ndf ? maps->ndf + (uint64_t)svf::kNdfTexels * c0 : nullptr, ctx->ndf_tex.p,
                     sizeof(float) * svf::kNdfTexels * n));
         SVF_CUDA(cudaEventRecord(ev(c, 6), ctx->stream));
@@ -1032,7 +1065,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     rs.ms_total = span(samples_on_device ? ev(0, 2) : ev(0, 0), ev(n_chunks - 1, 6));
     cudaGetLastError();
     rs.texels = T;
-    const svf::LmKernelChoice used = lay->tuned ? lay->choice : svf::lm_default_choice(L, stride);
+    const svf::LmKernelChoice used = lm_choice(lay, rgb ? stride3 : stride, rgb);
     rs.lm_threads = (uint32_t)used.threads;
     rs.lm_slots = (uint32_t)used.slots;
     if(run)
@@ -1053,11 +1086,13 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
     SVF_TRY(check_options(&opts[0].lsq));
 
     // per BTF: layout, default-init tables, sizes
+    const bool rgb = (opts[0].lsq.flags & SVF_LSQ_RGB) != 0;
+    const uint64_t kout = rgb ? 12 : 7;
     struct Item
     {
         Layout* lay = nullptr;
         const svf::InitLayout* init = nullptr;
-        uint64_t T = 0, stride = 0;
+        uint64_t T = 0, stride = 0, stride3 = 0;
         size_t texel_bytes = 0;
         bool on_device = false, default_init = false;
     };
@@ -1086,6 +1121,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             return fail(SVF_EINVAL, "btf %u: too many texels", b);
         SVF_TRY(get_layout(ctx, v.layout->lights_parabolic, v.layout->light_count, &x.lay));
         x.stride = round_up((uint64_t)x.lay->L * x.lay->L, 8);
+        x.stride3 = round_up(3ull * x.lay->L * x.lay->L, 8);
         x.texel_bytes = (v.sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)x.lay->L * x.lay->L;
         x.on_device = is_device_pointer(v.samples);
         x.default_init = o.init_mode == SVF_INIT_DEFAULT;
@@ -1104,7 +1140,8 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
     const size_t budget = free_b / 2;
     auto texel_cost = [&](uint32_t b) -> size_t {
         const Item& x = it[b];
-        return sizeof(float) * (x.stride + 3 + 7 + 7 + 1 + 12) + sizeof(svf_texel_stats) +
+        return sizeof(float) * (x.stride + 3 + 7 + kout + 1 + 12) + sizeof(svf_texel_stats) +
+               (rgb ? 2 * x.stride3 + sizeof(float) * 12 : 0) +
                (x.default_init ? 2 * 2 * x.stride + sizeof(float) * ndf_ld : 0) +
                (maps[b].ndf ? sizeof(float) * svf::kNdfTexels : 0) + (x.on_device ? 0 : x.texel_bytes);
     };
@@ -1113,9 +1150,10 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         uint32_t b;
         uint64_t first, count, k0;   // texels of BTF b; k0: position in the chunk
         uint64_t off;                // slab offset (floats) in the chunk
+        uint64_t off3;               // RGB slab offset (halves) in the chunk
     };
     std::vector<std::vector<Piece>> chunks(1);
-    uint64_t chunk_texels = 0, chunk_floats = 0;
+    uint64_t chunk_texels = 0, chunk_floats = 0, chunk_halves = 0;
     size_t chunk_bytes = 0;
     const uint64_t max_texels = 65535ull * 128;   // the NDF GEMM's grid rows of 128 texels
     for(uint32_t b = 0; b < n_btf; ++b)
@@ -1130,14 +1168,15 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                 if(chunks.back().empty())
                     return fail(SVF_ENOMEM, "btf %u: one texel does not fit in device memory", b);
                 chunks.emplace_back();
-                chunk_texels = chunk_floats = 0;
+                chunk_texels = chunk_floats = chunk_halves = 0;
                 chunk_bytes = 0;
                 continue;
             }
             const uint64_t n = std::min<uint64_t>(room, it[b].T - first);
-            chunks.back().push_back(Piece{ b, first, n, chunk_texels, chunk_floats });
+            chunks.back().push_back(Piece{ b, first, n, chunk_texels, chunk_floats, chunk_halves });
             chunk_texels += n;
             chunk_floats += n * it[b].stride;
+            chunk_halves += n * it[b].stride3;
             chunk_bytes += n * cost;
             first += n;
         }
@@ -1146,16 +1185,17 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         chunks.pop_back();
 
     // buffers for the largest chunk
-    uint64_t max_n = 0, max_floats = 0;
+    uint64_t max_n = 0, max_floats = 0, max_halves = 0;
     size_t max_stage = 0;
     bool any_ndf = false, any_default = false;
     for(auto& ch : chunks)
     {
-        uint64_t n = 0, f = 0;
+        uint64_t n = 0, f = 0, h = 0;
         for(auto& p : ch)
         {
             n += p.count;
             f += p.count * it[p.b].stride;
+            h += p.count * it[p.b].stride3;
             if(!it[p.b].on_device)
                 max_stage = std::max(max_stage, it[p.b].texel_bytes * (size_t)p.count);
             any_ndf = any_ndf || maps[p.b].ndf;
@@ -1163,11 +1203,18 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         }
         max_n = std::max(max_n, n);
         max_floats = std::max(max_floats, f);
+        max_halves = std::max(max_halves, h);
     }
     SVF_TRY(ctx->lum.ensure(sizeof(float) * max_floats));
     SVF_TRY(ctx->avg.ensure(sizeof(float) * 3 * max_n));
     SVF_TRY(ctx->init.ensure(sizeof(float) * 7 * max_n));
-    SVF_TRY(ctx->out.ensure(sizeof(float) * 7 * max_n));
+    SVF_TRY(ctx->out.ensure(sizeof(float) * kout * max_n));
+    if(rgb)
+    {
+        SVF_TRY(ctx->rgb16.ensure(2 * max_halves));
+        SVF_TRY(ctx->init_rgb.ensure(sizeof(float) * 12 * max_n));
+    }
+    float* init_used = rgb ? ctx->init_rgb.as<float>() : ctx->init.as<float>();
     SVF_TRY(ctx->rmse.ensure(sizeof(float) * max_n));
     SVF_TRY(ctx->stats.ensure(sizeof(svf_texel_stats) * max_n));
     SVF_TRY(ctx->maps_buf.ensure(sizeof(float) * 12 * max_n));
@@ -1211,7 +1258,8 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                                            ctx->avg.as<float>() + 3 * p.k0,
                                            x.default_init ? ctx->lum_hi.as<uint16_t>() + p.off : nullptr,
                                            x.default_init ? ctx->lum_lo.as<uint16_t>() + p.off : nullptr,
-                                           ctx->stream));
+                                           ctx->stream, rgb ? ctx->rgb16.as<uint16_t>() + p.off3 : nullptr,
+                                           x.stride3));
             if(x.default_init)
             {
                 cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.as<uint16_t>() + p.off, ctx->lum_lo.as<uint16_t>() + p.off,
@@ -1228,8 +1276,11 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                                                  ctx->stream));
             }
             else
-                SVF_TRY(to_device(ctx, ctx->init.as<float>() + 7 * p.k0, opts[p.b].init_params + 7 * p.first,
-                                  sizeof(float) * 7 * p.count));
+                SVF_TRY(to_device(ctx, init_used + kout * p.k0, opts[p.b].init_params + kout * p.first,
+                                  sizeof(float) * kout * p.count));
+            if(rgb && x.default_init)
+                SVF_CUDA(svf::launch_rgb_init(ctx->init.as<float>() + 7 * p.k0, ctx->avg.as<float>() + 3 * p.k0,
+                                              p.count, init_used + 12 * p.k0, ctx->stream));
         }
         SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
         // one LM launch over the pieces, whatever their layouts
@@ -1240,17 +1291,21 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         for(size_t i = 0; i < ch.size(); ++i)
         {
             const Item& x = it[ch[i].b];
-            seg[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride, ctx->lum.as<float>() + ch[i].off,
-                                     x.lay->geo.as<float>() };
+            if(rgb)
+                seg[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride3,
+                                         ctx->rgb16.as<uint16_t>() + ch[i].off3, x.lay->geo.as<float>() };
+            else
+                seg[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride, ctx->lum.as<float>() + ch[i].off,
+                                         x.lay->geo.as<float>() };
             all_up = all_up && x.lay->all_up;
-            max_stride = std::max(max_stride, x.stride);
+            max_stride = std::max(max_stride, rgb ? x.stride3 : x.stride);
             if(x.lay->L > big->L)
                 big = x.lay;
         }
         float* mb = ctx->maps_buf.as<float>();
-        LmRun r{ nullptr, max_stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
+        LmRun r{ nullptr, max_stride, init_used, ctx->out.as<float>(), ctx->rmse.as<float>(),
                  ctx->stats.as<svf_texel_stats>(), ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n,
-                 seg, (uint32_t)ch.size(), all_up };
+                 seg, (uint32_t)ch.size(), all_up, rgb };
         SVF_TRY(run_lm(ctx, big, &opts[0].lsq, r));
         SVF_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
         // outputs, piece by piece
@@ -1271,8 +1326,9 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             SVF_TRY(put(m.sigma ? m.sigma + 2 * f : nullptr, mb + 6 * n + 2 * k, sizeof(float) * 2 * c));
             SVF_TRY(put(m.basis ? m.basis + 4 * f : nullptr, mb + 8 * n + 4 * k, sizeof(float) * 4 * c));
             SVF_TRY(put(m.rmse ? m.rmse + f : nullptr, ctx->rmse.as<float>() + k, sizeof(float) * c));
-            SVF_TRY(put(m.params ? m.params + 7 * f : nullptr, ctx->out.as<float>() + 7 * k, sizeof(float) * 7 * c));
-            SVF_TRY(put(m.init ? m.init + 7 * f : nullptr, ctx->init.as<float>() + 7 * k, sizeof(float) * 7 * c));
+            SVF_TRY(put(m.params ? m.params + kout * f : nullptr, ctx->out.as<float>() + kout * k,
+                        sizeof(float) * kout * c));
+            SVF_TRY(put(m.init ? m.init + kout * f : nullptr, init_used + kout * k, sizeof(float) * kout * c));
             SVF_TRY(put(m.ndf ? m.ndf + (uint64_t)svf::kNdfTexels * f : nullptr,
                         ctx->ndf_tex.as<float>() + (uint64_t)svf::kNdfTexels * k, sizeof(float) * svf::kNdfTexels * c));
         }
@@ -1305,14 +1361,14 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
     SVF_CUDA(cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[4]));
     all.ms_total = ms;
     Layout* big = it[0].lay;
-    uint64_t big_stride = it[0].stride;
+    uint64_t big_stride = rgb ? it[0].stride3 : it[0].stride;
     for(auto& x : it)
         if(x.lay->L > big->L)
         {
             big = x.lay;
-            big_stride = x.stride;
+            big_stride = rgb ? x.stride3 : x.stride;
         }
-    const svf::LmKernelChoice used = big->tuned ? big->choice : svf::lm_default_choice(big->L, big_stride);
+    const svf::LmKernelChoice used = lm_choice(big, big_stride, rgb);
     for(auto& q : rs)
     {
         all.texels += q.texels;

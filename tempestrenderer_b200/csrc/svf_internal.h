@@ -27,8 +27,8 @@ struct LmSegment
 {
     uint32_t     first;        // first texel of the segment (segments in increasing order, seg[0].first = 0)
     uint32_t     L;            // directions of the layout (L^2 pairs)
-    uint64_t     stride;       // floats per slab, % 4 == 0
-    const float* lum;          // [count][stride], 16-byte aligned
+    uint64_t     stride;       // elements per slab; stride x element size % 16 == 0
+    const void*  lum;          // [count][stride] slab elements (FP32 luminance, or FP16 RGB for the RGB fit), 16-byte aligned
     const float* geo;          // [3][L] direction table, SoA: x, y, z
 };
 
@@ -39,8 +39,8 @@ struct LmArgs
     uint32_t     n_seg;        // >= 1
     uint32_t     L;            // the largest layout of the segments
     uint64_t     lum_stride;   // the largest slab stride (floats): sizes the shared memory
-    const float* init;         // [texels][7]
-    float*       out;          // [texels][7]
+    const float* init;         // [texels][7] ([texels][12] for the RGB fit)
+    float*       out;          // [texels][7] ([texels][12] for the RGB fit)
     float*       rmse;         // [texels]
     svf_texel_stats* stats;    // [texels] or null
     const float* avg_chroma;   // [texels][3] or null (needed by the RGB maps)
@@ -50,6 +50,7 @@ struct LmArgs
     float* map_basis;          // [texels][4] or null
     uint32_t texels;
     uint32_t all_up;           // every direction of every segment has z > 0
+    uint32_t rgb;              // the 11-parameter RGB fit (svf_lm.cu RgbModel)
     LmConfig cfg;
     uint32_t* work_counter;    // zeroed before the launch
     uint32_t* error_flag;      // set non-zero by a bounded wait that expired
@@ -62,10 +63,10 @@ struct LmKernelChoice
     int threads;
     int slots;
 };
-LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride);
+LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb = false);
 int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);
-size_t         lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c);
-int            lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c);
+size_t         lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb = false);
+int            lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb = false);
 cudaError_t    launch_lm_fit(const LmArgs& args, LmKernelChoice c, int grid, cudaStream_t stream);
 
 // svf_lsq_fit_batch_noalloc: repack, geometry and LM on `stream` with the
@@ -79,9 +80,18 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
 // src/image/btf.cc:1078-1116) for texels [0, texels) of an RGB sample array.
 // lum_hi/lum_lo (optional, both or neither): the BF16 split of the slice for the
 // NDF GEMM, same row pitch, columns [0, N) written.
+// rgb16 (optional): the samples again as FP16 RGB slabs [texels][rgb_stride]
+// for the RGB fit (rgb_stride >= 3 N, a multiple of 8).
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
                              float* lum, uint64_t lum_stride, float* avg_chroma, void* lum_hi, void* lum_lo,
-                             cudaStream_t stream);
+                             cudaStream_t stream, void* rgb16 = nullptr, uint64_t rgb_stride = 0);
+
+// The RGB fit's initial parameters {kd rgb, ks rgb, sx, sy, quaternion xyzw}
+// from a luminance initial guess {sx, sy, ks, kd, euler} and the texel's
+// average chromaticity (the colours SVBRDFFitPipeline::fit gives the maps,
+// svbrdf-fitting-pipeline.cc:692-697).
+cudaError_t launch_rgb_init(const float* init7, const float* avg_chroma, uint64_t texels, float* init12,
+                            cudaStream_t stream);
 
 // Repacks a caller's luminance array to the padded internal layout.
 cudaError_t launch_repack(const float* src, uint64_t src_stride, uint64_t texels, uint32_t N,

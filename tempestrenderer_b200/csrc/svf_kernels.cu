@@ -36,7 +36,8 @@ template <typename T>
 __global__ void __launch_bounds__(256) luminance_kernel(const T* __restrict__ samples, uint32_t N, float* __restrict__ lum,
                                                          uint64_t lum_stride, float* __restrict__ avg,
                                                          __nv_bfloat16* __restrict__ lum_hi,
-                                                         __nv_bfloat16* __restrict__ lum_lo)
+                                                         __nv_bfloat16* __restrict__ lum_lo,
+                                                         __half* __restrict__ rgb16, uint64_t rgb_stride)
 {
     const uint64_t t = blockIdx.x;
     const T* src = samples + t * (uint64_t)N * 3;
@@ -47,6 +48,14 @@ __global__ void __launch_bounds__(256) luminance_kernel(const T* __restrict__ sa
         float r = to_f(src[3 * i]), g = to_f(src[3 * i + 1]), b = to_f(src[3 * i + 2]);
         float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
         dst[i] = l;
+        if(rgb16)
+        {
+            // the RGB fit's slab: the samples in FP16, [L*L][3], 16-byte rows
+            __half* o = rgb16 + t * rgb_stride + 3 * (uint64_t)i;
+            o[0] = __float2half_rn(r);
+            o[1] = __float2half_rn(g);
+            o[2] = __float2half_rn(b);
+        }
         if(lum_hi)
         {
             // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
@@ -445,7 +454,8 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
 }
 
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N, float* lum,
-                             uint64_t lum_stride, float* avg, void* lum_hi, void* lum_lo, cudaStream_t stream)
+                             uint64_t lum_stride, float* avg, void* lum_hi, void* lum_lo, cudaStream_t stream,
+                             void* rgb16, uint64_t rgb_stride)
 {
     if(texels == 0)
         return cudaSuccess;
@@ -455,10 +465,48 @@ cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t
     __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(lum_lo);
     if(sample_type == SVF_SAMPLES_F16)
         luminance_kernel<__half><<<(unsigned)texels, 256, 0, stream>>>(static_cast<const __half*>(samples), N, lum,
-                                                                     lum_stride, avg, hi, lo);
+                                                                     lum_stride, avg, hi, lo,
+                                                                     static_cast<__half*>(rgb16), rgb_stride);
     else
         luminance_kernel<float><<<(unsigned)texels, 256, 0, stream>>>(static_cast<const float*>(samples), N, lum,
-                                                                    lum_stride, avg, hi, lo);
+                                                                    lum_stride, avg, hi, lo,
+                                                                    static_cast<__half*>(rgb16), rgb_stride);
+    return cudaGetLastError();
+}
+
+__global__ void rgb_init_kernel(const float* __restrict__ init7, const float* __restrict__ avg, uint64_t texels,
+                                float* __restrict__ init12)
+{
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if(t >= texels)
+        return;
+    const float* p = init7 + 7 * t;
+    const float* a = avg + 3 * t;
+    float* o = init12 + 12 * t;
+    for(int k = 0; k < 3; ++k)
+    {
+        o[k] = a[k] * p[3];
+        o[3 + k] = a[k] * p[2];
+    }
+    o[6] = p[0];
+    o[7] = p[1];
+    // ToQuaternion(euler), quaternion.hh:82-94
+    float s1, c1, s2, c2, s3, c3;
+    sincosf(0.5f * p[4], &s1, &c1);
+    sincosf(0.5f * p[5], &s2, &c2);
+    sincosf(0.5f * p[6], &s3, &c3);
+    o[8] = s1 * c2 * c3 + c1 * s2 * s3;
+    o[9] = -s1 * c2 * s3 + c1 * s2 * c3;
+    o[10] = c1 * c2 * s3 + s1 * s2 * c3;
+    o[11] = c1 * c2 * c3 - s1 * s2 * s3;
+}
+
+cudaError_t launch_rgb_init(const float* init7, const float* avg_chroma, uint64_t texels, float* init12,
+                            cudaStream_t stream)
+{
+    if(texels == 0)
+        return cudaSuccess;
+    rgb_init_kernel<<<(unsigned)((texels + 127) / 128), 128, 0, stream>>>(init7, avg_chroma, texels, init12);
     return cudaGetLastError();
 }
 

@@ -33,6 +33,7 @@
 // warps in FP64.  The LM control follows fitting.hh: the damped normal
 // equations by Cholesky, the small-step and gradient tests and the gain-ratio
 // accept/reject.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -48,8 +49,42 @@ namespace
 {
 
 constexpr int kEntry = 12;                   // floats per direction-table entry
-constexpr int kRed = kHessian + kParams;     // FP32 partial sums per thread (J^T J, J^T r)
 constexpr uint32_t kWaitSpins = 1u << 22;    // bound of every mbarrier wait
+
+// Packed upper triangle of a symmetric P x P matrix.
+template <int P>
+__host__ __device__ constexpr int hix(int i, int j)
+{
+    return i <= j ? i * P - (i * (i - 1)) / 2 + (j - i) : j * P - (j * (j - 1)) / 2 + (i - j);
+}
+
+// The two fits.  Luminance (the reference's LeastSquaresFitSGGX): 7 parameters
+// {sx, sy, ks, kd, euler xyz} on the luminance slice.  RGB: 11 parameters
+// {kd rgb, ks rgb, sx, sy, rotation phi xyz} on the three channels, the
+// orientation kept as a quaternion and updated by the local rotation phi.
+// kAcc: FP32 sums per lane of a pass (the RGB pass keeps the channel-factored
+// sums; the control warp expands them into J^T J and J^T r).
+struct LumModel
+{
+    static constexpr int P = 7;
+    static constexpr int B = 4;          // sx, sy, ks, kd are bounded below by 0
+    static constexpr int kAcc = 35;      // J^T J (28) and J^T r (7)
+    static constexpr int kChannels = 1;
+    static constexpr int kOut = 7;       // floats per texel of initial and fitted parameters
+    static constexpr bool kRgb = false;
+    using Slab = float;
+};
+
+struct RgbModel
+{
+    static constexpr int P = 11;
+    static constexpr int B = 8;          // kd rgb, ks rgb, sx, sy
+    static constexpr int kAcc = 39;      // see sym_pair_rgb
+    static constexpr int kChannels = 3;
+    static constexpr int kOut = 12;      // {kd rgb, ks rgb, sx, sy, quaternion xyzw}
+    static constexpr bool kRgb = true;
+    using Slab = __half;
+};
 
 enum : int
 {
@@ -110,32 +145,36 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
 // FP64 LM control (thread 0; the state lives in shared memory)
 // ------------------------------------------------------------------------------
 
+template <int P>
 struct LmState
 {
-    double p[kParams];      // current parameters
-    double pt[kParams];     // trial parameters
-    double d[kParams];      // step
-    double g[kParams];      // gradient J_r^T r of the residual r = y - f
-    double H[kHessian];     // J^T J, packed upper
+    double p[P];            // current parameters (RGB: the rotation entries are 0)
+    double pt[P];           // trial parameters
+    double d[P];            // step
+    double g[P];            // gradient J_r^T r of the residual r = y - f
+    double H[P * (P + 1) / 2];   // J^T J, packed upper
+    double q[4], qt[4];     // RGB: orientation at p and at the trial point (xyzw)
     double S;               // sum of squared residuals at p
     double lam, nu, rho;
     uint32_t iter, eff, njac, nres, status, restarts_left;
 };
 
 // Fresh damping from the current normal equations (fitting.hh:531-538).
-__device__ __forceinline__ void lm_reset_damping(LmState& st)
+template <int P>
+__device__ __forceinline__ void lm_reset_damping(LmState<P>& st)
 {
     double damping = 1.0;   // InitialMinDamping
 #pragma unroll
-    for(int i = 0; i < kParams; ++i)
-        damping = fmax(damping, st.H[hidx(i, i)]);
+    for(int i = 0; i < P; ++i)
+        damping = fmax(damping, st.H[hix<P>(i, i)]);
     st.lam = damping * 0.75;   // InitialDampingMultiplier
     st.nu = 2.0;               // DampingFailureMultiplier
 }
 
 // Where the reference's loop ends, optionally continue with fresh damping from
 // the same point; false when the fit is finished.
-__device__ __forceinline__ bool lm_restart(LmState& st, const LmConfig& cfg, double n_pairs)
+template <int P>
+__device__ __forceinline__ bool lm_restart(LmState<P>& st, const LmConfig& cfg, double n_pairs)
 {
     if(st.restarts_left == 0 || !(st.iter < cfg.max_iter && cfg.mse_target < st.S / n_pairs))
         return false;
@@ -153,79 +192,81 @@ __device__ __forceinline__ bool lm_restart(LmState& st, const LmConfig& cfg, dou
 // parameter at 0 for good; its central difference at exactly 0 (fitting.hh:
 // 896-905, step 1e-8) is below float resolution there.  False when the
 // factorisation fails.
-__device__ __noinline__ bool lm_solve(LmState& st)
+template <int P, int B>
+__device__ __noinline__ bool lm_solve(LmState<P>& st)
 {
+    constexpr int kH = P * (P + 1) / 2;
     uint32_t frozen = 0;
     for(int round = 0; round < 5; ++round)
     {
-        double A[kHessian], x[kParams];
+        double A[kH], x[P];
 #pragma unroll
-        for(int i = 0; i < kHessian; ++i)
+        for(int i = 0; i < kH; ++i)
             A[i] = st.H[i];
 #pragma unroll
-        for(int i = 0; i < kParams; ++i)
+        for(int i = 0; i < P; ++i)
         {
-            A[hidx(i, i)] += st.lam;
+            A[hix<P>(i, i)] += st.lam;
             x[i] = st.g[i];
         }
 #pragma unroll
-        for(int i = 0; i < 4; ++i)
+        for(int i = 0; i < B; ++i)
             if(frozen & (1u << i))
             {
 #pragma unroll
-                for(int j = 0; j < kParams; ++j)
+                for(int j = 0; j < P; ++j)
                     if(j != i)
-                        A[hidx(i, j)] = 0.0;
+                        A[hix<P>(i, j)] = 0.0;
                 x[i] = 0.0;
             }
         // A = L L^T; the diagonal keeps 1 / L_jj
         bool ok = true;
 #pragma unroll
-        for(int j = 0; j < kParams; ++j)
+        for(int j = 0; j < P; ++j)
         {
-            double s = A[hidx(j, j)];
+            double s = A[hix<P>(j, j)];
 #pragma unroll
             for(int k = 0; k < j; ++k)
-                s -= A[hidx(j, k)] * A[hidx(j, k)];
+                s -= A[hix<P>(j, k)] * A[hix<P>(j, k)];
             ok = ok && (s > 0.0) && isfinite(s);
             const double r = rsqrt(s);
-            A[hidx(j, j)] = r;
+            A[hix<P>(j, j)] = r;
 #pragma unroll
-            for(int i = j + 1; i < kParams; ++i)
+            for(int i = j + 1; i < P; ++i)
             {
-                double t = A[hidx(i, j)];
+                double t = A[hix<P>(i, j)];
 #pragma unroll
                 for(int k = 0; k < j; ++k)
-                    t -= A[hidx(i, k)] * A[hidx(j, k)];
-                A[hidx(i, j)] = t * r;
+                    t -= A[hix<P>(i, k)] * A[hix<P>(j, k)];
+                A[hix<P>(i, j)] = t * r;
             }
         }
         if(!ok)
             return false;
 #pragma unroll
-        for(int i = 0; i < kParams; ++i)
+        for(int i = 0; i < P; ++i)
         {
             double t = x[i];
 #pragma unroll
             for(int k = 0; k < i; ++k)
-                t -= A[hidx(i, k)] * x[k];
-            x[i] = t * A[hidx(i, i)];
+                t -= A[hix<P>(i, k)] * x[k];
+            x[i] = t * A[hix<P>(i, i)];
         }
 #pragma unroll
-        for(int i = kParams - 1; i >= 0; --i)
+        for(int i = P - 1; i >= 0; --i)
         {
             double t = x[i];
 #pragma unroll
-            for(int k = i + 1; k < kParams; ++k)
-                t -= A[hidx(k, i)] * x[k];
-            x[i] = t * A[hidx(i, i)];
+            for(int k = i + 1; k < P; ++k)
+                t -= A[hix<P>(k, i)] * x[k];
+            x[i] = t * A[hix<P>(i, i)];
         }
         uint32_t more = frozen;
 #pragma unroll
-        for(int i = 0; i < kParams; ++i)
+        for(int i = 0; i < P; ++i)
         {
             st.d[i] = x[i];
-            if(i < 4 && st.p[i] == 0.0 && x[i] > 0.0)
+            if(i < B && st.p[i] == 0.0 && x[i] > 0.0)
                 more |= 1u << i;
         }
         if(more == frozen)
@@ -237,7 +278,31 @@ __device__ __noinline__ bool lm_solve(LmState& st)
 
 // Top of one LM iteration (fitting.hh:541-590): find a step that passes the
 // constraints, or finish.  kCmdTrial (st.pt holds the trial point) or kCmdDone.
-__device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
+// Unit quaternion of the rotation vector phi (Exp([phi]x)), xyzw.
+__device__ __forceinline__ void quat_exp(const double* phi, double* q)
+{
+    const double a2 = phi[0] * phi[0] + phi[1] * phi[1] + phi[2] * phi[2];
+    const double a = sqrt(a2);
+    const double h = 0.5 * a;
+    const double k = a > 1e-12 ? sin(h) / a : 0.5 - a2 / 48.0;
+    q[0] = k * phi[0];
+    q[1] = k * phi[1];
+    q[2] = k * phi[2];
+    q[3] = cos(h);
+}
+
+// r = a (x) b, Hamilton product, xyzw: the rotation of a followed, in a's body
+// frame, by that of b (R(a b) = R(a) R(b)).
+__device__ __forceinline__ void quat_mul(const double* a, const double* b, double* r)
+{
+    r[0] = a[3] * b[0] + a[0] * b[3] + a[1] * b[2] - a[2] * b[1];
+    r[1] = a[3] * b[1] - a[0] * b[2] + a[1] * b[3] + a[2] * b[0];
+    r[2] = a[3] * b[2] + a[0] * b[1] - a[1] * b[0] + a[2] * b[3];
+    r[3] = a[3] * b[3] - a[0] * b[0] - a[1] * b[1] - a[2] * b[2];
+}
+
+template <class M>
+__device__ int lm_next(LmState<M::P>& st, const LmConfig& cfg, double n_pairs)
 {
     for(;;)
     {
@@ -247,7 +312,7 @@ __device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
                 st.status |= SVF_TEXEL_MAX_ITER;
             return kCmdDone;
         }
-        if(!lm_solve(st))
+        if(!lm_solve<M::P, M::B>(st))
         {
             // the reference's inverse came out non-finite: damp harder
             st.lam *= st.nu;
@@ -257,10 +322,10 @@ __device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
         }
         double step2 = 0.0, mag2 = 0.0;
 #pragma unroll
-        for(int i = 0; i < kParams; ++i)
+        for(int i = 0; i < M::P; ++i)
         {
             step2 += st.d[i] * st.d[i];
-            const double t = st.p[i] + cfg.eps;
+            const double t = st.p[i] + cfg.eps;   // (an RGB rotation entry is 0)
             mag2 += t * t;
         }
         const double step_len = sqrt(step2);
@@ -278,7 +343,7 @@ __device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
         // AcceptStepConstraints (svbrdf-lsq-fitting-internal.hh:67-77)
         bool accept = true;
 #pragma unroll
-        for(int i = 0; i < 4; ++i)
+        for(int i = 0; i < M::B; ++i)
             if(st.p[i] - st.d[i] < 0.0f)
                 accept = false;
         if(!accept)
@@ -289,19 +354,27 @@ __device__ int lm_next(LmState& st, const LmConfig& cfg, double n_pairs)
             continue;
         }
 #pragma unroll
-        for(int i = 0; i < kParams; ++i)
+        for(int i = 0; i < M::P; ++i)
             st.pt[i] = st.p[i] - st.d[i];
+        if(M::kRgb)
+        {
+            // the orientation moves by the local rotation phi = -d
+            double dq[4];
+            quat_exp(st.pt + M::B, dq);
+            quat_mul(st.q, dq, st.qt);
+        }
         return kCmdTrial;
     }
 }
 
 // After the trial residual (fitting.hh:597-612,661-674): accept or damp.
-__device__ int lm_after_trial(LmState& st, const LmConfig& cfg, double S1, double n_pairs)
+template <class M>
+__device__ int lm_after_trial(LmState<M::P>& st, const LmConfig& cfg, double S1, double n_pairs)
 {
     ++st.nres;
     double pred = 0.0;
 #pragma unroll
-    for(int i = 0; i < kParams; ++i)
+    for(int i = 0; i < M::P; ++i)
         pred += st.d[i] * (st.d[i] * st.lam + st.g[i]);
     pred *= 0.5;
     const double rho = 0.5 * (st.S - S1) / pred;
@@ -309,8 +382,17 @@ __device__ int lm_after_trial(LmState& st, const LmConfig& cfg, double S1, doubl
     {
         ++st.eff;
 #pragma unroll
-        for(int i = 0; i < kParams; ++i)
+        for(int i = 0; i < M::P; ++i)
             st.p[i] = st.pt[i];
+        if(M::kRgb)
+        {
+            const double n = sqrt(st.qt[0] * st.qt[0] + st.qt[1] * st.qt[1] + st.qt[2] * st.qt[2] +
+                                  st.qt[3] * st.qt[3]);
+            for(int i = 0; i < 4; ++i)
+                st.q[i] = st.qt[i] / n;
+            for(int i = M::B; i < M::P; ++i)
+                st.p[i] = 0.0;
+        }
         st.S = S1;
         st.rho = rho;
         if(S1 / n_pairs <= cfg.mse_target)
@@ -324,19 +406,22 @@ __device__ int lm_after_trial(LmState& st, const LmConfig& cfg, double S1, doubl
 }
 
 // After the Jacobian at an accepted point (fitting.hh:612-660).
-__device__ int lm_after_jacobian(LmState& st, const LmConfig& cfg, const double* red, double n_pairs)
+// hg: J^T J (packed upper) then J^T r, in FP64.
+template <int P>
+__device__ int lm_after_jacobian(LmState<P>& st, const LmConfig& cfg, const double* hg, double n_pairs)
 {
+    constexpr int kH = P * (P + 1) / 2;
     ++st.njac;
     double glen = 0.0;
 #pragma unroll
-    for(int i = 0; i < kParams; ++i)
+    for(int i = 0; i < P; ++i)
     {
-        st.g[i] = -red[kHessian + i];
+        st.g[i] = -hg[kH + i];
         glen += st.g[i] * st.g[i];
     }
 #pragma unroll
-    for(int i = 0; i < kHessian; ++i)
-        st.H[i] = red[i];
+    for(int i = 0; i < kH; ++i)
+        st.H[i] = hg[i];
     if(glen <= cfg.eps * cfg.eps)
         return lm_restart(st, cfg, n_pairs) ? kCmdContinue : kCmdDone;
     const double min_mul = (double)(1.0f / 3.0f);
@@ -356,6 +441,7 @@ struct PassConst
 {
     float u, v, rsx, rsy, ks, kd, ks_on, kd_on;
     float om[9];
+    float kdc[3], ksc[3];   // RGB: clamped per-channel albedos
 };
 
 __host__ __device__ inline uint32_t pad4(uint32_t x) { return (x + 3u) & ~3u; }
@@ -367,11 +453,15 @@ __host__ __device__ inline uint32_t pad4(uint32_t x) { return (x + 3u) & ~3u; }
 // The directions themselves are not
 // kept: R is orthonormal, so |w_i + w_o| = |s| and cos(h, w_i) = s.a_i / |s|
 // with s = a_i + a_o.  Built by the 32 lanes of the control warp.
+template <class M>
 __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32_t L, const float* pf, PassConst* pc,
                                             uint32_t lane)
 {
     ParamSet ps;
-    make_param_set(pf, ps);
+    if(M::kRgb)
+        make_param_set_rgb(pf, ps);
+    else
+        make_param_set(pf, ps);
     float4* core0 = reinterpret_cast<float4*>(tab);
     float4* core1 = core0 + pad4(L);
     float4* deriv = core1 + pad4(L);
@@ -399,6 +489,12 @@ __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32
 #pragma unroll
             for(int j = 0; j < 3; ++j)
                 pc->om[3 * k + j] = ps.om[k][j];
+        if(M::kRgb)
+            for(int k = 0; k < 3; ++k)
+            {
+                pc->kdc[k] = pf[k] > 0.0f ? pf[k] : 0.0f;
+                pc->ksc[k] = pf[3 + k] > 0.0f ? pf[3 + k] : 0.0f;
+            }
     }
 }
 
@@ -565,12 +661,104 @@ __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, co
     }
 }
 
+// The RGB pair: the geometry of sym_pair, three channels.  Per ordered pair k
+// and channel c:  f_kc = kd_c h_k + ks_c sp_k,  r_kc = y_kc - f_kc, and
+//   J_kc = kd_on_c h_k e_kd_c + ks_on_c sp_k e_ks_c + ks_c sp_k sum_j G_j e_j
+// over the geometric parameters j = {sx, sy, phi xyz} (G as V / ks in
+// sym_pair, with the identity body rates of the local rotation).  J^T J and
+// J^T r then need only channel-free sums, which each lane accumulates:
+//   acc[0..2]   sum h^2, sum sp^2, sum h sp
+//   acc[3..7]   sum h sp G_j          acc[8..12]  sum sp^2 G_j
+//   acc[13..27] sum sp^2 G_i G_j (i <= j)
+//   acc[28..30] sum h r_c             acc[31..33] sum sp r_c
+//   acc[34..38] sum sp G_j (sum_c ks_c r_c)
+// and expand_rgb assembles the 11 x 11 system from them in FP64.
+template <bool kFresnel, bool kAllUp>
+__device__ __forceinline__ void sym_pair_rgb(const PassConst& c, const Entry& ea, const Entry& eb, float refr,
+                                             const float* y1, const float* y2, float wt1, float wt2, float* acc,
+                                             double& r2)
+{
+    const float s0 = ea.a0 + eb.a0, s1 = ea.a1 + eb.a1, s2 = ea.a2 + eb.a2;
+    const float q0 = s0 * s0, q1 = s1 * s1, q2 = s2 * s2;
+    const float g = q0 + q1 + q2;
+    const float Q = c.u * q0 + c.v * q1 + q2;
+    const float S = ea.sp + eb.sp;
+    const float QQ = Q * Q;
+    const float QQS = QQ * S;
+    const float rden = QQS > 1e-37f ? rcp_approx(QQS) : 0.0f;
+    float F = 1.0f;
+    if(kFresnel)
+    {
+        const float wa[3] = { ea.a0, ea.a1, ea.a2 }, wb[3] = { eb.a0, eb.a1, eb.a2 };
+        F = fresnel_factor(refr, wb, wa);
+    }
+    const float C = F * g * g * rden;
+    const float w1 = kAllUp ? wt1 * ea.kv : wt1 * ea.kv * eb.up;
+    const float w2 = kAllUp ? wt2 * eb.kv : wt2 * eb.kv * ea.up;
+    const float h1 = kAllUp ? wt1 * eb.kdc : wt1 * ea.up * eb.kdc;
+    const float h2 = kAllUp ? wt2 * ea.kdc : wt2 * eb.up * ea.kdc;
+    const float sp1 = w1 * C, sp2 = w2 * C;
+    float r1[3], rb[3];
+    float e2 = 0.0f, k1 = 0.0f, k2 = 0.0f;
+#pragma unroll
+    for(int ch = 0; ch < 3; ++ch)
+    {
+        r1[ch] = y1[ch] - (c.kdc[ch] * h1 + c.ksc[ch] * sp1);
+        rb[ch] = y2[ch] - (c.kdc[ch] * h2 + c.ksc[ch] * sp2);
+        e2 = fmaf(r1[ch], r1[ch], fmaf(rb[ch], rb[ch], e2));
+        k1 = fmaf(c.ksc[ch], r1[ch], k1);
+        k2 = fmaf(c.ksc[ch], rb[ch], k2);
+    }
+    r2 += (double)e2;
+    const float rQ = Q * S * rden;
+    const float rS = QQ * rden;
+    const float t0 = s1 * s2 * (c.v - 1.0f);
+    const float t1 = s0 * s2 * (1.0f - c.u);
+    const float t2 = s0 * s1 * (c.u - c.v);
+    float G[5];
+    G[0] = c.rsx * (4.0f * c.u * q0 * rQ - 1.0f) - (ea.d0 + eb.d0) * rS;
+    G[1] = c.rsy * (4.0f * c.v * q1 * rQ - 1.0f) - (ea.d1 + eb.d1) * rS;
+    const float m4 = -4.0f * rQ;
+    G[2] = m4 * t0 - (ea.d2 + eb.d2) * rS;
+    G[3] = m4 * t1 - (ea.d3 + eb.d3) * rS;
+    G[4] = m4 * t2 - (ea.d4 + eb.d4) * rS;
+    const float Phh = h1 * h1 + h2 * h2, Pss = sp1 * sp1 + sp2 * sp2, Phs = h1 * sp1 + h2 * sp2;
+    const float R = sp1 * k1 + sp2 * k2;
+    acc[0] += Phh;
+    acc[1] += Pss;
+    acc[2] += Phs;
+    float PG[5];
+#pragma unroll
+    for(int j = 0; j < 5; ++j)
+    {
+        acc[3 + j] = fmaf(Phs, G[j], acc[3 + j]);
+        PG[j] = Pss * G[j];
+        acc[8 + j] += PG[j];
+        acc[34 + j] = fmaf(R, G[j], acc[34 + j]);
+    }
+    int n = 13;
+#pragma unroll
+    for(int i = 0; i < 5; ++i)
+#pragma unroll
+        for(int j = i; j < 5; ++j)
+        {
+            acc[n] = fmaf(PG[i], G[j], acc[n]);
+            ++n;
+        }
+#pragma unroll
+    for(int ch = 0; ch < 3; ++ch)
+    {
+        acc[28 + ch] = fmaf(h1, r1[ch], fmaf(h2, rb[ch], acc[28 + ch]));
+        acc[31 + ch] = fmaf(sp1, r1[ch], fmaf(sp2, rb[ch], acc[31 + ch]));
+    }
+}
+
 // One step of a worker lane over its unordered pairs: pair f = (a, d), then
 // f += 32 NW.  kGuard: f may be past the enumeration or, for even L, on the
 // repeated offset L/2 (such slots get zero weights, y = 0 and in-range
 // indices); without it every pair is valid (odd L, f < total).
-template <int NW, bool kFresnel, bool kAllUp, bool kGuard>
-__device__ __forceinline__ void pair_step(const float* tab, const PassConst& c, const float* slab, uint32_t L,
+template <class M, int NW, bool kFresnel, bool kAllUp, bool kGuard>
+__device__ __forceinline__ void pair_step(const float* tab, const PassConst& c, const typename M::Slab* slab, uint32_t L,
                                           uint32_t Lp, uint32_t nd, uint32_t total, uint32_t sa, uint32_t sd, float refr,
                                           uint32_t& f, uint32_t& a, uint32_t& d, float* acc, double& r2)
 {
@@ -581,11 +769,29 @@ __device__ __forceinline__ void pair_step(const float* tab, const PassConst& c, 
     const Entry ea = load_entry(tab, Lp, ia);
     const Entry eb = load_entry(tab, Lp, ib);
     // pair 1: view a, light b (slab row a); pair 2: view b, light a
-    const float y1 = valid ? slab[ia * L + ib] : 0.0f;
     const bool two = valid && d != 0u;
-    const float y2 = two ? slab[ib * L + ia] : 0.0f;
-    sym_pair<kFresnel, kAllUp>(c, ea, eb, refr, y1, y2, kGuard ? (valid ? 1.0f : 0.0f) : 1.0f, two ? 1.0f : 0.0f,
-                               acc, r2);
+    if(M::kRgb)
+    {
+        float y1[3], y2[3];
+        const __half* s1 = reinterpret_cast<const __half*>(slab) + 3 * (ia * L + ib);
+        const __half* s2 = reinterpret_cast<const __half*>(slab) + 3 * (ib * L + ia);
+#pragma unroll
+        for(int ch = 0; ch < 3; ++ch)
+        {
+            y1[ch] = valid ? __half2float(s1[ch]) : 0.0f;
+            y2[ch] = two ? __half2float(s2[ch]) : 0.0f;
+        }
+        sym_pair_rgb<kFresnel, kAllUp>(c, ea, eb, refr, y1, y2, kGuard ? (valid ? 1.0f : 0.0f) : 1.0f,
+                                       two ? 1.0f : 0.0f, acc, r2);
+    }
+    else
+    {
+        const float* fs = reinterpret_cast<const float*>(slab);
+        const float y1 = valid ? fs[ia * L + ib] : 0.0f;
+        const float y2 = two ? fs[ib * L + ia] : 0.0f;
+        sym_pair<kFresnel, kAllUp>(c, ea, eb, refr, y1, y2, kGuard ? (valid ? 1.0f : 0.0f) : 1.0f, two ? 1.0f : 0.0f,
+                                   acc, r2);
+    }
     f += 32u * NW;
     a += sa;
     d += sd;
@@ -600,11 +806,12 @@ __device__ __forceinline__ void pair_step(const float* tab, const PassConst& c, 
 // wtid, wtid + 32 NW, ...).  Writes the warp's partial sums: J^T J and J^T r
 // to red[wwarp][0..34] and r^2 to redd[wwarp].  Every lane runs the same
 // number of steps; for odd L only the last one needs the guard.
-template <int NW, bool kFresnel, bool kAllUp>
-__device__ void worker_pass(const float* tab, const PassConst& c, const float* slab, uint32_t L, float refr,
-                            float* red, double* redd, uint32_t wwarp, uint32_t lane)
+template <class M, int NW, bool kFresnel, bool kAllUp>
+__device__ void worker_pass(const float* tab, const PassConst& c, const typename M::Slab* slab, uint32_t L,
+                            float refr, float* red, double* redd, uint32_t wwarp, uint32_t lane)
 {
-    static_assert(kRed == 35, "reduction layout: 32 reduce-scattered sums + 3");
+    constexpr int kAcc = M::kAcc;
+    static_assert(kAcc >= 32, "reduction layout: 32 reduce-scattered sums + the rest");
     constexpr uint32_t kStride = 32u * NW;
     const uint32_t half = L >> 1, nd = half + 1, Lp = pad4(L);
     const uint32_t total = L * nd;
@@ -615,27 +822,28 @@ __device__ void worker_pass(const float* tab, const PassConst& c, const float* s
     uint32_t a = f / nd, d = f - a * nd;
 
     double r2 = 0.0;
-    float acc[kRed];
+    float acc[kAcc];
 #pragma unroll
-    for(int i = 0; i < kRed; ++i)
+    for(int i = 0; i < kAcc; ++i)
         acc[i] = 0.0f;
 
     for(uint32_t it = 0; it < full; ++it)
-        pair_step<NW, kFresnel, kAllUp, false>(tab, c, slab, L, Lp, nd, total, sa, sd, refr, f, a, d, acc, r2);
+        pair_step<M, NW, kFresnel, kAllUp, false>(tab, c, slab, L, Lp, nd, total, sa, sd, refr, f, a, d, acc, r2);
     for(uint32_t it = full; it < iters; ++it)
-        pair_step<NW, kFresnel, kAllUp, true>(tab, c, slab, L, Lp, nd, total, sa, sd, refr, f, a, d, acc, r2);
+        pair_step<M, NW, kFresnel, kAllUp, true>(tab, c, slab, L, Lp, nd, total, sa, sd, refr, f, a, d, acc, r2);
 
     r2 = warp_sum(r2);
     {
-        const float t32 = warp_sum(acc[32]), t33 = warp_sum(acc[33]), t34 = warp_sum(acc[34]);
+        float rest[kAcc - 32];
+#pragma unroll
+        for(int i = 32; i < kAcc; ++i)
+            rest[i - 32] = warp_sum(acc[i]);
         reduce_scatter32(acc, lane);
-        red[wwarp * kRed + lane] = acc[0];
+        red[wwarp * kAcc + lane] = acc[0];
         if(lane == 0)
-        {
-            red[wwarp * kRed + 32] = t32;
-            red[wwarp * kRed + 33] = t33;
-            red[wwarp * kRed + 34] = t34;
-        }
+#pragma unroll
+            for(int i = 32; i < kAcc; ++i)
+                red[wwarp * kAcc + i] = rest[i - 32];
     }
     if(lane == 0)
         redd[wwarp] = r2;
@@ -655,12 +863,14 @@ enum : int
 constexpr uint32_t kNoTexel = 0xffffffffu;
 
 // Per-slot control state (static shared memory).
+template <class M>
 struct Slot
 {
-    LmState st;
+    LmState<M::P> st;
     PassConst pc;
-    double sums[kRed + 1];
-    float pf[kParams];
+    double sums[M::kAcc + 1];                   // the pass's sums; [kAcc] = r^2
+    double hg[M::P * (M::P + 1) / 2 + M::P];    // J^T J and J^T r assembled from them
+    float pf[M::kOut];                          // the tabulated point
     uint64_t bar;         // the slab copy's mbarrier
     uint32_t texel;       // texel in the slot, or kNoTexel
     uint32_t parity;      // next phase of `bar`
@@ -671,19 +881,25 @@ struct Slot
     uint32_t arrived;     // worker warps done with the current pass (the last one sums)
     uint32_t L;           // layout of the texel in the slot
     uint32_t slab_bytes;
-    double npairs;        // L^2
+    double npairs;        // residuals per texel: channels x L^2
     const float* geo;
 };
 
 // Dynamic shared memory per slot: [stride] slab | [Lp][kEntry] table |
-// [NW] double partials | [NW][kRed] float partials (doubles first: NW * kRed
+// [NW] double partials | [NW][kAcc] float partials (doubles first: NW * kAcc
 // floats need not be a multiple of 8 bytes).  Every part starts 128-byte aligned.
-template <int NW>
+template <int NW, class M>
 struct SlotSmem
 {
-    __host__ __device__ static size_t slab_bytes(uint64_t stride) { return (sizeof(float) * stride + 127) & ~size_t(127); }
+    __host__ __device__ static size_t slab_bytes(uint64_t stride)
+    {
+        return (sizeof(typename M::Slab) * stride + 127) & ~size_t(127);
+    }
     __host__ __device__ static size_t tab_bytes(uint32_t L) { return (sizeof(float) * kEntry * pad4(L) + 127) & ~size_t(127); }
-    __host__ __device__ static size_t red_bytes() { return (sizeof(float) * NW * kRed + sizeof(double) * NW + 127) & ~size_t(127); }
+    __host__ __device__ static size_t red_bytes()
+    {
+        return (sizeof(float) * NW * M::kAcc + sizeof(double) * NW + 127) & ~size_t(127);
+    }
     __host__ __device__ static size_t bytes(uint32_t L, uint64_t stride)
     {
         return slab_bytes(stride) + tab_bytes(L) + red_bytes();
@@ -707,14 +923,57 @@ __device__ __forceinline__ uint32_t bar_done(int s) { return 1u + (uint32_t)S + 
 
 // Writes a finished texel's outputs (LeastSquaresFitSGGX :381-429,
 // SVBRDFFitPipeline::fit :692-697).  Control thread.
-__device__ void write_texel(const LmArgs& args, LmState& st, uint32_t t, double n_pairs)
+template <class M>
+__device__ void write_texel(const LmArgs& args, LmState<M::P>& st, uint32_t t, double n_pairs)
 {
-    float pout[kParams];
+    if(M::kRgb)
+    {
+        // {kd rgb, ks rgb, sx, sy, quaternion xyzw}; maps: the fitted albedos,
+        // sigma and the orientation
+        float pout[12];
+        for(int i = 0; i < 8; ++i)
+            pout[i] = (float)st.p[i];
+        for(int i = 0; i < 4; ++i)
+            pout[8 + i] = (float)st.q[i];
+        for(int i = 0; i < 12; ++i)
+            args.out[(uint64_t)t * 12 + i] = pout[i];
+        const double mse = st.S / n_pairs;
+        if(!isfinite(mse))
+            st.status |= SVF_TEXEL_NONFINITE;
+        args.rmse[t] = (float)sqrt(mse);
+        if(args.stats)
+        {
+            svf_texel_stats s;
+            s.iterations = st.iter;
+            s.effective = st.eff;
+            s.jacobians = st.njac;
+            s.residuals = st.nres;
+            s.status = st.status;
+            args.stats[t] = s;
+        }
+        for(int k = 0; k < 3; ++k)
+        {
+            if(args.map_diffuse)
+                args.map_diffuse[3 * (uint64_t)t + k] = pout[k];
+            if(args.map_specular)
+                args.map_specular[3 * (uint64_t)t + k] = pout[3 + k];
+        }
+        if(args.map_sigma)
+        {
+            args.map_sigma[2 * (uint64_t)t] = pout[6];
+            args.map_sigma[2 * (uint64_t)t + 1] = pout[7];
+        }
+        if(args.map_basis)
+            for(int i = 0; i < 4; ++i)
+                args.map_basis[4 * (uint64_t)t + i] = pout[8 + i];
+        return;
+    }
+    float pout[7];
 #pragma unroll
-    for(int i = 0; i < kParams; ++i)
+    for(int i = 0; i < 7; ++i)
     {
         pout[i] = (float)st.p[i];
-        args.out[(uint64_t)t * kParams + i] = pout[i];
+        args.out[(uint64_t)t * 7 + i] = pout[i];
     }
     const double mse = st.S / n_pairs;
     if(!isfinite(mse))
@@ -764,7 +1023,8 @@ __device__ void write_texel(const LmArgs& args, LmState& st, uint32_t t, double 
 
 // Control thread: takes the next texel for slot `sl` and starts its slab copy
 // (the slab is no longer read: the workers finished the slot's last pass).
-__device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot& sl, float* slab)
+template <class M>
+__device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot<M>& sl, void* slab)
 {
     const uint32_t t = sl.dead ? kNoTexel : atomicAdd(args.work_counter, 1u);
     if(t < args.texels)
@@ -775,10 +1035,11 @@ __device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot& sl, float* 
                 k = i;
         const LmSegment& g = args.seg[k];
         sl.L = g.L;
-        sl.npairs = (double)g.L * (double)g.L;
+        sl.npairs = (double)M::kChannels * (double)g.L * (double)g.L;
         sl.geo = g.geo;
-        sl.slab_bytes = (uint32_t)(g.stride * sizeof(float));
-        bulk_load(slab, g.lum + (uint64_t)(t - g.first) * g.stride, sl.slab_bytes, &sl.bar);
+        sl.slab_bytes = (uint32_t)(g.stride * sizeof(typename M::Slab));
+        bulk_load(slab, static_cast<const typename M::Slab*>(g.lum) + (uint64_t)(t - g.first) * g.stride, sl.slab_bytes,
+                  &sl.bar);
         sl.texel = t;
         sl.loading = 1;
     }
@@ -792,7 +1053,8 @@ __device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot& sl, float* 
 
 // Control thread: the slot's slab has arrived; set up the fit of its texel.
 // False when the copy did not arrive within the bound.
-__device__ __forceinline__ bool slot_start(const LmArgs& args, Slot& sl)
+template <class M>
+__device__ __forceinline__ bool slot_start(const LmArgs& args, Slot<M>& sl)
 {
     if(!mbar_wait(&sl.bar, sl.parity))
     {
@@ -807,13 +1069,31 @@ __device__ __forceinline__ bool slot_start(const LmArgs& args, Slot& sl)
     }
     sl.parity ^= 1u;
     sl.loading = 0;
-    LmState& st = sl.st;
+    LmState<M::P>& st = sl.st;
+    const float* in = args.init + (uint64_t)sl.texel * M::kOut;
 #pragma unroll
-    for(int i = 0; i < kParams; ++i)
+    for(int i = 0; i < M::kOut; ++i)
+        sl.pf[i] = in[i];
+    if(M::kRgb)
     {
-        st.p[i] = (double)args.init[(uint64_t)sl.texel * kParams + i];
-        sl.pf[i] = (float)st.p[i];
+        for(int i = 0; i < M::B; ++i)
+            st.p[i] = (double)in[i];
+        for(int i = M::B; i < M::P; ++i)
+            st.p[i] = 0.0;
+        double n = 0.0;
+        for(int i = 0; i < 4; ++i)
+        {
+            st.q[i] = (double)in[M::B + i];
+            n += st.q[i] * st.q[i];
+        }
+        n = n > 0.0 ? 1.0 / sqrt(n) : 0.0;
+        for(int i = 0; i < 4; ++i)
+            st.q[i] = n > 0.0 ? st.q[i] * n : (i == 3 ? 1.0 : 0.0);
     }
+    else
+#pragma unroll
+        for(int i = 0; i < M::P; ++i)
+            st.p[i] = (double)in[i];
     st.iter = st.eff = st.njac = st.nres = st.status = 0;
     st.restarts_left = args.cfg.restarts;
     sl.first = 1;
@@ -822,15 +1102,15 @@ __device__ __forceinline__ bool slot_start(const LmArgs& args, Slot& sl)
 }
 
 // FP64 sums of the worker warps' partials, one lane per sum, warps in order.
-template <int NW>
+template <int NW, int kAcc>
 __device__ __forceinline__ void sum_partials(const float* red, const double* redd, double* sums, uint32_t lane)
 {
-    for(uint32_t i = lane; i < (uint32_t)kRed; i += 32)
+    for(uint32_t i = lane; i < (uint32_t)kAcc; i += 32)
     {
         double t = 0.0;
 #pragma unroll
         for(int w = 0; w < NW; ++w)
-            t += (double)red[w * kRed + i];
+            t += (double)red[w * kAcc + i];
         sums[i] = t;
     }
     if(lane == 0)
@@ -839,26 +1119,73 @@ __device__ __forceinline__ void sum_partials(const float* red, const double* red
 #pragma unroll
         for(int w = 0; w < NW; ++w)
             t += redd[w];
-        sums[kRed] = t;
+        sums[kAcc] = t;
+    }
+}
+
+// J^T J and J^T r of the pass at the tabulated point pf (control thread).
+// Luminance: the sums are already in that layout.  RGB: assembled from the
+// channel-factored sums of sym_pair_rgb; the parameter order is kd rgb (0-2),
+// ks rgb (3-5), sx, sy, phi xyz (6-10), and kd_on / ks_on mask the albedo
+// derivatives as in the luminance fit.
+template <class M>
+__device__ void expand_sums(const double* sums, const float* pf, double* hg)
+{
+    constexpr int P = M::P, kH = P * (P + 1) / 2;
+    if(!M::kRgb)
+    {
+        for(int i = 0; i < kH + P; ++i)
+            hg[i] = sums[i];
+        return;
+    }
+    for(int i = 0; i < kH + P; ++i)
+        hg[i] = 0.0;
+    double ks[3], kdon[3], kson[3], ks2 = 0.0;
+    for(int c = 0; c < 3; ++c)
+    {
+        ks[c] = pf[3 + c] > 0.0f ? (double)pf[3 + c] : 0.0;
+        kdon[c] = pf[c] >= 0.0f ? 1.0 : 0.0;
+        kson[c] = pf[3 + c] >= 0.0f ? 1.0 : 0.0;
+        ks2 += ks[c] * ks[c];
+    }
+    for(int c = 0; c < 3; ++c)
+    {
+        hg[hix<P>(c, c)] = kdon[c] * sums[0];
+        hg[hix<P>(3 + c, 3 + c)] = kson[c] * sums[1];
+        hg[hix<P>(c, 3 + c)] = kdon[c] * kson[c] * sums[2];
+        for(int j = 0; j < 5; ++j)
+        {
+            hg[hix<P>(c, 6 + j)] = kdon[c] * ks[c] * sums[3 + j];
+            hg[hix<P>(3 + c, 6 + j)] = kson[c] * ks[c] * sums[8 + j];
+        }
+        hg[kH + c] = kdon[c] * sums[28 + c];
+        hg[kH + 3 + c] = kson[c] * sums[31 + c];
+    }
+    for(int i = 0; i < 5; ++i)
+    {
+        for(int j = i; j < 5; ++j)
+            hg[hix<P>(6 + i, 6 + j)] = ks2 * sums[13 + hix<5>(i, j)];
+        hg[kH + 6 + i] = sums[34 + i];
     }
 }
 
 // Resident CTAs per SM the register budget is sized for.
 constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : 2; }
 
-template <int NW, int S, bool kFresnel, bool kAllUp>
+template <class M, int NW, int S, bool kFresnel, bool kAllUp>
 __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_fit_kernel(LmArgs args)
 {
     constexpr uint32_t kThreads = 32 * (NW + 1);
-    using SM = SlotSmem<NW>;
+    using SM = SlotSmem<NW, M>;
+    using SlabT = typename M::Slab;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ Slot slots[S];
+    __shared__ Slot<M> slots[S];
 
     const uint32_t L = args.L;   // the largest layout: sizes each slot's shared memory
     const size_t per_slot = SM::bytes(L, args.lum_stride);
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
 
-    auto slab_of = [&](int s) { return reinterpret_cast<float*>(smem_raw + s * per_slot); };
+    auto slab_of = [&](int s) { return reinterpret_cast<SlabT*>(smem_raw + s * per_slot); };
     auto tab_of = [&](int s) { return reinterpret_cast<float*>(smem_raw + s * per_slot + SM::slab_bytes(args.lum_stride)); };
     auto redd_of = [&](int s) {
         return reinterpret_cast<double*>(smem_raw + s * per_slot + SM::slab_bytes(args.lum_stride) + SM::tab_bytes(L));
@@ -877,8 +1204,8 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 break;
             if(cmd == kSlotPass)
             {
-                worker_pass<NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), slots[s].L, args.cfg.fresnel,
-                                                  red_of(s), redd_of(s), wwarp, lane);
+                worker_pass<M, NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), slots[s].L,
+                                                     args.cfg.fresnel, red_of(s), redd_of(s), wwarp, lane);
                 // the last worker warp to finish sums the partials in FP64, in warp
                 // order (deterministic), while the others move on
                 __syncwarp();
@@ -893,7 +1220,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 if(prior == NW - 1)
                 {
                     __syncwarp();
-                    sum_partials<NW>(red_of(s), redd_of(s), slots[s].sums, lane);
+                    sum_partials<NW, M::kAcc>(red_of(s), redd_of(s), slots[s].sums, lane);
                     if(lane == 0)
                         slots[s].arrived = 0;
                     __syncwarp();
@@ -909,7 +1236,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
     {
         for(int s = 0; s < S; ++s)
         {
-            Slot& sl = slots[s];
+            Slot<M>& sl = slots[s];
             mbar_init(&sl.bar, 1);
             sl.parity = 0;
             sl.dead = 0;
@@ -924,21 +1251,21 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
     for(int s = 0; s < S; ++s)
     {
         if(slots[s].cmd == kSlotPass)
-            build_table(tab_of(s), slots[s].geo, slots[s].L, slots[s].pf, &slots[s].pc, lane);
+            build_table<M>(tab_of(s), slots[s].geo, slots[s].L, slots[s].pf, &slots[s].pc, lane);
         __syncwarp();
         nbar_arrive(bar_ready(s), kThreads);
     }
 
     for(int s = 0;; s = (s + 1 == S) ? 0 : s + 1)
     {
-        Slot& sl = slots[s];
+        Slot<M>& sl = slots[s];
         nbar_sync(bar_done<S>(s), kThreads);
         const int done_cmd = sl.cmd;   // the last worker warp has left the sums in sl.sums
 
         bool build = false, exit_now = false;
         if(lane == 0)
         {
-            LmState& st = sl.st;
+            LmState<M::P>& st = sl.st;
             int next = kCmdDone;
             if(done_cmd == kSlotPass)
             {
@@ -946,17 +1273,19 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 // the Jacobian of an accepted step is then already at hand, so
                 // the separate Jacobian evaluation of fitting.hh:612-616 at the
                 // same point is not repeated (same arithmetic, same result).
+                constexpr int kH = M::P * (M::P + 1) / 2;
+                expand_sums<M>(sl.sums, sl.pf, sl.hg);
                 if(sl.first)
                 {
                     sl.first = 0;
                     st.njac = 1;
-                    st.S = sl.sums[kRed];
+                    st.S = sl.sums[M::kAcc];
 #pragma unroll
-                    for(int i = 0; i < kParams; ++i)
-                        st.g[i] = -sl.sums[kHessian + i];
+                    for(int i = 0; i < M::P; ++i)
+                        st.g[i] = -sl.hg[kH + i];
 #pragma unroll
-                    for(int i = 0; i < kHessian; ++i)
-                        st.H[i] = sl.sums[i];
+                    for(int i = 0; i < kH; ++i)
+                        st.H[i] = sl.hg[i];
                     lm_reset_damping(st);
                     if(!isfinite(st.S))
                         st.status |= SVF_TEXEL_NONFINITE;
@@ -964,23 +1293,31 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 }
                 else
                 {
-                    next = lm_after_trial(st, args.cfg, sl.sums[kRed], sl.npairs);
+                    next = lm_after_trial<M>(st, args.cfg, sl.sums[M::kAcc], sl.npairs);
                     if(next == kCmdJacobian)
-                        next = lm_after_jacobian(st, args.cfg, sl.sums, sl.npairs);
+                        next = lm_after_jacobian(st, args.cfg, sl.hg, sl.npairs);
                 }
                 if(next == kCmdContinue)
-                    next = lm_next(st, args.cfg, sl.npairs);
+                    next = lm_next<M>(st, args.cfg, sl.npairs);
                 if(next == kCmdTrial)
                 {
+                    if(M::kRgb)
+                    {
+                        for(int i = 0; i < M::B; ++i)
+                            sl.pf[i] = (float)st.pt[i];
+                        for(int i = 0; i < 4; ++i)
+                            sl.pf[M::B + i] = (float)st.qt[i];
+                    }
+                    else
 #pragma unroll
-                    for(int i = 0; i < kParams; ++i)
-                        sl.pf[i] = (float)st.pt[i];
+                        for(int i = 0; i < M::P; ++i)
+                            sl.pf[i] = (float)st.pt[i];
                     sl.cmd = kSlotPass;
                     build = true;
                 }
                 else
                 {
-                    write_texel(args, st, sl.texel, sl.npairs);
+                    write_texel<M>(args, st, sl.texel, sl.npairs);
                     slot_fetch(args, sl, slab_of(s));
                 }
             }
@@ -1005,7 +1342,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
         build = __shfl_sync(0xffffffffu, build, 0);
         exit_now = __shfl_sync(0xffffffffu, exit_now, 0);
         if(build)
-            build_table(tab_of(s), sl.geo, sl.L, sl.pf, &sl.pc, lane);
+            build_table<M>(tab_of(s), sl.geo, sl.L, sl.pf, &sl.pc, lane);
         __syncwarp();
         nbar_arrive(bar_ready(s), kThreads);
         if(exit_now)
@@ -1021,62 +1358,74 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
 
 using KernelFn = void (*)(LmArgs);
 
-template <int NW, int S>
+template <class M, int NW, int S>
 KernelFn pick(bool fresnel, bool all_up)
 {
     if(fresnel)
-        return all_up ? lm_fit_kernel<NW, S, true, true> : lm_fit_kernel<NW, S, true, false>;
-    return all_up ? lm_fit_kernel<NW, S, false, true> : lm_fit_kernel<NW, S, false, false>;
+        return all_up ? lm_fit_kernel<M, NW, S, true, true> : lm_fit_kernel<M, NW, S, true, false>;
+    return all_up ? lm_fit_kernel<M, NW, S, false, true> : lm_fit_kernel<M, NW, S, false, false>;
 }
 
-KernelFn kernel_for(LmKernelChoice c, bool fresnel, bool all_up)
+template <class M>
+KernelFn kernel_for_model(LmKernelChoice c, bool fresnel, bool all_up)
 {
     if(c.threads == 256 && c.slots == 2)
-        return pick<7, 2>(fresnel, all_up);
+        return pick<M, 7, 2>(fresnel, all_up);
     if(c.threads == 256 && c.slots == 3)
-        return pick<7, 3>(fresnel, all_up);
+        return pick<M, 7, 3>(fresnel, all_up);
     if(c.threads == 128 && c.slots == 2)
-        return pick<3, 2>(fresnel, all_up);
+        return pick<M, 3, 2>(fresnel, all_up);
     if(c.threads == 128 && c.slots == 3)
-        return pick<3, 3>(fresnel, all_up);
+        return pick<M, 3, 3>(fresnel, all_up);
+    if(c.threads == 256 && c.slots == 1)   // the largest slabs: one texel per CTA, no overlap
+        return pick<M, 7, 1>(fresnel, all_up);
     return nullptr;
+}
+
+KernelFn kernel_for(LmKernelChoice c, bool fresnel, bool all_up, bool rgb)
+{
+    return rgb ? kernel_for_model<RgbModel>(c, fresnel, all_up) : kernel_for_model<LumModel>(c, fresnel, all_up);
 }
 
 } // namespace
 
-LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride)
+LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
 {
     // the first candidate whose shared memory fits on an SM (fewer slots at large L)
-    LmKernelChoice cand[4];
-    const int n = lm_candidates(L, cand, 4);
+    LmKernelChoice cand[5];
+    const int n = lm_candidates(L, cand, 5);
     for(int i = 0; i < n; ++i)
-        if(lm_max_ctas_per_sm(L, lum_stride, cand[i]) > 0)
+        if(lm_max_ctas_per_sm(L, lum_stride, cand[i], rgb) > 0)
             return cand[i];
     return cand[0];
 }
 
 int lm_candidates(uint32_t, LmKernelChoice* out, int max)
 {
-    const LmKernelChoice all[4] = { { 256, 3 }, { 256, 2 }, { 128, 3 }, { 128, 2 } };
+    const LmKernelChoice all[5] = { { 256, 3 }, { 256, 2 }, { 128, 3 }, { 128, 2 }, { 256, 1 } };
     int n = 0;
-    for(int i = 0; i < 4 && n < max; ++i)
+    for(int i = 0; i < 5 && n < max; ++i)
         out[n++] = all[i];
     return n;
 }
 
-size_t lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
+size_t lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb)
 {
-    const size_t per = c.threads == 128 ? SlotSmem<3>::bytes(L, lum_stride) : SlotSmem<7>::bytes(L, lum_stride);
+    size_t per;
+    if(rgb)
+        per = c.threads == 128 ? SlotSmem<3, RgbModel>::bytes(L, lum_stride) : SlotSmem<7, RgbModel>::bytes(L, lum_stride);
+    else
+        per = c.threads == 128 ? SlotSmem<3, LumModel>::bytes(L, lum_stride) : SlotSmem<7, LumModel>::bytes(L, lum_stride);
     return per * (size_t)c.slots;
 }
 
-int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
+int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb)
 {
-    // the variants share the launch configuration
-    KernelFn k = kernel_for(c, false, false);
+    // the Fresnel and horizon variants share the launch configuration
+    KernelFn k = kernel_for(c, false, false, rgb);
     if(!k || L == 0)
         return 0;
-    const size_t smem = lm_smem_bytes(L, lum_stride, c);
+    const size_t smem = lm_smem_bytes(L, lum_stride, c, rgb);
     if(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess ||
        cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100) != cudaSuccess)
     {
@@ -1094,10 +1443,11 @@ int lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoice c)
 
 cudaError_t launch_lm_fit(const LmArgs& args, LmKernelChoice c, int grid, cudaStream_t stream)
 {
-    KernelFn k = kernel_for(c, args.cfg.fresnel != 1.0f, args.all_up != 0);
+    const bool rgb = args.rgb != 0;
+    KernelFn k = kernel_for(c, args.cfg.fresnel != 1.0f, args.all_up != 0, rgb);
     if(!k || args.L == 0)
         return cudaErrorInvalidConfiguration;
-    const size_t smem = lm_smem_bytes(args.L, args.lum_stride, c);
+    const size_t smem = lm_smem_bytes(args.L, args.lum_stride, c, rgb);
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if(e != cudaSuccess)
         return e;

@@ -77,6 +77,8 @@ SVF_HD void sincos_f(float x, float* s, float* c)
 #endif
 }
 
+SVF_HD void finish_param_set(ParamSet& ps);
+
 // ToQuaternion(euler) (include/tempest/math/quaternion.hh:82-94) and its
 // derivative, then ToMatrix3 (quaternion.hh:122-139) and R^T dR/de_k.
 SVF_HD void make_param_set(const float* p, ParamSet& ps)
@@ -135,6 +137,12 @@ SVF_HD void make_param_set(const float* p, ParamSet& ps)
         ps.om[k][2] = 0.5f * (O(1, 0) - O(0, 1));
     }
 
+    finish_param_set(ps);
+}
+
+// The lobe constants of a parameter set whose sx, sy are set.
+SVF_HD void finish_param_set(ParamSet& ps)
+{
     bool lobe = ps.sx >= 1e-6f && ps.sy >= 1e-6f;
     float rsx = lobe ? rcp_model(ps.sx) : 0.0f;
     float rsy = lobe ? rcp_model(ps.sy) : 0.0f;
@@ -147,6 +155,31 @@ SVF_HD void make_param_set(const float* p, ParamSet& ps)
     ps.rsx = lobe ? rsx : 0.0f;
     ps.rsy = lobe ? rsy : 0.0f;
     ps.kspec = lobe ? (0.25f / kRefPi) * rsx * rsy : 0.0f;
+}
+
+// RGB mode (11 parameters): p = {kd rgb, ks rgb, sx, sy, quaternion xyzw}.
+// The orientation is the quaternion; its LM parameters are a rotation phi in
+// the body frame, R(phi) = R Exp([phi]x), evaluated at phi = 0, so the body
+// angular velocity of parameter k is the unit vector e_k.  Only the geometry
+// (R, sigma and the lobe constants) goes into the table; the albedos enter per
+// channel in the pair pass.
+SVF_HD void make_param_set_rgb(const float* p, ParamSet& ps)
+{
+    ps.sx = p[6] > 0.0f ? p[6] : 0.0f;
+    ps.sy = p[7] > 0.0f ? p[7] : 0.0f;
+    ps.ks = ps.kd = 1.0f;
+    ps.ks_on = ps.kd_on = 1.0f;
+    float ql = sqrtf(p[8] * p[8] + p[9] * p[9] + p[10] * p[10] + p[11] * p[11]);
+    float rq = ql > 0.0f ? rcp_model(ql) : 0.0f;
+    float x = p[8] * rq, y = p[9] * rq, z = p[10] * rq, w = ql > 0.0f ? p[11] * rq : 1.0f;
+    float* R = ps.R;
+    R[0] = 1.0f - 2.0f * (y * y + z * z); R[1] = 2.0f * (x * y + z * w);        R[2] = 2.0f * (x * z - y * w);
+    R[3] = 2.0f * (x * y - z * w);        R[4] = 1.0f - 2.0f * (x * x + z * z); R[5] = 2.0f * (y * z + x * w);
+    R[6] = 2.0f * (x * z + y * w);        R[7] = 2.0f * (y * z - x * w);        R[8] = 1.0f - 2.0f * (x * x + y * y);
+    for(int k = 0; k < 3; ++k)
+        for(int j = 0; j < 3; ++j)
+            ps.om[k][j] = k == j ? 1.0f : 0.0f;
+    finish_param_set(ps);
 }
 
 // Per-direction table entry for one parameter set.

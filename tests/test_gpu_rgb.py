@@ -1,0 +1,134 @@
+"""The 11-parameter RGB fit (SVF_LSQ_RGB): {kd rgb, ks rgb, sx, sy} and the
+orientation fitted to the three channels.  The reference has no RGB fit (it
+fits the luminance and colours the maps with the average chromaticity), so:
+
+* the RGB model is checked channel by channel against the FP64 oracle of the
+  luminance model (the same BRDF with that channel's albedos);
+* a fit from a perturbed ground truth must reach the residual of the ground
+  truth itself (the noise floor) within 1.01x on at least 3/4 of the texels;
+* from the reference's default initial guess, its RGB residual is held to the
+  statistical bar of test_gpu_lsq.py against the reference's own RGB
+  prediction (its luminance fit times the average chromaticity).
+
+Samples are staged as FP16 for the RGB fit; the residual checks include that
+rounding on both sides."""
+import numpy as np
+import pytest
+
+import tempestrenderer_b200 as svf
+
+pytestmark = pytest.mark.gpu
+
+
+def _rgb_params(oracle, t):
+    _, q = oracle.euler_to_matrix(np.array(t.euler[:], np.float32))
+    return np.array([*t.kd[:], *t.ks[:], t.sigma[0], t.sigma[1], *q], np.float32)
+
+
+def _model_rgb(oracle, p12, euler, lp):
+    """FP32 and FP64 RGB model values [N][3] (channel c: the luminance model with kd_c, ks_c)."""
+    f32, f64 = [], []
+    for c in range(3):
+        a, b = oracle.brdf_all(np.array([p12[6], p12[7], p12[3 + c], p12[c], *euler], np.float64), lp)
+        f32.append(a)
+        f64.append(b)
+    return np.stack(f32, 1), np.stack(f64, 1)
+
+
+def _layout(golden):
+    m = golden["mesh"]
+    return svf.Layout(m["lights_parabolic"], m["triangles"], m["edges"], m["edge_angles"])
+
+
+def test_rgb_model_against_fp64(gpu_ctx, oracle_lib, golden):
+    lay = _layout(golden)
+    lp = lay.lights_parabolic
+    one = svf.options(max_iterations=0, rgb=True)
+    for x in range(3):
+        t = oracle_lib.synth_truth(31, 1, x)
+        p = _rgb_params(oracle_lib, t)
+        _, f64 = _model_rgb(oracle_lib, p, t.euler[:], lp)
+        # zero data: the RMSE is the RMS of the GPU model
+        zero = np.zeros((1, 81 * 81, 3), np.float32)
+        maps, _ = gpu_ctx.fit_texels(lay, zero, 1, 1, opts=one, init=p[None], want=("rmse", "params"))
+        np.testing.assert_allclose(maps["rmse"][0], np.sqrt(np.mean(f64 ** 2)), rtol=1e-5)
+        np.testing.assert_allclose(maps["params"][0], p, atol=1e-6)
+        # model data through the FP16 staging
+        y = f64.astype(np.float32)[None]
+        maps, _ = gpu_ctx.fit_texels(lay, y, 1, 1, opts=one, init=p[None], want=("rmse",))
+        y16 = y[0].astype(np.float16).astype(np.float64)
+        np.testing.assert_allclose(maps["rmse"][0], np.sqrt(np.mean((y16 - f64) ** 2)), rtol=1e-3, atol=1e-9)
+
+
+def test_rgb_fit_reaches_the_noise_floor(gpu_ctx, oracle_lib, golden):
+    lay = _layout(golden)
+    lp = lay.lights_parabolic
+    T = 16
+    rng = np.random.default_rng(7)
+    rgb, init, floor = [], [], []
+    for x in range(T):
+        t = oracle_lib.synth_truth(41, 1, x)
+        y = oracle_lib.synth_render(41, x, t, lp)
+        p = _rgb_params(oracle_lib, t)
+        _, f64 = _model_rgb(oracle_lib, p, t.euler[:], lp)
+        floor.append(np.sqrt(np.mean((y.astype(np.float16).astype(np.float64) - f64) ** 2)))
+        e = np.array(t.euler[:], np.float32) + 0.1 * rng.standard_normal(3).astype(np.float32)
+        _, q = oracle_lib.euler_to_matrix(e)
+        p0 = p.copy()
+        p0[:8] = np.abs(p0[:8] * (1 + 0.15 * rng.standard_normal(8))) + 1e-3
+        p0[8:] = q
+        rgb.append(y)
+        init.append(p0)
+    maps, rs = gpu_ctx.fit_texels(lay, np.stack(rgb), T, 1, opts=svf.options(rgb=True), init=np.stack(init),
+                                  want=("rmse", "params", "stats"))
+    floor = np.array(floor)
+    within = maps["rmse"] <= 1.01 * floor + 1e-7
+    assert rs.failed_texels == 0
+    # (from a perturbed orientation a texel can stop in another local minimum, as
+    # the reference's LM can: the bar is on 3/4 of the texels and the median)
+    assert within.mean() >= 0.75, np.c_[maps["rmse"], floor]
+    assert np.median(maps["rmse"] / floor) <= 1.01, np.c_[maps["rmse"], floor]
+    q = maps["params"][:, 8:]
+    np.testing.assert_allclose(np.linalg.norm(q, axis=1), 1.0, atol=1e-5)
+
+
+def test_rgb_default_init_against_reference_rgb(gpu_ctx, oracle_lib, golden):
+    from test_gpu_lsq import parity_stats
+
+    lay = _layout(golden)
+    lp = lay.lights_parabolic
+    p = golden["pipeline"]
+    seed, mix = int(p["seed"]), int(p["mix"])
+    rgb = np.stack([oracle_lib.synth_render(seed, x, oracle_lib.synth_truth(seed, mix, x), lp) for x in range(8)])
+    maps, rs = gpu_ctx.fit_texels(lay, rgb, 8, 1, opts=svf.options(rgb=True), want=("rmse", "init", "params"))
+    assert rs.failed_texels == 0
+    ref = []
+    for x in range(8):
+        fit, avg = p["fit"][x], p["avg"][x]
+        f = np.stack([oracle_lib.brdf_all(np.array([fit[0], fit[1], fit[2] * avg[c], fit[3] * avg[c], *fit[4:]],
+                                                   np.float64), lp)[0] for c in range(3)], 1)
+        ref.append(np.sqrt(np.mean((rgb[x].astype(np.float64) - f) ** 2)))
+        # the RGB initial guess is the luminance one coloured by the average chromaticity
+        np.testing.assert_allclose(maps["init"][x][:3], avg * p["init"][x][3], rtol=1e-3, atol=1e-6)
+        np.testing.assert_allclose(maps["init"][x][3:6], avg * p["init"][x][2], rtol=1e-3, atol=1e-6)
+    mean_ratio, within, worst = parity_stats(maps["rmse"], np.array(ref))
+    assert mean_ratio <= 1.01 and within >= 0.75, (np.c_[maps["rmse"], ref], mean_ratio, within)
+
+
+def test_rgb_batch_matches_single(oracle_lib, golden):
+    lay = _layout(golden)
+    lp = lay.lights_parabolic
+    lp151 = svf.directions_fibonacci(151)
+    fib = svf.Layout(lp151, *svf.triangulate(lp151))
+    a = np.stack([oracle_lib.synth_render(3, x, oracle_lib.synth_truth(3, 1, x), lp) for x in range(12)])
+    b = np.stack([oracle_lib.synth_render(4, x, oracle_lib.synth_truth(4, 1, x), lp151) for x in range(6)])
+    o = svf.options(rgb=True)
+    with svf.Context(0) as ctx:
+        maps, runs, total = ctx.fit_btfs([dict(layout=lay, samples=a, width=4, height=3),
+                                          dict(layout=fib, samples=b, width=6, height=1)], opts=o,
+                                         want=("params", "rmse"))
+        assert total.failed_texels == 0
+        for (L, s, w, h), m in zip(((lay, a, 4, 3), (fib, b, 6, 1)), maps):
+            alone, _ = ctx.fit_texels(L, s, w, h, opts=o, want=("params", "rmse"))
+            np.testing.assert_array_equal(m["params"], alone["params"])
+            np.testing.assert_array_equal(m["rmse"], alone["rmse"])
