@@ -246,6 +246,26 @@ def run_ours(args):
         t_max = float(t.item())
     value = world * T * args.steps / (t_max / 1e3)
 
+    # the 11-parameter RGB fit on the same texels (an extra line item, not the headline)
+    rgb_fit = None
+    if args.rgb_steps > 0 and world == 1:
+        ropts = svf.options(max_iterations=1024, rgb=True)
+        rmaps = {k: torch.zeros(s, dtype=torch.float32, device=dev) for k, s in
+                 {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
+                  "params": (T, 12)}.items()}
+        ctx.fit_texels(layout, samples, W, H, opts=ropts, want=want, out=rmaps, check=False)
+        rstats = [ctx.fit_texels(layout, samples, W, H, opts=ropts, want=want, out=rmaps, check=False)[1]
+                  for _ in range(args.rgb_steps)]
+        rms = float(sum(r.ms_total for r in rstats))
+        rgb_fit = {"value": T * args.rgb_steps / (rms / 1e3), "unit": "texels/s",
+                   "ms_per_step": rms / args.rgb_steps,
+                   "phases_ms": {"luminance": sum(r.ms_luminance for r in rstats) / args.rgb_steps,
+                                 "init": sum(r.ms_init for r in rstats) / args.rgb_steps,
+                                 "lm": sum(r.ms_fit for r in rstats) / args.rgb_steps},
+                   "mean_rgb_rmse": float(rmaps["rmse"].mean().item()),
+                   "model": "11-parameter RGB fit (kd rgb, ks rgb, sigma, orientation), FP16 RGB slabs, "
+                            "default initial guess"}
+
     # e2e through the C ABI with pinned host buffers
     e2e = None
     if args.e2e_steps > 0:
@@ -324,7 +344,7 @@ def run_ours(args):
                           "ndf_gemm": ms_ndf / args.steps, "lm": ms_fit / args.steps},
             "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
                         "failed_texels": failed},
-            "clocks": clk, "e2e": e2e, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
+            "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
             "wall_s": wall,
         }
         print(json.dumps(line), flush=True)
@@ -344,6 +364,7 @@ def main():
     ap.add_argument("--width", type=int, default=WIDTH)
     ap.add_argument("--height", type=int, default=HEIGHT)
     ap.add_argument("--e2e-steps", type=int, default=2)
+    ap.add_argument("--rgb-steps", type=int, default=2, help="steps of the RGB fit line item (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
