@@ -324,6 +324,7 @@ def run_ours(args):
             "config": {"workload": f"svbrdffit texel loop, {W}x{H} texels per GPU, ring-81 layout (6561 pairs), "
                                    f"RGB FP32 in HBM, mix 20% near-diffuse/10% anisotropic, default init, LM 1024 max",
                        "texels_per_gpu": T, "l2": "inputs 12.6 GB per GPU, larger than L2",
+                       "cuda_graph": ["launched directly", "recorded and launched", "replayed"][stats[-1].graph],
                        "parallelism": f"texel shards x{world}"},
             "roofline": {"bound": "fp32", "kernel": "lm_fit_kernel", "achieved": achieved, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved / fp32_peak,

@@ -252,6 +252,9 @@ typedef struct svf_run_stats
     uint32_t lm_threads;        /* LM kernel configuration the autotuner chose: CTA size */
     uint32_t lm_slots;          /* and texels in flight per CTA */
     double   ms_ndf;            /* the NDF GEMM of the default initial guess (part of ms_init) */
+    uint32_t graph;             /* svf_fit_texels: 0 launched directly, 1 recorded into a CUDA graph
+                                   and launched, 2 replayed (a repeat of the previous call) */
+    uint32_t reserved;
 } svf_run_stats;
 
 svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -59,6 +60,10 @@ svf_status fail(svf_status s, const char* fmt, ...)
     } while(0)
 
 // A grow-only device allocation.
+// Bumped whenever a device buffer is (re)allocated: a captured CUDA graph
+// holds buffer addresses and is replayed only while this has not changed.
+std::atomic<uint64_t> g_buffer_gen{ 1 };
+
 struct DevBuf
 {
     void* p = nullptr;
@@ -67,6 +72,7 @@ struct DevBuf
     {
         if(bytes <= n)
             return SVF_OK;
+        g_buffer_gen.fetch_add(1);
         if(p)
             cudaFree(p);
         p = nullptr;
@@ -175,6 +181,9 @@ struct svf_ctx
     cudaEvent_t ev[8] = {};
     cudaEvent_t copied[2] = {}, freed[2] = {};   // staging handoff (no timing)
     std::vector<cudaEvent_t> chunk_ev;           // per-chunk phase timing
+    // CUDA graph of a repeated svf_fit_texels call (see svf_fit_texels)
+    std::vector<uint64_t> graph_key, pending_key;
+    cudaGraphExec_t graph_exec = nullptr;
     std::map<uint64_t, std::unique_ptr<Layout>> layouts;
     std::unique_ptr<svf::InitHostTables> tables;
     DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, samples2,
@@ -677,6 +686,9 @@ svf_status svf_create(int device, svf_ctx** out)
         SVF_CUDA(cudaEventCreateWithFlags(&ctx->copied[i], cudaEventDisableTiming));
         SVF_CUDA(cudaEventCreateWithFlags(&ctx->freed[i], cudaEventDisableTiming));
     }
+    // the LM's work counter and the error words, for the context's lifetime
+    SVF_TRY(ctx->counter.ensure(16));
+    SVF_TRY(ctx->error.ensure(16));
     *out = ctx.release();
     return SVF_OK;
 }
@@ -702,6 +714,8 @@ void svf_destroy(svf_ctx* ctx)
     }
     for(auto e : ctx->chunk_ev)
         cudaEventDestroy(e);
+    if(ctx->graph_exec)
+        cudaGraphExecDestroy(ctx->graph_exec);
     if(ctx->copy_stream)
         cudaStreamDestroy(ctx->copy_stream);
     if(ctx->stream)
@@ -937,6 +951,11 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         ctx->chunk_ev.push_back(e);
     }
     auto ev = [&](uint64_t c, int k) { return ctx->chunk_ev[kEv * c + (uint64_t)k]; };
+    // inside a graph capture a timing event must be an external record node
+    bool capturing = false;
+    auto mark = [&](cudaEvent_t e, cudaStream_t st) {
+        return cudaEventRecordWithFlags(e, st, capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+    };
 
     // host -> device copy of chunk c into staging buffer c % 2
     auto issue_copy = [&](uint64_t c) -> svf_status {
@@ -952,6 +971,9 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         return SVF_OK;
     };
 
+    // Everything the call puts on the streams; run directly, or recorded once
+    // into a CUDA graph and replayed (below).
+    auto enqueue = [&]() -> svf_status {
     SVF_TRY(zero_error_flags(ctx));
     if(!samples_on_device)
     {
@@ -973,7 +995,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             SVF_CUDA(cudaStreamWaitEvent(ctx->stream, ctx->copied[buf], 0));
             samples = staging[buf]->p;
         }
-        SVF_CUDA(cudaEventRecord(ev(c, 2), ctx->stream));
+        SVF_CUDA(mark(ev(c, 2), ctx->stream));
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
                                        ctx->avg.as<float>(), default_init ? ctx->lum_hi.p : nullptr,
                                        default_init ? ctx->lum_lo.p : nullptr, ctx->stream,
@@ -984,7 +1006,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             if(c + 2 < n_chunks)
                 SVF_TRY(issue_copy(c + 2));
         }
-        SVF_CUDA(cudaEventRecord(ev(c, 3), ctx->stream));
+        SVF_CUDA(mark(ev(c, 3), ctx->stream));
         if(default_init)
         {
             cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.p, ctx->lum_lo.p, n, stride, init_lay->ndf_op_hi,
@@ -993,7 +1015,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                                                ctx->stream);
             if(e != cudaSuccess)
                 return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
-            SVF_CUDA(cudaEventRecord(ev(c, 7), ctx->stream));
+            SVF_CUDA(mark(ev(c, 7), ctx->stream));
             SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->ndf.as<float>(), ndf_ld, n, ctx->init.as<float>(),
                                              nullptr, maps->ndf ? ctx->ndf_tex.as<float>() : nullptr, ctx->stream));
         }
@@ -1004,14 +1026,14 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             SVF_CUDA(svf::launch_rgb_init(ctx->init.as<float>(), ctx->avg.as<float>(), n, ctx->init_rgb.as<float>(),
                                           ctx->stream));
         const float* init_used = rgb ? ctx->init_rgb.as<float>() : ctx->init.as<float>();
-        SVF_CUDA(cudaEventRecord(ev(c, 4), ctx->stream));
+        SVF_CUDA(mark(ev(c, 4), ctx->stream));
         float* mb = ctx->maps_buf.as<float>();
         LmRun r{ rgb ? (const void*)ctx->rgb16.p : (const void*)ctx->lum.p, rgb ? stride3 : stride, init_used,
                  ctx->out.as<float>(), ctx->rmse.as<float>(), ctx->stats.as<svf_texel_stats>() + c0,
                  ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n };
         r.rgb = rgb;
         SVF_TRY(run_lm(ctx, lay, &opts->lsq, r));
-        SVF_CUDA(cudaEventRecord(ev(c, 5), ctx->stream));
+        SVF_CUDA(mark(ev(c, 5), ctx->stream));
         // outputs (into host or device buffers of the caller)
         auto put = [&](void* dst, const void* src, size_t bytes) -> svf_status {
             if(dst)
@@ -1027,7 +1049,109 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_TRY(put(maps->init ? maps->init + kout * c0 : nullptr, init_used, sizeof(float) * kout * n));
         SVF_TRY(put(maps->ndf ? maps->ndf + (uint64_t)svf::kNdfTexels * c0 : nullptr, ctx->ndf_tex.p,
                     sizeof(float) * svf::kNdfTexels * n));
-        SVF_CUDA(cudaEventRecord(ev(c, 6), ctx->stream));
+        SVF_CUDA(mark(ev(c, 6), ctx->stream));
+    }
+    return SVF_OK;
+    };
+
+    // CUDA graph.  A call that repeats the previous call exactly (the same
+    // device-resident samples, sizes, options, initial parameters and output
+    // buffers, all on the device or in pinned host memory; one chunk; no
+    // device buffer reallocated since) is recorded into a graph on its second
+    // occurrence and replayed from then on: its launches, copies and events
+    // go to the GPU as one graph launch.
+    uint32_t graph_mode = 0;   // svf_run_stats::graph
+    auto reachable = [&](const void* p) {
+        if(!p)
+            return true;
+        cudaPointerAttributes at;
+        if(cudaPointerGetAttributes(&at, p) != cudaSuccess)
+        {
+            cudaGetLastError();
+            return false;
+        }
+        return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged || at.type == cudaMemoryTypeHost;
+    };
+    bool eligible = samples_on_device && n_chunks == 1 && reachable(opts->init_params) &&
+                    reachable(maps->diffuse) && reachable(maps->specular) && reachable(maps->sigma) &&
+                    reachable(maps->basis) && reachable(maps->rmse) && reachable(maps->params) &&
+                    reachable(maps->init) && reachable(maps->ndf);
+    if(eligible && !rgb && !lay->tuned && T >= 4096)
+        SVF_TRY(tune_lm(ctx, lay, &opts->lsq));   // the autotuner synchronises: never inside a capture
+    std::vector<uint64_t> key;
+    if(eligible)
+    {
+        auto u = [&](const void* p) { key.push_back((uint64_t)(uintptr_t)p); };
+        u(btf->samples);
+        u(lay);
+        u(init_lay);
+        u(opts->init_params);
+        u(maps->diffuse);
+        u(maps->specular);
+        u(maps->sigma);
+        u(maps->basis);
+        u(maps->rmse);
+        u(maps->params);
+        u(maps->init);
+        u(maps->ndf);
+        key.insert(key.end(), { (uint64_t)btf->sample_type, T, (uint64_t)opts->init_mode,
+                                (uint64_t)opts->lsq.max_iterations, (uint64_t)opts->lsq.flags,
+                                (uint64_t)opts->lsq.restarts, g_buffer_gen.load(),
+                                (uint64_t)(lay->tuned ? lay->choice.threads * 16 + lay->choice.slots : 0) });
+        uint64_t bits[3];
+        std::memcpy(&bits[0], &opts->lsq.mse_target, 8);
+        std::memcpy(&bits[1], &opts->lsq.break_on_small_step, 8);
+        const double fr = opts->lsq.fresnel;
+        std::memcpy(&bits[2], &fr, 8);
+        key.insert(key.end(), bits, bits + 3);
+    }
+    if(eligible && ctx->graph_exec && key == ctx->graph_key)
+    {
+        SVF_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+        graph_mode = 2;
+    }
+    else if(eligible && key == ctx->pending_key)
+    {
+        if(ctx->graph_exec)
+        {
+            cudaGraphExecDestroy(ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+            ctx->graph_key.clear();
+        }
+        cudaGraph_t graph = nullptr;
+        bool captured = false;
+        if(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess)
+        {
+            capturing = true;
+            const svf_status st_enq = enqueue();
+            capturing = false;
+            const cudaError_t e_end = cudaStreamEndCapture(ctx->stream, &graph);
+            if(st_enq == SVF_OK && e_end == cudaSuccess && graph &&
+               cudaGraphInstantiate(&ctx->graph_exec, graph, 0) == cudaSuccess)
+                captured = true;
+            if(graph)
+                cudaGraphDestroy(graph);
+        }
+        cudaGetLastError();
+        if(captured)
+        {
+            ctx->graph_key = key;
+            SVF_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+            graph_mode = 1;
+        }
+        else
+        {
+            // not capturable here: run the call directly
+            ctx->graph_exec = nullptr;
+            ctx->pending_key.clear();
+            SVF_TRY(enqueue());
+        }
+    }
+    else
+    {
+        if(eligible)
+            ctx->pending_key = key;
+        SVF_TRY(enqueue());
     }
     std::vector<svf_texel_stats> st(T);
     SVF_CUDA(cudaMemcpyAsync(st.data(), ctx->stats.p, sizeof(svf_texel_stats) * T, cudaMemcpyDeviceToHost,
@@ -1065,6 +1189,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     rs.ms_total = span(samples_on_device ? ev(0, 2) : ev(0, 0), ev(n_chunks - 1, 6));
     cudaGetLastError();
     rs.texels = T;
+    rs.graph = graph_mode;
     const svf::LmKernelChoice used = lm_choice(lay, rgb ? stride3 : stride, rgb);
     rs.lm_threads = (uint32_t)used.threads;
     rs.lm_slots = (uint32_t)used.slots;

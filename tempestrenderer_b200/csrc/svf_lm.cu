@@ -356,7 +356,7 @@ __device__ int lm_next(LmState<M::P>& st, const LmConfig& cfg, double n_pairs)
 #pragma unroll
         for(int i = 0; i < M::P; ++i)
             st.pt[i] = st.p[i] - st.d[i];
-        if(M::kRgb)
+        if constexpr(M::kRgb)
         {
             // the orientation moves by the local rotation phi = -d
             double dq[4];
@@ -384,7 +384,7 @@ __device__ int lm_after_trial(LmState<M::P>& st, const LmConfig& cfg, double S1,
 #pragma unroll
         for(int i = 0; i < M::P; ++i)
             st.p[i] = st.pt[i];
-        if(M::kRgb)
+        if constexpr(M::kRgb)
         {
             const double n = sqrt(st.qt[0] * st.qt[0] + st.qt[1] * st.qt[1] + st.qt[2] * st.qt[2] +
                                   st.qt[3] * st.qt[3]);
@@ -458,7 +458,7 @@ __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32
                                             uint32_t lane)
 {
     ParamSet ps;
-    if(M::kRgb)
+    if constexpr(M::kRgb)
         make_param_set_rgb(pf, ps);
     else
         make_param_set(pf, ps);
@@ -489,7 +489,7 @@ __device__ __forceinline__ void build_table(float* tab, const float* geo, uint32
 #pragma unroll
             for(int j = 0; j < 3; ++j)
                 pc->om[3 * k + j] = ps.om[k][j];
-        if(M::kRgb)
+        if constexpr(M::kRgb)
             for(int k = 0; k < 3; ++k)
             {
                 pc->kdc[k] = pf[k] > 0.0f ? pf[k] : 0.0f;
@@ -770,7 +770,7 @@ __device__ __forceinline__ void pair_step(const float* tab, const PassConst& c, 
     const Entry eb = load_entry(tab, Lp, ib);
     // pair 1: view a, light b (slab row a); pair 2: view b, light a
     const bool two = valid && d != 0u;
-    if(M::kRgb)
+    if constexpr(M::kRgb)
     {
         float y1[3], y2[3];
         const __half* s1 = reinterpret_cast<const __half*>(slab) + 3 * (ia * L + ib);
@@ -926,7 +926,7 @@ __device__ __forceinline__ uint32_t bar_done(int s) { return 1u + (uint32_t)S + 
 template <class M>
 __device__ void write_texel(const LmArgs& args, LmState<M::P>& st, uint32_t t, double n_pairs)
 {
-    if(M::kRgb)
+    if constexpr(M::kRgb)
     {
         // {kd rgb, ks rgb, sx, sy, quaternion xyzw}; maps: the fitted albedos,
         // sigma and the orientation
@@ -966,8 +966,9 @@ __device__ void write_texel(const LmArgs& args, LmState<M::P>& st, uint32_t t, d
         if(args.map_basis)
             for(int i = 0; i < 4; ++i)
                 args.map_basis[4 * (uint64_t)t + i] = pout[8 + i];
-        return;
     }
+    else
+    {
     float pout[7];
 #pragma unroll
     for(int i = 0; i < 7; ++i)
@@ -1019,6 +1020,7 @@ __device__ void write_texel(const LmArgs& args, LmState<M::P>& st, uint32_t t, d
                 args.map_specular[3 * (uint64_t)t + k] = a[k] * pout[2];
         }
     }
+}
 }
 
 // Control thread: takes the next texel for slot `sl` and starts its slab copy
@@ -1074,7 +1076,7 @@ __device__ __forceinline__ bool slot_start(const LmArgs& args, Slot<M>& sl)
 #pragma unroll
     for(int i = 0; i < M::kOut; ++i)
         sl.pf[i] = in[i];
-    if(M::kRgb)
+    if constexpr(M::kRgb)
     {
         for(int i = 0; i < M::B; ++i)
             st.p[i] = (double)in[i];
@@ -1132,12 +1134,13 @@ template <class M>
 __device__ void expand_sums(const double* sums, const float* pf, double* hg)
 {
     constexpr int P = M::P, kH = P * (P + 1) / 2;
-    if(!M::kRgb)
+    if constexpr(!M::kRgb)
     {
         for(int i = 0; i < kH + P; ++i)
             hg[i] = sums[i];
-        return;
     }
+    else
+    {
     for(int i = 0; i < kH + P; ++i)
         hg[i] = 0.0;
     double ks[3], kdon[3], kson[3], ks2 = 0.0;
@@ -1167,6 +1170,7 @@ __device__ void expand_sums(const double* sums, const float* pf, double* hg)
             hg[hix<P>(6 + i, 6 + j)] = ks2 * sums[13 + hix<5>(i, j)];
         hg[kH + 6 + i] = sums[34 + i];
     }
+}
 }
 
 // Resident CTAs per SM the register budget is sized for.
@@ -1301,7 +1305,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                     next = lm_next<M>(st, args.cfg, sl.npairs);
                 if(next == kCmdTrial)
                 {
-                    if(M::kRgb)
+                    if constexpr(M::kRgb)
                     {
                         for(int i = 0; i < M::B; ++i)
                             sl.pf[i] = (float)st.pt[i];
