@@ -263,8 +263,10 @@ def run_ours(args):
                                  "init": sum(r.ms_init for r in rstats) / args.rgb_steps,
                                  "lm": sum(r.ms_fit for r in rstats) / args.rgb_steps},
                    "mean_rgb_rmse": float(rmaps["rmse"].mean().item()),
+                   "median_rgb_rmse": float(rmaps["rmse"].median().item()),
                    "model": "11-parameter RGB fit (kd rgb, ks rgb, sigma, orientation), FP16 RGB slabs, "
-                            "default initial guess"}
+                            "started from the luminance fit (default initial guess) coloured by the average "
+                            "chromaticity; init phase = NDF guess + luminance LM"}
 
     # e2e through the C ABI with pinned host buffers
     e2e = None
@@ -344,7 +346,8 @@ def run_ours(args):
             "phases_ms": {"luminance": ms_lum / args.steps, "init": ms_init / args.steps,
                           "ndf_gemm": ms_ndf / args.steps, "lm": ms_fit / args.steps},
             "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
-                        "failed_texels": failed},
+                        "failed_texels": failed, "mean_rmse": float(maps["rmse"].mean().item()),
+                        "median_rmse": float(maps["rmse"].median().item())},
             "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
             "wall_s": wall,
         }

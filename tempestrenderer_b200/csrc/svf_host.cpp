@@ -1023,8 +1023,16 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             SVF_TRY(to_device(ctx, rgb ? ctx->init_rgb.p : ctx->init.p, opts->init_params + kout * c0,
                               sizeof(float) * kout * n));
         if(rgb && default_init)
-            SVF_CUDA(svf::launch_rgb_init(ctx->init.as<float>(), ctx->avg.as<float>(), n, ctx->init_rgb.as<float>(),
+        {
+            // the RGB fit starts where the luminance fit from the default guess
+            // ends, coloured by the average chromaticity (svbrdffit's own maps):
+            // its accepted steps only lower that RGB residual
+            LmRun lr{ ctx->lum.p, stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
+                      ctx->stats.as<svf_texel_stats>() + c0, nullptr, nullptr, nullptr, nullptr, nullptr, n };
+            SVF_TRY(run_lm(ctx, lay, &opts->lsq, lr));
+            SVF_CUDA(svf::launch_rgb_init(ctx->out.as<float>(), ctx->avg.as<float>(), n, ctx->init_rgb.as<float>(),
                                           ctx->stream));
+        }
         const float* init_used = rgb ? ctx->init_rgb.as<float>() : ctx->init.as<float>();
         SVF_CUDA(mark(ev(c, 4), ctx->stream));
         float* mb = ctx->maps_buf.as<float>();
@@ -1076,7 +1084,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                     reachable(maps->diffuse) && reachable(maps->specular) && reachable(maps->sigma) &&
                     reachable(maps->basis) && reachable(maps->rmse) && reachable(maps->params) &&
                     reachable(maps->init) && reachable(maps->ndf);
-    if(eligible && !rgb && !lay->tuned && T >= 4096)
+    if(eligible && (!rgb || default_init) && !lay->tuned && T >= 4096)
         SVF_TRY(tune_lm(ctx, lay, &opts->lsq));   // the autotuner synchronises: never inside a capture
     std::vector<uint64_t> key;
     if(eligible)
@@ -1403,9 +1411,42 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             else
                 SVF_TRY(to_device(ctx, init_used + kout * p.k0, opts[p.b].init_params + kout * p.first,
                                   sizeof(float) * kout * p.count));
-            if(rgb && x.default_init)
-                SVF_CUDA(svf::launch_rgb_init(ctx->init.as<float>() + 7 * p.k0, ctx->avg.as<float>() + 3 * p.k0,
-                                              p.count, init_used + 12 * p.k0, ctx->stream));
+
+        }
+        // the RGB fit of default-initialised pieces starts from their luminance
+        // fit coloured by the average chromaticity (as in svf_fit_texels)
+        bool rgb_from_lum = false;
+        for(auto& p : ch)
+            rgb_from_lum = rgb_from_lum || (rgb && it[p.b].default_init);
+        if(rgb_from_lum)
+        {
+            // pieces with given RGB parameters ride along from a zero start
+            for(auto& p : ch)
+                if(!it[p.b].default_init)
+                    SVF_CUDA(cudaMemsetAsync(ctx->init.as<float>() + 7 * p.k0, 0, sizeof(float) * 7 * p.count,
+                                             ctx->stream));
+            svf::LmSegment ls[svf::kLmMaxSegments];
+            Layout* lbig = it[ch[0].b].lay;
+            bool lup = true;
+            uint64_t lstride = 0;
+            for(size_t i = 0; i < ch.size(); ++i)
+            {
+                const Item& x = it[ch[i].b];
+                ls[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride, ctx->lum.as<float>() + ch[i].off,
+                                        x.lay->geo.as<float>() };
+                lup = lup && x.lay->all_up;
+                lstride = std::max(lstride, x.stride);
+                if(x.lay->L > lbig->L)
+                    lbig = x.lay;
+            }
+            LmRun lr{ nullptr, lstride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
+                      ctx->stats.as<svf_texel_stats>(), nullptr, nullptr, nullptr, nullptr, nullptr, n,
+                      ls, (uint32_t)ch.size(), lup, false };
+            SVF_TRY(run_lm(ctx, lbig, &opts[0].lsq, lr));
+            for(auto& p : ch)
+                if(it[p.b].default_init)
+                    SVF_CUDA(svf::launch_rgb_init(ctx->out.as<float>() + 7 * p.k0, ctx->avg.as<float>() + 3 * p.k0,
+                                                  p.count, init_used + 12 * p.k0, ctx->stream));
         }
         SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
         // one LM launch over the pieces, whatever their layouts

@@ -1395,13 +1395,23 @@ KernelFn kernel_for(LmKernelChoice c, bool fresnel, bool all_up, bool rgb)
 
 LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
 {
-    // the first candidate whose shared memory fits on an SM (fewer slots at large L)
+    // Untuned: the candidate with the most worker warps resident per SM (ties:
+    // the earlier one), counting a single-slot CTA's at half (its workers wait
+    // for the control warp between passes); at large L only fewer slots fit.
     LmKernelChoice cand[5];
     const int n = lm_candidates(L, cand, 5);
+    int best = -1, best_w = 0;
     for(int i = 0; i < n; ++i)
-        if(lm_max_ctas_per_sm(L, lum_stride, cand[i], rgb) > 0)
-            return cand[i];
-    return cand[0];
+    {
+        const int ctas = lm_max_ctas_per_sm(L, lum_stride, cand[i], rgb);
+        const int w = ctas * (cand[i].threads / 32 - 1) * (cand[i].slots >= 2 ? 2 : 1);
+        if(w > best_w)
+        {
+            best_w = w;
+            best = i;
+        }
+    }
+    return best >= 0 ? cand[best] : cand[0];
 }
 
 int lm_candidates(uint32_t, LmKernelChoice* out, int max)
