@@ -202,6 +202,7 @@ svf_status svf_lsq_fit_batch_noalloc(const float* lights_parabolic, uint32_t lig
 
 #define SVF_INIT_DEFAULT 0u   /* the reference's default initial guess (NDF -> PCA -> SGGX projection) */
 #define SVF_INIT_GIVEN   1u   /* caller-supplied initial parameters (svbrdffit -r refit) */
+#define SVF_INIT_MLP     2u   /* the learned initial guess of svf_fit_options::mlp (see svf_mlp_train) */
 
 typedef struct svf_btf_view
 {
@@ -211,11 +212,20 @@ typedef struct svf_btf_view
     const svf_layout_desc* layout;
 } svf_btf_view;
 
+typedef struct svf_mlp svf_mlp;
+
 typedef struct svf_fit_options
 {
     svf_lsq_options lsq;
     uint32_t        init_mode;     /* SVF_INIT_* */
     const float*    init_params;   /* [texels][7] for SVF_INIT_GIVEN */
+    const svf_mlp*  mlp;           /* SVF_INIT_MLP: a model trained for the BTF's direction layout */
+    float           initial_damping;  /* LM's first damping as a multiple of the reference's rule
+                                         (0.75 max(1, max diag J^T J), fitting.hh:531-538).  0: that
+                                         rule, except 1e-3 of it from the learned guess, which starts
+                                         near a minimum where the full damping takes steps below
+                                         BreakOnSmallStep and ends the fit early.  No reference
+                                         counterpart. */
 } svf_fit_options;
 
 /* The five output maps of svbrdffit (svbrdf-fitting.cc:713-735, values as
@@ -272,6 +282,46 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
 svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, const svf_fit_options* options,
                         const svf_maps* maps, svf_run_stats* runs /* [n_btf] or NULL */,
                         svf_run_stats* total /* may be NULL */);
+
+/* Learned initial guess -------------------------------------------------------------
+ * No counterpart in the reference, whose only initial guess is the NDF -> PCA ->
+ * SGGX projection pipeline (svbrdf-fitting-pipeline.cc:350-660).  A small MLP
+ * (96 -> 256 -> 256 -> 10, GELU) maps the log RGB samples of 32 fixed direction
+ * pairs of a texel to the luminance fit's parameters; it is trained on seeded
+ * synthetic texels that the plain LM, started from the reference's default
+ * guess, has fitted.  SVF_INIT_MLP then starts LM from its prediction: the fit
+ * skips the NDF pipeline, and its result is judged against the plain LM's
+ * residual.  Inference uses BF16 weights with FP32 accumulation. */
+typedef struct svf_mlp_train_options
+{
+    uint32_t texels;          /* synthetic training texels (default 1 << 20) */
+    uint32_t seed, mix;       /* svf_synth_btf seed and parameter mix of the training texels */
+    uint32_t epochs;          /* passes over the texels (default 24) */
+    uint32_t batch;           /* texels per Adam step (default 4096) */
+    float    lr;              /* Adam step size (default 1e-3, cosine-decayed to 5% of it) */
+    uint32_t max_iterations;  /* of the LM that makes the targets (default 1024) */
+} svf_mlp_train_options;
+
+void       svf_mlp_train_options_default(svf_mlp_train_options* o);
+/* Trains a model for the direction layout lights_parabolic [L][2]; *final_loss
+ * (optional) is the MSE of the last epoch on the normalised targets. */
+svf_status svf_mlp_train(svf_ctx* ctx, const float* lights_parabolic, uint32_t L, const svf_mlp_train_options* o,
+                         svf_mlp** out, float* final_loss);
+/* The model's initial guess for texels of RGB samples [texels][L*L][3] (host or
+ * device): params [texels][7]; features [texels][96] (optional) receives the
+ * normalised network inputs. */
+svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples, uint32_t sample_type,
+                           uint32_t texels, float* params, float* features);
+/* One optimiser step on given normalised features [rows][96] and targets
+ * [rows][10] (sgd != 0: plain gradient step of size lr; else Adam); *loss is
+ * the MSE before the step.  For checking the training kernels. */
+svf_status svf_mlp_step(svf_ctx* ctx, svf_mlp* mlp, const float* features, const float* targets, uint32_t rows,
+                        float lr, uint32_t sgd, float* loss);
+/* Serialisation: *size is set to the bytes needed; with buf != NULL and
+ * *size large enough the model is written. */
+svf_status svf_mlp_save(const svf_mlp* mlp, void* buf, size_t* size);
+svf_status svf_mlp_load(svf_ctx* ctx, const void* buf, size_t size, svf_mlp** out);
+void       svf_mlp_destroy(svf_mlp* mlp);
 
 /* Synthetic BTFs (test and benchmark inputs) ------------------------------------ */
 /* Renders texels [first, first + count) of a seeded synthetic BTF straight into

@@ -28,13 +28,14 @@ SVF_TEXEL_NONFINITE, SVF_TEXEL_MAX_ITER, SVF_TEXEL_TIMEOUT = 1, 2, 4
 SVF_LSQ_DIFFUSE = 1 << 1
 SVF_LSQ_RGB = 1 << 8
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
-SVF_INIT_DEFAULT, SVF_INIT_GIVEN = 0, 1
+SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
 
 # every entry point include/svf.h declares
 EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_options_default", "svf_create",
            "svf_destroy", "svf_directions_ring81", "svf_directions_fibonacci", "svf_layout_triangulate",
            "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc", "svf_fit_texels", "svf_fit_btfs",
-           "svf_synth_btf")
+           "svf_synth_btf", "svf_mlp_train_options_default", "svf_mlp_train", "svf_mlp_predict", "svf_mlp_step",
+           "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy")
 
 
 class SvfError(RuntimeError):
@@ -69,7 +70,13 @@ class BtfView(C.Structure):
 
 
 class FitOptions(C.Structure):
-    _fields_ = [("lsq", LsqOptions), ("init_mode", C.c_uint32), ("init_params", C.c_void_p)]
+    _fields_ = [("lsq", LsqOptions), ("init_mode", C.c_uint32), ("init_params", C.c_void_p), ("mlp", C.c_void_p),
+                ("initial_damping", C.c_float)]
+
+
+class MlpTrainOptions(C.Structure):
+    _fields_ = [("texels", C.c_uint32), ("seed", C.c_uint32), ("mix", C.c_uint32), ("epochs", C.c_uint32),
+                ("batch", C.c_uint32), ("lr", C.c_float), ("max_iterations", C.c_uint32)]
 
 
 class Maps(C.Structure):
@@ -118,8 +125,18 @@ def load() -> C.CDLL:
         L.svf_synth_btf.argtypes = [vp, u32, u32, vp, u32, u64, u64, u32, f32, vp, vp]
         L.svf_fit_btfs.argtypes = [vp, C.POINTER(BtfView), u32, C.POINTER(FitOptions), C.POINTER(Maps),
                                    C.POINTER(RunStats), C.POINTER(RunStats)]
+        L.svf_mlp_train_options_default.argtypes = [C.POINTER(MlpTrainOptions)]
+        L.svf_mlp_train_options_default.restype = None
+        L.svf_mlp_train.argtypes = [vp, vp, u32, C.POINTER(MlpTrainOptions), C.POINTER(vp), C.POINTER(f32)]
+        L.svf_mlp_predict.argtypes = [vp, vp, vp, u32, u32, vp, vp]
+        L.svf_mlp_step.argtypes = [vp, vp, vp, vp, u32, f32, u32, C.POINTER(f32)]
+        L.svf_mlp_save.argtypes = [vp, vp, C.POINTER(C.c_size_t)]
+        L.svf_mlp_load.argtypes = [vp, vp, C.c_size_t, C.POINTER(vp)]
+        L.svf_mlp_destroy.argtypes = [vp]
+        L.svf_mlp_destroy.restype = None
         for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
-                     "svf_fit_texels", "svf_fit_btfs", "svf_synth_btf"):
+                     "svf_fit_texels", "svf_fit_btfs", "svf_synth_btf", "svf_mlp_train", "svf_mlp_predict",
+                     "svf_mlp_step", "svf_mlp_save", "svf_mlp_load"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -262,8 +279,10 @@ class Context:
     def fit_texels(self, layout: Layout, samples, width: int, height: int, sample_type=SVF_SAMPLES_F32,
                    opts: LsqOptions | None = None, init=None, want=("diffuse", "specular", "sigma", "basis", "rmse",
                                                                     "params", "init", "stats"), out=None,
-                   check=True):
-        """samples: [T][L*L][3] (numpy or torch, host or device).  Returns (maps dict, RunStats)."""
+                   check=True, mlp: "Mlp | None" = None, damping: float = 0.0):
+        """samples: [T][L*L][3] (numpy or torch, host or device).  init: given initial parameters; mlp: a
+        learned initial guess (SVF_INIT_MLP); neither: the default guess.  damping: LM's initial damping as a
+        multiple of the reference's rule (0: automatic).  Returns (maps dict, RunStats)."""
         T = width * height
         v = BtfView()
         v.samples = _ptr(samples)
@@ -274,6 +293,9 @@ class Context:
         fo.lsq = opts or options()
         fo.init_mode = SVF_INIT_DEFAULT if init is None else SVF_INIT_GIVEN
         fo.init_params = _ptr(init) if init is not None else None
+        if mlp is not None:
+            fo.init_mode, fo.mlp = SVF_INIT_MLP, mlp.handle
+        fo.initial_damping = damping
         kout = 12 if fo.lsq.flags & SVF_LSQ_RGB else 7
         shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
                   "params": (T, kout), "init": (T, kout), "ndf": (T, 64 * 64)}
@@ -293,7 +315,7 @@ class Context:
 
     def fit_btfs(self, btfs, opts: LsqOptions | None = None, want=("diffuse", "specular", "sigma", "basis", "rmse",
                                                                   "params", "init", "stats"), check=True):
-        """btfs: list of dicts {layout, samples, width, height[, sample_type][, init]}.  All texels go through
+        """btfs: list of dicts {layout, samples, width, height[, sample_type][, init][, mlp]}.  All texels go through
         shared LM launches (svf_fit_btfs).  Returns ([maps dict per BTF], [RunStats per BTF], RunStats total)."""
         n = len(btfs)
         views = (BtfView * n)()
@@ -309,6 +331,9 @@ class Context:
             fos[i].lsq = opts or options()
             init = b.get("init")
             fos[i].init_mode = SVF_INIT_DEFAULT if init is None else SVF_INIT_GIVEN
+            if b.get("mlp") is not None:
+                fos[i].init_mode, fos[i].mlp = SVF_INIT_MLP, b["mlp"].handle
+            fos[i].initial_damping = b.get("damping", 0.0)
             if init is not None:
                 init = np.ascontiguousarray(init, np.float32)
                 keep.append(init)
@@ -332,3 +357,66 @@ class Context:
         lp = np.ascontiguousarray(lights_parabolic, np.float32)
         _check(self._lib.svf_synth_btf(self.handle, seed, mix, lp.ctypes.data, lp.shape[0], first, count,
                                        sample_type, noise, _ptr(samples), _ptr(truth)))
+
+
+def mlp_train_options(**kw) -> MlpTrainOptions:
+    o = MlpTrainOptions()
+    load().svf_mlp_train_options_default(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class Mlp:
+    """A learned initial guess (svf_mlp_*).  Create with Mlp.train or Mlp.load."""
+
+    def __init__(self, ctx: Context, handle):
+        self._lib, self.ctx, self.handle = load(), ctx, handle
+
+    @classmethod
+    def train(cls, ctx: Context, lights_parabolic, opts: MlpTrainOptions | None = None):
+        """Returns (model, final epoch's loss on the normalised targets)."""
+        lp = np.ascontiguousarray(lights_parabolic, np.float32)
+        h, loss = C.c_void_p(), C.c_float()
+        _check(load().svf_mlp_train(ctx.handle, lp.ctypes.data, lp.shape[0], C.byref(opts or mlp_train_options()),
+                                    C.byref(h), C.byref(loss)))
+        return cls(ctx, h), float(loss.value)
+
+    @classmethod
+    def load(cls, ctx: Context, blob: bytes):
+        h = C.c_void_p()
+        buf = C.create_string_buffer(bytes(blob), len(blob))
+        _check(load().svf_mlp_load(ctx.handle, buf, len(blob), C.byref(h)))
+        return cls(ctx, h)
+
+    def save(self) -> bytes:
+        n = C.c_size_t(0)
+        _check(self._lib.svf_mlp_save(self.handle, None, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        _check(self._lib.svf_mlp_save(self.handle, buf, C.byref(n)))
+        return buf.raw[:n.value]
+
+    def predict(self, samples, texels: int, sample_type=SVF_SAMPLES_F32, features=False):
+        """Initial parameters [texels][7] (and the normalised inputs [texels][96] with features=True)."""
+        p = np.zeros((texels, 7), np.float32)
+        f = np.zeros((texels, 96), np.float32) if features else None
+        _check(self._lib.svf_mlp_predict(self.ctx.handle, self.handle, _ptr(samples), sample_type, texels,
+                                         p.ctypes.data, f.ctypes.data if features else None))
+        return (p, f) if features else p
+
+    def step(self, features, targets, lr: float, sgd: bool = False) -> float:
+        """One optimiser step; returns the MSE before it."""
+        x = np.ascontiguousarray(features, np.float32)
+        y = np.ascontiguousarray(targets, np.float32)
+        loss = C.c_float()
+        _check(self._lib.svf_mlp_step(self.ctx.handle, self.handle, x.ctypes.data, y.ctypes.data, x.shape[0], lr,
+                                      int(sgd), C.byref(loss)))
+        return float(loss.value)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.svf_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()

@@ -88,6 +88,16 @@ struct DevBuf
     }
     template <typename T>
     T* as() const { return static_cast<T*>(p); }
+    void reset()
+    {
+        if(p)
+            cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
     ~DevBuf()
     {
         if(p)
@@ -187,12 +197,214 @@ struct svf_ctx
     std::map<uint64_t, std::unique_ptr<Layout>> layouts;
     std::unique_ptr<svf::InitHostTables> tables;
     DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, samples2,
-        maps_buf, scratch, rgb16, init_rgb;
+        maps_buf, scratch, rgb16, init_rgb, mlp_x, mlp_h1, mlp_h2, mlp_y;
     PinnedBuf pinned;
+};
+
+// A learned initial-guess model (svf_mlp_*): FP32 master weights (Adam state
+// alongside), BF16 copies for inference, the normalisation of inputs and
+// targets, the 32 direction pairs and the layout it was trained for.
+struct svf_mlp
+{
+    int device = 0;
+    uint32_t L = 0;
+    std::vector<float> lp;               // [L][2]
+    uint32_t pairs[svf::kMlpPairs] = {};
+    // half-vector bins of the direction pairs (derived from lp): the pairs of bin
+    // b are order[start[b] .. start[b + 1]), their mean is the sum times bin_w[b]
+    std::vector<uint32_t> order, start;
+    std::vector<float> bin_w;
+    float xmean[svf::kMlpInputs] = {}, xrstd[svf::kMlpInputs] = {};
+    float ymean[svf::kMlpOutputs] = {}, ystd[svf::kMlpOutputs] = {};
+    DevBuf w, wbf, m, v, g, d_pairs, d_xmean, d_xrstd, d_ymean, d_ystd, d_order, d_start, d_binw;
+    int step = 0;
 };
 
 namespace
 {
+
+// The half-vector bins of a model's direction layout: h = normalize(w_i + w_o)
+// of every pair, in parabolic coordinates, on an 8 x 8 grid over the square
+// that holds them all.
+void mlp_bins(svf_mlp* mlp)
+{
+    using namespace svf;
+    const uint32_t L = mlp->L, N = L * L;
+    std::vector<float> w(3 * (size_t)L), hx(N), hy(N);
+    for(uint32_t d = 0; d < L; ++d)
+        parabolic_to_cartesian_ref(mlp->lp[2 * d], mlp->lp[2 * d + 1], &w[3 * d]);
+    float r = 1e-6f;
+    for(uint32_t i = 0; i < L; ++i)
+        for(uint32_t o = 0; o < L; ++o)
+        {
+            float h[3] = { w[3 * i] + w[3 * o], w[3 * i + 1] + w[3 * o + 1], w[3 * i + 2] + w[3 * o + 2] };
+            const float n = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+            const uint32_t k = i * L + o;
+            if(!(n > 1e-6f))
+            {
+                hx[k] = hy[k] = 1e30f;   // opposite directions: no half vector
+                continue;
+            }
+            for(float& c : h)
+                c /= n;
+            const float z = 1.0f + std::max(h[2], -0.999f);
+            hx[k] = h[0] / z;
+            hy[k] = h[1] / z;
+            if(hx[k] < 1e29f)
+                r = std::max(r, std::max(std::fabs(hx[k]), std::fabs(hy[k])));
+        }
+    const int G = 8;   // kMlpBins = G * G
+    std::vector<uint32_t> bin(N, (uint32_t)kMlpBins);
+    std::vector<uint32_t> count(kMlpBins + 1, 0);
+    for(uint32_t k = 0; k < N; ++k)
+    {
+        if(hx[k] > 1e29f)
+            continue;
+        const int bx = std::min(G - 1, (int)((hx[k] + r) / (2.0f * r) * G));
+        const int by = std::min(G - 1, (int)((hy[k] + r) / (2.0f * r) * G));
+        bin[k] = (uint32_t)(by * G + bx);   // hx, hy >= -r: bx, by >= 0
+        ++count[bin[k]];
+    }
+    mlp->start.assign(kMlpBins + 1, 0);
+    for(int b = 0; b < kMlpBins; ++b)
+        mlp->start[b + 1] = mlp->start[b] + count[b];
+    mlp->order.assign(mlp->start[kMlpBins], 0);
+    std::vector<uint32_t> fill(mlp->start.begin(), mlp->start.end() - 1);
+    for(uint32_t k = 0; k < N; ++k)
+        if(bin[k] < (uint32_t)kMlpBins)
+            mlp->order[fill[bin[k]]++] = k;
+    mlp->bin_w.assign(kMlpBins, 0.0f);
+    for(int b = 0; b < kMlpBins; ++b)
+        mlp->bin_w[b] = count[b] ? 1.0f / (float)count[b] : 0.0f;
+}
+
+// Uploads the host-side tables of a model and zeroes its optimiser state.
+svf_status mlp_upload(svf_ctx* ctx, svf_mlp* mlp, const std::vector<float>& w)
+{
+    using namespace svf;
+    mlp_bins(mlp);
+    SVF_TRY(mlp->d_order.ensure(sizeof(uint32_t) * std::max<size_t>(1, mlp->order.size())));
+    SVF_TRY(mlp->d_start.ensure(sizeof(uint32_t) * mlp->start.size()));
+    SVF_TRY(mlp->d_binw.ensure(sizeof(float) * mlp->bin_w.size()));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_order.p, mlp->order.data(), sizeof(uint32_t) * mlp->order.size(),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_start.p, mlp->start.data(), sizeof(uint32_t) * mlp->start.size(),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_binw.p, mlp->bin_w.data(), sizeof(float) * mlp->bin_w.size(),
+                             cudaMemcpyHostToDevice, ctx->stream));
+    SVF_TRY(mlp->w.ensure(sizeof(float) * kMlpParams));
+    SVF_TRY(mlp->g.ensure(sizeof(float) * kMlpParams));
+    SVF_TRY(mlp->m.ensure(sizeof(float) * kMlpParams));
+    SVF_TRY(mlp->v.ensure(sizeof(float) * kMlpParams));
+    SVF_TRY(mlp->wbf.ensure(2 * kMlpParams));
+    SVF_TRY(mlp->d_pairs.ensure(sizeof(uint32_t) * kMlpPairs));
+    SVF_TRY(mlp->d_xmean.ensure(sizeof(float) * kMlpInputs));
+    SVF_TRY(mlp->d_xrstd.ensure(sizeof(float) * kMlpInputs));
+    SVF_TRY(mlp->d_ymean.ensure(sizeof(float) * kMlpOutputs));
+    SVF_TRY(mlp->d_ystd.ensure(sizeof(float) * kMlpOutputs));
+    SVF_CUDA(cudaMemcpyAsync(mlp->w.p, w.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemsetAsync(mlp->m.p, 0, sizeof(float) * kMlpParams, ctx->stream));
+    SVF_CUDA(cudaMemsetAsync(mlp->v.p, 0, sizeof(float) * kMlpParams, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_pairs.p, mlp->pairs, sizeof(mlp->pairs), cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_xmean.p, mlp->xmean, sizeof(mlp->xmean), cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_xrstd.p, mlp->xrstd, sizeof(mlp->xrstd), cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_ymean.p, mlp->ymean, sizeof(mlp->ymean), cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_ystd.p, mlp->ystd, sizeof(mlp->ystd), cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(svf::mlp_to_bf16(mlp->w.as<float>(), kMlpParams, mlp->wbf.p, ctx->stream));
+    mlp->step = 0;
+    return SVF_OK;
+}
+
+// Forward pass of `rows` normalised inputs X [rows][96] -> Y [rows][10]; the
+// hidden activations H1, H2 and (training) their pre-activations Z1, Z2 are
+// [rows][256].  bf16: the inference copies of the weights.
+svf_status mlp_forward(svf_ctx* ctx, const svf_mlp* mlp, const float* X, int rows, float* Z1, float* H1, float* Z2,
+                       float* H2, float* Y, bool bf16)
+{
+    using namespace svf;
+    const float* w = mlp->w.as<float>();
+    auto W = [&](size_t off) -> const void* {
+        return bf16 ? static_cast<const void*>(mlp->wbf.as<uint16_t>() + off) : static_cast<const void*>(w + off);
+    };
+    const int block = 1 << 20;   // rows per launch (the GEMM grid's y extent)
+    for(int r0 = 0; r0 < rows; r0 += block)
+    {
+        const int r = std::min(block, rows - r0);
+        const size_t h = (size_t)r0 * kMlpHidden;
+        SVF_CUDA(mlp_gemm(false, true, r, kMlpHidden, kMlpInputs, X + (size_t)r0 * kMlpInputs, kMlpInputs, W(kMlpW1),
+                          bf16, kMlpInputs, H1 + h, kMlpHidden, w + kMlpB1, 1, Z1 ? Z1 + h : nullptr, nullptr,
+                          ctx->stream));
+        SVF_CUDA(mlp_gemm(false, true, r, kMlpHidden, kMlpHidden, H1 + h, kMlpHidden, W(kMlpW2), bf16, kMlpHidden,
+                          H2 + h, kMlpHidden, w + kMlpB2, 1, Z2 ? Z2 + h : nullptr, nullptr, ctx->stream));
+        SVF_CUDA(mlp_gemm(false, true, r, kMlpOutputs, kMlpHidden, H2 + h, kMlpHidden, W(kMlpW3), bf16, kMlpHidden,
+                          Y + (size_t)r0 * kMlpOutputs, kMlpOutputs, w + kMlpB3, 0, nullptr, nullptr, ctx->stream));
+    }
+    return SVF_OK;
+}
+
+// Features [n][96] of luminance slabs [n][stride] (normalised with the model's
+// statistics when `normalise`).
+cudaError_t mlp_features_of(const svf_mlp* mlp, const float* lum, uint64_t stride, uint64_t n, float* X,
+                            bool normalise, cudaStream_t stream)
+{
+    return svf::mlp_features(lum, stride, n, mlp->d_order.as<uint32_t>(), mlp->d_start.as<uint32_t>(),
+                             mlp->d_binw.as<float>(), mlp->d_pairs.as<uint32_t>(),
+                             normalise ? mlp->d_xmean.as<float>() : nullptr,
+                             normalise ? mlp->d_xrstd.as<float>() : nullptr, X, stream);
+}
+
+// Scratch of one training step for `rows` rows (in the context).
+struct MlpScratch
+{
+    DevBuf z1, h1, z2, h2, y, dy, dh2, dh1, dsum, loss;
+};
+
+// One optimiser step on normalised X [rows][96], T [rows][10]: forward, MSE
+// gradient, backward into mlp->g, Adam (or SGD); adds the loss to *loss_dev.
+svf_status mlp_train_step(svf_ctx* ctx, svf_mlp* mlp, MlpScratch& s, const float* X, const float* T, int rows,
+                          float lr, bool sgd)
+{
+    using namespace svf;
+    const size_t hr = (size_t)rows * kMlpHidden;
+    SVF_TRY(s.z1.ensure(sizeof(float) * hr));
+    SVF_TRY(s.h1.ensure(sizeof(float) * hr));
+    SVF_TRY(s.z2.ensure(sizeof(float) * hr));
+    SVF_TRY(s.h2.ensure(sizeof(float) * hr));
+    SVF_TRY(s.dh2.ensure(sizeof(float) * hr));
+    SVF_TRY(s.dh1.ensure(sizeof(float) * hr));
+    SVF_TRY(s.y.ensure(sizeof(float) * rows * kMlpOutputs));
+    SVF_TRY(s.dy.ensure(sizeof(float) * rows * kMlpOutputs));
+    SVF_TRY(s.dsum.ensure(sizeof(double) * kMlpHidden));
+    SVF_TRY(s.loss.ensure(sizeof(double)));
+    float *z1 = s.z1.as<float>(), *h1 = s.h1.as<float>(), *z2 = s.z2.as<float>(), *h2 = s.h2.as<float>();
+    float *y = s.y.as<float>(), *dy = s.dy.as<float>(), *dh2 = s.dh2.as<float>(), *dh1 = s.dh1.as<float>();
+    float* w = mlp->w.as<float>();
+    float* g = mlp->g.as<float>();
+    SVF_TRY(mlp_forward(ctx, mlp, X, rows, z1, h1, z2, h2, y, false));
+    SVF_CUDA(mlp_mse_grad(y, T, rows, kMlpOutputs, dy, s.loss.as<double>(), ctx->stream));
+    // layer 3
+    SVF_CUDA(mlp_gemm(true, false, kMlpOutputs, kMlpHidden, rows, dy, kMlpOutputs, h2, false, kMlpHidden,
+                      g + kMlpW3, kMlpHidden, nullptr, 0, nullptr, nullptr, ctx->stream));
+    SVF_CUDA(mlp_colsum(dy, rows, kMlpOutputs, s.dsum.as<double>(), nullptr, ctx->stream));
+    SVF_CUDA(mlp_to_float(s.dsum.as<double>(), kMlpOutputs, 1.0f, g + kMlpB3, ctx->stream));
+    SVF_CUDA(mlp_gemm(false, false, rows, kMlpHidden, kMlpOutputs, dy, kMlpOutputs, w + kMlpW3, false, kMlpHidden,
+                      dh2, kMlpHidden, nullptr, 2, nullptr, z2, ctx->stream));
+    // layer 2
+    SVF_CUDA(mlp_gemm(true, false, kMlpHidden, kMlpHidden, rows, dh2, kMlpHidden, h1, false, kMlpHidden,
+                      g + kMlpW2, kMlpHidden, nullptr, 0, nullptr, nullptr, ctx->stream));
+    SVF_CUDA(mlp_colsum(dh2, rows, kMlpHidden, s.dsum.as<double>(), nullptr, ctx->stream));
+    SVF_CUDA(mlp_to_float(s.dsum.as<double>(), kMlpHidden, 1.0f, g + kMlpB2, ctx->stream));
+    SVF_CUDA(mlp_gemm(false, false, rows, kMlpHidden, kMlpHidden, dh2, kMlpHidden, w + kMlpW2, false, kMlpHidden,
+                      dh1, kMlpHidden, nullptr, 2, nullptr, z1, ctx->stream));
+    // layer 1
+    SVF_CUDA(mlp_gemm(true, false, kMlpHidden, kMlpInputs, rows, dh1, kMlpHidden, X, false, kMlpInputs, g + kMlpW1,
+                      kMlpInputs, nullptr, 0, nullptr, nullptr, ctx->stream));
+    SVF_CUDA(mlp_colsum(dh1, rows, kMlpHidden, s.dsum.as<double>(), nullptr, ctx->stream));
+    SVF_CUDA(mlp_to_float(s.dsum.as<double>(), kMlpHidden, 1.0f, g + kMlpB1, ctx->stream));
+    ++mlp->step;
+    SVF_CUDA(mlp_adam(w, g, mlp->m.as<float>(), mlp->v.as<float>(), kMlpParams, lr, mlp->step, sgd, ctx->stream));
+    return SVF_OK;
+}
 
 svf_status check_ctx(svf_ctx* ctx)
 {
@@ -202,6 +414,18 @@ svf_status check_ctx(svf_ctx* ctx)
     if(e != cudaSuccess)
         return fail(SVF_ECUDA, "cudaSetDevice(%d): %s", ctx->device, cudaGetErrorString(e));
     return SVF_OK;
+}
+
+// Initial LM damping relative to the reference's rule for a BTF's fit options:
+// the learned guess starts close to a minimum, where the reference's damping
+// (sized for its default guess) takes steps below BreakOnSmallStep and stops
+// the fit early; it starts lighter unless the caller says otherwise.
+constexpr float kMlpInitialDamping = 1e-3f;
+float initial_damping(const svf_fit_options& o)
+{
+    if(o.initial_damping > 0.0f)
+        return o.initial_damping;
+    return o.init_mode == SVF_INIT_MLP ? kMlpInitialDamping : 1.0f;
 }
 
 svf_status check_options(const svf_lsq_options* o)
@@ -406,6 +630,7 @@ struct LmRun
     uint32_t n_seg = 0;
     bool all_up = false;
     bool rgb = false;      // the 11-parameter RGB fit
+    float damping = 0.0f;  // initial damping scale of a single-segment run (0: the reference's rule)
 };
 
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c);
@@ -543,7 +768,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     svf::LmArgs a{};
     if(r.n_seg == 0)
     {
-        a.seg[0] = svf::LmSegment{ 0, lay->L, r.stride, r.lum, lay->geo.as<float>() };
+        a.seg[0] = svf::LmSegment{ 0, lay->L, r.stride, r.lum, lay->geo.as<float>(), r.damping };
         a.n_seg = 1;
         a.L = lay->L;
         a.lum_stride = r.stride;
@@ -867,8 +1092,10 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     SVF_TRY(check_options(&opts->lsq));
     if(btf->sample_type != SVF_SAMPLES_F32 && btf->sample_type != SVF_SAMPLES_F16)
         return fail(SVF_EINVAL, "unknown sample_type %u", btf->sample_type);
-    if(opts->init_mode != SVF_INIT_DEFAULT && opts->init_mode != SVF_INIT_GIVEN)
+    if(opts->init_mode != SVF_INIT_DEFAULT && opts->init_mode != SVF_INIT_GIVEN && opts->init_mode != SVF_INIT_MLP)
         return fail(SVF_EINVAL, "unknown init_mode %u", opts->init_mode);
+    if(opts->init_mode == SVF_INIT_MLP && !opts->mlp)
+        return fail(SVF_EINVAL, "SVF_INIT_MLP needs a model (svf_fit_options::mlp)");
     if(opts->init_mode == SVF_INIT_GIVEN && !opts->init_params)
         return fail(SVF_EINVAL, "SVF_INIT_GIVEN needs init_params");
     const uint64_t T = (uint64_t)btf->width * btf->height;
@@ -884,6 +1111,11 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     const svf::InitLayout* init_lay = nullptr;
     if(opts->init_mode == SVF_INIT_DEFAULT)
         SVF_TRY(prepare_init(ctx, lay, desc, &init_lay));
+    const svf_mlp* mlp = opts->init_mode == SVF_INIT_MLP ? opts->mlp : nullptr;
+    if(mlp && (mlp->L != L || std::memcmp(mlp->lp.data(), lay->lp.data(), sizeof(float) * 2 * L) != 0))
+        return fail(SVF_EINVAL, "the model was trained for another direction layout");
+    if(mlp && mlp->device != ctx->device)
+        return fail(SVF_EINVAL, "the model lives on device %d, the context on %d", mlp->device, ctx->device);
 
     const size_t elem = btf->sample_type == SVF_SAMPLES_F16 ? 2 : 4;
     const size_t texel_bytes = elem * 3 * (size_t)N;
@@ -905,6 +1137,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     size_t free_b = 0, total_b = 0;
     SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t per_texel = sizeof(float) * (stride + 3 + 2 * kout + 7 + 1 + 12) + (rgb ? 2 * stride3 : 0) +
+                             (mlp ? sizeof(float) * (svf::kMlpInputs + 2 * svf::kMlpHidden + svf::kMlpOutputs) : 0) +
                              (default_init ? 2 * 2 * stride + sizeof(float) * ndf_ld : 0) +
                              (maps->ndf ? sizeof(float) * svf::kNdfTexels : 0) +
                              (samples_on_device ? 0 : 2 * texel_bytes);
@@ -935,6 +1168,13 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     }
     if(maps->ndf)
         SVF_TRY(ctx->ndf_tex.ensure(sizeof(float) * svf::kNdfTexels * chunk));
+    if(mlp)
+    {
+        SVF_TRY(ctx->mlp_x.ensure(sizeof(float) * svf::kMlpInputs * chunk));
+        SVF_TRY(ctx->mlp_h1.ensure(sizeof(float) * svf::kMlpHidden * chunk));
+        SVF_TRY(ctx->mlp_h2.ensure(sizeof(float) * svf::kMlpHidden * chunk));
+        SVF_TRY(ctx->mlp_y.ensure(sizeof(float) * svf::kMlpOutputs * chunk));
+    }
     DevBuf* staging[2] = { &ctx->samples, &ctx->samples2 };
     if(!samples_on_device)
     {
@@ -1019,16 +1259,27 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->ndf.as<float>(), ndf_ld, n, ctx->init.as<float>(),
                                              nullptr, maps->ndf ? ctx->ndf_tex.as<float>() : nullptr, ctx->stream));
         }
+        else if(mlp)
+        {
+            // the learned initial guess from the chunk's luminance slabs
+            SVF_CUDA(mlp_features_of(mlp, ctx->lum.as<float>(), stride, n, ctx->mlp_x.as<float>(), true,
+                                     ctx->stream));
+            SVF_TRY(mlp_forward(ctx, mlp, ctx->mlp_x.as<float>(), (int)n, nullptr, ctx->mlp_h1.as<float>(), nullptr,
+                                ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>(), true));
+            SVF_CUDA(svf::mlp_finish(ctx->mlp_y.as<float>(), n, mlp->d_ymean.as<float>(), mlp->d_ystd.as<float>(),
+                                     ctx->init.as<float>(), ctx->stream));
+        }
         else
             SVF_TRY(to_device(ctx, rgb ? ctx->init_rgb.p : ctx->init.p, opts->init_params + kout * c0,
                               sizeof(float) * kout * n));
-        if(rgb && default_init)
+        if(rgb && (default_init || mlp))
         {
             // the RGB fit starts where the luminance fit from the default guess
             // ends, coloured by the average chromaticity (svbrdffit's own maps):
             // its accepted steps only lower that RGB residual
             LmRun lr{ ctx->lum.p, stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
                       ctx->stats.as<svf_texel_stats>() + c0, nullptr, nullptr, nullptr, nullptr, nullptr, n };
+            lr.damping = initial_damping(*opts);
             SVF_TRY(run_lm(ctx, lay, &opts->lsq, lr));
             SVF_CUDA(svf::launch_rgb_init(ctx->out.as<float>(), ctx->avg.as<float>(), n, ctx->init_rgb.as<float>(),
                                           ctx->stream));
@@ -1040,6 +1291,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                  ctx->out.as<float>(), ctx->rmse.as<float>(), ctx->stats.as<svf_texel_stats>() + c0,
                  ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n };
         r.rgb = rgb;
+        // (the RGB fit chained from the luminance fit starts with the reference's damping)
+        r.damping = rgb && (default_init || mlp) ? 1.0f : initial_damping(*opts);
         SVF_TRY(run_lm(ctx, lay, &opts->lsq, r));
         SVF_CUDA(mark(ev(c, 5), ctx->stream));
         // outputs (into host or device buffers of the caller)
@@ -1084,7 +1337,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                     reachable(maps->diffuse) && reachable(maps->specular) && reachable(maps->sigma) &&
                     reachable(maps->basis) && reachable(maps->rmse) && reachable(maps->params) &&
                     reachable(maps->init) && reachable(maps->ndf);
-    if(eligible && (!rgb || default_init) && !lay->tuned && T >= 4096)
+    if(eligible && (!rgb || default_init || mlp) && !lay->tuned && T >= 4096)
         SVF_TRY(tune_lm(ctx, lay, &opts->lsq));   // the autotuner synchronises: never inside a capture
     std::vector<uint64_t> key;
     if(eligible)
@@ -1094,6 +1347,14 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         u(lay);
         u(init_lay);
         u(opts->init_params);
+        u(mlp);
+        key.push_back(mlp ? (uint64_t)mlp->step : 0);
+        {
+            const float dmp = initial_damping(*opts);
+            uint32_t bits;
+            std::memcpy(&bits, &dmp, 4);
+            key.push_back(bits);
+        }
         u(maps->diffuse);
         u(maps->specular);
         u(maps->sigma);
@@ -1228,6 +1489,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         uint64_t T = 0, stride = 0, stride3 = 0;
         size_t texel_bytes = 0;
         bool on_device = false, default_init = false;
+        const svf_mlp* mlp = nullptr;   // SVF_INIT_MLP
     };
     std::vector<Item> it(n_btf);
     for(uint32_t b = 0; b < n_btf; ++b)
@@ -1238,8 +1500,10 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             return fail(SVF_EINVAL, "btf %u: null layout/samples", b);
         if(v.sample_type != SVF_SAMPLES_F32 && v.sample_type != SVF_SAMPLES_F16)
             return fail(SVF_EINVAL, "btf %u: unknown sample_type %u", b, v.sample_type);
-        if(o.init_mode != SVF_INIT_DEFAULT && o.init_mode != SVF_INIT_GIVEN)
+        if(o.init_mode != SVF_INIT_DEFAULT && o.init_mode != SVF_INIT_GIVEN && o.init_mode != SVF_INIT_MLP)
             return fail(SVF_EINVAL, "btf %u: unknown init_mode %u", b, o.init_mode);
+        if(o.init_mode == SVF_INIT_MLP && !o.mlp)
+            return fail(SVF_EINVAL, "btf %u: SVF_INIT_MLP needs a model (svf_fit_options::mlp)", b);
         if(o.init_mode == SVF_INIT_GIVEN && !o.init_params)
             return fail(SVF_EINVAL, "btf %u: SVF_INIT_GIVEN needs init_params", b);
         const svf_lsq_options &a = o.lsq, &z = opts[0].lsq;
@@ -1260,6 +1524,15 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         x.default_init = o.init_mode == SVF_INIT_DEFAULT;
         if(x.default_init)
             SVF_TRY(prepare_init(ctx, x.lay, v.layout, &x.init));
+        if(o.init_mode == SVF_INIT_MLP)
+        {
+            x.mlp = o.mlp;
+            if(x.mlp->L != x.lay->L || std::memcmp(x.mlp->lp.data(), x.lay->lp.data(), sizeof(float) * 2 * x.mlp->L))
+                return fail(SVF_EINVAL, "btf %u: the model was trained for another direction layout", b);
+            if(x.mlp->device != ctx->device)
+                return fail(SVF_EINVAL, "btf %u: the model lives on device %d, the context on %d", b, x.mlp->device,
+                            ctx->device);
+        }
     }
     uint32_t ndf_ld = 0;   // NDF rows per texel (the same for every layout: the 64x64 texture's hemisphere)
     for(auto& x : it)
@@ -1276,6 +1549,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         return sizeof(float) * (x.stride + 3 + 7 + kout + 1 + 12) + sizeof(svf_texel_stats) +
                (rgb ? 2 * x.stride3 + sizeof(float) * 12 : 0) +
                (x.default_init ? 2 * 2 * x.stride + sizeof(float) * ndf_ld : 0) +
+               (x.mlp ? sizeof(float) * (svf::kMlpInputs + 2 * svf::kMlpHidden + svf::kMlpOutputs) : 0) +
                (maps[b].ndf ? sizeof(float) * svf::kNdfTexels : 0) + (x.on_device ? 0 : x.texel_bytes);
     };
     struct Piece
@@ -1318,7 +1592,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         chunks.pop_back();
 
     // buffers for the largest chunk
-    uint64_t max_n = 0, max_floats = 0, max_halves = 0;
+    uint64_t max_n = 0, max_floats = 0, max_halves = 0, max_mlp = 0;
     size_t max_stage = 0;
     bool any_ndf = false, any_default = false;
     for(auto& ch : chunks)
@@ -1333,6 +1607,8 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                 max_stage = std::max(max_stage, it[p.b].texel_bytes * (size_t)p.count);
             any_ndf = any_ndf || maps[p.b].ndf;
             any_default = any_default || it[p.b].default_init;
+            if(it[p.b].mlp)
+                max_mlp = std::max(max_mlp, p.count);
         }
         max_n = std::max(max_n, n);
         max_floats = std::max(max_floats, f);
@@ -1361,6 +1637,13 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         SVF_TRY(ctx->ndf_tex.ensure(sizeof(float) * svf::kNdfTexels * max_n));
     if(max_stage)
         SVF_TRY(ctx->samples.ensure(max_stage));
+    if(max_mlp)
+    {
+        SVF_TRY(ctx->mlp_x.ensure(sizeof(float) * svf::kMlpInputs * max_mlp));
+        SVF_TRY(ctx->mlp_h1.ensure(sizeof(float) * svf::kMlpHidden * max_mlp));
+        SVF_TRY(ctx->mlp_h2.ensure(sizeof(float) * svf::kMlpHidden * max_mlp));
+        SVF_TRY(ctx->mlp_y.ensure(sizeof(float) * svf::kMlpOutputs * max_mlp));
+    }
 
     std::vector<svf_run_stats> rs(n_btf);
     svf_run_stats all{};
@@ -1408,6 +1691,14 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                                                                : nullptr,
                                                  ctx->stream));
             }
+            else if(x.mlp)
+            {
+                SVF_CUDA(mlp_features_of(x.mlp, lum, x.stride, p.count, ctx->mlp_x.as<float>(), true, ctx->stream));
+                SVF_TRY(mlp_forward(ctx, x.mlp, ctx->mlp_x.as<float>(), (int)p.count, nullptr, ctx->mlp_h1.as<float>(),
+                                    nullptr, ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>(), true));
+                SVF_CUDA(svf::mlp_finish(ctx->mlp_y.as<float>(), p.count, x.mlp->d_ymean.as<float>(),
+                                         x.mlp->d_ystd.as<float>(), ctx->init.as<float>() + 7 * p.k0, ctx->stream));
+            }
             else
                 SVF_TRY(to_device(ctx, init_used + kout * p.k0, opts[p.b].init_params + kout * p.first,
                                   sizeof(float) * kout * p.count));
@@ -1417,12 +1708,12 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         // fit coloured by the average chromaticity (as in svf_fit_texels)
         bool rgb_from_lum = false;
         for(auto& p : ch)
-            rgb_from_lum = rgb_from_lum || (rgb && it[p.b].default_init);
+            rgb_from_lum = rgb_from_lum || (rgb && (it[p.b].default_init || it[p.b].mlp));
         if(rgb_from_lum)
         {
             // pieces with given RGB parameters ride along from a zero start
             for(auto& p : ch)
-                if(!it[p.b].default_init)
+                if(!it[p.b].default_init && !it[p.b].mlp)
                     SVF_CUDA(cudaMemsetAsync(ctx->init.as<float>() + 7 * p.k0, 0, sizeof(float) * 7 * p.count,
                                              ctx->stream));
             svf::LmSegment ls[svf::kLmMaxSegments];
@@ -1433,7 +1724,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             {
                 const Item& x = it[ch[i].b];
                 ls[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride, ctx->lum.as<float>() + ch[i].off,
-                                        x.lay->geo.as<float>() };
+                                        x.lay->geo.as<float>(), initial_damping(opts[ch[i].b]) };
                 lup = lup && x.lay->all_up;
                 lstride = std::max(lstride, x.stride);
                 if(x.lay->L > lbig->L)
@@ -1444,7 +1735,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                       ls, (uint32_t)ch.size(), lup, false };
             SVF_TRY(run_lm(ctx, lbig, &opts[0].lsq, lr));
             for(auto& p : ch)
-                if(it[p.b].default_init)
+                if(it[p.b].default_init || it[p.b].mlp)
                     SVF_CUDA(svf::launch_rgb_init(ctx->out.as<float>() + 7 * p.k0, ctx->avg.as<float>() + 3 * p.k0,
                                                   p.count, init_used + 12 * p.k0, ctx->stream));
         }
@@ -1457,12 +1748,14 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         for(size_t i = 0; i < ch.size(); ++i)
         {
             const Item& x = it[ch[i].b];
+            // (the RGB fit chained from the luminance fit starts with the reference's damping)
+            const float dmp = rgb && (x.default_init || x.mlp) ? 1.0f : initial_damping(opts[ch[i].b]);
             if(rgb)
                 seg[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride3,
-                                         ctx->rgb16.as<uint16_t>() + ch[i].off3, x.lay->geo.as<float>() };
+                                         ctx->rgb16.as<uint16_t>() + ch[i].off3, x.lay->geo.as<float>(), dmp };
             else
                 seg[i] = svf::LmSegment{ (uint32_t)ch[i].k0, x.lay->L, x.stride, ctx->lum.as<float>() + ch[i].off,
-                                         x.lay->geo.as<float>() };
+                                         x.lay->geo.as<float>(), dmp };
             all_up = all_up && x.lay->all_up;
             max_stride = std::max(max_stride, rgb ? x.stride3 : x.stride);
             if(x.lay->L > big->L)
@@ -1600,6 +1893,432 @@ svf_status svf_synth_btf(svf_ctx* ctx, uint32_t seed, uint32_t mix, const float*
     }
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));
     return SVF_OK;
+}
+
+} // extern "C"
+
+// ---- learned initial guess ------------------------------------------------------
+
+namespace
+{
+
+uint64_t splitmix64(uint64_t& x)
+{
+    uint64_t z = (x += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+
+double uniform01(uint64_t& x) { return (double)(splitmix64(x) >> 11) * (1.0 / 9007199254740992.0); }
+
+// 32 direction pairs (sample indices light * L + view): 16 near-mirror pairs
+// (the view closest to the light reflected about +z; parabolic (x, y) -> (-x,
+// -y)) over randomly drawn lights, then 16 distinct random pairs.
+void choose_pairs(const float* lp, uint32_t L, uint64_t seed, uint32_t* pairs)
+{
+    uint64_t r = seed ^ 0x5f3759dfull;
+    const uint32_t N = L * L;
+    int k = 0;
+    auto taken = [&](uint32_t p) { return std::find(pairs, pairs + k, p) != pairs + k; };
+    for(int tries = 0; k < svf::kMlpPairs / 2 && tries < 1000; ++tries)
+    {
+        const uint32_t i = (uint32_t)(splitmix64(r) % L);
+        uint32_t best = 0;
+        float bd = 1e30f;
+        for(uint32_t o = 0; o < L; ++o)
+        {
+            const float dx = lp[2 * o] + lp[2 * i], dy = lp[2 * o + 1] + lp[2 * i + 1];
+            if(dx * dx + dy * dy < bd)
+            {
+                bd = dx * dx + dy * dy;
+                best = o;
+            }
+        }
+        const uint32_t p = i * L + best;
+        if(!taken(p))
+            pairs[k++] = p;
+    }
+    while(k < svf::kMlpPairs)
+    {
+        const uint32_t p = (uint32_t)(splitmix64(r) % N);
+        if(!taken(p) || N <= (uint32_t)k)
+            pairs[k++] = p;
+    }
+}
+
+svf_status check_mlp(svf_ctx* ctx, const svf_mlp* mlp)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(!mlp)
+        return fail(SVF_EINVAL, "null model");
+    if(mlp->device != ctx->device)
+        return fail(SVF_EINVAL, "the model lives on device %d, the context on %d", mlp->device, ctx->device);
+    return SVF_OK;
+}
+
+constexpr char kMlpMagic[8] = { 'S', 'V', 'F', 'M', 'L', 'P', '0', '1' };
+
+size_t mlp_blob_bytes(uint32_t L)
+{
+    return sizeof(kMlpMagic) + 2 * sizeof(uint32_t) + sizeof(float) * 2 * L + sizeof(uint32_t) * svf::kMlpPairs +
+           sizeof(float) * 2 * (svf::kMlpInputs + svf::kMlpOutputs) + sizeof(float) * svf::kMlpParams;
+}
+
+} // namespace
+
+extern "C" {
+
+void svf_mlp_train_options_default(svf_mlp_train_options* o)
+{
+    if(!o)
+        return;
+    o->texels = 1u << 20;
+    o->seed = 12345;
+    o->mix = 1;
+    o->epochs = 24;
+    o->batch = 4096;
+    o->lr = 1e-3f;
+    o->max_iterations = 1024;
+}
+
+svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_mlp_train_options* opts, svf_mlp** out,
+                         float* final_loss)
+{
+    using namespace svf;
+    SVF_TRY(check_ctx(ctx));
+    if(!out || !lp)
+        return fail(SVF_EINVAL, "null output/lights");
+    *out = nullptr;
+    svf_mlp_train_options o;
+    svf_mlp_train_options_default(&o);
+    if(opts)
+        o = *opts;
+    if(L < 3 || L > 160)
+        return fail(SVF_EINVAL, "light_count %u outside 3..160", L);
+    if(o.texels < 256 || o.texels > (1u << 24) || o.batch < 16 || o.batch > (1u << 16) || o.epochs < 1 ||
+       o.epochs > 1000 || !(o.lr > 0.0f) || o.mix > 1)
+        return fail(SVF_EINVAL, "bad training options (texels 256..2^24, batch 16..65536, epochs 1..1000, lr > 0)");
+    std::unique_ptr<svf_mlp> mlp(new(std::nothrow) svf_mlp);
+    if(!mlp)
+        return fail(SVF_ENOMEM, "model allocation failed");
+    mlp->device = ctx->device;
+    mlp->L = L;
+    mlp->lp.resize(2 * (size_t)L);
+    SVF_CUDA(cudaMemcpy(mlp->lp.data(), lp, sizeof(float) * 2 * L, cudaMemcpyDefault));
+    choose_pairs(mlp->lp.data(), L, o.seed, mlp->pairs);
+    // Glorot-uniform weights, zero biases (statistics are filled in below)
+    std::vector<float> w(kMlpParams, 0.0f);
+    uint64_t r = o.seed * 0x2545f4914f6cdd1dull + 7;
+    auto glorot = [&](size_t off, int fan_out, int fan_in) {
+        const double a = std::sqrt(6.0 / (fan_in + fan_out));
+        for(size_t i = 0; i < (size_t)fan_out * fan_in; ++i)
+            w[off + i] = (float)((2.0 * uniform01(r) - 1.0) * a);
+    };
+    glorot(kMlpW1, kMlpHidden, kMlpInputs);
+    glorot(kMlpW2, kMlpHidden, kMlpHidden);
+    glorot(kMlpW3, kMlpOutputs, kMlpHidden);
+    SVF_TRY(mlp_upload(ctx, mlp.get(), w));
+
+    // training data: synthetic texels fitted by the plain LM from the default guess
+    const uint32_t N = L * L, T = o.texels;
+    const size_t texel_bytes = sizeof(float) * 3 * (size_t)N;
+    const uint32_t gen = (uint32_t)std::max<size_t>(256, std::min<size_t>(65536, (size_t(2) << 30) / texel_bytes));
+    const uint64_t stride = round_up(N, 8);
+    DevBuf samples, params, X, Y, lum, avg;
+    SVF_TRY(samples.ensure(texel_bytes * std::min(gen, T)));
+    SVF_TRY(lum.ensure(sizeof(float) * stride * std::min(gen, T)));
+    SVF_TRY(avg.ensure(sizeof(float) * 3 * std::min(gen, T)));
+    SVF_TRY(params.ensure(sizeof(float) * 7 * std::min(gen, T)));
+    SVF_TRY(X.ensure(sizeof(float) * kMlpInputs * (size_t)T));
+    SVF_TRY(Y.ensure(sizeof(float) * kMlpOutputs * (size_t)T));
+    const svf_layout_desc desc{ mlp->lp.data(), L, nullptr, 0, nullptr, nullptr, 0 };
+    svf_fit_options fo{};
+    svf_lsq_options_default(&fo.lsq);
+    fo.lsq.max_iterations = o.max_iterations;
+    fo.init_mode = SVF_INIT_DEFAULT;
+    for(uint32_t c0 = 0; c0 < T; c0 += gen)
+    {
+        const uint32_t n = std::min(gen, T - c0);
+        SVF_TRY(svf_synth_btf(ctx, o.seed, o.mix, mlp->lp.data(), L, c0, n, SVF_SAMPLES_F32, 0.0f, samples.p,
+                              nullptr));
+        const svf_btf_view v{ samples.p, SVF_SAMPLES_F32, n, 1, &desc };
+        svf_maps m{};
+        m.params = params.as<float>();
+        const svf_status st = svf_fit_texels(ctx, &v, &fo, &m, nullptr);
+        if(st != SVF_OK && st != SVF_EPARTIAL)
+            return st;
+        SVF_CUDA(launch_luminance(samples.p, SVF_SAMPLES_F32, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr,
+                                  nullptr, ctx->stream));
+        SVF_CUDA(mlp_features_of(mlp.get(), lum.as<float>(), stride, n, X.as<float>() + (size_t)kMlpInputs * c0,
+                                 false, ctx->stream));
+        SVF_CUDA(mlp_targets(params.as<float>(), n, Y.as<float>() + (size_t)kMlpOutputs * c0, ctx->stream));
+    }
+    samples.reset();
+    lum.reset();
+    // input statistics on the device, target statistics (finite rows only) on the host
+    DevBuf sums;
+    SVF_TRY(sums.ensure(sizeof(double) * 2 * kMlpInputs));
+    SVF_CUDA(mlp_colsum(X.as<float>(), (int)T, kMlpInputs, sums.as<double>(), sums.as<double>() + kMlpInputs,
+                        ctx->stream));
+    std::vector<double> hs(2 * kMlpInputs);
+    std::vector<float> hy((size_t)kMlpOutputs * T);
+    SVF_CUDA(cudaMemcpyAsync(hs.data(), sums.p, sizeof(double) * 2 * kMlpInputs, cudaMemcpyDeviceToHost, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(hy.data(), Y.p, sizeof(float) * hy.size(), cudaMemcpyDeviceToHost, ctx->stream));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    for(int f = 0; f < kMlpInputs; ++f)
+    {
+        const double mean = hs[f] / T, var = std::max(0.0, hs[kMlpInputs + f] / T - mean * mean);
+        mlp->xmean[f] = (float)mean;
+        mlp->xrstd[f] = var > 1e-12 ? (float)(1.0 / std::sqrt(var)) : 1.0f;
+    }
+    std::vector<uint32_t> valid;
+    valid.reserve(T);
+    double ys[kMlpOutputs] = {}, ys2[kMlpOutputs] = {};
+    for(uint32_t t = 0; t < T; ++t)
+    {
+        const float* y = hy.data() + (size_t)kMlpOutputs * t;
+        bool ok = true;
+        for(int k = 0; k < kMlpOutputs; ++k)
+            ok = ok && std::isfinite(y[k]);
+        if(!ok)
+            continue;
+        valid.push_back(t);
+        for(int k = 0; k < kMlpOutputs; ++k)
+        {
+            ys[k] += y[k];
+            ys2[k] += (double)y[k] * y[k];
+        }
+    }
+    if(valid.size() < o.batch)
+        return fail(SVF_EINVAL, "only %zu of %u training texels have a finite fit", valid.size(), T);
+    for(int k = 0; k < kMlpOutputs; ++k)
+    {
+        const double mean = ys[k] / valid.size(), var = std::max(0.0, ys2[k] / valid.size() - mean * mean);
+        mlp->ymean[k] = (float)mean;
+        mlp->ystd[k] = var > 1e-12 ? (float)std::sqrt(var) : 1.0f;
+    }
+    for(uint32_t t : valid)
+        for(int k = 0; k < kMlpOutputs; ++k)
+        {
+            float& y = hy[(size_t)kMlpOutputs * t + k];
+            y = (y - mlp->ymean[k]) / mlp->ystd[k];
+        }
+    SVF_CUDA(cudaMemcpyAsync(Y.p, hy.data(), sizeof(float) * hy.size(), cudaMemcpyHostToDevice, ctx->stream));
+    // (hy stays alive until the stream is synchronised below)
+
+    SVF_TRY(mlp_upload(ctx, mlp.get(), w));   // with the statistics
+    SVF_CUDA(mlp_normalize(X.as<float>(), (int)T, kMlpInputs, mlp->d_xmean.as<float>(), mlp->d_xrstd.as<float>(),
+                           ctx->stream));
+
+    // epochs of shuffled minibatches, Adam with a cosine-decayed step size
+    const uint32_t V = (uint32_t)valid.size(), B = o.batch;
+    const uint32_t per_epoch = (V + B - 1) / B;
+    const uint64_t total_steps = (uint64_t)per_epoch * o.epochs;
+    DevBuf idx, Xb, Yb;
+    SVF_TRY(idx.ensure(sizeof(uint32_t) * V));
+    SVF_TRY(Xb.ensure(sizeof(float) * kMlpInputs * B));
+    SVF_TRY(Yb.ensure(sizeof(float) * kMlpOutputs * B));
+    MlpScratch scratch;
+    std::vector<uint32_t> perm(valid);
+    uint64_t done = 0;
+    for(uint32_t e = 0; e < o.epochs; ++e)
+    {
+        for(uint32_t i = V - 1; i > 0; --i)
+            std::swap(perm[i], perm[splitmix64(r) % (i + 1)]);
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));   // the previous epoch's indices are consumed
+        SVF_CUDA(cudaMemcpyAsync(idx.p, perm.data(), sizeof(uint32_t) * V, cudaMemcpyHostToDevice, ctx->stream));
+        if(e + 1 == o.epochs)
+        {
+            SVF_TRY(scratch.loss.ensure(sizeof(double)));
+            SVF_CUDA(cudaMemsetAsync(scratch.loss.p, 0, sizeof(double), ctx->stream));
+        }
+        for(uint32_t b0 = 0; b0 < V; b0 += B, ++done)
+        {
+            const int rows = (int)std::min(B, V - b0);
+            SVF_CUDA(mlp_gather_rows(X.as<float>(), kMlpInputs, Y.as<float>(), kMlpOutputs, idx.as<uint32_t>() + b0,
+                                     rows, Xb.as<float>(), Yb.as<float>(), ctx->stream));
+            const double f = 0.5 * (1.0 + std::cos(3.14159265358979 * (double)done / (double)total_steps));
+            SVF_TRY(mlp_train_step(ctx, mlp.get(), scratch, Xb.as<float>(), Yb.as<float>(), rows,
+                                   (float)(o.lr * (0.05 + 0.95 * f)), false));
+        }
+    }
+    SVF_CUDA(mlp_to_bf16(mlp->w.as<float>(), kMlpParams, mlp->wbf.p, ctx->stream));
+    double loss = 0.0;
+    SVF_CUDA(cudaMemcpyAsync(&loss, scratch.loss.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    if(final_loss)
+        *final_loss = (float)(loss / per_epoch);
+    if(!std::isfinite(loss))
+        return fail(SVF_ECUDA, "training diverged (non-finite loss)");
+    *out = mlp.release();
+    return SVF_OK;
+}
+
+svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples, uint32_t sample_type,
+                           uint32_t texels, float* params, float* features)
+{
+    using namespace svf;
+    SVF_TRY(check_mlp(ctx, mlp));
+    if(!samples || !params)
+        return fail(SVF_EINVAL, "null samples/params");
+    if(sample_type != SVF_SAMPLES_F32 && sample_type != SVF_SAMPLES_F16)
+        return fail(SVF_EINVAL, "unknown sample_type %u", sample_type);
+    const uint32_t N = mlp->L * mlp->L;
+    const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)N;
+    const bool on_device = is_device_pointer(samples);
+    const uint32_t chunk = 65536;
+    const uint32_t c = std::min(chunk, texels);
+    const uint64_t stride = round_up(N, 8);
+    DevBuf staged, x, h1, h2, y, p, lum, avg;
+    if(!on_device)
+        SVF_TRY(staged.ensure(texel_bytes * c));
+    SVF_TRY(lum.ensure(sizeof(float) * stride * c));
+    SVF_TRY(avg.ensure(sizeof(float) * 3 * c));
+    SVF_TRY(x.ensure(sizeof(float) * kMlpInputs * c));
+    SVF_TRY(h1.ensure(sizeof(float) * kMlpHidden * c));
+    SVF_TRY(h2.ensure(sizeof(float) * kMlpHidden * c));
+    SVF_TRY(y.ensure(sizeof(float) * kMlpOutputs * c));
+    SVF_TRY(p.ensure(sizeof(float) * 7 * c));
+    for(uint32_t c0 = 0; c0 < texels; c0 += chunk)
+    {
+        const uint32_t n = std::min(chunk, texels - c0);
+        const void* s = static_cast<const char*>(samples) + c0 * texel_bytes;
+        if(!on_device)
+        {
+            SVF_CUDA(cudaMemcpyAsync(staged.p, s, texel_bytes * n, cudaMemcpyHostToDevice, ctx->stream));
+            s = staged.p;
+        }
+        SVF_CUDA(launch_luminance(s, sample_type, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr, nullptr,
+                                  ctx->stream));
+        SVF_CUDA(mlp_features_of(mlp, lum.as<float>(), stride, n, x.as<float>(), true, ctx->stream));
+        SVF_TRY(mlp_forward(ctx, mlp, x.as<float>(), (int)n, nullptr, h1.as<float>(), nullptr, h2.as<float>(),
+                            y.as<float>(), true));
+        SVF_CUDA(mlp_finish(y.as<float>(), n, mlp->d_ymean.as<float>(), mlp->d_ystd.as<float>(), p.as<float>(),
+                            ctx->stream));
+        SVF_CUDA(cudaMemcpyAsync(params + (size_t)7 * c0, p.p, sizeof(float) * 7 * n, cudaMemcpyDefault,
+                                 ctx->stream));
+        if(features)
+            SVF_CUDA(cudaMemcpyAsync(features + (size_t)kMlpInputs * c0, x.p, sizeof(float) * kMlpInputs * n,
+                                     cudaMemcpyDefault, ctx->stream));
+        // staged, x and p are reused by the next chunk
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return SVF_OK;
+}
+
+svf_status svf_mlp_step(svf_ctx* ctx, svf_mlp* mlp, const float* features, const float* targets, uint32_t rows,
+                        float lr, uint32_t sgd, float* loss)
+{
+    using namespace svf;
+    SVF_TRY(check_mlp(ctx, mlp));
+    if(!features || !targets || rows == 0 || rows > (1u << 20))
+        return fail(SVF_EINVAL, "null features/targets or rows outside 1..2^20");
+    DevBuf X, Y;
+    SVF_TRY(X.ensure(sizeof(float) * kMlpInputs * rows));
+    SVF_TRY(Y.ensure(sizeof(float) * kMlpOutputs * rows));
+    SVF_CUDA(cudaMemcpyAsync(X.p, features, sizeof(float) * kMlpInputs * rows, cudaMemcpyDefault, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(Y.p, targets, sizeof(float) * kMlpOutputs * rows, cudaMemcpyDefault, ctx->stream));
+    MlpScratch s;
+    SVF_TRY(s.loss.ensure(sizeof(double)));
+    SVF_CUDA(cudaMemsetAsync(s.loss.p, 0, sizeof(double), ctx->stream));
+    SVF_TRY(mlp_train_step(ctx, mlp, s, X.as<float>(), Y.as<float>(), (int)rows, lr, sgd != 0));
+    SVF_CUDA(mlp_to_bf16(mlp->w.as<float>(), kMlpParams, mlp->wbf.p, ctx->stream));
+    double l = 0.0;
+    SVF_CUDA(cudaMemcpyAsync(&l, s.loss.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    if(loss)
+        *loss = (float)l;
+    return SVF_OK;
+}
+
+svf_status svf_mlp_save(const svf_mlp* mlp, void* buf, size_t* size)
+{
+    using namespace svf;
+    if(!mlp || !size)
+        return fail(SVF_EINVAL, "null model/size");
+    const size_t need = mlp_blob_bytes(mlp->L);
+    if(!buf)
+    {
+        *size = need;
+        return SVF_OK;
+    }
+    if(*size < need)
+    {
+        *size = need;
+        return fail(SVF_EINVAL, "buffer of %zu bytes, %zu needed", *size, need);
+    }
+    *size = need;
+    SVF_CUDA(cudaSetDevice(mlp->device));
+    char* c = static_cast<char*>(buf);
+    auto put = [&](const void* src, size_t n) {
+        std::memcpy(c, src, n);
+        c += n;
+    };
+    const uint32_t hdr[2] = { mlp->L, (uint32_t)kMlpParams };
+    put(kMlpMagic, sizeof(kMlpMagic));
+    put(hdr, sizeof(hdr));
+    put(mlp->lp.data(), sizeof(float) * 2 * mlp->L);
+    put(mlp->pairs, sizeof(mlp->pairs));
+    put(mlp->xmean, sizeof(mlp->xmean));
+    put(mlp->xrstd, sizeof(mlp->xrstd));
+    put(mlp->ymean, sizeof(mlp->ymean));
+    put(mlp->ystd, sizeof(mlp->ystd));
+    // every function that changes the weights synchronises its stream before returning
+    SVF_CUDA(cudaMemcpy(c, mlp->w.p, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost));
+    return SVF_OK;
+}
+
+svf_status svf_mlp_load(svf_ctx* ctx, const void* buf, size_t size, svf_mlp** out)
+{
+    using namespace svf;
+    SVF_TRY(check_ctx(ctx));
+    if(!buf || !out)
+        return fail(SVF_EINVAL, "null buffer/output");
+    *out = nullptr;
+    const char* c = static_cast<const char*>(buf);
+    uint32_t hdr[2];
+    if(size < sizeof(kMlpMagic) + sizeof(hdr) || std::memcmp(c, kMlpMagic, sizeof(kMlpMagic)) != 0)
+        return fail(SVF_EINVAL, "not a model (bad magic)");
+    std::memcpy(hdr, c + sizeof(kMlpMagic), sizeof(hdr));
+    if(hdr[0] < 3 || hdr[0] > 160 || hdr[1] != kMlpParams || size != mlp_blob_bytes(hdr[0]))
+        return fail(SVF_EINVAL, "model header: L %u, %u parameters, %zu bytes (expected %zu parameters)", hdr[0],
+                    hdr[1], size, (size_t)kMlpParams);
+    std::unique_ptr<svf_mlp> mlp(new(std::nothrow) svf_mlp);
+    if(!mlp)
+        return fail(SVF_ENOMEM, "model allocation failed");
+    mlp->device = ctx->device;
+    mlp->L = hdr[0];
+    mlp->lp.resize(2 * (size_t)mlp->L);
+    c += sizeof(kMlpMagic) + sizeof(hdr);
+    auto get = [&](void* dst, size_t n) {
+        std::memcpy(dst, c, n);
+        c += n;
+    };
+    get(mlp->lp.data(), sizeof(float) * 2 * mlp->L);
+    get(mlp->pairs, sizeof(mlp->pairs));
+    get(mlp->xmean, sizeof(mlp->xmean));
+    get(mlp->xrstd, sizeof(mlp->xrstd));
+    get(mlp->ymean, sizeof(mlp->ymean));
+    get(mlp->ystd, sizeof(mlp->ystd));
+    for(uint32_t p : mlp->pairs)
+        if(p >= mlp->L * mlp->L)
+            return fail(SVF_EINVAL, "model pair index %u outside the %u samples", p, mlp->L * mlp->L);
+    std::vector<float> w(kMlpParams);
+    get(w.data(), sizeof(float) * kMlpParams);
+    SVF_TRY(mlp_upload(ctx, mlp.get(), w));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = mlp.release();
+    return SVF_OK;
+}
+
+void svf_mlp_destroy(svf_mlp* mlp)
+{
+    if(!mlp)
+        return;
+    cudaSetDevice(mlp->device);
+    cudaDeviceSynchronize();
+    delete mlp;
 }
 
 } // extern "C"

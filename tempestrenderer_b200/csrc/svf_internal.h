@@ -30,6 +30,7 @@ struct LmSegment
     uint64_t     stride;       // elements per slab; stride x element size % 16 == 0
     const void*  lum;          // [count][stride] slab elements (FP32 luminance, or FP16 RGB for the RGB fit), 16-byte aligned
     const float* geo;          // [3][L] direction table, SoA: x, y, z
+    float        damping;      // initial damping relative to the reference's rule (0 counts as 1)
 };
 
 // Arguments of the persistent LM kernel.
@@ -167,5 +168,41 @@ cudaError_t launch_ndf_tc(const void* a_hi, const void* a_lo, uint64_t texels, u
 // (optional): [texels][4096] NDF textures.
 cudaError_t launch_init_finish(const InitLayout& lay, const float* ndf_rows, uint32_t ldr, uint64_t texels,
                                float* init_params, float* init_info, float* ndf_out, cudaStream_t stream);
+
+// ---- learned initial guess (svf_mlp.cu) -----------------------------------------
+
+constexpr int kMlpBins = 64;                   // half-vector bins (8 x 8 over the parabolic disk)
+constexpr int kMlpPairs = 32;                  // single direction pairs per texel
+constexpr int kMlpInputs = kMlpBins + kMlpPairs;
+constexpr int kMlpHidden = 256;
+constexpr int kMlpOutputs = 8;                 // log S (6 elements), log ks, log kd
+// flat parameter vector: W1 [256][96], b1, W2 [256][256], b2, W3 [10][256], b3
+constexpr size_t kMlpW1 = 0, kMlpB1 = kMlpW1 + (size_t)kMlpHidden * kMlpInputs;
+constexpr size_t kMlpW2 = kMlpB1 + kMlpHidden, kMlpB2 = kMlpW2 + (size_t)kMlpHidden * kMlpHidden;
+constexpr size_t kMlpW3 = kMlpB2 + kMlpHidden, kMlpB3 = kMlpW3 + (size_t)kMlpOutputs * kMlpHidden;
+constexpr size_t kMlpParams = kMlpB3 + kMlpOutputs;
+
+// C[M][N] = op(A) op(B) (+ bias[n]); mode 1: Z = C (if Z), C = gelu(C); mode 2:
+// C *= gelu'(Zin).  b_bf16: B is BF16 (only with op(B) = B^T).
+cudaError_t mlp_gemm(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const void* B, bool b_bf16,
+                     int ldb, float* C, int ldc, const float* bias, int mode, float* Z, const float* Zin,
+                     cudaStream_t stream);
+cudaError_t mlp_colsum(const float* X, int M, int N, double* sum, double* sumsq, cudaStream_t stream);
+cudaError_t mlp_to_float(const double* x, int n, float scale, float* y, cudaStream_t stream);
+cudaError_t mlp_normalize(float* X, int M, int N, const float* mean, const float* rstd, cudaStream_t stream);
+cudaError_t mlp_mse_grad(const float* Y, const float* T, int M, int N, float* dY, double* loss, cudaStream_t stream);
+cudaError_t mlp_adam(float* w, const float* g, float* m, float* v, size_t n, float lr, int step, bool sgd,
+                     cudaStream_t stream);
+cudaError_t mlp_to_bf16(const float* x, size_t n, void* y, cudaStream_t stream);
+cudaError_t mlp_gather_rows(const float* X, int nx, const float* Y, int ny, const uint32_t* idx, int rows, float* Xb,
+                            float* Yb, cudaStream_t stream);
+// features [texels][96] of luminance slabs [texels][stride] (normalised when mean
+// != null): bins over order[start[b] .. start[b + 1]) scaled by bin_w[b], pairs
+cudaError_t mlp_features(const float* lum, uint64_t stride, uint64_t texels, const uint32_t* order,
+                         const uint32_t* start, const float* bin_w, const uint32_t* pairs, const float* mean,
+                         const float* rstd, float* X, cudaStream_t stream);
+cudaError_t mlp_targets(const float* p7, uint64_t texels, float* Y, cudaStream_t stream);
+cudaError_t mlp_finish(const float* Yn, uint64_t texels, const float* mean, const float* std, float* p7,
+                       cudaStream_t stream);
 
 } // namespace svf

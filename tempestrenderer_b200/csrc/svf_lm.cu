@@ -156,10 +156,12 @@ struct LmState
     double q[4], qt[4];     // RGB: orientation at p and at the trial point (xyzw)
     double S;               // sum of squared residuals at p
     double lam, nu, rho;
+    double damp_scale;      // of the initial damping (1: the reference's rule)
     uint32_t iter, eff, njac, nres, status, restarts_left;
 };
 
-// Fresh damping from the current normal equations (fitting.hh:531-538).
+// Fresh damping from the current normal equations (fitting.hh:531-538), times
+// the texel's scale (1 unless its segment asks for a lighter start).
 template <int P>
 __device__ __forceinline__ void lm_reset_damping(LmState<P>& st)
 {
@@ -167,7 +169,7 @@ __device__ __forceinline__ void lm_reset_damping(LmState<P>& st)
 #pragma unroll
     for(int i = 0; i < P; ++i)
         damping = fmax(damping, st.H[hix<P>(i, i)]);
-    st.lam = damping * 0.75;   // InitialDampingMultiplier
+    st.lam = damping * 0.75 * st.damp_scale;   // InitialDampingMultiplier
     st.nu = 2.0;               // DampingFailureMultiplier
 }
 
@@ -883,6 +885,7 @@ struct Slot
     uint32_t slab_bytes;
     double npairs;        // residuals per texel: channels x L^2
     const float* geo;
+    float damping;        // the segment's initial damping scale
 };
 
 // Dynamic shared memory per slot: [stride] slab | [Lp][kEntry] table |
@@ -1039,6 +1042,7 @@ __device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot<M>& sl, void
         sl.L = g.L;
         sl.npairs = (double)M::kChannels * (double)g.L * (double)g.L;
         sl.geo = g.geo;
+        sl.damping = g.damping > 0.0f ? g.damping : 1.0f;
         sl.slab_bytes = (uint32_t)(g.stride * sizeof(typename M::Slab));
         bulk_load(slab, static_cast<const typename M::Slab*>(g.lum) + (uint64_t)(t - g.first) * g.stride, sl.slab_bytes,
                   &sl.bar);
@@ -1098,6 +1102,7 @@ __device__ __forceinline__ bool slot_start(const LmArgs& args, Slot<M>& sl)
             st.p[i] = (double)in[i];
     st.iter = st.eff = st.njac = st.nres = st.status = 0;
     st.restarts_left = args.cfg.restarts;
+    st.damp_scale = (double)sl.damping;
     sl.first = 1;
     sl.cmd = kSlotPass;
     return true;
