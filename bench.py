@@ -177,6 +177,110 @@ def run_reference(args):
 # the GPU fitter
 # ----------------------------------------------------------------------------
 
+def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev):
+    """The learned initial guess (SVF_INIT_MLP) on the benchmark texels: train a model on
+    separately seeded synthetic texels, then fit the same texels from its prediction."""
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    model, loss = svf.Mlp.train(ctx, layout.lights_parabolic)   # 2^20 texels, 24 epochs (defaults)
+    torch.cuda.synchronize()
+    train_s = time.perf_counter() - t0
+    T = W * H
+    maps = {k: torch.zeros(s, dtype=torch.float32, device=dev) for k, s in
+            {"rmse": (T,), "params": (T, 7)}.items()}
+    opts = svf.options(max_iterations=1024)
+    run = lambda: ctx.fit_texels(layout, samples, W, H, opts=opts, want=tuple(maps), out=maps, check=False,
+                                 mlp=model)[1]
+    run()
+    st = [run() for _ in range(steps)]
+    ms = sum(r.ms_total for r in st) / steps
+    rmse = maps["rmse"].cpu().numpy()
+    ratio = rmse / np.maximum(ref_rmse, 1e-12)
+    model.close()
+    return {"value": T / (ms / 1e3), "unit": "texels/s", "ms_per_step": ms, "steps": steps,
+            "phases_ms": {"luminance": sum(r.ms_luminance for r in st) / steps,
+                          "init": sum(r.ms_init for r in st) / steps, "lm": sum(r.ms_fit for r in st) / steps},
+            "lm_work": {"jacobian_passes": st[-1].jacobians, "residual_passes": st[-1].residuals,
+                        "failed_texels": st[-1].failed_texels, "mean_iterations": st[-1].iterations / T},
+            "mean_rmse": float(rmse.mean()), "default_init_mean_rmse": float(ref_rmse.mean()),
+            "rmse_ratio_vs_default_init": {"median": float(np.median(ratio)), "within_1pct": float(np.mean(ratio <= 1.01)),
+                                           "better_1pct": float(np.mean(ratio < 0.99)), "p90": float(np.quantile(ratio, 0.9))},
+            "training": {"seconds": train_s, "final_loss": loss, "texels": 1 << 20, "epochs": 24},
+            "model": "MLP 96-256-256-8 (64 half-vector bins + 32 pairs of the luminance slab -> log S, ks, kd), "
+                     "BF16 inference; LM from its prediction with 1e-3 of the reference's initial damping"}
+
+
+def fib151_item(svf, ctx, steps, dev, side=768):
+    """768x768 texels on the 151-direction Fibonacci layout (22801 pairs), FP16 RGB samples."""
+    import torch
+
+    lp = svf.directions_fibonacci(151)
+    layout = svf.Layout(lp, *svf.triangulate(lp))
+    N = 151 * 151
+    T = side * side
+    samples = torch.empty((T, N, 3), dtype=torch.float16, device=dev)
+    ctx.synth_btf(SEED + 2, MIX, lp, 0, T, samples, sample_type=svf.SVF_SAMPLES_F16)
+    maps = {k: torch.zeros(s, dtype=torch.float32, device=dev) for k, s in
+            {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,)}.items()}
+    opts = svf.options(max_iterations=1024)
+    run = lambda: ctx.fit_texels(layout, samples, side, side, sample_type=svf.SVF_SAMPLES_F16, opts=opts,
+                                 want=tuple(maps), out=maps, check=False)[1]
+    run()
+    st = [run() for _ in range(steps)]
+    ms = sum(r.ms_total for r in st) / steps
+    ms_fit = sum(r.ms_fit for r in st) / steps
+    flops = N * (FLOPS_JACOBIAN_PASS * st[-1].jacobians + FLOPS_RESIDUAL_PASS * st[-1].residuals)
+    out = {"value": T / (ms / 1e3), "unit": "texels/s", "ms_per_step": ms, "steps": steps,
+           "workload": f"{side}x{side} texels, Fibonacci-151 layout (22801 pairs), FP16 RGB in HBM "
+                       f"({samples.numel() * 2 / 1e9:.1f} GB), mix 20% near-diffuse/10% anisotropic, default init",
+           "phases_ms": {"luminance": sum(r.ms_luminance for r in st) / steps,
+                         "init": sum(r.ms_init for r in st) / steps,
+                         "ndf_gemm": sum(r.ms_ndf for r in st) / steps, "lm": ms_fit},
+           "lm_tflops": flops / (ms_fit / 1e3) / 1e12,
+           "failed_texels": st[-1].failed_texels, "mean_rmse": float(maps["rmse"].mean().item())}
+    del samples
+    torch.cuda.empty_cache()
+    return out
+
+
+def batch_item(svf, ctx, steps, dev):
+    """Eight BTFs of uneven sizes and two layouts in one svf_fit_btfs call (FP16 RGB)."""
+    import torch
+
+    ring = ring81_mesh()
+    lp151 = svf.directions_fibonacci(151)
+    fib = svf.Layout(lp151, *svf.triangulate(lp151))
+    shapes = [(ring, 128), (ring, 256), (ring, 512), (ring, 1024), (fib, 128), (fib, 256), (fib, 384), (fib, 512)]
+    btfs = []
+    for i, (lay, side) in enumerate(shapes):
+        L = lay.light_count
+        s = torch.empty((side * side, L * L, 3), dtype=torch.float16, device=dev)
+        ctx.synth_btf(SEED + 10 + i, MIX, lay.lights_parabolic, 0, side * side, s, sample_type=svf.SVF_SAMPLES_F16)
+        btfs.append(dict(layout=lay, samples=s, width=side, height=side, sample_type=svf.SVF_SAMPLES_F16))
+    total_gb = sum(b["samples"].numel() * 2 for b in btfs) / 1e9
+    opts = svf.options(max_iterations=1024)
+    ctx.fit_btfs(btfs, opts=opts, want=("rmse",), check=False)
+    for _ in range(steps):
+        maps, runs, total = ctx.fit_btfs(btfs, opts=opts, want=("rmse", "stats"), check=False)
+    T = sum(b["width"] * b["height"] for b in btfs)
+    per = []
+    for (lay, side), m, r in zip(shapes, maps, runs):
+        it = m["stats"]["iterations"]
+        per.append({"btf": f"{side}x{side} @ {lay.light_count}", "texels": int(r.texels),
+                    "iterations_p50": float(np.percentile(it, 50)), "iterations_p99": float(np.percentile(it, 99)),
+                    "mean_rmse": float(m["rmse"].mean()), "max_rmse": float(m["rmse"].max()),
+                    "failed_texels": int(r.failed_texels)})
+    for b in btfs:
+        del b["samples"]
+    torch.cuda.empty_cache()
+    return {"value": T / (total.ms_total / 1e3), "unit": "texels/s", "ms_per_call": total.ms_total,
+            "texels": T, "samples_gb": total_gb, "per_btf": per,
+            "note": "each BTF's maps equal its own svf_fit_texels fit bit for bit (tests/test_gpu_batch.py), "
+                    "so the residual ratio to plain per-BTF LM is 1 by construction"}
+
+
 def run_ours(args):
     import torch
 
@@ -295,6 +399,23 @@ def run_ours(args):
                "d2h_bytes_per_step": d2h, "steps": args.e2e_steps}
         del host_samples
 
+    head_rmse = maps["rmse"].cpu().numpy()
+    learned = fib = batch = None
+    if world == 1 and args.mlp_steps > 0:
+        learned = learned_init_item(svf, ctx, layout, samples, W, H, head_rmse, args.mlp_steps, dev)
+    # the larger line items run in fresh contexts with the benchmark's buffers released
+    ctx.close()
+    del samples, maps
+    torch.cuda.empty_cache()
+    if world == 1 and args.fib_steps > 0:
+        with svf.Context(local) as c2:
+            fib = fib151_item(svf, c2, args.fib_steps, dev)
+        torch.cuda.empty_cache()
+    if world == 1 and args.batch_steps > 0:
+        with svf.Context(local) as c2:
+            batch = batch_item(svf, c2, args.batch_steps, dev)
+        torch.cuda.empty_cache()
+
     if rank == 0:
         props = torch.cuda.get_device_properties(dev)
         clk = clocks.summary()
@@ -346,13 +467,13 @@ def run_ours(args):
             "phases_ms": {"luminance": ms_lum / args.steps, "init": ms_init / args.steps,
                           "ndf_gemm": ms_ndf / args.steps, "lm": ms_fit / args.steps},
             "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
-                        "failed_texels": failed, "mean_rmse": float(maps["rmse"].mean().item()),
-                        "median_rmse": float(maps["rmse"].median().item())},
-            "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
+                        "failed_texels": failed, "mean_rmse": float(head_rmse.mean()),
+                        "median_rmse": float(np.median(head_rmse))},
+            "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "learned_init": learned, "fib151_768x768": fib,
+            "batch_8_btfs": batch, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
             "wall_s": wall,
         }
         print(json.dumps(line), flush=True)
-    ctx.close()
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -369,6 +490,9 @@ def main():
     ap.add_argument("--height", type=int, default=HEIGHT)
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--rgb-steps", type=int, default=2, help="steps of the RGB fit line item (0: skip)")
+    ap.add_argument("--mlp-steps", type=int, default=2, help="steps of the learned-initial-guess line item (0: skip)")
+    ap.add_argument("--fib-steps", type=int, default=1, help="steps of the 768x768 Fibonacci-151 line item (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=1, help="calls of the 8-BTF batch line item (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
