@@ -323,6 +323,48 @@ svf_status svf_mlp_save(const svf_mlp* mlp, void* buf, size_t* size);
 svf_status svf_mlp_load(svf_ctx* ctx, const void* buf, size_t size, svf_mlp** out);
 void       svf_mlp_destroy(svf_mlp* mlp);
 
+/* Factored BTF files ---------------------------------------------------------------
+ * The DFMF, FMF0 and FMF1 files LoadBTF reads (src/image/btf.cc:389-1028): the
+ * SVD planes are uploaded once and decoded on the GPU (BTFEvaluateMatrix +
+ * BTFFetchSpectrum, btf.hh:498-556,608-634), texel y*W + x after LoadBTF's row
+ * flip.  Only RGB (3-channel) files with 2-, 4- or 8-byte elements and colour
+ * model 0 or 11 are read, as BTFFetchSpectrum evaluates only those. */
+typedef struct svf_btf svf_btf;
+
+typedef struct svf_btf_info
+{
+    uint32_t format;          /* 0 DFMF, 1 FMF0, 2 FMF1 */
+    uint32_t width, height;
+    uint32_t light_count;     /* directions (views = lights) */
+    uint32_t data_size;       /* bytes per plane element: 2 (half), 4, 8 */
+    uint32_t color_model;     /* 0 or 11 (log-YUV) */
+    uint32_t dynamic_range_reduction;
+    uint32_t cosine_flag;
+    uint32_t version;         /* BTFCommonHeader::Version */
+    uint32_t components[3];   /* SVD components per channel */
+} svf_btf_info;
+
+/* Parses a file image on the host (no device, no context): SVF_EINVAL where
+ * LoadBTF rejects the file or its content is not decodable.  lights_parabolic
+ * (optional, [light_count][2], at most 160 directions) receives the directions
+ * as LoadBTF derives them (BTF::LightsParabolic). */
+svf_status svf_btf_probe(const void* file, size_t size, svf_btf_info* info, float* lights_parabolic);
+/* Parses a file image and uploads its planes to the context's device. */
+svf_status svf_btf_load(svf_ctx* ctx, const void* file, size_t size, svf_btf** out);
+svf_status svf_btf_load_file(svf_ctx* ctx, const char* path, svf_btf** out);
+svf_status svf_btf_get_info(const svf_btf* btf, svf_btf_info* info, float* lights_parabolic);
+/* RGB samples [count][L*L][3] (F32 or F16, device or host memory) of texels
+ * [first, first + count). */
+svf_status svf_btf_decode(svf_ctx* ctx, const svf_btf* btf, uint64_t first, uint64_t count, uint32_t sample_type,
+                          void* samples);
+/* svbrdffit on a loaded BTF: decodes texels chunk by chunk into device memory
+ * (FP32) and fits them as svf_fit_texels does.  mesh (optional): the
+ * interpolation mesh of the default initial guess (triangles and edges of the
+ * BTF's directions, e.g. LoadBTF's); NULL: the library's own triangulation. */
+svf_status svf_fit_btf(svf_ctx* ctx, const svf_btf* btf, const svf_layout_desc* mesh, const svf_fit_options* options,
+                       const svf_maps* maps, svf_run_stats* run);
+void       svf_btf_destroy(svf_btf* btf);
+
 /* Synthetic BTFs (test and benchmark inputs) ------------------------------------ */
 /* Renders texels [first, first + count) of a seeded synthetic BTF straight into
  * `samples` ([count][L*L][3], device memory, F32 or F16): per texel, ground-truth

@@ -97,6 +97,7 @@ def lib():
         L.svfo_synth_truth.argtypes = [C.c_uint32, C.c_uint32, C.c_uint64, C.POINTER(Truth)]
         L.svfo_synth_render.argtypes = [C.c_uint32, C.c_uint64, C.POINTER(Truth), _f32p, C.c_uint32,
                                         C.c_float, _f32p]
+        L.svfo_btf_decode.argtypes = [C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p]
         _oracle = L
     return _oracle
 
@@ -254,6 +255,114 @@ def write_dfmf(path, theta_phi, rgb_texels, width=None, height=1, data_size=4):
             u = np.ascontiguousarray(rgb_texels[:, :, c].T.astype(dt))   # [N][K]
             f.write(u.tobytes())
             f.write(eye.tobytes())                         # SxV [cols][K]
+
+
+def btf_file_bytes(theta_phi, width, height, planes, fmt="DFMF", data_size=4, color_model=0, drr=0,
+                   version=1, cosine_flag=0, xml=b"", channel_names=None, rotations=None, ext_version=1,
+                   heightmap=None, tail=b""):
+    """The bytes of a factored BTF file in the layout LoadBTF parses (src/image/btf.cc:389-1028).
+
+    planes: DFMF -- three (U [L*L][K_c], SxV [W*H][K_c]) pairs, one per channel;
+            FMF0 / FMF1 -- one (U [L*L*3][K], SxV [W*H][K]) pair, U rows interleaved by channel.
+    SxV rows are file columns: LoadBTF flips rows, so texel (x, y) reads column (H-1-y)*W + x.
+    version (BTFCommonHeader::Version) > 1 adds the cosine flag, > 2 an XML string, > 3 the
+    channel names; rotations (an [n][3][3] array) sets the 'R' marker; FMF1's ext_version >= 1
+    stores drr, >= 2 the height map ([h][w] uint16).  tail: bytes appended after the data.
+    """
+    import io
+
+    dt = {2: np.float16, 4: np.float32, 8: np.float64}[data_size]
+    tp = np.ascontiguousarray(theta_phi, np.float32)
+    L = tp.shape[0]
+    f = io.BytesIO()
+    f.write(b"!" + fmt.encode())
+    f.write({"DFMF": b"08FC", "FMF1": b"2FCE", "FMF0": b"6FC"}[fmt])
+    if rotations is not None:
+        f.write(b"R")
+    names = channel_names if channel_names is not None else [b"R", b"G", b"B"]
+    extra = b""
+    if version > 1:
+        extra += struct.pack("<I", cosine_flag)
+    if version > 2:
+        extra += struct.pack("<I", len(xml)) + xml
+    if version > 3:
+        extra += struct.pack("<I", len(names)) + b"".join(struct.pack("<I", len(n)) + n for n in names)
+    size = 264 + len(extra)
+    f.write(struct.pack("<II", size, version) + b"\0" * 240 + struct.pack("<f3f", 0.0, 1.0, 1.0, 1.0))
+    f.write(extra)
+    f.write(struct.pack("<I", L))
+    for v in range(L):
+        f.write(tp[v].tobytes())
+        f.write(struct.pack("<I", L))
+        f.write(tp.tobytes())
+    f.write(struct.pack("<II", width, height))
+    if rotations is not None:
+        rot = np.ascontiguousarray(rotations, np.float32)
+        f.write(struct.pack("<I", rot.shape[0]) + rot.tobytes())
+    if fmt == "DFMF":
+        f.write(struct.pack("<II", planes[0][0].shape[1], color_model))
+        f.write(struct.pack("<3f", 0.0, 0.0, 0.0))
+        f.write(np.eye(3, dtype=np.float32).tobytes())
+        for U, S in planes:
+            K = U.shape[1]
+            f.write(struct.pack("<B", data_size))
+            f.write(struct.pack("<III", K, U.shape[0], S.shape[0]))
+            f.write(np.ones(K, dt).tobytes())
+            f.write(np.ascontiguousarray(U, dt).tobytes())
+            f.write(np.ascontiguousarray(S, dt).tobytes())
+    else:
+        if fmt == "FMF1":
+            f.write(struct.pack("<B", ext_version))
+            if ext_version >= 1:
+                f.write(struct.pack("<I", drr))
+            if ext_version >= 2:
+                hm = np.zeros((0, 0), np.uint16) if heightmap is None else np.ascontiguousarray(heightmap, np.uint16)
+                f.write(struct.pack("<II", hm.shape[1], hm.shape[0]) + hm.tobytes())
+        U, S = planes
+        K = U.shape[1]
+        f.write(struct.pack("<I", K) + struct.pack("<B", data_size) + struct.pack("<I", K))
+        f.write(struct.pack("<II", U.shape[0], S.shape[0]))
+        f.write(np.ones(K, dt).tobytes())
+        f.write(np.ascontiguousarray(U, dt).tobytes())
+        f.write(np.ascontiguousarray(S, dt).tobytes())
+    f.write(tail)
+    return f.getvalue()
+
+
+class BtfPlanes(C.Structure):
+    _fields_ = [("data_size", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("light_count", C.c_uint32), ("color_model", C.c_uint32), ("drr", C.c_uint32),
+                ("u", C.c_void_p * 3), ("sxv", C.c_void_p * 3), ("k", C.c_uint32 * 3),
+                ("u_row", C.c_uint64 * 3), ("sxv_row", C.c_uint64 * 3)]
+
+
+def btf_decode(planes, fmt, width, height, light_count, data_size, color_model=0, drr=0, first=0, count=None):
+    """The oracle's BTFFetchSpectrum over texels [first, first + count): [count][L*L][3] float32."""
+    dt = {2: np.float16, 4: np.float32, 8: np.float64}[data_size]
+    p = BtfPlanes()
+    p.data_size, p.width, p.height, p.light_count = data_size, width, height, light_count
+    p.color_model, p.drr = color_model, drr
+    keep = []
+    if fmt == "DFMF":
+        for c, (U, S) in enumerate(planes):
+            U = np.ascontiguousarray(U, dt)
+            S = np.ascontiguousarray(S, dt)
+            keep += [U, S]
+            p.u[c], p.sxv[c], p.k[c] = U.ctypes.data, S.ctypes.data, U.shape[1]
+            p.u_row[c], p.sxv_row[c] = U.shape[1], S.shape[1]
+    else:
+        U = np.ascontiguousarray(planes[0], dt)
+        S = np.ascontiguousarray(planes[1], dt)
+        keep += [U, S]
+        K = U.shape[1]
+        for c in range(3):
+            p.u[c] = U.ctypes.data + c * K * data_size
+            p.sxv[c], p.k[c] = S.ctypes.data, K
+            p.u_row[c], p.sxv_row[c] = 3 * K, K
+    count = width * height - first if count is None else count
+    out = np.zeros((count, light_count * light_count, 3), np.float32)
+    lib().svfo_btf_decode(C.byref(p), first, count, out.ctypes.data)
+    return out
 
 
 # ----------------------------------------------------------------------------

@@ -1105,3 +1105,100 @@ void svfo_synth_render(uint32_t seed, uint64_t texel, const svfo_texel_truth* t,
         }
     }
 }
+
+/* ---------------------------------------------------------------------------
+ * Factored BTF decode
+ * ------------------------------------------------------------------------- */
+
+/* IEEE binary16 -> float (exact) */
+static float half_to_float(uint16_t h)
+{
+    uint32_t sign = (uint32_t)(h >> 15) << 31, e = (h >> 10) & 0x1f, m = h & 0x3ff, bits;
+    if(e == 0)
+    {
+        if(m == 0)
+            bits = sign;
+        else
+        {
+            /* subnormal: m * 2^-24 */
+            float f = (float)m * (1.0f / 16777216.0f);
+            return sign ? -f : f;
+        }
+    }
+    else if(e == 31)
+        bits = sign | 0x7f800000u | (m << 13);
+    else
+        bits = sign | ((e + 112u) << 23) | (m << 13);
+    float f;
+    memcpy(&f, &bits, 4);
+    return f;
+}
+
+static double plane_elem(const void* base, uint32_t data_size, uint64_t i)
+{
+    switch(data_size)
+    {
+    case 2: return half_to_float(((const uint16_t*)base)[i]);
+    case 4: return ((const float*)base)[i];
+    default: return ((const double*)base)[i];
+    }
+}
+
+void svfo_btf_decode(const svfo_btf_planes* p, uint64_t first, uint64_t count, float* out)
+{
+    const uint32_t L = p->light_count, N = L * L, W = p->width, H = p->height;
+    const float drr_eps = 1e-5f;
+    for(uint64_t t = first; t < first + count; ++t)
+    {
+        const uint64_t y = t / W, x = t % W, col = (H - 1 - y) * (uint64_t)W + x;
+        for(uint32_t lv = 0; lv < N; ++lv)
+        {
+            float c[3];
+            for(int ch = 0; ch < 3; ++ch)
+            {
+                /* BTFEvaluateMatrix<T, TOp>: TOp sum{}; sum += u*v (btf.hh:627-632) */
+                if(p->data_size == 8)
+                {
+                    double sum = 0.0;
+                    for(uint32_t k = 0; k < p->k[ch]; ++k)
+                        sum += plane_elem(p->u[ch], 8, lv * p->u_row[ch] + k) *
+                               plane_elem(p->sxv[ch], 8, col * p->sxv_row[ch] + k);
+                    c[ch] = (float)sum;
+                }
+                else
+                {
+                    float sum = 0.0f;
+                    for(uint32_t k = 0; k < p->k[ch]; ++k)
+                    {
+                        float u = (float)plane_elem(p->u[ch], p->data_size, lv * p->u_row[ch] + k);
+                        float v = (float)plane_elem(p->sxv[ch], p->data_size, col * p->sxv_row[ch] + k);
+                        float uv = u * v;
+                        sum += uv;
+                    }
+                    c[ch] = sum;
+                }
+            }
+            if(p->color_model == 11)
+            {
+                /* btf.hh:522-531, YUVToRGB spectrum.hh:344-350 */
+                float Y = expf(c[0]) - drr_eps;
+                float U = c[1] * Y + drr_eps;
+                float V = c[2] * Y + drr_eps;
+                float r = Y * 1.0f + U * 0.0f + V * 1.13983f;
+                float g = Y * 1.0f + U * -0.39465f + V * -0.5806f;
+                float b = Y * 1.0f + U * 2.03211f + V * 0.0f;
+                /* Vector3Clamp -> Clamp (functions.hh:156-159) */
+                c[0] = r <= 0.0f ? 0.0f : (r >= 1.0f ? 1.0f : r);
+                c[1] = g <= 0.0f ? 0.0f : (g >= 1.0f ? 1.0f : g);
+                c[2] = b <= 0.0f ? 0.0f : (b >= 1.0f ? 1.0f : b);
+            }
+            if(p->drr)
+                for(int ch = 0; ch < 3; ++ch)
+                    c[ch] = expf(c[ch]) - drr_eps;
+            float* o = out + ((t - first) * N + lv) * 3;
+            o[0] = c[0];
+            o[1] = c[1];
+            o[2] = c[2];
+        }
+    }
+}

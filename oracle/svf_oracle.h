@@ -136,6 +136,33 @@ void svfo_synth_truth(uint32_t seed, uint32_t mix, uint64_t texel, svfo_texel_tr
 void svfo_synth_render(uint32_t seed, uint64_t texel, const svfo_texel_truth* truth,
                        const float* lights_parabolic, uint32_t light_count, float noise, float* rgb);
 
+/* ---- factored BTF decode (BTFEvaluateMatrix btf.hh:608-634 + BTFFetchSpectrum
+ * btf.hh:498-556) ---------------------------------------------------------- */
+
+/* The planes of a factored BTF as LoadBTF leaves them (btf.cc:660-1022):
+ * channel c's sample is sum_k U_c[lv][k] * SxV_c[col][k] with U_c row lv at
+ * u[c] + lv * u_row[c] elements and SxV_c row col at sxv[c] + col * sxv_row[c]
+ * (DFMF: one plane pair per channel; FMF: U rows interleaved by channel and one
+ * shared SxV).  col is the file column of texel (x, y): LoadBTF flips rows, so
+ * texel y*W + x reads column (H - 1 - y)*W + x. */
+typedef struct svfo_btf_planes
+{
+    uint32_t data_size;              /* 2 (IEEE half), 4 (float) or 8 (double) */
+    uint32_t width, height, light_count;
+    uint32_t color_model;            /* 0 or 11 (log-YUV) */
+    uint32_t drr;                    /* DynamicRangeReduction: exp(x) - 1e-5 */
+    const void* u[3];
+    const void* sxv[3];
+    uint32_t k[3];
+    uint64_t u_row[3], sxv_row[3];   /* row strides in elements */
+} svfo_btf_planes;
+
+/* RGB samples [count][L*L][3] of texels [first, first + count) (texel index
+ * y*W + x, after the flip), each exactly as BTFFetchSpectrum computes it on the
+ * CPU: a sequential sum in the data type's accumulator (float for half and
+ * float, double for double), then the colour model and DRR with libm expf. */
+void svfo_btf_decode(const svfo_btf_planes* p, uint64_t first, uint64_t count, float* out);
+
 #ifdef __cplusplus
 }
 #endif

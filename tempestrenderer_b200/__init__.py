@@ -35,7 +35,8 @@ EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_op
            "svf_destroy", "svf_directions_ring81", "svf_directions_fibonacci", "svf_layout_triangulate",
            "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc", "svf_fit_texels", "svf_fit_btfs",
            "svf_synth_btf", "svf_mlp_train_options_default", "svf_mlp_train", "svf_mlp_predict", "svf_mlp_step",
-           "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy")
+           "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy", "svf_btf_probe", "svf_btf_load", "svf_btf_load_file",
+           "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_btf_destroy")
 
 
 class SvfError(RuntimeError):
@@ -72,6 +73,12 @@ class BtfView(C.Structure):
 class FitOptions(C.Structure):
     _fields_ = [("lsq", LsqOptions), ("init_mode", C.c_uint32), ("init_params", C.c_void_p), ("mlp", C.c_void_p),
                 ("initial_damping", C.c_float)]
+
+
+class BtfInfo(C.Structure):
+    _fields_ = [("format", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("light_count", C.c_uint32),
+                ("data_size", C.c_uint32), ("color_model", C.c_uint32), ("dynamic_range_reduction", C.c_uint32),
+                ("cosine_flag", C.c_uint32), ("version", C.c_uint32), ("components", C.c_uint32 * 3)]
 
 
 class MlpTrainOptions(C.Structure):
@@ -134,9 +141,18 @@ def load() -> C.CDLL:
         L.svf_mlp_load.argtypes = [vp, vp, C.c_size_t, C.POINTER(vp)]
         L.svf_mlp_destroy.argtypes = [vp]
         L.svf_mlp_destroy.restype = None
+        L.svf_btf_probe.argtypes = [vp, C.c_size_t, C.POINTER(BtfInfo), vp]
+        L.svf_btf_load.argtypes = [vp, vp, C.c_size_t, C.POINTER(vp)]
+        L.svf_btf_load_file.argtypes = [vp, C.c_char_p, C.POINTER(vp)]
+        L.svf_btf_get_info.argtypes = [vp, C.POINTER(BtfInfo), vp]
+        L.svf_btf_decode.argtypes = [vp, vp, u64, u64, u32, vp]
+        L.svf_fit_btf.argtypes = [vp, vp, vp, C.POINTER(FitOptions), C.POINTER(Maps), C.POINTER(RunStats)]
+        L.svf_btf_destroy.argtypes = [vp]
+        L.svf_btf_destroy.restype = None
         for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
                      "svf_fit_texels", "svf_fit_btfs", "svf_synth_btf", "svf_mlp_train", "svf_mlp_predict",
-                     "svf_mlp_step", "svf_mlp_save", "svf_mlp_load"):
+                     "svf_mlp_step", "svf_mlp_save", "svf_mlp_load", "svf_btf_probe", "svf_btf_load",
+                     "svf_btf_load_file", "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -416,6 +432,78 @@ class Mlp:
     def close(self):
         if getattr(self, "handle", None):
             self._lib.svf_mlp_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        self.close()
+
+
+def btf_probe(data: bytes):
+    """Parses a DFMF / FMF file image on the host: (BtfInfo, lights_parabolic [L][2])."""
+    info = BtfInfo()
+    lp = np.zeros((160, 2), np.float32)
+    buf = C.create_string_buffer(bytes(data), len(data))
+    _check(load().svf_btf_probe(buf, len(data), C.byref(info), lp.ctypes.data))
+    return info, lp[:info.light_count].copy()
+
+
+class Btf:
+    """A factored BTF file loaded onto a context's device (svf_btf_*)."""
+
+    def __init__(self, ctx: Context, data: bytes | None = None, path: str | None = None):
+        self._lib, self.ctx = load(), ctx
+        h = C.c_void_p()
+        if path is not None:
+            _check(self._lib.svf_btf_load_file(ctx.handle, path.encode(), C.byref(h)))
+        else:
+            buf = C.create_string_buffer(bytes(data), len(data))
+            _check(self._lib.svf_btf_load(ctx.handle, buf, len(data), C.byref(h)))
+        self.handle = h
+        self.info = BtfInfo()
+        lp = np.zeros((160, 2), np.float32)
+        _check(self._lib.svf_btf_get_info(h, C.byref(self.info), lp.ctypes.data))
+        self.lights_parabolic = lp[:self.info.light_count].copy()
+
+    @property
+    def texels(self) -> int:
+        return self.info.width * self.info.height
+
+    def decode(self, first: int = 0, count: int | None = None, sample_type=SVF_SAMPLES_F32, out=None):
+        """RGB samples [count][L*L][3] (numpy on the host unless `out` is given)."""
+        count = self.texels - first if count is None else count
+        N = self.info.light_count ** 2
+        if out is None:
+            out = np.zeros((count, N, 3), np.float16 if sample_type == SVF_SAMPLES_F16 else np.float32)
+        _check(self._lib.svf_btf_decode(self.ctx.handle, self.handle, first, count, sample_type, _ptr(out)))
+        return out
+
+    def fit(self, layout: "Layout | None" = None, opts: LsqOptions | None = None, init=None, mlp=None,
+            want=("diffuse", "specular", "sigma", "basis", "rmse", "params", "init", "stats"), check=True):
+        """svf_fit_btf: layout (optional) supplies the default guess's interpolation mesh."""
+        T = self.texels
+        fo = FitOptions()
+        fo.lsq = opts or options()
+        fo.init_mode = SVF_INIT_DEFAULT if init is None else SVF_INIT_GIVEN
+        fo.init_params = _ptr(init) if init is not None else None
+        if mlp is not None:
+            fo.init_mode, fo.mlp = SVF_INIT_MLP, mlp.handle
+        kout = 12 if fo.lsq.flags & SVF_LSQ_RGB else 7
+        shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
+                  "params": (T, kout), "init": (T, kout), "ndf": (T, 64 * 64)}
+        res = {k: (np.zeros(T, STATS_DTYPE) if k == "stats" else np.zeros(shapes[k], np.float32)) for k in want}
+        m = Maps()
+        for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params", "init", "stats", "ndf"):
+            setattr(m, k, _ptr(res[k]) if k in res else None)
+        rs = RunStats()
+        mesh = C.pointer(layout.desc) if layout is not None else None
+        st = self._lib.svf_fit_btf(self.ctx.handle, self.handle, mesh, C.byref(fo), C.byref(m), C.byref(rs))
+        if check:
+            _check(st)
+        return res, rs
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self._lib.svf_btf_destroy(self.handle)
             self.handle = None
 
     def __del__(self):

@@ -1,0 +1,184 @@
+// svf_btf.cu - decode of a factored BTF (DFMF / FMF planes resident in HBM)
+// into RGB samples [texels][L*L][3], texel-major, as svf_fit_texels reads them.
+//
+// Reference: BTFEvaluateMatrix (include/tempest/image/btf.hh:608-634) and
+// BTFFetchSpectrum (btf.hh:498-556).  Channel c of sample (lv, texel) is
+// sum_k U_c[lv][k] * SxV_c[col][k], summed in order k = 0, 1, ... in the
+// accumulator type of the plane elements (float for half and float planes,
+// double for double planes) with every product rounded before it is added, as
+// the reference's x86-64 build evaluates it; then colour model 11 (log-YUV ->
+// RGB) and the dynamic range reduction exp(x) - 1e-5.  col is the file column
+// of texel y*W + x: LoadBTF flips rows (btf.cc:1000-1022), so it is
+// (H - 1 - y)*W + x.
+//
+// The sums are bit-identical to the reference's; with colour model 11 or DRR
+// the exponentials are CUDA's expf (within 2 ulp of libm's), so those samples
+// agree to a few ulp.
+//
+// Work split: a CTA of 128 threads owns 128 consecutive pairs lv (one per
+// thread) and TX texels; the texels' SxV rows go through shared memory in
+// chunks of 32 components (transposed, so a thread reads TX of them with
+// vector broadcasts); each thread streams its own U row.  Writes: a warp stores
+// 32 consecutive pairs x 3 channels of one texel at a time (384 contiguous
+// bytes in FP32).  Bound by the FP32 pipe for K >= ~20 components (2 flops per
+// component per channel per sample), by the HBM write otherwise.
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "svf_internal.h"
+
+namespace svf
+{
+
+namespace
+{
+
+constexpr int kThreads = 128, kChunk = 32;
+
+__device__ __forceinline__ float elem(const __half* p, uint64_t i) { return __half2float(p[i]); }
+__device__ __forceinline__ float elem(const float* p, uint64_t i) { return p[i]; }
+__device__ __forceinline__ double elem(const double* p, uint64_t i) { return p[i]; }
+
+// sum + u * v with the product rounded first (no contraction into an FMA,
+// which would round once); for half elements the product is exact in float and
+// an FMA gives the same result.
+__device__ __forceinline__ float madd(float sum, float u, float v) { return __fadd_rn(sum, __fmul_rn(u, v)); }
+__device__ __forceinline__ double madd(double sum, double u, double v) { return __dadd_rn(sum, __dmul_rn(u, v)); }
+
+template <typename T, typename Acc, int TX>
+__global__ void __launch_bounds__(kThreads) btf_decode_kernel(BtfDecodeArgs a, uint64_t t_begin)
+{
+    __shared__ Acc s_sxv[kChunk][TX];
+    const uint32_t lv = blockIdx.x * kThreads + threadIdx.x;
+    const uint64_t t0 = t_begin + (uint64_t)blockIdx.y * TX;
+    const uint64_t t_end = a.first + a.count;
+    Acc acc[3][TX];
+#pragma unroll
+    for(int c = 0; c < 3; ++c)
+#pragma unroll
+        for(int j = 0; j < TX; ++j)
+            acc[c][j] = Acc(0);
+
+#pragma unroll
+    for(int c = 0; c < 3; ++c)
+    {
+        const T* U = static_cast<const T*>(a.u[c]);
+        const T* S = static_cast<const T*>(a.sxv[c]);
+        const uint32_t K = a.k[c];
+        const T* urow = U + (uint64_t)(lv < a.N ? lv : 0) * a.u_row[c];
+        for(uint32_t k0 = 0; k0 < K; k0 += kChunk)
+        {
+            __syncthreads();
+            for(int i = threadIdx.x; i < TX * kChunk; i += kThreads)
+            {
+                const int j = i / kChunk, kk = i % kChunk;
+                const uint64_t t = t0 + j;
+                Acc v = Acc(0);
+                if(t < t_end && k0 + kk < K)
+                {
+                    const uint64_t y = t / a.width, x = t - y * a.width;
+                    const uint64_t col = (a.height - 1 - y) * a.width + x;
+                    v = elem(S, col * a.sxv_row[c] + k0 + kk);
+                }
+                s_sxv[kk][j] = v;
+            }
+            __syncthreads();
+            if(lv < a.N)
+            {
+                const uint32_t n = K - k0 < (uint32_t)kChunk ? K - k0 : (uint32_t)kChunk;
+                for(uint32_t kk = 0; kk < n; ++kk)
+                {
+                    const Acc u = elem(urow, k0 + kk);
+#pragma unroll
+                    for(int j = 0; j < TX; ++j)
+                        acc[c][j] = madd(acc[c][j], u, s_sxv[kk][j]);
+                }
+            }
+        }
+    }
+    if(lv >= a.N)
+        return;
+    const float eps = 1e-5f;
+#pragma unroll
+    for(int j = 0; j < TX; ++j)
+    {
+        const uint64_t t = t0 + j;
+        if(t >= t_end)
+            break;
+        float r = (float)acc[0][j], g = (float)acc[1][j], b = (float)acc[2][j];
+        if(a.color_model == 11)
+        {
+            // btf.hh:522-531 and YUVToRGB (spectrum.hh:344-350): dot products
+            // with the conversion's columns, left to right, then a clamp to [0, 1]
+            const float Y = __fsub_rn(expf(r), eps);
+            const float U = __fadd_rn(__fmul_rn(g, Y), eps);
+            const float V = __fadd_rn(__fmul_rn(b, Y), eps);
+            float o[3];
+            o[0] = __fadd_rn(__fadd_rn(__fmul_rn(Y, 1.0f), __fmul_rn(U, 0.0f)), __fmul_rn(V, 1.13983f));
+            o[1] = __fadd_rn(__fadd_rn(__fmul_rn(Y, 1.0f), __fmul_rn(U, -0.39465f)), __fmul_rn(V, -0.5806f));
+            o[2] = __fadd_rn(__fadd_rn(__fmul_rn(Y, 1.0f), __fmul_rn(U, 2.03211f)), __fmul_rn(V, 0.0f));
+            // Clamp (functions.hh:156-159)
+#pragma unroll
+            for(int i = 0; i < 3; ++i)
+                o[i] = o[i] <= 0.0f ? 0.0f : (o[i] >= 1.0f ? 1.0f : o[i]);
+            r = o[0];
+            g = o[1];
+            b = o[2];
+        }
+        if(a.drr)
+        {
+            r = __fsub_rn(expf(r), eps);
+            g = __fsub_rn(expf(g), eps);
+            b = __fsub_rn(expf(b), eps);
+        }
+        const uint64_t o = ((t - a.first) * a.N + lv) * 3;
+        if(a.out_type == SVF_SAMPLES_F16)
+        {
+            __half* out = static_cast<__half*>(a.out) + o;
+            out[0] = __float2half_rn(r);
+            out[1] = __float2half_rn(g);
+            out[2] = __float2half_rn(b);
+        }
+        else
+        {
+            float* out = static_cast<float*>(a.out) + o;
+            out[0] = r;
+            out[1] = g;
+            out[2] = b;
+        }
+    }
+}
+
+template <typename T, typename Acc, int TX>
+cudaError_t launch_typed(const BtfDecodeArgs& a, cudaStream_t stream)
+{
+    const uint64_t per_launch = 65535ull * TX;   // grid.y limit
+    for(uint64_t t = a.first; t < a.first + a.count; t += per_launch)
+    {
+        const uint64_t n = a.first + a.count - t < per_launch ? a.first + a.count - t : per_launch;
+        dim3 grid((a.N + kThreads - 1) / kThreads, (unsigned)((n + TX - 1) / TX));
+        btf_decode_kernel<T, Acc, TX><<<grid, kThreads, 0, stream>>>(a, t);
+        const cudaError_t e = cudaGetLastError();
+        if(e != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
+} // namespace
+
+cudaError_t launch_btf_decode(const BtfDecodeArgs& a, cudaStream_t stream)
+{
+    if(a.count == 0)
+        return cudaSuccess;
+    switch(a.data_size)
+    {
+    case 2: return launch_typed<__half, float, 16>(a, stream);
+    case 4: return launch_typed<float, float, 16>(a, stream);
+    case 8: return launch_typed<double, double, 8>(a, stream);
+    default: return cudaErrorInvalidValue;
+    }
+}
+
+} // namespace svf

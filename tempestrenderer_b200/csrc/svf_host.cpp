@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <map>
 #include <memory>
 #include <new>
@@ -24,6 +25,7 @@
 
 #include "../../include/svf.h"
 #include "svf_internal.h"
+#include "svf_btf_file.h"
 #include "svf_layout.h"
 
 namespace
@@ -2319,6 +2321,288 @@ void svf_mlp_destroy(svf_mlp* mlp)
     cudaSetDevice(mlp->device);
     cudaDeviceSynchronize();
     delete mlp;
+}
+
+} // extern "C"
+
+// ---- factored BTF files -------------------------------------------------------------
+
+// A factored BTF resident on one device: its planes (DFMF: the three channels'
+// U planes back to back, then the SxV planes; FMF: the channel-interleaved U
+// and the shared SxV) and the parsed header.
+struct svf_btf
+{
+    int device = 0;
+    svf::BtfFile f;
+    DevBuf u, sxv;
+    const void* u_ptr[3] = {};
+    const void* sxv_ptr[3] = {};
+};
+
+namespace
+{
+
+void btf_info(const svf::BtfFile& f, svf_btf_info* info, float* lp)
+{
+    if(info)
+    {
+        *info = svf_btf_info{};
+        info->format = f.format;
+        info->width = f.width;
+        info->height = f.height;
+        info->light_count = f.light_count;
+        info->data_size = f.data_size;
+        info->color_model = f.color_model;
+        info->dynamic_range_reduction = f.drr;
+        info->cosine_flag = f.cosine_flag;
+        info->version = f.version;
+        for(int c = 0; c < 3; ++c)
+            info->components[c] = f.k[c];
+    }
+    if(lp)
+        std::memcpy(lp, f.lights_parabolic.data(), sizeof(float) * f.lights_parabolic.size());
+}
+
+svf::BtfDecodeArgs btf_args(const svf_btf* b, uint64_t first, uint64_t count, uint32_t type, void* out)
+{
+    svf::BtfDecodeArgs a{};
+    for(int c = 0; c < 3; ++c)
+    {
+        a.u[c] = b->u_ptr[c];
+        a.sxv[c] = b->sxv_ptr[c];
+        a.k[c] = b->f.k[c];
+        a.u_row[c] = b->f.u_row[c];
+        a.sxv_row[c] = b->f.sxv_row[c];
+    }
+    a.data_size = b->f.data_size;
+    a.color_model = b->f.color_model;
+    a.drr = b->f.drr;
+    a.width = b->f.width;
+    a.height = b->f.height;
+    a.N = b->f.light_count * b->f.light_count;
+    a.first = first;
+    a.count = count;
+    a.out_type = type;
+    a.out = out;
+    return a;
+}
+
+svf_status check_btf(svf_ctx* ctx, const svf_btf* btf)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(!btf)
+        return fail(SVF_EINVAL, "null BTF");
+    if(btf->device != ctx->device)
+        return fail(SVF_EINVAL, "the BTF lives on device %d, the context on %d", btf->device, ctx->device);
+    return SVF_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+svf_status svf_btf_probe(const void* file, size_t size, svf_btf_info* info, float* lights_parabolic)
+{
+    if(!file)
+        return fail(SVF_EINVAL, "null file image");
+    svf::BtfFile f;
+    char err[256];
+    if(!svf::parse_btf(static_cast<const uint8_t*>(file), size, f, err, sizeof(err)))
+        return fail(SVF_EINVAL, "%s", err);
+    btf_info(f, info, lights_parabolic);
+    return SVF_OK;
+}
+
+svf_status svf_btf_load(svf_ctx* ctx, const void* file, size_t size, svf_btf** out)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(!file || !out)
+        return fail(SVF_EINVAL, "null file image/output");
+    *out = nullptr;
+    std::unique_ptr<svf_btf> b(new(std::nothrow) svf_btf);
+    if(!b)
+        return fail(SVF_ENOMEM, "BTF allocation failed");
+    char err[256];
+    if(!svf::parse_btf(static_cast<const uint8_t*>(file), size, b->f, err, sizeof(err)))
+        return fail(SVF_EINVAL, "%s", err);
+    b->device = ctx->device;
+    const svf::BtfFile& f = b->f;
+    const char* src = static_cast<const char*>(file);
+    if(f.format == 0)
+    {
+        // three plane pairs, each copied to its place in one allocation
+        uint64_t ub = 0, sb = 0;
+        for(int c = 0; c < 3; ++c)
+        {
+            ub += round_up(f.u_bytes[c], 256);
+            sb += round_up(f.sxv_bytes[c], 256);
+        }
+        SVF_TRY(b->u.ensure(ub));
+        SVF_TRY(b->sxv.ensure(sb));
+        uint64_t uo = 0, so = 0;
+        for(int c = 0; c < 3; ++c)
+        {
+            char* ud = b->u.as<char>() + uo;
+            char* sd = b->sxv.as<char>() + so;
+            SVF_CUDA(cudaMemcpyAsync(ud, src + f.u_off[c], f.u_bytes[c], cudaMemcpyHostToDevice, ctx->stream));
+            SVF_CUDA(cudaMemcpyAsync(sd, src + f.sxv_off[c], f.sxv_bytes[c], cudaMemcpyHostToDevice, ctx->stream));
+            b->u_ptr[c] = ud;
+            b->sxv_ptr[c] = sd;
+            uo += round_up(f.u_bytes[c], 256);
+            so += round_up(f.sxv_bytes[c], 256);
+        }
+    }
+    else
+    {
+        SVF_TRY(b->u.ensure(f.u_bytes[0]));
+        SVF_TRY(b->sxv.ensure(f.sxv_bytes[0]));
+        SVF_CUDA(cudaMemcpyAsync(b->u.p, src + f.u_off[0], f.u_bytes[0], cudaMemcpyHostToDevice, ctx->stream));
+        SVF_CUDA(cudaMemcpyAsync(b->sxv.p, src + f.sxv_off[0], f.sxv_bytes[0], cudaMemcpyHostToDevice,
+                                 ctx->stream));
+        for(int c = 0; c < 3; ++c)
+        {
+            b->u_ptr[c] = b->u.as<char>() + (f.u_off[c] - f.u_off[0]);
+            b->sxv_ptr[c] = b->sxv.p;
+        }
+    }
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    *out = b.release();
+    return SVF_OK;
+}
+
+svf_status svf_btf_load_file(svf_ctx* ctx, const char* path, svf_btf** out)
+{
+    if(!path)
+        return fail(SVF_EINVAL, "null path");
+    std::ifstream fs(path, std::ios::binary);
+    if(!fs)
+        return fail(SVF_EINVAL, "failed to open BTF file %s", path);
+    std::vector<char> data((std::istreambuf_iterator<char>(fs)), std::istreambuf_iterator<char>());
+    if(!fs.good() && !fs.eof())
+        return fail(SVF_EINVAL, "failed to read BTF file %s", path);
+    return svf_btf_load(ctx, data.data(), data.size(), out);
+}
+
+svf_status svf_btf_get_info(const svf_btf* btf, svf_btf_info* info, float* lights_parabolic)
+{
+    if(!btf)
+        return fail(SVF_EINVAL, "null BTF");
+    btf_info(btf->f, info, lights_parabolic);
+    return SVF_OK;
+}
+
+svf_status svf_btf_decode(svf_ctx* ctx, const svf_btf* btf, uint64_t first, uint64_t count, uint32_t sample_type,
+                          void* samples)
+{
+    SVF_TRY(check_btf(ctx, btf));
+    const uint64_t T = (uint64_t)btf->f.width * btf->f.height;
+    if(!samples || first > T || count > T - first)
+        return fail(SVF_EINVAL, "null samples or texels [%llu, %llu) outside the BTF's %llu",
+                    (unsigned long long)first, (unsigned long long)(first + count), (unsigned long long)T);
+    if(sample_type != SVF_SAMPLES_F32 && sample_type != SVF_SAMPLES_F16)
+        return fail(SVF_EINVAL, "unknown sample_type %u", sample_type);
+    if(count == 0)
+        return SVF_OK;
+    const uint64_t N = (uint64_t)btf->f.light_count * btf->f.light_count;
+    const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * N;
+    if(is_device_pointer(samples))
+    {
+        SVF_CUDA(svf::launch_btf_decode(btf_args(btf, first, count, sample_type, samples), ctx->stream));
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+        return SVF_OK;
+    }
+    // host output: decode chunks on the device and copy them out
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(count, (size_t(1) << 30) / texel_bytes));
+    DevBuf buf;
+    SVF_TRY(buf.ensure(texel_bytes * chunk));
+    for(uint64_t c0 = 0; c0 < count; c0 += chunk)
+    {
+        const uint64_t n = std::min(chunk, count - c0);
+        SVF_CUDA(svf::launch_btf_decode(btf_args(btf, first + c0, n, sample_type, buf.p), ctx->stream));
+        SVF_CUDA(cudaMemcpyAsync(static_cast<char*>(samples) + c0 * texel_bytes, buf.p, texel_bytes * n,
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return SVF_OK;
+}
+
+svf_status svf_fit_btf(svf_ctx* ctx, const svf_btf* btf, const svf_layout_desc* mesh, const svf_fit_options* opts,
+                       const svf_maps* maps, svf_run_stats* run)
+{
+    SVF_TRY(check_btf(ctx, btf));
+    if(!opts || !maps)
+        return fail(SVF_EINVAL, "null options/maps");
+    const svf::BtfFile& f = btf->f;
+    const uint32_t L = f.light_count;
+    svf_layout_desc desc{ f.lights_parabolic.data(), L, nullptr, 0, nullptr, nullptr, 0 };
+    if(mesh)
+    {
+        if(mesh->light_count != L)
+            return fail(SVF_EINVAL, "the mesh has %u directions, the BTF %u", mesh->light_count, L);
+        desc.triangles = mesh->triangles;
+        desc.triangle_count = mesh->triangle_count;
+        desc.edges = mesh->edges;
+        desc.edge_angles = mesh->edge_angles;
+        desc.edge_count = mesh->edge_count;
+    }
+    const uint64_t T = (uint64_t)f.width * f.height, N = (uint64_t)L * L;
+    const size_t texel_bytes = sizeof(float) * 3 * N;
+    size_t free_b = 0, total_b = 0;
+    SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    // the decoded chunk takes a quarter of the free memory; the fit's own
+    // buffers grow within the rest
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(T, free_b / 4 / texel_bytes));
+    DevBuf buf;
+    SVF_TRY(buf.ensure(texel_bytes * chunk));
+    const uint32_t kout = (opts->lsq.flags & SVF_LSQ_RGB) ? 12 : 7;
+    svf_run_stats all{};
+    bool partial = false;
+    for(uint64_t c0 = 0; c0 < T; c0 += chunk)
+    {
+        const uint64_t n = std::min(chunk, T - c0);
+        SVF_CUDA(svf::launch_btf_decode(btf_args(btf, c0, n, SVF_SAMPLES_F32, buf.p), ctx->stream));
+        const svf_btf_view v{ buf.p, SVF_SAMPLES_F32, (uint32_t)n, 1, &desc };
+        svf_fit_options o = *opts;
+        if(o.init_params)
+            o.init_params += kout * c0;
+        auto off = [&](float* p, uint64_t k) { return p ? p + k * c0 : nullptr; };
+        svf_maps m{ off(maps->diffuse, 3), off(maps->specular, 3), off(maps->sigma, 2), off(maps->basis, 4),
+                    off(maps->rmse, 1), off(maps->params, kout), off(maps->init, kout),
+                    maps->stats ? maps->stats + c0 : nullptr, off(maps->ndf, svf::kNdfTexels) };
+        svf_run_stats rs{};
+        const svf_status st = svf_fit_texels(ctx, &v, &o, &m, &rs);
+        if(st == SVF_EPARTIAL)
+            partial = true;
+        else if(st != SVF_OK)
+            return st;
+        all.texels += rs.texels;
+        all.iterations += rs.iterations;
+        all.jacobians += rs.jacobians;
+        all.residuals += rs.residuals;
+        all.failed_texels += rs.failed_texels;
+        all.ms_total += rs.ms_total;
+        all.ms_luminance += rs.ms_luminance;
+        all.ms_init += rs.ms_init;
+        all.ms_fit += rs.ms_fit;
+        all.ms_copy += rs.ms_copy;
+        all.ms_ndf += rs.ms_ndf;
+        all.lm_threads = rs.lm_threads;
+        all.lm_slots = rs.lm_slots;
+    }
+    if(run)
+        *run = all;
+    if(partial)
+        return fail(SVF_EPARTIAL, "%llu texels did not produce a finite fit", (unsigned long long)all.failed_texels);
+    return SVF_OK;
+}
+
+void svf_btf_destroy(svf_btf* btf)
+{
+    if(!btf)
+        return;
+    cudaSetDevice(btf->device);
+    cudaDeviceSynchronize();
+    delete btf;
 }
 
 } // extern "C"

@@ -205,4 +205,22 @@ cudaError_t mlp_targets(const float* p7, uint64_t texels, float* Y, cudaStream_t
 cudaError_t mlp_finish(const float* Yn, uint64_t texels, const float* mean, const float* std, float* p7,
                        cudaStream_t stream);
 
+// ---- factored BTF decode (svf_btf.cu) ----------------------------------------------
+
+// Channel c: U_c row lv at u[c] + lv * u_row[c] elements, SxV_c row col at
+// sxv[c] + col * sxv_row[c]; k[c] components; elements of data_size bytes.
+struct BtfDecodeArgs
+{
+    const void* u[3];
+    const void* sxv[3];
+    uint32_t k[3];
+    uint64_t u_row[3], sxv_row[3];
+    uint32_t data_size, color_model, drr;
+    uint32_t width, height, N;
+    uint64_t first, count;     // texels [first, first + count), index y * width + x
+    uint32_t out_type;         // SVF_SAMPLES_F32 / F16
+    void* out;                 // device [count][N][3]
+};
+cudaError_t launch_btf_decode(const BtfDecodeArgs& a, cudaStream_t stream);
+
 } // namespace svf

@@ -35,17 +35,26 @@ inline void sincos_tan(float omega, float* s, float* c)
 
 } // namespace
 
-void angles_to_parabolic(float theta, float phi, float* out)
+void angles_to_cartesian(float theta, float phi, float* w)
 {
-    // SphereToCartesianCoordinates (vector3.hh:375-382) then
-    // CartesianToParabolicCoordinates (vector3.hh:384-387), as LoadBTF
-    // derives BTF::LightsParabolic (btf.cc:474-519).
+    // SphereToCartesianCoordinates (vector3.hh:375-382)
     float ct, st, cp, sp;
     sincos_tan(theta, &st, &ct);
     sincos_tan(phi, &sp, &cp);
-    float x = cp * st, y = sp * st, z = ct;
-    out[0] = x / (z + 1.0f);
-    out[1] = y / (z + 1.0f);
+    w[0] = cp * st;
+    w[1] = sp * st;
+    w[2] = ct;
+}
+
+void angles_to_parabolic(float theta, float phi, float* out)
+{
+    // SphereToCartesianCoordinates then CartesianToParabolicCoordinates
+    // (vector3.hh:384-387), as LoadBTF derives BTF::LightsParabolic
+    // (btf.cc:474-519).
+    float w[3];
+    angles_to_cartesian(theta, phi, w);
+    out[0] = w[0] / (w[2] + 1.0f);
+    out[1] = w[1] / (w[2] + 1.0f);
 }
 
 void parabolic_to_cartesian_ref(float px, float py, float* w)

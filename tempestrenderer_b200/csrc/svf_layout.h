@@ -7,7 +7,9 @@
 namespace svf
 {
 
-// (theta, phi) -> parabolic coordinates, as LoadBTF computes them.
+// (theta, phi) -> Cartesian direction and parabolic coordinates, as LoadBTF
+// computes them.
+void angles_to_cartesian(float theta, float phi, float* w);
 void angles_to_parabolic(float theta, float phi, float* out);
 // ParabolicToCartesianCoordinates in the reference's operation order.
 void parabolic_to_cartesian_ref(float px, float py, float* w);
