@@ -281,6 +281,83 @@ def batch_item(svf, ctx, steps, dev):
                     "so the residual ratio to plain per-BTF LM is 1 by construction"}
 
 
+def dfmf_bytes(theta_phi, width, height, u_planes, sxv_planes, data_size=2):
+    """A DFMF file image (the layout LoadBTF parses, src/image/btf.cc:389-843): one
+    (U [L*L][K], SxV [W*H][K]) plane pair per channel; SxV rows are file columns."""
+    import struct
+
+    dt = {2: np.float16, 4: np.float32}[data_size]
+    tp = np.ascontiguousarray(theta_phi, np.float32)
+    L = tp.shape[0]
+    parts = [b"!DFMF08FC", struct.pack("<II", 264, 1), b"\0" * 240, struct.pack("<f3f", 0.0, 1.0, 1.0, 1.0),
+             struct.pack("<I", L)]
+    for v in range(L):
+        parts += [tp[v].tobytes(), struct.pack("<I", L), tp.tobytes()]
+    parts += [struct.pack("<II", width, height), struct.pack("<II", u_planes[0].shape[1], 0),
+              struct.pack("<3f", 0, 0, 0), np.eye(3, dtype=np.float32).tobytes()]
+    for U, S in zip(u_planes, sxv_planes):
+        K = U.shape[1]
+        parts += [struct.pack("<B", data_size), struct.pack("<III", K, U.shape[0], S.shape[0]),
+                  np.ones(K, dt).tobytes(), np.ascontiguousarray(U, dt).tobytes(),
+                  np.ascontiguousarray(S, dt).tobytes()]
+    return b"".join(parts)
+
+
+def btf_file_item(svf, ctx, layout, W, H, steps, dev, K=48):
+    """A 400x400-texel DFMF file (FP16 planes, K components per channel): each texel
+    a convex mix of K synthetic prototype texels (U = the prototypes' samples, SxV =
+    Dirichlet weights).  Timed: the GPU decode alone, and svf_fit_btf (decode +
+    fit, default initial guess) over the whole file."""
+    import torch
+
+    L = layout.light_count
+    N, T = L * L, W * H
+    proto = torch.empty((K, N, 3), dtype=torch.float32, device=dev)
+    ctx.synth_btf(SEED + 5, MIX, layout.lights_parabolic, 0, K, proto)
+    proto = proto.cpu().numpy()
+    rng = np.random.default_rng(SEED)
+    wts = rng.dirichlet(np.full(K, 0.3), size=T).astype(np.float32)
+    theta_phi = np.zeros((L, 2), np.float32)
+    # the ring layout's angles: theta rings 0/15/.../75 degrees, phi uniform per ring
+    i = 0
+    for ring, count in zip(range(6), (1, 6, 12, 18, 20, 24)):
+        for k in range(count):
+            theta_phi[i] = (np.radians(15.0 * ring), 2 * np.pi * k / count)
+            i += 1
+    data = dfmf_bytes(theta_phi, W, H, [proto[:, :, c].T for c in range(3)], [wts] * 3)
+    t0 = time.perf_counter()
+    btf = svf.Btf(ctx, data)
+    load_s = time.perf_counter() - t0
+    out = torch.empty((T, N, 3), dtype=torch.float32, device=dev)
+    btf.decode(out=out)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        btf.decode(out=out)
+    torch.cuda.synchronize()
+    dec_s = (time.perf_counter() - t0) / steps
+    del out
+    torch.cuda.empty_cache()
+    want = ("diffuse", "specular", "sigma", "basis", "rmse")
+    btf.fit(layout=layout, want=want, check=False)
+    t0 = time.perf_counter()
+    maps, rs = btf.fit(layout=layout, want=want, check=False)
+    fit_s = time.perf_counter() - t0
+    btf.close()
+    flops = 2.0 * 3 * K * N * T
+    return {"workload": f"DFMF {W}x{H} texels, ring-81, FP16 planes, {K} components per channel "
+                        f"({len(data) / 1e6:.1f} MB file)",
+            "load_s": load_s,
+            "decode": {"value": T / dec_s, "unit": "texels/s", "ms": dec_s * 1e3,
+                       "output_gb_per_s": T * N * 3 * 4 / dec_s / 1e9, "tflops": flops / dec_s / 1e12,
+                       "note": "FP32 samples; sums in the reference's order (bit-exact), so the FP32 pipe "
+                               "runs 2 instructions per product"},
+            "fit_btf": {"value": T / fit_s, "unit": "texels/s", "seconds": fit_s, "ms_device_fit": rs.ms_total,
+                        "failed_texels": int(rs.failed_texels), "mean_rmse": float(maps["rmse"].mean()),
+                        "note": "host wall time of svf_fit_btf (decode into FP32 chunks + the fit pipeline); "
+                                "maps copied to host"}}
+
+
 def run_ours(args):
     import torch
 
@@ -400,9 +477,11 @@ def run_ours(args):
         del host_samples
 
     head_rmse = maps["rmse"].cpu().numpy()
-    learned = fib = batch = None
+    learned = fib = batch = btf_file = None
     if world == 1 and args.mlp_steps > 0:
         learned = learned_init_item(svf, ctx, layout, samples, W, H, head_rmse, args.mlp_steps, dev)
+    if world == 1 and args.btf_steps > 0:
+        btf_file = btf_file_item(svf, ctx, layout, W, H, args.btf_steps, dev)
     # the larger line items run in fresh contexts with the benchmark's buffers released
     ctx.close()
     del samples, maps
@@ -470,7 +549,7 @@ def run_ours(args):
                         "failed_texels": failed, "mean_rmse": float(head_rmse.mean()),
                         "median_rmse": float(np.median(head_rmse))},
             "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "learned_init": learned, "fib151_768x768": fib,
-            "batch_8_btfs": batch, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
+            "batch_8_btfs": batch, "btf_file": btf_file, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
             "wall_s": wall,
         }
         print(json.dumps(line), flush=True)
@@ -493,6 +572,7 @@ def main():
     ap.add_argument("--mlp-steps", type=int, default=2, help="steps of the learned-initial-guess line item (0: skip)")
     ap.add_argument("--fib-steps", type=int, default=1, help="steps of the 768x768 Fibonacci-151 line item (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=1, help="calls of the 8-BTF batch line item (0: skip)")
+    ap.add_argument("--btf-steps", type=int, default=3, help="decodes of the DFMF-file line item (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

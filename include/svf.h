@@ -365,6 +365,47 @@ svf_status svf_fit_btf(svf_ctx* ctx, const svf_btf* btf, const svf_layout_desc* 
                        const svf_maps* maps, svf_run_stats* run);
 void       svf_btf_destroy(svf_btf* btf);
 
+/* Error of fitted maps against a BTF ------------------------------------------------
+ * svbrdf-error-tool (tools/svbrdf-error-tool/svbrdf-error-tool.cc:88-250) on the
+ * GPU: per texel of the maps' region, the SGGX surface BRDF of the map values
+ * (Fresnel 1) against the BTF texel (x0 + x, y0 + y), residuals of the luminance
+ * or per channel (color), pair-wise (MSE over all light-view pairs) or max-view
+ * (the view with the largest sum over lights); RMSE and PSNR = 20 log10(peak /
+ * RMSE) with the peak BTF value of the pairs taken. */
+#define SVF_ERROR_PAIRWISE 0u
+#define SVF_ERROR_MAX_VIEW 1u
+
+typedef struct svf_svbrdf_maps
+{
+    const float* diffuse;      /* [height][width][3] */
+    const float* specular;     /* [height][width][3] */
+    const float* sigma;        /* [height][width][sigma_channels] */
+    uint32_t     sigma_channels;   /* 2: (sx, sy); 3: (sx, sy, sz), used as (sx/sz, sy/sz) */
+    const float* basis;        /* [height][width][4] quaternion xyzw */
+    uint32_t     width, height;
+} svf_svbrdf_maps;
+
+/* rmse, psnr: [height][width] ([height][width][3] with color), host or device;
+ * the maps likewise. */
+svf_status svf_error_maps(svf_ctx* ctx, const svf_btf* btf, const svf_svbrdf_maps* maps, uint32_t x0, uint32_t y0,
+                          uint32_t method, uint32_t color, float* rmse, float* psnr);
+
+/* OpenEXR maps ----------------------------------------------------------------------
+ * svbrdffit's output files (svbrdf-fitting.cc:713-735, SaveEXRImage in
+ * src/image/exr-image.cc): uncompressed FLOAT scanlines, channels R, G, B, A
+ * (the first 1..4), image row y stored as scanline height-1-y.  Host only. */
+svf_status svf_exr_write(const char* path, uint32_t width, uint32_t height, uint32_t channels,
+                         const float* data /* [height][width][channels] */);
+/* Reads an uncompressed scanline OpenEXR file of HALF or FLOAT channels named
+ * R/G/B/A into [height][width][channels] floats (LoadEXRImage's layout).  With
+ * data NULL only the dimensions are returned; capacity is data's length in floats. */
+svf_status svf_exr_read(const char* path, uint32_t* width, uint32_t* height, uint32_t* channels, float* data,
+                        size_t capacity);
+/* The svbrdffit file set <prefix>_albedo.exr (diffuse, RGB), _specular.exr (RGB),
+ * _sggx_scale.exr (RG), _sggx_basis.exr (RGBA quaternion) and _rmse.exr (R) from
+ * host maps of width x height texels; NULL maps are skipped. */
+svf_status svf_maps_write_exr(const char* prefix, uint32_t width, uint32_t height, const svf_maps* maps);
+
 /* Synthetic BTFs (test and benchmark inputs) ------------------------------------ */
 /* Renders texels [first, first + count) of a seeded synthetic BTF straight into
  * `samples` ([count][L*L][3], device memory, F32 or F16): per texel, ground-truth

@@ -396,6 +396,12 @@ def ref():
         L.ref_time_fit_texels.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.c_float, C.c_void_p]
         L.ref_time_fit_texels.restype = C.c_double
+        L.ref_exr_save.argtypes = [C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint32, _f32p]
+        L.ref_exr_save.restype = C.c_int
+        L.ref_exr_load.argtypes = [C.c_char_p, _u32p, C.c_void_p]
+        L.ref_exr_load.restype = C.c_int
+        L.ref_error_texel.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _f32p, _f32p, _f32p, _f32p, C.c_uint32,
+                                      C.c_uint32, _f32p, _f32p]
         _ref = L
     return _ref
 

@@ -30,6 +30,7 @@
 #include "tempest/utils/logging.hh"
 #include "tempest/utils/file-system.hh"
 #include "tempest/graphics/texture.hh"
+#include "tempest/image/exr-image.hh"
 #include "tempest/math/fitting.hh"
 
 #define EXPORT_EVALUATOR
@@ -304,6 +305,143 @@ double ref_time_fit_texels(void* handle, uint32_t first_texel, uint32_t texel_co
     pool->shutdown();
     /* the pool object itself is leaked on purpose, see SerialPool() */
     return std::chrono::duration<double>(t1 - t0).count();
+}
+
+/* ---- svbrdffit's EXR maps and svbrdf-error-tool -------------------------------- */
+
+/* SaveEXRImage (src/image/exr-image.cc:200-330) of [h][w][channels] floats. */
+int ref_exr_save(const char* path, uint32_t w, uint32_t h, uint32_t channels, const float* data)
+{
+    Tempest::TextureDescription desc;
+    desc.Width = w;
+    desc.Height = h;
+    static const Tempest::DataFormat fmts[4] = { Tempest::DataFormat::R32F, Tempest::DataFormat::RG32F,
+                                                 Tempest::DataFormat::RGB32F, Tempest::DataFormat::RGBA32F };
+    desc.Format = fmts[channels - 1];
+    return Tempest::SaveEXRImage(desc, data, Tempest::Path(path)) ? 1 : 0;
+}
+
+/* LoadEXRImage (exr-image.cc:14-198): dims = width, height, channels; data
+ * (optional) receives [h][w][channels] floats. */
+int ref_exr_load(const char* path, uint32_t* dims, float* data)
+{
+    std::unique_ptr<Tempest::Texture> tex(Tempest::LoadEXRImage(Tempest::Path(path)));
+    if(!tex)
+        return 0;
+    auto& hdr = tex->getHeader();
+    dims[0] = hdr.Width;
+    dims[1] = hdr.Height;
+    dims[2] = Tempest::DataFormatChannels(hdr.Format);
+    if(data)
+        std::memcpy(data, tex->getData(), sizeof(float) * dims[0] * dims[1] * dims[2]);
+    return 1;
+}
+
+/* svbrdf-error-tool's per-texel error (tools/svbrdf-error-tool/svbrdf-error-tool.cc:
+ * 88-250), restated for one texel with the reference's own functions: the
+ * material from the map values (stddev: sx, sy), the SGGX surface BRDF at every
+ * (light, view), residuals against the BTF's luminance (color 0) or RGB
+ * (color 1) slice; method 0 pair-wise, 1 max-view.  rmse3/psnr3: [0] or [0..2]. */
+void ref_error_texel(void* handle, uint32_t x, uint32_t y, const float* diffuse3, const float* specular3,
+                     const float* stddev2, const float* basis4, uint32_t method, uint32_t color, float* rmse3,
+                     float* psnr3)
+{
+    auto* btf = reinterpret_cast<Tempest::BTF*>(handle);
+    auto* pool = SerialPool();
+    const uint32_t L = btf->LightCount;
+    Tempest::RTSGGXSurface mat;
+    mat.SampleCount = 256;
+    mat.Depth = 0;
+    mat.Diffuse = Tempest::RGBToSpectrum(Tempest::Vector3{ diffuse3[0], diffuse3[1], diffuse3[2] });
+    mat.Specular = Tempest::RGBToSpectrum(Tempest::Vector3{ specular3[0], specular3[1], specular3[2] });
+    mat.SGGXBasis = Tempest::Vector4{ basis4[0], basis4[1], basis4[2], basis4[3] };
+    mat.StandardDeviation = Tempest::Vector2{ stddev2[0], stddev2[1] };
+    mat.SpecularMap = nullptr;
+    mat.DiffuseMap = nullptr;
+    mat.BasisMap = nullptr;
+    mat.StandardDeviationMap = nullptr;
+    mat.Fresnel = { 1.0f, 0.0f };
+    std::vector<float> lum(L * L);
+    std::vector<Tempest::Vector3> rgb(L * L);
+    float* lum_ptr = lum.data();
+    Tempest::Vector3* rgb_ptr = rgb.data();
+    if(color)
+        Tempest::BTFParallelExtractRGBSlice(btf, 0, *pool, x, y, &rgb_ptr);
+    else
+        Tempest::BTFParallelExtractLuminanceSlice(btf, 0, *pool, x, y, &lum_ptr);
+    auto brdf = [&](uint32_t light_idx, uint32_t view_idx) {
+        Tempest::SampleData sd{};
+        sd.Material = reinterpret_cast<Tempest::RTMaterial*>(&mat);
+        sd.Tangent = Tempest::Vector3{ 1.0f, 0.0f, 0.0f };
+        sd.Binormal = Tempest::Vector3{ 0.0f, 1.0f, 0.0f };
+        sd.Normal = Tempest::Vector3{ 0.0f, 0.0f, 1.0f };
+        sd.IncidentLight = Tempest::ParabolicToCartesianCoordinates(btf->LightsParabolic[light_idx]);
+        sd.OutgoingLight = Tempest::ParabolicToCartesianCoordinates(btf->LightsParabolic[view_idx]);
+        Tempest::Quaternion quat;
+        quat.V4 = mat.SGGXBasis;
+        sd.DirectionalDensity = Tempest::SGGXProjectedArea(
+            Tempest::Vector3{ mat.StandardDeviation.x, mat.StandardDeviation.y, 1.0f }, Tempest::ToMatrix3(quat),
+            sd.OutgoingLight);
+        return Tempest::SpectrumToRGB(Tempest::SGGXMicroFlakeSurfaceBRDF(sd));
+    };
+    const uint32_t nch = color ? 3 : 1;
+    float sq[3] = {}, mx[3] = {};
+    if(method == 0)
+    {
+        for(uint32_t view_idx = 0; view_idx < L; ++view_idx)
+            for(uint32_t light_idx = 0; light_idx < L; ++light_idx)
+            {
+                const uint32_t lv = view_idx * L + light_idx;
+                const auto f = brdf(light_idx, view_idx);
+                for(uint32_t c = 0; c < nch; ++c)
+                {
+                    const float b = color ? (&rgb[lv].x)[c] : lum[lv];
+                    const float m = color ? (&f.x)[c] : Tempest::RGBToLuminance(f);
+                    mx[c] = std::max(b, mx[c]);
+                    const float r = b - m;
+                    sq[c] += r * r;
+                }
+            }
+        for(uint32_t c = 0; c < nch; ++c)
+            sq[c] = sq[c] / (float)(L * L);
+    }
+    else
+    {
+        float best[3] = {}, best_mx[3] = {};
+        for(uint32_t view_idx = 0; view_idx < L; ++view_idx)
+        {
+            float vs[3] = {}, vm[3] = {};
+            for(uint32_t light_idx = 0; light_idx < L; ++light_idx)
+            {
+                const uint32_t lv = view_idx * L + light_idx;
+                const auto f = brdf(light_idx, view_idx);
+                for(uint32_t c = 0; c < nch; ++c)
+                {
+                    const float b = color ? (&rgb[lv].x)[c] : lum[lv];
+                    const float m = color ? (&f.x)[c] : Tempest::RGBToLuminance(f);
+                    vm[c] = std::max(b, vm[c]);
+                    const float r = b - m;
+                    vs[c] += r * r;
+                }
+            }
+            for(uint32_t c = 0; c < nch; ++c)
+                if(vs[c] > best[c])
+                {
+                    best[c] = vs[c];
+                    best_mx[c] = vm[c];
+                }
+        }
+        for(uint32_t c = 0; c < nch; ++c)
+        {
+            sq[c] = best[c] / (float)L;
+            mx[c] = best_mx[c];
+        }
+    }
+    for(uint32_t c = 0; c < nch; ++c)
+    {
+        rmse3[c] = sqrtf(sq[c]);
+        psnr3[c] = 20.0f * log10f(mx[c] / rmse3[c]);
+    }
 }
 
 }

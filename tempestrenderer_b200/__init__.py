@@ -29,6 +29,7 @@ SVF_LSQ_DIFFUSE = 1 << 1
 SVF_LSQ_RGB = 1 << 8
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
+SVF_ERROR_PAIRWISE, SVF_ERROR_MAX_VIEW = 0, 1
 
 # every entry point include/svf.h declares
 EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_options_default", "svf_create",
@@ -36,7 +37,8 @@ EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_op
            "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc", "svf_fit_texels", "svf_fit_btfs",
            "svf_synth_btf", "svf_mlp_train_options_default", "svf_mlp_train", "svf_mlp_predict", "svf_mlp_step",
            "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy", "svf_btf_probe", "svf_btf_load", "svf_btf_load_file",
-           "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_btf_destroy")
+           "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_btf_destroy", "svf_error_maps", "svf_exr_write",
+           "svf_exr_read", "svf_maps_write_exr")
 
 
 class SvfError(RuntimeError):
@@ -79,6 +81,11 @@ class BtfInfo(C.Structure):
     _fields_ = [("format", C.c_uint32), ("width", C.c_uint32), ("height", C.c_uint32), ("light_count", C.c_uint32),
                 ("data_size", C.c_uint32), ("color_model", C.c_uint32), ("dynamic_range_reduction", C.c_uint32),
                 ("cosine_flag", C.c_uint32), ("version", C.c_uint32), ("components", C.c_uint32 * 3)]
+
+
+class SvbrdfMaps(C.Structure):
+    _fields_ = [("diffuse", C.c_void_p), ("specular", C.c_void_p), ("sigma", C.c_void_p),
+                ("sigma_channels", C.c_uint32), ("basis", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32)]
 
 
 class MlpTrainOptions(C.Structure):
@@ -149,10 +156,15 @@ def load() -> C.CDLL:
         L.svf_fit_btf.argtypes = [vp, vp, vp, C.POINTER(FitOptions), C.POINTER(Maps), C.POINTER(RunStats)]
         L.svf_btf_destroy.argtypes = [vp]
         L.svf_btf_destroy.restype = None
+        L.svf_error_maps.argtypes = [vp, vp, C.POINTER(SvbrdfMaps), u32, u32, u32, u32, vp, vp]
+        L.svf_exr_write.argtypes = [C.c_char_p, u32, u32, u32, vp]
+        L.svf_exr_read.argtypes = [C.c_char_p, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), vp, C.c_size_t]
+        L.svf_maps_write_exr.argtypes = [C.c_char_p, u32, u32, C.POINTER(Maps)]
         for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
                      "svf_fit_texels", "svf_fit_btfs", "svf_synth_btf", "svf_mlp_train", "svf_mlp_predict",
                      "svf_mlp_step", "svf_mlp_save", "svf_mlp_load", "svf_btf_probe", "svf_btf_load",
-                     "svf_btf_load_file", "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf"):
+                     "svf_btf_load_file", "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_error_maps",
+                     "svf_exr_write", "svf_exr_read", "svf_maps_write_exr"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -501,6 +513,18 @@ class Btf:
             _check(st)
         return res, rs
 
+    def error_maps(self, diffuse, specular, sigma, basis, x0: int = 0, y0: int = 0, method=SVF_ERROR_PAIRWISE,
+                   color: bool = False):
+        """svbrdf-error-tool: maps [h][w][3|3|2or3|4] -> (rmse, psnr) [h][w] ([h][w][3] with color)."""
+        d, sp, sg, b = (np.ascontiguousarray(m, np.float32) for m in (diffuse, specular, sigma, basis))
+        h, w = d.shape[:2]
+        m = SvbrdfMaps(d.ctypes.data, sp.ctypes.data, sg.ctypes.data, sg.shape[2], b.ctypes.data, w, h)
+        shape = (h, w, 3) if color else (h, w)
+        rmse, psnr = np.zeros(shape, np.float32), np.zeros(shape, np.float32)
+        _check(self._lib.svf_error_maps(self.ctx.handle, self.handle, C.byref(m), x0, y0, method, int(color),
+                                        rmse.ctypes.data, psnr.ctypes.data))
+        return rmse, psnr
+
     def close(self):
         if getattr(self, "handle", None):
             self._lib.svf_btf_destroy(self.handle)
@@ -508,3 +532,31 @@ class Btf:
 
     def __del__(self):
         self.close()
+
+
+def exr_write(path: str, image) -> None:
+    """An [h][w] or [h][w][c] float image (c = 1..4) as svbrdffit saves its maps."""
+    img = np.ascontiguousarray(image, np.float32)
+    if img.ndim == 2:
+        img = img[:, :, None]
+    _check(load().svf_exr_write(path.encode(), img.shape[1], img.shape[0], img.shape[2], img.ctypes.data))
+
+
+def exr_read(path: str) -> np.ndarray:
+    """[h][w][c] float32 from an uncompressed OpenEXR file (LoadEXRImage's layout)."""
+    w, h, c = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    _check(load().svf_exr_read(path.encode(), C.byref(w), C.byref(h), C.byref(c), None, 0))
+    out = np.zeros((h.value, w.value, c.value), np.float32)
+    _check(load().svf_exr_read(path.encode(), C.byref(w), C.byref(h), C.byref(c), out.ctypes.data, out.size))
+    return out
+
+
+def maps_write_exr(prefix: str, width: int, height: int, maps: dict) -> None:
+    """svbrdffit's <prefix>_albedo/_specular/_sggx_scale/_sggx_basis/_rmse.exr from host maps."""
+    m = Maps()
+    keep = {}
+    for k in ("diffuse", "specular", "sigma", "basis", "rmse"):
+        if k in maps:
+            keep[k] = np.ascontiguousarray(maps[k], np.float32)
+            setattr(m, k, keep[k].ctypes.data)
+    _check(load().svf_maps_write_exr(prefix.encode(), width, height, C.byref(m)))

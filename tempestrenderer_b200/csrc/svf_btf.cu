@@ -16,12 +16,15 @@
 // agree to a few ulp.
 //
 // Work split: a CTA of 128 threads owns 128 consecutive pairs lv (one per
-// thread) and TX texels; the texels' SxV rows go through shared memory in
-// chunks of 32 components (transposed, so a thread reads TX of them with
-// vector broadcasts); each thread streams its own U row.  Writes: a warp stores
-// 32 consecutive pairs x 3 channels of one texel at a time (384 contiguous
-// bytes in FP32).  Bound by the FP32 pipe for K >= ~20 components (2 flops per
-// component per channel per sample), by the HBM write otherwise.
+// thread) and TX texels.  Per chunk of 32 components the CTA stages, with
+// coalesced loads, the 128 U rows (transposed, padded: a thread reads its pair's
+// value conflict-free) and the TX texels' SxV rows (transposed: a thread reads
+// TX of them with vector broadcasts) in shared memory.  Half planes accumulate
+// with FMAs (a product of two halves is exact in float, so the FMA rounds as the
+// reference's separate multiply and add do); float and double planes need the
+// separate multiply and add.  Writes: a warp stores 32 consecutive pairs x 3
+// channels of one texel at a time (384 contiguous bytes in FP32).  Bound by
+// the FP32 pipe for K >= ~20 components, by the HBM write otherwise.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -43,16 +46,28 @@ __device__ __forceinline__ double elem(const double* p, uint64_t i) { return p[i
 // sum + u * v with the product rounded first (no contraction into an FMA,
 // which would round once); for half elements the product is exact in float and
 // an FMA gives the same result.
+template <typename T>
 __device__ __forceinline__ float madd(float sum, float u, float v) { return __fadd_rn(sum, __fmul_rn(u, v)); }
+template <>
+__device__ __forceinline__ float madd<__half>(float sum, float u, float v) { return __fmaf_rn(u, v, sum); }
+template <typename T>
 __device__ __forceinline__ double madd(double sum, double u, double v) { return __dadd_rn(sum, __dmul_rn(u, v)); }
 
 template <typename T, typename Acc, int TX>
 __global__ void __launch_bounds__(kThreads) btf_decode_kernel(BtfDecodeArgs a, uint64_t t_begin)
 {
     __shared__ Acc s_sxv[kChunk][TX];
-    const uint32_t lv = blockIdx.x * kThreads + threadIdx.x;
+    __shared__ Acc s_u[kChunk][kThreads + 1];
+    __shared__ uint64_t s_col[TX];   // file column of each texel (after the row flip)
+    const uint32_t lv0 = blockIdx.x * kThreads, lv = lv0 + threadIdx.x;
     const uint64_t t0 = t_begin + (uint64_t)blockIdx.y * TX;
     const uint64_t t_end = a.first + a.count;
+    if(threadIdx.x < TX)
+    {
+        const uint64_t t = t0 + threadIdx.x;
+        const uint64_t y = t / a.width, x = t - y * a.width;
+        s_col[threadIdx.x] = t < t_end ? (a.height - 1 - y) * a.width + x : ~0ull;
+    }
     Acc acc[3][TX];
 #pragma unroll
     for(int c = 0; c < 3; ++c)
@@ -66,34 +81,31 @@ __global__ void __launch_bounds__(kThreads) btf_decode_kernel(BtfDecodeArgs a, u
         const T* U = static_cast<const T*>(a.u[c]);
         const T* S = static_cast<const T*>(a.sxv[c]);
         const uint32_t K = a.k[c];
-        const T* urow = U + (uint64_t)(lv < a.N ? lv : 0) * a.u_row[c];
         for(uint32_t k0 = 0; k0 < K; k0 += kChunk)
         {
             __syncthreads();
-            for(int i = threadIdx.x; i < TX * kChunk; i += kThreads)
+            // a warp reads 32 consecutive components of one row per step
+            const int kk = threadIdx.x % kChunk, r0 = threadIdx.x / kChunk;
+            const bool k_ok = k0 + kk < K;
+            for(int j = r0; j < TX; j += kThreads / kChunk)
             {
-                const int j = i / kChunk, kk = i % kChunk;
-                const uint64_t t = t0 + j;
-                Acc v = Acc(0);
-                if(t < t_end && k0 + kk < K)
-                {
-                    const uint64_t y = t / a.width, x = t - y * a.width;
-                    const uint64_t col = (a.height - 1 - y) * a.width + x;
-                    v = elem(S, col * a.sxv_row[c] + k0 + kk);
-                }
-                s_sxv[kk][j] = v;
+                const uint64_t col = s_col[j];
+                s_sxv[kk][j] = (col != ~0ull && k_ok) ? elem(S, col * a.sxv_row[c] + k0 + kk) : Acc(0);
+            }
+            {
+                const T* up = U + (uint64_t)(lv0 + r0) * a.u_row[c] + k0 + kk;
+                const uint64_t step = (uint64_t)(kThreads / kChunk) * a.u_row[c];
+                for(int row = r0; row < kThreads; row += kThreads / kChunk, up += step)
+                    s_u[kk][row] = (lv0 + row < a.N && k_ok) ? elem(up, 0) : Acc(0);
             }
             __syncthreads();
-            if(lv < a.N)
+            const uint32_t n = K - k0 < (uint32_t)kChunk ? K - k0 : (uint32_t)kChunk;
+            for(uint32_t kk = 0; kk < n; ++kk)
             {
-                const uint32_t n = K - k0 < (uint32_t)kChunk ? K - k0 : (uint32_t)kChunk;
-                for(uint32_t kk = 0; kk < n; ++kk)
-                {
-                    const Acc u = elem(urow, k0 + kk);
+                const Acc u = s_u[kk][threadIdx.x];
 #pragma unroll
-                    for(int j = 0; j < TX; ++j)
-                        acc[c][j] = madd(acc[c][j], u, s_sxv[kk][j]);
-                }
+                for(int j = 0; j < TX; ++j)
+                    acc[c][j] = madd<T>(acc[c][j], u, s_sxv[kk][j]);
             }
         }
     }
@@ -174,9 +186,9 @@ cudaError_t launch_btf_decode(const BtfDecodeArgs& a, cudaStream_t stream)
         return cudaSuccess;
     switch(a.data_size)
     {
-    case 2: return launch_typed<__half, float, 16>(a, stream);
-    case 4: return launch_typed<float, float, 16>(a, stream);
-    case 8: return launch_typed<double, double, 8>(a, stream);
+    case 2: return launch_typed<__half, float, 32>(a, stream);
+    case 4: return launch_typed<float, float, 32>(a, stream);
+    case 8: return launch_typed<double, double, 16>(a, stream);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -44,6 +44,24 @@ svf_status fail(svf_status s, const char* fmt, ...)
     return s;
 }
 
+} // namespace
+
+// The last-error reporting for the library's other host files.
+namespace svf
+{
+svf_status host_fail(svf_status s, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return s;
+}
+} // namespace svf
+
+namespace
+{
+
 #define SVF_CUDA(call)                                                                                     \
     do                                                                                                     \
     {                                                                                                      \
@@ -2593,6 +2611,78 @@ svf_status svf_fit_btf(svf_ctx* ctx, const svf_btf* btf, const svf_layout_desc* 
         *run = all;
     if(partial)
         return fail(SVF_EPARTIAL, "%llu texels did not produce a finite fit", (unsigned long long)all.failed_texels);
+    return SVF_OK;
+}
+
+svf_status svf_error_maps(svf_ctx* ctx, const svf_btf* btf, const svf_svbrdf_maps* maps, uint32_t x0, uint32_t y0,
+                          uint32_t method, uint32_t color, float* rmse, float* psnr)
+{
+    SVF_TRY(check_btf(ctx, btf));
+    if(!maps || !rmse || !psnr || !maps->diffuse || !maps->specular || !maps->sigma || !maps->basis)
+        return fail(SVF_EINVAL, "null maps/outputs");
+    if(method != SVF_ERROR_PAIRWISE && method != SVF_ERROR_MAX_VIEW)
+        return fail(SVF_EINVAL, "unknown method %u", method);
+    if(maps->sigma_channels != 2 && maps->sigma_channels != 3)
+        return fail(SVF_EINVAL, "sigma_channels %u (2 or 3)", maps->sigma_channels);
+    const svf::BtfFile& f = btf->f;
+    const uint32_t w = maps->width, h = maps->height;
+    if(w == 0 || h == 0 || x0 >= f.width || y0 >= f.height || w > f.width - x0 || h > f.height - y0)
+        return fail(SVF_EINVAL, "maps of %ux%u at (%u, %u) outside the %ux%u BTF", w, h, x0, y0, f.width, f.height);
+    Layout* lay = nullptr;
+    SVF_TRY(get_layout(ctx, f.lights_parabolic.data(), f.light_count, &lay));
+    const uint64_t N = (uint64_t)f.light_count * f.light_count;
+    const size_t row_bytes = sizeof(float) * 3 * N * f.width;
+    size_t free_b = 0, total_b = 0;
+    SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const uint32_t rows = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(h, free_b / 4 / row_bytes));
+    const uint32_t nout = color ? 3 : 1;
+    const uint32_t sc = maps->sigma_channels;
+    DevBuf samples, md, out;
+    SVF_TRY(samples.ensure(row_bytes * rows));
+    const uint64_t rt = (uint64_t)rows * w;
+    SVF_TRY(md.ensure(sizeof(float) * rt * (3 + 3 + sc + 4)));
+    SVF_TRY(out.ensure(sizeof(float) * rt * 2 * nout));
+    float* d_diff = md.as<float>();
+    float* d_spec = d_diff + 3 * rt;
+    float* d_sig = d_spec + 3 * rt;
+    float* d_basis = d_sig + sc * rt;
+    float* d_rmse = out.as<float>();
+    float* d_psnr = d_rmse + nout * rt;
+    for(uint32_t r0 = 0; r0 < h; r0 += rows)
+    {
+        const uint32_t nr = std::min(rows, h - r0);
+        const uint64_t n = (uint64_t)nr * w, m0 = (uint64_t)r0 * w;
+        SVF_CUDA(svf::launch_btf_decode(btf_args(btf, (uint64_t)(y0 + r0) * f.width, (uint64_t)nr * f.width,
+                                                 SVF_SAMPLES_F32, samples.p),
+                                        ctx->stream));
+        SVF_TRY(to_device(ctx, d_diff, maps->diffuse + 3 * m0, sizeof(float) * 3 * n));
+        SVF_TRY(to_device(ctx, d_spec, maps->specular + 3 * m0, sizeof(float) * 3 * n));
+        SVF_TRY(to_device(ctx, d_sig, maps->sigma + sc * m0, sizeof(float) * sc * n));
+        SVF_TRY(to_device(ctx, d_basis, maps->basis + 4 * m0, sizeof(float) * 4 * n));
+        svf::ErrorArgs a{};
+        a.samples = samples.p;
+        a.sample_type = SVF_SAMPLES_F32;
+        a.L = f.light_count;
+        a.N = (uint32_t)N;
+        a.geo = lay->geo.as<float>();
+        a.count = n;
+        a.region_w = w;
+        a.row_texels = f.width;
+        a.x0 = x0;
+        a.diffuse = d_diff;
+        a.specular = d_spec;
+        a.sigma = d_sig;
+        a.basis = d_basis;
+        a.sigma_channels = sc;
+        a.method = method;
+        a.color = color ? 1u : 0u;
+        a.rmse = d_rmse;
+        a.psnr = d_psnr;
+        SVF_CUDA(svf::launch_error(a, ctx->stream));
+        SVF_CUDA(cudaMemcpyAsync(rmse + nout * m0, d_rmse, sizeof(float) * nout * n, cudaMemcpyDefault, ctx->stream));
+        SVF_CUDA(cudaMemcpyAsync(psnr + nout * m0, d_psnr, sizeof(float) * nout * n, cudaMemcpyDefault, ctx->stream));
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
     return SVF_OK;
 }
 

@@ -223,4 +223,22 @@ struct BtfDecodeArgs
 };
 cudaError_t launch_btf_decode(const BtfDecodeArgs& a, cudaStream_t stream);
 
+// ---- error of fitted maps against a BTF (svf_error.cu) -----------------------------
+
+struct ErrorArgs
+{
+    const void* samples;       // device [rows * row_texels][N][3] decoded BTF rows
+    uint32_t sample_type;
+    uint32_t L, N;
+    const float* geo;          // [3][L] directions
+    uint64_t count;            // region texels in this launch: rows x region_w
+    uint32_t region_w;
+    uint64_t row_texels, x0;   // sample row of region texel (ry, rx): ry * row_texels + x0 + rx
+    const float *diffuse, *specular, *sigma, *basis;   // device maps [count][3|3|sigma_channels|4]
+    uint32_t sigma_channels;   // 2: (sx, sy); 3: (sx/sz, sy/sz)
+    uint32_t method, color;    // SVF_ERROR_*; color: per-channel outputs
+    float *rmse, *psnr;        // device [count] ([count][3] with color)
+};
+cudaError_t launch_error(const ErrorArgs& a, cudaStream_t stream);
+
 } // namespace svf
