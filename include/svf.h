@@ -390,6 +390,35 @@ typedef struct svf_svbrdf_maps
 svf_status svf_error_maps(svf_ctx* ctx, const svf_btf* btf, const svf_svbrdf_maps* maps, uint32_t x0, uint32_t y0,
                           uint32_t method, uint32_t color, float* rmse, float* psnr);
 
+/* Refit --------------------------------------------------------------------------------
+ * svbrdffit -r (refit from saved maps, svbrdf-fitting.cc:510-569 and
+ * SVBRDFFitPipeline::fit's reoptimize branch, pipeline.cc:661-670): the 7 fit
+ * parameters of maps -- diffuse and specular as RGBToLuminance of the albedos,
+ * the SGGX scales, Euler angles of the basis quaternion (ToMatrix3 then
+ * Matrix3::decompose) -- for svf_fit_texels with SVF_INIT_GIVEN; colour
+ * (optional, [texels][3]) receives specular / its luminance, the chromaticity the
+ * reference colours the refit maps with.  The reference decomposes an
+ * uninitialised matrix there instead of the quaternion's (SGGXProjectIntegrand::
+ * Basis is default-constructed); this function converts the quaternion itself. */
+svf_status svf_params_from_maps(const svf_svbrdf_maps* maps, float* params /* [texels][7] */, float* colour);
+
+/* svbrdffit -j (optimize-neighborhood, NeighborhoodPusherThread,
+ * svbrdf-fitting.cc:123-178) as one batched GPU pass: every texel's luminance
+ * slice is fitted from the parameters of each texel of its 3x3 neighbourhood
+ * (itself included, clipped to the image) -- nine LM fits per texel in one
+ * persistent launch -- and the texel keeps the first candidate, in row order,
+ * whose RMSE is below its current one (params_in, rmse_in: the first fit's).
+ * All candidates start from the input maps (the reference's threads update
+ * the maps while others read them).  The reference's loop, as written, fits the
+ * texel's own default guess nine times and stores a better result in the
+ * neighbour's slot (fit is called without its reoptimize flag, and the inner
+ * index shadows the texel's); this pass does what the option describes.
+ * out: params, rmse and the four maps of the selected parameters (coloured by
+ * the BTF's average chromaticity). */
+svf_status svf_refit_neighborhood(svf_ctx* ctx, const svf_btf_view* btf, const svf_lsq_options* options,
+                                  const float* params_in, const float* rmse_in, const svf_maps* out,
+                                  svf_run_stats* run);
+
 /* OpenEXR maps ----------------------------------------------------------------------
  * svbrdffit's output files (svbrdf-fitting.cc:713-735, SaveEXRImage in
  * src/image/exr-image.cc): uncompressed FLOAT scanlines, channels R, G, B, A

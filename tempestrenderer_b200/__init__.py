@@ -38,7 +38,7 @@ EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_op
            "svf_synth_btf", "svf_mlp_train_options_default", "svf_mlp_train", "svf_mlp_predict", "svf_mlp_step",
            "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy", "svf_btf_probe", "svf_btf_load", "svf_btf_load_file",
            "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_btf_destroy", "svf_error_maps", "svf_exr_write",
-           "svf_exr_read", "svf_maps_write_exr")
+           "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps", "svf_refit_neighborhood")
 
 
 class SvfError(RuntimeError):
@@ -160,11 +160,15 @@ def load() -> C.CDLL:
         L.svf_exr_write.argtypes = [C.c_char_p, u32, u32, u32, vp]
         L.svf_exr_read.argtypes = [C.c_char_p, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), vp, C.c_size_t]
         L.svf_maps_write_exr.argtypes = [C.c_char_p, u32, u32, C.POINTER(Maps)]
+        L.svf_params_from_maps.argtypes = [C.POINTER(SvbrdfMaps), vp, vp]
+        L.svf_refit_neighborhood.argtypes = [vp, C.POINTER(BtfView), C.POINTER(LsqOptions), vp, vp, C.POINTER(Maps),
+                                             C.POINTER(RunStats)]
         for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
                      "svf_fit_texels", "svf_fit_btfs", "svf_synth_btf", "svf_mlp_train", "svf_mlp_predict",
                      "svf_mlp_step", "svf_mlp_save", "svf_mlp_load", "svf_btf_probe", "svf_btf_load",
                      "svf_btf_load_file", "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_error_maps",
-                     "svf_exr_write", "svf_exr_read", "svf_maps_write_exr"):
+                     "svf_exr_write", "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps",
+                     "svf_refit_neighborhood"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -380,6 +384,29 @@ class Context:
             _check(st)
         return results, list(runs), total
 
+    def refit_neighborhood(self, layout: Layout, samples, width: int, height: int, params, rmse,
+                           sample_type=SVF_SAMPLES_F32, opts: LsqOptions | None = None,
+                           want=("params", "rmse", "diffuse", "specular", "sigma", "basis")):
+        """svbrdffit -j as one GPU pass (svf_refit_neighborhood).  Returns (maps dict, RunStats)."""
+        T = width * height
+        v = BtfView()
+        v.samples = _ptr(samples)
+        v.sample_type = sample_type
+        v.width, v.height = width, height
+        v.layout = C.pointer(layout.desc)
+        p = np.ascontiguousarray(params, np.float32)
+        r = np.ascontiguousarray(rmse, np.float32)
+        shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
+                  "params": (T, 7)}
+        res = {k: np.zeros(shapes[k], np.float32) for k in want}
+        m = Maps()
+        for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params"):
+            setattr(m, k, _ptr(res[k]) if k in res else None)
+        rs = RunStats()
+        _check(self._lib.svf_refit_neighborhood(self.handle, C.byref(v), C.byref(opts or options()), p.ctypes.data,
+                                                r.ctypes.data, C.byref(m), C.byref(rs)))
+        return res, rs
+
     def synth_btf(self, seed: int, mix: int, lights_parabolic, first: int, count: int, samples,
                   sample_type=SVF_SAMPLES_F32, noise: float = 0.01, truth=None):
         lp = np.ascontiguousarray(lights_parabolic, np.float32)
@@ -560,3 +587,15 @@ def maps_write_exr(prefix: str, width: int, height: int, maps: dict) -> None:
             keep[k] = np.ascontiguousarray(maps[k], np.float32)
             setattr(m, k, keep[k].ctypes.data)
     _check(load().svf_maps_write_exr(prefix.encode(), width, height, C.byref(m)))
+
+
+def params_from_maps(diffuse, specular, sigma, basis):
+    """svbrdffit -r: the 7 fit parameters of saved maps (and the colour they carry)."""
+    d, sp, sg, b = (np.ascontiguousarray(m, np.float32) for m in (diffuse, specular, sigma, basis))
+    T = d.shape[0] * (d.shape[1] if d.ndim == 3 else 1)
+    sc = sg.shape[-1]
+    m = SvbrdfMaps(d.ctypes.data, sp.ctypes.data, sg.ctypes.data, sc, b.ctypes.data, T, 1)
+    p = np.zeros((T, 7), np.float32)
+    colour = np.zeros((T, 3), np.float32)
+    _check(load().svf_params_from_maps(C.byref(m), p.ctypes.data, colour.ctypes.data))
+    return p, colour

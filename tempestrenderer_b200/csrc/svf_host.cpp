@@ -2686,6 +2686,149 @@ svf_status svf_error_maps(svf_ctx* ctx, const svf_btf* btf, const svf_svbrdf_map
     return SVF_OK;
 }
 
+svf_status svf_params_from_maps(const svf_svbrdf_maps* maps, float* params, float* colour)
+{
+    if(!maps || !params || !maps->diffuse || !maps->specular || !maps->sigma || !maps->basis)
+        return fail(SVF_EINVAL, "null maps/params");
+    if(maps->sigma_channels != 2 && maps->sigma_channels != 3)
+        return fail(SVF_EINVAL, "sigma_channels %u (2 or 3)", maps->sigma_channels);
+    const uint64_t T = (uint64_t)maps->width * maps->height;
+    const uint32_t sc = maps->sigma_channels;
+    for(uint64_t t = 0; t < T; ++t)
+    {
+        const float* d = maps->diffuse + 3 * t;
+        const float* sp = maps->specular + 3 * t;
+        const float* sg = maps->sigma + sc * t;
+        float* p = params + 7 * t;
+        // RGBToLuminance (spectrum.hh:328-331)
+        const float kd = 0.2126f * d[0] + 0.7152f * d[1] + 0.0722f * d[2];
+        const float ks = 0.2126f * sp[0] + 0.7152f * sp[1] + 0.0722f * sp[2];
+        p[0] = sc == 3 ? sg[0] / sg[2] : sg[0];
+        p[1] = sc == 3 ? sg[1] / sg[2] : sg[1];
+        p[2] = ks;
+        p[3] = kd;
+        svf::quaternion_to_euler(maps->basis + 4 * t, p + 4);
+        if(colour)
+            for(int c = 0; c < 3; ++c)
+                colour[3 * t + c] = sp[c] / ks;   // avg_spec = Specular / specular (pipeline.cc:669)
+    }
+    return SVF_OK;
+}
+
+svf_status svf_refit_neighborhood(svf_ctx* ctx, const svf_btf_view* btf, const svf_lsq_options* lsq,
+                                  const float* params_in, const float* rmse_in, const svf_maps* out,
+                                  svf_run_stats* run)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(!btf || !btf->samples || !btf->layout || !params_in || !rmse_in || !out)
+        return fail(SVF_EINVAL, "null btf/params/rmse/outputs");
+    svf_lsq_options o;
+    svf_lsq_options_default(&o);
+    if(lsq)
+        o = *lsq;
+    SVF_TRY(check_options(&o));
+    if(o.flags & SVF_LSQ_RGB)
+        return fail(SVF_EINVAL, "the neighbourhood refit fits the luminance model (no SVF_LSQ_RGB)");
+    if(btf->sample_type != SVF_SAMPLES_F32 && btf->sample_type != SVF_SAMPLES_F16)
+        return fail(SVF_EINVAL, "unknown sample_type %u", btf->sample_type);
+    const svf_layout_desc* desc = btf->layout;
+    Layout* lay = nullptr;
+    SVF_TRY(get_layout(ctx, desc->lights_parabolic, desc->light_count, &lay));
+    const uint32_t L = lay->L, N = L * L, W = btf->width, H = btf->height;
+    const uint64_t T = (uint64_t)W * H, stride = round_up(N, 8);
+    if(T == 0)
+        return SVF_OK;
+    const size_t texel_bytes = (btf->sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)N;
+    const bool on_device = is_device_pointer(btf->samples);
+    size_t free_b = 0, total_b = 0;
+    SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
+    const size_t per_texel = sizeof(float) * (stride + 3 + 9 * (7 + 7 + 1) + 7 + 1 + 12) + 9 * sizeof(svf_texel_stats) +
+                             (on_device ? 0 : texel_bytes);
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>({ T, (free_b / 2) / per_texel, 1ull << 22 }));
+    DevBuf all, cand, stage;
+    SVF_TRY(all.ensure(sizeof(float) * 8 * T));
+    float* d_params = all.as<float>();
+    float* d_rmse = d_params + 7 * T;
+    SVF_TRY(to_device(ctx, d_params, params_in, sizeof(float) * 7 * T));
+    SVF_TRY(to_device(ctx, d_rmse, rmse_in, sizeof(float) * T));
+    SVF_TRY(ctx->lum.ensure(sizeof(float) * stride * chunk));
+    SVF_TRY(ctx->avg.ensure(sizeof(float) * 3 * chunk));
+    SVF_TRY(cand.ensure(sizeof(float) * 9 * chunk * 15 + sizeof(svf_texel_stats) * 9 * chunk));
+    float* c_init = cand.as<float>();
+    float* c_out = c_init + 63 * chunk;
+    float* c_rmse = c_out + 63 * chunk;
+    svf_texel_stats* c_stats = reinterpret_cast<svf_texel_stats*>(c_rmse + 9 * chunk);
+    SVF_TRY(ctx->maps_buf.ensure(sizeof(float) * (12 + 7 + 1 + 1) * chunk));
+    float* mb = ctx->maps_buf.as<float>();
+    float* sel_params = mb + 12 * chunk;
+    float* sel_rmse = sel_params + 7 * chunk;
+    float* dummy_rmse = sel_rmse + chunk;
+    if(!on_device)
+        SVF_TRY(stage.ensure(texel_bytes * chunk));
+    svf_run_stats all_stats{};
+    std::vector<svf_texel_stats> hs;
+    SVF_TRY(zero_error_flags(ctx));
+    for(uint64_t c0 = 0; c0 < T; c0 += chunk)
+    {
+        const uint64_t n = std::min(chunk, T - c0);
+        const void* samples = static_cast<const char*>(btf->samples) + c0 * texel_bytes;
+        if(!on_device)
+        {
+            SVF_CUDA(cudaMemcpyAsync(stage.p, samples, texel_bytes * n, cudaMemcpyHostToDevice, ctx->stream));
+            samples = stage.p;
+        }
+        SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
+                                       ctx->avg.as<float>(), nullptr, nullptr, ctx->stream));
+        SVF_CUDA(svf::launch_refit_gather(d_params, c0, n, W, H, c_init, ctx->stream));
+        // nine candidate fits per texel in one launch: segment k holds candidate k
+        // of every texel, all reading the texels' own slabs
+        svf::LmSegment seg[9];
+        for(int k = 0; k < 9; ++k)
+            seg[k] = svf::LmSegment{ (uint32_t)(k * n), L, stride, ctx->lum.as<float>(), lay->geo.as<float>() };
+        if(9 * n > 0xffffffffull)
+            return fail(SVF_EINVAL, "internal: refit chunk too large");
+        LmRun r{ nullptr, stride, c_init, c_out, c_rmse, c_stats, nullptr, nullptr, nullptr, nullptr, nullptr, 9 * n,
+                 seg, 9, lay->all_up, false };
+        SVF_TRY(run_lm(ctx, lay, &o, r));
+        SVF_CUDA(svf::launch_refit_select(d_params, d_rmse, c0, n, W, H, c_out, c_rmse, sel_params, sel_rmse, nullptr,
+                                          ctx->stream));
+        // the maps of the selected parameters (a pass without iterations)
+        svf_lsq_options o0 = o;
+        o0.max_iterations = 0;
+        o0.restarts = 0;
+        LmRun m{ ctx->lum.as<float>(), stride, sel_params, sel_params, dummy_rmse, nullptr,
+                 ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n };
+        // out == init is safe: each texel reads its parameters before writing them
+        SVF_TRY(launch_lm(ctx, lay, &o0, m, lm_choice(lay, stride, false)));
+        auto put = [&](void* dst, const void* src, size_t bytes) -> svf_status {
+            if(dst)
+                SVF_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, ctx->stream));
+            return SVF_OK;
+        };
+        SVF_TRY(put(out->params ? out->params + 7 * c0 : nullptr, sel_params, sizeof(float) * 7 * n));
+        SVF_TRY(put(out->rmse ? out->rmse + c0 : nullptr, sel_rmse, sizeof(float) * n));
+        SVF_TRY(put(out->diffuse ? out->diffuse + 3 * c0 : nullptr, mb, sizeof(float) * 3 * n));
+        SVF_TRY(put(out->specular ? out->specular + 3 * c0 : nullptr, mb + 3 * n, sizeof(float) * 3 * n));
+        SVF_TRY(put(out->sigma ? out->sigma + 2 * c0 : nullptr, mb + 6 * n, sizeof(float) * 2 * n));
+        SVF_TRY(put(out->basis ? out->basis + 4 * c0 : nullptr, mb + 8 * n, sizeof(float) * 4 * n));
+        hs.resize(9 * n);
+        SVF_CUDA(cudaMemcpyAsync(hs.data(), c_stats, sizeof(svf_texel_stats) * 9 * n, cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+        all_stats.texels += n;
+        for(const auto& st : hs)
+        {
+            all_stats.iterations += st.iterations;
+            all_stats.jacobians += st.jacobians;
+            all_stats.residuals += st.residuals;
+        }
+    }
+    SVF_TRY(read_error_flag(ctx));
+    if(run)
+        *run = all_stats;
+    return SVF_OK;
+}
+
 void svf_btf_destroy(svf_btf* btf)
 {
     if(!btf)

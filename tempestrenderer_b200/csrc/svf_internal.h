@@ -205,6 +205,16 @@ cudaError_t mlp_targets(const float* p7, uint64_t texels, float* Y, cudaStream_t
 cudaError_t mlp_finish(const float* Yn, uint64_t texels, const float* mean, const float* std, float* p7,
                        cudaStream_t stream);
 
+// ---- neighbourhood refit (svf_kernels.cu) --------------------------------------------
+// cand [9n][7]: candidate k of texel c0 + i at row k*n + i (the 3x3 neighbour's
+// parameters, the texel's own outside the image)
+cudaError_t launch_refit_gather(const float* params, uint64_t c0, uint64_t n, uint32_t width, uint32_t height,
+                                float* cand, cudaStream_t stream);
+// sel_from (optional): 0..8 the winning neighbour, 9 the texel's own parameters
+cudaError_t launch_refit_select(const float* params, const float* rmse, uint64_t c0, uint64_t n, uint32_t width,
+                                uint32_t height, const float* cand_out, const float* cand_rmse, float* sel_params,
+                                float* sel_rmse, uint32_t* sel_from, cudaStream_t stream);
+
 // ---- factored BTF decode (svf_btf.cu) ----------------------------------------------
 
 // Channel c: U_c row lv at u[c] + lv * u_row[c] elements, SxV_c row col at

@@ -533,4 +533,84 @@ cudaError_t launch_synth(uint32_t seed, uint32_t mix, const float* lp, uint32_t 
     return cudaGetLastError();
 }
 
+// ---- neighbourhood refit (svbrdffit -j, svbrdf-fitting.cc:123-178) ----------------
+
+namespace
+{
+
+// Candidate k (0..8, the 3x3 neighbourhood row by row) of texel c0 + i starts
+// from the neighbour's parameters; a neighbour outside the image gives the
+// texel's own (the candidate is then ignored).
+__global__ void refit_gather_kernel(const float* __restrict__ params, uint64_t c0, uint64_t n, uint32_t width,
+                                    uint32_t height, float* __restrict__ cand)
+{
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if(j >= 9 * n)
+        return;
+    const uint64_t k = j / n, i = j - k * n, t = c0 + i;
+    const int64_t y = (int64_t)(t / width), x = (int64_t)(t - (uint64_t)y * width);
+    const int64_t ny = y + (int64_t)(k / 3) - 1, nx = x + (int64_t)(k % 3) - 1;
+    const bool in = ny >= 0 && ny < height && nx >= 0 && nx < width;
+    const uint64_t src = in ? (uint64_t)ny * width + (uint64_t)nx : t;
+    for(int p = 0; p < 7; ++p)
+        cand[7 * j + p] = params[7 * src + p];
+}
+
+// The texel keeps its parameters unless a candidate's RMSE is lower; candidates
+// are taken in neighbourhood order with a strict comparison, as the reference's
+// loop updates best_rmse.
+__global__ void refit_select_kernel(const float* __restrict__ params, const float* __restrict__ rmse, uint64_t c0,
+                                    uint64_t n, uint32_t width, uint32_t height, const float* __restrict__ cand_out,
+                                    const float* __restrict__ cand_rmse, float* __restrict__ sel_params,
+                                    float* __restrict__ sel_rmse, uint32_t* __restrict__ sel_from)
+{
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if(i >= n)
+        return;
+    const uint64_t t = c0 + i;
+    const int64_t y = (int64_t)(t / width), x = (int64_t)(t - (uint64_t)y * width);
+    float best = rmse[t];
+    int from = -1;
+    for(int k = 0; k < 9; ++k)
+    {
+        const int64_t ny = y + k / 3 - 1, nx = x + k % 3 - 1;
+        if(ny < 0 || ny >= height || nx < 0 || nx >= width)
+            continue;
+        const float r = cand_rmse[k * n + i];
+        if(r < best)   // (NaN never wins)
+        {
+            best = r;
+            from = k;
+        }
+    }
+    const float* src = from < 0 ? params + 7 * t : cand_out + 7 * ((uint64_t)from * n + i);
+    for(int p = 0; p < 7; ++p)
+        sel_params[7 * i + p] = src[p];
+    sel_rmse[i] = best;
+    if(sel_from)
+        sel_from[i] = (uint32_t)(from < 0 ? 9 : from);
+}
+
+} // namespace
+
+cudaError_t launch_refit_gather(const float* params, uint64_t c0, uint64_t n, uint32_t width, uint32_t height,
+                                float* cand, cudaStream_t stream)
+{
+    if(n == 0)
+        return cudaSuccess;
+    refit_gather_kernel<<<(unsigned)((9 * n + 255) / 256), 256, 0, stream>>>(params, c0, n, width, height, cand);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refit_select(const float* params, const float* rmse, uint64_t c0, uint64_t n, uint32_t width,
+                                uint32_t height, const float* cand_out, const float* cand_rmse, float* sel_params,
+                                float* sel_rmse, uint32_t* sel_from, cudaStream_t stream)
+{
+    if(n == 0)
+        return cudaSuccess;
+    refit_select_kernel<<<(unsigned)((n + 255) / 256), 256, 0, stream>>>(params, rmse, c0, n, width, height, cand_out,
+                                                                       cand_rmse, sel_params, sel_rmse, sel_from);
+    return cudaGetLastError();
+}
+
 } // namespace svf

@@ -35,6 +35,41 @@ inline void sincos_tan(float omega, float* s, float* c)
 
 } // namespace
 
+void quaternion_to_euler(const float* q, float* euler)
+{
+    // ToMatrix3 (quaternion.hh:122-139) then Matrix3::decompose
+    // (matrix3.hh:311-332); m[c][r] is column c, row r (Elements[c][r])
+    const float x = q[0], y = q[1], z = q[2], w = q[3];
+    const float xx = x * x, xy = x * y, xz = x * z, xw = x * w, yy = y * y, yz = y * z, yw = y * w, zz = z * z,
+                zw = z * w;
+    const float m[3][3] = { { 1.0f - 2.0f * (yy + zz), 2.0f * (xy + zw), 2.0f * (xz - yw) },
+                            { 2.0f * (xy - zw), 1.0f - 2.0f * (xx + zz), 2.0f * (yz + xw) },
+                            { 2.0f * (xz + yw), 2.0f * (yz - xw), 1.0f - 2.0f * (xx + yy) } };
+    float s[3];
+    for(int c = 0; c < 3; ++c)
+        s[c] = sqrtf(m[c][0] * m[c][0] + m[c][1] * m[c][1] + m[c][2] * m[c][2]);
+    const float pi = 3.141592f;   // MathPi (functions.hh:55)
+    const float m20 = m[2][0] / s[2];
+    if(m20 >= 0.9999f)
+    {
+        euler[0] = 0.0f;
+        euler[1] = pi * 0.5f;
+        euler[2] = atan2f(m[0][1], m[1][1]);
+    }
+    else if(m20 <= -0.9999f)
+    {
+        euler[0] = 0.0f;
+        euler[1] = -pi * 0.5f;
+        euler[2] = atan2f(m[0][1], m[1][1]);
+    }
+    else
+    {
+        euler[0] = atan2f(-m[2][1], m[2][2]);
+        euler[1] = asinf(m20);
+        euler[2] = atan2f(-m[1][0] / s[1], m[0][0] / s[0]);
+    }
+}
+
 void angles_to_cartesian(float theta, float phi, float* w)
 {
     // SphereToCartesianCoordinates (vector3.hh:375-382)

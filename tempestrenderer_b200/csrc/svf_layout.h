@@ -11,6 +11,9 @@ namespace svf
 // computes them.
 void angles_to_cartesian(float theta, float phi, float* w);
 void angles_to_parabolic(float theta, float phi, float* out);
+// Euler angles of a quaternion's rotation as the reference obtains them
+// (ToMatrix3, then Matrix3::decompose).
+void quaternion_to_euler(const float* q, float* euler);
 // ParabolicToCartesianCoordinates in the reference's operation order.
 void parabolic_to_cartesian_ref(float px, float py, float* w);
 

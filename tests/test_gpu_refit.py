@@ -1,0 +1,86 @@
+"""The neighbourhood refit on the GPU (svf_refit_neighborhood, svbrdffit -j):
+
+* every texel ends with exactly what the rule gives when its nine candidate fits
+  are run one by one with svf_fit_texels (SVF_INIT_GIVEN from each 3x3
+  neighbour's parameters, clipped to the image): the first candidate in row
+  order whose RMSE is below the texel's current one, else the texel's own --
+  bit for bit, since a texel's fit does not depend on the launch it runs in;
+* no texel gets worse, and texels whose first fit was spoiled recover from
+  their neighbours;
+* svbrdffit -r: a refit from saved maps (svf_params_from_maps + SVF_INIT_GIVEN)
+  lands where the first fit ended."""
+import numpy as np
+import pytest
+
+import tempestrenderer_b200 as svf
+
+pytestmark = pytest.mark.gpu
+
+
+def _layout(golden):
+    m = golden["mesh"]
+    return svf.Layout(m["lights_parabolic"], m["triangles"], m["edges"], m["edge_angles"])
+
+
+def _neighbour_params(params, W, H, k):
+    T = W * H
+    t = np.arange(T)
+    y, x = t // W, t % W
+    ny, nx = y + k // 3 - 1, x + k % 3 - 1
+    ok = (ny >= 0) & (ny < H) & (nx >= 0) & (nx < W)
+    src = np.where(ok, ny * W + nx, t)
+    return params[src], ok
+
+
+def test_refit_selects_like_the_candidate_fits(gpu_ctx, golden):
+    import torch
+
+    lay = _layout(golden)
+    W, H = 24, 16
+    T = W * H
+    s = torch.empty((T, 81 * 81, 3), dtype=torch.float32, device="cuda")
+    gpu_ctx.synth_btf(808, 1, lay.lights_parabolic, 0, T, s)
+    first, _ = gpu_ctx.fit_texels(lay, s, W, H, want=("params", "rmse"))
+    params, rmse = first["params"].copy(), first["rmse"].copy()
+    # spoil a quarter of the texels: a flat, wrongly oriented guess fitted for 2 steps
+    bad = np.random.default_rng(1).random(T) < 0.25
+    poor = np.tile(np.array([0.5, 0.5, 0.1, 0.0, 1.0, 0.5, 0.0], np.float32), (T, 1))
+    spoiled, _ = gpu_ctx.fit_texels(lay, s, W, H, opts=svf.options(max_iterations=2), init=poor,
+                                    want=("params", "rmse"))
+    params[bad], rmse[bad] = spoiled["params"][bad], spoiled["rmse"][bad]
+
+    out, rs = gpu_ctx.refit_neighborhood(lay, s, W, H, params, rmse)
+    assert rs.texels == T
+
+    # the rule, candidate by candidate
+    best, best_p = rmse.copy(), params.copy()
+    for k in range(9):
+        init, ok = _neighbour_params(params, W, H, k)
+        cand, _ = gpu_ctx.fit_texels(lay, s, W, H, init=init, want=("params", "rmse"))
+        take = ok & (cand["rmse"] < best)
+        best[take], best_p[take] = cand["rmse"][take], cand["params"][take]
+    np.testing.assert_array_equal(out["rmse"], best)
+    np.testing.assert_array_equal(out["params"], best_p)
+    assert (out["rmse"] <= rmse).all()
+    # spoiled texels recover: at most 1 % above their first fit on the median
+    assert np.median(out["rmse"][bad] / first["rmse"][bad]) <= 1.01
+    # the maps are those of the selected parameters
+    again, _ = gpu_ctx.fit_texels(lay, s, W, H, opts=svf.options(max_iterations=0), init=out["params"],
+                                  want=("diffuse", "specular", "sigma", "basis"))
+    for k in ("diffuse", "specular", "sigma", "basis"):
+        np.testing.assert_array_equal(out[k], again[k], err_msg=k)
+
+
+def test_refit_from_saved_maps(gpu_ctx, oracle_lib, golden):
+    """svbrdffit -r: the first fit's maps converted back and refitted end where the
+    first fit ended (LM restarts at its own minimum)."""
+    lay = _layout(golden)
+    lp = lay.lights_parabolic
+    T = 32
+    rgb = np.stack([oracle_lib.synth_render(61, x, oracle_lib.synth_truth(61, 1, x), lp) for x in range(T)])
+    first, _ = gpu_ctx.fit_texels(lay, rgb, T, 1, want=("diffuse", "specular", "sigma", "basis", "rmse"))
+    params, colour = svf.params_from_maps(first["diffuse"], first["specular"], first["sigma"], first["basis"])
+    re, rs = gpu_ctx.fit_texels(lay, rgb, T, 1, init=params, want=("rmse",))
+    assert rs.failed_texels == 0
+    assert np.median(re["rmse"] / first["rmse"]) <= 1.0 + 1e-4
+    assert (re["rmse"] <= first["rmse"] * 1.01 + 1e-7).mean() >= 0.9
