@@ -394,8 +394,9 @@ class Context:
         v.sample_type = sample_type
         v.width, v.height = width, height
         v.layout = C.pointer(layout.desc)
-        p = np.ascontiguousarray(params, np.float32)
-        r = np.ascontiguousarray(rmse, np.float32)
+        # numpy arrays or torch tensors (host or device)
+        p = params if hasattr(params, "data_ptr") else np.ascontiguousarray(params, np.float32)
+        r = rmse if hasattr(rmse, "data_ptr") else np.ascontiguousarray(rmse, np.float32)
         shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
                   "params": (T, 7)}
         res = {k: np.zeros(shapes[k], np.float32) for k in want}
@@ -403,8 +404,8 @@ class Context:
         for k in ("diffuse", "specular", "sigma", "basis", "rmse", "params"):
             setattr(m, k, _ptr(res[k]) if k in res else None)
         rs = RunStats()
-        _check(self._lib.svf_refit_neighborhood(self.handle, C.byref(v), C.byref(opts or options()), p.ctypes.data,
-                                                r.ctypes.data, C.byref(m), C.byref(rs)))
+        _check(self._lib.svf_refit_neighborhood(self.handle, C.byref(v), C.byref(opts or options()), _ptr(p),
+                                                _ptr(r), C.byref(m), C.byref(rs)))
         return res, rs
 
     def synth_btf(self, seed: int, mix: int, lights_parabolic, first: int, count: int, samples,
