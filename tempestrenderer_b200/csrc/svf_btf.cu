@@ -56,7 +56,11 @@ __device__ __forceinline__ double madd(double sum, double u, double v) { return 
 template <typename T, typename Acc, int TX>
 __global__ void __launch_bounds__(kThreads) btf_decode_kernel(BtfDecodeArgs a, uint64_t t_begin)
 {
-    __shared__ Acc s_sxv[kChunk][TX];
+    // rows padded by 4: the staging writes of one warp (32 components of one
+    // texel) spread over 8 banks, and rows stay 16-byte aligned for the
+    // vector broadcasts of the inner loop
+    __shared__ __align__(16) Acc s_sxv[kChunk][TX + 4];
+    __shared__ float s_out[kThreads / 32][96];   // one texel's 32 pairs x RGB per warp
     __shared__ Acc s_u[kChunk][kThreads + 1];
     __shared__ uint64_t s_col[TX];   // file column of each texel (after the row flip)
     const uint32_t lv0 = blockIdx.x * kThreads, lv = lv0 + threadIdx.x;
@@ -109,15 +113,16 @@ __global__ void __launch_bounds__(kThreads) btf_decode_kernel(BtfDecodeArgs a, u
             }
         }
     }
-    if(lv >= a.N)
-        return;
     const float eps = 1e-5f;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t lv_w = lv0 + warp * 32;   // the warp's first pair
+    const uint32_t nvalid = lv_w >= a.N ? 0u : (a.N - lv_w < 32u ? a.N - lv_w : 32u);
 #pragma unroll
     for(int j = 0; j < TX; ++j)
     {
         const uint64_t t = t0 + j;
         if(t >= t_end)
-            break;
+            break;   // (the same for the whole CTA)
         float r = (float)acc[0][j], g = (float)acc[1][j], b = (float)acc[2][j];
         if(a.color_model == 11)
         {
@@ -144,21 +149,26 @@ __global__ void __launch_bounds__(kThreads) btf_decode_kernel(BtfDecodeArgs a, u
             g = __fsub_rn(expf(g), eps);
             b = __fsub_rn(expf(b), eps);
         }
-        const uint64_t o = ((t - a.first) * a.N + lv) * 3;
+        // the warp's 32 samples are 96 consecutive values: stage them and store
+        // them lane-consecutive (each store instruction covers 32 neighbours)
+        s_out[warp][3 * lane] = r;
+        s_out[warp][3 * lane + 1] = g;
+        s_out[warp][3 * lane + 2] = b;
+        __syncwarp();
+        const uint64_t o = ((t - a.first) * a.N + lv_w) * 3;
         if(a.out_type == SVF_SAMPLES_F16)
         {
             __half* out = static_cast<__half*>(a.out) + o;
-            out[0] = __float2half_rn(r);
-            out[1] = __float2half_rn(g);
-            out[2] = __float2half_rn(b);
+            for(uint32_t e = lane; e < 3 * nvalid; e += 32)
+                out[e] = __float2half_rn(s_out[warp][e]);
         }
         else
         {
             float* out = static_cast<float*>(a.out) + o;
-            out[0] = r;
-            out[1] = g;
-            out[2] = b;
+            for(uint32_t e = lane; e < 3 * nvalid; e += 32)
+                out[e] = s_out[warp][e];
         }
+        __syncwarp();
     }
 }
 
