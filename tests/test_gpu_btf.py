@@ -62,8 +62,10 @@ def _ring_file(oracle, fmt, ds, ks, W, H, seed, cm=0, drr=0, scale=0.2):
     return planes, oracle.btf_file_bytes(tp, W, H, planes, fmt=fmt, data_size=ds, color_model=cm, drr=drr)
 
 
+# (150 components: five 32-component chunks, the last one partial)
 @pytest.mark.parametrize("fmt,ds,ks,drr", [("DFMF", 2, (24, 16, 40), 0), ("DFMF", 4, (33, 8, 20), 0),
-                                           ("FMF1", 2, (28,), 1), ("DFMF", 8, (12, 12, 12), 0)])
+                                           ("FMF1", 2, (28,), 1), ("DFMF", 8, (12, 12, 12), 0),
+                                           ("DFMF", 4, (150, 40, 9), 0)])
 def test_ring81_decode_matches_oracle(gpu_ctx, oracle_lib, fmt, ds, ks, drr):
     import torch
 
