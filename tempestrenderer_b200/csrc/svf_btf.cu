@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(kThreads) btf_decode_kernel(BtfDecodeArgs a, u
     __shared__ float s_out[kThreads / 32][96];   // one texel's 32 pairs x RGB per warp
     __shared__ Acc s_u[kChunk][kThreads + 1];
     __shared__ uint64_t s_col[TX];   // file column of each texel (after the row flip)
-    const uint32_t lv0 = blockIdx.x * kThreads, lv = lv0 + threadIdx.x;
+    const uint32_t lv0 = blockIdx.x * kThreads;
     const uint64_t t0 = t_begin + (uint64_t)blockIdx.y * TX;
     const uint64_t t_end = a.first + a.count;
     if(threadIdx.x < TX)
