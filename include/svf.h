@@ -419,6 +419,14 @@ svf_status svf_refit_neighborhood(svf_ctx* ctx, const svf_btf_view* btf, const s
                                   const float* params_in, const float* rmse_in, const svf_maps* out,
                                   svf_run_stats* run);
 
+/* Rendered BTF of SVBRDF maps: samples [texels][L*L][3] (lv = view * L + light;
+ * F32 or F16, device or host) of the SGGX surface BRDF (SGGXMicroFlakeSurfaceBRDF,
+ * ggx-models-impl.hh:476-552) with each texel's map values as material, as
+ * svbrdf-error-tool sets it up (fresnel: refractive index, 1 for none).  The
+ * inverse of the fit: fitting the rendered BTF recovers the maps. */
+svf_status svf_render_btf(svf_ctx* ctx, const float* lights_parabolic, uint32_t light_count,
+                          const svf_svbrdf_maps* maps, float fresnel, uint32_t sample_type, void* samples);
+
 /* OpenEXR maps ----------------------------------------------------------------------
  * svbrdffit's output files (svbrdf-fitting.cc:713-735, SaveEXRImage in
  * src/image/exr-image.cc): uncompressed FLOAT scanlines, channels R, G, B, A

@@ -38,7 +38,8 @@ EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_op
            "svf_synth_btf", "svf_mlp_train_options_default", "svf_mlp_train", "svf_mlp_predict", "svf_mlp_step",
            "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy", "svf_btf_probe", "svf_btf_load", "svf_btf_load_file",
            "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_btf_destroy", "svf_error_maps", "svf_exr_write",
-           "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps", "svf_refit_neighborhood")
+           "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps", "svf_refit_neighborhood",
+           "svf_render_btf")
 
 
 class SvfError(RuntimeError):
@@ -161,6 +162,7 @@ def load() -> C.CDLL:
         L.svf_exr_read.argtypes = [C.c_char_p, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), vp, C.c_size_t]
         L.svf_maps_write_exr.argtypes = [C.c_char_p, u32, u32, C.POINTER(Maps)]
         L.svf_params_from_maps.argtypes = [C.POINTER(SvbrdfMaps), vp, vp]
+        L.svf_render_btf.argtypes = [vp, vp, u32, C.POINTER(SvbrdfMaps), f32, u32, vp]
         L.svf_refit_neighborhood.argtypes = [vp, C.POINTER(BtfView), C.POINTER(LsqOptions), vp, vp, C.POINTER(Maps),
                                              C.POINTER(RunStats)]
         for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
@@ -168,7 +170,7 @@ def load() -> C.CDLL:
                      "svf_mlp_step", "svf_mlp_save", "svf_mlp_load", "svf_btf_probe", "svf_btf_load",
                      "svf_btf_load_file", "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_error_maps",
                      "svf_exr_write", "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps",
-                     "svf_refit_neighborhood"):
+                     "svf_refit_neighborhood", "svf_render_btf"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -407,6 +409,19 @@ class Context:
         _check(self._lib.svf_refit_neighborhood(self.handle, C.byref(v), C.byref(opts or options()), _ptr(p),
                                                 _ptr(r), C.byref(m), C.byref(rs)))
         return res, rs
+
+    def render_btf(self, lights_parabolic, diffuse, specular, sigma, basis, fresnel: float = 1.0,
+                   sample_type=SVF_SAMPLES_F32, out=None):
+        """Samples [texels][L*L][3] of SVBRDF maps ([texels][3|3|2or3|4]) -- svf_render_btf."""
+        lp = np.ascontiguousarray(lights_parabolic, np.float32)
+        d, sp, sg, b = (np.ascontiguousarray(m, np.float32).reshape(-1, m.shape[-1]) for m in
+                        (np.asarray(diffuse), np.asarray(specular), np.asarray(sigma), np.asarray(basis)))
+        T, L = d.shape[0], lp.shape[0]
+        m = SvbrdfMaps(d.ctypes.data, sp.ctypes.data, sg.ctypes.data, sg.shape[1], b.ctypes.data, T, 1)
+        if out is None:
+            out = np.zeros((T, L * L, 3), np.float16 if sample_type == SVF_SAMPLES_F16 else np.float32)
+        _check(self._lib.svf_render_btf(self.handle, lp.ctypes.data, L, C.byref(m), fresnel, sample_type, _ptr(out)))
+        return out
 
     def synth_btf(self, seed: int, mix: int, lights_parabolic, first: int, count: int, samples,
                   sample_type=SVF_SAMPLES_F32, noise: float = 0.01, truth=None):

@@ -1,5 +1,6 @@
 // svf_error.cu - the error of fitted SVBRDF maps against a BTF, per texel
-// (svbrdf-error-tool, tools/svbrdf-error-tool/svbrdf-error-tool.cc:88-250).
+// (svbrdf-error-tool, tools/svbrdf-error-tool/svbrdf-error-tool.cc:88-250),
+// and the rendered BTF of SVBRDF maps (the same BRDF written out).
 //
 // For texel t the map values give the material (diffuse and specular RGB, the
 // SGGX scales, the basis quaternion; Fresnel 1) and the SGGX surface BRDF is
@@ -228,6 +229,87 @@ __global__ void __launch_bounds__(kThreads) error_kernel(ErrorArgs a)
 }
 
 } // namespace
+
+// Rendered BTF: texel t's samples [L^2][3] from its map values (the same
+// material set-up and BRDF as the error kernel), lv = view * L + light.
+__global__ void __launch_bounds__(kThreads) render_kernel(RenderArgs a)
+{
+    extern __shared__ float smem[];
+    const uint32_t L = a.L;
+    DirEntry* tab = reinterpret_cast<DirEntry*>(smem);
+    float* dirs = reinterpret_cast<float*>(tab + L);
+    __shared__ ParamSet ps;
+    const uint64_t t = blockIdx.x;
+    float kd[3], ks[3];
+    for(int c = 0; c < 3; ++c)
+    {
+        kd[c] = a.diffuse[3 * t + c];
+        ks[c] = a.specular[3 * t + c];
+    }
+    if(threadIdx.x == 0)
+    {
+        float p[12];
+        float sx = a.sigma[a.sigma_channels * t], sy = a.sigma[a.sigma_channels * t + 1];
+        if(a.sigma_channels == 3)
+        {
+            const float sz = a.sigma[3 * t + 2];
+            sx = sx / sz;
+            sy = sy / sz;
+        }
+        p[6] = sx;
+        p[7] = sy;
+        for(int k = 0; k < 4; ++k)
+            p[8 + k] = a.basis[4 * t + k];
+        make_param_set_rgb(p, ps);
+    }
+    __syncthreads();
+    for(uint32_t d = threadIdx.x; d < L; d += kThreads)
+    {
+        const float wx = a.geo[d], wy = a.geo[L + d], wz = a.geo[2 * L + d];
+        make_dir_entry(ps, wx, wy, wz, tab[d]);
+        dirs[3 * d] = wx;
+        dirs[3 * d + 1] = wy;
+        dirs[3 * d + 2] = wz;
+    }
+    __syncthreads();
+    for(uint32_t lv = threadIdx.x; lv < L * L; lv += kThreads)
+    {
+        const uint32_t light = lv % L, view = lv / L;
+        const DirEntry& li = tab[light];
+        const DirEntry& vo = tab[view];
+        const float* wi = dirs + 3 * light;
+        const float* wo = dirs + 3 * view;
+        const float W0 = wi[0] + wo[0], W1 = wi[1] + wo[1], W2 = wi[2] + wo[2];
+        const float g = W0 * W0 + W1 * W1 + W2 * W2;
+        const float s0 = li.a[0] + vo.a[0], s1 = li.a[1] + vo.a[1], s2 = li.a[2] + vo.a[2];
+        const float Q = ps.u * s0 * s0 + ps.v * s1 * s1 + s2 * s2;
+        const float S = li.sp + vo.sp;
+        const float QQS = Q * Q * S;
+        const float F = a.fresnel == 1.0f ? 1.0f : fresnel_factor(a.fresnel, wi, wo);
+        const float spec = QQS > 0.0f ? ps.kspec * vo.kv * li.up * F * g * g / QQS : 0.0f;
+        const float diff = vo.up * li.kdc;
+        const uint64_t o = (t * L * L + lv) * 3;
+        for(int c = 0; c < 3; ++c)
+        {
+            const float f = kd[c] * diff + ks[c] * spec;
+            if(a.sample_type == SVF_SAMPLES_F16)
+                static_cast<__half*>(a.out)[o + c] = __float2half_rn(f);
+            else
+                static_cast<float*>(a.out)[o + c] = f;
+        }
+    }
+}
+
+cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream)
+{
+    if(a.count == 0)
+        return cudaSuccess;
+    if(a.count > 0x7fffffffull)
+        return cudaErrorInvalidValue;
+    const size_t smem = (sizeof(DirEntry) + 3 * sizeof(float)) * a.L;
+    render_kernel<<<(unsigned)a.count, kThreads, smem, stream>>>(a);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_error(const ErrorArgs& a, cudaStream_t stream)
 {

@@ -2686,6 +2686,51 @@ svf_status svf_error_maps(svf_ctx* ctx, const svf_btf* btf, const svf_svbrdf_map
     return SVF_OK;
 }
 
+svf_status svf_render_btf(svf_ctx* ctx, const float* lp, uint32_t L, const svf_svbrdf_maps* maps, float fresnel,
+                          uint32_t sample_type, void* samples)
+{
+    SVF_TRY(check_ctx(ctx));
+    if(!lp || !maps || !samples || !maps->diffuse || !maps->specular || !maps->sigma || !maps->basis)
+        return fail(SVF_EINVAL, "null lights/maps/samples");
+    if(maps->sigma_channels != 2 && maps->sigma_channels != 3)
+        return fail(SVF_EINVAL, "sigma_channels %u (2 or 3)", maps->sigma_channels);
+    if(sample_type != SVF_SAMPLES_F32 && sample_type != SVF_SAMPLES_F16)
+        return fail(SVF_EINVAL, "unknown sample_type %u", sample_type);
+    if(!(fresnel >= 1.0f))
+        return fail(SVF_EINVAL, "refractive index %g (>= 1)", fresnel);
+    Layout* lay = nullptr;
+    SVF_TRY(get_layout(ctx, lp, L, &lay));
+    const uint64_t T = (uint64_t)maps->width * maps->height, N = (uint64_t)L * L;
+    const uint32_t sc = maps->sigma_channels;
+    const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * N;
+    const bool out_dev = is_device_pointer(samples);
+    const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(T, (size_t(1) << 30) / texel_bytes));
+    DevBuf md, buf;
+    SVF_TRY(md.ensure(sizeof(float) * chunk * (3 + 3 + sc + 4)));
+    if(!out_dev)
+        SVF_TRY(buf.ensure(texel_bytes * chunk));
+    float* d_diff = md.as<float>();
+    float* d_spec = d_diff + 3 * chunk;
+    float* d_sig = d_spec + 3 * chunk;
+    float* d_basis = d_sig + sc * chunk;
+    for(uint64_t c0 = 0; c0 < T; c0 += chunk)
+    {
+        const uint64_t n = std::min(chunk, T - c0);
+        SVF_TRY(to_device(ctx, d_diff, maps->diffuse + 3 * c0, sizeof(float) * 3 * n));
+        SVF_TRY(to_device(ctx, d_spec, maps->specular + 3 * c0, sizeof(float) * 3 * n));
+        SVF_TRY(to_device(ctx, d_sig, maps->sigma + sc * c0, sizeof(float) * sc * n));
+        SVF_TRY(to_device(ctx, d_basis, maps->basis + 4 * c0, sizeof(float) * 4 * n));
+        void* out = out_dev ? static_cast<char*>(samples) + c0 * texel_bytes : buf.p;
+        svf::RenderArgs a{ L, lay->geo.as<float>(), n, d_diff, d_spec, d_sig, d_basis, sc, fresnel, sample_type, out };
+        SVF_CUDA(svf::launch_render(a, ctx->stream));
+        if(!out_dev)
+            SVF_CUDA(cudaMemcpyAsync(static_cast<char*>(samples) + c0 * texel_bytes, buf.p, texel_bytes * n,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+        SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    }
+    return SVF_OK;
+}
+
 svf_status svf_params_from_maps(const svf_svbrdf_maps* maps, float* params, float* colour)
 {
     if(!maps || !params || !maps->diffuse || !maps->specular || !maps->sigma || !maps->basis)

@@ -251,4 +251,17 @@ struct ErrorArgs
 };
 cudaError_t launch_error(const ErrorArgs& a, cudaStream_t stream);
 
+struct RenderArgs
+{
+    uint32_t L;
+    const float* geo;          // [3][L]
+    uint64_t count;            // texels
+    const float *diffuse, *specular, *sigma, *basis;   // device maps
+    uint32_t sigma_channels;
+    float fresnel;             // refractive index (1: no Fresnel term)
+    uint32_t sample_type;
+    void* out;                 // device [count][L^2][3]
+};
+cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream);
+
 } // namespace svf

@@ -8,7 +8,9 @@
 * no texel gets worse, and texels whose first fit was spoiled recover from
   their neighbours;
 * svbrdffit -r: a refit from saved maps (svf_params_from_maps + SVF_INIT_GIVEN)
-  lands where the first fit ended."""
+  lands where the first fit ended;
+* the rendered BTF of maps (svf_render_btf) is the BRDF of the maps, and a fit
+  of it recovers them."""
 import numpy as np
 import pytest
 
@@ -84,3 +86,31 @@ def test_refit_from_saved_maps(gpu_ctx, oracle_lib, golden):
     assert rs.failed_texels == 0
     assert np.median(re["rmse"] / first["rmse"]) <= 1.0 + 1e-4
     assert (re["rmse"] <= first["rmse"] * 1.01 + 1e-7).mean() >= 0.9
+
+
+def test_render_btf_and_round_trip(gpu_ctx, oracle_lib, golden):
+    """svf_render_btf: the SGGX surface BRDF of each texel's maps, against the FP64
+    oracle per channel (RMS relative 1e-5); scale maps with a third channel are
+    divided by it; fitting the rendered BTF in RGB mode recovers the maps' BRDF
+    (RMSE at the FP16 staging floor)."""
+    lay = _layout(golden)
+    lp = lay.lights_parabolic
+    T = 12
+    truths = [oracle_lib.synth_truth(77, 1, x) for x in range(T)]
+    diffuse = np.array([t.kd[:] for t in truths], np.float32)
+    specular = np.array([t.ks[:] for t in truths], np.float32)
+    sigma = np.array([t.sigma[:] for t in truths], np.float32)
+    basis = np.array([t.quat[:] for t in truths], np.float32)
+    out = gpu_ctx.render_btf(lp, diffuse, specular, sigma, basis)
+    for x in range(T):
+        e = np.array(truths[x].euler[:], np.float64)
+        for c in range(3):
+            _, f64 = oracle_lib.brdf_all(np.array([sigma[x, 0], sigma[x, 1], specular[x, c], diffuse[x, c], *e]), lp)
+            err = np.sqrt(np.mean((out[x, :, c] - f64) ** 2)) / np.sqrt(np.mean(f64 ** 2))
+            assert err < 1e-5, (x, c, err)
+    sig3 = np.concatenate([sigma * 3.0, np.full((T, 1), 3.0, np.float32)], 1)
+    np.testing.assert_allclose(gpu_ctx.render_btf(lp, diffuse, specular, sig3, basis), out, rtol=1e-6, atol=1e-8)
+    fit, rs = gpu_ctx.fit_texels(lay, out, T, 1, opts=svf.options(rgb=True), want=("rmse",))
+    assert rs.failed_texels == 0
+    peak = np.abs(out).max(axis=(1, 2))
+    assert np.median(fit["rmse"] / peak) < 1e-3
