@@ -226,6 +226,10 @@ typedef struct svf_fit_options
                                          near a minimum where the full damping takes steps below
                                          BreakOnSmallStep and ends the fit early.  No reference
                                          counterpart. */
+    float           mlp_fallback;  /* SVF_INIT_MLP, luminance fit, svf_fit_texels: texels whose RMSE
+                                      exceeds this fraction of their luminance slice's RMS are fitted
+                                      from the default guess as well, and keep the lower RMSE (the
+                                      plain-LM fallback); 0: off */
 } svf_fit_options;
 
 /* The five output maps of svbrdffit (svbrdf-fitting.cc:713-735, values as
@@ -264,7 +268,8 @@ typedef struct svf_run_stats
     double   ms_ndf;            /* the NDF GEMM of the default initial guess (part of ms_init) */
     uint32_t graph;             /* svf_fit_texels: 0 launched directly, 1 recorded into a CUDA graph
                                    and launched, 2 replayed (a repeat of the previous call) */
-    uint32_t reserved;
+    uint32_t fallback_texels;   /* SVF_INIT_MLP with mlp_fallback: texels fitted from the default guess
+                                   as well (svf_fit_texels) */
 } svf_run_stats;
 
 svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,
@@ -286,12 +291,17 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
 /* Learned initial guess -------------------------------------------------------------
  * No counterpart in the reference, whose only initial guess is the NDF -> PCA ->
  * SGGX projection pipeline (svbrdf-fitting-pipeline.cc:350-660).  A small MLP
- * (96 -> 256 -> 256 -> 10, GELU) maps the log RGB samples of 32 fixed direction
- * pairs of a texel to the luminance fit's parameters; it is trained on seeded
- * synthetic texels that the plain LM, started from the reference's default
- * guess, has fitted.  SVF_INIT_MLP then starts LM from its prediction: the fit
- * skips the NDF pipeline, and its result is judged against the plain LM's
- * residual.  Inference uses BF16 weights with FP32 accumulation. */
+ * (96 -> 256 -> 256 -> 8, GELU) maps 96 log-scaled features of a texel (32
+ * fixed direction pairs x RGB, or 64 half-vector bins + 32 pairs of its
+ * luminance) to the luminance fit's parameters, as log S (the SGGX matrix's
+ * logarithm, 6 values), log ks, log kd; it is trained on seeded synthetic texels
+ * that the plain LM, started from the reference's default guess, has fitted.
+ * SVF_INIT_MLP then starts LM from its prediction: the fit skips the NDF
+ * pipeline, and its result is judged against the plain LM's residual.
+ * Inference uses BF16 weights with FP32 accumulation. */
+#define SVF_MLP_FEATURES_PAIRS_RGB 0u   /* 32 fixed direction pairs x RGB, log-scaled */
+#define SVF_MLP_FEATURES_BINS      1u   /* 64 half-vector bins of the luminance slab + 32 pairs' luminance */
+
 typedef struct svf_mlp_train_options
 {
     uint32_t texels;          /* synthetic training texels (default 1 << 20) */
@@ -300,6 +310,7 @@ typedef struct svf_mlp_train_options
     uint32_t batch;           /* texels per Adam step (default 4096) */
     float    lr;              /* Adam step size (default 1e-3, cosine-decayed to 5% of it) */
     uint32_t max_iterations;  /* of the LM that makes the targets (default 1024) */
+    uint32_t features;        /* SVF_MLP_FEATURES_* (default SVF_MLP_FEATURES_BINS) */
 } svf_mlp_train_options;
 
 void       svf_mlp_train_options_default(svf_mlp_train_options* o);

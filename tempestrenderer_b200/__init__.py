@@ -30,6 +30,7 @@ SVF_LSQ_RGB = 1 << 8
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
 SVF_ERROR_PAIRWISE, SVF_ERROR_MAX_VIEW = 0, 1
+SVF_MLP_FEATURES_PAIRS_RGB, SVF_MLP_FEATURES_BINS = 0, 1
 
 # every entry point include/svf.h declares
 EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_options_default", "svf_create",
@@ -75,7 +76,7 @@ class BtfView(C.Structure):
 
 class FitOptions(C.Structure):
     _fields_ = [("lsq", LsqOptions), ("init_mode", C.c_uint32), ("init_params", C.c_void_p), ("mlp", C.c_void_p),
-                ("initial_damping", C.c_float)]
+                ("initial_damping", C.c_float), ("mlp_fallback", C.c_float)]
 
 
 class BtfInfo(C.Structure):
@@ -91,7 +92,8 @@ class SvbrdfMaps(C.Structure):
 
 class MlpTrainOptions(C.Structure):
     _fields_ = [("texels", C.c_uint32), ("seed", C.c_uint32), ("mix", C.c_uint32), ("epochs", C.c_uint32),
-                ("batch", C.c_uint32), ("lr", C.c_float), ("max_iterations", C.c_uint32)]
+                ("batch", C.c_uint32), ("lr", C.c_float), ("max_iterations", C.c_uint32),
+                ("features", C.c_uint32)]
 
 
 class Maps(C.Structure):
@@ -105,7 +107,7 @@ class RunStats(C.Structure):
                 ("residuals", C.c_uint64), ("failed_texels", C.c_uint64), ("ms_total", C.c_double),
                 ("ms_luminance", C.c_double), ("ms_init", C.c_double), ("ms_fit", C.c_double),
                 ("ms_copy", C.c_double), ("lm_threads", C.c_uint32), ("lm_slots", C.c_uint32),
-                ("ms_ndf", C.c_double), ("graph", C.c_uint32), ("reserved", C.c_uint32)]
+                ("ms_ndf", C.c_double), ("graph", C.c_uint32), ("fallback_texels", C.c_uint32)]
 
 
 _lib = None
@@ -313,7 +315,7 @@ class Context:
     def fit_texels(self, layout: Layout, samples, width: int, height: int, sample_type=SVF_SAMPLES_F32,
                    opts: LsqOptions | None = None, init=None, want=("diffuse", "specular", "sigma", "basis", "rmse",
                                                                     "params", "init", "stats"), out=None,
-                   check=True, mlp: "Mlp | None" = None, damping: float = 0.0):
+                   check=True, mlp: "Mlp | None" = None, damping: float = 0.0, fallback: float = 0.0):
         """samples: [T][L*L][3] (numpy or torch, host or device).  init: given initial parameters; mlp: a
         learned initial guess (SVF_INIT_MLP); neither: the default guess.  damping: LM's initial damping as a
         multiple of the reference's rule (0: automatic).  Returns (maps dict, RunStats)."""
@@ -330,6 +332,7 @@ class Context:
         if mlp is not None:
             fo.init_mode, fo.mlp = SVF_INIT_MLP, mlp.handle
         fo.initial_damping = damping
+        fo.mlp_fallback = fallback
         kout = 12 if fo.lsq.flags & SVF_LSQ_RGB else 7
         shapes = {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
                   "params": (T, kout), "init": (T, kout), "ndf": (T, 64 * 64)}

@@ -217,7 +217,8 @@ struct svf_ctx
     std::map<uint64_t, std::unique_ptr<Layout>> layouts;
     std::unique_ptr<svf::InitHostTables> tables;
     DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, samples2,
-        maps_buf, scratch, rgb16, init_rgb, mlp_x, mlp_h1, mlp_h2, mlp_y;
+        maps_buf, scratch, rgb16, init_rgb, mlp_x, mlp_h1, mlp_h2, mlp_y, fb_idx, fb_lum, fb_hi, fb_lo, fb_ndf,
+        fb_small;
     PinnedBuf pinned;
 };
 
@@ -228,6 +229,7 @@ struct svf_mlp
 {
     int device = 0;
     uint32_t L = 0;
+    uint32_t features = SVF_MLP_FEATURES_BINS;
     std::vector<float> lp;               // [L][2]
     uint32_t pairs[svf::kMlpPairs] = {};
     // half-vector bins of the direction pairs (derived from lp): the pairs of bin
@@ -362,15 +364,19 @@ svf_status mlp_forward(svf_ctx* ctx, const svf_mlp* mlp, const float* X, int row
     return SVF_OK;
 }
 
-// Features [n][96] of luminance slabs [n][stride] (normalised with the model's
-// statistics when `normalise`).
-cudaError_t mlp_features_of(const svf_mlp* mlp, const float* lum, uint64_t stride, uint64_t n, float* X,
-                            bool normalise, cudaStream_t stream)
+// Features [n][96] of n texels -- from their RGB samples [n][N][3] or their
+// luminance slabs [n][stride], as the model's feature set reads them --
+// normalised with the model's statistics when `normalise`.
+cudaError_t mlp_features_of(const svf_mlp* mlp, const void* samples, uint32_t sample_type, uint32_t N,
+                            const float* lum, uint64_t stride, uint64_t n, float* X, bool normalise,
+                            cudaStream_t stream)
 {
+    const float* mean = normalise ? mlp->d_xmean.as<float>() : nullptr;
+    const float* rstd = normalise ? mlp->d_xrstd.as<float>() : nullptr;
+    if(mlp->features == SVF_MLP_FEATURES_PAIRS_RGB)
+        return svf::mlp_features_rgb(samples, sample_type, n, N, mlp->d_pairs.as<uint32_t>(), mean, rstd, X, stream);
     return svf::mlp_features(lum, stride, n, mlp->d_order.as<uint32_t>(), mlp->d_start.as<uint32_t>(),
-                             mlp->d_binw.as<float>(), mlp->d_pairs.as<uint32_t>(),
-                             normalise ? mlp->d_xmean.as<float>() : nullptr,
-                             normalise ? mlp->d_xrstd.as<float>() : nullptr, X, stream);
+                             mlp->d_binw.as<float>(), mlp->d_pairs.as<uint32_t>(), mean, rstd, X, stream);
 }
 
 // Scratch of one training step for `rows` rows (in the context).
@@ -1148,6 +1154,13 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     const bool rgb = (opts->lsq.flags & SVF_LSQ_RGB) != 0;
     const uint64_t stride3 = round_up(3ull * N, 8);
     const uint64_t kout = rgb ? 12 : 7;
+    // the learned guess's fallback to the default guess (selected texels only)
+    const bool fallback = mlp && opts->mlp_fallback > 0.0f;
+    if(opts->mlp_fallback != 0.0f && (!mlp || rgb || !(opts->mlp_fallback > 0.0f)))
+        return fail(SVF_EINVAL, "mlp_fallback needs SVF_INIT_MLP, the luminance fit and a positive threshold");
+    if(fallback)
+        SVF_TRY(prepare_init(ctx, lay, desc, &init_lay));
+    const uint32_t fb_ld = fallback ? init_lay->ndf_rows_pad : 0;
 
     // Chunking.  Device-resident samples: as few chunks as the device memory
     // allows.  Host samples: a pipeline of chunks, each copied host -> device on
@@ -1159,6 +1172,9 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     const size_t per_texel = sizeof(float) * (stride + 3 + 2 * kout + 7 + 1 + 12) + (rgb ? 2 * stride3 : 0) +
                              (mlp ? sizeof(float) * (svf::kMlpInputs + 2 * svf::kMlpHidden + svf::kMlpOutputs) : 0) +
                              (default_init ? 2 * 2 * stride + sizeof(float) * ndf_ld : 0) +
+                             (fallback ? sizeof(float) * (stride + fb_ld + 3 + 7 + 7 + 1 + 12 + 1) + 2 * 2 * stride +
+                                             sizeof(svf_texel_stats)
+                                       : 0) +
                              (maps->ndf ? sizeof(float) * svf::kNdfTexels : 0) +
                              (samples_on_device ? 0 : 2 * texel_bytes);
     uint64_t chunk = std::max<uint64_t>(1, (uint64_t)(0.5 * (double)free_b / (double)per_texel));
@@ -1195,6 +1211,16 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_TRY(ctx->mlp_h2.ensure(sizeof(float) * svf::kMlpHidden * chunk));
         SVF_TRY(ctx->mlp_y.ensure(sizeof(float) * svf::kMlpOutputs * chunk));
     }
+    if(fallback)
+    {
+        SVF_TRY(ctx->fb_idx.ensure(sizeof(uint32_t) * (chunk + 4)));
+        SVF_TRY(ctx->fb_lum.ensure(sizeof(float) * stride * chunk));
+        SVF_TRY(ctx->fb_hi.ensure(2 * stride * chunk));
+        SVF_TRY(ctx->fb_lo.ensure(2 * stride * chunk));
+        SVF_TRY(ctx->fb_ndf.ensure(sizeof(float) * fb_ld * chunk));
+        SVF_TRY(ctx->fb_small.ensure((sizeof(float) * (3 + 7 + 7 + 1 + 12) + sizeof(svf_texel_stats)) * chunk));
+    }
+    uint64_t fallback_texels = 0;
     DevBuf* staging[2] = { &ctx->samples, &ctx->samples2 };
     if(!samples_on_device)
     {
@@ -1260,6 +1286,9 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                                        ctx->avg.as<float>(), default_init ? ctx->lum_hi.p : nullptr,
                                        default_init ? ctx->lum_lo.p : nullptr, ctx->stream,
                                        rgb ? ctx->rgb16.p : nullptr, stride3));
+        if(mlp)   // the learned guess's inputs, read before the staging buffer is handed back
+            SVF_CUDA(mlp_features_of(mlp, samples, btf->sample_type, N, ctx->lum.as<float>(), stride, n,
+                                     ctx->mlp_x.as<float>(), true, ctx->stream));
         if(!samples_on_device)
         {
             SVF_CUDA(cudaEventRecord(ctx->freed[buf], ctx->stream));
@@ -1281,9 +1310,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         }
         else if(mlp)
         {
-            // the learned initial guess from the chunk's luminance slabs
-            SVF_CUDA(mlp_features_of(mlp, ctx->lum.as<float>(), stride, n, ctx->mlp_x.as<float>(), true,
-                                     ctx->stream));
+            // the learned initial guess from the chunk's features
             SVF_TRY(mlp_forward(ctx, mlp, ctx->mlp_x.as<float>(), (int)n, nullptr, ctx->mlp_h1.as<float>(), nullptr,
                                 ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>(), true));
             SVF_CUDA(svf::mlp_finish(ctx->mlp_y.as<float>(), n, mlp->d_ymean.as<float>(), mlp->d_ystd.as<float>(),
@@ -1314,6 +1341,49 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         // (the RGB fit chained from the luminance fit starts with the reference's damping)
         r.damping = rgb && (default_init || mlp) ? 1.0f : initial_damping(*opts);
         SVF_TRY(run_lm(ctx, lay, &opts->lsq, r));
+        if(fallback)
+        {
+            // texels whose relative RMSE is above the threshold are fitted from
+            // the default guess too (their slabs gathered) and keep the lower RMSE
+            uint32_t* idx = ctx->fb_idx.as<uint32_t>();
+            uint32_t* count = idx + chunk;   // [0] selected, [1] replaced
+            SVF_CUDA(cudaMemsetAsync(count, 0, 2 * sizeof(uint32_t), ctx->stream));
+            SVF_CUDA(svf::launch_fallback_select(ctx->lum.as<float>(), stride, N, ctx->rmse.as<float>(), n,
+                                                 opts->mlp_fallback, idx, count, ctx->stream));
+            uint32_t m = 0;
+            SVF_CUDA(cudaMemcpyAsync(&m, count, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+            SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+            if(m)
+            {
+                float* g = ctx->fb_small.as<float>();
+                float* g_avg = g;
+                float* g_init = g_avg + 3 * (uint64_t)m;
+                float* g_out = g_init + 7 * (uint64_t)m;
+                float* g_rmse = g_out + 7 * (uint64_t)m;
+                float* g_maps = g_rmse + m;
+                svf_texel_stats* g_stats = reinterpret_cast<svf_texel_stats*>(g_maps + 12 * (uint64_t)m);
+                SVF_CUDA(svf::launch_gather_slabs(ctx->lum.as<float>(), stride, ctx->avg.as<float>(), idx, m,
+                                                  ctx->fb_lum.as<float>(), g_avg, ctx->stream));
+                SVF_CUDA(svf::launch_split_bf16(ctx->fb_lum.as<float>(), stride * m, ctx->fb_hi.p, ctx->fb_lo.p,
+                                                ctx->stream));
+                cudaError_t e = svf::launch_ndf_tc(ctx->fb_hi.p, ctx->fb_lo.p, m, stride, init_lay->ndf_op_hi,
+                                                   init_lay->ndf_op_lo, init_lay->ndf_rows_pad, init_lay->k_pad, N,
+                                                   ctx->fb_ndf.as<float>(), fb_ld, ctx->error.as<uint32_t>() + 2,
+                                                   ctx->stream);
+                if(e != cudaSuccess)
+                    return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
+                SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->fb_ndf.as<float>(), fb_ld, m, g_init, nullptr,
+                                                 nullptr, ctx->stream));
+                LmRun gr{ ctx->fb_lum.p, stride, g_init, g_out, g_rmse, g_stats, g_avg, g_maps, g_maps + 3 * m,
+                          g_maps + 6 * m, g_maps + 8 * m, m };
+                SVF_TRY(run_lm(ctx, lay, &opts->lsq, gr));
+                SVF_CUDA(svf::launch_fallback_merge(idx, m, g_out, g_rmse, g_stats, g_maps, g_init, n,
+                                                    ctx->out.as<float>(), ctx->rmse.as<float>(),
+                                                    ctx->stats.as<svf_texel_stats>() + c0, mb, ctx->init.as<float>(),
+                                                    count + 1, ctx->stream));
+                fallback_texels += m;
+            }
+        }
         SVF_CUDA(mark(ev(c, 5), ctx->stream));
         // outputs (into host or device buffers of the caller)
         auto put = [&](void* dst, const void* src, size_t bytes) -> svf_status {
@@ -1353,7 +1423,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         }
         return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged || at.type == cudaMemoryTypeHost;
     };
-    bool eligible = samples_on_device && n_chunks == 1 && reachable(opts->init_params) &&
+    bool eligible = samples_on_device && n_chunks == 1 && !fallback && reachable(opts->init_params) &&
                     reachable(maps->diffuse) && reachable(maps->specular) && reachable(maps->sigma) &&
                     reachable(maps->basis) && reachable(maps->rmse) && reachable(maps->params) &&
                     reachable(maps->init) && reachable(maps->ndf);
@@ -1482,6 +1552,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     const svf::LmKernelChoice used = lm_choice(lay, rgb ? stride3 : stride, rgb);
     rs.lm_threads = (uint32_t)used.threads;
     rs.lm_slots = (uint32_t)used.slots;
+    rs.fallback_texels = (uint32_t)fallback_texels;
     if(run)
         *run = rs;
     if(rs.failed_texels)
@@ -1524,6 +1595,8 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             return fail(SVF_EINVAL, "btf %u: unknown init_mode %u", b, o.init_mode);
         if(o.init_mode == SVF_INIT_MLP && !o.mlp)
             return fail(SVF_EINVAL, "btf %u: SVF_INIT_MLP needs a model (svf_fit_options::mlp)", b);
+        if(o.mlp_fallback != 0.0f)
+            return fail(SVF_EINVAL, "btf %u: mlp_fallback is taken by svf_fit_texels only", b);
         if(o.init_mode == SVF_INIT_GIVEN && !o.init_params)
             return fail(SVF_EINVAL, "btf %u: SVF_INIT_GIVEN needs init_params", b);
         const svf_lsq_options &a = o.lsq, &z = opts[0].lsq;
@@ -1713,7 +1786,8 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             }
             else if(x.mlp)
             {
-                SVF_CUDA(mlp_features_of(x.mlp, lum, x.stride, p.count, ctx->mlp_x.as<float>(), true, ctx->stream));
+                SVF_CUDA(mlp_features_of(x.mlp, samples, v.sample_type, N, lum, x.stride, p.count,
+                                         ctx->mlp_x.as<float>(), true, ctx->stream));
                 SVF_TRY(mlp_forward(ctx, x.mlp, ctx->mlp_x.as<float>(), (int)p.count, nullptr, ctx->mlp_h1.as<float>(),
                                     nullptr, ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>(), true));
                 SVF_CUDA(svf::mlp_finish(ctx->mlp_y.as<float>(), p.count, x.mlp->d_ymean.as<float>(),
@@ -1977,11 +2051,11 @@ svf_status check_mlp(svf_ctx* ctx, const svf_mlp* mlp)
     return SVF_OK;
 }
 
-constexpr char kMlpMagic[8] = { 'S', 'V', 'F', 'M', 'L', 'P', '0', '1' };
+constexpr char kMlpMagic[8] = { 'S', 'V', 'F', 'M', 'L', 'P', '0', '2' };
 
 size_t mlp_blob_bytes(uint32_t L)
 {
-    return sizeof(kMlpMagic) + 2 * sizeof(uint32_t) + sizeof(float) * 2 * L + sizeof(uint32_t) * svf::kMlpPairs +
+    return sizeof(kMlpMagic) + 3 * sizeof(uint32_t) + sizeof(float) * 2 * L + sizeof(uint32_t) * svf::kMlpPairs +
            sizeof(float) * 2 * (svf::kMlpInputs + svf::kMlpOutputs) + sizeof(float) * svf::kMlpParams;
 }
 
@@ -2000,6 +2074,7 @@ void svf_mlp_train_options_default(svf_mlp_train_options* o)
     o->batch = 4096;
     o->lr = 1e-3f;
     o->max_iterations = 1024;
+    o->features = SVF_MLP_FEATURES_BINS;
 }
 
 svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_mlp_train_options* opts, svf_mlp** out,
@@ -2017,13 +2092,15 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_ml
     if(L < 3 || L > 160)
         return fail(SVF_EINVAL, "light_count %u outside 3..160", L);
     if(o.texels < 256 || o.texels > (1u << 24) || o.batch < 16 || o.batch > (1u << 16) || o.epochs < 1 ||
-       o.epochs > 1000 || !(o.lr > 0.0f) || o.mix > 1)
-        return fail(SVF_EINVAL, "bad training options (texels 256..2^24, batch 16..65536, epochs 1..1000, lr > 0)");
+       o.epochs > 1000 || !(o.lr > 0.0f) || o.mix > 1 || o.features > SVF_MLP_FEATURES_BINS)
+        return fail(SVF_EINVAL, "bad training options (texels 256..2^24, batch 16..65536, epochs 1..1000, lr > 0, "
+                                "features 0..1)");
     std::unique_ptr<svf_mlp> mlp(new(std::nothrow) svf_mlp);
     if(!mlp)
         return fail(SVF_ENOMEM, "model allocation failed");
     mlp->device = ctx->device;
     mlp->L = L;
+    mlp->features = o.features;
     mlp->lp.resize(2 * (size_t)L);
     SVF_CUDA(cudaMemcpy(mlp->lp.data(), lp, sizeof(float) * 2 * L, cudaMemcpyDefault));
     choose_pairs(mlp->lp.data(), L, o.seed, mlp->pairs);
@@ -2070,8 +2147,8 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_ml
             return st;
         SVF_CUDA(launch_luminance(samples.p, SVF_SAMPLES_F32, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr,
                                   nullptr, ctx->stream));
-        SVF_CUDA(mlp_features_of(mlp.get(), lum.as<float>(), stride, n, X.as<float>() + (size_t)kMlpInputs * c0,
-                                 false, ctx->stream));
+        SVF_CUDA(mlp_features_of(mlp.get(), samples.p, SVF_SAMPLES_F32, N, lum.as<float>(), stride, n,
+                                 X.as<float>() + (size_t)kMlpInputs * c0, false, ctx->stream));
         SVF_CUDA(mlp_targets(params.as<float>(), n, Y.as<float>() + (size_t)kMlpOutputs * c0, ctx->stream));
     }
     samples.reset();
@@ -2211,7 +2288,8 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
         }
         SVF_CUDA(launch_luminance(s, sample_type, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr, nullptr,
                                   ctx->stream));
-        SVF_CUDA(mlp_features_of(mlp, lum.as<float>(), stride, n, x.as<float>(), true, ctx->stream));
+        SVF_CUDA(mlp_features_of(mlp, s, sample_type, N, lum.as<float>(), stride, n, x.as<float>(), true,
+                                 ctx->stream));
         SVF_TRY(mlp_forward(ctx, mlp, x.as<float>(), (int)n, nullptr, h1.as<float>(), nullptr, h2.as<float>(),
                             y.as<float>(), true));
         SVF_CUDA(mlp_finish(y.as<float>(), n, mlp->d_ymean.as<float>(), mlp->d_ystd.as<float>(), p.as<float>(),
@@ -2275,7 +2353,7 @@ svf_status svf_mlp_save(const svf_mlp* mlp, void* buf, size_t* size)
         std::memcpy(c, src, n);
         c += n;
     };
-    const uint32_t hdr[2] = { mlp->L, (uint32_t)kMlpParams };
+    const uint32_t hdr[3] = { mlp->L, (uint32_t)kMlpParams, mlp->features };
     put(kMlpMagic, sizeof(kMlpMagic));
     put(hdr, sizeof(hdr));
     put(mlp->lp.data(), sizeof(float) * 2 * mlp->L);
@@ -2297,11 +2375,12 @@ svf_status svf_mlp_load(svf_ctx* ctx, const void* buf, size_t size, svf_mlp** ou
         return fail(SVF_EINVAL, "null buffer/output");
     *out = nullptr;
     const char* c = static_cast<const char*>(buf);
-    uint32_t hdr[2];
+    uint32_t hdr[3];
     if(size < sizeof(kMlpMagic) + sizeof(hdr) || std::memcmp(c, kMlpMagic, sizeof(kMlpMagic)) != 0)
         return fail(SVF_EINVAL, "not a model (bad magic)");
     std::memcpy(hdr, c + sizeof(kMlpMagic), sizeof(hdr));
-    if(hdr[0] < 3 || hdr[0] > 160 || hdr[1] != kMlpParams || size != mlp_blob_bytes(hdr[0]))
+    if(hdr[0] < 3 || hdr[0] > 160 || hdr[1] != kMlpParams || hdr[2] > SVF_MLP_FEATURES_BINS ||
+       size != mlp_blob_bytes(hdr[0]))
         return fail(SVF_EINVAL, "model header: L %u, %u parameters, %zu bytes (expected %zu parameters)", hdr[0],
                     hdr[1], size, (size_t)kMlpParams);
     std::unique_ptr<svf_mlp> mlp(new(std::nothrow) svf_mlp);
@@ -2309,6 +2388,7 @@ svf_status svf_mlp_load(svf_ctx* ctx, const void* buf, size_t size, svf_mlp** ou
         return fail(SVF_ENOMEM, "model allocation failed");
     mlp->device = ctx->device;
     mlp->L = hdr[0];
+    mlp->features = hdr[2];
     mlp->lp.resize(2 * (size_t)mlp->L);
     c += sizeof(kMlpMagic) + sizeof(hdr);
     auto get = [&](void* dst, size_t n) {

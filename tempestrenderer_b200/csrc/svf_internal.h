@@ -201,9 +201,22 @@ cudaError_t mlp_gather_rows(const float* X, int nx, const float* Y, int ny, cons
 cudaError_t mlp_features(const float* lum, uint64_t stride, uint64_t texels, const uint32_t* order,
                          const uint32_t* start, const float* bin_w, const uint32_t* pairs, const float* mean,
                          const float* rstd, float* X, cudaStream_t stream);
+// features [texels][96] of RGB samples [texels][N][3]: 32 pairs x RGB
+cudaError_t mlp_features_rgb(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
+                             const uint32_t* pairs, const float* mean, const float* rstd, float* X, cudaStream_t stream);
 cudaError_t mlp_targets(const float* p7, uint64_t texels, float* Y, cudaStream_t stream);
 cudaError_t mlp_finish(const float* Yn, uint64_t texels, const float* mean, const float* std, float* p7,
                        cudaStream_t stream);
+
+// ---- learned guess: fallback to the default guess (svf_kernels.cu) ------------------
+cudaError_t launch_fallback_select(const float* lum, uint64_t stride, uint32_t N, const float* rmse, uint64_t n,
+                                   float threshold, uint32_t* idx, uint32_t* count, cudaStream_t stream);
+cudaError_t launch_gather_slabs(const float* lum, uint64_t stride, const float* avg, const uint32_t* idx, uint32_t m,
+                                float* g_lum, float* g_avg, cudaStream_t stream);
+cudaError_t launch_fallback_merge(const uint32_t* idx, uint32_t m, const float* g_out, const float* g_rmse,
+                                  const svf_texel_stats* g_stats, const float* g_maps, const float* g_init, uint64_t n,
+                                  float* out, float* rmse, svf_texel_stats* stats, float* maps, float* init,
+                                  uint32_t* taken, cudaStream_t stream);
 
 // ---- neighbourhood refit (svf_kernels.cu) --------------------------------------------
 // cand [9n][7]: candidate k of texel c0 + i at row k*n + i (the 3x3 neighbour's

@@ -613,4 +613,120 @@ cudaError_t launch_refit_select(const float* params, const float* rmse, uint64_t
     return cudaGetLastError();
 }
 
+// ---- learned guess: fallback to the default guess ---------------------------------
+
+namespace
+{
+
+// Texel t is selected when its RMSE relative to the RMS of its luminance slice
+// is above the threshold (one CTA per texel; the order of the selected list
+// follows the atomics, which changes nothing: each texel is fitted on its own).
+__global__ void __launch_bounds__(256) fallback_select_kernel(const float* __restrict__ lum, uint64_t stride,
+                                                              uint32_t N, const float* __restrict__ rmse,
+                                                              float threshold, uint32_t* __restrict__ idx,
+                                                              uint32_t* __restrict__ count)
+{
+    const uint64_t t = blockIdx.x;
+    const float* y = lum + t * stride;
+    double s = 0.0;
+    for(uint32_t i = threadIdx.x; i < N; i += blockDim.x)
+        s += (double)y[i] * y[i];
+    __shared__ double red[8];
+#pragma unroll
+    for(int o = 16; o > 0; o >>= 1)
+        s += __shfl_xor_sync(0xffffffffu, s, o);
+    if((threadIdx.x & 31) == 0)
+        red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if(threadIdx.x == 0)
+    {
+        double tot = 0.0;
+        for(int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            tot += red[w];
+        const double rms = sqrt(tot / N);
+        if(rms > 0.0 && (double)rmse[t] > threshold * rms)
+            idx[atomicAdd(count, 1u)] = (uint32_t)t;
+    }
+}
+
+__global__ void gather_slabs_kernel(const float* __restrict__ lum, uint64_t stride, const float* __restrict__ avg,
+                                    const uint32_t* __restrict__ idx, float* __restrict__ g_lum,
+                                    float* __restrict__ g_avg)
+{
+    const uint64_t i = blockIdx.x;
+    const uint64_t t = idx[i];
+    for(uint64_t k = threadIdx.x; k < stride; k += blockDim.x)
+        g_lum[i * stride + k] = lum[t * stride + k];
+    if(threadIdx.x < 3)
+        g_avg[3 * i + threadIdx.x] = avg[3 * t + threadIdx.x];
+}
+
+// The default-guess fit of selected texel i replaces the learned-guess fit of
+// texel idx[i] when its RMSE is lower.  Maps: diffuse 3 | specular 3 | sigma 2 |
+// basis 4, each a block of n (resp. m) texels.
+__global__ void fallback_merge_kernel(const uint32_t* __restrict__ idx, uint32_t m, const float* __restrict__ g_out,
+                                      const float* __restrict__ g_rmse, const svf_texel_stats* __restrict__ g_stats,
+                                      const float* __restrict__ g_maps, const float* __restrict__ g_init,
+                                      uint64_t n, float* __restrict__ out, float* __restrict__ rmse,
+                                      svf_texel_stats* __restrict__ stats, float* __restrict__ maps,
+                                      float* __restrict__ init, uint32_t* __restrict__ taken)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if(i >= m)
+        return;
+    const uint64_t t = idx[i];
+    if(!(g_rmse[i] < rmse[t]))
+        return;
+    atomicAdd(taken, 1u);
+    for(int p = 0; p < 7; ++p)
+    {
+        out[7 * t + p] = g_out[7 * i + p];
+        init[7 * t + p] = g_init[7 * i + p];
+    }
+    rmse[t] = g_rmse[i];
+    if(stats)
+        stats[t] = g_stats[i];
+    for(int c = 0; c < 3; ++c)
+    {
+        maps[3 * t + c] = g_maps[3 * i + c];
+        maps[3 * n + 3 * t + c] = g_maps[3 * (uint64_t)m + 3 * i + c];
+    }
+    for(int c = 0; c < 2; ++c)
+        maps[6 * n + 2 * t + c] = g_maps[6 * (uint64_t)m + 2 * i + c];
+    for(int c = 0; c < 4; ++c)
+        maps[8 * n + 4 * t + c] = g_maps[8 * (uint64_t)m + 4 * i + c];
+}
+
+} // namespace
+
+cudaError_t launch_fallback_select(const float* lum, uint64_t stride, uint32_t N, const float* rmse, uint64_t n,
+                                   float threshold, uint32_t* idx, uint32_t* count, cudaStream_t stream)
+{
+    if(n == 0)
+        return cudaSuccess;
+    fallback_select_kernel<<<(unsigned)n, 256, 0, stream>>>(lum, stride, N, rmse, threshold, idx, count);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather_slabs(const float* lum, uint64_t stride, const float* avg, const uint32_t* idx, uint32_t m,
+                                float* g_lum, float* g_avg, cudaStream_t stream)
+{
+    if(m == 0)
+        return cudaSuccess;
+    gather_slabs_kernel<<<m, 256, 0, stream>>>(lum, stride, avg, idx, g_lum, g_avg);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fallback_merge(const uint32_t* idx, uint32_t m, const float* g_out, const float* g_rmse,
+                                  const svf_texel_stats* g_stats, const float* g_maps, const float* g_init, uint64_t n,
+                                  float* out, float* rmse, svf_texel_stats* stats, float* maps, float* init,
+                                  uint32_t* taken, cudaStream_t stream)
+{
+    if(m == 0)
+        return cudaSuccess;
+    fallback_merge_kernel<<<(m + 255) / 256, 256, 0, stream>>>(idx, m, g_out, g_rmse, g_stats, g_maps, g_init, n, out,
+                                                               rmse, stats, maps, init, taken);
+    return cudaGetLastError();
+}
+
 } // namespace svf

@@ -4,9 +4,11 @@
 // guess is the NDF -> PCA -> projection pipeline, svbrdf-fitting-pipeline.cc:
 // 350-660); LM refinement always follows.
 //
-//   features  x = (log max(v, 1e-6) - mean) / std, 96 values:
+//   features  x = (log max(v, 1e-6) - mean) / std, 96 values, one of:
+//             32 fixed direction pairs x RGB (SVF_MLP_FEATURES_PAIRS_RGB), or
 //             64 half-vector bins (mean luminance of the direction pairs whose
-//             half vector falls in the bin) and 32 single direction pairs
+//             half vector falls in the bin) and 32 pairs' luminance
+//             (SVF_MLP_FEATURES_BINS)
 //   network   96 -> 256 -> 256 -> 8, GELU (tanh form) between layers
 //   targets   (log S (6 elements), log(ks + 1e-4), log(kd + 1e-4)) - mean) / std
 //             with S = R diag(sx^2, sy^2, 1) R^T the SGGX matrix: its logarithm
@@ -53,6 +55,7 @@ __device__ __forceinline__ float gelu_grad(float x)
 
 __device__ __forceinline__ float to_f(float x) { return x; }
 __device__ __forceinline__ float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
+__device__ __forceinline__ float to_f(__half x) { return __half2float(x); }
 
 // C[M][N] = op(A) op(B) with op(A)[m][k] = kTA ? A[k][m] : A[m][k] and
 // op(B)[k][n] = kTB ? B[n][k] : B[k][n] (leading dimensions lda, ldb); then
@@ -276,6 +279,25 @@ __global__ void __launch_bounds__(256) features_kernel(const float* __restrict__
     }
 }
 
+// Features of the 32 pairs' RGB samples (96 = 32 pairs x RGB), log-scaled and
+// normalised (mean may be null)
+template <typename T>
+__global__ void features_rgb_kernel(const T* __restrict__ samples, uint64_t texels, uint32_t N,
+                                    const uint32_t* __restrict__ pairs, const float* __restrict__ mean,
+                                    const float* __restrict__ rstd, float* __restrict__ X)
+{
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if(i >= texels * kMlpInputs)
+        return;
+    const uint64_t t = i / kMlpInputs;
+    const int f = (int)(i % kMlpInputs);
+    const float y = to_f(samples[(t * N + pairs[f / 3]) * 3 + (f % 3)]);
+    float x = logf(fmaxf(y, 1e-6f));
+    if(mean)
+        x = (x - mean[f]) * rstd[f];
+    X[i] = x;
+}
+
 // Targets of a fitted texel (params7 {sx, sy, ks, kd, euler}): log S, log ks, log kd
 __global__ void targets_kernel(const float* __restrict__ p7, uint64_t texels, float* __restrict__ Y)
 {
@@ -490,6 +512,21 @@ cudaError_t mlp_features(const float* lum, uint64_t stride, uint64_t texels, con
     if(texels > 0x7fffffffull)
         return cudaErrorInvalidValue;
     features_kernel<<<(unsigned)texels, 256, 0, stream>>>(lum, stride, order, start, bin_w, pairs, mean, rstd, X);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_features_rgb(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
+                             const uint32_t* pairs, const float* mean, const float* rstd, float* X, cudaStream_t stream)
+{
+    if(texels == 0)
+        return cudaSuccess;
+    const unsigned b = (unsigned)((texels * kMlpInputs + 255) / 256);
+    if(sample_type == SVF_SAMPLES_F16)
+        features_rgb_kernel<__half><<<b, 256, 0, stream>>>(static_cast<const __half*>(samples), texels, N, pairs,
+                                                            mean, rstd, X);
+    else
+        features_rgb_kernel<float><<<b, 256, 0, stream>>>(static_cast<const float*>(samples), texels, N, pairs, mean,
+                                                           rstd, X);
     return cudaGetLastError();
 }
 

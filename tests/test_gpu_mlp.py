@@ -79,9 +79,9 @@ def _bf16(x):
     return u.astype(np.uint32).view(np.float32)
 
 
-def _blob(lp, pairs, xmean, xrstd, ymean, ystd, w):
+def _blob(lp, pairs, xmean, xrstd, ymean, ystd, w, features=svf.SVF_MLP_FEATURES_BINS):
     L = lp.shape[0]
-    return (b"SVFMLP01" + struct.pack("<II", L, NPARAMS) + np.ascontiguousarray(lp, np.float32).tobytes() +
+    return (b"SVFMLP02" + struct.pack("<III", L, NPARAMS, features) + np.ascontiguousarray(lp, np.float32).tobytes() +
             np.asarray(pairs, np.uint32).tobytes() + np.asarray(xmean, np.float32).tobytes() +
             np.asarray(xrstd, np.float32).tobytes() + np.asarray(ymean, np.float32).tobytes() +
             np.asarray(ystd, np.float32).tobytes() + np.asarray(w, np.float32).tobytes())
@@ -209,6 +209,12 @@ def test_predict_matches_fp64_forward(gpu_ctx, oracle_lib, golden):
     p2 = m.predict(torch.from_numpy(rgb).cuda(), T)
     np.testing.assert_array_equal(p, p2)
     m.close()
+    # the other feature set: the 32 pairs' RGB samples, log-scaled
+    m = svf.Mlp.load(gpu_ctx, _blob(lp, pairs, xmean, xrstd, ymean, ystd, w, svf.SVF_MLP_FEATURES_PAIRS_RGB))
+    _, f_rgb = m.predict(rgb, T, features=True)
+    x_rgb = (np.log(np.maximum(rgb[:, pairs, :].reshape(T, INPUTS).astype(np.float64), 1e-6)) - xmean) * xrstd
+    np.testing.assert_allclose(f_rgb, x_rgb, rtol=1e-5, atol=1e-4)
+    m.close()
 
 
 def test_model_checks(gpu_ctx, golden):
@@ -219,6 +225,8 @@ def test_model_checks(gpu_ctx, golden):
         svf.Mlp.load(gpu_ctx, blob[:-4])
     with pytest.raises(svf.SvfError):
         svf.Mlp.load(gpu_ctx, b"XXXXXXXX" + blob[8:])
+    with pytest.raises(svf.SvfError):   # unknown feature set
+        svf.Mlp.load(gpu_ctx, _blob(lp, *model, features=7))
     bad_pairs = np.array(model[0])
     bad_pairs[3] = 81 * 81
     with pytest.raises(svf.SvfError):
@@ -292,3 +300,40 @@ def test_save_load_and_batch_with_a_model(gpu_ctx, golden, trained, oracle_lib):
                                  want=("rmse",))
         assert (rgb["rmse"] <= base["rmse"] * (1 + 1e-6)).all()
     m2.close()
+
+
+def test_plain_lm_fallback(gpu_ctx, golden, trained):
+    """SVF_INIT_MLP with mlp_fallback: texels whose RMSE from the learned guess is
+    above the threshold (relative to their luminance slice's RMS) are fitted from
+    the default guess as well and keep the lower RMSE; the others keep the
+    learned-guess fit.  Both fits are the ones the two modes give alone, bit for
+    bit, so the result is their per-texel minimum where selected."""
+    import torch
+
+    m, _ = trained
+    lay = _ring(golden)
+    W, H = 64, 64
+    T = W * H
+    s = torch.empty((T, 81 * 81, 3), dtype=torch.float32, device="cuda")
+    gpu_ctx.synth_btf(4040, 1, lay.lights_parabolic, 0, T, s)
+    want = ("rmse", "params", "diffuse", "basis")
+    plain, _ = gpu_ctx.fit_texels(lay, s, W, H, want=want)
+    learned, _ = gpu_ctx.fit_texels(lay, s, W, H, mlp=m, want=want)
+    x = s.cpu().numpy()
+    lum = (np.float32(0.2126) * x[..., 0] + np.float32(0.7152) * x[..., 1]) + np.float32(0.0722) * x[..., 2]
+    rel = learned["rmse"] / np.sqrt((lum.astype(np.float64) ** 2).mean(1))
+    th = float(np.median(rel))
+    got, rs = gpu_ctx.fit_texels(lay, s, W, H, mlp=m, fallback=th, want=want)
+    assert rs.failed_texels == 0
+    above, below = rel > th * (1 + 1e-5), rel < th * (1 - 1e-5)
+    assert above.sum() <= rs.fallback_texels <= T - below.sum()
+    best = np.minimum(learned["rmse"], plain["rmse"])
+    np.testing.assert_array_equal(got["rmse"][above], best[above])
+    np.testing.assert_array_equal(got["rmse"][below], learned["rmse"][below])
+    take = above & (plain["rmse"] < learned["rmse"])
+    for k in ("params", "diffuse", "basis"):
+        np.testing.assert_array_equal(got[k][take], plain[k][take], err_msg=k)
+        np.testing.assert_array_equal(got[k][below], learned[k][below], err_msg=k)
+    assert (got["rmse"] <= learned["rmse"]).all()
+    with pytest.raises(svf.SvfError):   # the fallback belongs to the learned guess
+        gpu_ctx.fit_texels(lay, s, W, H, fallback=0.5, want=("rmse",))
