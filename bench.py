@@ -198,6 +198,19 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev):
     ms = sum(r.ms_total for r in st) / steps
     rmse = maps["rmse"].cpu().numpy()
     ratio = rmse / np.maximum(ref_rmse, 1e-12)
+    # the plain-LM fallback at the median relative residual: about half the texels
+    # are fitted from the default guess as well and keep the lower RMSE
+    lum_rms = torch.sqrt(((0.2126 * samples[..., 0] + 0.7152 * samples[..., 1] + 0.0722 * samples[..., 2])
+                          .double() ** 2).mean(1)).cpu().numpy()
+    th = float(np.median(rmse / lum_rms))
+    fmaps = {k: torch.zeros_like(v) for k, v in maps.items()}
+    frun = lambda: ctx.fit_texels(layout, samples, W, H, opts=opts, want=tuple(fmaps), out=fmaps, check=False,
+                                  mlp=model, fallback=th)[1]
+    frun()
+    fst = [frun() for _ in range(steps)]
+    fms = sum(r.ms_total for r in fst) / steps
+    frmse = fmaps["rmse"].cpu().numpy()
+    fratio = frmse / np.maximum(ref_rmse, 1e-12)
     model.close()
     return {"value": T / (ms / 1e3), "unit": "texels/s", "ms_per_step": ms, "steps": steps,
             "phases_ms": {"luminance": sum(r.ms_luminance for r in st) / steps,
@@ -208,6 +221,12 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev):
             "rmse_ratio_vs_default_init": {"median": float(np.median(ratio)), "within_1pct": float(np.mean(ratio <= 1.01)),
                                            "better_1pct": float(np.mean(ratio < 0.99)), "p90": float(np.quantile(ratio, 0.9))},
             "training": {"seconds": train_s, "final_loss": loss, "texels": 1 << 20, "epochs": 24},
+            "with_fallback": {"value": T / (fms / 1e3), "unit": "texels/s", "ms_per_step": fms,
+                              "threshold_relative_rmse": th, "fallback_texels": fst[-1].fallback_texels,
+                              "mean_rmse": float(frmse.mean()),
+                              "rmse_ratio_vs_default_init": {"median": float(np.median(fratio)),
+                                                             "within_1pct": float(np.mean(fratio <= 1.01)),
+                                                             "p90": float(np.quantile(fratio, 0.9))}},
             "model": "MLP 96-256-256-8 (64 half-vector bins + 32 pairs of the luminance slab -> log S, ks, kd), "
                      "BF16 inference; LM from its prediction with 1e-3 of the reference's initial damping"}
 
