@@ -177,7 +177,39 @@ def run_reference(args):
 # the GPU fitter
 # ----------------------------------------------------------------------------
 
-def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev):
+def _normal_of_quat(q):
+    x, y, z, w = q[:, 0], q[:, 1], q[:, 2], q[:, 3]
+    n = np.stack([2 * (x * z + y * w), 2 * (y * z - x * w), 1 - 2 * (x * x + y * y)], 1)
+    return n / np.linalg.norm(n, axis=1, keepdims=True)
+
+
+def _quat_of_euler(e):
+    h = 0.5 * e.astype(np.float64)
+    s1, c1, s2, c2, s3, c3 = np.sin(h[:, 0]), np.cos(h[:, 0]), np.sin(h[:, 1]), np.cos(h[:, 1]), np.sin(h[:, 2]), \
+        np.cos(h[:, 2])
+    return np.stack([s1 * c2 * c3 + c1 * s2 * s3, -s1 * c2 * s3 + c1 * s2 * c3, c1 * c2 * s3 + s1 * s2 * c3,
+                     c1 * c2 * c3 - s1 * s2 * s3], 1)
+
+
+def param_error(params, truth):
+    """Fitted 7-parameter luminance model against the synthetic ground truth
+    ([T][16]: kd rgb, ks rgb, sigma, quaternion, euler, kind): normal angle, the
+    lobe's geometric-mean scale and anisotropy, the luminance albedos."""
+    p, t = np.asarray(params, np.float64), np.asarray(truth, np.float64)
+    w = np.array([0.2126, 0.7152, 0.0722])
+    ang = np.degrees(np.arccos(np.clip(np.abs((_normal_of_quat(_quat_of_euler(p[:, 4:7])) *
+                                               _normal_of_quat(t[:, 8:12])).sum(1)), 0, 1)))
+    gm = np.abs(np.log(np.sqrt(np.abs(p[:, 0] * p[:, 1]) + 1e-12) / np.sqrt(t[:, 6] * t[:, 7])))
+    an = lambda a, b: np.log(np.maximum(a, b) / np.maximum(np.minimum(a, b), 1e-6))
+    aniso = np.abs(an(np.abs(p[:, 0]), np.abs(p[:, 1])) - an(t[:, 6], t[:, 7]))
+    kd, ks = t[:, 0:3] @ w, t[:, 3:6] @ w
+    ekd = np.abs(p[:, 3] - kd) / np.maximum(kd, 0.02)
+    eks = np.abs(p[:, 2] - ks) / np.maximum(ks, 0.02)
+    q = lambda a: {"median": float(np.median(a)), "p90": float(np.quantile(a, 0.9))}
+    return {"normal_deg": q(ang), "log_scale": q(gm), "log_anisotropy": q(aniso), "kd_rel": q(ekd), "ks_rel": q(eks)}
+
+
+def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, truth=None):
     """The learned initial guess (SVF_INIT_MLP) on the benchmark texels: train a model on
     separately seeded synthetic texels, then fit the same texels from its prediction."""
     import torch
@@ -218,6 +250,7 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev):
             "lm_work": {"jacobian_passes": st[-1].jacobians, "residual_passes": st[-1].residuals,
                         "failed_texels": st[-1].failed_texels, "mean_iterations": st[-1].iterations / T},
             "mean_rmse": float(rmse.mean()), "default_init_mean_rmse": float(ref_rmse.mean()),
+            "ground_truth_error": None if truth is None else param_error(maps["params"].cpu().numpy(), truth),
             "rmse_ratio_vs_default_init": {"median": float(np.median(ratio)), "within_1pct": float(np.mean(ratio <= 1.01)),
                                            "better_1pct": float(np.mean(ratio < 0.99)), "p90": float(np.quantile(ratio, 0.9))},
             "training": {"seconds": train_s, "final_loss": loss, "texels": 1 << 20, "epochs": 24},
@@ -404,7 +437,8 @@ def run_ours(args):
     ctx = svf.Context(local)
     # this rank's shard of a larger synthetic BTF: texels [rank*T, (rank+1)*T)
     samples = torch.empty((T, N, 3), dtype=torch.float32, device=dev)
-    ctx.synth_btf(SEED, MIX, layout.lights_parabolic, rank * T, T, samples)
+    truth = torch.empty((T, 16), dtype=torch.float32, device=dev)
+    ctx.synth_btf(SEED, MIX, layout.lights_parabolic, rank * T, T, samples, truth=truth)
     torch.cuda.synchronize()
     maps = {k: torch.zeros(s, dtype=torch.float32, device=dev) for k, s in
             {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
@@ -496,6 +530,8 @@ def run_ours(args):
         del host_samples
 
     head_rmse = maps["rmse"].cpu().numpy()
+    truth_np = truth.cpu().numpy()
+    head_truth_err = param_error(maps["params"].cpu().numpy(), truth_np)
     learned = fib = batch = btf_file = refit = None
     if world == 1 and args.refit_steps > 0:
         # svbrdffit -j on the benchmark texels, from the headline fit's maps
@@ -514,7 +550,7 @@ def run_ours(args):
                  "note": "host wall time of svf_refit_neighborhood: luminance, 9 candidate LM fits per texel in one "
                          "launch, selection, maps pass; inputs on the device, maps to host"}
     if world == 1 and args.mlp_steps > 0:
-        learned = learned_init_item(svf, ctx, layout, samples, W, H, head_rmse, args.mlp_steps, dev)
+        learned = learned_init_item(svf, ctx, layout, samples, W, H, head_rmse, args.mlp_steps, dev, truth_np)
     if world == 1 and args.btf_steps > 0:
         btf_file = btf_file_item(svf, ctx, layout, W, H, args.btf_steps, dev)
     # the larger line items run in fresh contexts with the benchmark's buffers released
@@ -582,7 +618,7 @@ def run_ours(args):
                           "ndf_gemm": ms_ndf / args.steps, "lm": ms_fit / args.steps},
             "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
                         "failed_texels": failed, "mean_rmse": float(head_rmse.mean()),
-                        "median_rmse": float(np.median(head_rmse))},
+                        "median_rmse": float(np.median(head_rmse)), "ground_truth_error": head_truth_err},
             "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "learned_init": learned, "fib151_768x768": fib,
             "batch_8_btfs": batch, "btf_file": btf_file, "refit_neighborhood": refit, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
             "wall_s": wall,
