@@ -317,18 +317,38 @@ def batch_item(svf, ctx, steps, dev):
     for _ in range(steps):
         maps, runs, total = ctx.fit_btfs(btfs, opts=opts, want=("rmse", "stats"), check=False)
     T = sum(b["width"] * b["height"] for b in btfs)
+    # the same batch from the learned guess: one model per layout (2^18 texels, 12 epochs)
+    t0 = time.perf_counter()
+    models = {id(lay): svf.Mlp.train(ctx, lay.lights_parabolic,
+                                     svf.mlp_train_options(texels=1 << 18, epochs=12, batch=2048))[0]
+              for lay in (ring, fib)}
+    train_s = time.perf_counter() - t0
+    lbtfs = [dict(b, mlp=models[id(b["layout"])]) for b in btfs]
+    ctx.fit_btfs(lbtfs, opts=opts, want=("rmse",), check=False)
+    lmaps, lruns, ltotal = ctx.fit_btfs(lbtfs, opts=opts, want=("rmse", "stats"), check=False)
     per = []
-    for (lay, side), m, r in zip(shapes, maps, runs):
-        it = m["stats"]["iterations"]
+    for (lay, side), m, r, lm in zip(shapes, maps, runs, lmaps):
+        it, lit = m["stats"]["iterations"], lm["stats"]["iterations"]
+        ratio = lm["rmse"] / np.maximum(m["rmse"], 1e-12)
         per.append({"btf": f"{side}x{side} @ {lay.light_count}", "texels": int(r.texels),
                     "iterations_p50": float(np.percentile(it, 50)), "iterations_p99": float(np.percentile(it, 99)),
                     "mean_rmse": float(m["rmse"].mean()), "max_rmse": float(m["rmse"].max()),
-                    "failed_texels": int(r.failed_texels)})
+                    "failed_texels": int(r.failed_texels),
+                    "learned": {"iterations_p50": float(np.percentile(lit, 50)),
+                                "iterations_p99": float(np.percentile(lit, 99)),
+                                "mean_rmse": float(lm["rmse"].mean()),
+                                "residual_ratio_vs_plain": {"mean": float(lm["rmse"].mean() / m["rmse"].mean()),
+                                                            "median": float(np.median(ratio)),
+                                                            "max": float(ratio.max())}}})
+    for mdl in models.values():
+        mdl.close()
     for b in btfs:
         del b["samples"]
     torch.cuda.empty_cache()
     return {"value": T / (total.ms_total / 1e3), "unit": "texels/s", "ms_per_call": total.ms_total,
             "texels": T, "samples_gb": total_gb, "per_btf": per,
+            "learned": {"value": T / (ltotal.ms_total / 1e3), "unit": "texels/s", "ms_per_call": ltotal.ms_total,
+                        "training_s": train_s, "failed_texels": int(ltotal.failed_texels)},
             "note": "each BTF's maps equal its own svf_fit_texels fit bit for bit (tests/test_gpu_batch.py), "
                     "so the residual ratio to plain per-BTF LM is 1 by construction"}
 
