@@ -209,6 +209,45 @@ def param_error(params, truth):
     return {"normal_deg": q(ang), "log_scale": q(gm), "log_anisotropy": q(aniso), "kd_rel": q(ekd), "ks_rel": q(eks)}
 
 
+def config3_item(svf, ctx, layout, model, steps, dev, side=1024):
+    """1024x1024 texels, ring-81, FP16 samples: the plain GPU LM (default guess)
+    against the learned guess + LM, with their residuals and ground-truth errors."""
+    import torch
+
+    T = side * side
+    N = layout.light_count ** 2
+    samples = torch.empty((T, N, 3), dtype=torch.float16, device=dev)
+    truth = torch.empty((T, 16), dtype=torch.float32, device=dev)
+    ctx.synth_btf(SEED + 3, MIX, layout.lights_parabolic, 0, T, samples, sample_type=svf.SVF_SAMPLES_F16,
+                  truth=truth)
+    opts = svf.options(max_iterations=1024)
+    res = {}
+    for name, mlp in (("plain", None), ("learned", model)):
+        maps = {k: torch.zeros(s_, dtype=torch.float32, device=dev) for k, s_ in
+                {"rmse": (T,), "params": (T, 7)}.items()}
+        run = lambda: ctx.fit_texels(layout, samples, side, side, sample_type=svf.SVF_SAMPLES_F16, opts=opts,
+                                     want=tuple(maps), out=maps, check=False, mlp=mlp)[1]
+        run()
+        st = [run() for _ in range(steps)]
+        ms = sum(r.ms_total for r in st) / steps
+        res[name] = (ms, maps["rmse"].cpu().numpy(), maps["params"].cpu().numpy(), st[-1])
+    truth_np = truth.cpu().numpy()
+    del samples, truth
+    torch.cuda.empty_cache()
+    (pms, prm, ppar, prs), (lms, lrm, lpar, lrs) = res["plain"], res["learned"]
+    ratio = lrm / np.maximum(prm, 1e-12)
+    return {"workload": f"{side}x{side} texels, ring-81, FP16 RGB in HBM ({T * N * 6 / 1e9:.1f} GB), mix 20% "
+                        f"near-diffuse/10% anisotropic",
+            "plain": {"value": T / (pms / 1e3), "unit": "texels/s", "ms": pms, "mean_rmse": float(prm.mean()),
+                      "mean_iterations": prs.iterations / T, "ground_truth_error": param_error(ppar, truth_np)},
+            "learned": {"value": T / (lms / 1e3), "unit": "texels/s", "ms": lms, "mean_rmse": float(lrm.mean()),
+                        "mean_iterations": lrs.iterations / T, "ground_truth_error": param_error(lpar, truth_np),
+                        "failed_texels": int(lrs.failed_texels)},
+            "speedup": pms / lms,
+            "residual_ratio": {"mean": float(lrm.mean() / prm.mean()), "median": float(np.median(ratio)),
+                               "within_1pct": float(np.mean(ratio <= 1.01))}}
+
+
 def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, truth=None):
     """The learned initial guess (SVF_INIT_MLP) on the benchmark texels: train a model on
     separately seeded synthetic texels, then fit the same texels from its prediction."""
@@ -243,6 +282,8 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, tru
     fms = sum(r.ms_total for r in fst) / steps
     frmse = fmaps["rmse"].cpu().numpy()
     fratio = frmse / np.maximum(ref_rmse, 1e-12)
+    del fmaps
+    cfg3 = config3_item(svf, ctx, layout, model, steps, dev)
     model.close()
     return {"value": T / (ms / 1e3), "unit": "texels/s", "ms_per_step": ms, "steps": steps,
             "phases_ms": {"luminance": sum(r.ms_luminance for r in st) / steps,
@@ -254,6 +295,7 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, tru
             "rmse_ratio_vs_default_init": {"median": float(np.median(ratio)), "within_1pct": float(np.mean(ratio <= 1.01)),
                                            "better_1pct": float(np.mean(ratio < 0.99)), "p90": float(np.quantile(ratio, 0.9))},
             "training": {"seconds": train_s, "final_loss": loss, "texels": 1 << 20, "epochs": 24},
+            "config3_1024x1024_fp16": cfg3,
             "with_fallback": {"value": T / (fms / 1e3), "unit": "texels/s", "ms_per_step": fms,
                               "threshold_relative_rmse": th, "fallback_texels": fst[-1].fallback_texels,
                               "mean_rmse": float(frmse.mean()),

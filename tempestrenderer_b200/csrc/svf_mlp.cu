@@ -239,10 +239,12 @@ __global__ void gather_rows_kernel(const float* __restrict__ X, int nx, const fl
         Yb[(size_t)r * ny + j] = Y[src * ny + j];
 }
 
-// Features of one texel per CTA (256 threads) from its luminance slab row:
-// bins are summed warp by warp over the pairs listed in `order` (grouped by
-// bin, start[b] .. start[b + 1]) in a fixed order, so the result is
-// deterministic; then the 32 single pairs; log, normalised (mean may be null).
+// Features of one texel per CTA (256 threads) from its luminance slab row: the
+// row is staged in shared memory with coalesced 16-byte loads (each byte read
+// from HBM once), then bins are summed warp by warp over the pairs listed in
+// `order` (grouped by bin, start[b] .. start[b + 1]) in a fixed order, so the
+// result is deterministic; then the 32 single pairs; log, normalised (mean may
+// be null).
 __global__ void __launch_bounds__(256) features_kernel(const float* __restrict__ lum, uint64_t stride,
                                                        const uint32_t* __restrict__ order,
                                                        const uint32_t* __restrict__ start,
@@ -251,9 +253,16 @@ __global__ void __launch_bounds__(256) features_kernel(const float* __restrict__
                                                        const float* __restrict__ mean,
                                                        const float* __restrict__ rstd, float* __restrict__ X)
 {
+    extern __shared__ __align__(16) float y[];   // [stride] the texel's slab
     __shared__ float v[kMlpInputs];
     const uint64_t t = blockIdx.x;
-    const float* y = lum + t * stride;
+    {
+        const float4* src = reinterpret_cast<const float4*>(lum + t * stride);   // stride % 8 == 0
+        float4* dst = reinterpret_cast<float4*>(y);
+        for(uint32_t i = threadIdx.x; i < stride / 4; i += blockDim.x)
+            dst[i] = src[i];
+    }
+    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for(int b = warp; b < kMlpBins; b += 8)
     {
@@ -511,7 +520,18 @@ cudaError_t mlp_features(const float* lum, uint64_t stride, uint64_t texels, con
         return cudaSuccess;
     if(texels > 0x7fffffffull)
         return cudaErrorInvalidValue;
-    features_kernel<<<(unsigned)texels, 256, 0, stream>>>(lum, stride, order, start, bin_w, pairs, mean, rstd, X);
+    if(stride % 4 != 0 || (reinterpret_cast<uintptr_t>(lum) & 15u) != 0)
+        return cudaErrorInvalidValue;
+    const size_t smem = sizeof(float) * stride;
+    if(smem > 48 * 1024)
+    {
+        const cudaError_t e = cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem);
+        if(e != cudaSuccess)
+            return e;
+    }
+    features_kernel<<<(unsigned)texels, 256, smem, stream>>>(lum, stride, order, start, bin_w, pairs, mean, rstd,
+                                                             X);
     return cudaGetLastError();
 }
 
