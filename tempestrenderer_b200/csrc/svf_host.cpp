@@ -238,7 +238,8 @@ struct svf_mlp
     std::vector<float> bin_w;
     float xmean[svf::kMlpInputs] = {}, xrstd[svf::kMlpInputs] = {};
     float ymean[svf::kMlpOutputs] = {}, ystd[svf::kMlpOutputs] = {};
-    DevBuf w, wbf, m, v, g, d_pairs, d_xmean, d_xrstd, d_ymean, d_ystd, d_order, d_start, d_binw;
+    // tc_hi, tc_lo: the hidden layers' weights split into BF16 pairs (inference)
+    DevBuf w, tc_hi, tc_lo, m, v, g, d_pairs, d_xmean, d_xrstd, d_ymean, d_ystd, d_order, d_start, d_binw;
     int step = 0;
 };
 
@@ -318,7 +319,8 @@ svf_status mlp_upload(svf_ctx* ctx, svf_mlp* mlp, const std::vector<float>& w)
     SVF_TRY(mlp->g.ensure(sizeof(float) * kMlpParams));
     SVF_TRY(mlp->m.ensure(sizeof(float) * kMlpParams));
     SVF_TRY(mlp->v.ensure(sizeof(float) * kMlpParams));
-    SVF_TRY(mlp->wbf.ensure(2 * kMlpParams));
+    SVF_TRY(mlp->tc_hi.ensure(2 * kMlpTcWeights));
+    SVF_TRY(mlp->tc_lo.ensure(2 * kMlpTcWeights));
     SVF_TRY(mlp->d_pairs.ensure(sizeof(uint32_t) * kMlpPairs));
     SVF_TRY(mlp->d_xmean.ensure(sizeof(float) * kMlpInputs));
     SVF_TRY(mlp->d_xrstd.ensure(sizeof(float) * kMlpInputs));
@@ -332,34 +334,50 @@ svf_status mlp_upload(svf_ctx* ctx, svf_mlp* mlp, const std::vector<float>& w)
     SVF_CUDA(cudaMemcpyAsync(mlp->d_xrstd.p, mlp->xrstd, sizeof(mlp->xrstd), cudaMemcpyHostToDevice, ctx->stream));
     SVF_CUDA(cudaMemcpyAsync(mlp->d_ymean.p, mlp->ymean, sizeof(mlp->ymean), cudaMemcpyHostToDevice, ctx->stream));
     SVF_CUDA(cudaMemcpyAsync(mlp->d_ystd.p, mlp->ystd, sizeof(mlp->ystd), cudaMemcpyHostToDevice, ctx->stream));
-    SVF_CUDA(svf::mlp_to_bf16(mlp->w.as<float>(), kMlpParams, mlp->wbf.p, ctx->stream));
+    SVF_CUDA(svf::mlp_pack_weights(mlp->w.as<float>(), mlp->tc_hi.p, mlp->tc_lo.p, ctx->stream));
     mlp->step = 0;
     return SVF_OK;
 }
 
-// Forward pass of `rows` normalised inputs X [rows][96] -> Y [rows][10]; the
-// hidden activations H1, H2 and (training) their pre-activations Z1, Z2 are
-// [rows][256].  bf16: the inference copies of the weights.
+// Training forward pass (FP32) of `rows` normalised inputs X [rows][96] -> Y
+// [rows][8]; the hidden activations H1, H2 and their pre-activations Z1, Z2 are
+// [rows][256].
 svf_status mlp_forward(svf_ctx* ctx, const svf_mlp* mlp, const float* X, int rows, float* Z1, float* H1, float* Z2,
-                       float* H2, float* Y, bool bf16)
+                       float* H2, float* Y)
 {
     using namespace svf;
     const float* w = mlp->w.as<float>();
-    auto W = [&](size_t off) -> const void* {
-        return bf16 ? static_cast<const void*>(mlp->wbf.as<uint16_t>() + off) : static_cast<const void*>(w + off);
-    };
     const int block = 1 << 20;   // rows per launch (the GEMM grid's y extent)
     for(int r0 = 0; r0 < rows; r0 += block)
     {
         const int r = std::min(block, rows - r0);
         const size_t h = (size_t)r0 * kMlpHidden;
-        SVF_CUDA(mlp_gemm(false, true, r, kMlpHidden, kMlpInputs, X + (size_t)r0 * kMlpInputs, kMlpInputs, W(kMlpW1),
-                          bf16, kMlpInputs, H1 + h, kMlpHidden, w + kMlpB1, 1, Z1 ? Z1 + h : nullptr, nullptr,
+        SVF_CUDA(mlp_gemm(false, true, r, kMlpHidden, kMlpInputs, X + (size_t)r0 * kMlpInputs, kMlpInputs,
+                          w + kMlpW1, kMlpInputs, H1 + h, kMlpHidden, w + kMlpB1, 1, Z1 ? Z1 + h : nullptr, nullptr,
                           ctx->stream));
-        SVF_CUDA(mlp_gemm(false, true, r, kMlpHidden, kMlpHidden, H1 + h, kMlpHidden, W(kMlpW2), bf16, kMlpHidden,
+        SVF_CUDA(mlp_gemm(false, true, r, kMlpHidden, kMlpHidden, H1 + h, kMlpHidden, w + kMlpW2, kMlpHidden,
                           H2 + h, kMlpHidden, w + kMlpB2, 1, Z2 ? Z2 + h : nullptr, nullptr, ctx->stream));
-        SVF_CUDA(mlp_gemm(false, true, r, kMlpOutputs, kMlpHidden, H2 + h, kMlpHidden, W(kMlpW3), bf16, kMlpHidden,
+        SVF_CUDA(mlp_gemm(false, true, r, kMlpOutputs, kMlpHidden, H2 + h, kMlpHidden, w + kMlpW3, kMlpHidden,
                           Y + (size_t)r0 * kMlpOutputs, kMlpOutputs, w + kMlpB3, 0, nullptr, nullptr, ctx->stream));
+    }
+    return SVF_OK;
+}
+
+// Inference of `rows` normalised inputs X [rows][96] -> Y [rows][8] on the
+// tensor cores; C, act: scratch of [rows][256] floats each.  A bounded wait that
+// expires in a GEMM raises error word 2.
+svf_status mlp_infer(svf_ctx* ctx, const svf_mlp* mlp, const float* X, uint64_t rows, float* C, float* act, float* Y)
+{
+    using namespace svf;
+    const uint64_t block = 1ull << 20;   // rows per pass (within the GEMM grid's y extent)
+    for(uint64_t r0 = 0; r0 < rows; r0 += block)
+    {
+        const uint64_t r = std::min(block, rows - r0);
+        const cudaError_t e = mlp_forward_tc(X + r0 * kMlpInputs, r, mlp->tc_hi.p, mlp->tc_lo.p, mlp->w.as<float>(),
+                                             C + r0 * kMlpHidden, act + r0 * kMlpHidden, Y + r0 * kMlpOutputs,
+                                             ctx->error.as<uint32_t>() + 2, ctx->stream);
+        if(e != cudaSuccess)
+            return fail(SVF_ECUDA, "MLP inference launch: %s", cudaGetErrorString(e));
     }
     return SVF_OK;
 }
@@ -406,24 +424,24 @@ svf_status mlp_train_step(svf_ctx* ctx, svf_mlp* mlp, MlpScratch& s, const float
     float *y = s.y.as<float>(), *dy = s.dy.as<float>(), *dh2 = s.dh2.as<float>(), *dh1 = s.dh1.as<float>();
     float* w = mlp->w.as<float>();
     float* g = mlp->g.as<float>();
-    SVF_TRY(mlp_forward(ctx, mlp, X, rows, z1, h1, z2, h2, y, false));
+    SVF_TRY(mlp_forward(ctx, mlp, X, rows, z1, h1, z2, h2, y));
     SVF_CUDA(mlp_mse_grad(y, T, rows, kMlpOutputs, dy, s.loss.as<double>(), ctx->stream));
     // layer 3
-    SVF_CUDA(mlp_gemm(true, false, kMlpOutputs, kMlpHidden, rows, dy, kMlpOutputs, h2, false, kMlpHidden,
+    SVF_CUDA(mlp_gemm(true, false, kMlpOutputs, kMlpHidden, rows, dy, kMlpOutputs, h2, kMlpHidden,
                       g + kMlpW3, kMlpHidden, nullptr, 0, nullptr, nullptr, ctx->stream));
     SVF_CUDA(mlp_colsum(dy, rows, kMlpOutputs, s.dsum.as<double>(), nullptr, ctx->stream));
     SVF_CUDA(mlp_to_float(s.dsum.as<double>(), kMlpOutputs, 1.0f, g + kMlpB3, ctx->stream));
-    SVF_CUDA(mlp_gemm(false, false, rows, kMlpHidden, kMlpOutputs, dy, kMlpOutputs, w + kMlpW3, false, kMlpHidden,
+    SVF_CUDA(mlp_gemm(false, false, rows, kMlpHidden, kMlpOutputs, dy, kMlpOutputs, w + kMlpW3, kMlpHidden,
                       dh2, kMlpHidden, nullptr, 2, nullptr, z2, ctx->stream));
     // layer 2
-    SVF_CUDA(mlp_gemm(true, false, kMlpHidden, kMlpHidden, rows, dh2, kMlpHidden, h1, false, kMlpHidden,
+    SVF_CUDA(mlp_gemm(true, false, kMlpHidden, kMlpHidden, rows, dh2, kMlpHidden, h1, kMlpHidden,
                       g + kMlpW2, kMlpHidden, nullptr, 0, nullptr, nullptr, ctx->stream));
     SVF_CUDA(mlp_colsum(dh2, rows, kMlpHidden, s.dsum.as<double>(), nullptr, ctx->stream));
     SVF_CUDA(mlp_to_float(s.dsum.as<double>(), kMlpHidden, 1.0f, g + kMlpB2, ctx->stream));
-    SVF_CUDA(mlp_gemm(false, false, rows, kMlpHidden, kMlpHidden, dh2, kMlpHidden, w + kMlpW2, false, kMlpHidden,
+    SVF_CUDA(mlp_gemm(false, false, rows, kMlpHidden, kMlpHidden, dh2, kMlpHidden, w + kMlpW2, kMlpHidden,
                       dh1, kMlpHidden, nullptr, 2, nullptr, z1, ctx->stream));
     // layer 1
-    SVF_CUDA(mlp_gemm(true, false, kMlpHidden, kMlpInputs, rows, dh1, kMlpHidden, X, false, kMlpInputs, g + kMlpW1,
+    SVF_CUDA(mlp_gemm(true, false, kMlpHidden, kMlpInputs, rows, dh1, kMlpHidden, X, kMlpInputs, g + kMlpW1,
                       kMlpInputs, nullptr, 0, nullptr, nullptr, ctx->stream));
     SVF_CUDA(mlp_colsum(dh1, rows, kMlpHidden, s.dsum.as<double>(), nullptr, ctx->stream));
     SVF_CUDA(mlp_to_float(s.dsum.as<double>(), kMlpHidden, 1.0f, g + kMlpB1, ctx->stream));
@@ -842,7 +860,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     return SVF_OK;
 }
 
-// Error words: [0] LM kernel, [2] NDF GEMM.  Zeroed once per call, so that a
+// Error words: [0] LM kernel, [2] tensor-core GEMMs (NDF operator, MLP).  Zeroed once per call, so that a
 // flag raised by any launch of the call is seen.
 svf_status zero_error_flags(svf_ctx* ctx)
 {
@@ -859,7 +877,7 @@ svf_status read_error_flag(svf_ctx* ctx, bool with_ndf)
     if(flag[0])
         return fail(SVF_ETIMEOUT, "a bounded device wait expired (a texel slab did not arrive)");
     if(with_ndf && flag[2])
-        return fail(SVF_ETIMEOUT, "a bounded device wait expired in the NDF GEMM");
+        return fail(SVF_ETIMEOUT, "a bounded device wait expired in a tensor-core GEMM");
     return SVF_OK;
 }
 
@@ -1311,8 +1329,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         else if(mlp)
         {
             // the learned initial guess from the chunk's features
-            SVF_TRY(mlp_forward(ctx, mlp, ctx->mlp_x.as<float>(), (int)n, nullptr, ctx->mlp_h1.as<float>(), nullptr,
-                                ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>(), true));
+            SVF_TRY(mlp_infer(ctx, mlp, ctx->mlp_x.as<float>(), n, ctx->mlp_h1.as<float>(), ctx->mlp_h2.as<float>(),
+                              ctx->mlp_y.as<float>()));
             SVF_CUDA(svf::mlp_finish(ctx->mlp_y.as<float>(), n, mlp->d_ymean.as<float>(), mlp->d_ystd.as<float>(),
                                      ctx->init.as<float>(), ctx->stream));
         }
@@ -1515,7 +1533,7 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
     std::vector<svf_texel_stats> st(T);
     SVF_CUDA(cudaMemcpyAsync(st.data(), ctx->stats.p, sizeof(svf_texel_stats) * T, cudaMemcpyDeviceToHost,
                              ctx->stream));
-    SVF_TRY(read_error_flag(ctx, default_init));   // waits for the compute stream
+    SVF_TRY(read_error_flag(ctx, default_init || mlp));   // waits for the compute stream
     SVF_CUDA(cudaStreamSynchronize(ctx->copy_stream));
     if(maps->stats)
         SVF_CUDA(cudaMemcpy(maps->stats, st.data(), sizeof(svf_texel_stats) * T, cudaMemcpyDefault));
@@ -1788,8 +1806,8 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             {
                 SVF_CUDA(mlp_features_of(x.mlp, samples, v.sample_type, N, lum, x.stride, p.count,
                                          ctx->mlp_x.as<float>(), true, ctx->stream));
-                SVF_TRY(mlp_forward(ctx, x.mlp, ctx->mlp_x.as<float>(), (int)p.count, nullptr, ctx->mlp_h1.as<float>(),
-                                    nullptr, ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>(), true));
+                SVF_TRY(mlp_infer(ctx, x.mlp, ctx->mlp_x.as<float>(), p.count, ctx->mlp_h1.as<float>(),
+                                  ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>()));
                 SVF_CUDA(svf::mlp_finish(ctx->mlp_y.as<float>(), p.count, x.mlp->d_ymean.as<float>(),
                                          x.mlp->d_ystd.as<float>(), ctx->init.as<float>() + 7 * p.k0, ctx->stream));
             }
@@ -1886,7 +1904,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                         ctx->ndf_tex.as<float>() + (uint64_t)svf::kNdfTexels * k, sizeof(float) * svf::kNdfTexels * c));
         }
         SVF_CUDA(cudaEventRecord(ctx->ev[4], ctx->stream));
-        SVF_TRY(read_error_flag(ctx, any_default));   // waits for the chunk
+        SVF_TRY(read_error_flag(ctx, any_default || max_mlp));   // waits for the chunk
         for(auto& p : ch)
         {
             svf_run_stats& q = rs[p.b];
@@ -2240,7 +2258,7 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_ml
                                    (float)(o.lr * (0.05 + 0.95 * f)), false));
         }
     }
-    SVF_CUDA(mlp_to_bf16(mlp->w.as<float>(), kMlpParams, mlp->wbf.p, ctx->stream));
+    SVF_CUDA(mlp_pack_weights(mlp->w.as<float>(), mlp->tc_hi.p, mlp->tc_lo.p, ctx->stream));
     double loss = 0.0;
     SVF_CUDA(cudaMemcpyAsync(&loss, scratch.loss.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -2268,6 +2286,7 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
     const uint32_t c = std::min(chunk, texels);
     const uint64_t stride = round_up(N, 8);
     DevBuf staged, x, h1, h2, y, p, lum, avg;
+    SVF_TRY(zero_error_flags(ctx));
     if(!on_device)
         SVF_TRY(staged.ensure(texel_bytes * c));
     SVF_TRY(lum.ensure(sizeof(float) * stride * c));
@@ -2290,8 +2309,7 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
                                   ctx->stream));
         SVF_CUDA(mlp_features_of(mlp, s, sample_type, N, lum.as<float>(), stride, n, x.as<float>(), true,
                                  ctx->stream));
-        SVF_TRY(mlp_forward(ctx, mlp, x.as<float>(), (int)n, nullptr, h1.as<float>(), nullptr, h2.as<float>(),
-                            y.as<float>(), true));
+        SVF_TRY(mlp_infer(ctx, mlp, x.as<float>(), n, h1.as<float>(), h2.as<float>(), y.as<float>()));
         SVF_CUDA(mlp_finish(y.as<float>(), n, mlp->d_ymean.as<float>(), mlp->d_ystd.as<float>(), p.as<float>(),
                             ctx->stream));
         SVF_CUDA(cudaMemcpyAsync(params + (size_t)7 * c0, p.p, sizeof(float) * 7 * n, cudaMemcpyDefault,
@@ -2302,7 +2320,7 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
         // staged, x and p are reused by the next chunk
         SVF_CUDA(cudaStreamSynchronize(ctx->stream));
     }
-    return SVF_OK;
+    return read_error_flag(ctx, true);
 }
 
 svf_status svf_mlp_step(svf_ctx* ctx, svf_mlp* mlp, const float* features, const float* targets, uint32_t rows,
@@ -2321,7 +2339,7 @@ svf_status svf_mlp_step(svf_ctx* ctx, svf_mlp* mlp, const float* features, const
     SVF_TRY(s.loss.ensure(sizeof(double)));
     SVF_CUDA(cudaMemsetAsync(s.loss.p, 0, sizeof(double), ctx->stream));
     SVF_TRY(mlp_train_step(ctx, mlp, s, X.as<float>(), Y.as<float>(), (int)rows, lr, sgd != 0));
-    SVF_CUDA(mlp_to_bf16(mlp->w.as<float>(), kMlpParams, mlp->wbf.p, ctx->stream));
+    SVF_CUDA(mlp_pack_weights(mlp->w.as<float>(), mlp->tc_hi.p, mlp->tc_lo.p, ctx->stream));
     double l = 0.0;
     SVF_CUDA(cudaMemcpyAsync(&l, s.loss.p, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));

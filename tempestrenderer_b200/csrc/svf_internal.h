@@ -183,17 +183,15 @@ constexpr size_t kMlpW3 = kMlpB2 + kMlpHidden, kMlpB3 = kMlpW3 + (size_t)kMlpOut
 constexpr size_t kMlpParams = kMlpB3 + kMlpOutputs;
 
 // C[M][N] = op(A) op(B) (+ bias[n]); mode 1: Z = C (if Z), C = gelu(C); mode 2:
-// C *= gelu'(Zin).  b_bf16: B is BF16 (only with op(B) = B^T).
-cudaError_t mlp_gemm(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const void* B, bool b_bf16,
-                     int ldb, float* C, int ldc, const float* bias, int mode, float* Z, const float* Zin,
-                     cudaStream_t stream);
+// C *= gelu'(Zin).  FP32 (training).
+cudaError_t mlp_gemm(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const float* B, int ldb,
+                     float* C, int ldc, const float* bias, int mode, float* Z, const float* Zin, cudaStream_t stream);
 cudaError_t mlp_colsum(const float* X, int M, int N, double* sum, double* sumsq, cudaStream_t stream);
 cudaError_t mlp_to_float(const double* x, int n, float scale, float* y, cudaStream_t stream);
 cudaError_t mlp_normalize(float* X, int M, int N, const float* mean, const float* rstd, cudaStream_t stream);
 cudaError_t mlp_mse_grad(const float* Y, const float* T, int M, int N, float* dY, double* loss, cudaStream_t stream);
 cudaError_t mlp_adam(float* w, const float* g, float* m, float* v, size_t n, float lr, int step, bool sgd,
                      cudaStream_t stream);
-cudaError_t mlp_to_bf16(const float* x, size_t n, void* y, cudaStream_t stream);
 cudaError_t mlp_gather_rows(const float* X, int nx, const float* Y, int ny, const uint32_t* idx, int rows, float* Xb,
                             float* Yb, cudaStream_t stream);
 // features [texels][96] of luminance slabs [texels][stride] (normalised when mean
@@ -204,6 +202,17 @@ cudaError_t mlp_features(const float* lum, uint64_t stride, uint64_t texels, con
 // features [texels][96] of RGB samples [texels][N][3]: 32 pairs x RGB
 cudaError_t mlp_features_rgb(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
                              const uint32_t* pairs, const float* mean, const float* rstd, float* X, cudaStream_t stream);
+// Inference weights of the hidden layers for the tensor cores: BF16 hi/lo of
+// W1 | W2; kMlpTcWeights elements each.
+constexpr size_t kMlpTcWeights = (size_t)kMlpHidden * kMlpInputs + (size_t)kMlpHidden * kMlpHidden;
+cudaError_t mlp_pack_weights(const float* w, void* hi, void* lo, cudaStream_t stream);
+// Inference with the hidden layers on the tcgen05 tensor cores (the BF16x3 GEMM
+// of launch_ndf_tc) and the 8-output layer fused into the second layer's
+// epilogue: X [rows][96] -> Y [rows][8]; C: FP32 scratch [rows][256]; act:
+// BF16 scratch of 2 x [rows][256] (16-byte aligned); params: the FP32
+// parameter vector (biases, W3).
+cudaError_t mlp_forward_tc(const float* X, uint64_t rows, const void* w_hi, const void* w_lo, const float* params,
+                           float* C, void* act, float* Y, uint32_t* error_flag, cudaStream_t stream);
 cudaError_t mlp_targets(const float* p7, uint64_t texels, float* Y, cudaStream_t stream);
 cudaError_t mlp_finish(const float* Yn, uint64_t texels, const float* mean, const float* std, float* p7,
                        cudaStream_t stream);

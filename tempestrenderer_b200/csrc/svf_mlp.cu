@@ -54,15 +54,14 @@ __device__ __forceinline__ float gelu_grad(float x)
 }
 
 __device__ __forceinline__ float to_f(float x) { return x; }
-__device__ __forceinline__ float to_f(__nv_bfloat16 x) { return __bfloat162float(x); }
 __device__ __forceinline__ float to_f(__half x) { return __half2float(x); }
 
 // C[M][N] = op(A) op(B) with op(A)[m][k] = kTA ? A[k][m] : A[m][k] and
 // op(B)[k][n] = kTB ? B[n][k] : B[k][n] (leading dimensions lda, ldb); then
 // + bias[n]; mode 1: Z = C, C = gelu(Z); mode 2: C *= gelu'(Zin).
-template <bool kTA, bool kTB, typename TB>
+template <bool kTA, bool kTB>
 __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(int M, int N, int K, const float* __restrict__ A, int lda,
-                                                            const TB* __restrict__ B, int ldb, float* __restrict__ C,
+                                                            const float* __restrict__ B, int ldb, float* __restrict__ C,
                                                             int ldc, const float* __restrict__ bias, int mode,
                                                             float* __restrict__ Z, const float* __restrict__ Zin)
 {
@@ -79,7 +78,7 @@ __global__ void __launch_bounds__(kGemmThreads) gemm_kernel(int M, int N, int K,
             const int m = m0 + mm, k = k0 + kk;
             As[kk][mm] = (m < M && k < K) ? (kTA ? A[(size_t)k * lda + m] : A[(size_t)m * lda + k]) : 0.0f;
             const int n = n0 + mm;
-            Bs[kk][mm] = (n < N && k < K) ? to_f(kTB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n]) : 0.0f;
+            Bs[kk][mm] = (n < N && k < K) ? (kTB ? B[(size_t)n * ldb + k] : B[(size_t)k * ldb + n]) : 0.0f;
         }
         __syncthreads();
 #pragma unroll
@@ -215,13 +214,6 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
     m[i] = mi;
     v[i] = vi;
     w[i] -= lr * (mi * c1) / (sqrtf(vi * c2) + 1e-8f);
-}
-
-__global__ void to_bf16_kernel(const float* __restrict__ x, size_t n, __nv_bfloat16* __restrict__ y)
-{
-    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-    if(i < n)
-        y[i] = __float2bfloat16_rn(x[i]);
 }
 
 // rows[i] = X[idx[i]] for both the features and the targets
@@ -432,32 +424,109 @@ __global__ void finish_kernel(const float* __restrict__ Yn, uint64_t texels, con
     }
 }
 
+// Inference weights of the two hidden layers for the tensor-core GEMMs, split
+// x = hi + lo into BF16 pairs (the product of the split operands, three BF16
+// MMAs with FP32 accumulation, carries FP32 accuracy): W1 [256][96] | W2
+// [256][256], row-major (out x in).
+__global__ void pack_weights_kernel(const float* __restrict__ w, __nv_bfloat16* __restrict__ hi,
+                                    __nv_bfloat16* __restrict__ lo)
+{
+    const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    const size_t n1 = (size_t)kMlpHidden * kMlpInputs, n2 = (size_t)kMlpHidden * kMlpHidden;
+    if(i >= n1 + n2)
+        return;
+    const float v = i < n1 ? w[kMlpW1 + i] : w[kMlpW2 + (i - n1)];
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[i] = h;
+    lo[i] = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
+}
+
+// Layer epilogue of the tensor-core path: a = gelu(C + bias), split into BF16
+// hi/lo rows [rows][kMlpHidden] for the next GEMM's A operand.
+__global__ void act_split_kernel(const float* __restrict__ C, uint64_t rows, const float* __restrict__ bias,
+                                 __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo)
+{
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if(i >= rows * kMlpHidden)
+        return;
+    const float v = gelu(C[i] + bias[i % kMlpHidden]);
+    const __nv_bfloat16 h = __float2bfloat16_rn(v);
+    hi[i] = h;
+    lo[i] = __float2bfloat16_rn(__fsub_rn(v, __bfloat162float(h)));
+}
+
+// Second layer's epilogue and the output layer in one pass over C: one warp per
+// row, lane l holds h = gelu(C + b2) of columns 8l .. 8l+7 and the matching
+// columns of W3 (in registers, loaded once per warp), Y[r][j] = sum_k h_k W3[j][k]
+// + b3[j] in FP32 with a fixed butterfly reduction (every lane ends with the
+// same bits).  Persistent warps stride over the rows.
+__global__ void __launch_bounds__(256) act_out_kernel(const float* __restrict__ C, uint64_t rows,
+                                                      const float* __restrict__ b2, const float* __restrict__ w3,
+                                                      const float* __restrict__ b3, float* __restrict__ Y)
+{
+    static_assert(kMlpHidden == 32 * 8, "one warp covers a hidden row in 8-column slices");
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    float w[kMlpOutputs][8], b[8];
+#pragma unroll
+    for(int i = 0; i < 8; ++i)
+    {
+        b[i] = b2[8 * lane + i];
+#pragma unroll
+        for(int j = 0; j < kMlpOutputs; ++j)
+            w[j][i] = w3[j * kMlpHidden + 8 * lane + i];
+    }
+    const float bo = b3[lane % kMlpOutputs];
+    for(uint64_t r = warp; r < rows; r += warps)
+    {
+        const float4* src = reinterpret_cast<const float4*>(C + r * kMlpHidden + 8 * lane);
+        const float4 u = src[0], v = src[1];
+        const float a[8] = { u.x, u.y, u.z, u.w, v.x, v.y, v.z, v.w };
+        float acc[kMlpOutputs];
+#pragma unroll
+        for(int j = 0; j < kMlpOutputs; ++j)
+            acc[j] = 0.0f;
+#pragma unroll
+        for(int i = 0; i < 8; ++i)
+        {
+            const float h = gelu(a[i] + b[i]);
+#pragma unroll
+            for(int j = 0; j < kMlpOutputs; ++j)
+                acc[j] = fmaf(h, w[j][i], acc[j]);
+        }
+#pragma unroll
+        for(int off = 16; off > 0; off >>= 1)
+#pragma unroll
+            for(int j = 0; j < kMlpOutputs; ++j)
+                acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], off);
+        float out = acc[0];
+#pragma unroll
+        for(int j = 1; j < kMlpOutputs; ++j)
+            out = lane == j ? acc[j] : out;
+        if(lane < kMlpOutputs)
+            Y[r * kMlpOutputs + lane] = out + bo;
+    }
+}
+
 inline unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)((n + threads - 1) / threads); }
 
 } // namespace
 
-cudaError_t mlp_gemm(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const void* B, bool b_bf16,
-                     int ldb, float* C, int ldc, const float* bias, int mode, float* Z, const float* Zin,
+cudaError_t mlp_gemm(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc, const float* bias, int mode, float* Z, const float* Zin,
                      cudaStream_t stream)
 {
     dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
     if(grid.y > 65535)
         return cudaErrorInvalidValue;
-#define SVF_GEMM(TA, TB, T)                                                                                       \
-    gemm_kernel<TA, TB, T><<<grid, kGemmThreads, 0, stream>>>(M, N, K, A, lda, static_cast<const T*>(B), ldb, C, \
-                                                              ldc, bias, mode, Z, Zin)
-    if(b_bf16)
-    {
-        if(ta || !tb)
-            return cudaErrorInvalidValue;   // inference only: X W^T
-        SVF_GEMM(false, true, __nv_bfloat16);
-    }
-    else if(!ta && tb)
-        SVF_GEMM(false, true, float);
+#define SVF_GEMM(TA, TB) \
+    gemm_kernel<TA, TB><<<grid, kGemmThreads, 0, stream>>>(M, N, K, A, lda, B, ldb, C, ldc, bias, mode, Z, Zin)
+    if(!ta && tb)
+        SVF_GEMM(false, true);
     else if(ta && !tb)
-        SVF_GEMM(true, false, float);
+        SVF_GEMM(true, false);
     else if(!ta && !tb)
-        SVF_GEMM(false, false, float);
+        SVF_GEMM(false, false);
     else
         return cudaErrorInvalidValue;
 #undef SVF_GEMM
@@ -497,11 +566,6 @@ cudaError_t mlp_adam(float* w, const float* g, float* m, float* v, size_t n, flo
     return cudaGetLastError();
 }
 
-cudaError_t mlp_to_bf16(const float* x, size_t n, void* y, cudaStream_t stream)
-{
-    to_bf16_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(x, n, static_cast<__nv_bfloat16*>(y));
-    return cudaGetLastError();
-}
 
 cudaError_t mlp_gather_rows(const float* X, int nx, const float* Y, int ny, const uint32_t* idx, int rows, float* Xb,
                             float* Yb, cudaStream_t stream)
@@ -547,6 +611,46 @@ cudaError_t mlp_features_rgb(const void* samples, uint32_t sample_type, uint64_t
     else
         features_rgb_kernel<float><<<b, 256, 0, stream>>>(static_cast<const float*>(samples), texels, N, pairs, mean,
                                                            rstd, X);
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_pack_weights(const float* w, void* hi, void* lo, cudaStream_t stream)
+{
+    const size_t n = kMlpTcWeights;
+    pack_weights_kernel<<<blocks_for(n, 256), 256, 0, stream>>>(w, static_cast<__nv_bfloat16*>(hi),
+                                                                static_cast<__nv_bfloat16*>(lo));
+    return cudaGetLastError();
+}
+
+cudaError_t mlp_forward_tc(const float* X, uint64_t rows, const void* w_hi, const void* w_lo, const float* params,
+                           float* C, void* act, float* Y, uint32_t* error_flag, cudaStream_t stream)
+{
+    if(rows == 0)
+        return cudaSuccess;
+    __nv_bfloat16* a_hi = static_cast<__nv_bfloat16*>(act);
+    const size_t o2 = (size_t)kMlpHidden * kMlpInputs;
+    const __nv_bfloat16* whi = static_cast<const __nv_bfloat16*>(w_hi);
+    const __nv_bfloat16* wlo = static_cast<const __nv_bfloat16*>(w_lo);
+    // layer 1: A = X split, K = 96
+    cudaError_t e = launch_split_bf16(X, rows * kMlpInputs, a_hi, a_hi + rows * kMlpInputs, stream);
+    if(e != cudaSuccess)
+        return e;
+    e = launch_ndf_tc(a_hi, a_hi + rows * kMlpInputs, rows, kMlpInputs, whi, wlo, kMlpHidden, kMlpInputs, kMlpInputs,
+                      C, kMlpHidden, error_flag, stream);
+    if(e != cudaSuccess)
+        return e;
+    const unsigned bh = blocks_for(rows * kMlpHidden, 256);
+    __nv_bfloat16* a_lo = a_hi + rows * kMlpHidden;
+    act_split_kernel<<<bh, 256, 0, stream>>>(C, rows, params + kMlpB1, a_hi, a_lo);
+    // layer 2
+    e = launch_ndf_tc(a_hi, a_lo, rows, kMlpHidden, whi + o2, wlo + o2, kMlpHidden, kMlpHidden, kMlpHidden, C,
+                      kMlpHidden, error_flag, stream);
+    if(e != cudaSuccess)
+        return e;
+    // layer 2's activation and the 8-output layer
+    const uint64_t blocks = std::min<uint64_t>((rows + 7) / 8, 148ull * 8);
+    act_out_kernel<<<(unsigned)blocks, 256, 0, stream>>>(C, rows, params + kMlpB2, params + kMlpW3,
+                                                        params + kMlpB3, Y);
     return cudaGetLastError();
 }
 
