@@ -382,19 +382,34 @@ svf_status mlp_infer(svf_ctx* ctx, const svf_mlp* mlp, const float* X, uint64_t 
     return SVF_OK;
 }
 
-// Features [n][96] of n texels -- from their RGB samples [n][N][3] or their
-// luminance slabs [n][stride], as the model's feature set reads them --
-// normalised with the model's statistics when `normalise`.
-cudaError_t mlp_features_of(const svf_mlp* mlp, const void* samples, uint32_t sample_type, uint32_t N,
-                            const float* lum, uint64_t stride, uint64_t n, float* X, bool normalise,
-                            cudaStream_t stream)
+// Features [n][96] of n texels, normalised with the model's statistics when
+// `normalise`.  The bin features come out of the luminance pass (lum_features
+// gives its arguments; none for a model of another feature set or without a
+// model); the RGB-pair features are read from the samples (rgb_features, which
+// does nothing for a bins model).
+svf::LumFeatures lum_features(const svf_mlp* mlp, float* X, bool normalise)
 {
-    const float* mean = normalise ? mlp->d_xmean.as<float>() : nullptr;
-    const float* rstd = normalise ? mlp->d_xrstd.as<float>() : nullptr;
-    if(mlp->features == SVF_MLP_FEATURES_PAIRS_RGB)
-        return svf::mlp_features_rgb(samples, sample_type, n, N, mlp->d_pairs.as<uint32_t>(), mean, rstd, X, stream);
-    return svf::mlp_features(lum, stride, n, mlp->d_order.as<uint32_t>(), mlp->d_start.as<uint32_t>(),
-                             mlp->d_binw.as<float>(), mlp->d_pairs.as<uint32_t>(), mean, rstd, X, stream);
+    svf::LumFeatures f;
+    if(!mlp || mlp->features != SVF_MLP_FEATURES_BINS)
+        return f;
+    f.order = mlp->d_order.as<uint32_t>();
+    f.start = mlp->d_start.as<uint32_t>();
+    f.bin_w = mlp->d_binw.as<float>();
+    f.pairs = mlp->d_pairs.as<uint32_t>();
+    f.mean = normalise ? mlp->d_xmean.as<float>() : nullptr;
+    f.rstd = normalise ? mlp->d_xrstd.as<float>() : nullptr;
+    f.X = X;
+    return f;
+}
+
+cudaError_t rgb_features(const svf_mlp* mlp, const void* samples, uint32_t sample_type, uint32_t N, uint64_t n,
+                         float* X, bool normalise, cudaStream_t stream)
+{
+    if(!mlp || mlp->features != SVF_MLP_FEATURES_PAIRS_RGB)
+        return cudaSuccess;
+    return svf::mlp_features_rgb(samples, sample_type, n, N, mlp->d_pairs.as<uint32_t>(),
+                                 normalise ? mlp->d_xmean.as<float>() : nullptr,
+                                 normalise ? mlp->d_xrstd.as<float>() : nullptr, X, stream);
 }
 
 // Scratch of one training step for `rows` rows (in the context).
@@ -1303,10 +1318,10 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
                                        ctx->avg.as<float>(), default_init ? ctx->lum_hi.p : nullptr,
                                        default_init ? ctx->lum_lo.p : nullptr, ctx->stream,
-                                       rgb ? ctx->rgb16.p : nullptr, stride3));
-        if(mlp)   // the learned guess's inputs, read before the staging buffer is handed back
-            SVF_CUDA(mlp_features_of(mlp, samples, btf->sample_type, N, ctx->lum.as<float>(), stride, n,
-                                     ctx->mlp_x.as<float>(), true, ctx->stream));
+                                       rgb ? ctx->rgb16.p : nullptr, stride3,
+                                       lum_features(mlp, ctx->mlp_x.as<float>(), true)));
+        // the learned guess's inputs, read before the staging buffer is handed back
+        SVF_CUDA(rgb_features(mlp, samples, btf->sample_type, N, n, ctx->mlp_x.as<float>(), true, ctx->stream));
         if(!samples_on_device)
         {
             SVF_CUDA(cudaEventRecord(ctx->freed[buf], ctx->stream));
@@ -1786,7 +1801,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                                            x.default_init ? ctx->lum_hi.as<uint16_t>() + p.off : nullptr,
                                            x.default_init ? ctx->lum_lo.as<uint16_t>() + p.off : nullptr,
                                            ctx->stream, rgb ? ctx->rgb16.as<uint16_t>() + p.off3 : nullptr,
-                                           x.stride3));
+                                           x.stride3, lum_features(x.mlp, ctx->mlp_x.as<float>(), true)));
             if(x.default_init)
             {
                 cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.as<uint16_t>() + p.off, ctx->lum_lo.as<uint16_t>() + p.off,
@@ -1804,8 +1819,8 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             }
             else if(x.mlp)
             {
-                SVF_CUDA(mlp_features_of(x.mlp, samples, v.sample_type, N, lum, x.stride, p.count,
-                                         ctx->mlp_x.as<float>(), true, ctx->stream));
+                SVF_CUDA(rgb_features(x.mlp, samples, v.sample_type, N, p.count, ctx->mlp_x.as<float>(), true,
+                                      ctx->stream));
                 SVF_TRY(mlp_infer(ctx, x.mlp, ctx->mlp_x.as<float>(), p.count, ctx->mlp_h1.as<float>(),
                                   ctx->mlp_h2.as<float>(), ctx->mlp_y.as<float>()));
                 SVF_CUDA(svf::mlp_finish(ctx->mlp_y.as<float>(), p.count, x.mlp->d_ymean.as<float>(),
@@ -2163,10 +2178,10 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_ml
         const svf_status st = svf_fit_texels(ctx, &v, &fo, &m, nullptr);
         if(st != SVF_OK && st != SVF_EPARTIAL)
             return st;
+        float* Xc = X.as<float>() + (size_t)kMlpInputs * c0;
         SVF_CUDA(launch_luminance(samples.p, SVF_SAMPLES_F32, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr,
-                                  nullptr, ctx->stream));
-        SVF_CUDA(mlp_features_of(mlp.get(), samples.p, SVF_SAMPLES_F32, N, lum.as<float>(), stride, n,
-                                 X.as<float>() + (size_t)kMlpInputs * c0, false, ctx->stream));
+                                  nullptr, ctx->stream, nullptr, 0, lum_features(mlp.get(), Xc, false)));
+        SVF_CUDA(rgb_features(mlp.get(), samples.p, SVF_SAMPLES_F32, N, n, Xc, false, ctx->stream));
         SVF_CUDA(mlp_targets(params.as<float>(), n, Y.as<float>() + (size_t)kMlpOutputs * c0, ctx->stream));
     }
     samples.reset();
@@ -2306,9 +2321,8 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
             s = staged.p;
         }
         SVF_CUDA(launch_luminance(s, sample_type, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr, nullptr,
-                                  ctx->stream));
-        SVF_CUDA(mlp_features_of(mlp, s, sample_type, N, lum.as<float>(), stride, n, x.as<float>(), true,
-                                 ctx->stream));
+                                  ctx->stream, nullptr, 0, lum_features(mlp, x.as<float>(), true)));
+        SVF_CUDA(rgb_features(mlp, s, sample_type, N, n, x.as<float>(), true, ctx->stream));
         SVF_TRY(mlp_infer(ctx, mlp, x.as<float>(), n, h1.as<float>(), h2.as<float>(), y.as<float>()));
         SVF_CUDA(mlp_finish(y.as<float>(), n, mlp->d_ymean.as<float>(), mlp->d_ystd.as<float>(), p.as<float>(),
                             ctx->stream));

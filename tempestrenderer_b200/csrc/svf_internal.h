@@ -83,9 +83,23 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
 // NDF GEMM, same row pitch, columns [0, N) written.
 // rgb16 (optional): the samples again as FP16 RGB slabs [texels][rgb_stride]
 // for the RGB fit (rgb_stride >= 3 N, a multiple of 8).
+// The learned guess's half-vector-bin features, computed by the luminance pass
+// from the slab it holds in shared memory (X null: none).  The pairs of bin b
+// are order[start[b] .. start[b + 1]) and their mean is the sum times bin_w[b];
+// then the luminance of the 32 single pairs; log, normalised with mean/rstd
+// (mean null: raw).  X: [texels][kMlpInputs].
+struct LumFeatures
+{
+    const uint32_t *order = nullptr, *start = nullptr;
+    const float* bin_w = nullptr;
+    const uint32_t* pairs = nullptr;
+    const float *mean = nullptr, *rstd = nullptr;
+    float* X = nullptr;
+};
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
                              float* lum, uint64_t lum_stride, float* avg_chroma, void* lum_hi, void* lum_lo,
-                             cudaStream_t stream, void* rgb16 = nullptr, uint64_t rgb_stride = 0);
+                             cudaStream_t stream, void* rgb16 = nullptr, uint64_t rgb_stride = 0,
+                             const LumFeatures& features = LumFeatures{});
 
 // The RGB fit's initial parameters {kd rgb, ks rgb, sx, sy, quaternion xyzw}
 // from a luminance initial guess {sx, sy, ks, kd, euler} and the texel's
@@ -196,9 +210,6 @@ cudaError_t mlp_gather_rows(const float* X, int nx, const float* Y, int ny, cons
                             float* Yb, cudaStream_t stream);
 // features [texels][96] of luminance slabs [texels][stride] (normalised when mean
 // != null): bins over order[start[b] .. start[b + 1]) scaled by bin_w[b], pairs
-cudaError_t mlp_features(const float* lum, uint64_t stride, uint64_t texels, const uint32_t* order,
-                         const uint32_t* start, const float* bin_w, const uint32_t* pairs, const float* mean,
-                         const float* rstd, float* X, cudaStream_t stream);
 // features [texels][96] of RGB samples [texels][N][3]: 32 pairs x RGB
 cudaError_t mlp_features_rgb(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
                              const uint32_t* pairs, const float* mean, const float* rstd, float* X, cudaStream_t stream);

@@ -29,52 +29,115 @@ __device__ __forceinline__ float to_f<float>(float x) { return x; }
 template <>
 __device__ __forceinline__ float to_f<__half>(__half x) { return __half2float(x); }
 
-// One CTA per texel.  lum = 0.2126 R + 0.7152 G + 0.0722 B (spectrum.hh:328-331,
-// evaluated without fused multiply-adds, as the reference's x86-64 build does);
-// chromaticity rgb/lum, or (1,1,1) when lum <= 1e-6, averaged over the pairs.
-template <typename T>
-__global__ void __launch_bounds__(256) luminance_kernel(const T* __restrict__ samples, uint32_t N, float* __restrict__ lum,
-                                                         uint64_t lum_stride, float* __restrict__ avg,
-                                                         __nv_bfloat16* __restrict__ lum_hi,
-                                                         __nv_bfloat16* __restrict__ lum_lo,
-                                                         __half* __restrict__ rgb16, uint64_t rgb_stride)
+constexpr uint32_t kLumThreads = 256;
+constexpr int kLumUnroll = 4;   // pairs whose loads are in flight together per thread
+
+// The learned guess's features of one texel from its luminance slab y (shared
+// memory, complete), by a CTA of kLumThreads: bins summed warp by warp over
+// their pairs in `order` in a fixed order (deterministic), the single pairs,
+// log, normalised.  v: shared scratch of kMlpInputs floats.
+__device__ void texel_features(const float* y, const LumFeatures& f, uint64_t t, float* v)
 {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for(int b = warp; b < kMlpBins; b += kLumThreads / 32)
+    {
+        float s = 0.0f;
+        for(uint32_t k = f.start[b] + lane; k < f.start[b + 1]; k += 32)
+            s += y[f.order[k]];
+#pragma unroll
+        for(int o = 16; o > 0; o >>= 1)
+            s += __shfl_xor_sync(0xffffffffu, s, o);
+        if(lane == 0)
+            v[b] = s * f.bin_w[b];
+    }
+    if(threadIdx.x < kMlpPairs)
+        v[kMlpBins + threadIdx.x] = y[f.pairs[threadIdx.x]];
+    __syncthreads();
+    if(threadIdx.x < kMlpInputs)
+    {
+        const int i = threadIdx.x;
+        float x = logf(fmaxf(v[i], 1e-6f));
+        if(f.mean)
+            x = (x - f.mean[i]) * f.rstd[i];
+        f.X[t * kMlpInputs + i] = x;
+    }
+}
+
+// One CTA of kLumThreads per texel.  lum = 0.2126 R + 0.7152 G + 0.0722 B
+// (spectrum.hh:328-331, evaluated without fused multiply-adds, as the
+// reference's x86-64 build does); chromaticity rgb/lum, or (1,1,1) when lum <=
+// 1e-6, averaged over the pairs.  Thread j takes pairs j, j + 256, ... in that
+// order, the loads of kLumUnroll of them issued together (the pass is bound by
+// the bytes in flight).  With features, the slab is also kept in dynamic shared
+// memory and the features are computed from it.
+template <typename T>
+__global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restrict__ samples, uint32_t N,
+                                                                float* __restrict__ lum, uint64_t lum_stride,
+                                                                float* __restrict__ avg,
+                                                                __nv_bfloat16* __restrict__ lum_hi,
+                                                                __nv_bfloat16* __restrict__ lum_lo,
+                                                                __half* __restrict__ rgb16, uint64_t rgb_stride,
+                                                                LumFeatures feat)
+{
+    extern __shared__ __align__(16) float y[];   // [N] with features
     const uint64_t t = blockIdx.x;
     const T* src = samples + t * (uint64_t)N * 3;
     float* dst = lum + t * lum_stride;
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
-    for(uint32_t i = threadIdx.x; i < N; i += blockDim.x)
+    for(uint32_t i0 = threadIdx.x; i0 < N; i0 += kLumUnroll * kLumThreads)
     {
-        float r = to_f(src[3 * i]), g = to_f(src[3 * i + 1]), b = to_f(src[3 * i + 2]);
-        float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
-        dst[i] = l;
-        if(rgb16)
+        float rr[kLumUnroll], gg[kLumUnroll], bb[kLumUnroll];
+#pragma unroll
+        for(int u = 0; u < kLumUnroll; ++u)
         {
-            // the RGB fit's slab: the samples in FP16, [L*L][3], 16-byte rows
-            __half* o = rgb16 + t * rgb_stride + 3 * (uint64_t)i;
-            o[0] = __float2half_rn(r);
-            o[1] = __float2half_rn(g);
-            o[2] = __float2half_rn(b);
+            const uint32_t i = i0 + u * kLumThreads;
+            rr[u] = gg[u] = bb[u] = 0.0f;
+            if(i < N)
+            {
+                rr[u] = to_f(src[3 * i]);
+                gg[u] = to_f(src[3 * i + 1]);
+                bb[u] = to_f(src[3 * i + 2]);
+            }
         }
-        if(lum_hi)
+#pragma unroll
+        for(int u = 0; u < kLumUnroll; ++u)
         {
-            // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
-            const __nv_bfloat16 h = __float2bfloat16_rn(l);
-            lum_hi[t * lum_stride + i] = h;
-            lum_lo[t * lum_stride + i] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
-        }
-        if(l > 1e-6f)
-        {
-            float rl = 1.0f / l;
-            ax += r * rl;
-            ay += g * rl;
-            az += b * rl;
-        }
-        else
-        {
-            ax += 1.0f;
-            ay += 1.0f;
-            az += 1.0f;
+            const uint32_t i = i0 + u * kLumThreads;
+            if(i >= N)
+                break;
+            const float r = rr[u], g = gg[u], b = bb[u];
+            float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
+            dst[i] = l;
+            if(feat.X)
+                y[i] = l;
+            if(rgb16)
+            {
+                // the RGB fit's slab: the samples in FP16, [L*L][3], 16-byte rows
+                __half* o = rgb16 + t * rgb_stride + 3 * (uint64_t)i;
+                o[0] = __float2half_rn(r);
+                o[1] = __float2half_rn(g);
+                o[2] = __float2half_rn(b);
+            }
+            if(lum_hi)
+            {
+                // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
+                const __nv_bfloat16 h = __float2bfloat16_rn(l);
+                lum_hi[t * lum_stride + i] = h;
+                lum_lo[t * lum_stride + i] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
+            }
+            if(l > 1e-6f)
+            {
+                float rl = 1.0f / l;
+                ax += r * rl;
+                ay += g * rl;
+                az += b * rl;
+            }
+            else
+            {
+                ax += 1.0f;
+                ay += 1.0f;
+                az += 1.0f;
+            }
         }
     }
     for(uint32_t i = N + threadIdx.x; i < lum_stride; i += blockDim.x)
@@ -103,6 +166,9 @@ __global__ void __launch_bounds__(256) luminance_kernel(const T* __restrict__ sa
         // Vector3 / float multiplies by the reciprocal (vector3.hh:185-190)
         avg[3 * t + threadIdx.x] = s * (1.0f / (float)N);
     }
+    __shared__ float fv[kMlpInputs];
+    if(feat.X)   // y is complete: the __syncthreads above follows every write
+        texel_features(y, feat, t, fv);
 }
 
 __global__ void repack_kernel(const float* __restrict__ src, uint64_t src_stride, uint32_t N, float* __restrict__ dst,
@@ -455,23 +521,32 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
 
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N, float* lum,
                              uint64_t lum_stride, float* avg, void* lum_hi, void* lum_lo, cudaStream_t stream,
-                             void* rgb16, uint64_t rgb_stride)
+                             void* rgb16, uint64_t rgb_stride, const LumFeatures& features)
 {
     if(texels == 0)
         return cudaSuccess;
-    if((lum_hi == nullptr) != (lum_lo == nullptr))
+    if((lum_hi == nullptr) != (lum_lo == nullptr) || texels > 0x7fffffffull)
+        return cudaErrorInvalidValue;
+    if(features.X && !(features.order && features.start && features.bin_w && features.pairs &&
+                       (features.mean == nullptr) == (features.rstd == nullptr)))
         return cudaErrorInvalidValue;
     __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(lum_hi);
     __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(lum_lo);
+    const size_t smem = features.X ? sizeof(float) * N : 0;
+    const auto run = [&](auto kernel, const auto* src) -> cudaError_t {
+        if(smem > 48 * 1024)
+        {
+            const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if(e != cudaSuccess)
+                return e;
+        }
+        kernel<<<(unsigned)texels, kLumThreads, smem, stream>>>(src, N, lum, lum_stride, avg, hi, lo,
+                                                                static_cast<__half*>(rgb16), rgb_stride, features);
+        return cudaGetLastError();
+    };
     if(sample_type == SVF_SAMPLES_F16)
-        luminance_kernel<__half><<<(unsigned)texels, 256, 0, stream>>>(static_cast<const __half*>(samples), N, lum,
-                                                                     lum_stride, avg, hi, lo,
-                                                                     static_cast<__half*>(rgb16), rgb_stride);
-    else
-        luminance_kernel<float><<<(unsigned)texels, 256, 0, stream>>>(static_cast<const float*>(samples), N, lum,
-                                                                    lum_stride, avg, hi, lo,
-                                                                    static_cast<__half*>(rgb16), rgb_stride);
-    return cudaGetLastError();
+        return run(luminance_kernel<__half>, static_cast<const __half*>(samples));
+    return run(luminance_kernel<float>, static_cast<const float*>(samples));
 }
 
 __global__ void rgb_init_kernel(const float* __restrict__ init7, const float* __restrict__ avg, uint64_t texels,

@@ -20,7 +20,10 @@
 //
 // Training kernels: one tiled FP32 GEMM with transposes and fused bias / GELU /
 // GELU-derivative epilogues, column statistics, the MSE gradient and Adam.
-// Inference multiplies by BF16 copies of the weights, accumulating in FP32.
+// Inference: the hidden layers on the tcgen05 tensor cores (the BF16x3 GEMM of
+// svf_ndf_tc.cu, FP32 accuracy), the output layer fused into the second
+// layer's epilogue.  The bin features are computed by the luminance pass
+// (svf_kernels.cu) from the slab it holds in shared memory.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -229,55 +232,6 @@ __global__ void gather_rows_kernel(const float* __restrict__ X, int nx, const fl
         Xb[(size_t)r * nx + j] = X[src * nx + j];
     for(int j = threadIdx.x; j < ny; j += blockDim.x)
         Yb[(size_t)r * ny + j] = Y[src * ny + j];
-}
-
-// Features of one texel per CTA (256 threads) from its luminance slab row: the
-// row is staged in shared memory with coalesced 16-byte loads (each byte read
-// from HBM once), then bins are summed warp by warp over the pairs listed in
-// `order` (grouped by bin, start[b] .. start[b + 1]) in a fixed order, so the
-// result is deterministic; then the 32 single pairs; log, normalised (mean may
-// be null).
-__global__ void __launch_bounds__(256) features_kernel(const float* __restrict__ lum, uint64_t stride,
-                                                       const uint32_t* __restrict__ order,
-                                                       const uint32_t* __restrict__ start,
-                                                       const float* __restrict__ bin_w,
-                                                       const uint32_t* __restrict__ pairs,
-                                                       const float* __restrict__ mean,
-                                                       const float* __restrict__ rstd, float* __restrict__ X)
-{
-    extern __shared__ __align__(16) float y[];   // [stride] the texel's slab
-    __shared__ float v[kMlpInputs];
-    const uint64_t t = blockIdx.x;
-    {
-        const float4* src = reinterpret_cast<const float4*>(lum + t * stride);   // stride % 8 == 0
-        float4* dst = reinterpret_cast<float4*>(y);
-        for(uint32_t i = threadIdx.x; i < stride / 4; i += blockDim.x)
-            dst[i] = src[i];
-    }
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for(int b = warp; b < kMlpBins; b += 8)
-    {
-        float s = 0.0f;
-        for(uint32_t k = start[b] + lane; k < start[b + 1]; k += 32)
-            s += y[order[k]];
-#pragma unroll
-        for(int o = 16; o > 0; o >>= 1)
-            s += __shfl_xor_sync(0xffffffffu, s, o);
-        if(lane == 0)
-            v[b] = s * bin_w[b];
-    }
-    if(threadIdx.x < kMlpPairs)
-        v[kMlpBins + threadIdx.x] = y[pairs[threadIdx.x]];
-    __syncthreads();
-    if(threadIdx.x < kMlpInputs)
-    {
-        const int f = threadIdx.x;
-        float x = logf(fmaxf(v[f], 1e-6f));
-        if(mean)
-            x = (x - mean[f]) * rstd[f];
-        X[t * kMlpInputs + f] = x;
-    }
 }
 
 // Features of the 32 pairs' RGB samples (96 = 32 pairs x RGB), log-scaled and
@@ -513,8 +467,8 @@ inline unsigned blocks_for(size_t n, unsigned threads) { return (unsigned)((n + 
 
 } // namespace
 
-cudaError_t mlp_gemm(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const float* B, int ldb, float* C, int ldc, const float* bias, int mode, float* Z, const float* Zin,
-                     cudaStream_t stream)
+cudaError_t mlp_gemm(bool ta, bool tb, int M, int N, int K, const float* A, int lda, const float* B, int ldb,
+                     float* C, int ldc, const float* bias, int mode, float* Z, const float* Zin, cudaStream_t stream)
 {
     dim3 grid((N + kTile - 1) / kTile, (M + kTile - 1) / kTile);
     if(grid.y > 65535)
@@ -573,29 +527,6 @@ cudaError_t mlp_gather_rows(const float* X, int nx, const float* Y, int ny, cons
     if(rows == 0)
         return cudaSuccess;
     gather_rows_kernel<<<rows, 128, 0, stream>>>(X, nx, Y, ny, idx, rows, Xb, Yb);
-    return cudaGetLastError();
-}
-
-cudaError_t mlp_features(const float* lum, uint64_t stride, uint64_t texels, const uint32_t* order,
-                         const uint32_t* start, const float* bin_w, const uint32_t* pairs, const float* mean,
-                         const float* rstd, float* X, cudaStream_t stream)
-{
-    if(texels == 0)
-        return cudaSuccess;
-    if(texels > 0x7fffffffull)
-        return cudaErrorInvalidValue;
-    if(stride % 4 != 0 || (reinterpret_cast<uintptr_t>(lum) & 15u) != 0)
-        return cudaErrorInvalidValue;
-    const size_t smem = sizeof(float) * stride;
-    if(smem > 48 * 1024)
-    {
-        const cudaError_t e = cudaFuncSetAttribute(features_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)smem);
-        if(e != cudaSuccess)
-            return e;
-    }
-    features_kernel<<<(unsigned)texels, 256, smem, stream>>>(lum, stride, order, start, bin_w, pairs, mean, rstd,
-                                                             X);
     return cudaGetLastError();
 }
 
