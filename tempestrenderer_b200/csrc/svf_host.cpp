@@ -236,10 +236,15 @@ struct svf_mlp
     // b are order[start[b] .. start[b + 1]), their mean is the sum times bin_w[b]
     std::vector<uint32_t> order, start;
     std::vector<float> bin_w;
+    // the luminance pass keeps the slab in bin order: pair k at pos[k] (the pairs
+    // of bin b at start[b] .. start[b + 1], those with no half vector after them;
+    // zero-padded to a multiple of 8 entries); pair_pos: the single pairs' positions
+    std::vector<uint16_t> pos;
+    uint16_t pair_pos[svf::kMlpPairs] = {};
     float xmean[svf::kMlpInputs] = {}, xrstd[svf::kMlpInputs] = {};
     float ymean[svf::kMlpOutputs] = {}, ystd[svf::kMlpOutputs] = {};
     // tc_hi, tc_lo: the hidden layers' weights split into BF16 pairs (inference)
-    DevBuf w, tc_hi, tc_lo, m, v, g, d_pairs, d_xmean, d_xrstd, d_ymean, d_ystd, d_order, d_start, d_binw;
+    DevBuf w, tc_hi, tc_lo, m, v, g, d_pairs, d_xmean, d_xrstd, d_ymean, d_ystd, d_pos, d_pair_pos, d_start, d_binw;
     int step = 0;
 };
 
@@ -299,6 +304,19 @@ void mlp_bins(svf_mlp* mlp)
     mlp->bin_w.assign(kMlpBins, 0.0f);
     for(int b = 0; b < kMlpBins; ++b)
         mlp->bin_w[b] = count[b] ? 1.0f / (float)count[b] : 0.0f;
+    mlp->pos.clear();
+    if(N <= 65536u)   // 16-bit positions (the shared-memory slab holds far fewer pairs anyway)
+    {
+        mlp->pos.assign(round_up(N, 8), 0);   // whole 16-byte words for the luminance pass's copies
+        uint32_t next = mlp->start[kMlpBins];
+        for(uint32_t k = 0; k < mlp->start[kMlpBins]; ++k)
+            mlp->pos[mlp->order[k]] = (uint16_t)k;
+        for(uint32_t k = 0; k < N; ++k)
+            if(bin[k] == (uint32_t)kMlpBins)
+                mlp->pos[k] = (uint16_t)next++;
+        for(int j = 0; j < kMlpPairs; ++j)
+            mlp->pair_pos[j] = mlp->pos[mlp->pairs[j]];
+    }
 }
 
 // Uploads the host-side tables of a model and zeroes its optimiser state.
@@ -306,11 +324,14 @@ svf_status mlp_upload(svf_ctx* ctx, svf_mlp* mlp, const std::vector<float>& w)
 {
     using namespace svf;
     mlp_bins(mlp);
-    SVF_TRY(mlp->d_order.ensure(sizeof(uint32_t) * std::max<size_t>(1, mlp->order.size())));
+    SVF_TRY(mlp->d_pos.ensure(sizeof(uint16_t) * std::max<size_t>(1, mlp->pos.size())));
+    SVF_TRY(mlp->d_pair_pos.ensure(sizeof(mlp->pair_pos)));
     SVF_TRY(mlp->d_start.ensure(sizeof(uint32_t) * mlp->start.size()));
     SVF_TRY(mlp->d_binw.ensure(sizeof(float) * mlp->bin_w.size()));
-    SVF_CUDA(cudaMemcpyAsync(mlp->d_order.p, mlp->order.data(), sizeof(uint32_t) * mlp->order.size(),
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_pos.p, mlp->pos.data(), sizeof(uint16_t) * mlp->pos.size(),
                              cudaMemcpyHostToDevice, ctx->stream));
+    SVF_CUDA(cudaMemcpyAsync(mlp->d_pair_pos.p, mlp->pair_pos, sizeof(mlp->pair_pos), cudaMemcpyHostToDevice,
+                             ctx->stream));
     SVF_CUDA(cudaMemcpyAsync(mlp->d_start.p, mlp->start.data(), sizeof(uint32_t) * mlp->start.size(),
                              cudaMemcpyHostToDevice, ctx->stream));
     SVF_CUDA(cudaMemcpyAsync(mlp->d_binw.p, mlp->bin_w.data(), sizeof(float) * mlp->bin_w.size(),
@@ -392,10 +413,15 @@ svf::LumFeatures lum_features(const svf_mlp* mlp, float* X, bool normalise)
     svf::LumFeatures f;
     if(!mlp || mlp->features != SVF_MLP_FEATURES_BINS)
         return f;
-    f.order = mlp->d_order.as<uint32_t>();
+    if(mlp->pos.empty())
+    {
+        f.X = X;   // more direction pairs than 16-bit positions: launch_luminance rejects it
+        return f;
+    }
+    f.pos = mlp->d_pos.as<uint16_t>();
     f.start = mlp->d_start.as<uint32_t>();
     f.bin_w = mlp->d_binw.as<float>();
-    f.pairs = mlp->d_pairs.as<uint32_t>();
+    f.pair_pos = mlp->d_pair_pos.as<uint16_t>();
     f.mean = normalise ? mlp->d_xmean.as<float>() : nullptr;
     f.rstd = normalise ? mlp->d_xrstd.as<float>() : nullptr;
     f.X = X;
@@ -1315,8 +1341,10 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             samples = staging[buf]->p;
         }
         SVF_CUDA(mark(ev(c, 2), ctx->stream));
+        // the average chromaticity only colours the diffuse / specular maps and starts the RGB fit
+        const bool chroma = rgb || maps->diffuse || maps->specular;
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
-                                       ctx->avg.as<float>(), default_init ? ctx->lum_hi.p : nullptr,
+                                       chroma ? ctx->avg.as<float>() : nullptr, default_init ? ctx->lum_hi.p : nullptr,
                                        default_init ? ctx->lum_lo.p : nullptr, ctx->stream,
                                        rgb ? ctx->rgb16.p : nullptr, stride3,
                                        lum_features(mlp, ctx->mlp_x.as<float>(), true)));
@@ -1796,8 +1824,9 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
             }
             const uint32_t L = x.lay->L, N = L * L;
             float* lum = ctx->lum.as<float>() + p.off;
+            const bool chroma = rgb || maps[p.b].diffuse || maps[p.b].specular;
             SVF_CUDA(svf::launch_luminance(samples, v.sample_type, p.count, N, lum, x.stride,
-                                           ctx->avg.as<float>() + 3 * p.k0,
+                                           chroma ? ctx->avg.as<float>() + 3 * p.k0 : nullptr,
                                            x.default_init ? ctx->lum_hi.as<uint16_t>() + p.off : nullptr,
                                            x.default_init ? ctx->lum_lo.as<uint16_t>() + p.off : nullptr,
                                            ctx->stream, rgb ? ctx->rgb16.as<uint16_t>() + p.off3 : nullptr,
@@ -2155,10 +2184,9 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_ml
     const size_t texel_bytes = sizeof(float) * 3 * (size_t)N;
     const uint32_t gen = (uint32_t)std::max<size_t>(256, std::min<size_t>(65536, (size_t(2) << 30) / texel_bytes));
     const uint64_t stride = round_up(N, 8);
-    DevBuf samples, params, X, Y, lum, avg;
+    DevBuf samples, params, X, Y, lum;
     SVF_TRY(samples.ensure(texel_bytes * std::min(gen, T)));
     SVF_TRY(lum.ensure(sizeof(float) * stride * std::min(gen, T)));
-    SVF_TRY(avg.ensure(sizeof(float) * 3 * std::min(gen, T)));
     SVF_TRY(params.ensure(sizeof(float) * 7 * std::min(gen, T)));
     SVF_TRY(X.ensure(sizeof(float) * kMlpInputs * (size_t)T));
     SVF_TRY(Y.ensure(sizeof(float) * kMlpOutputs * (size_t)T));
@@ -2179,7 +2207,7 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_ml
         if(st != SVF_OK && st != SVF_EPARTIAL)
             return st;
         float* Xc = X.as<float>() + (size_t)kMlpInputs * c0;
-        SVF_CUDA(launch_luminance(samples.p, SVF_SAMPLES_F32, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr,
+        SVF_CUDA(launch_luminance(samples.p, SVF_SAMPLES_F32, n, N, lum.as<float>(), stride, nullptr, nullptr,
                                   nullptr, ctx->stream, nullptr, 0, lum_features(mlp.get(), Xc, false)));
         SVF_CUDA(rgb_features(mlp.get(), samples.p, SVF_SAMPLES_F32, N, n, Xc, false, ctx->stream));
         SVF_CUDA(mlp_targets(params.as<float>(), n, Y.as<float>() + (size_t)kMlpOutputs * c0, ctx->stream));
@@ -2300,12 +2328,11 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
     const uint32_t chunk = 65536;
     const uint32_t c = std::min(chunk, texels);
     const uint64_t stride = round_up(N, 8);
-    DevBuf staged, x, h1, h2, y, p, lum, avg;
+    DevBuf staged, x, h1, h2, y, p, lum;
     SVF_TRY(zero_error_flags(ctx));
     if(!on_device)
         SVF_TRY(staged.ensure(texel_bytes * c));
     SVF_TRY(lum.ensure(sizeof(float) * stride * c));
-    SVF_TRY(avg.ensure(sizeof(float) * 3 * c));
     SVF_TRY(x.ensure(sizeof(float) * kMlpInputs * c));
     SVF_TRY(h1.ensure(sizeof(float) * kMlpHidden * c));
     SVF_TRY(h2.ensure(sizeof(float) * kMlpHidden * c));
@@ -2320,7 +2347,7 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
             SVF_CUDA(cudaMemcpyAsync(staged.p, s, texel_bytes * n, cudaMemcpyHostToDevice, ctx->stream));
             s = staged.p;
         }
-        SVF_CUDA(launch_luminance(s, sample_type, n, N, lum.as<float>(), stride, avg.as<float>(), nullptr, nullptr,
+        SVF_CUDA(launch_luminance(s, sample_type, n, N, lum.as<float>(), stride, nullptr, nullptr, nullptr,
                                   ctx->stream, nullptr, 0, lum_features(mlp, x.as<float>(), true)));
         SVF_CUDA(rgb_features(mlp, s, sample_type, N, n, x.as<float>(), true, ctx->stream));
         SVF_TRY(mlp_infer(ctx, mlp, x.as<float>(), n, h1.as<float>(), h2.as<float>(), y.as<float>()));

@@ -84,18 +84,24 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
 // rgb16 (optional): the samples again as FP16 RGB slabs [texels][rgb_stride]
 // for the RGB fit (rgb_stride >= 3 N, a multiple of 8).
 // The learned guess's half-vector-bin features, computed by the luminance pass
-// from the slab it holds in shared memory (X null: none).  The pairs of bin b
-// are order[start[b] .. start[b + 1]) and their mean is the sum times bin_w[b];
-// then the luminance of the 32 single pairs; log, normalised with mean/rstd
-// (mean null: raw).  X: [texels][kMlpInputs].
+// from the slab it holds in shared memory in bin order (X null: none): pair k
+// at pos[k], so that bin b holds positions start[b] .. start[b + 1]; a bin's
+// feature is the sum of its positions, in order, times bin_w[b]; then the
+// luminance at the 32 single pairs' positions pair_pos; log, normalised with
+// mean/rstd (mean null: raw).  X: [texels][kMlpInputs].
 struct LumFeatures
 {
-    const uint32_t *order = nullptr, *start = nullptr;
+    const uint16_t* pos = nullptr;
+    const uint32_t* start = nullptr;
     const float* bin_w = nullptr;
-    const uint32_t* pairs = nullptr;
+    const uint16_t* pair_pos = nullptr;
     const float *mean = nullptr, *rstd = nullptr;
     float* X = nullptr;
 };
+// The luminance slabs [texels][lum_stride] of RGB samples [texels][N][3]; every
+// other output is optional (null: not computed): the average chromaticity
+// [texels][3], the BF16 hi/lo split of the slabs, the FP16 RGB slabs and the
+// learned guess's features.
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
                              float* lum, uint64_t lum_stride, float* avg_chroma, void* lum_hi, void* lum_lo,
                              cudaStream_t stream, void* rgb16 = nullptr, uint64_t rgb_stride = 0,

@@ -8,6 +8,9 @@
 
 #include <algorithm>
 #include <mutex>
+#include <array>
+#include <type_traits>
+#include <utility>
 
 #include "svf_internal.h"
 #include "svf_model.cuh"
@@ -30,20 +33,21 @@ template <>
 __device__ __forceinline__ float to_f<__half>(__half x) { return __half2float(x); }
 
 constexpr uint32_t kLumThreads = 256;
-constexpr int kLumUnroll = 4;   // pairs whose loads are in flight together per thread
+constexpr uint32_t kLumChunk = 1024;   // pairs per shared-memory chunk (a multiple of kLumThreads)
 
-// The learned guess's features of one texel from its luminance slab y (shared
-// memory, complete), by a CTA of kLumThreads: bins summed warp by warp over
-// their pairs in `order` in a fixed order (deterministic), the single pairs,
-// log, normalised.  v: shared scratch of kMlpInputs floats.
-__device__ void texel_features(const float* y, const LumFeatures& f, uint64_t t, float* v)
+// The learned guess's features of one texel from its luminance slab y in bin
+// order (shared memory, complete), by a CTA of kLumThreads: each bin's run
+// summed by one warp, lane-strided then a fixed butterfly (deterministic), the
+// single pairs, log, normalised.  st: the bin starts (shared); v: shared
+// scratch of kMlpInputs floats.
+__device__ void texel_features(const float* y, const uint32_t* st, const LumFeatures& f, uint64_t t, float* v)
 {
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for(int b = warp; b < kMlpBins; b += kLumThreads / 32)
     {
         float s = 0.0f;
-        for(uint32_t k = f.start[b] + lane; k < f.start[b + 1]; k += 32)
-            s += y[f.order[k]];
+        for(uint32_t k = st[b] + lane; k < st[b + 1]; k += 32)
+            s += y[k];
 #pragma unroll
         for(int o = 16; o > 0; o >>= 1)
             s += __shfl_xor_sync(0xffffffffu, s, o);
@@ -51,7 +55,7 @@ __device__ void texel_features(const float* y, const LumFeatures& f, uint64_t t,
             v[b] = s * f.bin_w[b];
     }
     if(threadIdx.x < kMlpPairs)
-        v[kMlpBins + threadIdx.x] = y[f.pairs[threadIdx.x]];
+        v[kMlpBins + threadIdx.x] = y[f.pair_pos[threadIdx.x]];
     __syncthreads();
     if(threadIdx.x < kMlpInputs)
     {
@@ -63,14 +67,62 @@ __device__ void texel_features(const float* y, const LumFeatures& f, uint64_t t,
     }
 }
 
+// Shared-memory staging of the luminance pass: chunks of kLumChunk pairs
+// (a multiple of kLumThreads, so each thread keeps its pairs), double-buffered.
+template <typename T>
+struct LumStage
+{
+    static constexpr uint32_t kChunkBytes = kLumChunk * 3 * sizeof(T) + 16;   // + the alignment offset
+    static constexpr uint32_t kPosBytes = kLumChunk * sizeof(uint16_t);
+    static size_t smem(uint32_t N, bool features)
+    {
+        return 2 * (size_t)kChunkBytes + (features ? 2 * (size_t)kPosBytes + sizeof(float) * N : 0);
+    }
+};
+
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(smem_dst)),
+                 "l"(gmem_src)
+                 : "memory");
+}
+
+// Copies the bytes [g0, g1) of the samples (T-aligned) into buf + (g0 & 15), so
+// that 16-byte words of global memory land on 16-byte words of shared memory:
+// the aligned interior by cp.async, the ragged head and tail (under 16 bytes
+// each) element by element.
+template <typename T>
+__device__ __forceinline__ void stage_bytes(const char* g0, const char* g1, unsigned char* buf)
+{
+    const uintptr_t a0 = reinterpret_cast<uintptr_t>(g0), a1 = reinterpret_cast<uintptr_t>(g1);
+    unsigned char* dst = buf + (a0 & 15u);
+    uintptr_t ia = (a0 + 15u) & ~uintptr_t(15), ib = a1 & ~uintptr_t(15);
+    if(ia > ib)
+        ia = ib = a1;   // inside one 16-byte word: all of it is head
+    const uint32_t words = (uint32_t)((ib - ia) / 16);
+    for(uint32_t w = threadIdx.x; w < words; w += kLumThreads)
+        cp_async16(dst + (ia - a0) + 16 * w, reinterpret_cast<const void*>(ia + 16 * w));
+    const uint32_t head = (uint32_t)((ia - a0) / sizeof(T)), tail = (uint32_t)((a1 - ib) / sizeof(T));
+    const uint32_t tail0 = (uint32_t)((ib - a0) / sizeof(T));
+    if(threadIdx.x < head)
+        reinterpret_cast<T*>(dst)[threadIdx.x] = reinterpret_cast<const T*>(g0)[threadIdx.x];
+    else if(threadIdx.x >= 32 && threadIdx.x - 32 < tail)
+        reinterpret_cast<T*>(dst)[tail0 + threadIdx.x - 32] = reinterpret_cast<const T*>(ib)[threadIdx.x - 32];
+}
+
 // One CTA of kLumThreads per texel.  lum = 0.2126 R + 0.7152 G + 0.0722 B
 // (spectrum.hh:328-331, evaluated without fused multiply-adds, as the
 // reference's x86-64 build does); chromaticity rgb/lum, or (1,1,1) when lum <=
 // 1e-6, averaged over the pairs.  Thread j takes pairs j, j + 256, ... in that
-// order, the loads of kLumUnroll of them issued together (the pass is bound by
-// the bytes in flight).  With features, the slab is also kept in dynamic shared
-// memory and the features are computed from it.
-template <typename T>
+// order.  The texel's samples stream through shared memory in chunks by
+// cp.async (16-byte copies that hold no registers, the next chunk in flight
+// while this one is converted), since the pass is bound by the bytes in flight.
+// With features, the slab is also kept in shared memory in bin order and the
+// features are computed from it.  The optional outputs are template flags
+// (kHiLo: the BF16 split for the NDF GEMM; kRgb: the FP16 RGB slab; kFeat: the
+// features; kChroma: the average chromaticity, which only the colour maps and
+// the RGB fit read), so that the per-pair loop carries no branches for them.
+template <typename T, bool kHiLo, bool kRgb, bool kFeat, bool kChroma>
 __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restrict__ samples, uint32_t N,
                                                                 float* __restrict__ lum, uint64_t lum_stride,
                                                                 float* __restrict__ avg,
@@ -79,38 +131,54 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
                                                                 __half* __restrict__ rgb16, uint64_t rgb_stride,
                                                                 LumFeatures feat)
 {
-    extern __shared__ __align__(16) float y[];   // [N] with features
+    using S = LumStage<T>;
+    // [2][kChunkBytes] samples; with features [2][kLumChunk] positions, then y [N]
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint16_t* pos_buf = reinterpret_cast<uint16_t*>(smem + 2 * S::kChunkBytes);
+    float* y = reinterpret_cast<float*>(smem + 2 * S::kChunkBytes + 2 * S::kPosBytes);
+    __shared__ uint32_t st[kMlpBins + 1];
+    if(kFeat && threadIdx.x <= kMlpBins)
+        st[threadIdx.x] = feat.start[threadIdx.x];
     const uint64_t t = blockIdx.x;
-    const T* src = samples + t * (uint64_t)N * 3;
+    const char* src = reinterpret_cast<const char*>(samples + t * (uint64_t)N * 3);
     float* dst = lum + t * lum_stride;
+    const uint32_t chunks = (N + kLumChunk - 1) / kLumChunk;
+    const auto stage = [&](uint32_t c) {
+        const uint32_t p0 = c * kLumChunk, pn = min(kLumChunk, N - p0);
+        stage_bytes<T>(src + (size_t)p0 * 3 * sizeof(T), src + (size_t)(p0 + pn) * 3 * sizeof(T),
+                       smem + (c & 1) * S::kChunkBytes);
+        if(kFeat)   // positions: 16-byte words (the table is padded to a multiple of 8 entries)
+            for(uint32_t w = threadIdx.x; w < (pn + 7) / 8; w += kLumThreads)
+                cp_async16(pos_buf + (c & 1) * kLumChunk + 8 * w, feat.pos + p0 + 8 * w);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    };
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
-    for(uint32_t i0 = threadIdx.x; i0 < N; i0 += kLumUnroll * kLumThreads)
+    if(chunks)
+        stage(0);
+    for(uint32_t c = 0; c < chunks; ++c)
     {
-        float rr[kLumUnroll], gg[kLumUnroll], bb[kLumUnroll];
-#pragma unroll
-        for(int u = 0; u < kLumUnroll; ++u)
+        if(c + 1 < chunks)
         {
-            const uint32_t i = i0 + u * kLumThreads;
-            rr[u] = gg[u] = bb[u] = 0.0f;
-            if(i < N)
-            {
-                rr[u] = to_f(src[3 * i]);
-                gg[u] = to_f(src[3 * i + 1]);
-                bb[u] = to_f(src[3 * i + 2]);
-            }
+            stage(c + 1);
+            asm volatile("cp.async.wait_group 1;" ::: "memory");
         }
-#pragma unroll
-        for(int u = 0; u < kLumUnroll; ++u)
+        else
+            asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();
+        const uint32_t p0 = c * kLumChunk, pn = min(kLumChunk, N - p0);
+        const uintptr_t g0 = reinterpret_cast<uintptr_t>(src + (size_t)p0 * 3 * sizeof(T));
+        const T* cs = reinterpret_cast<const T*>(smem + (c & 1) * S::kChunkBytes + (g0 & 15u));
+        const uint16_t* cp = pos_buf + (c & 1) * kLumChunk;
+#pragma unroll 4
+        for(uint32_t k = threadIdx.x; k < pn; k += kLumThreads)
         {
-            const uint32_t i = i0 + u * kLumThreads;
-            if(i >= N)
-                break;
-            const float r = rr[u], g = gg[u], b = bb[u];
+            const uint32_t i = p0 + k;
+            const float r = to_f(cs[3 * k]), g = to_f(cs[3 * k + 1]), b = to_f(cs[3 * k + 2]);
             float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
             dst[i] = l;
-            if(feat.X)
-                y[i] = l;
-            if(rgb16)
+            if(kFeat)
+                y[cp[k]] = l;
+            if(kRgb)
             {
                 // the RGB fit's slab: the samples in FP16, [L*L][3], 16-byte rows
                 __half* o = rgb16 + t * rgb_stride + 3 * (uint64_t)i;
@@ -118,13 +186,15 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
                 o[1] = __float2half_rn(g);
                 o[2] = __float2half_rn(b);
             }
-            if(lum_hi)
+            if(kHiLo)
             {
                 // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
                 const __nv_bfloat16 h = __float2bfloat16_rn(l);
                 lum_hi[t * lum_stride + i] = h;
                 lum_lo[t * lum_stride + i] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
             }
+            if constexpr(!kChroma)
+                continue;
             if(l > 1e-6f)
             {
                 float rl = 1.0f / l;
@@ -139,36 +209,40 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
                 az += 1.0f;
             }
         }
+        __syncthreads();   // the buffer is refilled two chunks on (and y is complete after the last)
     }
     for(uint32_t i = N + threadIdx.x; i < lum_stride; i += blockDim.x)
         dst[i] = 0.0f;
-    __shared__ float red[3][8];
+    if constexpr(kChroma)
+    {
+        __shared__ float red[3][8];
 #pragma unroll
-    for(int o = 16; o > 0; o >>= 1)
-    {
-        ax += __shfl_xor_sync(0xffffffffu, ax, o);
-        ay += __shfl_xor_sync(0xffffffffu, ay, o);
-        az += __shfl_xor_sync(0xffffffffu, az, o);
-    }
-    const uint32_t warp = threadIdx.x >> 5;
-    if((threadIdx.x & 31u) == 0)
-    {
-        red[0][warp] = ax;
-        red[1][warp] = ay;
-        red[2][warp] = az;
-    }
-    __syncthreads();
-    if(threadIdx.x < 3)
-    {
-        float s = 0.0f;
-        for(uint32_t w = 0; w < blockDim.x / 32; ++w)
-            s += red[threadIdx.x][w];
-        // Vector3 / float multiplies by the reciprocal (vector3.hh:185-190)
-        avg[3 * t + threadIdx.x] = s * (1.0f / (float)N);
+        for(int o = 16; o > 0; o >>= 1)
+        {
+            ax += __shfl_xor_sync(0xffffffffu, ax, o);
+            ay += __shfl_xor_sync(0xffffffffu, ay, o);
+            az += __shfl_xor_sync(0xffffffffu, az, o);
+        }
+        const uint32_t warp = threadIdx.x >> 5;
+        if((threadIdx.x & 31u) == 0)
+        {
+            red[0][warp] = ax;
+            red[1][warp] = ay;
+            red[2][warp] = az;
+        }
+        __syncthreads();
+        if(threadIdx.x < 3)
+        {
+            float s = 0.0f;
+            for(uint32_t w = 0; w < blockDim.x / 32; ++w)
+                s += red[threadIdx.x][w];
+            // Vector3 / float multiplies by the reciprocal (vector3.hh:185-190)
+            avg[3 * t + threadIdx.x] = s * (1.0f / (float)N);
+        }
     }
     __shared__ float fv[kMlpInputs];
-    if(feat.X)   // y is complete: the __syncthreads above follows every write
-        texel_features(y, feat, t, fv);
+    if(kFeat)
+        texel_features(y, st, feat, t, fv);
 }
 
 __global__ void repack_kernel(const float* __restrict__ src, uint64_t src_stride, uint32_t N, float* __restrict__ dst,
@@ -519,6 +593,27 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
     return cudaStreamSynchronize(stream);
 }
 
+namespace
+{
+
+template <typename T, int... F>
+auto luminance_kernel_table(std::integer_sequence<int, F...>)
+{
+    using K = decltype(&luminance_kernel<T, false, false, false, false>);
+    return std::array<K, sizeof...(F)>{ &luminance_kernel<T, (F & 1) != 0, (F & 2) != 0, (F & 4) != 0,
+                                                          (F & 8) != 0>... };
+}
+
+// The instance for output flags 1 kHiLo | 2 kRgb | 4 kFeat | 8 kChroma
+template <typename T>
+auto luminance_kernel_of(int flags, const T*)
+{
+    static const auto table = luminance_kernel_table<T>(std::make_integer_sequence<int, 16>{});
+    return table[flags];
+}
+
+} // namespace
+
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N, float* lum,
                              uint64_t lum_stride, float* avg, void* lum_hi, void* lum_lo, cudaStream_t stream,
                              void* rgb16, uint64_t rgb_stride, const LumFeatures& features)
@@ -527,13 +622,14 @@ cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t
         return cudaSuccess;
     if((lum_hi == nullptr) != (lum_lo == nullptr) || texels > 0x7fffffffull)
         return cudaErrorInvalidValue;
-    if(features.X && !(features.order && features.start && features.bin_w && features.pairs &&
-                       (features.mean == nullptr) == (features.rstd == nullptr)))
+    if(features.X && !(features.pos && features.start && features.bin_w && features.pair_pos &&
+                       (features.mean == nullptr) == (features.rstd == nullptr) && N <= 65536u))
         return cudaErrorInvalidValue;
     __nv_bfloat16* hi = static_cast<__nv_bfloat16*>(lum_hi);
     __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(lum_lo);
-    const size_t smem = features.X ? sizeof(float) * N : 0;
     const auto run = [&](auto kernel, const auto* src) -> cudaError_t {
+        using T = std::remove_cv_t<std::remove_pointer_t<decltype(src)>>;
+        const size_t smem = LumStage<T>::smem(N, features.X != nullptr);
         if(smem > 48 * 1024)
         {
             const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -544,9 +640,10 @@ cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t
                                                                 static_cast<__half*>(rgb16), rgb_stride, features);
         return cudaGetLastError();
     };
+    const int flags = (hi ? 1 : 0) | (rgb16 ? 2 : 0) | (features.X ? 4 : 0) | (avg ? 8 : 0);
     if(sample_type == SVF_SAMPLES_F16)
-        return run(luminance_kernel<__half>, static_cast<const __half*>(samples));
-    return run(luminance_kernel<float>, static_cast<const float*>(samples));
+        return run(luminance_kernel_of(flags, static_cast<const __half*>(samples)), static_cast<const __half*>(samples));
+    return run(luminance_kernel_of(flags, static_cast<const float*>(samples)), static_cast<const float*>(samples));
 }
 
 __global__ void rgb_init_kernel(const float* __restrict__ init7, const float* __restrict__ avg, uint64_t texels,
