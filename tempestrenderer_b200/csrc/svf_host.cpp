@@ -237,8 +237,8 @@ struct svf_mlp
     std::vector<uint32_t> order, start;
     std::vector<float> bin_w;
     // the luminance pass keeps the slab in bin order: pair k at pos[k] (the pairs
-    // of bin b at start[b] .. start[b + 1], those with no half vector after them;
-    // zero-padded to a multiple of 8 entries); pair_pos: the single pairs' positions
+    // of bin b at start[b] .. start[b + 1], those with no half vector after
+    // them); pair_pos: the single pairs' positions
     std::vector<uint16_t> pos;
     uint16_t pair_pos[svf::kMlpPairs] = {};
     float xmean[svf::kMlpInputs] = {}, xrstd[svf::kMlpInputs] = {};
@@ -307,7 +307,7 @@ void mlp_bins(svf_mlp* mlp)
     mlp->pos.clear();
     if(N <= 65536u)   // 16-bit positions (the shared-memory slab holds far fewer pairs anyway)
     {
-        mlp->pos.assign(round_up(N, 8), 0);   // whole 16-byte words for the luminance pass's copies
+        mlp->pos.assign(N, 0);
         uint32_t next = mlp->start[kMlpBins];
         for(uint32_t k = 0; k < mlp->start[kMlpBins]; ++k)
             mlp->pos[mlp->order[k]] = (uint16_t)k;

@@ -34,6 +34,7 @@ __device__ __forceinline__ float to_f<__half>(__half x) { return __half2float(x)
 
 constexpr uint32_t kLumThreads = 256;
 constexpr uint32_t kLumChunk = 1024;   // pairs per shared-memory chunk (a multiple of kLumThreads)
+constexpr int kLumUnroll = 4;          // pairs a thread has in flight on the direct path
 
 // The learned guess's features of one texel from its luminance slab y in bin
 // order (shared memory, complete), by a CTA of kLumThreads: each bin's run
@@ -67,16 +68,20 @@ __device__ void texel_features(const float* y, const uint32_t* st, const LumFeat
     }
 }
 
-// Shared-memory staging of the luminance pass: chunks of kLumChunk pairs
-// (a multiple of kLumThreads, so each thread keeps its pairs), double-buffered.
-template <typename T>
-struct LumStage
+// The luminance pass reads FP16 samples through shared memory (kStaged: chunks
+// of kLumChunk pairs, a multiple of kLumThreads so that each thread keeps its
+// pairs, double-buffered) and FP32 samples straight into registers, kLumUnroll
+// pairs a thread in flight: a warp's direct 2-byte loads carry too few bytes
+// to cover the latency, its 4-byte loads enough (measured both ways on both
+// types).  With features the slab is kept in shared memory (direct path).
+template <typename T, bool kFeat>
+struct LumPass
 {
+    static constexpr bool kStaged = sizeof(T) == 2 && !kFeat;
     static constexpr uint32_t kChunkBytes = kLumChunk * 3 * sizeof(T) + 16;   // + the alignment offset
-    static constexpr uint32_t kPosBytes = kLumChunk * sizeof(uint16_t);
-    static size_t smem(uint32_t N, bool features)
+    static size_t smem(uint32_t N)
     {
-        return 2 * (size_t)kChunkBytes + (features ? 2 * (size_t)kPosBytes + sizeof(float) * N : 0);
+        return kStaged ? 2 * (size_t)kChunkBytes : (kFeat ? sizeof(float) * N : 0);
     }
 };
 
@@ -110,18 +115,61 @@ __device__ __forceinline__ void stage_bytes(const char* g0, const char* g1, unsi
         reinterpret_cast<T*>(dst)[tail0 + threadIdx.x - 32] = reinterpret_cast<const T*>(ib)[threadIdx.x - 32];
 }
 
-// One CTA of kLumThreads per texel.  lum = 0.2126 R + 0.7152 G + 0.0722 B
+// One pair of the luminance pass: lum = 0.2126 R + 0.7152 G + 0.0722 B
 // (spectrum.hh:328-331, evaluated without fused multiply-adds, as the
-// reference's x86-64 build does); chromaticity rgb/lum, or (1,1,1) when lum <=
-// 1e-6, averaged over the pairs.  Thread j takes pairs j, j + 256, ... in that
-// order.  The texel's samples stream through shared memory in chunks by
-// cp.async (16-byte copies that hold no registers, the next chunk in flight
-// while this one is converted), since the pass is bound by the bytes in flight.
-// With features, the slab is also kept in shared memory in bin order and the
-// features are computed from it.  The optional outputs are template flags
-// (kHiLo: the BF16 split for the NDF GEMM; kRgb: the FP16 RGB slab; kFeat: the
-// features; kChroma: the average chromaticity, which only the colour maps and
-// the RGB fit read), so that the per-pair loop carries no branches for them.
+// reference's x86-64 build does) and the optional outputs; chromaticity rgb/lum,
+// or (1,1,1) when lum <= 1e-6, added to the thread's sums.
+template <bool kHiLo, bool kRgb, bool kFeat, bool kChroma>
+__device__ __forceinline__ void lum_pair(uint32_t i, float r, float g, float b, uint32_t ypos, uint64_t t,
+                                         float* dst, float* y, __half* rgb16, uint64_t rgb_stride,
+                                         __nv_bfloat16* lum_hi, __nv_bfloat16* lum_lo, uint64_t lum_stride,
+                                         float& ax, float& ay, float& az)
+{
+    const float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
+    dst[i] = l;
+    if constexpr(kFeat)
+        y[ypos] = l;
+    if constexpr(kRgb)
+    {
+        // the RGB fit's slab: the samples in FP16, [L*L][3], 16-byte rows
+        __half* o = rgb16 + t * rgb_stride + 3 * (uint64_t)i;
+        o[0] = __float2half_rn(r);
+        o[1] = __float2half_rn(g);
+        o[2] = __float2half_rn(b);
+    }
+    if constexpr(kHiLo)
+    {
+        // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
+        const __nv_bfloat16 h = __float2bfloat16_rn(l);
+        lum_hi[t * lum_stride + i] = h;
+        lum_lo[t * lum_stride + i] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
+    }
+    if constexpr(kChroma)
+    {
+        if(l > 1e-6f)
+        {
+            const float rl = 1.0f / l;
+            ax += r * rl;
+            ay += g * rl;
+            az += b * rl;
+        }
+        else
+        {
+            ax += 1.0f;
+            ay += 1.0f;
+            az += 1.0f;
+        }
+    }
+}
+
+// One CTA of kLumThreads per texel: the luminance slab, and the average
+// chromaticity over the pairs.  Thread j takes pairs j, j + 256, ... in that
+// order whichever way the samples arrive (LumPass).  With features, the slab
+// is also kept in shared memory in bin order and the features are computed
+// from it.  The optional outputs are template flags (kHiLo: the BF16 split for
+// the NDF GEMM; kRgb: the FP16 RGB slab; kFeat: the features; kChroma: the
+// average chromaticity, which only the colour maps and the RGB fit read), so
+// that the per-pair loop carries no branches for them.
 template <typename T, bool kHiLo, bool kRgb, bool kFeat, bool kChroma>
 __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restrict__ samples, uint32_t N,
                                                                 float* __restrict__ lum, uint64_t lum_stride,
@@ -131,85 +179,83 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
                                                                 __half* __restrict__ rgb16, uint64_t rgb_stride,
                                                                 LumFeatures feat)
 {
-    using S = LumStage<T>;
-    // [2][kChunkBytes] samples; with features [2][kLumChunk] positions, then y [N]
+    using S = LumPass<T, kFeat>;
+    // staged: [2][kChunkBytes] samples; with features: y [N] in bin order
     extern __shared__ __align__(16) unsigned char smem[];
-    uint16_t* pos_buf = reinterpret_cast<uint16_t*>(smem + 2 * S::kChunkBytes);
-    float* y = reinterpret_cast<float*>(smem + 2 * S::kChunkBytes + 2 * S::kPosBytes);
+    float* y = reinterpret_cast<float*>(smem);
     __shared__ uint32_t st[kMlpBins + 1];
     if(kFeat && threadIdx.x <= kMlpBins)
         st[threadIdx.x] = feat.start[threadIdx.x];
     const uint64_t t = blockIdx.x;
-    const char* src = reinterpret_cast<const char*>(samples + t * (uint64_t)N * 3);
+    const T* src = samples + t * (uint64_t)N * 3;
     float* dst = lum + t * lum_stride;
-    const uint32_t chunks = (N + kLumChunk - 1) / kLumChunk;
-    const auto stage = [&](uint32_t c) {
-        const uint32_t p0 = c * kLumChunk, pn = min(kLumChunk, N - p0);
-        stage_bytes<T>(src + (size_t)p0 * 3 * sizeof(T), src + (size_t)(p0 + pn) * 3 * sizeof(T),
-                       smem + (c & 1) * S::kChunkBytes);
-        if(kFeat)   // positions: 16-byte words (the table is padded to a multiple of 8 entries)
-            for(uint32_t w = threadIdx.x; w < (pn + 7) / 8; w += kLumThreads)
-                cp_async16(pos_buf + (c & 1) * kLumChunk + 8 * w, feat.pos + p0 + 8 * w);
-        asm volatile("cp.async.commit_group;" ::: "memory");
-    };
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
-    if(chunks)
-        stage(0);
-    for(uint32_t c = 0; c < chunks; ++c)
+    if constexpr(S::kStaged)
     {
-        if(c + 1 < chunks)
+        const char* bytes = reinterpret_cast<const char*>(src);
+        const uint32_t chunks = (N + kLumChunk - 1) / kLumChunk;
+        const auto stage = [&](uint32_t c) {
+            const uint32_t p0 = c * kLumChunk, pn = min(kLumChunk, N - p0);
+            stage_bytes<T>(bytes + (size_t)p0 * 3 * sizeof(T), bytes + (size_t)(p0 + pn) * 3 * sizeof(T),
+                           smem + (c & 1) * S::kChunkBytes);
+            asm volatile("cp.async.commit_group;" ::: "memory");
+        };
+        if(chunks)
+            stage(0);
+        for(uint32_t c = 0; c < chunks; ++c)
         {
-            stage(c + 1);
-            asm volatile("cp.async.wait_group 1;" ::: "memory");
-        }
-        else
-            asm volatile("cp.async.wait_group 0;" ::: "memory");
-        __syncthreads();
-        const uint32_t p0 = c * kLumChunk, pn = min(kLumChunk, N - p0);
-        const uintptr_t g0 = reinterpret_cast<uintptr_t>(src + (size_t)p0 * 3 * sizeof(T));
-        const T* cs = reinterpret_cast<const T*>(smem + (c & 1) * S::kChunkBytes + (g0 & 15u));
-        const uint16_t* cp = pos_buf + (c & 1) * kLumChunk;
-#pragma unroll 4
-        for(uint32_t k = threadIdx.x; k < pn; k += kLumThreads)
-        {
-            const uint32_t i = p0 + k;
-            const float r = to_f(cs[3 * k]), g = to_f(cs[3 * k + 1]), b = to_f(cs[3 * k + 2]);
-            float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
-            dst[i] = l;
-            if(kFeat)
-                y[cp[k]] = l;
-            if(kRgb)
+            if(c + 1 < chunks)
             {
-                // the RGB fit's slab: the samples in FP16, [L*L][3], 16-byte rows
-                __half* o = rgb16 + t * rgb_stride + 3 * (uint64_t)i;
-                o[0] = __float2half_rn(r);
-                o[1] = __float2half_rn(g);
-                o[2] = __float2half_rn(b);
-            }
-            if(kHiLo)
-            {
-                // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
-                const __nv_bfloat16 h = __float2bfloat16_rn(l);
-                lum_hi[t * lum_stride + i] = h;
-                lum_lo[t * lum_stride + i] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
-            }
-            if constexpr(!kChroma)
-                continue;
-            if(l > 1e-6f)
-            {
-                float rl = 1.0f / l;
-                ax += r * rl;
-                ay += g * rl;
-                az += b * rl;
+                stage(c + 1);
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
             }
             else
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
+            __syncthreads();
+            const uint32_t p0 = c * kLumChunk, pn = min(kLumChunk, N - p0);
+            const uintptr_t g0 = reinterpret_cast<uintptr_t>(bytes + (size_t)p0 * 3 * sizeof(T));
+            const T* cs = reinterpret_cast<const T*>(smem + (c & 1) * S::kChunkBytes + (g0 & 15u));
+#pragma unroll 4
+            for(uint32_t k = threadIdx.x; k < pn; k += kLumThreads)
+                lum_pair<kHiLo, kRgb, kFeat, kChroma>(p0 + k, to_f(cs[3 * k]), to_f(cs[3 * k + 1]),
+                                                      to_f(cs[3 * k + 2]), 0, t, dst, y, rgb16, rgb_stride, lum_hi,
+                                                      lum_lo, lum_stride, ax, ay, az);
+            __syncthreads();   // the buffer is refilled two chunks on
+        }
+    }
+    else
+    {
+        for(uint32_t i0 = threadIdx.x; i0 < N; i0 += kLumUnroll * kLumThreads)
+        {
+            float rr[kLumUnroll], gg[kLumUnroll], bb[kLumUnroll];
+            uint32_t pp[kLumUnroll];
+#pragma unroll
+            for(int u = 0; u < kLumUnroll; ++u)
             {
-                ax += 1.0f;
-                ay += 1.0f;
-                az += 1.0f;
+                const uint32_t i = i0 + u * kLumThreads;
+                rr[u] = gg[u] = bb[u] = 0.0f;
+                pp[u] = 0;
+                if(i < N)
+                {
+                    rr[u] = to_f(src[3 * i]);
+                    gg[u] = to_f(src[3 * i + 1]);
+                    bb[u] = to_f(src[3 * i + 2]);
+                    if(kFeat)
+                        pp[u] = feat.pos[i];
+                }
+            }
+#pragma unroll
+            for(int u = 0; u < kLumUnroll; ++u)
+            {
+                const uint32_t i = i0 + u * kLumThreads;
+                if(i >= N)
+                    break;
+                lum_pair<kHiLo, kRgb, kFeat, kChroma>(i, rr[u], gg[u], bb[u], pp[u], t, dst, y, rgb16, rgb_stride,
+                                                      lum_hi, lum_lo, lum_stride, ax, ay, az);
             }
         }
-        __syncthreads();   // the buffer is refilled two chunks on (and y is complete after the last)
+        if constexpr(kFeat)
+            __syncthreads();   // y is complete
     }
     for(uint32_t i = N + threadIdx.x; i < lum_stride; i += blockDim.x)
         dst[i] = 0.0f;
@@ -629,7 +675,7 @@ cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t
     __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(lum_lo);
     const auto run = [&](auto kernel, const auto* src) -> cudaError_t {
         using T = std::remove_cv_t<std::remove_pointer_t<decltype(src)>>;
-        const size_t smem = LumStage<T>::smem(N, features.X != nullptr);
+        const size_t smem = features.X ? LumPass<T, true>::smem(N) : LumPass<T, false>::smem(N);
         if(smem > 48 * 1024)
         {
             const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
