@@ -303,7 +303,8 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, tru
                                                              "within_1pct": float(np.mean(fratio <= 1.01)),
                                                              "p90": float(np.quantile(fratio, 0.9))}},
             "model": "MLP 96-256-256-8 (64 half-vector bins + 32 pairs of the luminance slab -> log S, ks, kd), "
-                     "BF16 inference; LM from its prediction with 1e-3 of the reference's initial damping"}
+                     "features from the luminance pass, hidden layers on the tcgen05 tensor cores (BF16x3, FP32 "
+                     "accuracy); LM from its prediction with 1e-3 of the reference's initial damping"}
 
 
 def fib151_item(svf, ctx, steps, dev, side=768):
