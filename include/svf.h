@@ -298,7 +298,9 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
  * that the plain LM, started from the reference's default guess, has fitted.
  * SVF_INIT_MLP then starts LM from its prediction: the fit skips the NDF
  * pipeline, and its result is judged against the plain LM's residual.
- * Inference uses BF16 weights with FP32 accumulation. */
+ * Inference runs the hidden layers on the tensor cores with weights and
+ * activations split into BF16 hi/lo pairs, accumulating in FP32 (the FP32
+ * network to about 1e-5). */
 #define SVF_MLP_FEATURES_PAIRS_RGB 0u   /* 32 fixed direction pairs x RGB, log-scaled */
 #define SVF_MLP_FEATURES_BINS      1u   /* 64 half-vector bins of the luminance slab + 32 pairs' luminance */
 

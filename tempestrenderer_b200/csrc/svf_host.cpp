@@ -223,7 +223,8 @@ struct svf_ctx
 };
 
 // A learned initial-guess model (svf_mlp_*): FP32 master weights (Adam state
-// alongside), BF16 copies for inference, the normalisation of inputs and
+// alongside), the hidden layers' weights split into BF16 hi/lo pairs for the
+// tensor-core inference, the normalisation of inputs and
 // targets, the 32 direction pairs and the layout it was trained for.
 struct svf_mlp
 {
