@@ -255,7 +255,8 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, tru
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    model, loss = svf.Mlp.train(ctx, layout.lights_parabolic)   # 2^20 texels, 24 epochs (defaults)
+    topts = svf.mlp_train_options()   # the defaults: 2^20 texels, 48 epochs
+    model, loss = svf.Mlp.train(ctx, layout.lights_parabolic, topts)
     torch.cuda.synchronize()
     train_s = time.perf_counter() - t0
     T = W * H
@@ -294,7 +295,8 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, tru
             "ground_truth_error": None if truth is None else param_error(maps["params"].cpu().numpy(), truth),
             "rmse_ratio_vs_default_init": {"median": float(np.median(ratio)), "within_1pct": float(np.mean(ratio <= 1.01)),
                                            "better_1pct": float(np.mean(ratio < 0.99)), "p90": float(np.quantile(ratio, 0.9))},
-            "training": {"seconds": train_s, "final_loss": loss, "texels": 1 << 20, "epochs": 24},
+            "training": {"seconds": train_s, "final_loss": loss, "texels": topts.texels, "epochs": topts.epochs,
+                         "lr": topts.lr},
             "config3_1024x1024_fp16": cfg3,
             "with_fallback": {"value": T / (fms / 1e3), "unit": "texels/s", "ms_per_step": fms,
                               "threshold_relative_rmse": th, "fallback_texels": fst[-1].fallback_texels,

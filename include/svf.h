@@ -308,9 +308,9 @@ typedef struct svf_mlp_train_options
 {
     uint32_t texels;          /* synthetic training texels (default 1 << 20) */
     uint32_t seed, mix;       /* svf_synth_btf seed and parameter mix of the training texels */
-    uint32_t epochs;          /* passes over the texels (default 24) */
+    uint32_t epochs;          /* passes over the texels (default 48) */
     uint32_t batch;           /* texels per Adam step (default 4096) */
-    float    lr;              /* Adam step size (default 1e-3, cosine-decayed to 5% of it) */
+    float    lr;              /* Adam step size (default 2e-3, cosine-decayed to 5% of it) */
     uint32_t max_iterations;  /* of the LM that makes the targets (default 1024) */
     uint32_t features;        /* SVF_MLP_FEATURES_* (default SVF_MLP_FEATURES_BINS) */
 } svf_mlp_train_options;

@@ -2133,9 +2133,9 @@ void svf_mlp_train_options_default(svf_mlp_train_options* o)
     o->texels = 1u << 20;
     o->seed = 12345;
     o->mix = 1;
-    o->epochs = 24;
+    o->epochs = 48;
     o->batch = 4096;
-    o->lr = 1e-3f;
+    o->lr = 2e-3f;
     o->max_iterations = 1024;
     o->features = SVF_MLP_FEATURES_BINS;
 }
