@@ -305,19 +305,16 @@ void mlp_bins(svf_mlp* mlp)
     mlp->bin_w.assign(kMlpBins, 0.0f);
     for(int b = 0; b < kMlpBins; ++b)
         mlp->bin_w[b] = count[b] ? 1.0f / (float)count[b] : 0.0f;
-    mlp->pos.clear();
-    if(N <= 65536u)   // 16-bit positions (the shared-memory slab holds far fewer pairs anyway)
-    {
-        mlp->pos.assign(N, 0);
-        uint32_t next = mlp->start[kMlpBins];
-        for(uint32_t k = 0; k < mlp->start[kMlpBins]; ++k)
-            mlp->pos[mlp->order[k]] = (uint16_t)k;
-        for(uint32_t k = 0; k < N; ++k)
-            if(bin[k] == (uint32_t)kMlpBins)
-                mlp->pos[k] = (uint16_t)next++;
-        for(int j = 0; j < kMlpPairs; ++j)
-            mlp->pair_pos[j] = mlp->pos[mlp->pairs[j]];
-    }
+    // 16-bit positions: a model's layout has at most 160 directions (25600 pairs)
+    mlp->pos.assign(N, 0);
+    uint32_t next = mlp->start[kMlpBins];
+    for(uint32_t k = 0; k < mlp->start[kMlpBins]; ++k)
+        mlp->pos[mlp->order[k]] = (uint16_t)k;
+    for(uint32_t k = 0; k < N; ++k)
+        if(bin[k] == (uint32_t)kMlpBins)
+            mlp->pos[k] = (uint16_t)next++;
+    for(int j = 0; j < kMlpPairs; ++j)
+        mlp->pair_pos[j] = mlp->pos[mlp->pairs[j]];
 }
 
 // Uploads the host-side tables of a model and zeroes its optimiser state.
@@ -414,11 +411,6 @@ svf::LumFeatures lum_features(const svf_mlp* mlp, float* X, bool normalise)
     svf::LumFeatures f;
     if(!mlp || mlp->features != SVF_MLP_FEATURES_BINS)
         return f;
-    if(mlp->pos.empty())
-    {
-        f.X = X;   // more direction pairs than 16-bit positions: launch_luminance rejects it
-        return f;
-    }
     f.pos = mlp->d_pos.as<uint16_t>();
     f.start = mlp->d_start.as<uint32_t>();
     f.bin_w = mlp->d_binw.as<float>();
