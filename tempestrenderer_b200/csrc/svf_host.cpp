@@ -1416,8 +1416,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                 float* g_rmse = g_out + 7 * (uint64_t)m;
                 float* g_maps = g_rmse + m;
                 svf_texel_stats* g_stats = reinterpret_cast<svf_texel_stats*>(g_maps + 12 * (uint64_t)m);
-                SVF_CUDA(svf::launch_gather_slabs(ctx->lum.as<float>(), stride, ctx->avg.as<float>(), idx, m,
-                                                  ctx->fb_lum.as<float>(), g_avg, ctx->stream));
+                SVF_CUDA(svf::launch_gather_slabs(ctx->lum.as<float>(), stride, chroma ? ctx->avg.as<float>() : nullptr,
+                                                  idx, m, ctx->fb_lum.as<float>(), g_avg, ctx->stream));
                 SVF_CUDA(svf::launch_split_bf16(ctx->fb_lum.as<float>(), stride * m, ctx->fb_hi.p, ctx->fb_lo.p,
                                                 ctx->stream));
                 cudaError_t e = svf::launch_ndf_tc(ctx->fb_hi.p, ctx->fb_lo.p, m, stride, init_lay->ndf_op_hi,
@@ -1428,8 +1428,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                     return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
                 SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->fb_ndf.as<float>(), fb_ld, m, g_init, nullptr,
                                                  nullptr, ctx->stream));
-                LmRun gr{ ctx->fb_lum.p, stride, g_init, g_out, g_rmse, g_stats, g_avg, g_maps, g_maps + 3 * m,
-                          g_maps + 6 * m, g_maps + 8 * m, m };
+                LmRun gr{ ctx->fb_lum.p, stride, g_init, g_out, g_rmse, g_stats, chroma ? g_avg : nullptr, g_maps,
+                          g_maps + 3 * m, g_maps + 6 * m, g_maps + 8 * m, m };
                 SVF_TRY(run_lm(ctx, lay, &opts->lsq, gr));
                 SVF_CUDA(svf::launch_fallback_merge(idx, m, g_out, g_rmse, g_stats, g_maps, g_init, n,
                                                     ctx->out.as<float>(), ctx->rmse.as<float>(),

@@ -875,7 +875,7 @@ __global__ void gather_slabs_kernel(const float* __restrict__ lum, uint64_t stri
     const uint64_t t = idx[i];
     for(uint64_t k = threadIdx.x; k < stride; k += blockDim.x)
         g_lum[i * stride + k] = lum[t * stride + k];
-    if(threadIdx.x < 3)
+    if(avg && threadIdx.x < 3)   // the average chromaticity, when it was computed
         g_avg[3 * i + threadIdx.x] = avg[3 * t + threadIdx.x];
 }
 
