@@ -1328,6 +1328,11 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 {
                     write_texel<M>(args, st, sl.texel, sl.npairs);
                     slot_fetch(args, sl, slab_of(s));
+                    // the next texel starts in this visit (its slab copy is short
+                    // next to the other slots' passes, which the workers run
+                    // meanwhile) rather than after a round with the slot idle
+                    if(sl.loading)
+                        build = slot_start(args, sl);
                 }
             }
             else if(sl.loading)
