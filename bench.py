@@ -16,7 +16,8 @@ reference's default initial guess (NDF -> PCA -> SGGX projection), LM
   region.
 * roofline: the LM kernel (the dominant kernel) against the FP32 CUDA-core peak
   (SMs x 128 lanes x 2 flops x SM clock sampled under load), with its
-  algorithmic flops counted per ordered direction pair (see DESIGN.md);
+  algorithmic flops counted per ordered direction pair (169 per Jacobian
+  evaluation, 33 per residual, an FMA counted as 2);
   traffic from the ncu capture summarised in profiles/.
 * roofline_ndf: the NDF GEMM of the default initial guess (tcgen05 tensor
   cores) against the measured BF16 peak in MEASURED_PEAKS.json.

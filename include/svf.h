@@ -297,7 +297,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
  * logarithm, 6 values), log ks, log kd; it is trained on seeded synthetic texels
  * that the plain LM, started from the reference's default guess, has fitted.
  * SVF_INIT_MLP then starts LM from its prediction: the fit skips the NDF
- * pipeline, and its result is judged against the plain LM's residual.
+ * pipeline, and its result is compared with the plain LM's residual.
  * Inference runs the hidden layers on the tensor cores with weights and
  * activations split into BF16 hi/lo pairs, accumulating in FP32 (the FP32
  * network to about 1e-5). */

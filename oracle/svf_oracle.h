@@ -43,7 +43,7 @@ void svfo_angles_to_parabolic(const float* theta_phi, uint32_t count, float* par
  * LM hands them to the evaluator. */
 float svfo_brdf_f32(const double* params7, const float* lights_parabolic, uint32_t light_count,
                     uint32_t view, uint32_t light, float fresnel);
-/* The same model evaluated in double precision throughout (the FP64 judge). */
+/* The same model evaluated in double precision throughout (the FP64 reference values). */
 double svfo_brdf_f64(const double* params7, const float* lights_parabolic, uint32_t light_count,
                      uint32_t view, uint32_t light, double fresnel);
 /* All L*L pairs. */

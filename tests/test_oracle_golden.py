@@ -135,7 +135,7 @@ def test_reference_lm_is_sensitive_to_one_ulp(oracle_lib, golden):
     initial parameter by one float ulp changes the final RMSE of four of the
     eight golden texels by more than 1%, two of them for the worse (texel 5
     ends 5.6x worse).  This is why parity of the GPU fit from that start is
-    judged on RMSE statistics (tests/test_gpu_lsq.py), not texel by texel."""
+    compared on RMSE statistics (tests/test_gpu_lsq.py), not texel by texel."""
     p = golden["pipeline"]
     lp = golden["mesh"]["lights_parabolic"]
     r = []
