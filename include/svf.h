@@ -326,7 +326,7 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lights_parabolic, uint32_t L
 svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples, uint32_t sample_type,
                            uint32_t texels, float* params, float* features);
 /* One optimiser step on given normalised features [rows][96] and targets
- * [rows][10] (sgd != 0: plain gradient step of size lr; else Adam); *loss is
+ * [rows][8] (sgd != 0: plain gradient step of size lr; else Adam); *loss is
  * the MSE before the step.  For checking the training kernels. */
 svf_status svf_mlp_step(svf_ctx* ctx, svf_mlp* mlp, const float* features, const float* targets, uint32_t rows,
                         float lr, uint32_t sgd, float* loss);

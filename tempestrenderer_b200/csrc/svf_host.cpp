@@ -437,7 +437,7 @@ struct MlpScratch
     DevBuf z1, h1, z2, h2, y, dy, dh2, dh1, dsum, loss;
 };
 
-// One optimiser step on normalised X [rows][96], T [rows][10]: forward, MSE
+// One optimiser step on normalised X [rows][96], T [rows][8]: forward, MSE
 // gradient, backward into mlp->g, Adam (or SGD); adds the loss to *loss_dev.
 svf_status mlp_train_step(svf_ctx* ctx, svf_mlp* mlp, MlpScratch& s, const float* X, const float* T, int rows,
                           float lr, bool sgd)

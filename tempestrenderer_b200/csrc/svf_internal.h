@@ -196,7 +196,7 @@ constexpr int kMlpPairs = 32;                  // single direction pairs per tex
 constexpr int kMlpInputs = kMlpBins + kMlpPairs;
 constexpr int kMlpHidden = 256;
 constexpr int kMlpOutputs = 8;                 // log S (6 elements), log ks, log kd
-// flat parameter vector: W1 [256][96], b1, W2 [256][256], b2, W3 [10][256], b3
+// flat parameter vector: W1 [256][96], b1, W2 [256][256], b2, W3 [8][256], b3
 constexpr size_t kMlpW1 = 0, kMlpB1 = kMlpW1 + (size_t)kMlpHidden * kMlpInputs;
 constexpr size_t kMlpW2 = kMlpB1 + kMlpHidden, kMlpB2 = kMlpW2 + (size_t)kMlpHidden * kMlpHidden;
 constexpr size_t kMlpW3 = kMlpB2 + kMlpHidden, kMlpB3 = kMlpW3 + (size_t)kMlpOutputs * kMlpHidden;
