@@ -18,7 +18,7 @@ reference's default initial guess (NDF -> PCA -> SGGX projection), LM
   (SMs x 128 lanes x 2 flops x SM clock sampled under load), with its
   algorithmic flops counted per ordered direction pair (169 per Jacobian
   evaluation, 33 per residual, an FMA counted as 2);
-  traffic from the ncu capture summarised in profiles/.
+  traffic per texel from an ncu capture of a 160x160-texel case.
 * roofline_ndf: the NDF GEMM of the default initial guess (tcgen05 tensor
   cores) against the measured BF16 peak in MEASURED_PEAKS.json.
 * cpu_baseline: the reference's own CPU fitter (oracle/_ref, compiled from the
@@ -51,12 +51,12 @@ WIDTH = HEIGHT = 400
 # unordered pair (svf_lm.cu::sym_pair), so it executes fewer.
 FLOPS_JACOBIAN_PASS = 169
 FLOPS_RESIDUAL_PASS = 33
-# DRAM bytes per texel of lm_fit_kernel, measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum = 675.3 MB + 6.6 MB for 25600 texels; the luminance slab
-# is read once): profiles/lm_fit_kernel_160x160_ring81.md.
+# DRAM bytes per texel of lm_fit_kernel, measured by ncu on a 160x160-texel ring-81
+# capture (dram__bytes_read.sum + dram__bytes_write.sum = 675.3 MB + 6.6 MB for
+# 25600 texels; the luminance slab is read once).
 LM_DRAM_BYTES_PER_TEXEL = (675.3e6 + 6.6e6) / 25600
-# DRAM bytes per texel of ndf_tc_kernel, measured by ncu (2.30 GB + 335 MB for
-# 25600 texels): profiles/ndf_tc_kernel_160x160_ring81.md.
+# DRAM bytes per texel of ndf_tc_kernel, measured by ncu on the same capture
+# (2.30 GB + 335 MB for 25600 texels).
 NDF_DRAM_BYTES_PER_TEXEL = (2.30e9 + 335e6) / 25600
 NDF_ROWS, NDF_ROWS_PAD = 3217, 3328   # 64x64 NDF texels inside the hemisphere, padded to the tile
 
@@ -128,9 +128,10 @@ def ring81_mesh():
 # the reference's CPU fitter
 # ----------------------------------------------------------------------------
 
-def reference_fit_rate(texels: int, first: int = 0, threads: int | None = None):
+def reference_fit_rate(texels: int, first: int = 0, threads: int | None = None, indices=None):
     """Times the reference's texel loop (oracle/_ref) on `texels` texels of the
-    benchmark BTF, all host threads; returns (texels/s, seconds, threads)."""
+    benchmark BTF (texels first.. or the given texel indices), all host threads;
+    returns (texels/s, seconds, threads, per-texel RMSE)."""
     import oracle
 
     if not oracle.ref_available():
@@ -138,11 +139,29 @@ def reference_fit_rate(texels: int, first: int = 0, threads: int | None = None):
     threads = threads or os.cpu_count() or 1
     tp = oracle.ring81_angles()
     lp = oracle.angles_to_parabolic(tp)
-    rgb = np.stack([oracle.synth_render(SEED, first + t, oracle.synth_truth(SEED, MIX, first + t), lp)
-                    for t in range(texels)])
+    idx = list(range(first, first + texels)) if indices is None else [int(i) for i in indices]
+    rgb = np.stack([oracle.synth_render(SEED, t, oracle.synth_truth(SEED, MIX, t), lp) for t in idx])
     btf = oracle.RefBTF.from_texels(tp, rgb)
-    secs, rmse = btf.time_fit(0, texels, threads, 0)
-    return texels / secs, secs, threads, rmse
+    secs, rmse = btf.time_fit(0, len(idx), threads, 0)
+    return len(idx) / secs, secs, threads, np.asarray(rmse, np.float64)
+
+
+# Texels of the benchmark BTF that the reference also fits for the parity block:
+# PARITY_TEXELS indices spread evenly over the 400x400 texels.
+PARITY_TEXELS = 256
+
+
+def parity_indices(T: int, n: int = PARITY_TEXELS):
+    return np.unique(np.linspace(0, T - 1, n).round().astype(np.int64))
+
+
+def parity_block(gpu_rmse, ref_rmse):
+    """Per-texel final RMSE of the GPU fit over the reference CPU fit's, same texels."""
+    g, r = np.asarray(gpu_rmse, np.float64), np.asarray(ref_rmse, np.float64)
+    ratio = g / np.maximum(r, 1e-30)
+    return {"texels": int(len(g)), "mean_ratio": float(g.mean() / r.mean()), "median_ratio": float(np.median(ratio)),
+            "within_1pct": float(np.mean(ratio <= 1.01)), "p99_ratio": float(np.quantile(ratio, 0.99)),
+            "max_ratio": float(ratio.max()), "below_0.99": float(np.mean(ratio < 0.99))}
 
 
 def run_reference(args):
@@ -363,6 +382,13 @@ def batch_item(svf, ctx, steps, dev):
     for _ in range(steps):
         maps, runs, total = ctx.fit_btfs(btfs, opts=opts, want=("rmse", "stats"), check=False)
     T = sum(b["width"] * b["height"] for b in btfs)
+    # each BTF alone (its own svf_fit_texels call): its texels/s
+    alone = []
+    for b in btfs:
+        fit1 = lambda: ctx.fit_texels(b["layout"], b["samples"], b["width"], b["height"],
+                                      sample_type=svf.SVF_SAMPLES_F16, opts=opts, want=("rmse",), check=False)[1]
+        fit1()
+        alone.append(fit1().ms_total)
     # the same batch from the learned guess: one model per layout (2^18 texels, 12 epochs)
     t0 = time.perf_counter()
     models = {id(lay): svf.Mlp.train(ctx, lay.lights_parabolic,
@@ -373,10 +399,11 @@ def batch_item(svf, ctx, steps, dev):
     ctx.fit_btfs(lbtfs, opts=opts, want=("rmse",), check=False)
     lmaps, lruns, ltotal = ctx.fit_btfs(lbtfs, opts=opts, want=("rmse", "stats"), check=False)
     per = []
-    for (lay, side), m, r, lm in zip(shapes, maps, runs, lmaps):
+    for (lay, side), m, r, lm, ms1 in zip(shapes, maps, runs, lmaps, alone):
         it, lit = m["stats"]["iterations"], lm["stats"]["iterations"]
         ratio = lm["rmse"] / np.maximum(m["rmse"], 1e-12)
         per.append({"btf": f"{side}x{side} @ {lay.light_count}", "texels": int(r.texels),
+                    "texels_per_s": side * side / (ms1 / 1e3), "ms_alone": ms1,
                     "iterations_p50": float(np.percentile(it, 50)), "iterations_p99": float(np.percentile(it, 99)),
                     "mean_rmse": float(m["rmse"].mean()), "max_rmse": float(m["rmse"].max()),
                     "failed_texels": int(r.failed_texels),
@@ -474,6 +501,34 @@ def btf_file_item(svf, ctx, layout, W, H, steps, dev, K=48):
                         "failed_texels": int(rs.failed_texels), "mean_rmse": float(maps["rmse"].mean()),
                         "note": "host wall time of svf_fit_btf (decode into FP32 chunks + the fit pipeline); "
                                 "maps copied to host"}}
+
+
+def summarize(line, parity):
+    """The line items' headline figures in a few short keys."""
+    def r3(x):
+        return None if x is None else float(f"{x:.4g}")
+
+    out = {"parity_vs_reference": parity}
+    li = line.get("learned_init")
+    if li and li.get("config3_1024x1024_fp16"):
+        c3 = li["config3_1024x1024_fp16"]
+        out["config3"] = {"speedup_vs_plain_gpu_lm": r3(c3["speedup"]),
+                          "speedup_with_fallback": r3(c3.get("with_fallback", {}).get("speedup")),
+                          "residual_ratio_mean": r3(c3["residual_ratio"]["mean"]),
+                          "residual_ratio_mean_with_fallback": r3(c3.get("with_fallback", {}).get("residual_ratio_mean")),
+                          "normal_p90_deg": {"plain": r3(c3["plain"]["ground_truth_error"]["normal_deg"]["p90"]),
+                                             "learned": r3(c3["learned"]["ground_truth_error"]["normal_deg"]["p90"]),
+                                             "with_fallback": r3(c3.get("with_fallback", {}).get("normal_p90_deg"))}}
+    b = line.get("batch_8_btfs")
+    if b:
+        out["config4"] = {"batch_texels_per_s": r3(b["value"]),
+                          "per_btf_texels_per_s": {p["btf"]: r3(p.get("texels_per_s")) for p in b["per_btf"]},
+                          "learned_residual_ratio_mean": {p["btf"]: r3(p["learned"]["residual_ratio_vs_plain"]["mean"])
+                                                          for p in b["per_btf"]}}
+    f = line.get("fib151_768x768")
+    if f:
+        out["config2"] = {"texels_per_s": r3(f["value"]), "fp64_check": f.get("fp64_check_summary")}
+    return out
 
 
 def run_ours(args):
@@ -646,13 +701,16 @@ def run_ours(args):
         ndf_alg = 2.0 * T * NDF_ROWS * N * args.steps               # one FP32 GEMM
         ndf_hw = 2.0 * T * NDF_ROWS_PAD * ((kp + 63) // 64 * 64) * 3 * args.steps   # BF16x3, padded tiles
         ndf_ach = ndf_alg / (ms_ndf / 1e3) / 1e12 if ms_ndf > 0 else None
-        cpu = None
+        cpu = parity = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                rate, secs, thr, _ = reference_fit_rate(max(16, 2 * (os.cpu_count() or 1)))
+                idx = parity_indices(T)
+                rate, secs, thr, ref_rmse = reference_fit_rate(len(idx), indices=idx)
                 cpu = {"value": rate, "unit": "texels/s", "cores": thr, "kind": "reference",
-                       "sample": f"first {max(16, 2 * thr)} texels of the benchmark BTF, {thr} threads, "
-                                 f"{secs:.1f} s"}
+                       "sample": f"{len(idx)} texels spread evenly over the benchmark BTF (indices "
+                                 f"linspace(0, {T - 1}, {len(idx)})), {thr} threads, {secs:.1f} s"}
+                parity = dict(parity_block(head_rmse[idx], ref_rmse),
+                              what="GPU RMSE / reference CPU RMSE per texel, the same texels (default init)")
             except Exception as e:  # the checker may be absent on a box without it built
                 cpu = {"value": None, "unit": "texels/s", "cores": os.cpu_count(), "kind": "reference",
                        "sample": f"unavailable: {e}"}
@@ -668,7 +726,7 @@ def run_ours(args):
             "roofline": {"bound": "fp32", "kernel": "lm_fit_kernel", "achieved": achieved, "peak": fp32_peak,
                          "unit": "TFLOP/s", "frac": achieved / fp32_peak,
                          "traffic": LM_DRAM_BYTES_PER_TEXEL * T,
-                         "traffic_source": "ncu dram bytes per texel (profiles/lm_fit_kernel_160x160_ring81.md) x texels",
+                         "traffic_source": "ncu dram bytes per texel (160x160-texel ring-81 capture) x texels",
                          "peak_source": f"derived: {props.multi_processor_count} SMs x 128 FP32 lanes x 2 x "
                                         f"{sm_mhz:.0f} MHz (sampled SM clock under load); MEASURED_PEAKS.json "
                                         f"has no FP32 figure"},
@@ -686,9 +744,11 @@ def run_ours(args):
                         "failed_texels": failed, "mean_rmse": float(head_rmse.mean()),
                         "median_rmse": float(np.median(head_rmse)), "ground_truth_error": head_truth_err},
             "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "learned_init": learned, "fib151_768x768": fib,
-            "batch_8_btfs": batch, "btf_file": btf_file, "refit_neighborhood": refit, "gpu_launches": 4 * args.steps, "cpu_baseline": cpu,
-            "wall_s": wall,
+            "batch_8_btfs": batch, "btf_file": btf_file, "refit_neighborhood": refit, "gpu_launches": 4 * args.steps,
+            "wall_s": wall, "cpu_baseline": cpu,
         }
+        # short summaries last, so that a reader of the line's tail sees them
+        line["summary"] = summarize(line, parity)
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -176,8 +176,13 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lights_parabolic, uint32
  * static device array of SVF_NOALLOC_SCRATCH_BYTES that every GPU which loads
  * the library holds until the process exits.
  *
- * - Every buffer (lights_parabolic, lum, init, out, rmse, stats) must be device
- *   memory of the current device; stats may be NULL.
+ * - Every buffer (lights_parabolic, lum, init, out, rmse, stats) must be plain
+ *   device memory of the current device (not host, managed or another GPU's
+ *   memory); stats may be NULL.  Other buffers are rejected with SVF_EINVAL
+ *   before anything is launched.
+ * - Status: as svf_lsq_fit_batch.  SVF_ETIMEOUT when a bounded device wait
+ *   expired; with stats given, SVF_EPARTIAL when some texel ends with
+ *   SVF_TEXEL_NONFINITE or SVF_TEXEL_TIMEOUT.
  * - Limits: light_count <= 160 and texel_count * (L*L rounded up to 8) <=
  *   SVF_NOALLOC_MAX_SLAB_FLOATS (79 texels at 81 directions); larger sizes are
  *   rejected with SVF_EINVAL.
@@ -185,7 +190,9 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lights_parabolic, uint32
  *   enqueues its work there and waits for it before returning.
  * - The first call on each device looks up the address of the static array
  *   (cudaGetSymbolAddress) with that device current; make that first call
- *   before any stream capture.
+ *   before any stream capture.  The address is kept for the life of the
+ *   process: after a cudaDeviceReset of a device this entry point must not be
+ *   called on that device again in the same process.
  * - All calls share the array and it keeps the last call's contents; calls
  *   whose work overlaps on the GPU (other threads or streams) race on it and
  *   must be serialised by the caller. */

@@ -31,6 +31,7 @@ SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
 SVF_ERROR_PAIRWISE, SVF_ERROR_MAX_VIEW = 0, 1
 SVF_MLP_FEATURES_PAIRS_RGB, SVF_MLP_FEATURES_BINS = 0, 1
+SVF_NOALLOC_MAX_SLAB_FLOATS = 1 << 19   # include/svf.h
 
 # every entry point include/svf.h declares
 EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_options_default", "svf_create",

@@ -177,6 +177,20 @@ bool is_device_pointer(const void* p)
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
+// Plain device memory (not managed, not host) of device `dev`.
+bool is_device_pointer_on(const void* p, int dev)
+{
+    if(!p)
+        return false;
+    cudaPointerAttributes a;
+    if(cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice && a.device == dev;
+}
+
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 
 // Default-init tables of one (direction table, mesh) pair.
@@ -841,6 +855,21 @@ svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmR
     return launch_lm(ctx, lay, o, r, lm_choice(lay, r.stride, r.rgb));
 }
 
+// Fault injection for the tests of the bounded slab wait, read from the
+// environment at each launch: SVF_FAULT_SKIP_SLAB_COPY=<texel> leaves that
+// texel's slab copy unissued (its wait runs out: SVF_ETIMEOUT, the texel's status
+// SVF_TEXEL_TIMEOUT), SVF_FAULT_WAIT_SPINS=<n> shortens the wait's bound.  No
+// GPU fault is involved: the wait is on a barrier that nothing completes.
+void lm_fault_injection(svf::LmArgs& a)
+{
+    a.fault_skip_texel = svf::kLmNoFault;
+    a.wait_spins = 0;
+    if(const char* e = std::getenv("SVF_FAULT_SKIP_SLAB_COPY"))
+        a.fault_skip_texel = (uint32_t)std::strtoul(e, nullptr, 10);
+    if(const char* e = std::getenv("SVF_FAULT_WAIT_SPINS"))
+        a.wait_spins = (uint32_t)std::strtoul(e, nullptr, 10);
+}
+
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c)
 {
     svf::LmArgs a{};
@@ -884,6 +913,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     SVF_TRY(ctx->error.ensure(16));
     a.work_counter = ctx->counter.as<uint32_t>();
     a.error_flag = ctx->error.as<uint32_t>();
+    lm_fault_injection(a);
     SVF_CUDA(cudaMemsetAsync(ctx->counter.p, 0, 16, ctx->stream));   // the error words are zeroed per call
     a.rgb = r.rgb ? 1u : 0u;
     int per_sm = svf::lm_max_ctas_per_sm(a.L, a.lum_stride, c, r.rgb);
@@ -1131,23 +1161,36 @@ svf_status svf_lsq_fit_batch_noalloc(const float* lp, uint32_t L, const float* l
                     "split the batch",
                     texels, L, (unsigned long long)((uint64_t)texels * slab), SVF_NOALLOC_MAX_SLAB_FLOATS,
                     (unsigned long long)(SVF_NOALLOC_MAX_SLAB_FLOATS / slab));
-    const void* must_be_device[] = { lp, lum, init, out, rmse };
-    for(const void* p : must_be_device)
-        if(!is_device_pointer(p))
-            return fail(SVF_EINVAL, "svf_lsq_fit_batch_noalloc: every buffer must be device memory (and not NULL)");
-    if(stats && !is_device_pointer(stats))
-        return fail(SVF_EINVAL, "svf_lsq_fit_batch_noalloc: stats must be device memory or NULL");
+    // device memory of the current device only: a buffer of another GPU (or
+    // managed memory) would make the kernels read or write a peer's memory
+    int dev = -1;
+    SVF_CUDA(cudaGetDevice(&dev));
+    const void* must_be_device[] = { lp, lum, init, out, rmse, stats };
+    for(int i = 0; i < 6; ++i)
+    {
+        const void* p = must_be_device[i];
+        if(!p && i == 5)
+            break;   // stats may be NULL
+        if(!is_device_pointer_on(p, dev))
+            return fail(SVF_EINVAL,
+                        "svf_lsq_fit_batch_noalloc: every buffer must be device memory of the current device "
+                        "(device %d; not NULL, not host, managed or another GPU's memory)",
+                        dev);
+    }
     svf::LmConfig cfg;
     cfg.max_iter = opts->max_iterations;
     cfg.mse_target = opts->mse_target;
     cfg.eps = opts->break_on_small_step;
     cfg.fresnel = opts->fresnel;
     cfg.restarts = opts->restarts;
-    uint32_t error_flag = 0;
+    uint32_t flags[2] = { 0, 0 };
     SVF_CUDA(svf::launch_lm_fit_noalloc(lp, L, lum, lum_stride, texels, cfg, init, out, rmse, stats,
-                                        static_cast<cudaStream_t>(stream), &error_flag));
-    if(error_flag)
+                                        static_cast<cudaStream_t>(stream), flags));
+    if(flags[0])
         return fail(SVF_ETIMEOUT, "a bounded device wait expired (a texel slab did not arrive)");
+    // the status contract of svf_lsq_fit_batch
+    if(flags[1])
+        return fail(SVF_EPARTIAL, "some texels did not produce a finite fit");
     return SVF_OK;
 }
 

@@ -55,7 +55,13 @@ struct LmArgs
     LmConfig cfg;
     uint32_t* work_counter;    // zeroed before the launch
     uint32_t* error_flag;      // set non-zero by a bounded wait that expired
+    // Fault injection for tests (the host sets it from the environment): the slab
+    // copy of texel fault_skip_texel is not issued, so its wait runs out;
+    // kLmNoFault for none.  wait_spins: the bound of every slab wait (0: default).
+    uint32_t fault_skip_texel;
+    uint32_t wait_spins;
 };
+constexpr uint32_t kLmNoFault = 0xffffffffu;
 
 // LM kernel configuration (svf_lm.cu): CTA size (one control warp + pair
 // workers) and the texel slots each CTA keeps in flight.
@@ -71,11 +77,12 @@ int            lm_max_ctas_per_sm(uint32_t L, uint64_t lum_stride, LmKernelChoic
 cudaError_t    launch_lm_fit(const LmArgs& args, LmKernelChoice c, int grid, cudaStream_t stream);
 
 // svf_lsq_fit_batch_noalloc: repack, geometry and LM on `stream` with the
-// library's static device scratch array; waits for the stream and returns the
-// kernel's error flag in *error_flag.
+// library's static device scratch array; waits for the stream.  flags[0]: the
+// kernel's error flag (a bounded wait expired); flags[1]: the OR of the texels'
+// SVF_TEXEL_NONFINITE | SVF_TEXEL_TIMEOUT bits (0 when stats is NULL).
 cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, const float* lum, uint64_t lum_stride,
                                   uint32_t texels, const LmConfig& cfg, const float* init, float* out, float* rmse,
-                                  svf_texel_stats* stats, cudaStream_t stream, uint32_t* error_flag);
+                                  svf_texel_stats* stats, cudaStream_t stream, uint32_t flags[2]);
 
 // Luminance slice + average chromaticity (BTFParallelExtractLuminanceSlice,
 // src/image/btf.cc:1078-1116) for texels [0, texels) of an RGB sample array.

@@ -552,6 +552,18 @@ __global__ void geo_from_parabolic_kernel(const float* __restrict__ lp, uint32_t
     geo[2 * L + d] = __fdiv_rn(__fsub_rn(1.0f, len_sq), __fadd_rn(1.0f, len_sq));
 }
 
+// ORs the texels' "no finite fit" bits (SVF_TEXEL_NONFINITE, SVF_TEXEL_TIMEOUT)
+// into *partial, so the host learns of them from one word.
+__global__ void partial_scan_kernel(const svf_texel_stats* __restrict__ stats, uint32_t texels, uint32_t* partial)
+{
+    uint32_t bits = 0;
+    for(uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < texels; t += gridDim.x * blockDim.x)
+        bits |= stats[t].status & (SVF_TEXEL_NONFINITE | SVF_TEXEL_TIMEOUT);
+    bits = __reduce_or_sync(0xffffffffu, bits);
+    if(bits && (threadIdx.x & 31u) == 0)
+        atomicOr(partial, bits);
+}
+
 } // namespace
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SVF_NOALLOC_SCRATCH_BYTES];
@@ -563,7 +575,9 @@ std::mutex g_noalloc_mutex;
 void* g_noalloc_address[kNoAllocMaxDevices];
 
 // Device address of g_noalloc_scratch on the current device, looked up once per
-// device.  In host code the array's name is only a host-side stand-in.
+// device and kept for the life of the process (a cudaDeviceReset of the device
+// would leave it stale).  In host code the array's name is only a host-side
+// stand-in.
 cudaError_t noalloc_scratch_address(void** out)
 {
     int dev = 0;
@@ -588,7 +602,7 @@ cudaError_t noalloc_scratch_address(void** out)
 
 cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, const float* lum, uint64_t lum_stride,
                                   uint32_t texels, const LmConfig& cfg, const float* init, float* out, float* rmse,
-                                  svf_texel_stats* stats, cudaStream_t stream, uint32_t* error_flag)
+                                  svf_texel_stats* stats, cudaStream_t stream, uint32_t host_flags[2])
 {
     void* base = nullptr;
     cudaError_t e = noalloc_scratch_address(&base);
@@ -627,6 +641,8 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
     a.cfg = cfg;
     a.work_counter = flags;
     a.error_flag = flags + 1;
+    a.fault_skip_texel = kLmNoFault;
+    a.wait_spins = 0;
     const LmKernelChoice choice = lm_default_choice(L, stride);
     const int per_sm = lm_max_ctas_per_sm(L, stride, choice);
     if(per_sm <= 0)
@@ -634,7 +650,14 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
     const uint64_t grid = std::min<uint64_t>((uint64_t)per_sm * sms, texels);
     if((e = launch_lm_fit(a, choice, (int)std::max<uint64_t>(grid, 1), stream)) != cudaSuccess)
         return e;
-    if((e = cudaMemcpyAsync(error_flag, flags + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
+    if(stats)
+    {
+        partial_scan_kernel<<<(texels + 255) / 256, 256, 0, stream>>>(stats, texels, flags + 2);
+        if((e = cudaGetLastError()) != cudaSuccess)
+            return e;
+    }
+    // flags[1]: a bounded wait expired; flags[2]: texels without a finite fit
+    if((e = cudaMemcpyAsync(host_flags, flags + 1, 2 * sizeof(uint32_t), cudaMemcpyDeviceToHost, stream)) != cudaSuccess)
         return e;
     return cudaStreamSynchronize(stream);
 }

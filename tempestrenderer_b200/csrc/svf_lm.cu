@@ -122,11 +122,13 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                  : "memory");
 }
 
-// Bounded wait for phase `parity` of `bar`; false when the bound expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity)
+// Bounded wait for phase `parity` of `bar` (at most `spins` polls, 0: the
+// default bound); false when the bound expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t spins = 0)
 {
     const uint32_t b = smem_addr(bar);
-    for(uint32_t i = 0; i < kWaitSpins; ++i)
+    const uint32_t bound = spins ? spins : kWaitSpins;
+    for(uint32_t i = 0; i < bound; ++i)
     {
         uint32_t done;
         asm volatile("{\n\t.reg .pred p;\n\t"
@@ -880,6 +882,8 @@ struct Slot
     int first;            // the pending pass is at the texel's initial point (else at a trial point)
     int loading;          // the slab copy of `texel` is in flight
     int dead;             // a copy did not arrive: the slot takes no more texels
+    int issued;           // the pending slab copy was issued (it may still land)
+    int drain;            // dead with a copy possibly in flight: wait for it before exit
     uint32_t arrived;     // worker warps done with the current pass (the last one sums)
     uint32_t L;           // layout of the texel in the slot
     uint32_t slab_bytes;
@@ -1044,8 +1048,11 @@ __device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot<M>& sl, void
         sl.geo = g.geo;
         sl.damping = g.damping > 0.0f ? g.damping : 1.0f;
         sl.slab_bytes = (uint32_t)(g.stride * sizeof(typename M::Slab));
-        bulk_load(slab, static_cast<const typename M::Slab*>(g.lum) + (uint64_t)(t - g.first) * g.stride, sl.slab_bytes,
-                  &sl.bar);
+        // (fault injection: the copy of one texel is not issued and its wait runs out)
+        sl.issued = t != args.fault_skip_texel;
+        if(sl.issued)
+            bulk_load(slab, static_cast<const typename M::Slab*>(g.lum) + (uint64_t)(t - g.first) * g.stride,
+                      sl.slab_bytes, &sl.bar);
         sl.texel = t;
         sl.loading = 1;
     }
@@ -1062,12 +1069,13 @@ __device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot<M>& sl, void
 template <class M>
 __device__ __forceinline__ bool slot_start(const LmArgs& args, Slot<M>& sl)
 {
-    if(!mbar_wait(&sl.bar, sl.parity))
+    if(!mbar_wait(&sl.bar, sl.parity, args.wait_spins))
     {
         atomicOr(args.error_flag, 1u);
         if(args.stats)
             args.stats[sl.texel].status = SVF_TEXEL_TIMEOUT;
         sl.dead = 1;
+        sl.drain = sl.issued;   // the copy may still land in the slot's shared memory
         sl.loading = 0;
         sl.texel = kNoTexel;
         sl.cmd = kSlotIdle;
@@ -1249,6 +1257,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
             mbar_init(&sl.bar, 1);
             sl.parity = 0;
             sl.dead = 0;
+            sl.drain = 0;
             sl.arrived = 0;
             slot_fetch(args, sl, slab_of(s));
         }
@@ -1365,6 +1374,12 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
             // then meet the exit command of slot s
             for(int j = 1; j < S; ++j)
                 nbar_sync(bar_done<S>((s + j) % S), kThreads);
+            // a slab copy whose wait expired may still be in flight: wait for it
+            // (bounded again) before the CTA's shared memory is released
+            if(lane == 0)
+                for(int j = 0; j < S; ++j)
+                    if(slots[j].drain)
+                        mbar_wait(&slots[j].bar, slots[j].parity, args.wait_spins);
             break;
         }
     }
