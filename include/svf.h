@@ -73,12 +73,22 @@ typedef enum svf_status
  * {kd rgb, ks rgb, sx, sy, quaternion xyzw}; the diffuse / specular maps are
  * the fitted albedos and rmse is over the three channels. */
 #define SVF_LSQ_RGB          (1u << 8)
+/* The small-step stopping test per parameter (no counterpart in the reference):
+ * LM stops when every step entry is small against its own parameter,
+ * |d_i| <= e (|p_i| + e) for sigma, specular and diffuse and |d_i| <= e (1 + e)
+ * for the angles (e = break_on_small_step), instead of the reference's test on
+ * the whole vector, |d| <= e (|p + e| + e) (fitting.hh:583-588).  The whole-vector
+ * test is dominated by the largest entries (the Euler angles, up to pi), so it
+ * stops while a narrow lobe's sigma (0.01 - 0.05) may still move by a tenth of
+ * itself, where the residual is steep.  Set by svf_lsq_options_default; clear
+ * it for the reference's test. */
+#define SVF_LSQ_STEP_PER_PARAMETER (1u << 9)
 
 typedef struct svf_lsq_options
 {
     uint32_t max_iterations;      /* CurveFitSteps (svbrdf-fitting.hh:51): 1024 */
     float    fresnel;             /* refractive index of the Fresnel term; 1 = no Fresnel */
-    uint32_t flags;               /* must contain SVF_LSQ_DIFFUSE */
+    uint32_t flags;               /* must contain SVF_LSQ_DIFFUSE; default also SVF_LSQ_STEP_PER_PARAMETER */
     double   mse_target;          /* LevenbergMarquardtCurveFit mean_sq_error: 1e-6 */
     double   break_on_small_step; /* LevenbergMarquardtSettings::BreakOnSmallStep: 1e-3 */
     uint32_t restarts;            /* times LM continues, with fresh damping, from the point where

@@ -272,11 +272,24 @@ double ref_time_fit_texels(void* handle, uint32_t first_texel, uint32_t texel_co
                            float fresnel, float* rmse_out)
 {
     auto* btf = reinterpret_cast<Tempest::BTF*>(handle);
-    Tempest::ThreadPool* pool = new Tempest::ThreadPool(pool_threads);
+    /* pool_threads > 0: one pool shared by the workers, as svbrdffit shares one;
+     * a texel's parallel loops are then partly run by other workers, which race
+     * on the shared-seed loops of the default initial guess
+     * (svbrdf-fitting-pipeline.cc:451-456), so results depend on scheduling.
+     * pool_threads == 0: each worker runs its texels' loops itself on a private
+     * zero-thread pool, so every texel's fit is the deterministic one that a
+     * single-texel run gives (the same work, spread over the workers by texel). */
+    const bool shared = pool_threads > 0;
+    Tempest::ThreadPool* pool = shared ? new Tempest::ThreadPool(pool_threads) : nullptr;
     std::atomic<uint32_t> counter(0);
+    std::vector<Tempest::ThreadPool*> pools(workers, pool);
     std::vector<uint32_t> ids(workers);
     for(uint32_t w = 0; w < workers; ++w)
-        ids[w] = pool->allocateThreadNumber();
+    {
+        if(!shared)
+            pools[w] = new Tempest::ThreadPool(0);   /* never destroyed, see SerialPool() */
+        ids[w] = pools[w]->allocateThreadNumber();
+    }
 
     auto t0 = std::chrono::steady_clock::now();
     std::vector<std::thread> threads;
@@ -292,8 +305,8 @@ double ref_time_fit_texels(void* handle, uint32_t first_texel, uint32_t texel_co
                 uint32_t t = first_texel + k;
                 uint32_t x = t % btf->Width, y = t / btf->Width;
                 SGGXParameters out;
-                pipeline.cache(ids[w], *pool, x, y, popts, nullptr);
-                pipeline.fit(ids[w], *pool, x, y, &opts, popts, nullptr, &out, false);
+                pipeline.cache(ids[w], *pools[w], x, y, popts, nullptr);
+                pipeline.fit(ids[w], *pools[w], x, y, &opts, popts, nullptr, &out, false);
                 if(rmse_out)
                     rmse_out[k] = out.RMSE;
             }
@@ -302,8 +315,9 @@ double ref_time_fit_texels(void* handle, uint32_t first_texel, uint32_t texel_co
     for(auto& t : threads)
         t.join();
     auto t1 = std::chrono::steady_clock::now();
-    pool->shutdown();
-    /* the pool object itself is leaked on purpose, see SerialPool() */
+    if(shared)
+        pool->shutdown();
+    /* the pool objects themselves are leaked on purpose, see SerialPool() */
     return std::chrono::duration<double>(t1 - t0).count();
 }
 

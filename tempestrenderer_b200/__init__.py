@@ -27,6 +27,7 @@ SVF_OK, SVF_EINVAL, SVF_ENOMEM, SVF_ECUDA, SVF_ETIMEOUT, SVF_EPARTIAL, SVF_ENODE
 SVF_TEXEL_NONFINITE, SVF_TEXEL_MAX_ITER, SVF_TEXEL_TIMEOUT = 1, 2, 4
 SVF_LSQ_DIFFUSE = 1 << 1
 SVF_LSQ_RGB = 1 << 8
+SVF_LSQ_STEP_PER_PARAMETER = 1 << 9
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
 SVF_ERROR_PAIRWISE, SVF_ERROR_MAX_VIEW = 0, 1
@@ -185,14 +186,17 @@ def _check(status: int):
 
 
 def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | None = None,
-            rgb: bool = False) -> LsqOptions:
-    """LM options; rgb selects the 11-parameter RGB fit (svf_fit_texels / svf_fit_btfs)."""
+            rgb: bool = False, step_per_parameter: bool = True) -> LsqOptions:
+    """LM options; rgb selects the 11-parameter RGB fit (svf_fit_texels / svf_fit_btfs);
+    step_per_parameter=False restores the reference's whole-vector small-step test."""
     o = LsqOptions()
     load().svf_lsq_options_default(C.byref(o))
     o.max_iterations = max_iterations
     o.fresnel = fresnel
     if rgb:
         o.flags |= SVF_LSQ_RGB
+    if not step_per_parameter:
+        o.flags &= ~SVF_LSQ_STEP_PER_PARAMETER
     if restarts is not None:
         o.restarts = restarts
     return o

@@ -526,8 +526,9 @@ svf_status check_options(const svf_lsq_options* o)
         return fail(SVF_EINVAL, "null options");
     if(!(o->flags & SVF_LSQ_DIFFUSE))
         return fail(SVF_EINVAL, "only the fits with the diffuse term (SVF_LSQ_DIFFUSE) are supported");
-    if(o->flags & ~(SVF_LSQ_DIFFUSE | SVF_LSQ_RGB))
-        return fail(SVF_EINVAL, "unknown lsq flags 0x%x", o->flags & ~(SVF_LSQ_DIFFUSE | SVF_LSQ_RGB));
+    constexpr uint32_t known = SVF_LSQ_DIFFUSE | SVF_LSQ_RGB | SVF_LSQ_STEP_PER_PARAMETER;
+    if(o->flags & ~known)
+        return fail(SVF_EINVAL, "unknown lsq flags 0x%x", o->flags & ~known);
     if(!(o->fresnel >= 1.0f) || !std::isfinite(o->fresnel))
         return fail(SVF_EINVAL, "fresnel (refractive index) must be >= 1, got %g", o->fresnel);
     if(!(o->mse_target >= 0.0) || !(o->break_on_small_step > 0.0))
@@ -909,6 +910,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     a.cfg.eps = o->break_on_small_step;
     a.cfg.fresnel = o->fresnel;
     a.cfg.restarts = o->restarts;
+    a.cfg.step_per_param = (o->flags & SVF_LSQ_STEP_PER_PARAMETER) ? 1u : 0u;
     SVF_TRY(ctx->counter.ensure(16));
     SVF_TRY(ctx->error.ensure(16));
     a.work_counter = ctx->counter.as<uint32_t>();
@@ -978,7 +980,7 @@ void svf_lsq_options_default(svf_lsq_options* o)
         return;
     o->max_iterations = 1024;            // CurveFitSteps
     o->fresnel = 1.0f;
-    o->flags = SVF_LSQ_DIFFUSE;
+    o->flags = SVF_LSQ_DIFFUSE | SVF_LSQ_STEP_PER_PARAMETER;
     o->mse_target = 1e-6;
     o->break_on_small_step = (double)1e-3f;   // settings.BreakOnSmallStep = 1e-3f
     o->restarts = 1;
@@ -1183,6 +1185,7 @@ svf_status svf_lsq_fit_batch_noalloc(const float* lp, uint32_t L, const float* l
     cfg.eps = opts->break_on_small_step;
     cfg.fresnel = opts->fresnel;
     cfg.restarts = opts->restarts;
+    cfg.step_per_param = (opts->flags & SVF_LSQ_STEP_PER_PARAMETER) ? 1u : 0u;
     uint32_t flags[2] = { 0, 0 };
     SVF_CUDA(svf::launch_lm_fit_noalloc(lp, L, lum, lum_stride, texels, cfg, init, out, rmse, stats,
                                         static_cast<cudaStream_t>(stream), flags));

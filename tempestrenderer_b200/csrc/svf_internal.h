@@ -18,6 +18,7 @@ struct LmConfig
     double   eps;          // BreakOnSmallStep
     float    fresnel;
     uint32_t restarts;     // continuations from a stop point with fresh damping
+    uint32_t step_per_param;   // the small-step test per parameter (SVF_LSQ_STEP_PER_PARAMETER)
 };
 
 // A run of texels of one direction layout in an LM launch: texels

@@ -325,12 +325,16 @@ __device__ int lm_next(LmState<M::P>& st, const LmConfig& cfg, double n_pairs)
             continue;
         }
         double step2 = 0.0, mag2 = 0.0;
+        bool each_small = true;
 #pragma unroll
         for(int i = 0; i < M::P; ++i)
         {
             step2 += st.d[i] * st.d[i];
             const double t = st.p[i] + cfg.eps;   // (an RGB rotation entry is 0)
             mag2 += t * t;
+            // per parameter: albedos and sigmas against themselves, angles against 1 rad
+            const double scale = i < M::B ? fabs(st.p[i]) : 1.0;
+            each_small = each_small && fabs(st.d[i]) <= cfg.eps * (scale + cfg.eps);
         }
         const double step_len = sqrt(step2);
         if(!isfinite(step_len))
@@ -338,7 +342,7 @@ __device__ int lm_next(LmState<M::P>& st, const LmConfig& cfg, double n_pairs)
             st.status |= SVF_TEXEL_NONFINITE;
             return kCmdDone;
         }
-        if(step_len <= cfg.eps * (sqrt(mag2) + cfg.eps))
+        if(cfg.step_per_param ? each_small : step_len <= cfg.eps * (sqrt(mag2) + cfg.eps))
         {
             if(lm_restart(st, cfg, n_pairs))
                 continue;

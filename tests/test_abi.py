@@ -46,7 +46,7 @@ def test_create_without_usable_device_fails_cleanly(svf_lib):
 def test_null_arguments_rejected(svf_lib):
     o = svf.LsqOptions()
     svf_lib.svf_lsq_options_default(C.byref(o))
-    assert o.max_iterations == 1024 and o.fresnel == 1.0 and o.flags == svf.SVF_LSQ_DIFFUSE
+    assert o.max_iterations == 1024 and o.fresnel == 1.0 and o.flags == svf.SVF_LSQ_DIFFUSE | svf.SVF_LSQ_STEP_PER_PARAMETER
     assert svf_lib.svf_lsq_fit_batch(None, None, 81, None, 0, 1, C.byref(o), None, None, None, None) == svf.SVF_EINVAL
     assert svf_lib.svf_fit_texels(None, None, None, None, None) == svf.SVF_EINVAL
 
