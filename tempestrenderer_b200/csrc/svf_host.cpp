@@ -197,9 +197,57 @@ inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 struct InitData
 {
     svf::InitLayout init{};
-    DevBuf op, op_hi, op_lo, row_texel, denom_w, pca_cell_id, pca_cell_start, pca_index, pca_frac, pca_dir, proj_dir, proj_frac,
-        proj_cell;
+    DevBuf op, row_texel, denom_w, pca_cell_id, pca_cell_start, pca_index, pca_frac, pca_dir, proj_dir, proj_frac,
+        proj_cell, col_pos, col_of, tile_hi, tile_lo, tile_kb, tile_start;
 };
+
+// Interleaves the bits of x and y (x in the even bits).
+uint64_t morton2(uint32_t x, uint32_t y)
+{
+    uint64_t z = 0;
+    for(int b = 0; b < 16; ++b)
+        z |= (uint64_t)((x >> b) & 1u) << (2 * b) | (uint64_t)((y >> b) & 1u) << (2 * b + 1);
+    return z;
+}
+
+// The NDF GEMM's column order: pairs lv = view L + light sorted (stably) by the
+// Morton code of their half vector's parabolic coordinates on a 256 x 256 grid,
+// so that neighbouring columns reach neighbouring NDF texels.
+void half_vector_order(const std::vector<float>& lp, uint32_t L, std::vector<uint32_t>& col_of,
+                       std::vector<uint16_t>& col_pos)
+{
+    const uint32_t N = L * L;
+    std::vector<float> w(3 * L);
+    for(uint32_t d = 0; d < L; ++d)
+        svf::parabolic_to_cartesian_ref(lp[2 * d], lp[2 * d + 1], &w[3 * d]);
+    std::vector<uint64_t> code(N);
+    const auto q = [](double v) { return (uint32_t)std::min(255.0, std::max(0.0, std::floor((v + 1.0) * 128.0))); };
+    for(uint32_t v = 0; v < L; ++v)
+        for(uint32_t l = 0; l < L; ++l)
+        {
+            double h[3] = { (double)w[3 * v] + w[3 * l], (double)w[3 * v + 1] + w[3 * l + 1],
+                            (double)w[3 * v + 2] + w[3 * l + 2] };
+            const double n = std::sqrt(h[0] * h[0] + h[1] * h[1] + h[2] * h[2]);
+            double px = 0.0, py = 0.0;
+            if(n > 1e-12)
+            {
+                const double den = 1.0 + h[2] / n;
+                if(den > 1e-12)
+                {
+                    px = h[0] / n / den;
+                    py = h[1] / n / den;
+                }
+            }
+            code[v * L + l] = morton2(q(px), q(py));
+        }
+    col_of.resize(N);
+    for(uint32_t k = 0; k < N; ++k)
+        col_of[k] = k;
+    std::stable_sort(col_of.begin(), col_of.end(), [&](uint32_t a, uint32_t b) { return code[a] < code[b]; });
+    col_pos.resize(N);
+    for(uint32_t p = 0; p < N; ++p)
+        col_pos[col_of[p]] = (uint16_t)p;
+}
 
 // Direction layout: LM geometry and, once needed, the default-init tables per
 // interpolation mesh (the caller's mesh, or the library's own triangulation).
@@ -643,7 +691,25 @@ svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc, 
     il.ndf_rows_pad = (uint32_t)round_up(il.ndf_rows, 256);
     SVF_TRY(dd->op.ensure(sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
     SVF_CUDA(cudaMemset(dd->op.p, 0, sizeof(float) * il.ndf_rows_pad * (size_t)il.k_pad));
-    SVF_TRY(upload(dd->row_texel, t.ndf_row_texel));
+    // operator rows in Morton order of their NDF texel (a 256-row tile is then a
+    // compact block of the texture)
+    std::vector<uint32_t> row_order(il.ndf_rows);
+    for(uint32_t r = 0; r < il.ndf_rows; ++r)
+        row_order[r] = r;
+    std::stable_sort(row_order.begin(), row_order.end(), [&](uint32_t a, uint32_t b) {
+        const int32_t ta = t.ndf_row_texel[a], tb = t.ndf_row_texel[b];
+        return morton2((uint32_t)(ta % svf::kNdfRes), (uint32_t)(ta / svf::kNdfRes)) <
+               morton2((uint32_t)(tb % svf::kNdfRes), (uint32_t)(tb / svf::kNdfRes));
+    });
+    std::vector<int32_t> row_texel(il.ndf_rows);
+    std::vector<float> row_normal(3 * (size_t)il.ndf_rows);
+    for(uint32_t r = 0; r < il.ndf_rows; ++r)
+    {
+        row_texel[r] = t.ndf_row_texel[row_order[r]];
+        for(int c = 0; c < 3; ++c)
+            row_normal[3 * r + c] = t.ndf_row_normal[3 * row_order[r] + c];
+    }
+    SVF_TRY(upload(dd->row_texel, row_texel));
     SVF_TRY(upload(dd->denom_w, t.denom_w));
     SVF_TRY(upload(dd->pca_cell_id, t.pca_cell_id));
     SVF_TRY(upload(dd->pca_cell_start, t.pca_cell_start));
@@ -679,24 +745,87 @@ svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc, 
     SVF_TRY(upload(d_edges, edges));
     SVF_TRY(upload(d_eang, eang));
     SVF_TRY(upload(d_dirs, t.ndf_dirs));
-    SVF_TRY(upload(d_normals, t.ndf_row_normal));
+    SVF_TRY(upload(d_normals, row_normal));
     SVF_TRY(d_ltri.ensure(sizeof(int32_t) * svf::kNdfSamples));
     SVF_TRY(d_lbary.ensure(sizeof(float) * 3 * svf::kNdfSamples));
     svf::MeshDevice mesh{ d_lp.as<float>(), d_tri.as<uint32_t>(), (uint32_t)(tris.size() / 3), d_edges.as<uint32_t>(),
                           d_eang.as<float>(), (uint32_t)(edges.size() / 3) };
     SVF_CUDA(svf::launch_ndf_operator(il, mesh, d_dirs.as<float>(), d_normals.as<float>(), t.ndf_scale,
                                       d_ltri.as<int32_t>(), d_lbary.as<float>(), ctx->stream));
-    // its BF16 hi/lo split for the tensor-core GEMM
-    const uint64_t op_elems = (uint64_t)il.ndf_rows_pad * il.k_pad;
-    SVF_TRY(dd->op_hi.ensure(2 * op_elems));
-    SVF_TRY(dd->op_lo.ensure(2 * op_elems));
-    SVF_CUDA(svf::launch_split_bf16(il.ndf_op, op_elems, dd->op_hi.p, dd->op_lo.p, ctx->stream));
-    il.ndf_op_hi = dd->op_hi.p;
-    il.ndf_op_lo = dd->op_lo.p;
+    // its non-empty 256 x 64 tiles (columns in half-vector order), packed as the
+    // BF16 hi/lo split for the tensor-core GEMM
+    std::vector<uint32_t> col_of;
+    std::vector<uint16_t> col_pos;
+    half_vector_order(lay->lp, L, col_of, col_pos);
+    SVF_TRY(upload(dd->col_of, col_of));
+    SVF_TRY(upload(dd->col_pos, col_pos));
+    il.col_of = dd->col_of.as<uint32_t>();
+    il.col_pos = dd->col_pos.as<uint16_t>();
+    const uint32_t ktiles = (N + 63) / 64, ntiles = il.ndf_rows_pad / 256;
+    DevBuf d_flags;
+    SVF_TRY(d_flags.ensure(sizeof(uint32_t) * ktiles * ntiles));
+    SVF_CUDA(svf::launch_ndf_tile_flags(il.ndf_op, il.k_pad, il.col_of, N, il.ndf_rows_pad, d_flags.as<uint32_t>(),
+                                        ctx->stream));
+    std::vector<uint32_t> flags(ktiles * ntiles);
+    SVF_CUDA(cudaMemcpyAsync(flags.data(), d_flags.p, sizeof(uint32_t) * flags.size(), cudaMemcpyDeviceToHost,
+                             ctx->stream));
+    SVF_CUDA(cudaStreamSynchronize(ctx->stream));
+    std::vector<uint32_t> tile_n, tile_kb, tile_start(ntiles + 1, 0);
+    for(uint32_t n = 0; n < ntiles; ++n)
+    {
+        tile_start[n] = (uint32_t)tile_kb.size();
+        for(uint32_t kb = 0; kb < ktiles; ++kb)
+            if(flags[n * ktiles + kb])
+            {
+                tile_n.push_back(n);
+                tile_kb.push_back(kb);
+            }
+    }
+    tile_start[ntiles] = (uint32_t)tile_kb.size();
+    il.packed_tiles = (uint32_t)tile_kb.size();
+    if(il.packed_tiles == 0)
+    {
+        // an operator without a non-zero: one zero tile that no row tile lists
+        tile_n.push_back(0);
+        tile_kb.push_back(0);
+    }
+    const uint32_t alloc_tiles = (uint32_t)tile_kb.size();
+    DevBuf d_tile_n;
+    SVF_TRY(upload(d_tile_n, tile_n));
+    SVF_TRY(upload(dd->tile_kb, tile_kb));
+    SVF_TRY(upload(dd->tile_start, tile_start));
+    SVF_TRY(dd->tile_hi.ensure(sizeof(uint16_t) * 256 * 64 * (size_t)alloc_tiles));
+    SVF_TRY(dd->tile_lo.ensure(sizeof(uint16_t) * 256 * 64 * (size_t)alloc_tiles));
+    if(il.packed_tiles == 0)
+    {
+        SVF_CUDA(cudaMemsetAsync(dd->tile_hi.p, 0, sizeof(uint16_t) * 256 * 64, ctx->stream));
+        SVF_CUDA(cudaMemsetAsync(dd->tile_lo.p, 0, sizeof(uint16_t) * 256 * 64, ctx->stream));
+    }
+    else
+        SVF_CUDA(svf::launch_ndf_tile_pack(il.ndf_op, il.k_pad, il.col_of, N, d_tile_n.as<uint32_t>(),
+                                           dd->tile_kb.as<uint32_t>(), il.packed_tiles, dd->tile_hi.p, dd->tile_lo.p,
+                                           ctx->stream));
+    il.packed_tiles = alloc_tiles;
+    il.tile_hi = dd->tile_hi.p;
+    il.tile_lo = dd->tile_lo.p;
+    il.tile_kb = dd->tile_kb.as<uint32_t>();
+    il.tile_start = dd->tile_start.as<uint32_t>();
+    if(getenv("SVF_DEBUG"))
+        fprintf(stderr, "svf: NDF operator L=%u: %u of %u tiles non-empty (%.1f%%)\n", L, tile_start[ntiles],
+                ktiles * ntiles, 100.0 * tile_start[ntiles] / (ktiles * ntiles));
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));
     *out = &dd->init;
     lay->inits.emplace(key, std::move(data));
     return SVF_OK;
+}
+
+// The NDF rows of `texels` luminance splits (columns in the operator's order) on
+// the tensor cores, over the operator's non-empty tiles.
+cudaError_t launch_ndf(const svf::InitLayout& il, const void* a_hi, const void* a_lo, uint64_t texels, uint64_t lda,
+                       float* C, uint32_t ldc, uint32_t* error_flag, cudaStream_t stream)
+{
+    return svf::launch_ndf_tc_tiles(a_hi, a_lo, texels, lda, il.tile_hi, il.tile_lo, il.ndf_rows_pad, il.k_pad, il.N,
+                                    C, ldc, error_flag, stream, il.tile_kb, il.tile_start, il.packed_tiles);
 }
 
 // Copies `bytes` from src (host or device) to the device buffer dst.
@@ -740,6 +869,10 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
 {
     if(lay->tuned)
         return SVF_OK;
+    // the plain passes only: the packed pass (one 256-thread CTA per SM at its
+    // register count) wins on this short probe but loses on full launches
+    // (measured: 59.4 against 52.2 ms for 160000 ring-81 texels), so it is left
+    // to SVF_LM_KERNEL
     svf::LmKernelChoice cand[4];
     const int n_cand = svf::lm_candidates(lay->L, cand, 4);
     lay->choice = cand[0];
@@ -765,7 +898,7 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
     SVF_CUDA(svf::launch_synth(0x5EEDu, 1, d_lp.as<float>(), L, 0, T, SVF_SAMPLES_F32, 0.01f, samples.p,
                                truth.as<float>(), ctx->stream));
     SVF_CUDA(svf::launch_luminance(samples.p, SVF_SAMPLES_F32, T, N, lum.as<float>(), stride, avg.as<float>(),
-                                   nullptr, nullptr, ctx->stream));
+                                   nullptr, nullptr, nullptr, ctx->stream));
     std::vector<float> tr(16 * T), in(7 * T);
     SVF_CUDA(cudaMemcpyAsync(tr.data(), truth.p, sizeof(float) * 16 * T, cudaMemcpyDeviceToHost, ctx->stream));
     SVF_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -822,8 +955,8 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
             flops += (double)N * (169.0 * s.jacobians + 33.0 * s.residuals);
         const double rate = flops / std::max(1e-3, (double)ms);
         if(getenv("SVF_DEBUG"))
-            fprintf(stderr, "svf: LM tune L=%u threads=%d slots=%d: %.3f ms, %.2f TFLOP/s (model)\n", L,
-                    cand[c].threads, cand[c].slots, ms, rate * 1e-9);
+            fprintf(stderr, "svf: LM tune L=%u threads=%d slots=%d packed=%d: %.3f ms, %.2f TFLOP/s (model)\n", L,
+                    cand[c].threads, cand[c].slots, cand[c].packed, ms, rate * 1e-9);
         if(c == 0)
             first_rate = rate;
         if(rate > best_rate)
@@ -844,6 +977,21 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
 // first that fits for the RGB fit (its slabs differ from the probe's).
 svf::LmKernelChoice lm_choice(Layout* lay, uint64_t stride, bool rgb)
 {
+    // SVF_LM_KERNEL=threads,slots,packed pins one candidate of svf::lm_candidates
+    // (for tests and measurements); others are ignored
+    if(const char* e = std::getenv("SVF_LM_KERNEL"))
+    {
+        svf::LmKernelChoice c{ 0, 0, 0 };
+        if(std::sscanf(e, "%d,%d,%d", &c.threads, &c.slots, &c.packed) == 3)
+        {
+            svf::LmKernelChoice cand[8];
+            const int n = svf::lm_candidates(lay->L, cand, 8);
+            for(int i = 0; i < n; ++i)
+                if(cand[i].threads == c.threads && cand[i].slots == c.slots && cand[i].packed == c.packed &&
+                   svf::lm_max_ctas_per_sm(lay->L, stride, c, rgb) > 0)
+                    return c;
+        }
+    }
     if(rgb)
         return svf::lm_default_choice(lay->L, stride, true);
     return lay->tuned ? lay->choice : svf::lm_default_choice(lay->L, stride);
@@ -851,7 +999,7 @@ svf::LmKernelChoice lm_choice(Layout* lay, uint64_t stride, bool rgb)
 
 svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r)
 {
-    if(!r.rgb && !lay->tuned && r.texels >= 4096)
+    if(!r.rgb && !lay->tuned && r.texels >= 4096 && !std::getenv("SVF_LM_KERNEL"))
         SVF_TRY(tune_lm(ctx, lay, o));
     return launch_lm(ctx, lay, o, r, lm_choice(lay, r.stride, r.rgb));
 }
@@ -1384,7 +1532,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         const bool chroma = rgb || maps->diffuse || maps->specular;
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
                                        chroma ? ctx->avg.as<float>() : nullptr, default_init ? ctx->lum_hi.p : nullptr,
-                                       default_init ? ctx->lum_lo.p : nullptr, ctx->stream,
+                                       default_init ? ctx->lum_lo.p : nullptr,
+                                       default_init ? init_lay->col_pos : nullptr, ctx->stream,
                                        rgb ? ctx->rgb16.p : nullptr, stride3,
                                        lum_features(mlp, ctx->mlp_x.as<float>(), true)));
         // the learned guess's inputs, read before the staging buffer is handed back
@@ -1398,10 +1547,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
         SVF_CUDA(mark(ev(c, 3), ctx->stream));
         if(default_init)
         {
-            cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.p, ctx->lum_lo.p, n, stride, init_lay->ndf_op_hi,
-                                               init_lay->ndf_op_lo, init_lay->ndf_rows_pad, init_lay->k_pad, N,
-                                               ctx->ndf.as<float>(), ndf_ld, ctx->error.as<uint32_t>() + 2,
-                                               ctx->stream);
+            cudaError_t e = launch_ndf(*init_lay, ctx->lum_hi.p, ctx->lum_lo.p, n, stride, ctx->ndf.as<float>(),
+                                       ndf_ld, ctx->error.as<uint32_t>() + 2, ctx->stream);
             if(e != cudaSuccess)
                 return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
             SVF_CUDA(mark(ev(c, 7), ctx->stream));
@@ -1464,12 +1611,10 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
                 svf_texel_stats* g_stats = reinterpret_cast<svf_texel_stats*>(g_maps + 12 * (uint64_t)m);
                 SVF_CUDA(svf::launch_gather_slabs(ctx->lum.as<float>(), stride, chroma ? ctx->avg.as<float>() : nullptr,
                                                   idx, m, ctx->fb_lum.as<float>(), g_avg, ctx->stream));
-                SVF_CUDA(svf::launch_split_bf16(ctx->fb_lum.as<float>(), stride * m, ctx->fb_hi.p, ctx->fb_lo.p,
-                                                ctx->stream));
-                cudaError_t e = svf::launch_ndf_tc(ctx->fb_hi.p, ctx->fb_lo.p, m, stride, init_lay->ndf_op_hi,
-                                                   init_lay->ndf_op_lo, init_lay->ndf_rows_pad, init_lay->k_pad, N,
-                                                   ctx->fb_ndf.as<float>(), fb_ld, ctx->error.as<uint32_t>() + 2,
-                                                   ctx->stream);
+                SVF_CUDA(svf::launch_split_bf16_permuted(ctx->fb_lum.as<float>(), m, stride, N, init_lay->col_of,
+                                                         ctx->fb_hi.p, ctx->fb_lo.p, ctx->stream));
+                cudaError_t e = launch_ndf(*init_lay, ctx->fb_hi.p, ctx->fb_lo.p, m, stride, ctx->fb_ndf.as<float>(),
+                                           fb_ld, ctx->error.as<uint32_t>() + 2, ctx->stream);
                 if(e != cudaSuccess)
                     return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
                 SVF_CUDA(svf::launch_init_finish(*init_lay, ctx->fb_ndf.as<float>(), fb_ld, m, g_init, nullptr,
@@ -1868,15 +2013,15 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                                            chroma ? ctx->avg.as<float>() + 3 * p.k0 : nullptr,
                                            x.default_init ? ctx->lum_hi.as<uint16_t>() + p.off : nullptr,
                                            x.default_init ? ctx->lum_lo.as<uint16_t>() + p.off : nullptr,
+                                           x.default_init ? x.init->col_pos : nullptr,
                                            ctx->stream, rgb ? ctx->rgb16.as<uint16_t>() + p.off3 : nullptr,
                                            x.stride3, lum_features(x.mlp, ctx->mlp_x.as<float>(), true)));
             if(x.default_init)
             {
-                cudaError_t e = svf::launch_ndf_tc(ctx->lum_hi.as<uint16_t>() + p.off, ctx->lum_lo.as<uint16_t>() + p.off,
-                                                   p.count, x.stride, x.init->ndf_op_hi, x.init->ndf_op_lo,
-                                                   x.init->ndf_rows_pad, x.init->k_pad, N,
-                                                   ctx->ndf.as<float>() + p.k0 * ndf_ld, ndf_ld,
-                                                   ctx->error.as<uint32_t>() + 2, ctx->stream);
+                cudaError_t e = launch_ndf(*x.init, ctx->lum_hi.as<uint16_t>() + p.off,
+                                           ctx->lum_lo.as<uint16_t>() + p.off, p.count, x.stride,
+                                           ctx->ndf.as<float>() + p.k0 * ndf_ld, ndf_ld,
+                                           ctx->error.as<uint32_t>() + 2, ctx->stream);
                 if(e != cudaSuccess)
                     return fail(SVF_ECUDA, "NDF GEMM launch: %s", cudaGetErrorString(e));
                 SVF_CUDA(svf::launch_init_finish(*x.init, ctx->ndf.as<float>() + p.k0 * ndf_ld, ndf_ld, p.count,
@@ -2247,7 +2392,7 @@ svf_status svf_mlp_train(svf_ctx* ctx, const float* lp, uint32_t L, const svf_ml
             return st;
         float* Xc = X.as<float>() + (size_t)kMlpInputs * c0;
         SVF_CUDA(launch_luminance(samples.p, SVF_SAMPLES_F32, n, N, lum.as<float>(), stride, nullptr, nullptr,
-                                  nullptr, ctx->stream, nullptr, 0, lum_features(mlp.get(), Xc, false)));
+                                  nullptr, nullptr, ctx->stream, nullptr, 0, lum_features(mlp.get(), Xc, false)));
         SVF_CUDA(rgb_features(mlp.get(), samples.p, SVF_SAMPLES_F32, N, n, Xc, false, ctx->stream));
         SVF_CUDA(mlp_targets(params.as<float>(), n, Y.as<float>() + (size_t)kMlpOutputs * c0, ctx->stream));
     }
@@ -2386,7 +2531,7 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
             SVF_CUDA(cudaMemcpyAsync(staged.p, s, texel_bytes * n, cudaMemcpyHostToDevice, ctx->stream));
             s = staged.p;
         }
-        SVF_CUDA(launch_luminance(s, sample_type, n, N, lum.as<float>(), stride, nullptr, nullptr, nullptr,
+        SVF_CUDA(launch_luminance(s, sample_type, n, N, lum.as<float>(), stride, nullptr, nullptr, nullptr, nullptr,
                                   ctx->stream, nullptr, 0, lum_features(mlp, x.as<float>(), true)));
         SVF_CUDA(rgb_features(mlp, s, sample_type, N, n, x.as<float>(), true, ctx->stream));
         SVF_TRY(mlp_infer(ctx, mlp, x.as<float>(), n, h1.as<float>(), h2.as<float>(), y.as<float>()));
@@ -3001,7 +3146,7 @@ svf_status svf_refit_neighborhood(svf_ctx* ctx, const svf_btf_view* btf, const s
             samples = stage.p;
         }
         SVF_CUDA(svf::launch_luminance(samples, btf->sample_type, n, N, ctx->lum.as<float>(), stride,
-                                       ctx->avg.as<float>(), nullptr, nullptr, ctx->stream));
+                                       ctx->avg.as<float>(), nullptr, nullptr, nullptr, ctx->stream));
         SVF_CUDA(svf::launch_refit_gather(d_params, c0, n, W, H, c_init, ctx->stream));
         // nine candidate fits per texel in one launch: segment k holds candidate k
         // of every texel, all reading the texels' own slabs

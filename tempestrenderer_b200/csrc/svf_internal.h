@@ -70,6 +70,7 @@ struct LmKernelChoice
 {
     int threads;
     int slots;
+    int packed;   // the pair pass in paired FP32 instructions (luminance fit, no Fresnel factor)
 };
 LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb = false);
 int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);
@@ -88,7 +89,8 @@ cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, con
 // Luminance slice + average chromaticity (BTFParallelExtractLuminanceSlice,
 // src/image/btf.cc:1078-1116) for texels [0, texels) of an RGB sample array.
 // lum_hi/lum_lo (optional, both or neither): the BF16 split of the slice for the
-// NDF GEMM, same row pitch, columns [0, N) written.
+// NDF GEMM, same row pitch (a multiple of 8), pair k at column hilo_pos[k] (the
+// operator's column order), columns [N, lum_stride) zero.
 // rgb16 (optional): the samples again as FP16 RGB slabs [texels][rgb_stride]
 // for the RGB fit (rgb_stride >= 3 N, a multiple of 8).
 // The learned guess's half-vector-bin features, computed by the luminance pass
@@ -112,7 +114,8 @@ struct LumFeatures
 // learned guess's features.
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N,
                              float* lum, uint64_t lum_stride, float* avg_chroma, void* lum_hi, void* lum_lo,
-                             cudaStream_t stream, void* rgb16 = nullptr, uint64_t rgb_stride = 0,
+                             const uint16_t* hilo_pos, cudaStream_t stream, void* rgb16 = nullptr,
+                             uint64_t rgb_stride = 0,
                              const LumFeatures& features = LumFeatures{});
 
 // The RGB fit's initial parameters {kd rgb, ks rgb, sx, sy, quaternion xyzw}
@@ -149,9 +152,19 @@ struct InitLayout
     uint32_t ndf_rows;         // NDF texels inside the hemisphere (rows of the operator)
     uint32_t ndf_rows_pad;     // rows padded to a multiple of 256 (the GEMM's N tile)
     float*    ndf_op;          // [ndf_rows_pad][k_pad] NDF = op * lum (row-major, FP32)
-    void*     ndf_op_hi;       // [ndf_rows_pad][k_pad] BF16 hi/lo split of ndf_op
-    void*     ndf_op_lo;
-    int32_t*  ndf_row_texel;   // [ndf_rows] NDF texel index of each operator row
+    int32_t*  ndf_row_texel;   // [ndf_rows] NDF texel index of each operator row (rows in Morton order
+                               // of their texel, so that a 256-row tile is a compact block of the NDF)
+    // The GEMM runs over the operator's non-empty tiles only.  Its columns (the
+    // luminance pairs) are taken in Morton order of the pair's half vector, so
+    // that a 64-column K-block reaches few NDF rows; the luminance pass writes the
+    // BF16 split in that order.
+    uint16_t* col_pos;         // [N] position of pair k in the permuted order
+    uint32_t* col_of;          // [N] pair at permuted position p
+    uint32_t  packed_tiles;    // non-empty 256 x 64 operator tiles
+    void*     tile_hi;         // [packed_tiles][256][64] BF16 hi/lo split of them
+    void*     tile_lo;
+    uint32_t* tile_kb;         // [packed_tiles] K-block of each, grouped by row tile
+    uint32_t* tile_start;      // [ndf_rows_pad / 256 + 1] each row tile's range in them
     float*    denom_w;         // [4096] ndf_denom = denom_w . NDF
     // PCA search samples, grouped by the bilinear cell they fall in
     uint32_t  pca_cells;       // cells that hold samples
@@ -188,9 +201,25 @@ cudaError_t launch_ndf_operator(const InitLayout& lay, const MeshDevice& mesh, c
 // columns of each are used.
 size_t      ndf_tc_smem_bytes();
 cudaError_t launch_split_bf16(const float* x, uint64_t n, void* hi, void* lo, cudaStream_t stream);
+// hi/lo[t][p] = BF16 split of x[t][col_of[p]] (p < N; 0 up to stride).
+cudaError_t launch_split_bf16_permuted(const float* x, uint64_t rows, uint64_t stride, uint32_t N,
+                                       const uint32_t* col_of, void* hi, void* lo, cudaStream_t stream);
+// flags[n][kb]: the operator tile (row tile n, K-block kb of the permuted columns) is non-empty.
+cudaError_t launch_ndf_tile_flags(const float* op, uint32_t k_pad, const uint32_t* col_of, uint32_t N,
+                                  uint32_t rows_pad, uint32_t* flags, cudaStream_t stream);
+// Packs the listed tiles (tile_n[j], tile_kb[j]) as BF16 hi/lo [packed_tiles][256][64].
+cudaError_t launch_ndf_tile_pack(const float* op, uint32_t k_pad, const uint32_t* col_of, uint32_t N,
+                                 const uint32_t* tile_n, const uint32_t* tile_kb, uint32_t packed_tiles, void* hi,
+                                 void* lo, cudaStream_t stream);
 cudaError_t launch_ndf_tc(const void* a_hi, const void* a_lo, uint64_t texels, uint64_t lda, const void* b_hi,
                           const void* b_lo, uint32_t rows_pad, uint64_t ldb, uint32_t k, float* C, uint32_t ldc,
                           uint32_t* error_flag, cudaStream_t stream);
+// The GEMM over the packed operator tiles (tile_kb/tile_start non-null): row
+// tile n multiplies only its K-blocks; b_hi/b_lo are the packed tiles.
+cudaError_t launch_ndf_tc_tiles(const void* a_hi, const void* a_lo, uint64_t texels, uint64_t lda, const void* b_hi,
+                                const void* b_lo, uint32_t rows_pad, uint64_t ldb, uint32_t k, float* C, uint32_t ldc,
+                                uint32_t* error_flag, cudaStream_t stream, const uint32_t* tile_kb,
+                                const uint32_t* tile_start, uint32_t packed_tiles);
 // ndf_rows: [texels][ldr] operator-row NDF values.  init_info (optional):
 // [texels][8] = ndf_denom, normal xyz, tangent xyz, pca value; ndf_out
 // (optional): [texels][4096] NDF textures.

@@ -79,9 +79,15 @@ struct LumPass
 {
     static constexpr bool kStaged = sizeof(T) == 2 && !kFeat;
     static constexpr uint32_t kChunkBytes = kLumChunk * 3 * sizeof(T) + 16;   // + the alignment offset
-    static size_t smem(uint32_t N)
+    __host__ __device__ static size_t smem(uint32_t N)
     {
         return kStaged ? 2 * (size_t)kChunkBytes : (kFeat ? sizeof(float) * N : 0);
+    }
+    // with the BF16 split: its hi and lo rows after the above, 16-byte aligned
+    __host__ __device__ static size_t split_offset(uint32_t N) { return (smem(N) + 15) & ~size_t(15); }
+    static size_t smem(uint32_t N, uint64_t lum_stride, bool hilo)
+    {
+        return hilo ? split_offset(N) + 2 * sizeof(__nv_bfloat16) * lum_stride : smem(N);
     }
 };
 
@@ -122,7 +128,7 @@ __device__ __forceinline__ void stage_bytes(const char* g0, const char* g1, unsi
 template <bool kHiLo, bool kRgb, bool kFeat, bool kChroma>
 __device__ __forceinline__ void lum_pair(uint32_t i, float r, float g, float b, uint32_t ypos, uint64_t t,
                                          float* dst, float* y, __half* rgb16, uint64_t rgb_stride,
-                                         __nv_bfloat16* lum_hi, __nv_bfloat16* lum_lo, uint64_t lum_stride,
+                                         __nv_bfloat16* sh_hi, __nv_bfloat16* sh_lo, const uint16_t* hilo_pos,
                                          float& ax, float& ay, float& az)
 {
     const float l = __fadd_rn(__fadd_rn(__fmul_rn(0.2126f, r), __fmul_rn(0.7152f, g)), __fmul_rn(0.0722f, b));
@@ -139,10 +145,12 @@ __device__ __forceinline__ void lum_pair(uint32_t i, float r, float g, float b, 
     }
     if constexpr(kHiLo)
     {
-        // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM
+        // x = hi + lo to 16 significant bits, for the BF16x3 NDF GEMM, at the
+        // pair's column of the operator (shared memory; written out at the end)
         const __nv_bfloat16 h = __float2bfloat16_rn(l);
-        lum_hi[t * lum_stride + i] = h;
-        lum_lo[t * lum_stride + i] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
+        const uint32_t p = __ldg(hilo_pos + i);
+        sh_hi[p] = h;
+        sh_lo[p] = __float2bfloat16_rn(__fsub_rn(l, __bfloat162float(h)));
     }
     if constexpr(kChroma)
     {
@@ -176,6 +184,7 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
                                                                 float* __restrict__ avg,
                                                                 __nv_bfloat16* __restrict__ lum_hi,
                                                                 __nv_bfloat16* __restrict__ lum_lo,
+                                                                const uint16_t* __restrict__ hilo_pos,
                                                                 __half* __restrict__ rgb16, uint64_t rgb_stride,
                                                                 LumFeatures feat)
 {
@@ -190,6 +199,8 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
     const T* src = samples + t * (uint64_t)N * 3;
     float* dst = lum + t * lum_stride;
     float ax = 0.0f, ay = 0.0f, az = 0.0f;
+    __nv_bfloat16* sh_hi = reinterpret_cast<__nv_bfloat16*>(smem + S::split_offset(N));
+    __nv_bfloat16* sh_lo = sh_hi + lum_stride;
     if constexpr(S::kStaged)
     {
         const char* bytes = reinterpret_cast<const char*>(src);
@@ -218,8 +229,8 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
 #pragma unroll 4
             for(uint32_t k = threadIdx.x; k < pn; k += kLumThreads)
                 lum_pair<kHiLo, kRgb, kFeat, kChroma>(p0 + k, to_f(cs[3 * k]), to_f(cs[3 * k + 1]),
-                                                      to_f(cs[3 * k + 2]), 0, t, dst, y, rgb16, rgb_stride, lum_hi,
-                                                      lum_lo, lum_stride, ax, ay, az);
+                                                      to_f(cs[3 * k + 2]), 0, t, dst, y, rgb16, rgb_stride, sh_hi,
+                                                      sh_lo, hilo_pos, ax, ay, az);
             __syncthreads();   // the buffer is refilled two chunks on
         }
     }
@@ -251,7 +262,7 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
                 if(i >= N)
                     break;
                 lum_pair<kHiLo, kRgb, kFeat, kChroma>(i, rr[u], gg[u], bb[u], pp[u], t, dst, y, rgb16, rgb_stride,
-                                                      lum_hi, lum_lo, lum_stride, ax, ay, az);
+                                                      sh_hi, sh_lo, hilo_pos, ax, ay, az);
             }
         }
         if constexpr(kFeat)
@@ -259,6 +270,22 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
     }
     for(uint32_t i = N + threadIdx.x; i < lum_stride; i += blockDim.x)
         dst[i] = 0.0f;
+    if constexpr(kHiLo)
+    {
+        // the split rows, in the operator's column order, out in 16-byte words
+        for(uint32_t i = N + threadIdx.x; i < lum_stride; i += blockDim.x)
+            sh_hi[i] = sh_lo[i] = __float2bfloat16_rn(0.0f);
+        __syncthreads();
+        const uint4* sh4 = reinterpret_cast<const uint4*>(sh_hi);
+        const uint32_t words = (uint32_t)(lum_stride / 8);
+        uint4* gh = reinterpret_cast<uint4*>(lum_hi + t * lum_stride);
+        uint4* gl = reinterpret_cast<uint4*>(lum_lo + t * lum_stride);
+        for(uint32_t w = threadIdx.x; w < words; w += blockDim.x)
+        {
+            gh[w] = sh4[w];
+            gl[w] = sh4[words + w];
+        }
+    }
     if constexpr(kChroma)
     {
         __shared__ float red[3][8];
@@ -684,12 +711,16 @@ auto luminance_kernel_of(int flags, const T*)
 } // namespace
 
 cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t texels, uint32_t N, float* lum,
-                             uint64_t lum_stride, float* avg, void* lum_hi, void* lum_lo, cudaStream_t stream,
-                             void* rgb16, uint64_t rgb_stride, const LumFeatures& features)
+                             uint64_t lum_stride, float* avg, void* lum_hi, void* lum_lo, const uint16_t* hilo_pos,
+                             cudaStream_t stream, void* rgb16, uint64_t rgb_stride, const LumFeatures& features)
 {
     if(texels == 0)
         return cudaSuccess;
     if((lum_hi == nullptr) != (lum_lo == nullptr) || texels > 0x7fffffffull)
+        return cudaErrorInvalidValue;
+    // the split: a column table, 16-byte rows and bases
+    if(lum_hi && (!hilo_pos || lum_stride % 8 != 0 || (reinterpret_cast<uintptr_t>(lum_hi) & 15u) ||
+                  (reinterpret_cast<uintptr_t>(lum_lo) & 15u)))
         return cudaErrorInvalidValue;
     if(features.X && !(features.pos && features.start && features.bin_w && features.pair_pos &&
                        (features.mean == nullptr) == (features.rstd == nullptr) && N <= 65536u))
@@ -698,14 +729,16 @@ cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t
     __nv_bfloat16* lo = static_cast<__nv_bfloat16*>(lum_lo);
     const auto run = [&](auto kernel, const auto* src) -> cudaError_t {
         using T = std::remove_cv_t<std::remove_pointer_t<decltype(src)>>;
-        const size_t smem = features.X ? LumPass<T, true>::smem(N) : LumPass<T, false>::smem(N);
+        const bool hl = hi != nullptr;
+        const size_t smem = features.X ? LumPass<T, true>::smem(N, lum_stride, hl)
+                                       : LumPass<T, false>::smem(N, lum_stride, hl);
         if(smem > 48 * 1024)
         {
             const cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
             if(e != cudaSuccess)
                 return e;
         }
-        kernel<<<(unsigned)texels, kLumThreads, smem, stream>>>(src, N, lum, lum_stride, avg, hi, lo,
+        kernel<<<(unsigned)texels, kLumThreads, smem, stream>>>(src, N, lum, lum_stride, avg, hi, lo, hilo_pos,
                                                                 static_cast<__half*>(rgb16), rgb_stride, features);
         return cudaGetLastError();
     };

@@ -669,6 +669,161 @@ __device__ __forceinline__ void sym_pair(const PassConst& c, const Entry& ea, co
     }
 }
 
+// ------------------------------------------------------------------------------
+// packed pair evaluation: two unordered pairs per lane, one in each half of the
+// sm_100 paired FP32 instructions (add/mul/fma .f32x2), for the luminance fit
+// without a Fresnel factor.  Arithmetic per pair as in sym_pair; the two halves
+// accumulate separately and are added once at the end of the pass.
+// ------------------------------------------------------------------------------
+
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b)
+{
+    float2 r;
+    asm("{\n\t.reg .b64 x, y, z;\n\tmov.b64 x, {%2, %3};\n\tmov.b64 y, {%4, %5};\n\t"
+        "sub.rn.f32x2 z, x, y;\n\tmov.b64 {%0, %1}, z;\n\t}"
+        : "=f"(r.x), "=f"(r.y)
+        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+    return r;
+}
+
+// Per-pass constants of sym_pair in paired form (both halves equal), with the
+// products that do not depend on the pair folded in.
+struct PassConst2
+{
+    float2 u, v, kd, ks, kd_on, ks_on;
+    float2 k4u, nksrsx, k4v, nksrsy;   // 4 u ks rsx, -ks rsx, 4 v ks rsy, -ks rsy
+    float2 c[9];                       // -4 ks om[3k+j] x {v - 1, 1 - u, u - v}[j]
+};
+
+__device__ __forceinline__ PassConst2 make_pass_const2(const PassConst& c)
+{
+    PassConst2 p;
+    p.u = f2(c.u);
+    p.v = f2(c.v);
+    p.kd = f2(c.kd);
+    p.ks = f2(c.ks);
+    p.kd_on = f2(c.kd_on);
+    p.ks_on = f2(c.ks_on);
+    p.k4u = f2(4.0f * c.u * c.ks * c.rsx);
+    p.nksrsx = f2(-(c.ks * c.rsx));
+    p.k4v = f2(4.0f * c.v * c.ks * c.rsy);
+    p.nksrsy = f2(-(c.ks * c.rsy));
+    const float tf[3] = { c.v - 1.0f, 1.0f - c.u, c.u - c.v };
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+#pragma unroll
+        for(int j = 0; j < 3; ++j)
+            p.c[3 * k + j] = f2(-4.0f * c.ks * c.om[3 * k + j] * tf[j]);
+    return p;
+}
+
+// Two unordered pairs {a, b} (x half) and {a', b'} (y half).  ea/eb: their
+// entries; y1/y2: the samples of the ordered pairs (view a, light b) and
+// (view b, light a); wt1/wt2: their weights (0 for a guarded slot or the
+// diagonal's second pair).  acc: 35 paired sums (the upper J^T J and J^T r).
+template <bool kAllUp>
+__device__ __forceinline__ void sym_pair2(const PassConst2& c, const Entry& eaA, const Entry& ebA, const Entry& eaB,
+                                          const Entry& ebB, float2 y1, float2 y2, float2 wt1, float2 wt2, float2* acc,
+                                          double& r2)
+{
+    const float2 s0 = make_float2(eaA.a0 + ebA.a0, eaB.a0 + ebB.a0);
+    const float2 s1 = make_float2(eaA.a1 + ebA.a1, eaB.a1 + ebB.a1);
+    const float2 s2 = make_float2(eaA.a2 + ebA.a2, eaB.a2 + ebB.a2);
+    const float2 S = make_float2(eaA.sp + ebA.sp, eaB.sp + ebB.sp);
+    const float2 q0 = mul2(s0, s0), q1 = mul2(s1, s1), q2 = mul2(s2, s2);
+    const float2 g = add2(add2(q0, q1), q2);
+    const float2 Q = fma2(c.u, q0, fma2(c.v, q1, q2));
+    const float2 QQ = mul2(Q, Q);
+    const float2 QQS = mul2(QQ, S);
+    const float2 rden = make_float2(QQS.x > 1e-37f ? rcp_approx(QQS.x) : 0.0f, QQS.y > 1e-37f ? rcp_approx(QQS.y) : 0.0f);
+    const float2 C = mul2(mul2(g, g), rden);
+    const float2 kv1 = make_float2(eaA.kv, eaB.kv), kv2 = make_float2(ebA.kv, ebB.kv);
+    const float2 kdc1 = make_float2(ebA.kdc, ebB.kdc), kdc2 = make_float2(eaA.kdc, eaB.kdc);
+    float2 w1, w2, h1, h2;
+    if(kAllUp)
+    {
+        w1 = mul2(wt1, kv1);
+        w2 = mul2(wt2, kv2);
+        h1 = mul2(wt1, kdc1);
+        h2 = mul2(wt2, kdc2);
+    }
+    else
+    {
+        const float2 upa = make_float2(eaA.up, eaB.up), upb = make_float2(ebA.up, ebB.up);
+        w1 = mul2(mul2(wt1, kv1), upb);
+        w2 = mul2(mul2(wt2, kv2), upa);
+        h1 = mul2(mul2(wt1, upa), kdc1);
+        h2 = mul2(mul2(wt2, upb), kdc2);
+    }
+    const float2 sp1 = mul2(w1, C), sp2 = mul2(w2, C);
+    const float2 r1 = sub2(y1, fma2(c.kd, h1, mul2(c.ks, sp1)));
+    const float2 rb = sub2(y2, fma2(c.kd, h2, mul2(c.ks, sp2)));
+    r2 = fma((double)r1.x, (double)r1.x, r2);
+    r2 = fma((double)rb.x, (double)rb.x, r2);
+    r2 = fma((double)r1.y, (double)r1.y, r2);
+    r2 = fma((double)rb.y, (double)rb.y, r2);
+    const float2 rQ = mul2(mul2(Q, S), rden);   // 1/Q
+    const float2 rSk = mul2(mul2(QQ, rden), c.ks);   // ks/S
+    const float2 p12 = mul2(s1, s2), p02 = mul2(s0, s2), p01 = mul2(s0, s1);
+    float2 V[kParams];
+    {
+        const float2 nd0 = make_float2(-(eaA.d0 + ebA.d0), -(eaB.d0 + ebB.d0));
+        const float2 nd1 = make_float2(-(eaA.d1 + ebA.d1), -(eaB.d1 + ebB.d1));
+        V[0] = fma2(nd0, rSk, fma2(c.k4u, mul2(q0, rQ), c.nksrsx));
+        V[1] = fma2(nd1, rSk, fma2(c.k4v, mul2(q1, rQ), c.nksrsy));
+    }
+    V[2] = c.ks_on;
+    V[3] = f2(0.0f);
+    {
+        const float2 nd[3] = { make_float2(-(eaA.d2 + ebA.d2), -(eaB.d2 + ebB.d2)),
+                               make_float2(-(eaA.d3 + ebA.d3), -(eaB.d3 + ebB.d3)),
+                               make_float2(-(eaA.d4 + ebA.d4), -(eaB.d4 + ebB.d4)) };
+#pragma unroll
+        for(int k = 0; k < 3; ++k)
+        {
+            const float2 dq = fma2(c.c[3 * k], p12, fma2(c.c[3 * k + 1], p02, mul2(c.c[3 * k + 2], p01)));
+            V[4 + k] = fma2(rQ, dq, mul2(nd[k], rSk));
+        }
+    }
+    const float2 P = fma2(sp1, sp1, mul2(sp2, sp2));
+    const float2 X = mul2(c.kd_on, fma2(sp1, h1, mul2(sp2, h2)));
+    const float2 Z = mul2(c.kd_on, fma2(h1, h1, mul2(h2, h2)));
+    const float2 R = fma2(sp1, r1, mul2(sp2, rb));
+    const float2 U = mul2(c.kd_on, fma2(h1, r1, mul2(h2, rb)));
+    float2 PV[kParams];
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+        PV[i] = mul2(P, V[i]);
+    int n = 0;
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+#pragma unroll
+        for(int j = i; j < kParams; ++j)
+        {
+            if(i == 3 && j == 3)
+                acc[n] = add2(acc[n], Z);
+            else if(i == 3)
+                acc[n] = fma2(X, V[j], acc[n]);
+            else if(j == 3)
+                acc[n] = fma2(X, V[i], acc[n]);
+            else
+                acc[n] = fma2(PV[i], V[j], acc[n]);
+            ++n;
+        }
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+    {
+        if(i == 3)
+            acc[kHessian + i] = add2(acc[kHessian + i], U);
+        else
+            acc[kHessian + i] = fma2(R, V[i], acc[kHessian + i]);
+    }
+}
+
 // The RGB pair: the geometry of sym_pair, three channels.  Per ordered pair k
 // and channel c:  f_kc = kd_c h_k + ks_c sp_k,  r_kc = y_kc - f_kc, and
 //   J_kc = kd_on_c h_k e_kd_c + ks_on_c sp_k e_ks_c + ks_c sp_k sum_j G_j e_j
@@ -840,6 +995,111 @@ __device__ void worker_pass(const float* tab, const PassConst& c, const typename
     for(uint32_t it = full; it < iters; ++it)
         pair_step<M, NW, kFresnel, kAllUp, true>(tab, c, slab, L, Lp, nd, total, sa, sd, refr, f, a, d, acc, r2);
 
+    r2 = warp_sum(r2);
+    {
+        float rest[kAcc - 32];
+#pragma unroll
+        for(int i = 32; i < kAcc; ++i)
+            rest[i - 32] = warp_sum(acc[i]);
+        reduce_scatter32(acc, lane);
+        red[wwarp * kAcc + lane] = acc[0];
+        if(lane == 0)
+#pragma unroll
+            for(int i = 32; i < kAcc; ++i)
+                red[wwarp * kAcc + i] = rest[i - 32];
+    }
+    if(lane == 0)
+        redd[wwarp] = r2;
+}
+
+// Advances an unordered pair (f, a, d) by one worker stride (sa, sd): f += 32 NW.
+__device__ __forceinline__ void pair_advance(uint32_t stride, uint32_t nd, uint32_t sa, uint32_t sd, uint32_t& f,
+                                             uint32_t& a, uint32_t& d)
+{
+    f += stride;
+    a += sa;
+    d += sd;
+    if(d >= nd)
+    {
+        d -= nd;
+        ++a;
+    }
+}
+
+// Loads one unordered pair's entries and samples (see pair_step).
+template <bool kGuard>
+__device__ __forceinline__ void pair_load(const float* tab, const float* fs, uint32_t L, uint32_t Lp, uint32_t total,
+                                          uint32_t f, uint32_t a, uint32_t d, Entry& ea, Entry& eb, float& y1,
+                                          float& y2, float& wt1, float& wt2)
+{
+    const bool valid = !kGuard || (f < total && !(2u * d == L && a >= (L >> 1)));
+    uint32_t b = a + d;
+    b = b >= L ? b - L : b;
+    const uint32_t ia = valid ? a : 0u, ib = valid ? b : 0u;
+    ea = load_entry(tab, Lp, ia);
+    eb = load_entry(tab, Lp, ib);
+    const bool two = valid && d != 0u;
+    y1 = valid ? fs[ia * L + ib] : 0.0f;
+    y2 = two ? fs[ib * L + ia] : 0.0f;
+    wt1 = kGuard ? (valid ? 1.0f : 0.0f) : 1.0f;
+    wt2 = two ? 1.0f : 0.0f;
+}
+
+// One packed step: the lane's pairs f and f + 32 NW, then f += 64 NW.
+template <int NW, bool kAllUp, bool kGuard>
+__device__ __forceinline__ void pair_step2(const float* tab, const PassConst2& c, const float* fs, uint32_t L, uint32_t Lp,
+                                           uint32_t nd, uint32_t total, uint32_t sa, uint32_t sd, uint32_t& f,
+                                           uint32_t& a, uint32_t& d, float2* acc, double& r2)
+{
+    constexpr uint32_t kStride = 32u * NW;
+    uint32_t fB = f, aB = a, dB = d;
+    pair_advance(kStride, nd, sa, sd, fB, aB, dB);
+    Entry eaA, ebA, eaB, ebB;
+    float yA1, yA2, yB1, yB2, wA1, wA2, wB1, wB2;
+    pair_load<kGuard>(tab, fs, L, Lp, total, f, a, d, eaA, ebA, yA1, yA2, wA1, wA2);
+    pair_load<kGuard>(tab, fs, L, Lp, total, fB, aB, dB, eaB, ebB, yB1, yB2, wB1, wB2);
+    sym_pair2<kAllUp>(c, eaA, ebA, eaB, ebB, make_float2(yA1, yB1), make_float2(yA2, yB2), make_float2(wA1, wB1),
+                      make_float2(wA2, wB2), acc, r2);
+    f = fB;
+    a = aB;
+    d = dB;
+    pair_advance(kStride, nd, sa, sd, f, a, d);
+}
+
+// worker_pass for the luminance fit without a Fresnel factor, two pairs a lane
+// per step in the paired FP32 instructions.  Same enumeration and outputs.
+template <int NW, bool kAllUp>
+__device__ void worker_pass2(const float* tab, const PassConst& c1, const float* slab, uint32_t L, float* red,
+                             double* redd, uint32_t wwarp, uint32_t lane)
+{
+    constexpr int kAcc = LumModel::kAcc;
+    constexpr uint32_t kStride = 32u * NW;
+    const uint32_t half = L >> 1, nd = half + 1, Lp = pad4(L);
+    const uint32_t total = L * nd;
+    const uint32_t iters = (total + kStride - 1) / kStride;
+    const uint32_t full = (L & 1u) ? total / kStride : 0u;   // single steps with every pair valid
+    const uint32_t sa = kStride / nd, sd = kStride - sa * nd;
+    uint32_t f = wwarp * 32u + lane;
+    uint32_t a = f / nd, d = f - a * nd;
+    const PassConst2 c = make_pass_const2(c1);
+
+    double r2 = 0.0;
+    float2 acc2[kAcc];
+#pragma unroll
+    for(int i = 0; i < kAcc; ++i)
+        acc2[i] = f2(0.0f);
+    // double steps: the first full / 2 need no guard, the rest cover the
+    // remaining single steps (a pair past the enumeration gets zero weights)
+    const uint32_t full2 = full / 2u, iters2 = (iters + 1u) / 2u;
+    for(uint32_t it = 0; it < full2; ++it)
+        pair_step2<NW, kAllUp, false>(tab, c, slab, L, Lp, nd, total, sa, sd, f, a, d, acc2, r2);
+    for(uint32_t it = full2; it < iters2; ++it)
+        pair_step2<NW, kAllUp, true>(tab, c, slab, L, Lp, nd, total, sa, sd, f, a, d, acc2, r2);
+
+    float acc[kAcc];
+#pragma unroll
+    for(int i = 0; i < kAcc; ++i)
+        acc[i] = acc2[i].x + acc2[i].y;
     r2 = warp_sum(r2);
     {
         float rest[kAcc - 32];
@@ -1193,9 +1453,10 @@ __device__ void expand_sums(const double* sums, const float* pf, double* hg)
 // Resident CTAs per SM the register budget is sized for.
 constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : 2; }
 
-template <class M, int NW, int S, bool kFresnel, bool kAllUp>
-__global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_fit_kernel(LmArgs args)
+template <class M, int NW, int S, bool kFresnel, bool kAllUp, bool kPacked>
+__global__ void __launch_bounds__(32 * (NW + 1), kPacked ? 1 : min_blocks(32 * (NW + 1))) lm_fit_kernel(LmArgs args)
 {
+    static_assert(!kPacked || (!M::kRgb && !kFresnel), "the packed pass is the luminance fit without Fresnel");
     constexpr uint32_t kThreads = 32 * (NW + 1);
     using SM = SlotSmem<NW, M>;
     using SlabT = typename M::Slab;
@@ -1225,8 +1486,12 @@ __global__ void __launch_bounds__(32 * (NW + 1), min_blocks(32 * (NW + 1))) lm_f
                 break;
             if(cmd == kSlotPass)
             {
-                worker_pass<M, NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), slots[s].L,
-                                                     args.cfg.fresnel, red_of(s), redd_of(s), wwarp, lane);
+                if constexpr(kPacked)
+                    worker_pass2<NW, kAllUp>(tab_of(s), slots[s].pc, reinterpret_cast<const float*>(slab_of(s)),
+                                             slots[s].L, red_of(s), redd_of(s), wwarp, lane);
+                else
+                    worker_pass<M, NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), slots[s].L,
+                                                         args.cfg.fresnel, red_of(s), redd_of(s), wwarp, lane);
                 // the last worker warp to finish sums the partials in FP64, in warp
                 // order (deterministic), while the others move on
                 __syncwarp();
@@ -1395,17 +1660,38 @@ template <class M, int NW, int S>
 KernelFn pick(bool fresnel, bool all_up)
 {
     if(fresnel)
-        return all_up ? lm_fit_kernel<M, NW, S, true, true> : lm_fit_kernel<M, NW, S, true, false>;
-    return all_up ? lm_fit_kernel<M, NW, S, false, true> : lm_fit_kernel<M, NW, S, false, false>;
+        return all_up ? lm_fit_kernel<M, NW, S, true, true, false> : lm_fit_kernel<M, NW, S, true, false, false>;
+    return all_up ? lm_fit_kernel<M, NW, S, false, true, false> : lm_fit_kernel<M, NW, S, false, false, false>;
+}
+
+// The packed instances (luminance, no Fresnel factor).
+template <int NW, int S>
+KernelFn pick_packed(bool all_up)
+{
+    return all_up ? lm_fit_kernel<LumModel, NW, S, false, true, true> : lm_fit_kernel<LumModel, NW, S, false, false, true>;
 }
 
 template <class M>
 KernelFn kernel_for_model(LmKernelChoice c, bool fresnel, bool all_up)
 {
+    if constexpr(!M::kRgb)
+        if(c.packed && !fresnel)
+        {
+            if(c.threads == 256 && c.slots == 3)
+                return pick_packed<7, 3>(all_up);
+            if(c.threads == 256 && c.slots == 4)
+                return pick_packed<7, 4>(all_up);
+            if(c.threads == 128 && c.slots == 3)
+                return pick_packed<3, 3>(all_up);
+            return nullptr;
+        }
+    // (a packed choice runs the plain pass where the packed one does not apply)
     if(c.threads == 256 && c.slots == 2)
         return pick<M, 7, 2>(fresnel, all_up);
     if(c.threads == 256 && c.slots == 3)
         return pick<M, 7, 3>(fresnel, all_up);
+    if(c.threads == 256 && c.slots == 4)
+        return pick<M, 7, 4>(fresnel, all_up);
     if(c.threads == 128 && c.slots == 2)
         return pick<M, 3, 2>(fresnel, all_up);
     if(c.threads == 128 && c.slots == 3)
@@ -1428,7 +1714,7 @@ LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
     // the earlier one), counting a single-slot CTA's at half (its workers wait
     // for the control warp between passes); at large L only fewer slots fit.
     LmKernelChoice cand[5];
-    const int n = lm_candidates(L, cand, 5);
+    const int n = lm_candidates(L, cand, 5);   // the plain passes
     int best = -1, best_w = 0;
     for(int i = 0; i < n; ++i)
     {
@@ -1445,9 +1731,12 @@ LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
 
 int lm_candidates(uint32_t, LmKernelChoice* out, int max)
 {
-    const LmKernelChoice all[5] = { { 256, 3 }, { 256, 2 }, { 128, 3 }, { 128, 2 }, { 256, 1 } };
+    // the plain passes first (the untuned default picks among them), then the
+    // packed ones (one CTA of 256 threads per SM at their register count)
+    const LmKernelChoice all[8] = { { 256, 3, 0 }, { 256, 2, 0 }, { 128, 3, 0 }, { 128, 2, 0 },
+                                    { 256, 1, 0 }, { 256, 3, 1 }, { 256, 4, 1 }, { 128, 3, 1 } };
     int n = 0;
-    for(int i = 0; i < 5 && n < max; ++i)
+    for(int i = 0; i < 8 && n < max; ++i)
         out[n++] = all[i];
     return n;
 }

@@ -134,9 +134,14 @@ struct TcMaps
     CUtensorMap a_hi, a_lo, b_hi, b_lo;
 };
 
+// Dense: every CTA runs the ktiles K-blocks, B tiles at (K-block, n0).  Tile
+// list (tile_kb non-null): the CTA of row tile n runs the K-blocks
+// tile_kb[tile_start[n] .. tile_start[n + 1]), and B is the packed operator
+// whose tile j (256 rows x 64 columns) sits at row 256 j.
 __global__ void __launch_bounds__(128, 1) ndf_tc_kernel(const __grid_constant__ TcMaps maps, uint32_t ktiles,
                                                         uint64_t M, uint32_t ldc, float* __restrict__ C,
-                                                        uint32_t* error_flag)
+                                                        uint32_t* error_flag, const uint32_t* __restrict__ tile_kb,
+                                                        const uint32_t* __restrict__ tile_start)
 {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     // 1024-byte alignment of every operand tile (the swizzle atom)
@@ -150,6 +155,8 @@ __global__ void __launch_bounds__(128, 1) ndf_tc_kernel(const __grid_constant__ 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint64_t m0 = (uint64_t)blockIdx.y * kTileM;
     const uint32_t n0 = blockIdx.x * kTileN;
+    const uint32_t j0 = tile_kb ? tile_start[blockIdx.x] : 0u;
+    const uint32_t nkb = tile_kb ? tile_start[blockIdx.x + 1] - j0 : ktiles;
 
     if(threadIdx.x == 0)
     {
@@ -187,7 +194,7 @@ __global__ void __launch_bounds__(128, 1) ndf_tc_kernel(const __grid_constant__ 
     if(warp == 0 && lane == 0)
     {
         // TMA producer
-        for(uint32_t kb = 0; kb < ktiles; ++kb)
+        for(uint32_t kb = 0; kb < nkb; ++kb)
         {
             const int s = kb % kStages;
             if(kb >= (uint32_t)kStages && !mbar_wait(&empty[s], ((kb / kStages) - 1) & 1u, &abort_flag))
@@ -196,11 +203,14 @@ __global__ void __launch_bounds__(128, 1) ndf_tc_kernel(const __grid_constant__ 
                 break;
             }
             mbar_expect_tx(&full[s], kStageBytes);
-            const int32_t kx = (int32_t)(kb * kBlockK);
+            // A: the K-block's columns; B: the dense operator at (K-block, n0) or packed tile j
+            const int32_t kx = (int32_t)((tile_kb ? tile_kb[j0 + kb] : kb) * kBlockK);
+            const int32_t bx = tile_kb ? 0 : kx;
+            const int32_t by = tile_kb ? (int32_t)((j0 + kb) * kTileN) : (int32_t)n0;
             tma_load_2d(stage_ptr(s, 0), &maps.a_hi, kx, (int32_t)m0, &full[s]);
             tma_load_2d(stage_ptr(s, 1), &maps.a_lo, kx, (int32_t)m0, &full[s]);
-            tma_load_2d(stage_ptr(s, 2), &maps.b_hi, kx, (int32_t)n0, &full[s]);
-            tma_load_2d(stage_ptr(s, 3), &maps.b_lo, kx, (int32_t)n0, &full[s]);
+            tma_load_2d(stage_ptr(s, 2), &maps.b_hi, bx, by, &full[s]);
+            tma_load_2d(stage_ptr(s, 3), &maps.b_lo, bx, by, &full[s]);
             issued = kb + 1;
         }
     }
@@ -208,7 +218,7 @@ __global__ void __launch_bounds__(128, 1) ndf_tc_kernel(const __grid_constant__ 
     {
         // MMA issuer
         uint32_t kb = 0;
-        for(; kb < ktiles; ++kb)
+        for(; kb < nkb; ++kb)
         {
             const int s = kb % kStages;
             if(!mbar_wait(&full[s], (kb / kStages) & 1u, &abort_flag))
@@ -230,7 +240,7 @@ __global__ void __launch_bounds__(128, 1) ndf_tc_kernel(const __grid_constant__ 
             }
             umma_commit(&empty[s]);
         }
-        if(kb == ktiles)
+        if(kb == nkb)
             umma_commit(&done);
     }
     __syncwarp();
@@ -245,7 +255,12 @@ __global__ void __launch_bounds__(128, 1) ndf_tc_kernel(const __grid_constant__ 
         for(int c = 0; c < kTileN; c += 32)
         {
             uint32_t r[32];
-            tmem_ld32(tmem + ((warp * 32u) << 16) + (uint32_t)c, r);
+            if(nkb)
+                tmem_ld32(tmem + ((warp * 32u) << 16) + (uint32_t)c, r);
+            else
+#pragma unroll
+                for(int q = 0; q < 32; ++q)
+                    r[q] = 0u;   // a row tile without K-blocks: its rows are 0
             if(m < M)
             {
                 float4* dst = reinterpret_cast<float4*>(C + m * ldc + n0 + c);
@@ -355,6 +370,15 @@ cudaError_t launch_ndf_tc(const void* a_hi, const void* a_lo, uint64_t texels, u
                           const void* b_lo, uint32_t rows_pad, uint64_t ldb, uint32_t k, float* C, uint32_t ldc,
                           uint32_t* error_flag, cudaStream_t stream)
 {
+    return launch_ndf_tc_tiles(a_hi, a_lo, texels, lda, b_hi, b_lo, rows_pad, ldb, k, C, ldc, error_flag, stream,
+                               nullptr, nullptr, 0);
+}
+
+cudaError_t launch_ndf_tc_tiles(const void* a_hi, const void* a_lo, uint64_t texels, uint64_t lda, const void* b_hi,
+                                const void* b_lo, uint32_t rows_pad, uint64_t ldb, uint32_t k, float* C, uint32_t ldc,
+                                uint32_t* error_flag, cudaStream_t stream, const uint32_t* tile_kb,
+                                const uint32_t* tile_start, uint32_t packed_tiles)
+{
     if(texels == 0)
         return cudaSuccess;
     // TMA: 16-byte aligned bases and row pitches; 16-byte output rows
@@ -363,9 +387,15 @@ cudaError_t launch_ndf_tc(const void* a_hi, const void* a_lo, uint64_t texels, u
        ldc < rows_pad || texels > 65535ull * kTileM || misaligned(a_hi) || misaligned(a_lo) || misaligned(b_hi) ||
        misaligned(b_lo) || misaligned(C))
         return cudaErrorInvalidValue;
+    if((tile_kb == nullptr) != (tile_start == nullptr) || (tile_kb && packed_tiles == 0))
+        return cudaErrorInvalidValue;
     TcMaps maps;
+    // B: the dense operator [rows_pad][k], or the packed tiles [packed_tiles * 256][64]
+    const uint64_t b_rows = tile_kb ? (uint64_t)packed_tiles * kTileN : rows_pad;
+    const uint64_t b_cols = tile_kb ? (uint64_t)kBlockK : k, b_ld = tile_kb ? (uint64_t)kBlockK : ldb;
     if(!make_map(&maps.a_hi, a_hi, texels, k, lda, kTileM) || !make_map(&maps.a_lo, a_lo, texels, k, lda, kTileM) ||
-       !make_map(&maps.b_hi, b_hi, rows_pad, k, ldb, kTileN) || !make_map(&maps.b_lo, b_lo, rows_pad, k, ldb, kTileN))
+       !make_map(&maps.b_hi, b_hi, b_rows, b_cols, b_ld, kTileN) ||
+       !make_map(&maps.b_lo, b_lo, b_rows, b_cols, b_ld, kTileN))
         return cudaErrorInvalidValue;
     const size_t smem = ndf_tc_smem_bytes();
     cudaError_t e = cudaFuncSetAttribute(ndf_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -373,7 +403,106 @@ cudaError_t launch_ndf_tc(const void* a_hi, const void* a_lo, uint64_t texels, u
         return e;
     const uint32_t ktiles = (k + kBlockK - 1) / kBlockK;
     dim3 grid(rows_pad / kTileN, (unsigned)((texels + kTileM - 1) / kTileM));
-    ndf_tc_kernel<<<grid, 128, smem, stream>>>(maps, ktiles, texels, ldc, C, error_flag);
+    ndf_tc_kernel<<<grid, 128, smem, stream>>>(maps, ktiles, texels, ldc, C, error_flag, tile_kb, tile_start);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// the NDF operator's non-empty tiles, packed
+// ---------------------------------------------------------------------------
+
+namespace
+{
+
+// flags[n * ktiles + kb] = 1 when the operator tile of row tile n and K-block kb
+// (columns in the permuted order col_of) holds a non-zero.  One thread a row.
+__global__ void __launch_bounds__(kTileN) tile_flags_kernel(const float* __restrict__ op, uint32_t k_pad,
+                                                             const uint32_t* __restrict__ col_of, uint32_t N,
+                                                             uint32_t ktiles, uint32_t* __restrict__ flags)
+{
+    const uint32_t kb = blockIdx.x, n = blockIdx.y;
+    const float* row = op + (uint64_t)(n * kTileN + threadIdx.x) * k_pad;
+    int any = 0;
+    for(uint32_t c = 0; c < (uint32_t)kBlockK; ++c)
+    {
+        const uint32_t p = kb * kBlockK + c;
+        if(p < N && row[col_of[p]] != 0.0f)
+            any = 1;
+    }
+    any = __syncthreads_or(any);
+    if(threadIdx.x == 0)
+        flags[n * ktiles + kb] = any ? 1u : 0u;
+}
+
+// Packed tile j (row tile tile_n[j], K-block tile_kb[j]) as BF16 hi/lo
+// [256][64], columns in the permuted order (past N: 0).  One thread a row.
+__global__ void __launch_bounds__(kTileN) tile_pack_kernel(const float* __restrict__ op, uint32_t k_pad,
+                                                            const uint32_t* __restrict__ col_of, uint32_t N,
+                                                            const uint32_t* __restrict__ tile_n,
+                                                            const uint32_t* __restrict__ tile_kb,
+                                                            __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo)
+{
+    const uint32_t j = blockIdx.x;
+    const float* row = op + (uint64_t)(tile_n[j] * kTileN + threadIdx.x) * k_pad;
+    const uint64_t o = ((uint64_t)j * kTileN + threadIdx.x) * kBlockK;
+    for(uint32_t c = 0; c < (uint32_t)kBlockK; ++c)
+    {
+        const uint32_t p = tile_kb[j] * kBlockK + c;
+        const float v = p < N ? row[col_of[p]] : 0.0f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        hi[o + c] = h;
+        lo[o + c] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
+
+// hi/lo[t][p] = split of x[t][col_of[p]] for p < N, 0 for N <= p < stride.
+__global__ void split_bf16_permuted_kernel(const float* __restrict__ x, uint64_t rows, uint64_t stride, uint32_t N,
+                                           const uint32_t* __restrict__ col_of, __nv_bfloat16* __restrict__ hi,
+                                           __nv_bfloat16* __restrict__ lo)
+{
+    const uint64_t t = blockIdx.x;
+    for(uint32_t p = threadIdx.x; p < stride; p += blockDim.x)
+    {
+        const float v = p < N ? x[t * stride + col_of[p]] : 0.0f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        hi[t * stride + p] = h;
+        lo[t * stride + p] = __float2bfloat16_rn(v - __bfloat162float(h));
+    }
+}
+
+} // namespace
+
+cudaError_t launch_ndf_tile_flags(const float* op, uint32_t k_pad, const uint32_t* col_of, uint32_t N,
+                                  uint32_t rows_pad, uint32_t* flags, cudaStream_t stream)
+{
+    if(rows_pad % kTileN != 0 || N == 0)
+        return cudaErrorInvalidValue;
+    const uint32_t ktiles = (N + kBlockK - 1) / kBlockK;
+    tile_flags_kernel<<<dim3(ktiles, rows_pad / kTileN), kTileN, 0, stream>>>(op, k_pad, col_of, N, ktiles, flags);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ndf_tile_pack(const float* op, uint32_t k_pad, const uint32_t* col_of, uint32_t N,
+                                 const uint32_t* tile_n, const uint32_t* tile_kb, uint32_t packed_tiles, void* hi,
+                                 void* lo, cudaStream_t stream)
+{
+    if(packed_tiles == 0)
+        return cudaSuccess;
+    tile_pack_kernel<<<packed_tiles, kTileN, 0, stream>>>(op, k_pad, col_of, N, tile_n, tile_kb,
+                                                         static_cast<__nv_bfloat16*>(hi), static_cast<__nv_bfloat16*>(lo));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_split_bf16_permuted(const float* x, uint64_t rows, uint64_t stride, uint32_t N,
+                                       const uint32_t* col_of, void* hi, void* lo, cudaStream_t stream)
+{
+    if(rows == 0)
+        return cudaSuccess;
+    if(rows > 0x7fffffffull || stride < N)
+        return cudaErrorInvalidValue;
+    split_bf16_permuted_kernel<<<(unsigned)rows, 256, 0, stream>>>(x, rows, stride, N, col_of,
+                                                                  static_cast<__nv_bfloat16*>(hi),
+                                                                  static_cast<__nv_bfloat16*>(lo));
     return cudaGetLastError();
 }
 
