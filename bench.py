@@ -697,9 +697,10 @@ def run_ours(args):
         lm_flops = N * (FLOPS_JACOBIAN_PASS * jac + FLOPS_RESIDUAL_PASS * res)
         achieved = lm_flops / (ms_fit / 1e3) / 1e12
         bf16_peak = peaks.get("bf16_tflops")
-        kp = (N + 7) // 8 * 8
         ndf_alg = 2.0 * T * NDF_ROWS * N * args.steps               # one FP32 GEMM
-        ndf_hw = 2.0 * T * NDF_ROWS_PAD * ((kp + 63) // 64 * 64) * 3 * args.steps   # BF16x3, padded tiles
+        # the tensor cores multiply the operator's non-empty 256 x 64 tiles only, 3 BF16 products each
+        ndf_tiles, ndf_tiles_total = stats[-1].ndf_tiles, stats[-1].ndf_tiles_total
+        ndf_hw = 2.0 * T * 256 * 64 * ndf_tiles * 3 * args.steps
         ndf_ach = ndf_alg / (ms_ndf / 1e3) / 1e12 if ms_ndf > 0 else None
         cpu = parity = None
         if world == 1 and not args.no_cpu_baseline:
@@ -736,8 +737,10 @@ def run_ours(args):
                 "hw_bf16_tflops": ndf_hw / (ms_ndf / 1e3) / 1e12,
                 "hw_frac": ndf_hw / (ms_ndf / 1e3) / 1e12 / bf16_peak,
                 "traffic": NDF_DRAM_BYTES_PER_TEXEL * T,
-                "note": "achieved counts one FP32 GEMM (2 x texels x 3217 x 6561); hw counts the 3 BF16 "
-                        "products over padded tiles the tensor cores execute"},
+                "tiles": {"multiplied": ndf_tiles, "all": ndf_tiles_total},
+                "note": "achieved counts the dense FP32 product (2 x texels x 3217 x 6561) that the tile-skipping "
+                        "GEMM delivers; hw counts the 3 BF16 products over the non-empty 256 x 64 operator "
+                        "tiles the tensor cores execute"},
             "phases_ms": {"luminance": ms_lum / args.steps, "init": ms_init / args.steps,
                           "ndf_gemm": ms_ndf / args.steps, "lm": ms_fit / args.steps},
             "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,

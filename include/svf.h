@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define SVF_ABI_VERSION 2u
+#define SVF_ABI_VERSION 3u
 
 typedef enum svf_status
 {
@@ -287,6 +287,9 @@ typedef struct svf_run_stats
                                    and launched, 2 replayed (a repeat of the previous call) */
     uint32_t fallback_texels;   /* SVF_INIT_MLP with mlp_fallback: texels fitted from the default guess
                                    as well (svf_fit_texels) */
+    uint32_t ndf_tiles;         /* the NDF GEMM's operator tiles (256 rows x 64 pairs) that hold a
+                                   non-zero, which it multiplies, */
+    uint32_t ndf_tiles_total;   /* of all its tiles (0 when no default guess ran) */
 } svf_run_stats;
 
 svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_options* options,

@@ -109,7 +109,8 @@ class RunStats(C.Structure):
                 ("residuals", C.c_uint64), ("failed_texels", C.c_uint64), ("ms_total", C.c_double),
                 ("ms_luminance", C.c_double), ("ms_init", C.c_double), ("ms_fit", C.c_double),
                 ("ms_copy", C.c_double), ("lm_threads", C.c_uint32), ("lm_slots", C.c_uint32),
-                ("ms_ndf", C.c_double), ("graph", C.c_uint32), ("fallback_texels", C.c_uint32)]
+                ("ms_ndf", C.c_double), ("graph", C.c_uint32), ("fallback_texels", C.c_uint32),
+                ("ndf_tiles", C.c_uint32), ("ndf_tiles_total", C.c_uint32)]
 
 
 _lib = None

@@ -806,6 +806,8 @@ svf_status prepare_init(svf_ctx* ctx, Layout* lay, const svf_layout_desc* desc, 
                                            dd->tile_kb.as<uint32_t>(), il.packed_tiles, dd->tile_hi.p, dd->tile_lo.p,
                                            ctx->stream));
     il.packed_tiles = alloc_tiles;
+    il.nonempty_tiles = tile_start[ntiles];
+    il.all_tiles = ktiles * ntiles;
     il.tile_hi = dd->tile_hi.p;
     il.tile_lo = dd->tile_lo.p;
     il.tile_kb = dd->tile_kb.as<uint32_t>();
@@ -867,7 +869,7 @@ svf_status read_error_flag(svf_ctx* ctx, bool with_ndf = false);
 // texels, keeps every texel of a call on one configuration.
 svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
 {
-    if(lay->tuned)
+    if(lay->tuned || std::getenv("SVF_LM_KERNEL"))   // (a pinned configuration needs no probe)
         return SVF_OK;
     // the plain passes only: the packed pass (one 256-thread CTA per SM at its
     // register count) wins on this short probe but loses on full launches
@@ -955,8 +957,8 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
             flops += (double)N * (169.0 * s.jacobians + 33.0 * s.residuals);
         const double rate = flops / std::max(1e-3, (double)ms);
         if(getenv("SVF_DEBUG"))
-            fprintf(stderr, "svf: LM tune L=%u threads=%d slots=%d packed=%d: %.3f ms, %.2f TFLOP/s (model)\n", L,
-                    cand[c].threads, cand[c].slots, cand[c].packed, ms, rate * 1e-9);
+            fprintf(stderr, "svf: LM tune L=%u threads=%d slots=%d pass=%d: %.3f ms, %.2f TFLOP/s (model)\n", L,
+                    cand[c].threads, cand[c].slots, cand[c].pass, ms, rate * 1e-9);
         if(c == 0)
             first_rate = rate;
         if(rate > best_rate)
@@ -977,17 +979,17 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
 // first that fits for the RGB fit (its slabs differ from the probe's).
 svf::LmKernelChoice lm_choice(Layout* lay, uint64_t stride, bool rgb)
 {
-    // SVF_LM_KERNEL=threads,slots,packed pins one candidate of svf::lm_candidates
+    // SVF_LM_KERNEL=threads,slots,pass pins one candidate of svf::lm_candidates
     // (for tests and measurements); others are ignored
     if(const char* e = std::getenv("SVF_LM_KERNEL"))
     {
         svf::LmKernelChoice c{ 0, 0, 0 };
-        if(std::sscanf(e, "%d,%d,%d", &c.threads, &c.slots, &c.packed) == 3)
+        if(std::sscanf(e, "%d,%d,%d", &c.threads, &c.slots, &c.pass) == 3)
         {
-            svf::LmKernelChoice cand[8];
-            const int n = svf::lm_candidates(lay->L, cand, 8);
+            svf::LmKernelChoice cand[svf::kLmCandidates];
+            const int n = svf::lm_candidates(lay->L, cand, svf::kLmCandidates);
             for(int i = 0; i < n; ++i)
-                if(cand[i].threads == c.threads && cand[i].slots == c.slots && cand[i].packed == c.packed &&
+                if(cand[i].threads == c.threads && cand[i].slots == c.slots && cand[i].pass == c.pass &&
                    svf::lm_max_ctas_per_sm(lay->L, stride, c, rgb) > 0)
                     return c;
         }
@@ -999,7 +1001,7 @@ svf::LmKernelChoice lm_choice(Layout* lay, uint64_t stride, bool rgb)
 
 svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r)
 {
-    if(!r.rgb && !lay->tuned && r.texels >= 4096 && !std::getenv("SVF_LM_KERNEL"))
+    if(!r.rgb && !lay->tuned && r.texels >= 4096)
         SVF_TRY(tune_lm(ctx, lay, o));
     return launch_lm(ctx, lay, o, r, lm_choice(lay, r.stride, r.rgb));
 }
@@ -1788,6 +1790,11 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
             rs.ms_ndf += span(ev(c, 3), ev(c, 7));
         rs.ms_fit += span(ev(c, 4), ev(c, 5));
         rs.ms_copy += span(ev(c, 5), ev(c, 6));
+    }
+    if(default_init)
+    {
+        rs.ndf_tiles = init_lay->nonempty_tiles;
+        rs.ndf_tiles_total = init_lay->all_tiles;
     }
     // the whole call: from the first copy (or the first kernel) to the last output
     rs.ms_total = span(samples_on_device ? ev(0, 2) : ev(0, 0), ev(n_chunks - 1, 6));

@@ -404,23 +404,38 @@ __global__ void __launch_bounds__(kFinishThreads) init_finish_kernel(InitLayout 
     }
     // every sample that can reach B lives in a cell whose corner maximum reaches
     // it (bilinear weights are in [0, 1]; the slack covers their rounding)
+    // A warp per cell, its lanes over the cell's samples (a cell holds about 64):
+    // the work of the cells that pass is spread over all threads whichever cells
+    // they are.  Each warp tests 32 cells at a time, one per lane, and walks the
+    // passing ones (the argmax's tie rule makes the order irrelevant).
     float best_v = -INFINITY;
     uint32_t best_i = 0xffffffffu;
-    for(uint32_t c = threadIdx.x; c < lay.pca_cells; c += kFinishThreads)
     {
-        const int32_t cell = lay.pca_cell_id[c];
-        const float u = cell_bound(ndf, cell);
-        if(u + fabsf(u) * 1e-5f < B)
-            continue;
-        for(uint32_t k = lay.pca_cell_start[c], e = lay.pca_cell_start[c + 1]; k < e; ++k)
+        const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+        for(uint32_t c0 = warp * 32u; c0 < lay.pca_cells; c0 += kFinishThreads)
         {
-            float2 fr = lay.pca_frac[k];
-            float v = bilinear(ndf, cell, fr.x, fr.y);
-            uint32_t idx = lay.pca_index[k];
-            if(better(v, idx, best_v, best_i))
+            const uint32_t c = c0 + lane;
+            bool pass = false;
+            if(c < lay.pca_cells)
             {
-                best_v = v;
-                best_i = idx;
+                const float u = cell_bound(ndf, lay.pca_cell_id[c]);
+                pass = !(u + fabsf(u) * 1e-5f < B);
+            }
+            for(uint32_t m = __ballot_sync(0xffffffffu, pass); m; m &= m - 1)
+            {
+                const uint32_t cc = c0 + (uint32_t)(__ffs(m) - 1);
+                const int32_t cell = lay.pca_cell_id[cc];
+                for(uint32_t k = lay.pca_cell_start[cc] + lane, e = lay.pca_cell_start[cc + 1]; k < e; k += 32)
+                {
+                    float2 fr = lay.pca_frac[k];
+                    float v = bilinear(ndf, cell, fr.x, fr.y);
+                    uint32_t idx = lay.pca_index[k];
+                    if(better(v, idx, best_v, best_i))
+                    {
+                        best_v = v;
+                        best_i = idx;
+                    }
+                }
             }
         }
     }

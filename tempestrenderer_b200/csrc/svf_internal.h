@@ -70,8 +70,10 @@ struct LmKernelChoice
 {
     int threads;
     int slots;
-    int packed;   // the pair pass in paired FP32 instructions (luminance fit, no Fresnel factor)
+    int pass;     // pair pass: 0 plain; 1 paired FP32 instructions; 2 J^T J on the tensor cores
+                  // (1 and 2: luminance fit without a Fresnel factor)
 };
+constexpr int kLmCandidates = 10;
 LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb = false);
 int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);
 size_t         lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb = false);
@@ -160,7 +162,9 @@ struct InitLayout
     // BF16 split in that order.
     uint16_t* col_pos;         // [N] position of pair k in the permuted order
     uint32_t* col_of;          // [N] pair at permuted position p
-    uint32_t  packed_tiles;    // non-empty 256 x 64 operator tiles
+    uint32_t  packed_tiles;    // packed tiles (the non-empty 256 x 64 operator tiles; at least 1)
+    uint32_t  nonempty_tiles;  // of them non-empty, and all tiles of the operator
+    uint32_t  all_tiles;
     void*     tile_hi;         // [packed_tiles][256][64] BF16 hi/lo split of them
     void*     tile_lo;
     uint32_t* tile_kb;         // [packed_tiles] K-block of each, grouped by row tile

@@ -824,6 +824,93 @@ __device__ __forceinline__ void sym_pair2(const PassConst2& c, const Entry& eaA,
     }
 }
 
+// ------------------------------------------------------------------------------
+// J^T J on the tensor cores: the Jacobian rows of a warp's pairs contracted by
+// mma.sync m16n8k8 TF32 with FP32 accumulation (luminance fit, no Fresnel).
+// J^T r and r^2 stay on the FP32 / FP64 pipes (the gradient decides where LM
+// stops, so it keeps FP32 products).
+// ------------------------------------------------------------------------------
+
+// Floats per lane of a warp's staging buffer: J1[0..7] and J2[0..7] interleaved
+// as (J1[g], J2[g]); the stride of 24 makes the fragment loads of a half-warp
+// hit 32 distinct banks.
+constexpr uint32_t kTcLaneStride = 24;
+constexpr uint32_t kTcWarpFloats = 32 * kTcLaneStride;
+
+// D[16x8] += A[16x8] B[8x8], A and B TF32 (an FP32 bit pattern is read with its
+// low 13 mantissa bits ignored), D FP32.
+__device__ __forceinline__ void mma_tf32(float* d, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1)
+{
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
+                 "{%0, %1, %2, %3};"
+                 : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+                 : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+// sym_pair without the J^T J sums: writes the Jacobian rows of the two ordered
+// pairs, J1 = sp1 V + kd_on h1 e_kd and J2 likewise (8 entries, the last 0), to
+// this lane's staging row, and accumulates J^T r (gr) and r^2.
+template <bool kAllUp>
+__device__ __forceinline__ void sym_pair_rows(const PassConst& c, const Entry& ea, const Entry& eb, float y1, float y2,
+                                              float wt1, float wt2, float* row, float* gr, double& r2)
+{
+    const float s0 = ea.a0 + eb.a0, s1 = ea.a1 + eb.a1, s2 = ea.a2 + eb.a2;
+    const float q0 = s0 * s0, q1 = s1 * s1, q2 = s2 * s2;
+    const float g = q0 + q1 + q2;
+    const float Q = c.u * q0 + c.v * q1 + q2;
+    const float S = ea.sp + eb.sp;
+    const float QQ = Q * Q;
+    const float QQS = QQ * S;
+    const float rden = QQS > 1e-37f ? rcp_approx(QQS) : 0.0f;
+    const float C = g * g * rden;
+    const float w1 = kAllUp ? wt1 * ea.kv : wt1 * ea.kv * eb.up;
+    const float w2 = kAllUp ? wt2 * eb.kv : wt2 * eb.kv * ea.up;
+    const float h1 = kAllUp ? wt1 * eb.kdc : wt1 * ea.up * eb.kdc;
+    const float h2 = kAllUp ? wt2 * ea.kdc : wt2 * eb.up * ea.kdc;
+    const float sp1 = w1 * C, sp2 = w2 * C;
+    const float r1 = y1 - (c.kd * h1 + c.ks * sp1);
+    const float r2b = y2 - (c.kd * h2 + c.ks * sp2);
+    r2 = fma((double)r1, (double)r1, r2);
+    r2 = fma((double)r2b, (double)r2b, r2);
+    const float rQ = Q * S * rden;
+    const float rS = QQ * rden;
+    const float t0 = s1 * s2 * (c.v - 1.0f);
+    const float t1 = s0 * s2 * (1.0f - c.u);
+    const float t2 = s0 * s1 * (c.u - c.v);
+    float V[kParams];
+    V[0] = c.ks * (c.rsx * (4.0f * c.u * q0 * rQ - 1.0f) - (ea.d0 + eb.d0) * rS);
+    V[1] = c.ks * (c.rsy * (4.0f * c.v * q1 * rQ - 1.0f) - (ea.d1 + eb.d1) * rS);
+    V[2] = c.ks_on;
+    V[3] = 0.0f;
+    const float m4 = -4.0f * rQ;
+    const float dd[3] = { ea.d2 + eb.d2, ea.d3 + eb.d3, ea.d4 + eb.d4 };
+#pragma unroll
+    for(int k = 0; k < 3; ++k)
+    {
+        const float dq = c.om[3 * k] * t0 + c.om[3 * k + 1] * t1 + c.om[3 * k + 2] * t2;
+        V[4 + k] = c.ks * (m4 * dq - dd[k] * rS);
+    }
+    const float R = sp1 * r1 + sp2 * r2b;
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+        if(i != 3)
+            gr[i] = fmaf(R, V[i], gr[i]);
+    gr[3] += c.kd_on * (h1 * r1 + h2 * r2b);
+    float J1[8], J2[8];
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+    {
+        J1[i] = i == 3 ? c.kd_on * h1 : sp1 * V[i];
+        J2[i] = i == 3 ? c.kd_on * h2 : sp2 * V[i];
+    }
+    J1[7] = J2[7] = 0.0f;
+    float4* r4 = reinterpret_cast<float4*>(row);
+#pragma unroll
+    for(int i = 0; i < 8; i += 2)
+        r4[i / 2] = make_float4(J1[i], J2[i], J1[i + 1], J2[i + 1]);
+}
+
 // The RGB pair: the geometry of sym_pair, three channels.  Per ordered pair k
 // and channel c:  f_kc = kd_c h_k + ks_c sp_k,  r_kc = y_kc - f_kc, and
 //   J_kc = kd_on_c h_k e_kd_c + ks_on_c sp_k e_ks_c + ks_c sp_k sum_j G_j e_j
@@ -1113,6 +1200,71 @@ __device__ void worker_pass2(const float* tab, const PassConst& c1, const float*
             for(int i = 32; i < kAcc; ++i)
                 red[wwarp * kAcc + i] = rest[i - 32];
     }
+    if(lane == 0)
+        redd[wwarp] = r2;
+}
+
+// worker_pass with J^T J on the tensor cores.  Each step every lane stages the
+// Jacobian rows of its unordered pair (two ordered pairs) in the warp's buffer
+// wbuf; then 8 mma.sync contract them: mma m takes the ordered pairs of lanes
+// 4m .. 4m+3 (k = t: first pair of lane 4m+t, k = t+4: its second) as
+// A[param][k] (rows 8-15 unused) and B[k][param], so D = sum_k J_k J_k^T.
+// Lane (g, t) loads (J1[g], J2[g]) of lane 4m+t, which is both a0/a2 and b0/b1.
+template <int NW, bool kAllUp>
+__device__ void worker_pass_tc(const float* tab, const PassConst& c, const float* slab, uint32_t L, float* red,
+                               double* redd, float* wbuf, uint32_t wwarp, uint32_t lane)
+{
+    constexpr int kAcc = LumModel::kAcc;
+    constexpr uint32_t kStride = 32u * NW;
+    const uint32_t half = L >> 1, nd = half + 1, Lp = pad4(L);
+    const uint32_t total = L * nd;
+    const uint32_t iters = (total + kStride - 1) / kStride;
+    const uint32_t sa = kStride / nd, sd = kStride - sa * nd;
+    uint32_t f = wwarp * 32u + lane;
+    uint32_t a = f / nd, d = f - a * nd;
+    const uint32_t g = lane >> 2, t = lane & 3u;
+    float* my_row = wbuf + lane * kTcLaneStride;
+
+    double r2 = 0.0;
+    float gr[kParams];
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+        gr[i] = 0.0f;
+    float D[4] = { 0.0f, 0.0f, 0.0f, 0.0f };
+    for(uint32_t it = 0; it < iters; ++it)
+    {
+        Entry ea, eb;
+        float y1, y2, wt1, wt2;
+        pair_load<true>(tab, slab, L, Lp, total, f, a, d, ea, eb, y1, y2, wt1, wt2);
+        sym_pair_rows<kAllUp>(c, ea, eb, y1, y2, wt1, wt2, my_row, gr, r2);
+        __syncwarp();
+#pragma unroll
+        for(uint32_t m = 0; m < 8; ++m)
+        {
+            const float2 u = *reinterpret_cast<const float2*>(wbuf + (4u * m + t) * kTcLaneStride + 2u * g);
+            const uint32_t x = __float_as_uint(u.x), y = __float_as_uint(u.y);
+            mma_tf32(D, x, 0u, y, 0u, x, y);
+        }
+        __syncwarp();   // the rows are read before the next step writes them
+        pair_advance(kStride, nd, sa, sd, f, a, d);
+    }
+    // J^T J: lane (g, t) holds D[g][2t] and D[g][2t + 1]; the upper triangle of
+    // the 7 x 7 block goes to the partials in the packed order
+#pragma unroll
+    for(int q = 0; q < 2; ++q)
+    {
+        const uint32_t n = 2u * t + (uint32_t)q;
+        if(g < (uint32_t)kParams && n < (uint32_t)kParams && g <= n)
+            red[wwarp * kAcc + hix<kParams>((int)g, (int)n)] = D[q];
+    }
+#pragma unroll
+    for(int i = 0; i < kParams; ++i)
+    {
+        const float s = warp_sum(gr[i]);
+        if(lane == 0)
+            red[wwarp * kAcc + kHessian + i] = s;
+    }
+    r2 = warp_sum(r2);
     if(lane == 0)
         redd[wwarp] = r2;
 }
@@ -1453,10 +1605,23 @@ __device__ void expand_sums(const double* sums, const float* pf, double* hg)
 // Resident CTAs per SM the register budget is sized for.
 constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : 2; }
 
-template <class M, int NW, int S, bool kFresnel, bool kAllUp, bool kPacked>
-__global__ void __launch_bounds__(32 * (NW + 1), kPacked ? 1 : min_blocks(32 * (NW + 1))) lm_fit_kernel(LmArgs args)
+// Pair passes: 0 plain, 1 paired FP32 instructions (worker_pass2), 2 J^T J on
+// the tensor cores (worker_pass_tc); 1 and 2 for the luminance fit without a
+// Fresnel factor.
+enum : int
 {
-    static_assert(!kPacked || (!M::kRgb && !kFresnel), "the packed pass is the luminance fit without Fresnel");
+    kPassPlain = 0,
+    kPassPacked = 1,
+    kPassTc = 2
+};
+
+template <class M, int NW, int S, bool kFresnel, bool kAllUp, int kPass>
+__global__ void __launch_bounds__(32 * (NW + 1), kPass == kPassPacked ? 1 : min_blocks(32 * (NW + 1)))
+    lm_fit_kernel(LmArgs args)
+{
+    static_assert(kPass == kPassPlain || (!M::kRgb && !kFresnel),
+                  "the packed and tensor-core passes are the luminance fit without Fresnel");
+    __shared__ __align__(16) float tc_rows[kPass == kPassTc ? NW * kTcWarpFloats : 4];
     constexpr uint32_t kThreads = 32 * (NW + 1);
     using SM = SlotSmem<NW, M>;
     using SlabT = typename M::Slab;
@@ -1486,9 +1651,13 @@ __global__ void __launch_bounds__(32 * (NW + 1), kPacked ? 1 : min_blocks(32 * (
                 break;
             if(cmd == kSlotPass)
             {
-                if constexpr(kPacked)
+                if constexpr(kPass == kPassPacked)
                     worker_pass2<NW, kAllUp>(tab_of(s), slots[s].pc, reinterpret_cast<const float*>(slab_of(s)),
                                              slots[s].L, red_of(s), redd_of(s), wwarp, lane);
+                else if constexpr(kPass == kPassTc)
+                    worker_pass_tc<NW, kAllUp>(tab_of(s), slots[s].pc, reinterpret_cast<const float*>(slab_of(s)),
+                                               slots[s].L, red_of(s), redd_of(s), tc_rows + wwarp * kTcWarpFloats,
+                                               wwarp, lane);
                 else
                     worker_pass<M, NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc, slab_of(s), slots[s].L,
                                                          args.cfg.fresnel, red_of(s), redd_of(s), wwarp, lane);
@@ -1660,32 +1829,40 @@ template <class M, int NW, int S>
 KernelFn pick(bool fresnel, bool all_up)
 {
     if(fresnel)
-        return all_up ? lm_fit_kernel<M, NW, S, true, true, false> : lm_fit_kernel<M, NW, S, true, false, false>;
-    return all_up ? lm_fit_kernel<M, NW, S, false, true, false> : lm_fit_kernel<M, NW, S, false, false, false>;
+        return all_up ? lm_fit_kernel<M, NW, S, true, true, kPassPlain> : lm_fit_kernel<M, NW, S, true, false, kPassPlain>;
+    return all_up ? lm_fit_kernel<M, NW, S, false, true, kPassPlain> : lm_fit_kernel<M, NW, S, false, false, kPassPlain>;
 }
 
-// The packed instances (luminance, no Fresnel factor).
-template <int NW, int S>
-KernelFn pick_packed(bool all_up)
+// The packed and tensor-core instances (luminance, no Fresnel factor).
+template <int NW, int S, int kPass>
+KernelFn pick_pass(bool all_up)
 {
-    return all_up ? lm_fit_kernel<LumModel, NW, S, false, true, true> : lm_fit_kernel<LumModel, NW, S, false, false, true>;
+    return all_up ? lm_fit_kernel<LumModel, NW, S, false, true, kPass> : lm_fit_kernel<LumModel, NW, S, false, false, kPass>;
 }
 
 template <class M>
 KernelFn kernel_for_model(LmKernelChoice c, bool fresnel, bool all_up)
 {
     if constexpr(!M::kRgb)
-        if(c.packed && !fresnel)
+        if(c.pass == kPassPacked && !fresnel)
         {
             if(c.threads == 256 && c.slots == 3)
-                return pick_packed<7, 3>(all_up);
+                return pick_pass<7, 3, kPassPacked>(all_up);
             if(c.threads == 256 && c.slots == 4)
-                return pick_packed<7, 4>(all_up);
+                return pick_pass<7, 4, kPassPacked>(all_up);
             if(c.threads == 128 && c.slots == 3)
-                return pick_packed<3, 3>(all_up);
+                return pick_pass<3, 3, kPassPacked>(all_up);
             return nullptr;
         }
-    // (a packed choice runs the plain pass where the packed one does not apply)
+        else if(c.pass == kPassTc && !fresnel)
+        {
+            if(c.threads == 256 && c.slots == 2)
+                return pick_pass<7, 2, kPassTc>(all_up);
+            if(c.threads == 128 && c.slots == 3)
+                return pick_pass<3, 3, kPassTc>(all_up);
+            return nullptr;
+        }
+    // (a packed or tensor-core choice runs the plain pass where those do not apply)
     if(c.threads == 256 && c.slots == 2)
         return pick<M, 7, 2>(fresnel, all_up);
     if(c.threads == 256 && c.slots == 3)
@@ -1732,11 +1909,13 @@ LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
 int lm_candidates(uint32_t, LmKernelChoice* out, int max)
 {
     // the plain passes first (the untuned default picks among them), then the
-    // packed ones (one CTA of 256 threads per SM at their register count)
-    const LmKernelChoice all[8] = { { 256, 3, 0 }, { 256, 2, 0 }, { 128, 3, 0 }, { 128, 2, 0 },
-                                    { 256, 1, 0 }, { 256, 3, 1 }, { 256, 4, 1 }, { 128, 3, 1 } };
+    // packed ones (one CTA of 256 threads per SM at their register count), then
+    // the tensor-core J^T J ones (their staging rows take shared memory)
+    const LmKernelChoice all[kLmCandidates] = { { 256, 3, 0 }, { 256, 2, 0 }, { 128, 3, 0 }, { 128, 2, 0 },
+                                                { 256, 1, 0 }, { 256, 3, 1 }, { 256, 4, 1 }, { 128, 3, 1 },
+                                                { 256, 2, 2 }, { 128, 3, 2 } };
     int n = 0;
-    for(int i = 0; i < 8 && n < max; ++i)
+    for(int i = 0; i < kLmCandidates && n < max; ++i)
         out[n++] = all[i];
     return n;
 }
