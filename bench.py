@@ -329,8 +329,50 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, tru
                      "accuracy); LM from its prediction with 1e-3 of the reference's initial damping"}
 
 
+def _fp64_brdf_rows(args):
+    """The FP64 oracle's BRDF (svfo_brdf_f64) of 7-parameter vectors over all pairs
+    of a layout: rows as FP32 and each row's RMS in FP64 (a worker of a spawned pool)."""
+    import oracle
+
+    params, lp = args
+    rows = np.zeros((len(params), lp.shape[0] ** 2), np.float32)
+    rms = np.zeros(len(params))
+    ref32 = np.zeros(len(params))
+    for i, p in enumerate(params):
+        f32, f64 = oracle.brdf_all(np.asarray(p, np.float64), lp)
+        rows[i] = f64
+        rms[i] = np.sqrt(np.mean(f64 ** 2))
+        # the reference's own FP32 evaluation (the oracle restates it bit for bit)
+        ref32[i] = np.sqrt(np.mean((f32.astype(np.float64) - f64) ** 2)) / max(rms[i], 1e-30)
+    return rows, rms, ref32
+
+
+def fp64_check(svf, ctx, lp, params, chunk=512):
+    """BRDF relative error of the GPU's FP32 model against the FP64 oracle at the
+    given parameters: per texel RMS(GPU - FP64) / RMS(FP64) over all pairs, read as
+    the RMSE of a zero-iteration GPU fit to the FP64 values."""
+    import multiprocessing as mp
+
+    n = len(params)
+    parts = [(params[i:i + chunk], lp) for i in range(0, n, chunk)]
+    err = np.zeros(n)
+    with mp.get_context("spawn").Pool(min(len(parts) * 4, os.cpu_count() or 1)) as pool:
+        sub = [(p[j:j + 32], lp) for p, _ in parts for j in range(0, len(p), 32)]
+        res = pool.map(_fp64_brdf_rows, sub)
+    rows = np.concatenate([r[0] for r in res])
+    rms = np.concatenate([r[1] for r in res])
+    ref32 = np.concatenate([r[2] for r in res])
+    for i in range(0, n, chunk):
+        _, rmse, _ = ctx.lsq_fit_batch(lp, rows[i:i + chunk], np.ascontiguousarray(params[i:i + chunk], np.float32),
+                                       svf.options(max_iterations=0))
+        err[i:i + chunk] = rmse / np.maximum(rms[i:i + chunk], 1e-30)
+    return err, ref32
+
+
 def fib151_item(svf, ctx, steps, dev, side=768):
-    """768x768 texels on the 151-direction Fibonacci layout (22801 pairs), FP16 RGB samples."""
+    """768x768 texels on the 151-direction Fibonacci layout (22801 pairs), FP16 RGB samples;
+    BRDF error against the FP64 oracle and parameter error against the ground truth on a
+    seeded 4096-texel subset."""
     import torch
 
     lp = svf.directions_fibonacci(151)
@@ -338,9 +380,11 @@ def fib151_item(svf, ctx, steps, dev, side=768):
     N = 151 * 151
     T = side * side
     samples = torch.empty((T, N, 3), dtype=torch.float16, device=dev)
-    ctx.synth_btf(SEED + 2, MIX, lp, 0, T, samples, sample_type=svf.SVF_SAMPLES_F16)
+    truth = torch.empty((T, 16), dtype=torch.float32, device=dev)
+    ctx.synth_btf(SEED + 2, MIX, lp, 0, T, samples, sample_type=svf.SVF_SAMPLES_F16, truth=truth)
     maps = {k: torch.zeros(s, dtype=torch.float32, device=dev) for k, s in
-            {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,)}.items()}
+            {"diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4), "rmse": (T,),
+             "params": (T, 7)}.items()}
     opts = svf.options(max_iterations=1024)
     run = lambda: ctx.fit_texels(layout, samples, side, side, sample_type=svf.SVF_SAMPLES_F16, opts=opts,
                                  want=tuple(maps), out=maps, check=False)[1]
@@ -357,8 +401,21 @@ def fib151_item(svf, ctx, steps, dev, side=768):
                          "ndf_gemm": sum(r.ms_ndf for r in st) / steps, "lm": ms_fit},
            "lm_tflops": flops / (ms_fit / 1e3) / 1e12,
            "failed_texels": st[-1].failed_texels, "mean_rmse": float(maps["rmse"].mean().item())}
-    del samples
+    params = maps["params"].cpu().numpy()
+    truth_np = truth.cpu().numpy()
+    del samples, truth
     torch.cuda.empty_cache()
+    idx = np.sort(np.random.default_rng(SEED + 2).choice(T, 4096, replace=False))
+    err, ref32 = fp64_check(svf, ctx, lp, params[idx])
+    q = lambda a: {"median": float(np.median(a)), "p99": float(np.quantile(a, 0.99)), "max": float(a.max())}
+    out["fp64_check"] = {"texels": len(idx), "subset": "4096 texels drawn with seed SEED + 2",
+                         "brdf_rel_error": q(err), "bar": 1e-5, "within_bar": float(np.mean(err <= 1e-5)),
+                         "reference_fp32_brdf_rel_error": dict(q(ref32), within_bar=float(np.mean(ref32 <= 1e-5))),
+                         "ground_truth_error_subset": param_error(params[idx], truth_np[idx]),
+                         "ground_truth_error_all": param_error(params, truth_np)}
+    out["fp64_check_summary"] = {"brdf_rel_error_max": float(err.max()), "within_1e-5": float(np.mean(err <= 1e-5)),
+                                 "reference_fp32_within_1e-5": float(np.mean(ref32 <= 1e-5)),
+                                 "normal_p90_deg": out["fp64_check"]["ground_truth_error_subset"]["normal_deg"]["p90"]}
     return out
 
 

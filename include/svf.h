@@ -63,7 +63,13 @@ typedef enum svf_status
 #define SVF_TEXEL_TIMEOUT    4u  /* the texel's samples did not arrive (bounded wait expired) */
 
 /* LeastSquaresFitOptions (svbrdf-fitting.hh:100-107) for the supported path */
-#define SVF_LSQ_DIFFUSE      (1u << 1)   /* LSF_OPTON_DIFFUSE: fit the Lambert term (7 parameters) */
+#define SVF_LSQ_DIFFUSE      (1u << 1)   /* LSF_OPTON_DIFFUSE: fit the Lambert term (7 parameters);
+                                            without it the specular-only fit of svbrdffit's default
+                                            (6 parameters {sx, sy, ks, euler}, diffuse held at 0;
+                                            svbrdf-lsq-fitting-setup.cc:248-262) */
+#define SVF_LSQ_DISABLE_DIRECTION_FITTING (1u << 2)   /* LSF_OPTION_DISABLE_DIRECTION_FITTING: the Euler
+                                            angles are held at their initial values
+                                            (svbrdf-lsq-fitting-setup.cc:265-268) */
 /* The RGB fit (no counterpart in the reference, which fits the luminance and
  * colours the maps with the average chromaticity): 11 parameters per texel,
  * {kd rgb, ks rgb, sx, sy} plus the orientation, fitted to the three channels
@@ -94,6 +100,12 @@ typedef struct svf_lsq_options
     uint32_t restarts;            /* times LM continues, with fresh damping, from the point where
                                      the reference's stopping rules end it; 0 = the reference's
                                      single run.  Default 1. */
+    uint32_t downsample_light_view; /* LeastSquaresFitOptions::DownSampleLightView (svbrdffit -S):
+                                     when 2 <= n < L, svf_lsq_fit_sggx / svf_lsq_fit_batch fit the
+                                     n x n pairs of the n directions svf_downsample_light_view
+                                     picks, and report the RMSE over all L x L pairs at Fresnel 1
+                                     (svbrdf-lsq-fitting-setup.cc:314-330,403-421).  0 = off
+                                     (the default); the texel-loop entry points take 0 only. */
 } svf_lsq_options;
 
 typedef struct svf_texel_stats
@@ -156,6 +168,12 @@ uint32_t svf_directions_fibonacci(uint32_t count, float* lights_parabolic);
 uint32_t svf_layout_triangulate(const float* lights_parabolic, uint32_t light_count,
                                 uint32_t* triangles, uint32_t* edges, float* edge_angles,
                                 uint32_t* edge_count);
+
+/* DownsampleLightView's choice of directions (svbrdf-lsq-fitting-setup.cc:129-163):
+ * writes the n (2 <= n < L) kept direction indices, one drawn pseudo-randomly
+ * per stride of (L - 1)/(n - 1) with the reference's seeded hash, to idx[n].
+ * Returns n, or 0 for sizes out of range. */
+uint32_t svf_downsample_light_view(uint32_t light_count, uint32_t n, uint32_t* idx);
 
 /* LeastSquaresFitSGGX ------------------------------------------------------------ */
 /* One texel, synchronous: fits `init` to the luminance slice `lum` ([L*L],

@@ -376,10 +376,32 @@ def ref_available() -> bool:
     return os.path.exists(REF_SO)
 
 
+# The reference pipeline with the drop-in LeastSquaresFitSGGX (svf_shim.cc on
+# libsvf.so) in place of its CPU one: the same harness entry points.
+REF_SVF_SO = os.path.join(HERE, "_ref", "libtempest_ref_svf.so")
+_ref_svf = None
+
+
+def ref_svf_available() -> bool:
+    return os.path.exists(REF_SVF_SO)
+
+
+def ref_svf():
+    global _ref_svf
+    if _ref_svf is None:
+        _ref_svf = _bind_harness(C.CDLL(REF_SVF_SO))
+    return _ref_svf
+
+
 def ref():
     global _ref
     if _ref is None:
-        L = C.CDLL(REF_SO)
+        _ref = _bind_harness(C.CDLL(REF_SO))
+    return _ref
+
+
+def _bind_harness(L):
+    if True:
         L.ref_btf_load.argtypes = [C.c_char_p]
         L.ref_btf_load.restype = C.c_void_p
         L.ref_btf_free.argtypes = [C.c_void_p]
@@ -402,31 +424,37 @@ def ref():
         L.ref_exr_load.restype = C.c_int
         L.ref_error_texel.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, _f32p, _f32p, _f32p, _f32p, C.c_uint32,
                                       C.c_uint32, _f32p, _f32p]
-        _ref = L
-    return _ref
+        L.ref_lsq_opts.argtypes = [_f32p, C.c_uint32, _f32p, C.c_float, C.c_uint32, C.c_uint32, _f32p, _f32p,
+                                   C.POINTER(C.c_float), _u32p]
+        if hasattr(L, "ref_downsample"):   # (not in the seam library)
+            L.ref_downsample.argtypes = [_f32p, C.c_uint32, _f32p, C.c_uint32, _f32p, _f32p]
+    return L
 
 
 LSF_OPTON_DIFFUSE = 1 << 1
+LSF_OPTION_DISABLE_DIRECTION_FITTING = 1 << 2
 
 
 class RefBTF:
     """A BTF loaded by the reference's LoadBTF."""
 
-    def __init__(self, path):
-        self.handle = ref().ref_btf_load(path.encode())
+    def __init__(self, path, lib=None):
+        """lib: the harness library that loads and fits it (default: the reference's own)."""
+        self.lib = lib or ref()
+        self.handle = self.lib.ref_btf_load(path.encode())
         if not self.handle:
             raise RuntimeError(f"LoadBTF failed on {path}")
         dims = np.zeros(5, np.uint32)
-        ref().ref_btf_info(self.handle, dims)
+        self.lib.ref_btf_info(self.handle, dims)
         self.width, self.height, self.light_count, self.tri_count, self.edge_count = map(int, dims)
 
     @staticmethod
-    def from_texels(theta_phi, rgb_texels, data_size=4) -> "RefBTF":
+    def from_texels(theta_phi, rgb_texels, data_size=4, lib=None) -> "RefBTF":
         fd, path = tempfile.mkstemp(suffix=".btf")
         os.close(fd)
         try:
             write_dfmf(path, theta_phi, rgb_texels, data_size=data_size)
-            return RefBTF(path)
+            return RefBTF(path, lib)
         finally:
             os.unlink(path)
 
@@ -436,14 +464,14 @@ class RefBTF:
         tri = np.zeros((self.tri_count, 3), np.uint32)
         e = np.zeros((self.edge_count, 3), np.uint32)
         ea = np.zeros((self.edge_count, 2), np.float32)
-        ref().ref_btf_geometry(self.handle, lp, tri, e, ea)
+        self.lib.ref_btf_geometry(self.handle, lp, tri, e, ea)
         return MeshData(lp, tri, e, ea)
 
     def lum_slice(self, x, y=0):
         N = self.light_count ** 2
         lum = np.zeros(N, np.float32)
         avg = np.zeros(3, np.float32)
-        ref().ref_btf_lum_slice(self.handle, x, y, lum, avg)
+        self.lib.ref_btf_lum_slice(self.handle, x, y, lum, avg)
         return lum, avg
 
     def fit_texel(self, x, y=0, fresnel=1.0, want_ndf=False):
@@ -453,7 +481,7 @@ class RefBTF:
         rmse = C.c_float()
         st = np.zeros(2, np.uint32)
         ndf = np.zeros(64 * 64, np.float32) if want_ndf else None
-        rc = ref().ref_fit_texel(self.handle, x, y, fresnel, init7, fit7, maps, C.byref(rmse), st,
+        rc = self.lib.ref_fit_texel(self.handle, x, y, fresnel, init7, fit7, maps, C.byref(rmse), st,
                                  ndf.ctypes.data if want_ndf else None, None)
         if rc != 0:
             raise RuntimeError("reference pipeline did not reach LeastSquaresFitSGGX")
@@ -462,14 +490,14 @@ class RefBTF:
 
     def time_fit(self, first, count, workers, pool_threads, fresnel=1.0):
         rm = np.zeros(count, np.float32)
-        secs = ref().ref_time_fit_texels(self.handle, first, count, workers, pool_threads, fresnel,
+        secs = self.lib.ref_time_fit_texels(self.handle, first, count, workers, pool_threads, fresnel,
                                          rm.ctypes.data)
         return secs, rm
 
     def __del__(self):
         try:
             if self.handle:
-                ref().ref_btf_free(self.handle)
+                self.lib.ref_btf_free(self.handle)
         except Exception:
             pass
 
@@ -482,6 +510,26 @@ def ref_lsq(lum, lights_parabolic, init7, fresnel=1.0, flags=LSF_OPTON_DIFFUSE):
     ref().ref_lsq(lp, lp.shape[0], np.ascontiguousarray(lum, np.float32), fresnel, flags,
                   np.ascontiguousarray(init7, np.float32), out, C.byref(rmse), st)
     return out, rmse.value, int(st[0]), int(st[1])
+
+
+def ref_lsq_opts(lum, lights_parabolic, init7, fresnel=1.0, flags=LSF_OPTON_DIFFUSE, downsample=0xFFFFFFFF):
+    """LeastSquaresFitSGGX with the given LeastSquaresFitOptions flags and DownSampleLightView."""
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    out = np.zeros(7, np.float32)
+    rmse = C.c_float()
+    st = np.zeros(2, np.uint32)
+    ref().ref_lsq_opts(lp, lp.shape[0], np.ascontiguousarray(lum, np.float32), fresnel, flags, downsample,
+                       np.ascontiguousarray(init7, np.float32), out, C.byref(rmse), st)
+    return out, rmse.value, int(st[0]), int(st[1])
+
+
+def ref_downsample(lum, lights_parabolic, n):
+    """DownsampleLightView: the kept directions and the n x n slice."""
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    dirs = np.zeros((n, 2), np.float32)
+    sl = np.zeros(n * n, np.float32)
+    ref().ref_downsample(lp, lp.shape[0], np.ascontiguousarray(lum, np.float32), n, dirs, sl)
+    return dirs, sl
 
 
 def ref_brdf_all(params7, lights_parabolic, fresnel=1.0):

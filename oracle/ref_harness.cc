@@ -37,6 +37,11 @@
 #include "svbrdf-fitting.hh"
 #include "svbrdf-lsq-fitting-internal.hh"
 
+/* defined in svbrdf-lsq-fitting-setup.cc:129, declared in no header */
+void DownsampleLightView(const Tempest::Vector2* orig_light_dirs, uint32_t orig_light_count, float* orig_lv_lum_slice,
+                         Tempest::Vector2* downsample_light_dirs, uint32_t downsample_light_count,
+                         float* downsampled_lum_slice);
+
 #include <atomic>
 #include <chrono>
 #include <cstdio>
@@ -93,12 +98,12 @@ Tempest::ThreadPool* SerialPool()
     return pool;
 }
 
-LeastSquaresFitOptions MakeOptions(float fresnel, uint32_t flags)
+LeastSquaresFitOptions MakeOptions(float fresnel, uint32_t flags, uint32_t downsample = ~0u)
 {
     LeastSquaresFitOptions o;
     o.MultiScatteringBounceCount = ~0u;
     o.Fresnel = fresnel;
-    o.DownSampleLightView = ~0u;
+    o.DownSampleLightView = downsample;
     o.Flags = flags;
     return o;
 }
@@ -195,6 +200,41 @@ void ref_brdf_eval(const float* lights_parabolic, uint32_t light_count, float fr
     for(uint32_t idx = 0; idx < light_count*light_count; ++idx)
         out[idx] = ev(0, idx, params);
 }
+
+/* LeastSquaresFitSGGX with LeastSquaresFitOptions::Flags and DownSampleLightView
+ * as given (downsample ~0u: off).  stats as ref_lsq. */
+void ref_lsq_opts(const float* lights_parabolic, uint32_t light_count, const float* lum, float fresnel, uint32_t flags,
+                  uint32_t downsample, const float* init7, float* out7, float* rmse, uint32_t* stats)
+{
+    Tempest::BTF btf;
+    btf.LightCount = light_count;
+    std::vector<Tempest::Vector2> lights(light_count);
+    std::memcpy(lights.data(), lights_parabolic, light_count*sizeof(Tempest::Vector2));
+    btf.LightsParabolic = lights.data();
+    std::vector<float> lum_copy(lum, lum + (size_t)light_count*light_count);
+    OptimizationParameters init, out;
+    std::memcpy(init.ParametersArray, init7, sizeof(init.ParametersArray));
+    auto opts = MakeOptions(fresnel, flags, downsample);
+    LeastSquaresFitSGGX(0, *SerialPool(), &btf, lum_copy.data(), opts, init, &out, rmse);
+    ParseIterationLog();
+    std::memcpy(out7, out.ParametersArray, sizeof(out.ParametersArray));
+    stats[0] = g_iterations;
+    stats[1] = g_effective;
+    btf.LightsParabolic = nullptr;
+}
+
+#ifndef SVF_SHIM_BUILD
+/* DownsampleLightView (svbrdf-lsq-fitting-setup.cc:129-163): the kept directions
+ * (parabolic) and the downsampled slice.  (Not in the seam library, which has the
+ * drop-in LeastSquaresFitSGGX in place of that file.) */
+void ref_downsample(const float* lights_parabolic, uint32_t light_count, const float* lum, uint32_t n,
+                    float* out_lights, float* out_slice)
+{
+    std::vector<float> lum_copy(lum, lum + (size_t)light_count*light_count);
+    DownsampleLightView(reinterpret_cast<const Tempest::Vector2*>(lights_parabolic), light_count, lum_copy.data(),
+                        reinterpret_cast<Tempest::Vector2*>(out_lights), n, out_slice);
+}
+#endif
 
 /* LeastSquaresFitSGGX on a given luminance slice and initial guess.
  * stats[0] = iterations, stats[1] = effective (accepted) iterations. */

@@ -28,6 +28,7 @@ SVF_TEXEL_NONFINITE, SVF_TEXEL_MAX_ITER, SVF_TEXEL_TIMEOUT = 1, 2, 4
 SVF_LSQ_DIFFUSE = 1 << 1
 SVF_LSQ_RGB = 1 << 8
 SVF_LSQ_STEP_PER_PARAMETER = 1 << 9
+SVF_LSQ_DISABLE_DIRECTION_FITTING = 1 << 2
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
 SVF_ERROR_PAIRWISE, SVF_ERROR_MAX_VIEW = 0, 1
@@ -42,7 +43,7 @@ EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_op
            "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy", "svf_btf_probe", "svf_btf_load", "svf_btf_load_file",
            "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_btf_destroy", "svf_error_maps", "svf_exr_write",
            "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps", "svf_refit_neighborhood",
-           "svf_render_btf")
+           "svf_render_btf", "svf_downsample_light_view")
 
 
 class SvfError(RuntimeError):
@@ -53,7 +54,8 @@ class SvfError(RuntimeError):
 
 class LsqOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_uint32), ("fresnel", C.c_float), ("flags", C.c_uint32),
-                ("mse_target", C.c_double), ("break_on_small_step", C.c_double), ("restarts", C.c_uint32)]
+                ("mse_target", C.c_double), ("break_on_small_step", C.c_double), ("restarts", C.c_uint32),
+                ("downsample_light_view", C.c_uint32)]
 
 
 class TexelStats(C.Structure):
@@ -135,6 +137,8 @@ def load() -> C.CDLL:
         L.svf_directions_ring81.restype = u32
         L.svf_directions_fibonacci.argtypes = [u32, vp]
         L.svf_directions_fibonacci.restype = u32
+        L.svf_downsample_light_view.argtypes = [u32, u32, vp]
+        L.svf_downsample_light_view.restype = u32
         L.svf_layout_triangulate.argtypes = [vp, u32, vp, vp, vp, C.POINTER(u32)]
         L.svf_layout_triangulate.restype = u32
         L.svf_lsq_fit_sggx.argtypes = [vp, vp, u32, vp, C.POINTER(LsqOptions), vp, vp, vp, C.POINTER(TexelStats)]
@@ -187,13 +191,21 @@ def _check(status: int):
 
 
 def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | None = None,
-            rgb: bool = False, step_per_parameter: bool = True) -> LsqOptions:
+            rgb: bool = False, step_per_parameter: bool = True, diffuse: bool = True,
+            fit_direction: bool = True, downsample: int = 0) -> LsqOptions:
     """LM options; rgb selects the 11-parameter RGB fit (svf_fit_texels / svf_fit_btfs);
-    step_per_parameter=False restores the reference's whole-vector small-step test."""
+    step_per_parameter=False restores the reference's whole-vector small-step test;
+    diffuse=False the specular-only fit, fit_direction=False holds the Euler angles,
+    downsample=n fits n of the directions (svf_lsq_fit_sggx / svf_lsq_fit_batch)."""
     o = LsqOptions()
     load().svf_lsq_options_default(C.byref(o))
     o.max_iterations = max_iterations
     o.fresnel = fresnel
+    o.downsample_light_view = downsample
+    if not diffuse:
+        o.flags &= ~SVF_LSQ_DIFFUSE
+    if not fit_direction:
+        o.flags |= SVF_LSQ_DISABLE_DIRECTION_FITTING
     if rgb:
         o.flags |= SVF_LSQ_RGB
     if not step_per_parameter:
@@ -218,6 +230,14 @@ def directions_ring81() -> np.ndarray:
     n = load().svf_directions_ring81(lp.ctypes.data)
     assert n == 81
     return lp
+
+
+def downsample_light_view(light_count: int, n: int) -> np.ndarray:
+    """The direction indices DownsampleLightView keeps (svf_downsample_light_view)."""
+    idx = np.zeros(max(n, 1), np.uint32)[:n]
+    if n < 2 or load().svf_downsample_light_view(light_count, n, idx.ctypes.data) != n:
+        raise SvfError(SVF_EINVAL, f"no draw of {n} of {light_count} directions")
+    return idx
 
 
 def directions_fibonacci(count: int) -> np.ndarray:

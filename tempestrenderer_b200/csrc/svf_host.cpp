@@ -568,13 +568,18 @@ float initial_damping(const svf_fit_options& o)
     return o.init_mode == SVF_INIT_MLP ? kMlpInitialDamping : 1.0f;
 }
 
-svf_status check_options(const svf_lsq_options* o)
+svf_status check_options(const svf_lsq_options* o, bool downsample_ok = false)
 {
     if(!o)
         return fail(SVF_EINVAL, "null options");
-    if(!(o->flags & SVF_LSQ_DIFFUSE))
-        return fail(SVF_EINVAL, "only the fits with the diffuse term (SVF_LSQ_DIFFUSE) are supported");
-    constexpr uint32_t known = SVF_LSQ_DIFFUSE | SVF_LSQ_RGB | SVF_LSQ_STEP_PER_PARAMETER;
+    if(o->downsample_light_view == 1 || (o->downsample_light_view && !downsample_ok) ||
+       (o->downsample_light_view && (o->flags & SVF_LSQ_RGB)))
+        return fail(SVF_EINVAL, "downsample_light_view %u: 0, or 2 and more with svf_lsq_fit_sggx / svf_lsq_fit_batch",
+                    o->downsample_light_view);
+    if((o->flags & SVF_LSQ_RGB) && (o->flags & SVF_LSQ_DISABLE_DIRECTION_FITTING || !(o->flags & SVF_LSQ_DIFFUSE)))
+        return fail(SVF_EINVAL, "the RGB fit (SVF_LSQ_RGB) fits every parameter, with the diffuse term");
+    constexpr uint32_t known =
+        SVF_LSQ_DIFFUSE | SVF_LSQ_RGB | SVF_LSQ_STEP_PER_PARAMETER | SVF_LSQ_DISABLE_DIRECTION_FITTING;
     if(o->flags & ~known)
         return fail(SVF_EINVAL, "unknown lsq flags 0x%x", o->flags & ~known);
     if(!(o->fresnel >= 1.0f) || !std::isfinite(o->fresnel))
@@ -1006,6 +1011,19 @@ svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmR
     return launch_lm(ctx, lay, o, r, lm_choice(lay, r.stride, r.rgb));
 }
 
+// The parameters LM holds: the diffuse albedo (at 0) without SVF_LSQ_DIFFUSE,
+// the Euler angles with SVF_LSQ_DISABLE_DIRECTION_FITTING (the luminance fit).
+void lm_masks(const svf_lsq_options* o, svf::LmConfig& cfg)
+{
+    cfg.fixed_mask = cfg.zero_mask = 0;
+    if(o->flags & SVF_LSQ_RGB)
+        return;
+    if(!(o->flags & SVF_LSQ_DIFFUSE))
+        cfg.fixed_mask = cfg.zero_mask = 1u << 3;
+    if(o->flags & SVF_LSQ_DISABLE_DIRECTION_FITTING)
+        cfg.fixed_mask |= 0x70u;
+}
+
 // Fault injection for the tests of the bounded slab wait, read from the
 // environment at each launch: SVF_FAULT_SKIP_SLAB_COPY=<texel> leaves that
 // texel's slab copy unissued (its wait runs out: SVF_ETIMEOUT, the texel's status
@@ -1061,6 +1079,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     a.cfg.fresnel = o->fresnel;
     a.cfg.restarts = o->restarts;
     a.cfg.step_per_param = (o->flags & SVF_LSQ_STEP_PER_PARAMETER) ? 1u : 0u;
+    lm_masks(o, a.cfg);
     SVF_TRY(ctx->counter.ensure(16));
     SVF_TRY(ctx->error.ensure(16));
     a.work_counter = ctx->counter.as<uint32_t>();
@@ -1134,6 +1153,14 @@ void svf_lsq_options_default(svf_lsq_options* o)
     o->mse_target = 1e-6;
     o->break_on_small_step = (double)1e-3f;   // settings.BreakOnSmallStep = 1e-3f
     o->restarts = 1;
+    o->downsample_light_view = 0;   // DownSampleLightView = ~0u: all directions
+}
+
+uint32_t svf_downsample_light_view(uint32_t L, uint32_t n, uint32_t* idx)
+{
+    if(!idx || !svf::downsample_light_view(L, n, idx))
+        return 0;
+    return n;
 }
 
 svf_status svf_create(int device, svf_ctx** out)
@@ -1244,7 +1271,7 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
                              svf_texel_stats* stats)
 {
     SVF_TRY(check_ctx(ctx));
-    SVF_TRY(check_options(opts));
+    SVF_TRY(check_options(opts, true));
     if(opts->flags & SVF_LSQ_RGB)
         return fail(SVF_EINVAL, "the RGB fit (SVF_LSQ_RGB) takes RGB samples: use svf_fit_texels");
     if(!lum || !init || !out || !rmse)
@@ -1269,7 +1296,47 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
     LmRun r{ ctx->lum.as<float>(), stride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
              ctx->stats.as<svf_texel_stats>(), nullptr, nullptr, nullptr, nullptr, nullptr, T };
     SVF_TRY(zero_error_flags(ctx));
-    SVF_TRY(run_lm(ctx, lay, opts, r));
+    const uint32_t n = opts->downsample_light_view;
+    DevBuf d_pairs, d_sub;
+    if(n >= 2 && n < L)
+    {
+        // DownsampleLightView: the n x n pairs of the kept directions, fitted on
+        // their own layout (svbrdf-lsq-fitting-setup.cc:314-330)
+        std::vector<uint32_t> idx(n);
+        if(!svf::downsample_light_view(L, n, idx.data()))
+            return fail(SVF_EINVAL, "downsample_light_view %u of %u directions: no draw", n, L);
+        std::vector<float> sub_lp(2 * (size_t)n);
+        std::vector<uint32_t> pairs((size_t)n * n);
+        for(uint32_t k = 0; k < n; ++k)
+        {
+            sub_lp[2 * k] = lay->lp[2 * idx[k]];
+            sub_lp[2 * k + 1] = lay->lp[2 * idx[k] + 1];
+            for(uint32_t l = 0; l < n; ++l)
+                pairs[(size_t)k * n + l] = idx[k] * L + idx[l];
+        }
+        Layout* sub = nullptr;
+        SVF_TRY(get_layout(ctx, sub_lp.data(), n, &sub));
+        const uint64_t sstride = round_up((uint64_t)n * n, 8);
+        SVF_TRY(upload(d_pairs, pairs));
+        SVF_TRY(d_sub.ensure(sizeof(float) * sstride * T));
+        SVF_CUDA(svf::launch_gather_pairs(ctx->lum.as<float>(), stride, d_pairs.as<uint32_t>(), n * n, T,
+                                          d_sub.as<float>(), sstride, ctx->stream));
+        LmRun rs = r;
+        rs.lum = d_sub.p;
+        rs.stride = sstride;
+        SVF_TRY(run_lm(ctx, sub, opts, rs));
+        // the RMSE the reference reports: all L x L pairs at the fitted parameters,
+        // Fresnel 1 (svbrdf-lsq-fitting-setup.cc:403-421)
+        svf_lsq_options full = *opts;
+        full.max_iterations = 0;
+        full.fresnel = 1.0f;
+        LmRun rf = r;
+        rf.init = ctx->out.as<float>();
+        rf.stats = nullptr;
+        SVF_TRY(launch_lm(ctx, lay, &full, rf, lm_choice(lay, stride, false)));
+    }
+    else
+        SVF_TRY(run_lm(ctx, lay, opts, r));
     SVF_CUDA(cudaMemcpyAsync(out, ctx->out.p, sizeof(float) * 7 * T, cudaMemcpyDefault, ctx->stream));
     SVF_CUDA(cudaMemcpyAsync(rmse, ctx->rmse.p, sizeof(float) * T, cudaMemcpyDefault, ctx->stream));
     if(stats)
@@ -1336,6 +1403,9 @@ svf_status svf_lsq_fit_batch_noalloc(const float* lp, uint32_t L, const float* l
     cfg.fresnel = opts->fresnel;
     cfg.restarts = opts->restarts;
     cfg.step_per_param = (opts->flags & SVF_LSQ_STEP_PER_PARAMETER) ? 1u : 0u;
+    lm_masks(opts, cfg);
+    if(opts->downsample_light_view)
+        return fail(SVF_EINVAL, "svf_lsq_fit_batch_noalloc: downsample_light_view must be 0");
     uint32_t flags[2] = { 0, 0 };
     SVF_CUDA(svf::launch_lm_fit_noalloc(lp, L, lum, lum_stride, texels, cfg, init, out, rmse, stats,
                                         static_cast<cudaStream_t>(stream), flags));

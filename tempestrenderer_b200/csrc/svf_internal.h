@@ -19,6 +19,8 @@ struct LmConfig
     float    fresnel;
     uint32_t restarts;     // continuations from a stop point with fresh damping
     uint32_t step_per_param;   // the small-step test per parameter (SVF_LSQ_STEP_PER_PARAMETER)
+    uint32_t fixed_mask;       // parameters held at their initial values (bits of the parameter index)
+    uint32_t zero_mask;        // parameters set to 0 before the fit (with fixed_mask: not fitted)
 };
 
 // A run of texels of one direction layout in an LM launch: texels
@@ -119,6 +121,10 @@ cudaError_t launch_luminance(const void* samples, uint32_t sample_type, uint64_t
                              const uint16_t* hilo_pos, cudaStream_t stream, void* rgb16 = nullptr,
                              uint64_t rgb_stride = 0,
                              const LumFeatures& features = LumFeatures{});
+
+// dst[t][j] = src[t][pairs[j]] for j < n_pairs, 0 up to dst_stride.
+cudaError_t launch_gather_pairs(const float* src, uint64_t src_stride, const uint32_t* pairs, uint32_t n_pairs,
+                                uint64_t texels, float* dst, uint64_t dst_stride, cudaStream_t stream);
 
 // The RGB fit's initial parameters {kd rgb, ks rgb, sx, sy, quaternion xyzw}
 // from a luminance initial guess {sx, sy, ks, kd, euler} and the texel's

@@ -318,6 +318,15 @@ __global__ void __launch_bounds__(kLumThreads) luminance_kernel(const T* __restr
         texel_features(y, st, feat, t, fv);
 }
 
+__global__ void gather_pairs_kernel(const float* __restrict__ src, uint64_t src_stride,
+                                    const uint32_t* __restrict__ pairs, uint32_t n_pairs, float* __restrict__ dst,
+                                    uint64_t dst_stride)
+{
+    const uint64_t t = blockIdx.x;
+    for(uint32_t j = threadIdx.x; j < dst_stride; j += blockDim.x)
+        dst[t * dst_stride + j] = j < n_pairs ? src[t * src_stride + pairs[j]] : 0.0f;
+}
+
 __global__ void repack_kernel(const float* __restrict__ src, uint64_t src_stride, uint32_t N, float* __restrict__ dst,
                               uint64_t dst_stride)
 {
@@ -626,6 +635,17 @@ cudaError_t noalloc_scratch_address(void** out)
     return cudaSuccess;
 }
 } // namespace
+
+cudaError_t launch_gather_pairs(const float* src, uint64_t src_stride, const uint32_t* pairs, uint32_t n_pairs,
+                                uint64_t texels, float* dst, uint64_t dst_stride, cudaStream_t stream)
+{
+    if(texels == 0)
+        return cudaSuccess;
+    if(texels > 0x7fffffffull || dst_stride < n_pairs)
+        return cudaErrorInvalidValue;
+    gather_pairs_kernel<<<(unsigned)texels, 256, 0, stream>>>(src, src_stride, pairs, n_pairs, dst, dst_stride);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_lm_fit_noalloc(const float* lights_parabolic, uint32_t L, const float* lum, uint64_t lum_stride,
                                   uint32_t texels, const LmConfig& cfg, const float* init, float* out, float* rmse,

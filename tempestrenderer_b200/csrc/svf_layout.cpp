@@ -528,4 +528,48 @@ void build_init_host_tables(InitHostTables& t)
     }
 }
 
+// MurmurHash3's 32-bit finaliser (fmix32), the reference's Hash32
+// (functions.hh:220-229).
+static uint32_t fmix32(uint32_t h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+bool downsample_light_view(uint32_t L, uint32_t n, uint32_t* idx)
+{
+    // DownsampleLightView (svbrdf-lsq-fitting-setup.cc:129-163): direction k of
+    // n is drawn in [ceil(r k), ceil(r (k + 1))), r = (L - 1) / (n - 1), by
+    // FastRandRange (min + Hash32(seed) % (max - min), seed 42 carried along),
+    // redrawn while it repeats the previous draw
+    if(n < 2 || n >= L)
+        return false;
+    const float step = (float)(L - 1) / (float)(n - 1);
+    uint32_t last = ~0u, lo = 0, seed = 42;
+    for(uint32_t k = 0; k < n; ++k)
+    {
+        const uint32_t c = (uint32_t)std::ceil(step * (float)(k + 1));
+        const uint32_t hi = c < L ? c : L;
+        if(hi <= lo)
+            return false;
+        uint32_t s;
+        uint32_t guard = 0;
+        do
+        {
+            seed = fmix32(seed);
+            s = lo + seed % (hi - lo);
+            if(++guard > 1000000u)
+                return false;   // (one value in range and it repeats the last: the reference would not end)
+        } while(s == last);
+        last = s;
+        idx[k] = s;
+        lo = hi;
+    }
+    return true;
+}
+
 } // namespace svf

@@ -53,4 +53,9 @@ struct InitHostTables
 
 void build_init_host_tables(InitHostTables& tables);
 
+// The directions DownsampleLightView keeps (svbrdf-lsq-fitting-setup.cc:129-163):
+// n of L (2 <= n < L), one pseudo-randomly drawn per stride of (L - 1)/(n - 1).
+// False when the draw cannot proceed (an empty stride).
+bool downsample_light_view(uint32_t L, uint32_t n, uint32_t* idx);
+
 } // namespace svf

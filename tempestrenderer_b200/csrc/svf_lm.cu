@@ -160,6 +160,8 @@ struct LmState
     double lam, nu, rho;
     double damp_scale;      // of the initial damping (1: the reference's rule)
     uint32_t iter, eff, njac, nres, status, restarts_left;
+    uint32_t fixed;         // parameters held (the reference's fit_params_count below 7 and its
+                            // specular-only parameter set): no step, no share in the tests
 };
 
 // Fresh damping from the current normal equations (fitting.hh:531-538), times
@@ -170,7 +172,8 @@ __device__ __forceinline__ void lm_reset_damping(LmState<P>& st)
     double damping = 1.0;   // InitialMinDamping
 #pragma unroll
     for(int i = 0; i < P; ++i)
-        damping = fmax(damping, st.H[hix<P>(i, i)]);
+        if(!(st.fixed & (1u << i)))
+            damping = fmax(damping, st.H[hix<P>(i, i)]);
     st.lam = damping * 0.75 * st.damp_scale;   // InitialDampingMultiplier
     st.nu = 2.0;               // DampingFailureMultiplier
 }
@@ -200,7 +203,7 @@ template <int P, int B>
 __device__ __noinline__ bool lm_solve(LmState<P>& st)
 {
     constexpr int kH = P * (P + 1) / 2;
-    uint32_t frozen = 0;
+    uint32_t frozen = st.fixed;
     for(int round = 0; round < 5; ++round)
     {
         double A[kH], x[P];
@@ -214,7 +217,7 @@ __device__ __noinline__ bool lm_solve(LmState<P>& st)
             x[i] = st.g[i];
         }
 #pragma unroll
-        for(int i = 0; i < B; ++i)
+        for(int i = 0; i < P; ++i)
             if(frozen & (1u << i))
             {
 #pragma unroll
@@ -329,6 +332,8 @@ __device__ int lm_next(LmState<M::P>& st, const LmConfig& cfg, double n_pairs)
 #pragma unroll
         for(int i = 0; i < M::P; ++i)
         {
+            if(st.fixed & (1u << i))
+                continue;   // (the reference's vectors hold the fitted parameters only)
             step2 += st.d[i] * st.d[i];
             const double t = st.p[i] + cfg.eps;   // (an RGB rotation entry is 0)
             mag2 += t * t;
@@ -424,7 +429,7 @@ __device__ int lm_after_jacobian(LmState<P>& st, const LmConfig& cfg, const doub
 #pragma unroll
     for(int i = 0; i < P; ++i)
     {
-        st.g[i] = -hg[kH + i];
+        st.g[i] = (st.fixed & (1u << i)) ? 0.0 : -hg[kH + i];
         glen += st.g[i] * st.g[i];
     }
 #pragma unroll
@@ -1521,9 +1526,16 @@ __device__ __forceinline__ bool slot_start(const LmArgs& args, Slot<M>& sl)
             st.q[i] = n > 0.0 ? st.q[i] * n : (i == 3 ? 1.0 : 0.0);
     }
     else
+    {
 #pragma unroll
         for(int i = 0; i < M::P; ++i)
-            st.p[i] = (double)in[i];
+        {
+            if(args.cfg.zero_mask & (1u << i))
+                sl.pf[i] = 0.0f;
+            st.p[i] = (double)sl.pf[i];
+        }
+    }
+    st.fixed = M::kRgb ? 0u : args.cfg.fixed_mask;
     st.iter = st.eff = st.njac = st.nres = st.status = 0;
     st.restarts_left = args.cfg.restarts;
     st.damp_scale = (double)sl.damping;
@@ -1738,7 +1750,7 @@ __global__ void __launch_bounds__(32 * (NW + 1), kPass == kPassPacked ? 1 : min_
                     st.S = sl.sums[M::kAcc];
 #pragma unroll
                     for(int i = 0; i < M::P; ++i)
-                        st.g[i] = -sl.hg[kH + i];
+                        st.g[i] = (st.fixed & (1u << i)) ? 0.0 : -sl.hg[kH + i];
 #pragma unroll
                     for(int i = 0; i < kH; ++i)
                         st.H[i] = sl.hg[i];

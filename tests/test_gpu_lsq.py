@@ -165,6 +165,6 @@ def test_invalid_arguments(gpu_ctx, golden):
         gpu_ctx.lsq_fit_sggx(lp, lum, np.zeros(7, np.float32), svf.options(fresnel=0.5))
     assert e.value.status == svf.SVF_EINVAL
     o = svf.options()
-    o.flags = 0
+    o.flags |= 1 << 20   # no such option
     with pytest.raises(svf.SvfError):
         gpu_ctx.lsq_fit_sggx(lp, lum, np.zeros(7, np.float32), o)

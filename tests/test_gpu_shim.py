@@ -1,0 +1,67 @@
+"""The drop-in seam, compiled and run: TempestRenderer's own SVBRDFFitPipeline
+(svbrdf-fitting-pipeline.cc, cache + fit, fit():684 calling LeastSquaresFitSGGX)
+linked with oracle/svf_shim.cc -- the LeastSquaresFitSGGX replacement that
+INTEGRATION.md shows a maintainer adding, with the reference's signature
+(svbrdf-fitting.hh:126-127) and the fit done by libsvf.so's svf_lsq_fit_sggx --
+in place of its CPU fitter (oracle/_ref/libtempest_ref_svf.so, oracle/Makefile).
+
+On the golden texels (loaded by the reference's LoadBTF), the reference pipeline
+running through the shim gives:
+* the reference's own default initial guess (the reference code computes it);
+* the GPU's fit of that guess, bit for bit what svf_lsq_fit_sggx returns for it
+  called directly;
+* the output maps the reference assembles from that fit (pipeline.cc:692-697),
+  equal to the maps svf_fit_texels writes from the same initial parameters
+  (SVF_INIT_GIVEN) up to float rounding (its quaternion uses the GPU's sincosf).
+"""
+import numpy as np
+import pytest
+
+import tempestrenderer_b200 as svf
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def shim_fits(oracle_lib, golden):
+    if not oracle_lib.ref_svf_available():
+        pytest.fail("oracle/_ref/libtempest_ref_svf.so is not built (oracle/Makefile target shim)")
+    p = golden["pipeline"]
+    lp = golden["mesh"]["lights_parabolic"]
+    tp = golden["angles"]
+    rgb = np.stack([oracle_lib.synth_render(int(p["seed"]), x, oracle_lib.synth_truth(int(p["seed"]), int(p["mix"]), x),
+                                            lp) for x in range(8)])
+    btf = oracle_lib.RefBTF.from_texels(tp, rgb, lib=oracle_lib.ref_svf())
+    fits = [btf.fit_texel(x) for x in range(8)]
+    lums = [btf.lum_slice(x) for x in range(8)]
+    return rgb, fits, lums
+
+
+def test_shim_pipeline_uses_reference_guess_and_gpu_fit(gpu_ctx, golden, shim_fits):
+    _, fits, lums = shim_fits
+    p = golden["pipeline"]
+    lp = golden["mesh"]["lights_parabolic"]
+    for x, (r, (lum, _)) in enumerate(zip(fits, lums)):
+        # the pipeline's default initial guess is the reference's (the golden run's)
+        assert np.array_equal(r["init"], p["init"][x]), x
+        # its fit is svf_lsq_fit_sggx's for that guess, bit for bit
+        out, rmse, st = gpu_ctx.lsq_fit_sggx(lp, lum, r["init"])
+        assert np.array_equal(r["fit"], out), (x, r["fit"], out)
+        assert np.float32(r["rmse"]) == np.float32(rmse)
+        assert r["iterations"] == st.iterations and r["effective"] == st.effective
+
+
+def test_shim_pipeline_maps_equal_gpu_maps(gpu_ctx, golden, shim_fits):
+    rgb, fits, _ = shim_fits
+    m = golden["mesh"]
+    lay = svf.Layout(m["lights_parabolic"], m["triangles"], m["edges"], m["edge_angles"])
+    init = np.stack([r["init"] for r in fits]).astype(np.float32)
+    maps, rs = gpu_ctx.fit_texels(lay, np.ascontiguousarray(rgb), 8, 1, init=init)
+    assert rs.failed_texels == 0
+    for x, r in enumerate(fits):
+        ref = r["maps"]   # sigma xy, quaternion xyzw, diffuse rgb, specular rgb
+        np.testing.assert_array_equal(maps["params"][x], r["fit"])
+        np.testing.assert_array_equal(maps["sigma"][x], ref[0:2])
+        np.testing.assert_allclose(maps["basis"][x], ref[2:6], rtol=0, atol=2e-6)
+        np.testing.assert_allclose(maps["diffuse"][x], ref[6:9], rtol=2e-6, atol=1e-8)
+        np.testing.assert_allclose(maps["specular"][x], ref[9:12], rtol=2e-6, atol=1e-8)
