@@ -55,9 +55,9 @@ FLOPS_RESIDUAL_PASS = 33
 # capture (dram__bytes_read.sum + dram__bytes_write.sum = 675.3 MB + 6.6 MB for
 # 25600 texels; the luminance slab is read once).
 LM_DRAM_BYTES_PER_TEXEL = (675.3e6 + 6.6e6) / 25600
-# DRAM bytes per texel of ndf_tc_kernel, measured by ncu on the same capture
-# (2.30 GB + 335 MB for 25600 texels).
-NDF_DRAM_BYTES_PER_TEXEL = (2.30e9 + 335e6) / 25600
+# DRAM bytes per texel of ndf_tc_kernel over the operator's non-empty tiles,
+# measured by ncu on the same case (1.95 GB + 332 MB for 25600 texels).
+NDF_DRAM_BYTES_PER_TEXEL = (1.95e9 + 332e6) / 25600
 NDF_ROWS, NDF_ROWS_PAD = 3217, 3328   # 64x64 NDF texels inside the hemisphere, padded to the tile
 
 
@@ -538,7 +538,12 @@ def btf_file_item(svf, ctx, layout, W, H, steps, dev, K=48):
         btf.decode(out=out)
     torch.cuda.synchronize()
     dec_s = (time.perf_counter() - t0) / steps
-    del out
+    # the fit alone on the decoded samples resident in HBM: the same texels as svf_fit_btf fits
+    dmaps = {k: torch.zeros(sh, dtype=torch.float32, device=dev) for k, sh in
+             {"rmse": (T,), "diffuse": (T, 3), "specular": (T, 3), "sigma": (T, 2), "basis": (T, 4)}.items()}
+    ctx.fit_texels(layout, out, T, 1, want=tuple(dmaps), out=dmaps, check=False)
+    rs_res = ctx.fit_texels(layout, out, T, 1, want=tuple(dmaps), out=dmaps, check=False)[1]
+    del out, dmaps
     torch.cuda.empty_cache()
     want = ("diffuse", "specular", "sigma", "basis", "rmse")
     btf.fit(layout=layout, want=want, check=False)
@@ -556,8 +561,14 @@ def btf_file_item(svf, ctx, layout, W, H, steps, dev, K=48):
                                "runs 2 instructions per product"},
             "fit_btf": {"value": T / fit_s, "unit": "texels/s", "seconds": fit_s, "ms_device_fit": rs.ms_total,
                         "failed_texels": int(rs.failed_texels), "mean_rmse": float(maps["rmse"].mean()),
+                        "mean_iterations": rs.iterations / T,
                         "note": "host wall time of svf_fit_btf (decode into FP32 chunks + the fit pipeline); "
-                                "maps copied to host"}}
+                                "maps copied to host"},
+            "fit_of_decoded_samples_in_hbm": {"value": T / (rs_res.ms_total / 1e3), "unit": "texels/s",
+                                              "ms": rs_res.ms_total, "mean_iterations": rs_res.iterations / T,
+                                              "note": "svf_fit_texels on the decoded samples: these texels are "
+                                                      "mixtures of 48 prototypes, which the one-lobe model fits in "
+                                                      "more LM iterations than the synthetic one-lobe texels"}}
 
 
 def summarize(line, parity):

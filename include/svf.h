@@ -257,7 +257,7 @@ typedef struct svf_fit_options
     const svf_mlp*  mlp;           /* SVF_INIT_MLP: a model trained for the BTF's direction layout */
     float           initial_damping;  /* LM's first damping as a multiple of the reference's rule
                                          (0.75 max(1, max diag J^T J), fitting.hh:531-538).  0: that
-                                         rule, except 1e-3 of it from the learned guess, which starts
+                                         rule, except 1e-4 of it from the learned guess, which starts
                                          near a minimum where the full damping takes steps below
                                          BreakOnSmallStep and ends the fit early.  No reference
                                          counterpart. */

@@ -280,7 +280,8 @@ struct svf_ctx
     std::unique_ptr<svf::InitHostTables> tables;
     DevBuf lum, lum_hi, lum_lo, avg, ndf, ndf_tex, init, out, rmse, stats, counter, error, samples, samples2,
         maps_buf, scratch, rgb16, init_rgb, mlp_x, mlp_h1, mlp_h2, mlp_y, fb_idx, fb_lum, fb_hi, fb_lo, fb_ndf,
-        fb_small;
+        fb_small,
+        btf_decoded /* svf_fit_btf: the decoded chunk, kept between calls */;
     PinnedBuf pinned;
 };
 
@@ -560,7 +561,7 @@ svf_status check_ctx(svf_ctx* ctx)
 // the learned guess starts close to a minimum, where the reference's damping
 // (sized for its default guess) takes steps below BreakOnSmallStep and stops
 // the fit early; it starts lighter unless the caller says otherwise.
-constexpr float kMlpInitialDamping = 1e-3f;
+constexpr float kMlpInitialDamping = 1e-4f;
 float initial_damping(const svf_fit_options& o)
 {
     if(o.initial_damping > 0.0f)
@@ -2970,7 +2971,7 @@ svf_status svf_fit_btf(svf_ctx* ctx, const svf_btf* btf, const svf_layout_desc* 
     // the decoded chunk takes a quarter of the free memory; the fit's own
     // buffers grow within the rest
     const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(T, free_b / 4 / texel_bytes));
-    DevBuf buf;
+    DevBuf& buf = ctx->btf_decoded;   // (kept: a fresh 10 GB buffer per call costs more than the decode)
     SVF_TRY(buf.ensure(texel_bytes * chunk));
     const uint32_t kout = (opts->lsq.flags & SVF_LSQ_RGB) ? 12 : 7;
     svf_run_stats all{};
