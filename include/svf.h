@@ -70,6 +70,11 @@ typedef enum svf_status
 #define SVF_LSQ_DISABLE_DIRECTION_FITTING (1u << 2)   /* LSF_OPTION_DISABLE_DIRECTION_FITTING: the Euler
                                             angles are held at their initial values
                                             (svbrdf-lsq-fitting-setup.cc:265-268) */
+#define SVF_LSQ_FIT_TOP      (1u << 4)   /* LSF_OPTION_FIT_TOP (svf_lsq_fit_sggx / svf_lsq_fit_batch only):
+                                            fit the L samples of the top-most view (the direction nearest
+                                            the pole), modelled as seen from direction 0 as the
+                                            reference's evaluator sees them; RMSE over all L x L pairs at
+                                            Fresnel 1 (svbrdf-lsq-fitting-setup.cc:289-313,403-421) */
 /* The RGB fit (no counterpart in the reference, which fits the luminance and
  * colours the maps with the average chromaticity): 11 parameters per texel,
  * {kd rgb, ks rgb, sx, sy} plus the orientation, fitted to the three channels

@@ -433,6 +433,7 @@ def _bind_harness(L):
 
 LSF_OPTON_DIFFUSE = 1 << 1
 LSF_OPTION_DISABLE_DIRECTION_FITTING = 1 << 2
+LSF_OPTION_FIT_TOP = 1 << 4
 
 
 class RefBTF:

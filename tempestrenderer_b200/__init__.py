@@ -29,6 +29,7 @@ SVF_LSQ_DIFFUSE = 1 << 1
 SVF_LSQ_RGB = 1 << 8
 SVF_LSQ_STEP_PER_PARAMETER = 1 << 9
 SVF_LSQ_DISABLE_DIRECTION_FITTING = 1 << 2
+SVF_LSQ_FIT_TOP = 1 << 4
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
 SVF_ERROR_PAIRWISE, SVF_ERROR_MAX_VIEW = 0, 1
@@ -192,7 +193,7 @@ def _check(status: int):
 
 def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | None = None,
             rgb: bool = False, step_per_parameter: bool = True, diffuse: bool = True,
-            fit_direction: bool = True, downsample: int = 0) -> LsqOptions:
+            fit_direction: bool = True, downsample: int = 0, fit_top: bool = False) -> LsqOptions:
     """LM options; rgb selects the 11-parameter RGB fit (svf_fit_texels / svf_fit_btfs);
     step_per_parameter=False restores the reference's whole-vector small-step test;
     diffuse=False the specular-only fit, fit_direction=False holds the Euler angles,
@@ -206,6 +207,8 @@ def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | No
         o.flags &= ~SVF_LSQ_DIFFUSE
     if not fit_direction:
         o.flags |= SVF_LSQ_DISABLE_DIRECTION_FITTING
+    if fit_top:
+        o.flags |= SVF_LSQ_FIT_TOP
     if rgb:
         o.flags |= SVF_LSQ_RGB
     if not step_per_parameter:

@@ -573,14 +573,16 @@ svf_status check_options(const svf_lsq_options* o, bool downsample_ok = false)
 {
     if(!o)
         return fail(SVF_EINVAL, "null options");
+    if((o->flags & SVF_LSQ_FIT_TOP) && (!downsample_ok || (o->flags & SVF_LSQ_RGB)))
+        return fail(SVF_EINVAL, "SVF_LSQ_FIT_TOP is taken by svf_lsq_fit_sggx / svf_lsq_fit_batch (luminance fit)");
     if(o->downsample_light_view == 1 || (o->downsample_light_view && !downsample_ok) ||
        (o->downsample_light_view && (o->flags & SVF_LSQ_RGB)))
         return fail(SVF_EINVAL, "downsample_light_view %u: 0, or 2 and more with svf_lsq_fit_sggx / svf_lsq_fit_batch",
                     o->downsample_light_view);
     if((o->flags & SVF_LSQ_RGB) && (o->flags & SVF_LSQ_DISABLE_DIRECTION_FITTING || !(o->flags & SVF_LSQ_DIFFUSE)))
         return fail(SVF_EINVAL, "the RGB fit (SVF_LSQ_RGB) fits every parameter, with the diffuse term");
-    constexpr uint32_t known =
-        SVF_LSQ_DIFFUSE | SVF_LSQ_RGB | SVF_LSQ_STEP_PER_PARAMETER | SVF_LSQ_DISABLE_DIRECTION_FITTING;
+    constexpr uint32_t known = SVF_LSQ_DIFFUSE | SVF_LSQ_RGB | SVF_LSQ_STEP_PER_PARAMETER |
+                               SVF_LSQ_DISABLE_DIRECTION_FITTING | SVF_LSQ_FIT_TOP;
     if(o->flags & ~known)
         return fail(SVF_EINVAL, "unknown lsq flags 0x%x", o->flags & ~known);
     if(!(o->fresnel >= 1.0f) || !std::isfinite(o->fresnel))
@@ -1080,6 +1082,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     a.cfg.fresnel = o->fresnel;
     a.cfg.restarts = o->restarts;
     a.cfg.step_per_param = (o->flags & SVF_LSQ_STEP_PER_PARAMETER) ? 1u : 0u;
+    a.cfg.row_fit = (o->flags & SVF_LSQ_FIT_TOP) ? 1u : 0u;
     lm_masks(o, a.cfg);
     SVF_TRY(ctx->counter.ensure(16));
     SVF_TRY(ctx->error.ensure(16));
@@ -1299,7 +1302,44 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
     SVF_TRY(zero_error_flags(ctx));
     const uint32_t n = opts->downsample_light_view;
     DevBuf d_pairs, d_sub;
-    if(n >= 2 && n < L)
+    if(opts->flags & SVF_LSQ_FIT_TOP)
+    {
+        // the top-most view's row (svbrdf-lsq-fitting-setup.cc:291-305: the first
+        // direction of least parabolic length, from 1 down)
+        uint32_t top = 0;
+        float len = 1.0f;
+        for(uint32_t v = 0; v < L; ++v)
+        {
+            const float px = lay->lp[2 * v], py = lay->lp[2 * v + 1];
+            const float cur = std::sqrt(px * px + py * py);
+            if(cur < len)
+            {
+                len = cur;
+                top = v;
+            }
+        }
+        std::vector<uint32_t> pairs(L);
+        for(uint32_t l = 0; l < L; ++l)
+            pairs[l] = top * L + l;
+        const uint64_t rstride = round_up(L, 8);
+        SVF_TRY(upload(d_pairs, pairs));
+        SVF_TRY(d_sub.ensure(sizeof(float) * rstride * T));
+        SVF_CUDA(svf::launch_gather_pairs(ctx->lum.as<float>(), stride, d_pairs.as<uint32_t>(), L, T,
+                                          d_sub.as<float>(), rstride, ctx->stream));
+        LmRun rr = r;
+        rr.lum = d_sub.p;
+        rr.stride = rstride;
+        SVF_TRY(launch_lm(ctx, lay, opts, rr, lm_choice(lay, rstride, false)));
+        svf_lsq_options full = *opts;
+        full.flags &= ~SVF_LSQ_FIT_TOP;
+        full.max_iterations = 0;
+        full.fresnel = 1.0f;
+        LmRun rf = r;
+        rf.init = ctx->out.as<float>();
+        rf.stats = nullptr;
+        SVF_TRY(launch_lm(ctx, lay, &full, rf, lm_choice(lay, stride, false)));
+    }
+    else if(n >= 2 && n < L)
     {
         // DownsampleLightView: the n x n pairs of the kept directions, fitted on
         // their own layout (svbrdf-lsq-fitting-setup.cc:314-330)
@@ -1404,9 +1444,10 @@ svf_status svf_lsq_fit_batch_noalloc(const float* lp, uint32_t L, const float* l
     cfg.fresnel = opts->fresnel;
     cfg.restarts = opts->restarts;
     cfg.step_per_param = (opts->flags & SVF_LSQ_STEP_PER_PARAMETER) ? 1u : 0u;
+    cfg.row_fit = 0;
     lm_masks(opts, cfg);
-    if(opts->downsample_light_view)
-        return fail(SVF_EINVAL, "svf_lsq_fit_batch_noalloc: downsample_light_view must be 0");
+    if(opts->downsample_light_view || (opts->flags & SVF_LSQ_FIT_TOP))
+        return fail(SVF_EINVAL, "svf_lsq_fit_batch_noalloc: no downsampling or top-view fit");
     uint32_t flags[2] = { 0, 0 };
     SVF_CUDA(svf::launch_lm_fit_noalloc(lp, L, lum, lum_stride, texels, cfg, init, out, rmse, stats,
                                         static_cast<cudaStream_t>(stream), flags));

@@ -21,6 +21,7 @@ struct LmConfig
     uint32_t step_per_param;   // the small-step test per parameter (SVF_LSQ_STEP_PER_PARAMETER)
     uint32_t fixed_mask;       // parameters held at their initial values (bits of the parameter index)
     uint32_t zero_mask;        // parameters set to 0 before the fit (with fixed_mask: not fitted)
+    uint32_t row_fit;          // slabs hold one view row (L samples): LSF_OPTION_FIT_TOP's fit
 };
 
 // A run of texels of one direction layout in an LM launch: texels

@@ -1104,6 +1104,50 @@ __device__ void worker_pass(const float* tab, const PassConst& c, const typename
         redd[wwarp] = r2;
 }
 
+// The row fit of LeastSquaresFitSGGX's LSF_OPTION_FIT_TOP
+// (svbrdf-lsq-fitting-setup.cc:289-313): the slab holds one view row, the L
+// samples of the top-most view, and the model sees them as the pairs (view 0,
+// light b) -- the reference's evaluator maps sample b < L to view b / L = 0.
+// In sym_pair's terms these are the unordered pairs {0, b} with the second
+// ordered pair weighted 0.  Lanes take the lights b; same outputs as
+// worker_pass.
+template <int NW, bool kFresnel, bool kAllUp>
+__device__ void worker_pass_row(const float* tab, const PassConst& c, const float* row, uint32_t L, float refr,
+                                float* red, double* redd, uint32_t wwarp, uint32_t lane)
+{
+    constexpr int kAcc = LumModel::kAcc;
+    constexpr uint32_t kStride = 32u * NW;
+    const uint32_t Lp = pad4(L);
+    double r2 = 0.0;
+    float acc[kAcc];
+#pragma unroll
+    for(int i = 0; i < kAcc; ++i)
+        acc[i] = 0.0f;
+    const Entry ea = load_entry(tab, Lp, 0);
+    const uint32_t iters = (L + kStride - 1) / kStride;
+    for(uint32_t it = 0; it < iters; ++it)
+    {
+        const uint32_t b = it * kStride + wwarp * 32u + lane;
+        const bool valid = b < L;
+        const Entry eb = load_entry(tab, Lp, valid ? b : 0u);
+        sym_pair<kFresnel, kAllUp>(c, ea, eb, refr, valid ? row[b] : 0.0f, 0.0f, valid ? 1.0f : 0.0f, 0.0f, acc, r2);
+    }
+    r2 = warp_sum(r2);
+    float rest[kAcc - 32];
+#pragma unroll
+    for(int i = 32; i < kAcc; ++i)
+        rest[i - 32] = warp_sum(acc[i]);
+    reduce_scatter32(acc, lane);
+    red[wwarp * kAcc + lane] = acc[0];
+    if(lane == 0)
+    {
+#pragma unroll
+        for(int i = 32; i < kAcc; ++i)
+            red[wwarp * kAcc + i] = rest[i - 32];
+        redd[wwarp] = r2;
+    }
+}
+
 // Advances an unordered pair (f, a, d) by one worker stride (sa, sd): f += 32 NW.
 __device__ __forceinline__ void pair_advance(uint32_t stride, uint32_t nd, uint32_t sa, uint32_t sd, uint32_t& f,
                                              uint32_t& a, uint32_t& d)
@@ -1465,7 +1509,8 @@ __device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot<M>& sl, void
                 k = i;
         const LmSegment& g = args.seg[k];
         sl.L = g.L;
-        sl.npairs = (double)M::kChannels * (double)g.L * (double)g.L;
+        // (a row fit has one residual per light)
+        sl.npairs = args.cfg.row_fit ? (double)g.L : (double)M::kChannels * (double)g.L * (double)g.L;
         sl.geo = g.geo;
         sl.damping = g.damping > 0.0f ? g.damping : 1.0f;
         sl.slab_bytes = (uint32_t)(g.stride * sizeof(typename M::Slab));
@@ -1663,7 +1708,14 @@ __global__ void __launch_bounds__(32 * (NW + 1), kPass == kPassPacked ? 1 : min_
                 break;
             if(cmd == kSlotPass)
             {
-                if constexpr(kPass == kPassPacked)
+                if(!M::kRgb && args.cfg.row_fit)
+                {
+                    if constexpr(!M::kRgb)
+                        worker_pass_row<NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc,
+                                                              reinterpret_cast<const float*>(slab_of(s)), slots[s].L,
+                                                              args.cfg.fresnel, red_of(s), redd_of(s), wwarp, lane);
+                }
+                else if constexpr(kPass == kPassPacked)
                     worker_pass2<NW, kAllUp>(tab_of(s), slots[s].pc, reinterpret_cast<const float*>(slab_of(s)),
                                              slots[s].L, red_of(s), redd_of(s), wwarp, lane);
                 else if constexpr(kPass == kPassTc)

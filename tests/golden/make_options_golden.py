@@ -11,6 +11,8 @@ ref_pipeline.npz (seed 11, mix 1, ring-81), from perturbed ground truth:
 * down41 -- DownSampleLightView = 41 (svbrdffit -S 41): the 41 x 41 pairs of
   the directions DownsampleLightView keeps (:129-163, :314-330), RMSE over all
   81 x 81 pairs at Fresnel 1 (:403-421);
+* top -- LSF_OPTON_DIFFUSE | LSF_OPTION_FIT_TOP: the 81 samples of the top-most
+  view (:289-313), RMSE over all pairs at Fresnel 1;
 
 and DownsampleLightView's kept directions for n = 20, 41, 60 (dirs_<n>).  (At 81
 directions the reference divides by zero for n = 40, 76 and 79: in float, the
@@ -37,7 +39,8 @@ SEED, MIX, TEXELS = 11, 1, 8
 CASES = {"specular": (0, 0xFFFFFFFF),
          "nodir": (O.LSF_OPTON_DIFFUSE | O.LSF_OPTION_DISABLE_DIRECTION_FITTING, 0xFFFFFFFF),
          "specular_nodir": (O.LSF_OPTION_DISABLE_DIRECTION_FITTING, 0xFFFFFFFF),
-         "down41": (O.LSF_OPTON_DIFFUSE, 41)}
+         "down41": (O.LSF_OPTON_DIFFUSE, 41),
+         "top": (O.LSF_OPTON_DIFFUSE | O.LSF_OPTION_FIT_TOP, 0xFFFFFFFF)}
 
 
 def main():

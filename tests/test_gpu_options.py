@@ -7,12 +7,15 @@ the reference's own fits from the same perturbed ground truth
   values, bit for bit;
 * both;
 * downsample_light_view = 41: the fit of the 41 x 41 pairs of the kept
-  directions, RMSE over all 81 x 81 pairs at Fresnel 1.
+  directions, RMSE over all 81 x 81 pairs at Fresnel 1;
+* SVF_LSQ_FIT_TOP: the fit of the top-most view's 81 samples, RMSE over all
+  pairs at Fresnel 1.
 
 Bar: the RMSE <= 1.01x the reference's + 1e-7 on every texel (a good start, as
 test_gpu_lsq.py's perturbed-truth test).  The downsampled fit reports the RMSE
 over all pairs while it fits a subset, where a small difference in the fitted
-parameters moves the reported RMSE more: there the bar of the default-guess
+parameters moves the reported RMSE more (the same for the top-view fit): there
+the bar of the default-guess
 fits (mean <= 1.01x, at least 3/4 of the texels within 1.01x, none worse than
 1.25x).
 """
@@ -27,7 +30,8 @@ pytestmark = pytest.mark.gpu
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CASES = {"specular": dict(diffuse=False), "nodir": dict(fit_direction=False),
-         "specular_nodir": dict(diffuse=False, fit_direction=False), "down41": dict(downsample=41)}
+         "specular_nodir": dict(diffuse=False, fit_direction=False), "down41": dict(downsample=41),
+         "top": dict(fit_top=True)}
 
 
 @pytest.fixture(scope="module")
@@ -44,7 +48,7 @@ def test_option_against_reference(gpu_ctx, golden, opts_golden, case):
     ref = g[f"{case}_rmse"].astype(np.float64)
     ratio = rmse / ref
     print(case, "GPU / reference RMSE:", np.round(ratio, 4))
-    if "downsample" in CASES[case]:
+    if "downsample" in CASES[case] or "fit_top" in CASES[case]:
         assert rmse.mean() <= 1.01 * ref.mean() and np.mean(ratio <= 1.01) >= 0.75 and ratio.max() <= 1.25, ratio
     else:
         assert (rmse <= 1.01 * ref + 1e-7).all(), np.c_[rmse, ref]
