@@ -26,9 +26,12 @@ CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["svf_kernels.cu", "svf_lm.cu", "svf_init.cu", "svf_ndf_tc.cu", "svf_mlp.cu", "svf_btf.cu",
               "svf_error.cu"]
-CXX_SOURCES = {"svf_host.cpp": ["-O2", "-ffp-contract=off"], "svf_layout.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"],
+CXX_SOURCES = {"svf_host.cpp": ["-O2", "-ffp-contract=off"], "svf_host_init.cpp": ["-O2", "-ffp-contract=off"],
+               "svf_host_lm.cpp": ["-O2", "-ffp-contract=off"], "svf_host_fit.cpp": ["-O2", "-ffp-contract=off"],
+               "svf_host_mlp.cpp": ["-O2", "-ffp-contract=off"], "svf_host_btf.cpp": ["-O2", "-ffp-contract=off"],
+               "svf_layout.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"],
                "svf_btf_file.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "svf_exr.cpp": ["-O2"]}
-HEADERS = ["svf_internal.h", "svf_model.cuh", "svf_layout.h", "svf_btf_file.h"]
+HEADERS = ["svf_internal.h", "svf_host.h", "svf_model.cuh", "svf_layout.h", "svf_btf_file.h"]
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr", "-ccbin", CXX]

@@ -1,4 +1,4 @@
-// svf_internal.h - declarations shared by the host orchestration (svf_host.cpp)
+// svf_internal.h - declarations shared by the host orchestration (svf_host*.cpp)
 // and the CUDA translation units.  Not part of the public ABI.
 #pragma once
 
