@@ -571,6 +571,93 @@ def btf_file_item(svf, ctx, layout, W, H, steps, dev, K=48):
                                                       "more LM iterations than the synthetic one-lobe texels"}}
 
 
+def reference_ms_eval_rate(lp, bounces, threads=None, tasks=None):
+    """The reference's multi-scattering evaluator (oracle/_ref, BRDFEvaluator with
+    BounceCount) on all host threads: pair evaluations per second over `tasks`
+    parameter vectors x all pairs of the layout."""
+    import concurrent.futures as cf
+
+    import oracle
+
+    if not oracle.ref_available():
+        raise RuntimeError("oracle/_ref/libtempest_ref.so is not built")
+    threads = threads or os.cpu_count() or 1
+    tasks = tasks or threads
+    rng = np.random.default_rng(5)
+    params = [np.array([0.05 + 0.4 * rng.random(), 0.05 + 0.4 * rng.random(), 0.5 + rng.random(), 0.2 * rng.random(),
+                        *(0.6 * (rng.random(3) - 0.5))]) for _ in range(tasks)]
+    oracle.ref_brdf_all_ms(params[0], lp[:4], bounces)   # load and bind first
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:   # ctypes calls release the GIL
+        list(ex.map(lambda p: oracle.ref_brdf_all_ms(p, lp, bounces), params))
+    secs = time.perf_counter() - t0
+    return tasks * lp.shape[0] ** 2 / secs, secs, threads
+
+
+def multi_scattering_item(svf, ctx, steps, dev, bounces=2, render_texels=256, fit_texels=64):
+    """The pseudo-volume multi-scattering BRDF (svbrdffit -m) on ring-81: rendering
+    (svf_render_btf_ms) and the SVF_LSQ_MULTI_SCATTERING fit, against the
+    reference's evaluator on the host cores."""
+    import torch
+
+    lp = svf.directions_ring81()
+    N = lp.shape[0] ** 2
+    rng = np.random.default_rng(11)
+    T = render_texels
+    sigma = (0.08 + 0.3 * rng.random((T, 2))).astype(np.float32)
+    quat = rng.standard_normal((T, 4)).astype(np.float32)
+    quat /= np.linalg.norm(quat, axis=1, keepdims=True)
+    kd = (0.2 * rng.random(T)).astype(np.float32)
+    ks = (0.5 + rng.random(T)).astype(np.float32)
+    grey = lambda a: np.repeat(a[:, None], 3, 1)
+    out = torch.zeros((T, N, 3), dtype=torch.float32, device=dev)
+    ctx.render_btf_ms(lp, grey(kd), grey(ks), sigma, quat, bounces, out=out)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        ctx.render_btf_ms(lp, grey(kd), grey(ks), sigma, quat, bounces, out=out)
+    torch.cuda.synchronize()
+    r_s = (time.perf_counter() - t0) / steps
+    # the fit: the first fit_texels rendered texels (grey albedos, Euler angles 0:
+    # the truth is a zero of the model) from a perturbed start
+    F = fit_texels
+    quat0 = np.tile(np.array([0, 0, 0, 1], np.float32), (F, 1))
+    lum_rgb = ctx.render_btf_ms(lp, grey(kd[:F]), grey(ks[:F]), sigma[:F], quat0, bounces)
+    lum = np.ascontiguousarray(lum_rgb[:, :, 0])
+    truth = np.stack([sigma[:F, 0], sigma[:F, 1], ks[:F], kd[:F], np.zeros(F), np.zeros(F), np.zeros(F)], 1)
+    init = (truth * (1 + 0.2 * rng.standard_normal((F, 7)))).astype(np.float32)
+    init[:, :4] = np.abs(init[:, :4]) + 1e-3
+    init[:, 4:] = 0.05 * rng.standard_normal((F, 3))
+    opts = svf.options(multi_scattering=bounces)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    fo, fr, fst = ctx.lsq_fit_batch(lp, lum, init, opts)
+    torch.cuda.synchronize()
+    f_s = time.perf_counter() - t0
+    r0 = ctx.lsq_fit_batch(lp, lum, init, svf.options(max_iterations=0, multi_scattering=bounces))[1]
+    evals_per_texel = float((14 * fst["jacobians"] + fst["residuals"]).mean()) * N
+    item = {"workload": f"ring-81 (6561 pairs), {bounces} bounces, 256 walks per evaluation (the fitter's evaluator)",
+            "render": {"value": T * N / r_s, "unit": "pair evaluations/s", "texels": T, "ms": r_s * 1e3,
+                       "texels_per_s": T / r_s, "note": "svf_render_btf_ms into device memory, RGB"},
+            "fit": {"value": F / f_s, "unit": "texels/s", "texels": F, "seconds": f_s,
+                    "mean_iterations": float(fst["iterations"].mean()),
+                    "mean_jacobians": float(fst["jacobians"].mean()),
+                    "mean_residual_evaluations": float(fst["residuals"].mean()),
+                    "evaluations_per_texel": evals_per_texel, "evaluations_per_s": F * evals_per_texel / f_s,
+                    "mean_rmse_start": float(r0.mean()), "mean_rmse": float(fr.mean()),
+                    "note": "host wall time of svf_lsq_fit_batch (SVF_LSQ_MULTI_SCATTERING), slices on the host"}}
+    try:
+        rate, secs, thr = reference_ms_eval_rate(lp, bounces)
+        item["reference_cpu"] = {"value": rate, "unit": "pair evaluations/s", "cores": thr, "seconds": secs,
+                                 "kind": "reference",
+                                 "fit_texels_per_s_estimate": rate / evals_per_texel,
+                                 "sample": f"{thr} parameter vectors x 6561 pairs on {thr} threads; the fit estimate "
+                                           f"divides by the GPU fit's evaluations per texel (the same LM)"}
+    except Exception as e:  # the checker may be absent on a box without it built
+        item["reference_cpu"] = {"value": None, "sample": f"unavailable: {e}"}
+    return item
+
+
 def summarize(line, parity):
     """The line items' headline figures in a few short keys."""
     def r3(x):
@@ -596,6 +683,13 @@ def summarize(line, parity):
     f = line.get("fib151_768x768")
     if f:
         out["config2"] = {"texels_per_s": r3(f["value"]), "fp64_check": f.get("fp64_check_summary")}
+    m = line.get("multi_scattering")
+    if m:
+        ref = m.get("reference_cpu") or {}
+        out["multi_scattering"] = {"render_evals_per_s": r3(m["render"]["value"]),
+                                   "fit_texels_per_s": r3(m["fit"]["value"]),
+                                   "reference_cpu_evals_per_s": r3(ref.get("value")),
+                                   "reference_fit_texels_per_s_estimate": r3(ref.get("fit_texels_per_s_estimate"))}
     return out
 
 
@@ -754,6 +848,11 @@ def run_ours(args):
         with svf.Context(local) as c2:
             batch = batch_item(svf, c2, args.batch_steps, dev)
         torch.cuda.empty_cache()
+    ms_item = None
+    if world == 1 and args.ms_steps > 0:
+        with svf.Context(local) as c2:
+            ms_item = multi_scattering_item(svf, c2, args.ms_steps, dev)
+        torch.cuda.empty_cache()
 
     if rank == 0:
         props = torch.cuda.get_device_properties(dev)
@@ -815,7 +914,8 @@ def run_ours(args):
                         "failed_texels": failed, "mean_rmse": float(head_rmse.mean()),
                         "median_rmse": float(np.median(head_rmse)), "ground_truth_error": head_truth_err},
             "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "learned_init": learned, "fib151_768x768": fib,
-            "batch_8_btfs": batch, "btf_file": btf_file, "refit_neighborhood": refit, "gpu_launches": 4 * args.steps,
+            "batch_8_btfs": batch, "btf_file": btf_file, "refit_neighborhood": refit, "multi_scattering": ms_item,
+            "gpu_launches": 4 * args.steps,
             "wall_s": wall, "cpu_baseline": cpu,
         }
         # short summaries last, so that a reader of the line's tail sees them
@@ -842,6 +942,8 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=1, help="calls of the 8-BTF batch line item (0: skip)")
     ap.add_argument("--btf-steps", type=int, default=3, help="decodes of the DFMF-file line item (0: skip)")
     ap.add_argument("--refit-steps", type=int, default=1, help="runs of the neighbourhood-refit line item (0: skip)")
+    ap.add_argument("--ms-steps", type=int, default=1,
+                    help="renders of the multi-scattering line item, which also times one fit (0: skip)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":

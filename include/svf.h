@@ -44,7 +44,7 @@
 extern "C" {
 #endif
 
-#define SVF_ABI_VERSION 3u
+#define SVF_ABI_VERSION 4u
 
 typedef enum svf_status
 {
@@ -94,6 +94,18 @@ typedef enum svf_status
  * itself, where the residual is steep.  Set by svf_lsq_options_default; clear
  * it for the reference's test. */
 #define SVF_LSQ_STEP_PER_PARAMETER (1u << 9)
+/* The multi-scattering model (LeastSquaresFitOptions::MultiScatteringBounceCount
+ * != ~0u, svbrdffit -m; svf_lsq_fit_sggx / svf_lsq_fit_batch, with
+ * SVF_LSQ_DIFFUSE and none of the other options): the fit's BRDF is the
+ * pseudo-volume SGGXMicroFlakePseudoVolumeBRDF (ggx-models-impl.hh:621-758; 256
+ * random walks of at most multi_scattering_bounces events per evaluation, the
+ * evaluator's LCG seed 0; Fresnel is not part of it), fitted by the reference's
+ * LevenbergMarquardtCurveFit as written (fitting.hh:457-678: the central-
+ * difference Jacobian of fitting.hh:883-908, the whole-vector small-step test,
+ * no restarts); the RMSE is over all pairs.  Each evaluation runs its walks in
+ * order, as their random numbers follow one another: a fit costs about
+ * 15 L^2 x 256 x bounces walk steps per iteration. */
+#define SVF_LSQ_MULTI_SCATTERING (1u << 10)
 
 typedef struct svf_lsq_options
 {
@@ -111,6 +123,9 @@ typedef struct svf_lsq_options
                                      picks, and report the RMSE over all L x L pairs at Fresnel 1
                                      (svbrdf-lsq-fitting-setup.cc:314-330,403-421).  0 = off
                                      (the default); the texel-loop entry points take 0 only. */
+    uint32_t multi_scattering_bounces; /* MultiScatteringBounceCount with SVF_LSQ_MULTI_SCATTERING:
+                                     the walk depth (0 = the pseudo volume's single-scattering
+                                     term only).  Default 2. */
 } svf_lsq_options;
 
 typedef struct svf_texel_stats
@@ -482,6 +497,18 @@ svf_status svf_refit_neighborhood(svf_ctx* ctx, const svf_btf_view* btf, const s
  * inverse of the fit: fitting the rendered BTF recovers the maps. */
 svf_status svf_render_btf(svf_ctx* ctx, const float* lights_parabolic, uint32_t light_count,
                           const svf_svbrdf_maps* maps, float fresnel, uint32_t sample_type, void* samples);
+
+/* Rendered BTF of SVBRDF maps with the pseudo-volume multi-scattering BRDF
+ * (SGGXMicroFlakePseudoVolumeBRDF, ggx-models-impl.hh:621-758) in RGB: per
+ * pair, `samples` random walks of at most `bounces` scattering events from LCG
+ * state `seed` (the fitter's evaluator: 256 walks, seed 0, which is what the
+ * SVF_LSQ_MULTI_SCATTERING fit models), the walk continuing while every
+ * channel's throughput is above 1e-3; the basis quaternion is used as stored
+ * (unnormalised, as the pseudo-volume BRDF takes it).  Layout and sample types as
+ * svf_render_btf. */
+svf_status svf_render_btf_ms(svf_ctx* ctx, const float* lights_parabolic, uint32_t light_count,
+                             const svf_svbrdf_maps* maps, uint32_t bounces, uint32_t samples, uint32_t seed,
+                             uint32_t sample_type, void* samples_out);
 
 /* OpenEXR maps ----------------------------------------------------------------------
  * svbrdffit's output files (svbrdf-fitting.cc:713-735, SaveEXRImage in

@@ -81,9 +81,15 @@ def lib():
         L.svfo_brdf_f64.argtypes = [_f64p, _f32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_double]
         L.svfo_brdf_f64.restype = C.c_double
         L.svfo_brdf_eval_all.argtypes = [_f64p, _f32p, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p]
+        L.svfo_brdf_ms_eval_all.argtypes = [_f64p, _f32p, C.c_uint32, C.c_uint32, _f32p]
+        L.svfo_pseudo_volume_rgb.argtypes = [_f32p, _f32p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                             C.c_uint32, _f32p]
         L.svfo_lsq_fit.argtypes = [_f32p, _f32p, C.c_uint32, C.c_float, C.c_uint32, _f32p, _f32p,
                                    C.POINTER(LsqStats)]
         L.svfo_lsq_fit.restype = C.c_float
+        L.svfo_lsq_fit_ms.argtypes = [_f32p, _f32p, C.c_uint32, C.c_uint32, C.c_uint32, _f32p, _f32p,
+                                      C.POINTER(LsqStats)]
+        L.svfo_lsq_fit_ms.restype = C.c_float
         L.svfo_lum_slice.argtypes = [_f32p, C.c_uint32, _f32p, _f32p]
         L.svfo_sample_lum.argtypes = [C.POINTER(Mesh), _f32p, _f32p, _f32p]
         L.svfo_sample_lum.restype = C.c_float
@@ -124,6 +130,36 @@ def brdf_all(params7, lights_parabolic, fresnel=1.0):
     f64 = np.zeros(L * L, np.float64)
     lib().svfo_brdf_eval_all(p, lp, L, fresnel, f32.ctypes.data, f64.ctypes.data)
     return f32, f64
+
+
+def brdf_all_ms(params7, lights_parabolic, bounces):
+    """The fitter's pseudo-volume (multi-scattering) BRDF over all pairs (FP32, the
+    reference's operation order and random sequence)."""
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    L = lp.shape[0]
+    out = np.zeros(L * L, np.float32)
+    lib().svfo_brdf_ms_eval_all(np.ascontiguousarray(params7, np.float64), lp, L, bounces, out)
+    return out
+
+
+def pseudo_volume_rgb(params_rgb, lights_parabolic, view, light, bounces, samples=256, seed=0):
+    """The pseudo-volume BRDF of one material (sx, sy, quaternion xyzw, diffuse rgb,
+    specular rgb) for one direction pair, RGB."""
+    out = np.zeros(3, np.float32)
+    lib().svfo_pseudo_volume_rgb(np.ascontiguousarray(params_rgb, np.float32),
+                                 np.ascontiguousarray(lights_parabolic, np.float32), view, light, bounces, samples,
+                                 seed, out)
+    return out
+
+
+def lsq_fit_ms(lum, lights_parabolic, init7, bounces, max_steps=1024):
+    """The reference LM on the pseudo-volume model (svbrdffit -m bounces)."""
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    out = np.zeros(7, np.float32)
+    st = LsqStats()
+    rmse = lib().svfo_lsq_fit_ms(np.ascontiguousarray(lum, np.float32), lp, lp.shape[0], bounces, max_steps,
+                                 np.ascontiguousarray(init7, np.float32), out, C.byref(st))
+    return out, float(rmse), st
 
 
 def lsq_fit(lum, lights_parabolic, init7, fresnel=1.0, max_steps=1024):
@@ -426,6 +462,9 @@ def _bind_harness(L):
                                       C.c_uint32, _f32p, _f32p]
         L.ref_lsq_opts.argtypes = [_f32p, C.c_uint32, _f32p, C.c_float, C.c_uint32, C.c_uint32, _f32p, _f32p,
                                    C.POINTER(C.c_float), _u32p]
+        L.ref_brdf_eval_ms.argtypes = [_f32p, C.c_uint32, C.c_uint32, C.c_float, _f64p, _f32p]
+        L.ref_lsq_ms.argtypes = [_f32p, C.c_uint32, _f32p, C.c_float, C.c_uint32, C.c_uint32, _f32p, _f32p,
+                                 C.POINTER(C.c_float), _u32p]
         if hasattr(L, "ref_downsample"):   # (not in the seam library)
             L.ref_downsample.argtypes = [_f32p, C.c_uint32, _f32p, C.c_uint32, _f32p, _f32p]
     return L
@@ -531,6 +570,26 @@ def ref_downsample(lum, lights_parabolic, n):
     sl = np.zeros(n * n, np.float32)
     ref().ref_downsample(lp, lp.shape[0], np.ascontiguousarray(lum, np.float32), n, dirs, sl)
     return dirs, sl
+
+
+def ref_lsq_ms(lum, lights_parabolic, init7, bounces, fresnel=1.0, flags=LSF_OPTON_DIFFUSE):
+    """LeastSquaresFitSGGX with MultiScatteringBounceCount = bounces (the pseudo-volume model)."""
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    out = np.zeros(7, np.float32)
+    rmse = C.c_float()
+    st = np.zeros(2, np.uint32)
+    ref().ref_lsq_ms(lp, lp.shape[0], np.ascontiguousarray(lum, np.float32), fresnel, flags, bounces,
+                     np.ascontiguousarray(init7, np.float32), out, C.byref(rmse), st)
+    return out, rmse.value, int(st[0]), int(st[1])
+
+
+def ref_brdf_all_ms(params7, lights_parabolic, bounces, fresnel=1.0):
+    """The reference's BRDFEvaluator with BounceCount = bounces over all pairs."""
+    lp = np.ascontiguousarray(lights_parabolic, np.float32)
+    L = lp.shape[0]
+    out = np.zeros(L * L, np.float32)
+    ref().ref_brdf_eval_ms(lp, L, bounces, fresnel, np.ascontiguousarray(params7, np.float64), out)
+    return out
 
 
 def ref_brdf_all(params7, lights_parabolic, fresnel=1.0):

@@ -98,10 +98,10 @@ Tempest::ThreadPool* SerialPool()
     return pool;
 }
 
-LeastSquaresFitOptions MakeOptions(float fresnel, uint32_t flags, uint32_t downsample = ~0u)
+LeastSquaresFitOptions MakeOptions(float fresnel, uint32_t flags, uint32_t downsample = ~0u, uint32_t bounces = ~0u)
 {
     LeastSquaresFitOptions o;
-    o.MultiScatteringBounceCount = ~0u;
+    o.MultiScatteringBounceCount = bounces;
     o.Fresnel = fresnel;
     o.DownSampleLightView = downsample;
     o.Flags = flags;
@@ -199,6 +199,39 @@ void ref_brdf_eval(const float* lights_parabolic, uint32_t light_count, float fr
     BRDFEvaluator ev{ reinterpret_cast<const Tempest::Vector2*>(lights_parabolic), light_count, ~0u, fresnel };
     for(uint32_t idx = 0; idx < light_count*light_count; ++idx)
         out[idx] = ev(0, idx, params);
+}
+
+/* BRDFEvaluator with BounceCount = bounces (svbrdffit -m): the pseudo-volume
+ * multi-scattering BRDF (SGGXMicroFlakePseudoVolumeBRDF, ggx-models-impl.hh:621-758,
+ * 256 random walks of at most `bounces` scattering events) over all L*L pairs. */
+void ref_brdf_eval_ms(const float* lights_parabolic, uint32_t light_count, uint32_t bounces, float fresnel,
+                      const double* params, float* out)
+{
+    BRDFEvaluator ev{ reinterpret_cast<const Tempest::Vector2*>(lights_parabolic), light_count, bounces, fresnel };
+    for(uint32_t idx = 0; idx < light_count*light_count; ++idx)
+        out[idx] = ev(0, idx, params);
+}
+
+/* LeastSquaresFitSGGX with LeastSquaresFitOptions::MultiScatteringBounceCount =
+ * bounces (the fit's model is then the pseudo-volume BRDF).  stats as ref_lsq. */
+void ref_lsq_ms(const float* lights_parabolic, uint32_t light_count, const float* lum, float fresnel, uint32_t flags,
+                uint32_t bounces, const float* init7, float* out7, float* rmse, uint32_t* stats)
+{
+    Tempest::BTF btf;
+    btf.LightCount = light_count;
+    std::vector<Tempest::Vector2> lights(light_count);
+    std::memcpy(lights.data(), lights_parabolic, light_count*sizeof(Tempest::Vector2));
+    btf.LightsParabolic = lights.data();
+    std::vector<float> lum_copy(lum, lum + (size_t)light_count*light_count);
+    OptimizationParameters init, out;
+    std::memcpy(init.ParametersArray, init7, sizeof(init.ParametersArray));
+    auto opts = MakeOptions(fresnel, flags, ~0u, bounces);
+    LeastSquaresFitSGGX(0, *SerialPool(), &btf, lum_copy.data(), opts, init, &out, rmse);
+    ParseIterationLog();
+    std::memcpy(out7, out.ParametersArray, sizeof(out.ParametersArray));
+    stats[0] = g_iterations;
+    stats[1] = g_effective;
+    btf.LightsParabolic = nullptr;
 }
 
 /* LeastSquaresFitSGGX with LeastSquaresFitOptions::Flags and DownSampleLightView

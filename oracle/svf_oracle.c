@@ -257,6 +257,235 @@ float svfo_brdf_f32(const double* params7, const float* lp, uint32_t light_count
     return surface_brdf(kd, ks, stddev, &basis, out_density, wi, wo, fresnel);
 }
 
+/* ---------------------------------------------------------------------------
+ * Pseudo-volume multi-scattering BRDF (svbrdffit -m)
+ * ------------------------------------------------------------------------- */
+
+static inline v3 reflect(v3 inc, v3 n);
+
+/* Matrix3 * Matrix3, matrix3.hh:355-360: column j of the product is
+ * rhs.c[j].x * lhs.c[0] + rhs.c[j].y * lhs.c[1] + rhs.c[j].z * lhs.c[2]. */
+static m3 m3mul(const m3* lhs, const m3* rhs)
+{
+    m3 r;
+    for(int j = 0; j < 3; ++j)
+        r.c[j] = v3add(v3add(v3scale(lhs->c[0], rhs->c[j].x), v3scale(lhs->c[1], rhs->c[j].y)),
+                       v3scale(lhs->c[2], rhs->c[j].z));
+    return r;
+}
+
+/* Matrix3::transpose, matrix3.hh:92-97 */
+static m3 m3transpose(const m3* m)
+{
+    m3 r;
+    r.c[0] = v3make(m->c[0].x, m->c[1].x, m->c[2].x);
+    r.c[1] = v3make(m->c[0].y, m->c[1].y, m->c[2].y);
+    r.c[2] = v3make(m->c[0].z, m->c[1].z, m->c[2].z);
+    return r;
+}
+
+/* Matrix3::transformCovariance, matrix3.hh:151-158 */
+static m3 m3covariance(const m3* b, v3 var)
+{
+    const v3* C = b->c;
+    m3 r;
+    r.c[0] = v3add(v3add(v3scale(v3scale(C[0], var.x), C[0].x), v3scale(v3scale(C[1], var.y), C[1].x)),
+                   v3scale(v3scale(C[2], var.z), C[2].x));
+    r.c[1] = v3add(v3add(v3scale(v3scale(C[0], var.x), C[0].y), v3scale(v3scale(C[1], var.y), C[1].y)),
+                   v3scale(v3scale(C[2], var.z), C[2].y));
+    r.c[2] = v3add(v3add(v3scale(v3scale(C[0], var.x), C[0].z), v3scale(v3scale(C[1], var.y), C[1].z)),
+                   v3scale(v3scale(C[2], var.z), C[2].z));
+    return r;
+}
+
+/* Matrix3::transform, matrix3.hh:144-147 */
+static inline v3 m3transform(const m3* m, v3 v)
+{
+    return v3add(v3add(v3scale(m->c[0], v.x), v3scale(m->c[1], v.y)), v3scale(m->c[2], v.z));
+}
+
+/* Matrix3::makeBasis, matrix3.hh:99-108 */
+static m3 m3basis(v3 n)
+{
+    v3 d0 = v3cross(v3make(1.0f, 0.0f, 0.0f), n), d1 = v3cross(v3make(0.0f, 1.0f, 0.0f), n);
+    float l0 = v3dot(d0, d0), l1 = v3dot(d1, d1);
+    m3 r;
+    r.c[0] = l0 > l1 ? v3div(d0, sqrtf(l0)) : v3div(d1, sqrtf(l1));
+    r.c[1] = v3cross(n, r.c[0]);
+    r.c[2] = n;
+    return r;
+}
+
+/* Matrix3::choleskyDecomposition, matrix3.hh:173-191 (columns of the lower factor) */
+static m3 m3cholesky(const m3* m)
+{
+    float l00 = sqrtf(m->c[0].x);
+    float rcp_l00 = 1.0f / l00;
+    float l10 = rcp_l00 * m->c[0].y;
+    float l20 = rcp_l00 * m->c[0].z;
+    float l11 = sqrtf(m->c[1].y - l10 * l10);
+    float rcp_l11 = 1.0f / l11;
+    float l21 = rcp_l11 * (m->c[1].z - l20 * l10);
+    float l22 = sqrtf(m->c[2].z - l21 * l21 - l20 * l20);
+    m3 r;
+    r.c[0] = v3make(l00, l10, l20);
+    r.c[1] = v3make(0.0f, l11, l21);
+    r.c[2] = v3make(0.0f, 0.0f, l22);
+    return r;
+}
+
+/* UniformSampleSphere, sampling3.hh:106-116 */
+static inline v3 uniform_sphere(float ra, float rb)
+{
+    float phi = 2.0f * REF_PI * ra;
+    float s, c;
+    sincos_tan(phi, &s, &c);
+    float cos_theta = 2.0f * rb - 1.0f;
+    float sin_theta = sqrtf(1.0f - cos_theta * cos_theta);
+    return v3make(c * sin_theta, s * sin_theta, cos_theta);
+}
+
+/* SGGXMicroFlakeSampleIncidentLight(out_light, ...), ggx-models-impl.hh:554-570:
+ * a visible normal of the SGGX distribution seen from out_light (the uniform
+ * sphere sample mapped through the Cholesky factor of the covariance in the
+ * out_light frame), and out_light reflected about it.  The reference passes two
+ * FastFloatRand(seed) calls as UniformSampleSphere's arguments; its x86-64 GCC
+ * build evaluates them right to left, so the second argument draws first. */
+static v3 sggx_sample_incident(v3 wo, v3 stddev, const m3* basis, unsigned* seed)
+{
+    float rb = lcg_float(seed);
+    float ra = lcg_float(seed);
+    v3 u = uniform_sphere(ra, rb);
+    m3 S = m3covariance(basis, v3mul(stddev, stddev));
+    m3 ob = m3basis(wo), obt = m3transpose(&ob);
+    m3 t = m3mul(&ob, &S);
+    S = m3mul(&t, &obt);
+    m3 L = m3cholesky(&S);
+    v3 vn = v3normalize(m3_rot_inverse(&L, u));
+    vn = m3transform(&ob, vn);
+    return reflect(wo, vn);
+}
+
+/* SGGXMicroFlakePseudoVolumeBRDF, ggx-models-impl.hh:621-758, in the fitting
+ * frame (tangent x, binormal y, normal z) for `channels` spectrum channels (the
+ * walk is shared: it continues while every channel's throughput is above
+ * 1e-3), `samples` random walks of at most `depth` scattering events from the
+ * LCG state `seed` (the reference seeds it from the texture coordinate, 0 for
+ * the fitter's evaluator).  The Fresnel branch is compiled out in the reference
+ * (USE_PSEUDO_VOLUME_FRESNEL is not defined). */
+static void pseudo_volume_brdf(const float* spec, const float* diff, int channels, v3 stddev, const m3* basis,
+                               float out_density, v3 wi, v3 wo, uint32_t depth, uint32_t samples, unsigned seed,
+                               float* out)
+{
+    float dot_inc = wi.z, dot_out = wo.z;
+    for(int c = 0; c < channels; ++c)
+        out[c] = 0.0f;
+    if(dot_out < 0.0f || dot_inc < 0.0f)
+        return;
+    if(stddev.x < 1e-6f || stddev.y < 1e-6f)
+        return;
+    (void)lcg_float(&seed);
+    float incoming_density = sggx_projected_area(stddev, basis, wi);
+    v3 micro = v3normalize(v3add(wo, wi));
+    float contrib = (float)samples / (out_density + incoming_density * dot_out / dot_inc);
+    float ndf = sggx_ndf(stddev, basis, micro);
+    float radiance[3], thr[3];
+    for(int c = 0; c < channels; ++c)
+        radiance[c] = spec[c] * contrib * ndf * 2.0f * (1.0f / 4.0f);
+    for(uint32_t s = 0; s < samples; ++s)
+    {
+        for(int c = 0; c < channels; ++c)
+            thr[c] = spec[c];
+        v3 out_l = wo;
+        float dir_density = out_density;
+        float t = lcg_float(&seed);
+        float log_step = -logf(t);
+        float step = log_step / dir_density;
+        float depth_in = step * dot_out;
+        for(uint32_t it = 0; it < depth; ++it)
+        {
+            int alive = 1;
+            for(int c = 0; c < channels; ++c)
+                alive &= thr[c] > 1e-3f;
+            if(!alive)
+                break;
+            v3 inc_l = sggx_sample_incident(out_l, stddev, basis, &seed);
+            dir_density = sggx_projected_area(stddev, basis, inc_l);
+            out_l = v3make(-inc_l.x, -inc_l.y, -inc_l.z);
+            t = lcg_float(&seed);
+            log_step = -logf(t);
+            step = log_step / dir_density;
+            depth_in += step * out_l.z;
+            if(depth_in < 0.0f)
+                break;
+            float distance = depth_in / dot_inc;
+            float extinction = expf(-incoming_density * distance);
+            if(extinction < 1e-9f)
+                break;
+            v3 mn = v3normalize(v3add(out_l, wi));
+            float brdf = sggx_ndf(stddev, basis, mn) * 2.0f / (4.0f * dir_density);
+            for(int c = 0; c < channels; ++c)
+            {
+                thr[c] *= spec[c];
+                radiance[c] += extinction * thr[c] * brdf;
+            }
+        }
+    }
+    float rcp = 1.0f / (float)samples;
+    for(int c = 0; c < channels; ++c)
+        out[c] = radiance[c] * rcp + diff[c] * dot_inc * (1.0f / REF_PI);
+}
+
+float svfo_brdf_ms_f32(const double* params7, const float* lp, uint32_t light_count, uint32_t view, uint32_t light,
+                       uint32_t bounces)
+{
+    /* BRDFEvaluator::operator() with BounceCount = bounces, svbrdf-lsq-fitting-internal.hh:91-153:
+     * SampleCount 256, Depth bounces, the unnormalised ToMatrix3(ToQuaternion(euler))
+     * as the SGGX basis (ggx-models-impl.hh:660) and the directional density. */
+    float p[7];
+    for(int i = 0; i < 7; ++i)
+        p[i] = (float)params7[i];
+    v3 stddev = v3make(p[0] > 0.0f ? p[0] : 0.0f, p[1] > 0.0f ? p[1] : 0.0f, 1.0f);
+    float quat[4];
+    euler_to_quat(p + 4, quat);
+    float kd = p[3] > 0.0f ? p[3] : 0.0f;
+    float ks = p[2] > 0.0f ? p[2] : 0.0f;
+    v3 wi = parabolic_to_cartesian(lp[2 * light], lp[2 * light + 1]);
+    v3 wo = parabolic_to_cartesian(lp[2 * view], lp[2 * view + 1]);
+    m3 basis = quat_to_matrix(quat);
+    float out_density = sggx_projected_area(stddev, &basis, wo);
+    float r;
+    (void)light_count;
+    pseudo_volume_brdf(&ks, &kd, 1, stddev, &basis, out_density, wi, wo, bounces, 256, 0u, &r);
+    return r;
+}
+
+void svfo_brdf_ms_eval_all(const double* params7, const float* lp, uint32_t light_count, uint32_t bounces,
+                           float* out)
+{
+    for(uint32_t v = 0; v < light_count; ++v)
+        for(uint32_t l = 0; l < light_count; ++l)
+            out[v * light_count + l] = svfo_brdf_ms_f32(params7, lp, light_count, v, l, bounces);
+}
+
+void svfo_pseudo_volume_rgb(const float* params_rgb, const float* lp, uint32_t view, uint32_t light,
+                            uint32_t bounces, uint32_t samples, uint32_t seed, float* rgb)
+{
+    /* params_rgb: sx, sy, quaternion xyzw (as stored, unnormalised), diffuse rgb, specular rgb */
+    v3 stddev = v3make(params_rgb[0] > 0.0f ? params_rgb[0] : 0.0f, params_rgb[1] > 0.0f ? params_rgb[1] : 0.0f, 1.0f);
+    m3 basis = quat_to_matrix(params_rgb + 2);
+    float kd[3], ks[3];
+    for(int c = 0; c < 3; ++c)
+    {
+        kd[c] = params_rgb[6 + c];
+        ks[c] = params_rgb[9 + c];
+    }
+    v3 wi = parabolic_to_cartesian(lp[2 * light], lp[2 * light + 1]);
+    v3 wo = parabolic_to_cartesian(lp[2 * view], lp[2 * view + 1]);
+    float out_density = sggx_projected_area(stddev, &basis, wo);
+    pseudo_volume_brdf(ks, kd, 3, stddev, &basis, out_density, wi, wo, bounces, samples, seed, rgb);
+}
+
 /* The same model in double precision.  sin/cos replace FastSinCos (exact up to
  * rounding), pi is the true value, and the constant 1e-6 thresholds of the
  * reference are kept. */
@@ -355,7 +584,17 @@ typedef struct
     const float* lp;
     uint32_t L, N;
     float fresnel;
+    int ms;              /* the pseudo-volume model (BounceCount != ~0u) */
+    uint32_t bounces;
 } lsq_problem;
+
+/* BRDFEvaluator::operator() of the problem's model */
+static float model_f32(const lsq_problem* pb, const double* params, uint32_t idx)
+{
+    if(pb->ms)
+        return svfo_brdf_ms_f32(params, pb->lp, pb->L, idx / pb->L, idx % pb->L, pb->bounces);
+    return svfo_brdf_f32(params, pb->lp, pb->L, idx / pb->L, idx % pb->L, pb->fresnel);
+}
 
 /* ParallelResidualEvaluator::computeResidual, fitting.hh:106-141: residual in
  * float, squared in float, summed in double (one worker, index order). */
@@ -365,7 +604,7 @@ static double compute_residual(const lsq_problem* pb, const double* params, doub
     for(uint32_t idx = 0; idx < pb->N; ++idx)
     {
         float out = pb->lum[idx];
-        float f = svfo_brdf_f32(params, pb->lp, pb->L, idx / pb->L, idx % pb->L, pb->fresnel);
+        float f = model_f32(pb, params, idx);
         float r = out - f;
         sum += r * r;
         res[idx] = r;
@@ -387,9 +626,9 @@ static void compute_jacobian(const lsq_problem* pb, const double* params, uint32
             double prev = tmp[k];
             double step = (fabs(prev) + h) * h;
             tmp[k] = prev + step;
-            float next_res = -svfo_brdf_f32(tmp, pb->lp, pb->L, idx / pb->L, idx % pb->L, pb->fresnel);
+            float next_res = -model_f32(pb, tmp, idx);
             tmp[k] = prev - step;
-            float prev_res = -svfo_brdf_f32(tmp, pb->lp, pb->L, idx / pb->L, idx % pb->L, pb->fresnel);
+            float prev_res = -model_f32(pb, tmp, idx);
             jac[idx * P + k] = (next_res - prev_res) / (2.0f * step);
             tmp[k] = prev;
         }
@@ -434,13 +673,32 @@ static void invert(const double* a, uint32_t n, double* inv)
             inv[i * n + j] = m[i * 2 * n + n + j];
 }
 
+static float lsq_fit(const lsq_problem* problem, uint32_t max_steps, const float* init7, float* out7,
+                     svfo_lsq_stats* stats);
+
 float svfo_lsq_fit(const float* lum, const float* lp, uint32_t L, float fresnel, uint32_t max_steps,
                    const float* init7, float* out7, svfo_lsq_stats* stats)
+{
+    lsq_problem pb = { lum, lp, L, L * L, fresnel, 0, 0 };
+    return lsq_fit(&pb, max_steps, init7, out7, stats);
+}
+
+float svfo_lsq_fit_ms(const float* lum, const float* lp, uint32_t L, uint32_t bounces, uint32_t max_steps,
+                      const float* init7, float* out7, svfo_lsq_stats* stats)
+{
+    /* LeastSquaresFitOptions::MultiScatteringBounceCount = bounces: the same LM on the
+     * pseudo-volume model (its Fresnel term is compiled out in the reference) */
+    lsq_problem pb = { lum, lp, L, L * L, 1.0f, 1, bounces };
+    return lsq_fit(&pb, max_steps, init7, out7, stats);
+}
+
+static float lsq_fit(const lsq_problem* problem, uint32_t max_steps, const float* init7, float* out7,
+                     svfo_lsq_stats* stats)
 {
     /* LeastSquaresFitSGGX with LSF_OPTON_DIFFUSE, svbrdf-lsq-fitting-setup.cc:234-431,
      * running LevenbergMarquardtCurveFit (fitting.hh:457-678). */
     const uint32_t P = 7;
-    lsq_problem pb = { lum, lp, L, L * L, fresnel };
+    lsq_problem pb = *problem;
     const uint32_t N = pb.N;
     const double mean_sq_error = 1e-6;
     const double break_criteria = (double)1e-3f;   /* settings.BreakOnSmallStep = 1e-3f */

@@ -46,6 +46,19 @@ float svfo_brdf_f32(const double* params7, const float* lights_parabolic, uint32
 /* The same model evaluated in double precision throughout (the FP64 reference values). */
 double svfo_brdf_f64(const double* params7, const float* lights_parabolic, uint32_t light_count,
                      uint32_t view, uint32_t light, double fresnel);
+/* The fitter's evaluator with BounceCount = bounces (svbrdffit -m): the pseudo-volume
+ * multi-scattering BRDF (SGGXMicroFlakePseudoVolumeBRDF, ggx-models-impl.hh:621-758),
+ * 256 random walks from LCG seed 0, in the reference's operation order. */
+float svfo_brdf_ms_f32(const double* params7, const float* lights_parabolic, uint32_t light_count,
+                       uint32_t view, uint32_t light, uint32_t bounces);
+/* svfo_brdf_ms_f32 over all L*L pairs (lv = view * L + light). */
+void svfo_brdf_ms_eval_all(const double* params7, const float* lights_parabolic, uint32_t light_count,
+                           uint32_t bounces, float* out);
+/* The pseudo-volume BRDF of one material in RGB: params_rgb = sx, sy, quaternion xyzw
+ * (unnormalised, as ToMatrix3 takes it), diffuse rgb, specular rgb; `samples` walks
+ * of at most `bounces` events from LCG state `seed`. */
+void svfo_pseudo_volume_rgb(const float* params_rgb, const float* lights_parabolic, uint32_t view, uint32_t light,
+                            uint32_t bounces, uint32_t samples, uint32_t seed, float* rgb);
 /* All L*L pairs. */
 void svfo_brdf_eval_all(const double* params7, const float* lights_parabolic, uint32_t light_count,
                         float fresnel, float* out_f32, double* out_f64);
@@ -67,6 +80,10 @@ typedef struct
  * (CurveFitSteps = 1024 in the reference).  Returns RMSE. */
 float svfo_lsq_fit(const float* lum, const float* lights_parabolic, uint32_t light_count, float fresnel,
                    uint32_t max_steps, const float* init7, float* out7, svfo_lsq_stats* stats);
+/* The same fit on the pseudo-volume model (LeastSquaresFitOptions::MultiScatteringBounceCount
+ * = bounces, svbrdffit -m). */
+float svfo_lsq_fit_ms(const float* lum, const float* lights_parabolic, uint32_t light_count, uint32_t bounces,
+                      uint32_t max_steps, const float* init7, float* out7, svfo_lsq_stats* stats);
 
 /* ---- luminance slice (btf.cc:1078-1116) --------------------------------- */
 

@@ -30,6 +30,7 @@ SVF_LSQ_RGB = 1 << 8
 SVF_LSQ_STEP_PER_PARAMETER = 1 << 9
 SVF_LSQ_DISABLE_DIRECTION_FITTING = 1 << 2
 SVF_LSQ_FIT_TOP = 1 << 4
+SVF_LSQ_MULTI_SCATTERING = 1 << 10
 SVF_SAMPLES_F32, SVF_SAMPLES_F16 = 0, 1
 SVF_INIT_DEFAULT, SVF_INIT_GIVEN, SVF_INIT_MLP = 0, 1, 2
 SVF_ERROR_PAIRWISE, SVF_ERROR_MAX_VIEW = 0, 1
@@ -44,7 +45,7 @@ EXPORTS = ("svf_abi_version", "svf_status_string", "svf_last_error", "svf_lsq_op
            "svf_mlp_save", "svf_mlp_load", "svf_mlp_destroy", "svf_btf_probe", "svf_btf_load", "svf_btf_load_file",
            "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_btf_destroy", "svf_error_maps", "svf_exr_write",
            "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps", "svf_refit_neighborhood",
-           "svf_render_btf", "svf_downsample_light_view")
+           "svf_render_btf", "svf_downsample_light_view", "svf_render_btf_ms")
 
 
 class SvfError(RuntimeError):
@@ -56,7 +57,7 @@ class SvfError(RuntimeError):
 class LsqOptions(C.Structure):
     _fields_ = [("max_iterations", C.c_uint32), ("fresnel", C.c_float), ("flags", C.c_uint32),
                 ("mse_target", C.c_double), ("break_on_small_step", C.c_double), ("restarts", C.c_uint32),
-                ("downsample_light_view", C.c_uint32)]
+                ("downsample_light_view", C.c_uint32), ("multi_scattering_bounces", C.c_uint32)]
 
 
 class TexelStats(C.Structure):
@@ -173,6 +174,7 @@ def load() -> C.CDLL:
         L.svf_maps_write_exr.argtypes = [C.c_char_p, u32, u32, C.POINTER(Maps)]
         L.svf_params_from_maps.argtypes = [C.POINTER(SvbrdfMaps), vp, vp]
         L.svf_render_btf.argtypes = [vp, vp, u32, C.POINTER(SvbrdfMaps), f32, u32, vp]
+        L.svf_render_btf_ms.argtypes = [vp, vp, u32, C.POINTER(SvbrdfMaps), u32, u32, u32, u32, vp]
         L.svf_refit_neighborhood.argtypes = [vp, C.POINTER(BtfView), C.POINTER(LsqOptions), vp, vp, C.POINTER(Maps),
                                              C.POINTER(RunStats)]
         for name in ("svf_create", "svf_lsq_fit_sggx", "svf_lsq_fit_batch", "svf_lsq_fit_batch_noalloc",
@@ -180,7 +182,7 @@ def load() -> C.CDLL:
                      "svf_mlp_step", "svf_mlp_save", "svf_mlp_load", "svf_btf_probe", "svf_btf_load",
                      "svf_btf_load_file", "svf_btf_get_info", "svf_btf_decode", "svf_fit_btf", "svf_error_maps",
                      "svf_exr_write", "svf_exr_read", "svf_maps_write_exr", "svf_params_from_maps",
-                     "svf_refit_neighborhood", "svf_render_btf"):
+                     "svf_refit_neighborhood", "svf_render_btf", "svf_render_btf_ms"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -193,16 +195,21 @@ def _check(status: int):
 
 def options(max_iterations: int = 1024, fresnel: float = 1.0, restarts: int | None = None,
             rgb: bool = False, step_per_parameter: bool = True, diffuse: bool = True,
-            fit_direction: bool = True, downsample: int = 0, fit_top: bool = False) -> LsqOptions:
+            fit_direction: bool = True, downsample: int = 0, fit_top: bool = False,
+            multi_scattering: int | None = None) -> LsqOptions:
     """LM options; rgb selects the 11-parameter RGB fit (svf_fit_texels / svf_fit_btfs);
     step_per_parameter=False restores the reference's whole-vector small-step test;
     diffuse=False the specular-only fit, fit_direction=False holds the Euler angles,
-    downsample=n fits n of the directions (svf_lsq_fit_sggx / svf_lsq_fit_batch)."""
+    downsample=n fits n of the directions, multi_scattering=bounces the pseudo-volume
+    model (svf_lsq_fit_sggx / svf_lsq_fit_batch)."""
     o = LsqOptions()
     load().svf_lsq_options_default(C.byref(o))
     o.max_iterations = max_iterations
     o.fresnel = fresnel
     o.downsample_light_view = downsample
+    if multi_scattering is not None:
+        o.flags |= SVF_LSQ_MULTI_SCATTERING
+        o.multi_scattering_bounces = multi_scattering
     if not diffuse:
         o.flags &= ~SVF_LSQ_DIFFUSE
     if not fit_direction:
@@ -453,6 +460,21 @@ class Context:
         if out is None:
             out = np.zeros((T, L * L, 3), np.float16 if sample_type == SVF_SAMPLES_F16 else np.float32)
         _check(self._lib.svf_render_btf(self.handle, lp.ctypes.data, L, C.byref(m), fresnel, sample_type, _ptr(out)))
+        return out
+
+    def render_btf_ms(self, lights_parabolic, diffuse, specular, sigma, basis, bounces: int, samples: int = 256,
+                      seed: int = 0, sample_type=SVF_SAMPLES_F32, out=None):
+        """Samples [texels][L*L][3] of SVBRDF maps with the pseudo-volume multi-scattering
+        BRDF -- svf_render_btf_ms."""
+        lp = np.ascontiguousarray(lights_parabolic, np.float32)
+        d, sp, sg, b = (np.ascontiguousarray(m, np.float32).reshape(-1, m.shape[-1]) for m in
+                        (np.asarray(diffuse), np.asarray(specular), np.asarray(sigma), np.asarray(basis)))
+        T, L = d.shape[0], lp.shape[0]
+        m = SvbrdfMaps(d.ctypes.data, sp.ctypes.data, sg.ctypes.data, sg.shape[1], b.ctypes.data, T, 1)
+        if out is None:
+            out = np.zeros((T, L * L, 3), np.float16 if sample_type == SVF_SAMPLES_F16 else np.float32)
+        _check(self._lib.svf_render_btf_ms(self.handle, lp.ctypes.data, L, C.byref(m), bounces, samples, seed,
+                                           sample_type, _ptr(out)))
         return out
 
     def synth_btf(self, seed: int, mix: int, lights_parabolic, first: int, count: int, samples,

@@ -25,10 +25,14 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 CU_SOURCES = ["svf_kernels.cu", "svf_lm.cu", "svf_init.cu", "svf_ndf_tc.cu", "svf_mlp.cu", "svf_btf.cu",
-              "svf_error.cu"]
+              "svf_error.cu", "svf_ms.cu"]
+# per-file nvcc flags: the pseudo-volume BRDF rounds every float operation on its
+# own (no fused multiply-adds), as the reference's x86-64 build does
+CU_FLAGS = {"svf_ms.cu": ["-fmad=false"]}
 CXX_SOURCES = {"svf_host.cpp": ["-O2", "-ffp-contract=off"], "svf_host_init.cpp": ["-O2", "-ffp-contract=off"],
                "svf_host_lm.cpp": ["-O2", "-ffp-contract=off"], "svf_host_fit.cpp": ["-O2", "-ffp-contract=off"],
                "svf_host_mlp.cpp": ["-O2", "-ffp-contract=off"], "svf_host_btf.cpp": ["-O2", "-ffp-contract=off"],
+               "svf_host_ms.cpp": ["-O2", "-ffp-contract=off"],
                "svf_layout.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"],
                "svf_btf_file.cpp": ["-O2", "-ffp-contract=off", "-fno-fast-math"], "svf_exr.cpp": ["-O2"]}
 HEADERS = ["svf_internal.h", "svf_host.h", "svf_model.cuh", "svf_layout.h", "svf_btf_file.h"]
@@ -53,7 +57,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         o = os.path.join(BUILD, src + ".o")
         objs.append(o)
         if force or _newer(o, [s] + headers):
-            cmd = [NVCC, *NVCC_FLAGS, "-c", s, "-o", o]
+            cmd = [NVCC, *NVCC_FLAGS, *CU_FLAGS.get(src, []), "-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

@@ -113,10 +113,21 @@ float initial_damping(const svf_fit_options& o)
     return o.init_mode == SVF_INIT_MLP ? kMlpInitialDamping : 1.0f;
 }
 
-svf_status check_options(const svf_lsq_options* o, bool downsample_ok)
+svf_status check_options(const svf_lsq_options* o, bool downsample_ok, bool ms_ok)
 {
     if(!o)
         return fail(SVF_EINVAL, "null options");
+    if(o->flags & SVF_LSQ_MULTI_SCATTERING)
+    {
+        if(!ms_ok)
+            return fail(SVF_EINVAL, "SVF_LSQ_MULTI_SCATTERING is taken by svf_lsq_fit_sggx / svf_lsq_fit_batch");
+        constexpr uint32_t other = SVF_LSQ_RGB | SVF_LSQ_DISABLE_DIRECTION_FITTING | SVF_LSQ_FIT_TOP;
+        if(!(o->flags & SVF_LSQ_DIFFUSE) || (o->flags & other) || o->downsample_light_view)
+            return fail(SVF_EINVAL, "SVF_LSQ_MULTI_SCATTERING fits the 7 parameters (SVF_LSQ_DIFFUSE) without "
+                                    "other options");
+        if(o->multi_scattering_bounces > 1024)
+            return fail(SVF_EINVAL, "multi_scattering_bounces %u (at most 1024)", o->multi_scattering_bounces);
+    }
     if((o->flags & SVF_LSQ_FIT_TOP) && (!downsample_ok || (o->flags & SVF_LSQ_RGB)))
         return fail(SVF_EINVAL, "SVF_LSQ_FIT_TOP is taken by svf_lsq_fit_sggx / svf_lsq_fit_batch (luminance fit)");
     if(o->downsample_light_view == 1 || (o->downsample_light_view && !downsample_ok) ||
@@ -126,7 +137,7 @@ svf_status check_options(const svf_lsq_options* o, bool downsample_ok)
     if((o->flags & SVF_LSQ_RGB) && (o->flags & SVF_LSQ_DISABLE_DIRECTION_FITTING || !(o->flags & SVF_LSQ_DIFFUSE)))
         return fail(SVF_EINVAL, "the RGB fit (SVF_LSQ_RGB) fits every parameter, with the diffuse term");
     constexpr uint32_t known = SVF_LSQ_DIFFUSE | SVF_LSQ_RGB | SVF_LSQ_STEP_PER_PARAMETER |
-                               SVF_LSQ_DISABLE_DIRECTION_FITTING | SVF_LSQ_FIT_TOP;
+                               SVF_LSQ_DISABLE_DIRECTION_FITTING | SVF_LSQ_FIT_TOP | SVF_LSQ_MULTI_SCATTERING;
     if(o->flags & ~known)
         return fail(SVF_EINVAL, "unknown lsq flags 0x%x", o->flags & ~known);
     if(!(o->fresnel >= 1.0f) || !std::isfinite(o->fresnel))
@@ -244,6 +255,7 @@ void svf_lsq_options_default(svf_lsq_options* o)
     o->break_on_small_step = (double)1e-3f;   // settings.BreakOnSmallStep = 1e-3f
     o->restarts = 1;
     o->downsample_light_view = 0;   // DownSampleLightView = ~0u: all directions
+    o->multi_scattering_bounces = 2;   // used with SVF_LSQ_MULTI_SCATTERING only
 }
 
 uint32_t svf_downsample_light_view(uint32_t L, uint32_t n, uint32_t* idx)

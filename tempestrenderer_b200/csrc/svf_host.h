@@ -9,6 +9,7 @@
 //   svf_host_fit.cpp   svf_fit_texels, svf_fit_btfs, svf_synth_btf
 //   svf_host_mlp.cpp   the learned initial guess (svf_mlp_*)
 //   svf_host_btf.cpp   factored BTF files, error maps, rendering, neighbourhood refit
+//   svf_host_ms.cpp    the pseudo-volume multi-scattering BRDF: rendering, the -m fit
 #pragma once
 
 #include <cuda_runtime.h>
@@ -223,7 +224,8 @@ svf_status check_ctx(svf_ctx* ctx);
 // Initial LM damping relative to the reference's rule for a BTF's fit options.
 float initial_damping(const svf_fit_options& o);
 // downsample_ok: the entry point takes downsample_light_view and SVF_LSQ_FIT_TOP.
-svf_status check_options(const svf_lsq_options* o, bool downsample_ok = false);
+// ms_ok: the entry point takes SVF_LSQ_MULTI_SCATTERING.
+svf_status check_options(const svf_lsq_options* o, bool downsample_ok = false, bool ms_ok = false);
 svf_status get_layout(svf_ctx* ctx, const float* lp_in, uint32_t L, Layout** out);
 // Copies `bytes` from src (host or device) to the device buffer dst.
 svf_status to_device(svf_ctx* ctx, void* dst, const void* src, size_t bytes);
@@ -268,6 +270,10 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
 svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o);
 svf::LmKernelChoice lm_choice(Layout* lay, uint64_t stride, bool rgb);
 svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r);
+
+// ---- the multi-scattering fit (svf_host_ms.cpp)
+svf_status run_ms_fit(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const float* lum, uint64_t stride,
+                      uint64_t T, const float* init, float* out, float* rmse, svf_texel_stats* stats);
 
 // ---- the learned initial guess (svf_host_mlp.cpp)
 svf_status mlp_infer(svf_ctx* ctx, const svf_mlp* mlp, const float* X, uint64_t rows, float* C, float* act, float* Y);

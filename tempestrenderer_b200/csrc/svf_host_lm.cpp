@@ -269,7 +269,7 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
                              svf_texel_stats* stats)
 {
     SVF_TRY(check_ctx(ctx));
-    SVF_TRY(check_options(opts, true));
+    SVF_TRY(check_options(opts, true, true));
     if(opts->flags & SVF_LSQ_RGB)
         return fail(SVF_EINVAL, "the RGB fit (SVF_LSQ_RGB) takes RGB samples: use svf_fit_texels");
     if(!lum || !init || !out || !rmse)
@@ -296,7 +296,10 @@ svf_status svf_lsq_fit_batch(svf_ctx* ctx, const float* lp, uint32_t L, const fl
     SVF_TRY(zero_error_flags(ctx));
     const uint32_t n = opts->downsample_light_view;
     DevBuf d_pairs, d_sub;
-    if(opts->flags & SVF_LSQ_FIT_TOP)
+    if(opts->flags & SVF_LSQ_MULTI_SCATTERING)
+        SVF_TRY(run_ms_fit(ctx, lay, opts, ctx->lum.as<float>(), stride, T, ctx->init.as<float>(),
+                           ctx->out.as<float>(), ctx->rmse.as<float>(), ctx->stats.as<svf_texel_stats>()));
+    else if(opts->flags & SVF_LSQ_FIT_TOP)
     {
         // the top-most view's row (svbrdf-lsq-fitting-setup.cc:291-305: the first
         // direction of least parabolic length, from 1 down)

@@ -351,4 +351,72 @@ struct RenderArgs
 };
 cudaError_t launch_render(const RenderArgs& a, cudaStream_t stream);
 
+// ---- the pseudo-volume multi-scattering BRDF (svf_ms.cu) -------------------------------
+
+struct MsRenderArgs
+{
+    uint32_t L;
+    const float* geo;          // [3][L]
+    uint64_t count;            // texels
+    const float *diffuse, *specular, *sigma, *basis;   // device maps
+    uint32_t sigma_channels;
+    uint32_t bounces, samples, seed;   // walk depth, walks per evaluation, LCG state
+    uint32_t sample_type;
+    void* out;                 // device [count][L^2][3]
+};
+cudaError_t launch_ms_render(const MsRenderArgs& a, cudaStream_t stream);
+
+// The LM state of one texel of the multi-scattering fit (FP64, as the
+// reference's LevenbergMarquardtCurveFit keeps it).
+struct MsTexel
+{
+    double p[7], tmp[7], step[7], grad[7], hess[49];
+    double damping, mult, last, trial, gain;
+    uint32_t phase, iter, effective, jacobians, residuals;
+};
+enum : uint32_t
+{
+    kMsStep = 0,       // the next iteration computes a step
+    kMsTrial = 1,      // its trial point awaits its residual
+    kMsJacobian = 2,   // the accepted point awaits its Jacobian
+    kMsDone = 3
+};
+enum : uint32_t
+{
+    kMsEvalCurrent = 0,    // residuals at p (the first evaluation)
+    kMsEvalTrial = 1,      // residuals at the trial point
+    kMsEvalJacobian = 2    // the 14 central-difference evaluations per pair at p
+};
+enum : uint32_t
+{
+    kMsStageStart = 0,     // initial damping from the first J^T J
+    kMsStageStep = 1,      // damped solve, small-step and constraint tests
+    kMsStageGain = 2,      // gain ratio, accept or reject
+    kMsStageDamping = 3    // gradient test and damping update after a Jacobian
+};
+struct MsFitArgs
+{
+    uint32_t L;
+    const float* geo;          // [3][L]
+    uint32_t bounces;
+    uint64_t texels;           // texels of the batch
+    const float* lum;          // [texels][lum_stride] luminance slices
+    uint64_t lum_stride;
+    MsTexel* st;               // [texels]
+    float* res;                // [texels][L^2] residuals
+    float* fev;                // [texels][L^2][14] negated perturbed evaluations
+    uint32_t* list;            // texels of the next evaluation
+    uint32_t* counts;          // [0] trial list length, [1] Jacobian list length, [2] texels not done
+    uint32_t max_iter;
+    double mse_target, eps;    // LevenbergMarquardtCurveFit mean_sq_error, BreakOnSmallStep
+};
+cudaError_t launch_ms_setup(const MsFitArgs& a, const float* init, cudaStream_t stream);
+// Evaluations of the listed texels and their reductions: `count` of them, or,
+// with dcount (device) non-null, *dcount of at most `count`.
+cudaError_t launch_ms_eval(const MsFitArgs& a, uint32_t mode, uint32_t count, const uint32_t* dcount,
+                           cudaStream_t stream);
+cudaError_t launch_ms_control(const MsFitArgs& a, uint32_t stage, cudaStream_t stream);
+cudaError_t launch_ms_finish(const MsFitArgs& a, const float* init, float* out, float* rmse, svf_texel_stats* stats,
+                             cudaStream_t stream);
+
 } // namespace svf

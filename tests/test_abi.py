@@ -28,7 +28,7 @@ def test_library_exports_every_declared_function(svf_lib):
 
 
 def test_abi_version_and_status_strings(svf_lib):
-    assert svf_lib.svf_abi_version() == 3
+    assert svf_lib.svf_abi_version() == 4
     assert svf_lib.svf_status_string(svf.SVF_EINVAL) == b"invalid argument"
 
 
