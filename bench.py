@@ -910,7 +910,8 @@ def run_ours(args):
                         "tiles the tensor cores execute"},
             "phases_ms": {"luminance": ms_lum / args.steps, "init": ms_init / args.steps,
                           "ndf_gemm": ms_ndf / args.steps, "lm": ms_fit / args.steps},
-            "lm_work": {"jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
+            "lm_work": {"kernel_config": {"threads": stats[-1].lm_threads, "slots": stats[-1].lm_slots},
+                        "jacobian_passes": jac / args.steps, "residual_passes": res / args.steps,
                         "failed_texels": failed, "mean_rmse": float(head_rmse.mean()),
                         "median_rmse": float(np.median(head_rmse)), "ground_truth_error": head_truth_err},
             "clocks": clk, "e2e": e2e, "rgb_fit": rgb_fit, "learned_init": learned, "fib151_768x768": fib,

@@ -1664,20 +1664,23 @@ constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : 2; }
 
 // Pair passes: 0 plain, 1 paired FP32 instructions (worker_pass2), 2 J^T J on
 // the tensor cores (worker_pass_tc); 1 and 2 for the luminance fit without a
-// Fresnel factor.
+// Fresnel factor.  3: the row fit of LSF_OPTION_FIT_TOP (worker_pass_row), its
+// own instance so that the other passes carry no branch for it.
 enum : int
 {
     kPassPlain = 0,
     kPassPacked = 1,
-    kPassTc = 2
+    kPassTc = 2,
+    kPassRow = 3
 };
 
 template <class M, int NW, int S, bool kFresnel, bool kAllUp, int kPass>
 __global__ void __launch_bounds__(32 * (NW + 1), kPass == kPassPacked ? 1 : min_blocks(32 * (NW + 1)))
     lm_fit_kernel(LmArgs args)
 {
-    static_assert(kPass == kPassPlain || (!M::kRgb && !kFresnel),
-                  "the packed and tensor-core passes are the luminance fit without Fresnel");
+    static_assert(kPass == kPassPlain || (!M::kRgb && (!kFresnel || kPass == kPassRow)),
+                  "the packed and tensor-core passes are the luminance fit without Fresnel, the row pass "
+                  "the luminance fit");
     __shared__ __align__(16) float tc_rows[kPass == kPassTc ? NW * kTcWarpFloats : 4];
     constexpr uint32_t kThreads = 32 * (NW + 1);
     using SM = SlotSmem<NW, M>;
@@ -1708,13 +1711,10 @@ __global__ void __launch_bounds__(32 * (NW + 1), kPass == kPassPacked ? 1 : min_
                 break;
             if(cmd == kSlotPass)
             {
-                if(!M::kRgb && args.cfg.row_fit)
-                {
-                    if constexpr(!M::kRgb)
-                        worker_pass_row<NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc,
-                                                              reinterpret_cast<const float*>(slab_of(s)), slots[s].L,
-                                                              args.cfg.fresnel, red_of(s), redd_of(s), wwarp, lane);
-                }
+                if constexpr(kPass == kPassRow)
+                    worker_pass_row<NW, kFresnel, kAllUp>(tab_of(s), slots[s].pc,
+                                                          reinterpret_cast<const float*>(slab_of(s)), slots[s].L,
+                                                          args.cfg.fresnel, red_of(s), redd_of(s), wwarp, lane);
                 else if constexpr(kPass == kPassPacked)
                     worker_pass2<NW, kAllUp>(tab_of(s), slots[s].pc, reinterpret_cast<const float*>(slab_of(s)),
                                              slots[s].L, red_of(s), redd_of(s), wwarp, lane);
@@ -1908,7 +1908,18 @@ template <class M>
 KernelFn kernel_for_model(LmKernelChoice c, bool fresnel, bool all_up)
 {
     if constexpr(!M::kRgb)
-        if(c.pass == kPassPacked && !fresnel)
+        if(c.pass == kPassRow)
+        {
+            // a row slab is L floats: one configuration serves every layout
+            if(c.threads != 256 || c.slots != 2)
+                return nullptr;
+            if(fresnel)
+                return all_up ? lm_fit_kernel<LumModel, 7, 2, true, true, kPassRow>
+                              : lm_fit_kernel<LumModel, 7, 2, true, false, kPassRow>;
+            return all_up ? lm_fit_kernel<LumModel, 7, 2, false, true, kPassRow>
+                          : lm_fit_kernel<LumModel, 7, 2, false, false, kPassRow>;
+        }
+        else if(c.pass == kPassPacked && !fresnel)
         {
             if(c.threads == 256 && c.slots == 3)
                 return pick_pass<7, 3, kPassPacked>(all_up);
@@ -1951,20 +1962,28 @@ KernelFn kernel_for(LmKernelChoice c, bool fresnel, bool all_up, bool rgb)
 
 LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
 {
-    // Untuned: the candidate with the most worker warps resident per SM (ties:
-    // the earlier one), counting a single-slot CTA's at half (its workers wait
-    // for the control warp between passes); at large L only fewer slots fit.
+    // The candidate with the most texels in flight per SM (resident CTAs x
+    // slots, a single-slot CTA's counted at half: its workers wait for the
+    // control warp between passes); ties go to more CTAs (more control warps
+    // running the FP64 steps side by side), then to more worker warps.
+    // Measured on the B200 (full launches): ring-81 slabs, 160000 texels --
+    // 128 threads x 2 slots (3 CTAs, 6 texels per SM) 52.2 ms, 256 x 2 54.7,
+    // 256 x 3 55.9, 128 x 3 57.7; Fibonacci-151 slabs, 589824 texels --
+    // 256 x 2 (1 CTA) 564 ms, 256 x 1 (2 CTAs) 595, 128 x 2 773.
     LmKernelChoice cand[5];
     const int n = lm_candidates(L, cand, 5);   // the plain passes
-    int best = -1, best_w = 0;
+    int best = -1, best_t = 0, best_c = 0, best_w = 0;
     for(int i = 0; i < n; ++i)
     {
         const int ctas = lm_max_ctas_per_sm(L, lum_stride, cand[i], rgb);
-        const int w = ctas * (cand[i].threads / 32 - 1) * (cand[i].slots >= 2 ? 2 : 1);
-        if(w > best_w)
+        const int t = ctas * (cand[i].slots >= 2 ? 2 * cand[i].slots : 1);   // half-texels in flight
+        const int w = ctas * (cand[i].threads / 32 - 1);
+        if(ctas > 0 && (t > best_t || (t == best_t && (ctas > best_c || (ctas == best_c && w > best_w)))))
         {
-            best_w = w;
             best = i;
+            best_t = t;
+            best_c = ctas;
+            best_w = w;
         }
     }
     return best >= 0 ? cand[best] : cand[0];
