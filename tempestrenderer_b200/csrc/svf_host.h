@@ -264,12 +264,15 @@ struct LmRun
     bool all_up = false;
     bool rgb = false;      // the 11-parameter RGB fit
     float damping = 0.0f;  // initial damping scale of a single-segment run (0: the reference's rule)
+    uint32_t base = 0;     // first texel of the launch (texels are base .. base + texels - 1)
 };
 
 svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r, svf::LmKernelChoice c);
 svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o);
 svf::LmKernelChoice lm_choice(Layout* lay, uint64_t stride, bool rgb);
 svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmRun& r);
+// An LM run over r.seg[0 .. r.n_seg), segment i of layout lays[i].
+svf_status run_lm_segments(svf_ctx* ctx, Layout* const* lays, const svf_lsq_options* o, const LmRun& r);
 
 // ---- the multi-scattering fit (svf_host_ms.cpp)
 svf_status run_ms_fit(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const float* lum, uint64_t stride,

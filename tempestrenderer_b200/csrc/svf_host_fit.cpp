@@ -738,7 +738,6 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                     SVF_CUDA(cudaMemsetAsync(ctx->init.as<float>() + 7 * p.k0, 0, sizeof(float) * 7 * p.count,
                                              ctx->stream));
             svf::LmSegment ls[svf::kLmMaxSegments];
-            Layout* lbig = it[ch[0].b].lay;
             bool lup = true;
             uint64_t lstride = 0;
             for(size_t i = 0; i < ch.size(); ++i)
@@ -748,22 +747,23 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                                         x.lay->geo.as<float>(), initial_damping(opts[ch[i].b]) };
                 lup = lup && x.lay->all_up;
                 lstride = std::max(lstride, x.stride);
-                if(x.lay->L > lbig->L)
-                    lbig = x.lay;
             }
             LmRun lr{ nullptr, lstride, ctx->init.as<float>(), ctx->out.as<float>(), ctx->rmse.as<float>(),
                       ctx->stats.as<svf_texel_stats>(), nullptr, nullptr, nullptr, nullptr, nullptr, n,
                       ls, (uint32_t)ch.size(), lup, false };
-            SVF_TRY(run_lm(ctx, lbig, &opts[0].lsq, lr));
+            std::vector<Layout*> llays(ch.size());
+            for(size_t i = 0; i < ch.size(); ++i)
+                llays[i] = it[ch[i].b].lay;
+            SVF_TRY(run_lm_segments(ctx, llays.data(), &opts[0].lsq, lr));
             for(auto& p : ch)
                 if(it[p.b].default_init || it[p.b].mlp)
                     SVF_CUDA(svf::launch_rgb_init(ctx->out.as<float>() + 7 * p.k0, ctx->avg.as<float>() + 3 * p.k0,
                                                   p.count, init_used + 12 * p.k0, ctx->stream));
         }
         SVF_CUDA(cudaEventRecord(ctx->ev[2], ctx->stream));
-        // one LM launch over the pieces, whatever their layouts
+        // LM over the pieces, whatever their layouts: one launch per run of pieces
+        // whose layouts choose the same kernel configuration
         svf::LmSegment seg[svf::kLmMaxSegments];
-        Layout* big = it[ch[0].b].lay;
         bool all_up = true;
         uint64_t max_stride = 0;
         for(size_t i = 0; i < ch.size(); ++i)
@@ -779,14 +779,15 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
                                          x.lay->geo.as<float>(), dmp };
             all_up = all_up && x.lay->all_up;
             max_stride = std::max(max_stride, rgb ? x.stride3 : x.stride);
-            if(x.lay->L > big->L)
-                big = x.lay;
         }
         float* mb = ctx->maps_buf.as<float>();
         LmRun r{ nullptr, max_stride, init_used, ctx->out.as<float>(), ctx->rmse.as<float>(),
                  ctx->stats.as<svf_texel_stats>(), ctx->avg.as<float>(), mb, mb + 3 * n, mb + 6 * n, mb + 8 * n, n,
                  seg, (uint32_t)ch.size(), all_up, rgb };
-        SVF_TRY(run_lm(ctx, big, &opts[0].lsq, r));
+        std::vector<Layout*> lays(ch.size());
+        for(size_t i = 0; i < ch.size(); ++i)
+            lays[i] = it[ch[i].b].lay;
+        SVF_TRY(run_lm_segments(ctx, lays.data(), &opts[0].lsq, r));
         SVF_CUDA(cudaEventRecord(ctx->ev[3], ctx->stream));
         // outputs, piece by piece
         std::vector<svf_texel_stats> st(n);

@@ -196,6 +196,46 @@ svf_status run_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const LmR
     return launch_lm(ctx, lay, o, r, lm_choice(lay, r.stride, r.rgb));
 }
 
+// Consecutive segments whose layouts choose the same kernel configuration
+// share a launch, so that every texel is fitted by the configuration of its own
+// layout's single fit: a texel's result depends on the number of worker warps
+// through the order of its reductions, and this keeps a batch bit-identical to
+// fitting its BTFs one by one.
+svf_status run_lm_segments(svf_ctx* ctx, Layout* const* lays, const svf_lsq_options* o, const LmRun& r)
+{
+    const uint32_t n = r.n_seg;
+    std::vector<svf::LmKernelChoice> ch(n);
+    for(uint32_t i = 0; i < n; ++i)
+    {
+        if(!r.rgb && !lays[i]->tuned && r.texels >= 4096)
+            SVF_TRY(tune_lm(ctx, lays[i], o));
+        ch[i] = lm_choice(lays[i], r.seg[i].stride, r.rgb);
+    }
+    for(uint32_t a = 0; a < n;)
+    {
+        uint32_t b = a + 1;
+        while(b < n && ch[b].threads == ch[a].threads && ch[b].slots == ch[a].slots && ch[b].pass == ch[a].pass)
+            ++b;
+        LmRun rr = r;
+        rr.seg = r.seg + a;
+        rr.n_seg = b - a;
+        rr.base = r.seg[a].first;
+        rr.texels = (b < n ? (uint64_t)r.seg[b].first : r.texels) - r.seg[a].first;
+        rr.all_up = true;
+        Layout* big = lays[a];
+        for(uint32_t i = a; i < b; ++i)
+        {
+            rr.all_up = rr.all_up && lays[i]->all_up;
+            if(lays[i]->L > big->L)
+                big = lays[i];
+        }
+        if(rr.texels > 0)
+            SVF_TRY(launch_lm(ctx, big, o, rr, ch[a]));
+        a = b;
+    }
+    return SVF_OK;
+}
+
 // The parameters LM holds: the diffuse albedo (at 0) without SVF_LSQ_DIFFUSE,
 // the Euler angles with SVF_LSQ_DISABLE_DIRECTION_FITTING (the luminance fit).
 void lm_masks(const svf_lsq_options* o, svf::LmConfig& cfg)
@@ -258,6 +298,7 @@ svf_status launch_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o, const 
     a.map_sigma = r.sigma;
     a.map_basis = r.basis;
     a.texels = (uint32_t)r.texels;
+    a.texel_base = r.base;
     a.cfg.max_iter = o->max_iterations;
     a.cfg.mse_target = o->mse_target;
     a.cfg.eps = o->break_on_small_step;

@@ -53,7 +53,8 @@ struct LmArgs
     float* map_specular;       // [texels][3] or null
     float* map_sigma;          // [texels][2] or null
     float* map_basis;          // [texels][4] or null
-    uint32_t texels;
+    uint32_t texels;           // texels of this launch: texel_base .. texel_base + texels - 1
+    uint32_t texel_base;
     uint32_t all_up;           // every direction of every segment has z > 0
     uint32_t rgb;              // the 11-parameter RGB fit (svf_lm.cu RgbModel)
     LmConfig cfg;

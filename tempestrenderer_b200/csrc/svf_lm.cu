@@ -1500,9 +1500,10 @@ __device__ void write_texel(const LmArgs& args, LmState<M::P>& st, uint32_t t, d
 template <class M>
 __device__ __forceinline__ void slot_fetch(const LmArgs& args, Slot<M>& sl, void* slab)
 {
-    const uint32_t t = sl.dead ? kNoTexel : atomicAdd(args.work_counter, 1u);
-    if(t < args.texels)
+    const uint32_t c = sl.dead ? kNoTexel : atomicAdd(args.work_counter, 1u);
+    if(c < args.texels)
     {
+        const uint32_t t = args.texel_base + c;
         uint32_t k = 0;
         for(uint32_t i = 1; i < args.n_seg; ++i)
             if(t >= args.seg[i].first)
