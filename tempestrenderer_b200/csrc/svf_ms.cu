@@ -160,26 +160,44 @@ __device__ __forceinline__ void sincos_tan(float w, float* s, float* c)
 // SGGXProjectedArea (ggx-models-impl.hh:102-105)
 __device__ __forceinline__ float projected_area(V3 sd, const M3& b, V3 w) { return len(mul(rot_inverse(b, w), sd)); }
 
-// SGGXMicroFlakeNDF(stddev, basis, normal) (ggx-models-impl.hh:49-57)
-__device__ __forceinline__ float sggx_ndf(V3 sd, const M3& b, V3 n)
+// SGGXMicroFlakeNDF(stddev, basis, normal) (ggx-models-impl.hh:49-57), split
+// into what one evaluation's parameters fix (the inverse covariance, its
+// determinant test and the numerator 0.5 sqrt(det)) and the per-normal rest;
+// the same operations in the same order as the reference's single function.
+struct NdfConst
+{
+    M3 ic;
+    float num;   // 0.5 sqrt(det); 0 where det < 1e-6 (the reference returns 0)
+};
+
+__device__ __forceinline__ NdfConst ndf_const(V3 sd, const M3& b)
 {
     const V3 sq = mul(sd, sd);
-    const M3 ic = covariance(b, v3(1.0f / sq.x, 1.0f / sq.y, 1.0f / sq.z));
+    NdfConst k;
+    k.ic = covariance(b, v3(1.0f / sq.x, 1.0f / sq.y, 1.0f / sq.z));
+    const M3& ic = k.ic;
     // Matrix3::determinant (matrix3.hh:193-201), Elements[i][j] = column i, row j
     const float det = ic.c[0].x * (ic.c[1].y * ic.c[2].z - ic.c[1].z * ic.c[2].y) -
                       ic.c[1].x * (ic.c[0].y * ic.c[2].z - ic.c[0].z * ic.c[2].y) +
                       ic.c[2].x * (ic.c[0].y * ic.c[1].z - ic.c[0].z * ic.c[1].y);
-    if(det < 1e-6f)
+    k.num = det < 1e-6f ? 0.0f : 0.5f * sqrtf(det);
+    return k;
+}
+
+__device__ __forceinline__ float sggx_ndf(const NdfConst& k, V3 n)
+{
+    if(k.num == 0.0f)
         return 0.0f;
-    const float den = dot(n, transform(ic, n));
-    return 0.5f * sqrtf(det) / (kPi * den * den);
+    const float den = dot(n, transform(k.ic, n));
+    return k.num / (kPi * den * den);
 }
 
 // SGGXMicroFlakeSampleIncidentLight (ggx-models-impl.hh:554-570): a visible
 // normal of the distribution seen from `wo`, and wo reflected about it.  The
 // reference's GCC build evaluates the two FastFloatRand arguments of
 // UniformSampleSphere right to left: the second draws first.
-__device__ __forceinline__ V3 sample_incident(V3 wo, V3 sd, const M3& b, unsigned& seed)
+// cov: Matrix3::transformCovariance of the basis by stddev^2, fixed per evaluation.
+__device__ __forceinline__ V3 sample_incident(V3 wo, const M3& cov, unsigned& seed)
 {
     const float rb = lcg(seed);
     const float ra = lcg(seed);
@@ -190,7 +208,7 @@ __device__ __forceinline__ V3 sample_incident(V3 wo, V3 sd, const M3& b, unsigne
     const float st = sqrtf(1.0f - ct * ct);
     const V3 u = v3(c * st, s * st, ct);
     const M3 ob = basis_of(wo);
-    const M3 S = mmul(mmul(ob, covariance(b, mul(sd, sd))), transpose(ob));
+    const M3 S = mmul(mmul(ob, cov), transpose(ob));
     const V3 vn = transform(ob, normalize(rot_inverse(cholesky(S), u)));
     return reflect(wo, vn);
 }
@@ -215,7 +233,10 @@ __device__ void pseudo_volume(const float* spec, const float* diff, V3 sd, const
     const float in_density = projected_area(sd, b, wi);
     const V3 h = normalize(add(wo, wi));
     const float contrib = (float)samples / (out_density + in_density * dot_out / dot_inc);
-    const float ndf = sggx_ndf(sd, b, h);
+    // what the evaluation's parameters fix, computed once (the reference recomputes it per call)
+    const NdfConst nk = ndf_const(sd, b);
+    const M3 cov = covariance(b, mul(sd, sd));
+    const float ndf = sggx_ndf(nk, h);
     float rad[C], thr[C];
 #pragma unroll
     for(int c = 0; c < C; ++c)
@@ -236,7 +257,7 @@ __device__ void pseudo_volume(const float* spec, const float* diff, V3 sd, const
                 alive = alive && thr[c] > 1e-3f;
             if(!alive)
                 break;
-            const V3 inc_l = sample_incident(out_l, sd, b, seed);
+            const V3 inc_l = sample_incident(out_l, cov, seed);
             dd = projected_area(sd, b, inc_l);
             out_l = v3(-inc_l.x, -inc_l.y, -inc_l.z);
             depth_in += (-logf(lcg(seed)) / dd) * out_l.z;
@@ -245,7 +266,7 @@ __device__ void pseudo_volume(const float* spec, const float* diff, V3 sd, const
             const float ext = expf(-in_density * (depth_in / dot_inc));
             if(ext < 1e-9f)
                 break;
-            const float f = sggx_ndf(sd, b, normalize(add(out_l, wi))) * 2.0f / (4.0f * dd);
+            const float f = sggx_ndf(nk, normalize(add(out_l, wi))) * 2.0f / (4.0f * dd);
 #pragma unroll
             for(int c = 0; c < C; ++c)
             {
