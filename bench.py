@@ -265,7 +265,12 @@ def config3_item(svf, ctx, layout, model, steps, dev, side=1024):
                         "failed_texels": int(lrs.failed_texels)},
             "speedup": pms / lms,
             "residual_ratio": {"mean": float(lrm.mean() / prm.mean()), "median": float(np.median(ratio)),
-                               "within_1pct": float(np.mean(ratio <= 1.01))}}
+                               "within_1pct": float(np.mean(ratio <= 1.01)),
+                               # the reference's LM stops at MSE <= 1e-6 (fitting.hh:557): a texel whose RMSE
+                               # is at or below 1e-3 has met its own target whatever the other fit reached
+                               "within_1pct_or_at_target": float(np.mean((ratio <= 1.01) | (lrm <= 1e-3))),
+                               "learned_at_target": float(np.mean(lrm <= 1e-3)),
+                               "plain_at_target": float(np.mean(prm <= 1e-3))}}
 
 
 def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, truth=None):
@@ -670,6 +675,7 @@ def summarize(line, parity):
         out["config3"] = {"speedup_vs_plain_gpu_lm": r3(c3["speedup"]),
                           "speedup_with_fallback": r3(c3.get("with_fallback", {}).get("speedup")),
                           "residual_ratio_mean": r3(c3["residual_ratio"]["mean"]),
+                          "within_1pct_or_at_target": r3(c3["residual_ratio"].get("within_1pct_or_at_target")),
                           "residual_ratio_mean_with_fallback": r3(c3.get("with_fallback", {}).get("residual_ratio_mean")),
                           "normal_p90_deg": {"plain": r3(c3["plain"]["ground_truth_error"]["normal_deg"]["p90"]),
                                              "learned": r3(c3["learned"]["ground_truth_error"]["normal_deg"]["p90"]),

@@ -451,6 +451,9 @@ def _bind_harness(L):
         L.ref_fit_texel.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, _f32p, _f32p, _f32p,
                                     C.POINTER(C.c_float), _u32p, C.c_void_p, C.c_void_p]
         L.ref_fit_texel.restype = C.c_int
+        L.ref_fit_texel_opts.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_float, C.c_uint32, C.c_uint32,
+                                         C.c_uint32, _f32p, _f32p, _f32p, C.POINTER(C.c_float), _u32p]
+        L.ref_fit_texel_opts.restype = C.c_int
         L.ref_time_fit_texels.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.c_float, C.c_void_p]
         L.ref_time_fit_texels.restype = C.c_double
@@ -527,6 +530,18 @@ class RefBTF:
             raise RuntimeError("reference pipeline did not reach LeastSquaresFitSGGX")
         return dict(init=init7, fit=fit7, maps=maps, rmse=rmse.value, iterations=int(st[0]),
                     effective=int(st[1]), ndf=ndf)
+
+    def fit_texel_opts(self, x, y=0, fresnel=1.0, flags=LSF_OPTON_DIFFUSE, downsample=0xFFFFFFFF,
+                       bounces=0xFFFFFFFF):
+        """The pipeline's fit of texel (x, y) with the given LeastSquaresFitOptions."""
+        init7, fit7, maps = np.zeros(7, np.float32), np.zeros(7, np.float32), np.zeros(12, np.float32)
+        rmse = C.c_float()
+        st = np.zeros(2, np.uint32)
+        rc = self.lib.ref_fit_texel_opts(self.handle, x, y, fresnel, flags, downsample, bounces, init7, fit7, maps,
+                                         C.byref(rmse), st)
+        if rc != 0:
+            raise RuntimeError("reference pipeline did not reach LeastSquaresFitSGGX")
+        return dict(init=init7, fit=fit7, maps=maps, rmse=rmse.value, iterations=int(st[0]), effective=int(st[1]))
 
     def time_fit(self, first, count, workers, pool_threads, fresnel=1.0):
         rm = np.zeros(count, np.float32)

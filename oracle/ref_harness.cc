@@ -300,14 +300,33 @@ void ref_lsq(const float* lights_parabolic, uint32_t light_count, const float* l
  *   rmse, stats (iterations, effective iterations),
  *   ndf    - the 64x64 NDF texture (may be null),
  *   lum    - the luminance slice (may be null). */
+static int FitTexel(void* handle, uint32_t x, uint32_t y, const LeastSquaresFitOptions& opts_in, float* init7,
+                    float* fit7, float* maps12, float* rmse, uint32_t* stats, float* ndf, float* lum);
+
 int ref_fit_texel(void* handle, uint32_t x, uint32_t y, float fresnel,
                   float* init7, float* fit7, float* maps12, float* rmse, uint32_t* stats, float* ndf, float* lum)
+{
+    return FitTexel(handle, x, y, MakeOptions(fresnel, LSF_OPTON_DIFFUSE), init7, fit7, maps12, rmse, stats, ndf,
+                    lum);
+}
+
+/* The same with LeastSquaresFitOptions::Flags, DownSampleLightView and
+ * MultiScatteringBounceCount as given (~0u: off). */
+int ref_fit_texel_opts(void* handle, uint32_t x, uint32_t y, float fresnel, uint32_t flags, uint32_t downsample,
+                       uint32_t bounces, float* init7, float* fit7, float* maps12, float* rmse, uint32_t* stats)
+{
+    return FitTexel(handle, x, y, MakeOptions(fresnel, flags, downsample, bounces), init7, fit7, maps12, rmse, stats,
+                    nullptr, nullptr);
+}
+
+static int FitTexel(void* handle, uint32_t x, uint32_t y, const LeastSquaresFitOptions& opts_in, float* init7,
+                    float* fit7, float* maps12, float* rmse, uint32_t* stats, float* ndf, float* lum)
 {
     auto* btf = reinterpret_cast<Tempest::BTF*>(handle);
     auto* pool = SerialPool();
     SVBRDFFitPipeline pipeline(btf);
     auto popts = MakePipelineOptions();
-    auto opts = MakeOptions(fresnel, LSF_OPTON_DIFFUSE);
+    auto opts = opts_in;
     SGGXParameters out;
     g_record_valid = false;
     pipeline.cache(0, *pool, x, y, popts, nullptr);

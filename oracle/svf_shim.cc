@@ -37,8 +37,9 @@ void LeastSquaresFitSGGX(uint32_t id, Tempest::ThreadPool& pool, const Tempest::
     }
     // what svf_lsq_fit_sggx does not implement stays with the CPU path
     // (LSF_OPTION_CUDA asks for the GPU fit, which this is)
-    if(opts.DownSampleLightView != ~0u || (opts.Flags & ~(LSF_OPTON_DIFFUSE | LSF_OPTION_CUDA)) != 0 ||
-       opts.MultiScatteringBounceCount != ~0u)
+    constexpr uint32_t handled = LSF_OPTON_DIFFUSE | LSF_OPTION_CUDA | LSF_OPTION_DISABLE_DIRECTION_FITTING |
+                                 LSF_OPTION_FIT_TOP;
+    if((opts.Flags & ~handled) != 0)
     {
         Tempest::Log(Tempest::LogLevel::Error, "svf_lsq_fit_sggx: unsupported LeastSquaresFitOptions");
         *opt_parameters = parameters;
@@ -50,6 +51,20 @@ void LeastSquaresFitSGGX(uint32_t id, Tempest::ThreadPool& pool, const Tempest::
     o.fresnel = opts.Fresnel;
     if(!(opts.Flags & LSF_OPTON_DIFFUSE))
         o.flags &= ~SVF_LSQ_DIFFUSE;
+    if(opts.Flags & LSF_OPTION_DISABLE_DIRECTION_FITTING)
+        o.flags |= SVF_LSQ_DISABLE_DIRECTION_FITTING;
+    if(opts.Flags & LSF_OPTION_FIT_TOP)
+        o.flags |= SVF_LSQ_FIT_TOP;
+    // DownSampleLightView ~0u (or not below the direction count): all directions
+    if(opts.DownSampleLightView < btf->LightCount)
+        o.downsample_light_view = opts.DownSampleLightView;
+    // svbrdffit -m: the pseudo-volume model, fitted by the reference's LM as written
+    if(opts.MultiScatteringBounceCount != ~0u)
+    {
+        o.flags |= SVF_LSQ_MULTI_SCATTERING;
+        o.flags &= ~SVF_LSQ_STEP_PER_PARAMETER;
+        o.multi_scattering_bounces = opts.MultiScatteringBounceCount;
+    }
     o.max_iterations = CurveFitSteps;
     svf_texel_stats st{};
     const svf_status s = svf_lsq_fit_sggx(g_svf, &btf->LightsParabolic[0].x, btf->LightCount, lv_lum_slice, &o,

@@ -66,3 +66,35 @@ def test_shim_pipeline_maps_equal_gpu_maps(gpu_ctx, golden, shim_fits):
         np.testing.assert_allclose(maps["basis"][x], ref[2:6], rtol=0, atol=2e-6)
         np.testing.assert_allclose(maps["diffuse"][x], ref[6:9], rtol=2e-5, atol=1e-8)
         np.testing.assert_allclose(maps["specular"][x], ref[9:12], rtol=2e-5, atol=1e-8)
+
+
+@pytest.mark.parametrize("case", ["nodir", "specular", "top", "down41", "ms1"])
+def test_shim_pipeline_with_options(gpu_ctx, golden, oracle_lib, case):
+    """The reference pipeline through the shim with LeastSquaresFitOptions beyond the
+    default -- direction fitting disabled, the specular-only fit, LSF_OPTION_FIT_TOP,
+    DownSampleLightView 41, MultiScatteringBounceCount 1 (svbrdffit -m) -- gives
+    svf_lsq_fit_sggx's fit of the same options, bit for bit."""
+    if not oracle_lib.ref_svf_available():
+        pytest.fail("oracle/_ref/libtempest_ref_svf.so is not built (oracle/Makefile target shim)")
+    O = oracle_lib
+    flags, down, bounces = {"nodir": (O.LSF_OPTON_DIFFUSE | O.LSF_OPTION_DISABLE_DIRECTION_FITTING, None, None),
+                            "specular": (0, None, None),
+                            "top": (O.LSF_OPTON_DIFFUSE | O.LSF_OPTION_FIT_TOP, None, None),
+                            "down41": (O.LSF_OPTON_DIFFUSE, 41, None),
+                            "ms1": (O.LSF_OPTON_DIFFUSE, None, 1)}[case]
+    p = golden["pipeline"]
+    lp = golden["mesh"]["lights_parabolic"]
+    x = 3
+    rgb = O.synth_render(int(p["seed"]), x, O.synth_truth(int(p["seed"]), int(p["mix"]), x), lp)[None]
+    btf = O.RefBTF.from_texels(golden["angles"], rgb, lib=O.ref_svf())
+    r = btf.fit_texel_opts(0, flags=flags, downsample=0xFFFFFFFF if down is None else down,
+                           bounces=0xFFFFFFFF if bounces is None else bounces)
+    lum, _ = btf.lum_slice(0)
+    opts = svf.options(diffuse=bool(flags & O.LSF_OPTON_DIFFUSE),
+                       fit_direction=not (flags & O.LSF_OPTION_DISABLE_DIRECTION_FITTING),
+                       fit_top=bool(flags & O.LSF_OPTION_FIT_TOP), downsample=down or 0, multi_scattering=bounces)
+    if bounces is not None:
+        opts.flags &= ~svf.SVF_LSQ_STEP_PER_PARAMETER
+    out, rmse, st = gpu_ctx.lsq_fit_sggx(lp, lum, r["init"], opts)
+    assert np.array_equal(r["fit"], out), (case, r["fit"], out)
+    assert np.float32(r["rmse"]) == np.float32(rmse)
