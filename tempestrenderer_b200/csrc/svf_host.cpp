@@ -151,8 +151,8 @@ svf_status check_options(const svf_lsq_options* o, bool downsample_ok, bool ms_o
 
 svf_status get_layout(svf_ctx* ctx, const float* lp_in, uint32_t L, Layout** out)
 {
-    if(L < 3 || L > 160)
-        return fail(SVF_EINVAL, "light_count must be in [3, 160], got %u", L);
+    if(L < 3 || L > svf::kMaxLayout)
+        return fail(SVF_EINVAL, "light_count must be in [3, %u], got %u", svf::kMaxLayout, L);
     if(!lp_in)
         return fail(SVF_EINVAL, "null lights_parabolic");
     std::vector<float> lp(2 * L);

@@ -27,6 +27,9 @@ struct LmConfig
 // A run of texels of one direction layout in an LM launch: texels
 // [first, next segment's first) take their slabs from lum + (t - first) * stride.
 constexpr int kLmMaxSegments = 16;
+// The largest direction layout the library takes (light_count; L^2 pairs).
+constexpr uint32_t kMaxLayout = 160;
+
 struct LmSegment
 {
     uint32_t     first;        // first texel of the segment (segments in increasing order, seg[0].first = 0)
