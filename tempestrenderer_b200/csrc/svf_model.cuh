@@ -79,8 +79,8 @@ SVF_HD void sincos_f(float x, float* s, float* c)
 
 SVF_HD void finish_param_set(ParamSet& ps);
 
-// ToQuaternion(euler) (include/tempest/math/quaternion.hh:82-94) and its
-// derivative, then ToMatrix3 (quaternion.hh:122-139) and R^T dR/de_k.
+// ToQuaternion(euler) (include/tempest/math/quaternion.hh:82-94), then
+// ToMatrix3 (quaternion.hh:122-139) and the body rates R^T dR/de_k in closed form.
 SVF_HD void make_param_set(const float* p, ParamSet& ps)
 {
     ps.sx = p[0] > 0.0f ? p[0] : 0.0f;
@@ -100,13 +100,6 @@ SVF_HD void make_param_set(const float* p, ParamSet& ps)
     sincos_f(0.5f * p[6], &s3, &c3);
     float q[4] = { s1 * c2 * c3 + c1 * s2 * s3, -s1 * c2 * s3 + c1 * s2 * c3,
                    c1 * c2 * s3 + s1 * s2 * c3, c1 * c2 * c3 - s1 * s2 * s3 };
-    float dq[3][4] = {
-        { 0.5f * (c1 * c2 * c3 - s1 * s2 * s3), 0.5f * (-c1 * c2 * s3 - s1 * s2 * c3),
-          0.5f * (-s1 * c2 * s3 + c1 * s2 * c3), 0.5f * (-s1 * c2 * c3 - c1 * s2 * s3) },
-        { 0.5f * (-s1 * s2 * c3 + c1 * c2 * s3), 0.5f * (s1 * s2 * s3 + c1 * c2 * c3),
-          0.5f * (-c1 * s2 * s3 + s1 * c2 * c3), 0.5f * (-c1 * s2 * c3 - s1 * c2 * s3) },
-        { 0.5f * (-s1 * c2 * s3 + c1 * s2 * c3), 0.5f * (-s1 * c2 * c3 - c1 * s2 * s3),
-          0.5f * (c1 * c2 * c3 - s1 * s2 * s3), 0.5f * (-c1 * c2 * s3 - s1 * s2 * c3) } };
     // the lobe uses ToMatrix3(Normalize(q)) (ggx-models-impl.hh:520)
     float ql = sqrtf(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
     float rq = rcp_model(ql);
@@ -115,27 +108,20 @@ SVF_HD void make_param_set(const float* p, ParamSet& ps)
     R[0] = 1.0f - 2.0f * (y * y + z * z); R[1] = 2.0f * (x * y + z * w);        R[2] = 2.0f * (x * z - y * w);
     R[3] = 2.0f * (x * y - z * w);        R[4] = 1.0f - 2.0f * (x * x + z * z); R[5] = 2.0f * (y * z + x * w);
     R[6] = 2.0f * (x * z + y * w);        R[7] = 2.0f * (y * z - x * w);        R[8] = 1.0f - 2.0f * (x * x + y * y);
-    for(int k = 0; k < 3; ++k)
-    {
-        float dx = dq[k][0] * rq, dy = dq[k][1] * rq, dz = dq[k][2] * rq, dw = dq[k][3] * rq;
-        float dR[9];
-        dR[0] = -4.0f * (y * dy + z * dz);
-        dR[1] = 2.0f * (dx * y + x * dy + dz * w + z * dw);
-        dR[2] = 2.0f * (dx * z + x * dz - dy * w - y * dw);
-        dR[3] = 2.0f * (dx * y + x * dy - dz * w - z * dw);
-        dR[4] = -4.0f * (x * dx + z * dz);
-        dR[5] = 2.0f * (dy * z + y * dz + dx * w + x * dw);
-        dR[6] = 2.0f * (dx * z + x * dz + dy * w + y * dw);
-        dR[7] = 2.0f * (dy * z + y * dz - dx * w - x * dw);
-        dR[8] = -4.0f * (x * dx + y * dy);
-        // Omega[i][j] = column_i(R) . column_j(dR); w = (O21 - O12, O02 - O20, O10 - O01)/2
-        auto O = [&](int i, int j) {
-            return R[3 * i] * dR[3 * j] + R[3 * i + 1] * dR[3 * j + 1] + R[3 * i + 2] * dR[3 * j + 2];
-        };
-        ps.om[k][0] = 0.5f * (O(2, 1) - O(1, 2));
-        ps.om[k][1] = 0.5f * (O(0, 2) - O(2, 0));
-        ps.om[k][2] = 0.5f * (O(1, 0) - O(0, 1));
-    }
+    // q = qx(e0) qy(e1) qz(e2), so R = Rx(e0) Ry(e1) Rz(e2) and the body-frame
+    // angular velocities (R^T dR/de_k = [w_k]x) are w_2 = z, w_1 = Rz^T y and
+    // w_0 = (Ry Rz)^T x, from the half-angle sines and cosines already at hand.
+    const float sb = 2.0f * s2 * c2, cb = (c2 - s2) * (c2 + s2);   // sin, cos of e1
+    const float sc = 2.0f * s3 * c3, cc = (c3 - s3) * (c3 + s3);   // sin, cos of e2
+    ps.om[0][0] = cc * cb;
+    ps.om[0][1] = -sc * cb;
+    ps.om[0][2] = sb;
+    ps.om[1][0] = sc;
+    ps.om[1][1] = cc;
+    ps.om[1][2] = 0.0f;
+    ps.om[2][0] = 0.0f;
+    ps.om[2][1] = 0.0f;
+    ps.om[2][2] = 1.0f;
 
     finish_param_set(ps);
 }
