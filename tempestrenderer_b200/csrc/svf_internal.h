@@ -80,7 +80,7 @@ struct LmKernelChoice
     int pass;     // pair pass: 0 plain; 1 paired FP32 instructions; 2 J^T J on the tensor cores
                   // (1 and 2: luminance fit without a Fresnel factor)
 };
-constexpr int kLmCandidates = 10;
+constexpr int kLmCandidates = 12;
 LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb = false);
 int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);
 size_t         lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb = false);

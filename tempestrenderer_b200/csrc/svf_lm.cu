@@ -1661,7 +1661,9 @@ __device__ void expand_sums(const double* sums, const float* pf, double* hg)
 }
 
 // Resident CTAs per SM the register budget is sized for.
-constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : 2; }
+// Resident CTAs the register budget is sized for (128 registers a thread at
+// 128 and 160 threads).
+constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : (threads <= 160 ? 3 : 2); }
 
 // Pair passes: 0 plain, 1 paired FP32 instructions (worker_pass2), 2 J^T J on
 // the tensor cores (worker_pass_tc); 1 and 2 for the luminance fit without a
@@ -1949,6 +1951,10 @@ KernelFn kernel_for_model(LmKernelChoice c, bool fresnel, bool all_up)
         return pick<M, 3, 2>(fresnel, all_up);
     if(c.threads == 128 && c.slots == 3)
         return pick<M, 3, 3>(fresnel, all_up);
+    if(c.threads == 160 && c.slots == 2)
+        return pick<M, 4, 2>(fresnel, all_up);
+    if(c.threads == 160 && c.slots == 3)
+        return pick<M, 4, 3>(fresnel, all_up);
     if(c.threads == 256 && c.slots == 1)   // the largest slabs: one texel per CTA, no overlap
         return pick<M, 7, 1>(fresnel, all_up);
     return nullptr;
@@ -1971,8 +1977,8 @@ LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
     // 128 threads x 2 slots (3 CTAs, 6 texels per SM) 52.2 ms, 256 x 2 54.7,
     // 256 x 3 55.9, 128 x 3 57.7; Fibonacci-151 slabs, 589824 texels --
     // 256 x 2 (1 CTA) 564 ms, 256 x 1 (2 CTAs) 595, 128 x 2 773.
-    LmKernelChoice cand[5];
-    const int n = lm_candidates(L, cand, 5);   // the plain passes
+    LmKernelChoice cand[7];
+    const int n = lm_candidates(L, cand, 7);   // the plain passes
     int best = -1, best_t = 0, best_c = 0, best_w = 0;
     for(int i = 0; i < n; ++i)
     {
@@ -1996,8 +2002,8 @@ int lm_candidates(uint32_t, LmKernelChoice* out, int max)
     // packed ones (one CTA of 256 threads per SM at their register count), then
     // the tensor-core J^T J ones (their staging rows take shared memory)
     const LmKernelChoice all[kLmCandidates] = { { 256, 3, 0 }, { 256, 2, 0 }, { 128, 3, 0 }, { 128, 2, 0 },
-                                                { 256, 1, 0 }, { 256, 3, 1 }, { 256, 4, 1 }, { 128, 3, 1 },
-                                                { 256, 2, 2 }, { 128, 3, 2 } };
+                                                { 256, 1, 0 }, { 160, 2, 0 }, { 160, 3, 0 }, { 256, 3, 1 },
+                                                { 256, 4, 1 }, { 128, 3, 1 }, { 256, 2, 2 }, { 128, 3, 2 } };
     int n = 0;
     for(int i = 0; i < kLmCandidates && n < max; ++i)
         out[n++] = all[i];

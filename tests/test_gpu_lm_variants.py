@@ -19,8 +19,8 @@ import tempestrenderer_b200 as svf
 pytestmark = pytest.mark.gpu
 
 # threads, slots, pair pass (0 plain, 1 paired FP32, 2 J^T J on the tensor cores)
-CONFIGS = ["256,3,0", "256,2,0", "128,3,0", "128,2,0", "256,1,0", "256,3,1", "256,4,1", "128,3,1", "256,2,2",
-           "128,3,2"]
+CONFIGS = ["256,3,0", "256,2,0", "128,3,0", "128,2,0", "256,1,0", "160,2,0", "160,3,0", "256,3,1", "256,4,1",
+           "128,3,1", "256,2,2", "128,3,2"]
 
 
 def _lp(golden):
