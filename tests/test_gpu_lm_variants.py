@@ -84,3 +84,23 @@ def test_lm_configuration(gpu_ctx, oracle_lib, golden, batch96, plain_batch, con
     dev = np.abs(rmse.astype(np.float64) / ref - 1.0)
     assert np.median(dev) < 1e-4 and np.mean(dev <= 1e-3) >= 0.90, np.sort(dev)[-8:]
     assert rmse.mean() <= 1.01 * ref.mean()
+
+
+def test_default_configuration_rule():
+    """Without SVF_LM_KERNEL the configuration comes from the occupancy rule
+    (svf::lm_default_choice), which ranks configurations as full B200 launches
+    measured them: 160 threads x 2 slots on ring-81 slabs (three CTAs per SM),
+    256 x 2 on Fibonacci-151 slabs (one CTA per SM fits two 91 KB slabs)."""
+    import os
+
+    import oracle
+
+    assert "SVF_LM_KERNEL" not in os.environ
+    for lp, want in ((svf.directions_ring81(), (160, 2)), (svf.directions_fibonacci(151), (256, 2))):
+        L = lp.shape[0]
+        tri, edges, angles = svf.triangulate(lp)
+        layout = svf.Layout(lp, tri, edges, angles)
+        rgb = np.stack([oracle.synth_render(3, t, oracle.synth_truth(3, 1, t), lp) for t in range(2)])
+        with svf.Context(0) as ctx:   # (a fresh context: the configuration is chosen per layout)
+            _, run = ctx.fit_texels(layout, rgb, 2, 1, want=("rmse",))
+        assert (run.lm_threads, run.lm_slots) == want, (L, run.lm_threads, run.lm_slots)
