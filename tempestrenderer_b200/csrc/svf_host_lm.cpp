@@ -56,8 +56,8 @@ svf_status tune_lm(svf_ctx* ctx, Layout* lay, const svf_lsq_options* o)
     // register count) wins on this short probe but loses on full launches
     // (measured: 59.4 against 52.2 ms for 160000 ring-81 texels), so it is left
     // to SVF_LM_KERNEL
-    svf::LmKernelChoice cand[7];
-    const int n_cand = svf::lm_candidates(lay->L, cand, 7);
+    svf::LmKernelChoice cand[svf::kLmPlainCandidates];
+    const int n_cand = svf::lm_candidates(lay->L, cand, svf::kLmPlainCandidates);
     lay->choice = cand[0];
     if(n_cand <= 1)
     {

@@ -81,6 +81,7 @@ struct LmKernelChoice
                   // (1 and 2: luminance fit without a Fresnel factor)
 };
 constexpr int kLmCandidates = 12;
+constexpr int kLmPlainCandidates = 7;   // the first candidates: plain pair passes
 LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb = false);
 int            lm_candidates(uint32_t L, LmKernelChoice* out, int max);
 size_t         lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb = false);

@@ -1663,7 +1663,7 @@ __device__ void expand_sums(const double* sums, const float* pf, double* hg)
 // Resident CTAs per SM the register budget is sized for.
 // Resident CTAs the register budget is sized for (128 registers a thread at
 // 128 and 160 threads).
-constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : (threads <= 160 ? 3 : 2); }
+constexpr int min_blocks(int threads) { return threads <= 128 ? 4 : (threads <= 160 ? 3 : (threads <= 256 ? 2 : 1)); }
 
 // Pair passes: 0 plain, 1 paired FP32 instructions (worker_pass2), 2 J^T J on
 // the tensor cores (worker_pass_tc); 1 and 2 for the luminance fit without a
@@ -1977,8 +1977,8 @@ LmKernelChoice lm_default_choice(uint32_t L, uint64_t lum_stride, bool rgb)
     // 128 threads x 2 slots (3 CTAs, 6 texels per SM) 52.2 ms, 256 x 2 54.7,
     // 256 x 3 55.9, 128 x 3 57.7; Fibonacci-151 slabs, 589824 texels --
     // 256 x 2 (1 CTA) 564 ms, 256 x 1 (2 CTAs) 595, 128 x 2 773.
-    LmKernelChoice cand[7];
-    const int n = lm_candidates(L, cand, 7);   // the plain passes
+    LmKernelChoice cand[kLmPlainCandidates];
+    const int n = lm_candidates(L, cand, kLmPlainCandidates);   // the plain passes
     int best = -1, best_t = 0, best_c = 0, best_w = 0;
     for(int i = 0; i < n; ++i)
     {
@@ -2010,13 +2010,18 @@ int lm_candidates(uint32_t, LmKernelChoice* out, int max)
     return n;
 }
 
+// SlotSmem<NW, M>::bytes for the configuration's worker count NW = threads / 32 - 1.
+template <class M>
+size_t slot_bytes(int nw, uint32_t L, uint64_t stride)
+{
+    const size_t red = (sizeof(float) * nw * M::kAcc + sizeof(double) * nw + 127) & ~size_t(127);
+    return SlotSmem<1, M>::slab_bytes(stride) + SlotSmem<1, M>::tab_bytes(L) + red;
+}
+
 size_t lm_smem_bytes(uint32_t L, uint64_t lum_stride, LmKernelChoice c, bool rgb)
 {
-    size_t per;
-    if(rgb)
-        per = c.threads == 128 ? SlotSmem<3, RgbModel>::bytes(L, lum_stride) : SlotSmem<7, RgbModel>::bytes(L, lum_stride);
-    else
-        per = c.threads == 128 ? SlotSmem<3, LumModel>::bytes(L, lum_stride) : SlotSmem<7, LumModel>::bytes(L, lum_stride);
+    const int nw = c.threads / 32 - 1;
+    const size_t per = rgb ? slot_bytes<RgbModel>(nw, L, lum_stride) : slot_bytes<LumModel>(nw, L, lum_stride);
     return per * (size_t)c.slots;
 }
 
