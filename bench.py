@@ -66,18 +66,61 @@ def log(*a):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML polled every 10 ms on a thread (read-only queries), or
+    nvidia-smi at 200 ms where NVML is not available."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", 0x4))
 
     def __init__(self, device_index: int):
         self.dev = device_index
         self.proc = None
         self.path = os.path.join("/tmp", f"svf_clocks_{os.getpid()}.csv")
+        self.nvml = None
+        self.rows = []
+        try:
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            props = torch.cuda.get_device_properties(device_index)
+            try:   # the same physical GPU as the CUDA ordinal, whatever CUDA_VISIBLE_DEVICES says
+                handle = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+            except Exception:
+                handle = pynvml.nvmlDeviceGetHandleByIndex(device_index)
+            self.nvml = (pynvml, handle)
+            self.max_mhz = float(pynvml.nvmlDeviceGetMaxClockInfo(handle, pynvml.NVML_CLOCK_SM))
+        except Exception:
+            self.nvml = None
+
+    def _poll(self):
+        pynvml, h = self.nvml
+        while not self.stop_evt.is_set():
+            try:
+                sm = pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+                try:
+                    bits = pynvml.nvmlDeviceGetCurrentClocksEventReasons(h)
+                except Exception:
+                    bits = pynvml.nvmlDeviceGetCurrentClocksThrottleReasons(h)
+                self.rows.append((float(sm), int(bits)))
+            except Exception:
+                pass
+            self.stop_evt.wait(0.01)
 
     def __enter__(self):
+        if self.nvml:
+            import threading
+
+            self.stop_evt = threading.Event()
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -87,6 +130,10 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.nvml:
+            self.stop_evt.set()
+            self.thread.join(timeout=5)
+            return
         if self.proc:
             self.proc.terminate()
             try:
@@ -95,6 +142,18 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
+        if self.nvml:
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "source": "nvml"}
+            pynvml = self.nvml[0]
+            reasons = set()
+            for _, bits in self.rows:
+                for name, const, default in self.REASONS:
+                    if bits & getattr(pynvml, const, default):
+                        reasons.add(name)
+            sm = np.array([r[0] for r in self.rows])
+            return {"sm_mhz": float(np.median(sm)), "sm_mhz_min": float(sm.min()), "sm_max_mhz": self.max_mhz,
+                    "reasons": sorted(reasons), "samples": len(self.rows), "source": "nvml, 10 ms"}
         rows = []
         try:
             for line in open(self.path):
@@ -113,7 +172,7 @@ class ClockSampler:
                 if val.lower() == "active":
                     reasons.add(name)
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 def ring81_mesh():
