@@ -67,8 +67,8 @@ def log(*a):
 
 class ClockSampler:
     """SM clocks and clock-event (throttle) reasons sampled during the timed
-    region: NVML polled every 10 ms on a thread (read-only queries), or
-    nvidia-smi at 200 ms where NVML is not available."""
+    region: NVML polled every 10 ms on a thread (read-only queries), and
+    nvidia-smi at 200 ms, whose samples are reported where NVML gave none."""
 
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -84,14 +84,19 @@ class ClockSampler:
         self.path = os.path.join("/tmp", f"svf_clocks_{os.getpid()}.csv")
         self.nvml = None
         self.rows = []
-        try:
-            import pynvml
+        self.smi_id = str(device_index)
+        try:   # the same physical GPU as the CUDA ordinal, whatever CUDA_VISIBLE_DEVICES says
             import torch
 
+            self.smi_id = "GPU-" + str(torch.cuda.get_device_properties(device_index).uuid)
+        except Exception:
+            pass
+        try:
+            import pynvml
+
             pynvml.nvmlInit()
-            props = torch.cuda.get_device_properties(device_index)
-            try:   # the same physical GPU as the CUDA ordinal, whatever CUDA_VISIBLE_DEVICES says
-                handle = pynvml.nvmlDeviceGetHandleByUUID("GPU-" + str(props.uuid))
+            try:
+                handle = pynvml.nvmlDeviceGetHandleByUUID(self.smi_id)
             except Exception:
                 handle = pynvml.nvmlDeviceGetHandleByIndex(device_index)
             self.nvml = (pynvml, handle)
@@ -120,9 +125,9 @@ class ClockSampler:
             self.stop_evt = threading.Event()
             self.thread = threading.Thread(target=self._poll, daemon=True)
             self.thread.start()
-            return self
+        # nvidia-smi alongside: its samples stand in if NVML delivered none
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}",
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.smi_id}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
@@ -133,7 +138,6 @@ class ClockSampler:
         if self.nvml:
             self.stop_evt.set()
             self.thread.join(timeout=5)
-            return
         if self.proc:
             self.proc.terminate()
             try:
@@ -142,9 +146,7 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if self.nvml:
-            if not self.rows:
-                return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"], "source": "nvml"}
+        if self.nvml and self.rows:
             pynvml = self.nvml[0]
             reasons = set()
             for _, bits in self.rows:
