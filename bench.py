@@ -397,7 +397,7 @@ def learned_init_item(svf, ctx, layout, samples, W, H, ref_rmse, steps, dev, tru
                                                              "p90": float(np.quantile(fratio, 0.9))}},
             "model": "MLP 96-256-256-8 (64 half-vector bins + 32 pairs of the luminance slab -> log S, ks, kd), "
                      "features from the luminance pass, hidden layers on the tcgen05 tensor cores (BF16x3, FP32 "
-                     "accuracy); LM from its prediction with 1e-3 of the reference's initial damping"}
+                     "accuracy); LM from its prediction with 1e-4 of the reference's initial damping (the library default for the learned guess)"}
 
 
 def _fp64_brdf_rows(args):
