@@ -14,12 +14,19 @@ For every 16th texel (256 of the 4096) the reference's pipeline
 is deterministic) gives the initial guess, the fit, the RMSE and the iteration
 counts.  LeastSquaresFitSGGX caps LM at CurveFitSteps = 1024 iterations
 (svbrdf-fitting.hh:51); the iteration counts show where a 100 cap would bind.
+
+    python tests/golden/make_config0_golden.py --full
+
+does the same for all 4096 texels (tests/golden/ref_config0_full.npz; 64-texel
+BTFs, one per worker task) and records the wall time and worker count of the
+run.
 """
 from __future__ import annotations
 
 import multiprocessing as mp
 import os
 import sys
+import time
 
 import numpy as np
 
@@ -42,20 +49,50 @@ def fit_one(t):
     return r["init"], r["fit"], r["rmse"], r["iterations"], r["effective"]
 
 
+def fit_chunk(first):
+    """Texels first .. first+CHUNK-1 as one BTF of CHUNK texels."""
+    import oracle as O
+
+    tp = O.ring81_angles()
+    lp = O.angles_to_parabolic(tp)
+    ts = range(first, first + CHUNK)
+    rgb = np.stack([O.synth_render(SEED, t, O.synth_truth(SEED, MIX, t), lp) for t in ts])
+    btf = O.RefBTF.from_texels(tp, rgb)
+    rows = []
+    for x in range(CHUNK):
+        r = btf.fit_texel(x)
+        rows.append((r["init"], r["fit"], r["rmse"], r["iterations"], r["effective"]))
+    return rows
+
+
+CHUNK = 64
+
+
 def main():
     import oracle as O
 
     O.build()
     assert O.ref_available(), "oracle/_ref/libtempest_ref.so was not built (reference sources missing?)"
-    idx = np.arange(0, SIDE * SIDE, STEP, dtype=np.int64)
-    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
-        rows = pool.map(fit_one, [int(t) for t in idx])
+    full = "--full" in sys.argv[1:]
+    workers = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    if full:
+        idx = np.arange(SIDE * SIDE, dtype=np.int64)
+        with mp.get_context("spawn").Pool(workers) as pool:
+            rows = [r for chunk in pool.map(fit_chunk, list(range(0, SIDE * SIDE, CHUNK))) for r in chunk]
+    else:
+        idx = np.arange(0, SIDE * SIDE, STEP, dtype=np.int64)
+        with mp.get_context("spawn").Pool(workers) as pool:
+            rows = pool.map(fit_one, [int(t) for t in idx])
+    secs = time.perf_counter() - t0
     init, fit, rmse, it, ef = zip(*rows)
-    np.savez(os.path.join(HERE, "ref_config0.npz"), seed=SEED, mix=MIX, side=SIDE, idx=idx,
-             init=np.asarray(init, np.float32), fit=np.asarray(fit, np.float32), rmse=np.asarray(rmse, np.float32),
-             iterations=np.asarray(it, np.uint32), effective=np.asarray(ef, np.uint32))
-    print(f"{len(idx)} texels: mean rmse {np.mean(rmse):.4e}, iterations max {max(it)}, "
-          f"above 100: {sum(i > 100 for i in it)}")
+    extra = dict(wall_seconds=secs, workers=workers) if full else {}
+    np.savez(os.path.join(HERE, "ref_config0_full.npz" if full else "ref_config0.npz"), seed=SEED, mix=MIX,
+             side=SIDE, idx=idx, init=np.asarray(init, np.float32), fit=np.asarray(fit, np.float32),
+             rmse=np.asarray(rmse, np.float32), iterations=np.asarray(it, np.uint32),
+             effective=np.asarray(ef, np.uint32), **extra)
+    print(f"{len(idx)} texels in {secs:.0f} s on {workers} workers: mean rmse {np.mean(rmse):.4e}, "
+          f"iterations max {max(it)}, above 100: {sum(i > 100 for i in it)}")
 
 
 if __name__ == "__main__":
