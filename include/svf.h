@@ -28,7 +28,9 @@
  *     svbrdf-fitting.hh:55-65).
  *   - Buffers are caller-owned.  Every pointer argument may point to host
  *     memory or to device memory of the context's device; the library detects
- *     which.  Host buffers are staged through pinned memory in chunks.
+ *     which.  Host buffers are staged through pinned memory in chunks.  A
+ *     sample or output buffer in device memory of another GPU is rejected with
+ *     SVF_EINVAL before anything is launched.
  *
  * Errors are returned as svf_status codes; no exception crosses the ABI.
  * svf_last_error() gives a message for the calling thread's last failure.

@@ -91,6 +91,32 @@ bool is_device_pointer_on(const void* p, int dev)
     return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
+svf_status buffer_location(const void* p, const char* what, bool* on_device)
+{
+    *on_device = false;
+    if(!p)
+        return SVF_OK;
+    cudaPointerAttributes a;
+    if(cudaPointerGetAttributes(&a, p) != cudaSuccess)
+    {
+        cudaGetLastError();
+        return SVF_OK;   // memory CUDA does not know: pageable host memory
+    }
+    if(a.type == cudaMemoryTypeManaged)
+    {
+        *on_device = true;
+        return SVF_OK;
+    }
+    if(a.type != cudaMemoryTypeDevice)
+        return SVF_OK;
+    int dev = 0;
+    SVF_CUDA(cudaGetDevice(&dev));
+    if(a.device != dev)
+        return fail(SVF_EINVAL, "%s is device memory of GPU %d; the context runs on GPU %d", what, a.device, dev);
+    *on_device = true;
+    return SVF_OK;
+}
+
 svf_status check_ctx(svf_ctx* ctx)
 {
     if(!ctx)

@@ -142,6 +142,11 @@ inline uint64_t fnv1a(const void* data, size_t bytes, uint64_t h = 1469598103934
 bool is_device_pointer(const void* p);
 // Plain device memory (not managed, not host) of device `dev`.
 bool is_device_pointer_on(const void* p, int dev);
+// Where a caller's buffer that an entry point may hand to its kernels lives:
+// *on_device for device memory of the current device or managed memory, false
+// for host memory (pageable or pinned); SVF_EINVAL for device memory of
+// another GPU, which the kernels on this one must not read or write.
+svf_status buffer_location(const void* p, const char* what, bool* on_device);
 
 inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
 

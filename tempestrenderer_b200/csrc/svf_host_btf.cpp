@@ -203,7 +203,9 @@ svf_status svf_btf_decode(svf_ctx* ctx, const svf_btf* btf, uint64_t first, uint
         return SVF_OK;
     const uint64_t N = (uint64_t)btf->f.light_count * btf->f.light_count;
     const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * N;
-    if(is_device_pointer(samples))
+    bool out_dev = false;
+    SVF_TRY(buffer_location(samples, "samples", &out_dev));
+    if(out_dev)
     {
         SVF_CUDA(svf::launch_btf_decode(btf_args(btf, first, count, sample_type, samples), ctx->stream));
         SVF_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -383,7 +385,8 @@ svf_status svf_render_btf(svf_ctx* ctx, const float* lp, uint32_t L, const svf_s
     const uint64_t T = (uint64_t)maps->width * maps->height, N = (uint64_t)L * L;
     const uint32_t sc = maps->sigma_channels;
     const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * N;
-    const bool out_dev = is_device_pointer(samples);
+    bool out_dev = false;
+    SVF_TRY(buffer_location(samples, "samples", &out_dev));
     const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(T, (size_t(1) << 30) / texel_bytes));
     DevBuf md, buf;
     SVF_TRY(md.ensure(sizeof(float) * chunk * (3 + 3 + sc + 4)));
@@ -464,7 +467,8 @@ svf_status svf_refit_neighborhood(svf_ctx* ctx, const svf_btf_view* btf, const s
     if(T == 0)
         return SVF_OK;
     const size_t texel_bytes = (btf->sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)N;
-    const bool on_device = is_device_pointer(btf->samples);
+    bool on_device = false;
+    SVF_TRY(buffer_location(btf->samples, "samples", &on_device));
     size_t free_b = 0, total_b = 0;
     SVF_CUDA(cudaMemGetInfo(&free_b, &total_b));
     const size_t per_texel = sizeof(float) * (stride + 3 + 9 * (7 + 7 + 1) + 7 + 1 + 12) + 9 * sizeof(svf_texel_stats) +

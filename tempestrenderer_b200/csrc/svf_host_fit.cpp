@@ -67,7 +67,8 @@ svf_status svf_fit_texels(svf_ctx* ctx, const svf_btf_view* btf, const svf_fit_o
 
     const size_t elem = btf->sample_type == SVF_SAMPLES_F16 ? 2 : 4;
     const size_t texel_bytes = elem * 3 * (size_t)N;
-    const bool samples_on_device = is_device_pointer(btf->samples);
+    bool samples_on_device = false;
+    SVF_TRY(buffer_location(btf->samples, "samples", &samples_on_device));
     const bool default_init = opts->init_mode == SVF_INIT_DEFAULT;
     if(maps->ndf && !default_init)
         return fail(SVF_EINVAL, "the NDF map exists only with the default initial guess");
@@ -539,7 +540,7 @@ svf_status svf_fit_btfs(svf_ctx* ctx, const svf_btf_view* btfs, uint32_t n_btf, 
         x.stride = round_up((uint64_t)x.lay->L * x.lay->L, 8);
         x.stride3 = round_up(3ull * x.lay->L * x.lay->L, 8);
         x.texel_bytes = (v.sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)x.lay->L * x.lay->L;
-        x.on_device = is_device_pointer(v.samples);
+        SVF_TRY(buffer_location(v.samples, "samples", &x.on_device));
         x.default_init = o.init_mode == SVF_INIT_DEFAULT;
         if(x.default_init)
             SVF_TRY(prepare_init(ctx, x.lay, v.layout, &x.init));
@@ -884,7 +885,9 @@ svf_status svf_synth_btf(svf_ctx* ctx, uint32_t seed, uint32_t mix, const float*
     SVF_TRY(check_ctx(ctx));
     if(!samples || !lp)
         return fail(SVF_EINVAL, "null samples/lights");
-    if(!is_device_pointer(samples))
+    bool samples_dev = false;
+    SVF_TRY(buffer_location(samples, "samples", &samples_dev));
+    if(!samples_dev)
         return fail(SVF_EINVAL, "samples must be device memory");
     if(mix > 1 || (sample_type != SVF_SAMPLES_F32 && sample_type != SVF_SAMPLES_F16) || L < 1 || L > 160)
         return fail(SVF_EINVAL, "bad mix/sample_type/light_count");
@@ -896,7 +899,9 @@ svf_status svf_synth_btf(svf_ctx* ctx, uint32_t seed, uint32_t mix, const float*
     const uint64_t step = 1u << 20;
     float* truth_dev = nullptr;
     DevBuf d_truth;
-    const bool truth_host = truth && !is_device_pointer(truth);
+    bool truth_on_device = false;
+    SVF_TRY(buffer_location(truth, "truth", &truth_on_device));
+    const bool truth_host = truth && !truth_on_device;
     if(truth_host)
     {
         SVF_TRY(d_truth.ensure(sizeof(float) * 16 * std::min<uint64_t>(count, step)));

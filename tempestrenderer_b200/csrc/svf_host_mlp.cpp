@@ -531,7 +531,8 @@ svf_status svf_mlp_predict(svf_ctx* ctx, const svf_mlp* mlp, const void* samples
         return fail(SVF_EINVAL, "unknown sample_type %u", sample_type);
     const uint32_t N = mlp->L * mlp->L;
     const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * (size_t)N;
-    const bool on_device = is_device_pointer(samples);
+    bool on_device = false;
+    SVF_TRY(buffer_location(samples, "samples", &on_device));
     const uint32_t chunk = 65536;
     const uint32_t c = std::min(chunk, texels);
     const uint64_t stride = round_up(N, 8);

@@ -107,7 +107,8 @@ svf_status svf_render_btf_ms(svf_ctx* ctx, const float* lp, uint32_t L, const sv
     const uint64_t T = (uint64_t)maps->width * maps->height, N = (uint64_t)L * L;
     const uint32_t sc = maps->sigma_channels;
     const size_t texel_bytes = (sample_type == SVF_SAMPLES_F16 ? 2 : 4) * 3 * N;
-    const bool out_dev = is_device_pointer(samples_out);
+    bool out_dev = false;
+    SVF_TRY(buffer_location(samples_out, "samples", &out_dev));
     const uint64_t chunk = std::max<uint64_t>(1, std::min<uint64_t>(T, (size_t(1) << 28) / texel_bytes));
     DevBuf md, buf;
     SVF_TRY(md.ensure(sizeof(float) * chunk * (3 + 3 + sc + 4)));
