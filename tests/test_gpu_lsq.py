@@ -5,8 +5,11 @@ Tolerances:
 * BRDF: the RMS of (GPU f32 - FP64 model) over all pairs, relative to the RMS
   of the FP64 values, is <= 1e-5 (observed through a zero-iteration fit, whose
   RMSE is the RMS of the model error against the slice it is given).
-* Fit from a good start (perturbed ground truth): per texel, final RMSE <=
-  1.01 x the reference's + 1e-7.
+* Fit from a good start (the golden fits' perturbed ground truth): per texel,
+  final RMSE <= 1.01 x the reference's + 1e-7.
+* Fit from a rough start (ground truth moved by 15 % per parameter, 64 texels
+  of the uneven mix, every one of them also fitted by the oracle): such starts
+  reach the chaotic regime too, so the bar is the statistical one below.
 * Fit from the reference's default initial guess: LM from that rough start is
   chaotic -- the reference itself, started one float ulp away, ends more than
   1.01x worse on 2 of the 8 golden texels (5.6x on one; see
@@ -117,7 +120,7 @@ def test_batch_matches_single_and_device_pointers(gpu_ctx, oracle_lib, golden):
 
 def test_many_texels_against_oracle(gpu_ctx, oracle_lib, golden):
     """64 texels of the uneven parameter mix, each fitted by the GPU and by the
-    oracle LM from the same start."""
+    oracle LM (the reference's, bit for bit) from the same rough start."""
     lp = _lp(golden)
     T = 64
     lums, inits, ref_rmse = [], [], []
@@ -134,12 +137,12 @@ def test_many_texels_against_oracle(gpu_ctx, oracle_lib, golden):
     lums = np.stack(lums)
     inits = np.stack(inits)
     out, rmse, stats = gpu_ctx.lsq_fit_batch(lp, lums, inits)
-    for t in range(0, T, 4):
+    for t in range(T):
         _, r, _ = oracle_lib.lsq_fit(lums[t], lp, inits[t])
         ref_rmse.append(r)
     ref_rmse = np.array(ref_rmse)
-    mean_ratio, within, worst = parity_stats(rmse[::4], ref_rmse)
-    assert mean_ratio <= 1.01 and within >= 0.75, (np.c_[rmse[::4], ref_rmse], mean_ratio, within)
+    mean_ratio, within, worst = parity_stats(rmse, ref_rmse)
+    assert mean_ratio <= 1.01 and within >= 0.75, (np.c_[rmse, ref_rmse], mean_ratio, within, worst)
 
 
 def test_nonfinite_texel_is_flagged(gpu_ctx, oracle_lib, golden):
